@@ -1,0 +1,687 @@
+"""FP64 CPU restatement of the reference solver's per-timestep hot path.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: `tests/`,
+`__graft_entry__.smoke()` and the `cpu_baseline` leg of `bench.py` may call it,
+the product path (the CUDA library and its host mirror) never does.
+
+Parity status: pinned.  Each operator below is checked against golden vectors
+produced by the reference's own code built headlessly (oracle/refbuild ->
+oracle/_ref/libfsref.so, fixtures in tests/golden/).
+
+Layout: cell arrays are [nz, ny, nx] (x fastest, the reference's ARRAY_3D
+order, ARRAY_3D.h:98); MAC face arrays carry one extra entry on their own
+axis: u [nz, ny, nx+1], v [nz, ny+1, nx], w [nz+1, ny, nx].
+
+Arithmetic follows the reference expression by expression (same operand order
+and the same divisions), so with a single thread the stencil operators agree
+bit for bit; sums that the reference accumulates sequentially (dot products,
+the right-hand-side mean) are accumulated sequentially here too (`_seqsum`).
+
+Two modes exist where the reference's executed air/water step is defective:
+`faithful` reproduces the reference operator as it runs; `corrected` is the
+specification the GPU path implements.  Differences are listed per function.
+"""
+import math
+
+import numpy as np
+
+PI = 3.14159265358979323846  # MACROS.h:13
+G = 3                        # ghost width of the reference's ghost copies
+
+
+# ----------------------------------------------------------------------------
+# helpers
+# ----------------------------------------------------------------------------
+
+def _seqsum(a):
+    """Sequential left-to-right sum (the reference's single-thread order)."""
+    a = np.ravel(a)
+    if a.size == 0:
+        return 0.0
+    return float(np.cumsum(a)[-1])
+
+
+def _seqdot(a, b):
+    return _seqsum(np.ravel(a) * np.ravel(b))
+
+
+def face_shape(n, axis):
+    nx, ny, nz = n
+    return {0: (nz, ny, nx + 1), 1: (nz, ny + 1, nx), 2: (nz + 1, ny, nx)}[axis]
+
+
+def extrapolate_ghosts(phi, g=G):
+    """Ghosted copy of a cell field, linear extrapolation outward.
+
+    Faces follow FillGhostCellsContinuousDerivativesFrom
+    (FIELD_STRUCTURE_3D.h:1776-1895): ghost(-m) = 2*ghost(-m+1) - ghost(-m+2)
+    evaluated outward, i.e. (1+m)*phi0 - m*phi1.  Edges and corners, which the
+    reference fills only partially (three edges, FIELD_STRUCTURE_3D.h:1897-1940,
+    the rest commented out), are defined here by extending x first, then y over
+    the x-extended rows, then z: the same face values, and a well-defined edge.
+    Layout of the result: [nz+2g, ny+2g, nx+2g].
+    """
+    nz, ny, nx = phi.shape
+    a = np.zeros((nz + 2 * g, ny + 2 * g, nx + 2 * g))
+    a[g:g + nz, g:g + ny, g:g + nx] = phi
+    for m in range(1, g + 1):  # x
+        a[g:g + nz, g:g + ny, g - m] = 2.0 * a[g:g + nz, g:g + ny, g - m + 1] - a[g:g + nz, g:g + ny, g - m + 2]
+        a[g:g + nz, g:g + ny, g + nx - 1 + m] = 2.0 * a[g:g + nz, g:g + ny, g + nx - 2 + m] - a[g:g + nz, g:g + ny, g + nx - 3 + m]
+    for m in range(1, g + 1):  # y
+        a[g:g + nz, g - m, :] = 2.0 * a[g:g + nz, g - m + 1, :] - a[g:g + nz, g - m + 2, :]
+        a[g:g + nz, g + ny - 1 + m, :] = 2.0 * a[g:g + nz, g + ny - 2 + m, :] - a[g:g + nz, g + ny - 3 + m, :]
+    for m in range(1, g + 1):  # z
+        a[g - m] = 2.0 * a[g - m + 1] - a[g - m + 2]
+        a[g + nz - 1 + m] = 2.0 * a[g + nz - 2 + m] - a[g + nz - 3 + m]
+    return a
+
+
+def zero_ghosts(f, g=G):
+    """Ghosted copy with zero ghost values (FillGhostCellsZero,
+    FIELD_STRUCTURE_3D.h:538-661, with edges and corners also zero)."""
+    return np.pad(f, g)
+
+
+# ----------------------------------------------------------------------------
+# WENO5 (ADVECTION_METHOD_3D.h:42-279)
+# ----------------------------------------------------------------------------
+
+def _shift(fg, axis, s, g=G):
+    """View of the ghosted array fg shifted by s along `axis` over the
+    interior of the un-ghosted field."""
+    sl = [slice(g, fg.shape[d] - g) for d in range(3)]
+    ax = 2 - axis  # numpy axis of x is 2
+    sl[ax] = slice(g + s, fg.shape[ax] - g + s)
+    return fg[tuple(sl)]
+
+
+def _weno_smoothness(a, b, c, first):
+    # (T)13/12*(..)*(..) + (T)1/4*(..)*(..), ADVECTION_METHOD_3D.h:97-99
+    c1312 = 13.0 / 12.0
+    t = (a - 2.0 * b) + c
+    if first == 1:
+        q = (a - 4.0 * b) + 3.0 * c
+    elif first == 2:
+        q = a - c
+    else:
+        q = (3.0 * a - 4.0 * b) + c
+    return (c1312 * t) * t + (0.25 * q) * q
+
+
+def _weno_side(r1, r2, r3, r4, r5, eps):
+    s1 = _weno_smoothness(r1, r2, r3, 1)
+    s2 = _weno_smoothness(r2, r3, r4, 2)
+    s3 = _weno_smoothness(r3, r4, r5, 3)
+    a1 = (1.0 / 10.0 * 1.0) / ((eps + s1) * (eps + s1))
+    a2 = (6.0 / 10.0 * 1.0) / ((eps + s2) * (eps + s2))
+    a3 = (3.0 / 10.0 * 1.0) / ((eps + s3) * (eps + s3))
+    sm = (a1 + a2) + a3
+    w1, w2, w3 = a1 / sm, a2 / sm, a3 / sm
+    t1 = (r1 * 1.0 / 3.0 - r2 * 7.0 / 6.0) + r3 * 11.0 / 6.0
+    t2 = (r2 * (-1.0 / 6.0) + r3 * 5.0 / 6.0) + r4 * 1.0 / 3.0
+    t3 = (r3 * 1.0 / 3.0 + r4 * 5.0 / 6.0) - r5 * 1.0 / 6.0
+    return (w1 * t1 + w2 * t2) + w3 * t3
+
+
+def weno5_derivatives(fg, axis, inv_h, eps, g=G):
+    """One-sided WENO5 derivatives D-, D+ along `axis` of a ghosted field."""
+    f = lambda s: _shift(fg, axis, s, g)
+    m1 = inv_h * (f(-2) - f(-3))
+    m2 = inv_h * (f(-1) - f(-2))
+    m3 = inv_h * (f(0) - f(-1))
+    m4 = inv_h * (f(1) - f(0))
+    m5 = inv_h * (f(2) - f(1))
+    p1 = inv_h * (f(3) - f(2))
+    p2 = inv_h * (f(2) - f(1))
+    p3 = inv_h * (f(1) - f(0))
+    p4 = inv_h * (f(0) - f(-1))
+    p5 = inv_h * (f(-1) - f(-2))
+    return _weno_side(m1, m2, m3, m4, m5, eps), _weno_side(p1, p2, p3, p4, p5, eps)
+
+
+def _upwind_update(rho, dt, uvel, vvel, wvel, dxm, dxp, dym, dyp, dzm, dzp):
+    dx_ = np.where(uvel > 0, dxm, dxp)
+    dy_ = np.where(vvel > 0, dym, dyp)
+    dz_ = np.where(wvel > 0, dzm, dzp)
+    return rho - dt * ((uvel * dx_ + vvel * dy_) + wvel * dz_)
+
+
+def weno5_levelset(phi, u, v, w, dx, dt, eps):
+    """phi - dt*(u.grad phi) with WENO5 upwind derivatives; the upwind side
+    is the sign of the cell-averaged face velocity.  The stencil source is the
+    linearly extrapolated ghost copy of the current phi."""
+    inv = 1.0 / dx
+    pg = extrapolate_ghosts(phi)
+    dxm, dxp = weno5_derivatives(pg, 0, inv, eps)
+    dym, dyp = weno5_derivatives(pg, 1, inv, eps)
+    dzm, dzp = weno5_derivatives(pg, 2, inv, eps)
+    uc = (u[:, :, 1:] + u[:, :, :-1]) * 0.5
+    vc = (v[:, 1:, :] + v[:, :-1, :]) * 0.5
+    wc = (w[1:, :, :] + w[:-1, :, :]) * 0.5
+    return _upwind_update(phi, dt, uc, vc, wc, dxm, dxp, dym, dyp, dzm, dzp)
+
+
+def _face_velocities(axis, ug, vg, wg):
+    """Velocity at the faces of component `axis` (ADVECTION_METHOD_3D.h:207-224):
+    the component itself and 4-point averages of the other two, read from
+    zero-ghosted copies."""
+    S = lambda fg, dx_, dy_, dz_, shp: fg[G + dz_:G + dz_ + shp[0], G + dy_:G + dy_ + shp[1], G + dx_:G + dx_ + shp[2]]
+    nz, ny, nx = ug.shape[0] - 2 * G, ug.shape[1] - 2 * G, ug.shape[2] - 2 * G - 1
+    shp = face_shape((nx, ny, nz), axis)
+    if axis == 0:
+        uvel = S(ug, 0, 0, 0, shp)
+        vvel = (((S(vg, 0, 0, 0, shp) + S(vg, 0, 1, 0, shp)) + S(vg, -1, 0, 0, shp)) + S(vg, -1, 1, 0, shp)) * 0.25
+        wvel = (((S(wg, 0, 0, 0, shp) + S(wg, 0, 0, 1, shp)) + S(wg, -1, 0, 0, shp)) + S(wg, -1, 0, 1, shp)) * 0.25
+    elif axis == 1:
+        uvel = (((S(ug, 0, 0, 0, shp) + S(ug, 1, 0, 0, shp)) + S(ug, 0, -1, 0, shp)) + S(ug, 1, -1, 0, shp)) * 0.25
+        vvel = S(vg, 0, 0, 0, shp)
+        wvel = (((S(wg, 0, 0, 0, shp) + S(wg, 0, 0, 1, shp)) + S(wg, 0, -1, 0, shp)) + S(wg, 0, -1, 1, shp)) * 0.25
+    else:
+        uvel = (((S(ug, 0, 0, 0, shp) + S(ug, 1, 0, 0, shp)) + S(ug, 0, 0, -1, shp)) + S(ug, 1, 0, -1, shp)) * 0.25
+        vvel = (((S(vg, 0, 0, 0, shp) + S(vg, 0, 1, 0, shp)) + S(vg, 0, 0, -1, shp)) + S(vg, 0, 1, -1, shp)) * 0.25
+        wvel = S(wg, 0, 0, 0, shp)
+    return uvel, vvel, wvel
+
+
+def weno5_velocity(u, v, w, dx, dt, eps):
+    """Forward-Euler WENO5 self-advection of the three MAC components, every
+    face of each component grid (boundary faces included), velocity ghosts
+    zero, each component's stencil read from its own zero-ghosted copy.
+
+    The reference's WENO5 velocity call (ADVECTION_3D.h:317-319) passes the
+    x-component ghost copy as the stencil source of v and w as well; indexed
+    with v's and w's (i, j, k) that copy is read outside its own extent, so
+    that call has no well-defined result to reproduce.  The x component,
+    which does read its own copy, is identical in both."""
+    inv = 1.0 / dx
+    ug, vg, wg = zero_ghosts(u), zero_ghosts(v), zero_ghosts(w)
+    out = []
+    for axis, comp in enumerate((u, v, w)):
+        src = (ug, vg, wg)[axis]
+        uvel, vvel, wvel = _face_velocities(axis, ug, vg, wg)
+        dxm, dxp = weno5_derivatives(src, 0, inv, eps)
+        dym, dyp = weno5_derivatives(src, 1, inv, eps)
+        dzm, dzp = weno5_derivatives(src, 2, inv, eps)
+        out.append(_upwind_update(comp, dt, uvel, vvel, wvel, dxm, dxp, dym, dyp, dzm, dzp))
+    return tuple(out)
+
+
+# ----------------------------------------------------------------------------
+# Sussman reinitialisation (ADVECTION_METHOD_3D.h:745-1637,
+# EULERIAN_FLUID_SOLVER_3D.h Reinitialization)
+# ----------------------------------------------------------------------------
+
+def sign_function(phi, dx):
+    return phi / np.sqrt(phi * phi + dx * dx)
+
+
+def _godunov_axis(s, dm, dp):
+    """Per-axis Godunov selection of the reference's case tree.
+    Returns (value, code): code 0 = D-, 1 = D+, 2 = dropped (expansion)."""
+    sm, sp = s * dm, s * dp
+    both_pos = (sp >= 0) & (sm >= 0)
+    both_neg = (sp <= 0) & (sm <= 0) & ~both_pos
+    expansion = (sp > 0) & (sm < 0)
+    shock = (sp < 0) & (sm > 0)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ss = s * (np.abs(dp) - np.abs(dm)) / (dp - dm)
+    use_m = both_pos | (shock & (ss > 0))
+    use_p = both_neg | (shock & ~(ss > 0))
+    code = np.where(use_m, 0, np.where(use_p, 1, 2))
+    val = np.where(code == 0, dm, np.where(code == 1, dp, 0.0))
+    return val, code, shock
+
+
+def sussman_step(phi, s, dx, dtau, eps, typo=False, ghost_source=None):
+    """One forward-Euler pseudo-step phi - dtau*S*(|grad phi|_G - 1) with the
+    sign-preserving clamp (ADVECTION_METHOD_3D.h:1624-1634).
+
+    typo=True reproduces the two leaves of the reference tree that compute
+    sqrt(a^2) + b^2 - 1 instead of sqrt(a^2 + b^2) - 1 (x shock, y shock
+    resolved to D+, z expansion: ADVECTION_METHOD_3D.h:1463,1605).
+    ghost_source: ghosted array to read the stencil from (default: the
+    extrapolated copy of phi)."""
+    inv = 1.0 / dx
+    pg = extrapolate_ghosts(phi) if ghost_source is None else ghost_source
+    dxm, dxp = weno5_derivatives(pg, 0, inv, eps)
+    dym, dyp = weno5_derivatives(pg, 1, inv, eps)
+    dzm, dzp = weno5_derivatives(pg, 2, inv, eps)
+    gx, cx, shx = _godunov_axis(s, dxm, dxp)
+    gy, cy, shy = _godunov_axis(s, dym, dyp)
+    gz, cz, shz = _godunov_axis(s, dzm, dzp)
+    mag = np.sqrt((gx * gx + gy * gy) + gz * gz) - 1.0
+    if typo:
+        bad = shx & shy & (cy == 1) & (cz == 2)
+        mag = np.where(bad, (np.sqrt(gx * gx) + gy * gy) - 1.0, mag)
+    out = phi - dtau * s * mag
+    flip = s * out < 0.0
+    out = np.where(flip & (s < 0), -eps, np.where(flip & (s > 0), eps, out))
+    return out
+
+
+def reinitialization_block(phi, dx, iterations, scaling, eps, typo=False):
+    """S from the block's input phi, then `iterations` pseudo-steps of
+    dtau = dx/scaling, each reading freshly extrapolated ghosts."""
+    s = sign_function(phi, dx)
+    dtau = dx / scaling
+    for _ in range(iterations):
+        phi = sussman_step(phi, s, dx, dtau, eps, typo)
+    return phi
+
+
+# ----------------------------------------------------------------------------
+# Heaviside, density, viscosity
+# ----------------------------------------------------------------------------
+
+def heaviside_projection(phi, e):
+    """PROJECTION_3D.h:1452-1470."""
+    ooe, oop = 1.0 / e, 1.0 / PI
+    mid = (0.5 + phi * ooe * 0.5) + 0.5 * oop * np.sin(PI * phi * ooe)
+    return np.where(phi < -e, 0.0, np.where(phi > e, 1.0, mid))
+
+
+def heaviside_viscosity(phi, e):
+    """VISCOSITY_3D.h:1234-1253."""
+    ooe, oop = 1.0 / e, 1.0 / PI
+    mid = 0.5 * ((1.0 + phi * ooe) + oop * np.sin(PI * phi * ooe))
+    return np.where(phi < -e, 0.0, np.where(phi > e, 1.0, mid))
+
+
+def mix(neg, pos, h):
+    """value(phi) = neg + (pos - neg)*H(phi): neg is the phase at phi <= 0."""
+    return neg + (pos - neg) * h
+
+
+# ----------------------------------------------------------------------------
+# Pressure projection (PROJECTION_3D.h:416-1449, POISSON_SOLVER_3D.h)
+# ----------------------------------------------------------------------------
+
+def divergence(u, v, w, dx, dt):
+    """DetermineDivergence (PROJECTION_3D.h:681-722): zero-ghost MAC
+    divergence, then scaled by 1/dt."""
+    inv = 1.0 / dx
+    d = (inv * (u[:, :, 1:] - u[:, :, :-1]) + inv * (v[:, 1:, :] - v[:, :-1, :])) + inv * (w[1:, :, :] - w[:-1, :, :])
+    return d * (1.0 / dt)
+
+
+def face_betas(phi, rho_neg, rho_pos):
+    """beta on every MAC face from the sharp cell 1/rho
+    (POISSON_SOLVER_3D.h:1080-1085); zero on the box's wall faces."""
+    nz, ny, nx = phi.shape
+    var = 1.0 / np.where(phi <= 0, rho_neg, rho_pos)
+    a = np.abs(phi)
+
+    def beta(vc, vn, ac, an):
+        # written as the 'r' arm: vc*vn*(|n|+|c|)/(vn*|c| + vc*|n|)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return vc * vn * (an + ac) / (vn * ac + vc * an)
+
+    bx = np.zeros((nz, ny, nx + 1)); by = np.zeros((nz, ny + 1, nx)); bz = np.zeros((nz + 1, ny, nx))
+    bx[:, :, 1:-1] = beta(var[:, :, :-1], var[:, :, 1:], a[:, :, :-1], a[:, :, 1:])
+    by[:, 1:-1, :] = beta(var[:, :-1, :], var[:, 1:, :], a[:, :-1, :], a[:, 1:, :])
+    bz[1:-1, :, :] = beta(var[:-1, :, :], var[1:, :, :], a[:-1, :, :], a[1:, :, :])
+    return bx, by, bz, var
+
+
+def poisson_operator(phi, dx, rho_neg, rho_pos, deflate=True):
+    """Matrix-free form of BuildLinearSystemNodeJumpConditionVaribleCoefficient
+    (air/water branch, Neumann walls, POISSON_SOLVER_3D.h:1065-1214).
+
+    Row of cell c: diag = inv_dx2 * (sum of beta to full neighbours in the
+    order l, r, b, t, d, u), off-diagonal -beta*inv_dx2.  The first cell
+    (i=j=k=0) additionally adds the beta of its bottom and down Neumann ghosts
+    (the reference's deflation fix, :1145-1179); with the clamped ghost 1/rho
+    those betas equal 1/rho of that cell.  A coefficient sum of 0 becomes 1."""
+    bx, by, bz, var = face_betas(phi, rho_neg, rho_pos)
+    inv2 = 1.0 / (dx * dx)
+    coef = ((((bx[:, :, :-1] + bx[:, :, 1:]) + by[:, :-1, :]) + by[:, 1:, :]) + bz[:-1, :, :]) + bz[1:, :, :]
+    if deflate:
+        # beta to the clamped ghost: var*var*(|g|+|c|)/(var*|c|+var*|g|) with
+        # the ghost phi extrapolated; equals var unless both |phi| are 0.
+        pg = extrapolate_ghosts(phi, 1)
+        c = abs(phi[0, 0, 0]); gb = abs(pg[1, 0, 1]); gd = abs(pg[0, 1, 1]); vv = var[0, 0, 0]
+        beta_b = vv * vv * (gb + c) / (vv * gb + vv * c)
+        beta_d = vv * vv * (gd + c) / (vv * gd + vv * c)
+        coef[0, 0, 0] = (coef[0, 0, 0] + beta_b) + beta_d
+    coef = np.where(coef == 0, 1.0, coef)
+    return bx * inv2, by * inv2, bz * inv2, inv2 * coef
+
+
+def apply_poisson(op, p):
+    """q = A p in the reference's CSR row order (l, r, b, t, d, u, diag)."""
+    ax, ay, az, diag = op
+    pg = np.pad(p, 1)
+    c = (slice(1, -1),) * 3
+    q = np.zeros_like(p)
+    q = q + (-ax[:, :, :-1]) * pg[1:-1, 1:-1, :-2]
+    q = q + (-ax[:, :, 1:]) * pg[1:-1, 1:-1, 2:]
+    q = q + (-ay[:, :-1, :]) * pg[1:-1, :-2, 1:-1]
+    q = q + (-ay[:, 1:, :]) * pg[1:-1, 2:, 1:-1]
+    q = q + (-az[:-1, :, :]) * pg[:-2, 1:-1, 1:-1]
+    q = q + (-az[1:, :, :]) * pg[2:, 1:-1, 1:-1]
+    q = q + diag * p
+    return q
+
+
+def poisson_csr(op):
+    """The same operator as a CSR matrix in the reference's row numbering
+    (k, j, i order) and entry order; used to compare with the reference."""
+    ax, ay, az, diag = op
+    nz, ny, nx = diag.shape
+    vals, cols, rowptr = [], [], [0]
+    idx = lambda i, j, k: i + nx * (j + ny * k)
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                for (cond, val, col) in ((i > 0, ax[k, j, i], (i - 1, j, k)), (i < nx - 1, ax[k, j, i + 1], (i + 1, j, k)),
+                                         (j > 0, ay[k, j, i], (i, j - 1, k)), (j < ny - 1, ay[k, j + 1, i], (i, j + 1, k)),
+                                         (k > 0, az[k, j, i], (i, j, k - 1)), (k < nz - 1, az[k + 1, j, i], (i, j, k + 1))):
+                    if cond:
+                        vals.append(-val); cols.append(idx(*col))
+                vals.append(diag[k, j, i]); cols.append(idx(i, j, k))
+                rowptr.append(len(vals))
+    return np.array(vals), np.array(cols, dtype=np.int32), np.array(rowptr, dtype=np.int32)
+
+
+def pcg(apply_A, diag, b, x0, tol, max_iter, criterion="abs"):
+    """Jacobi-PCG of PCG_METHOD.cpp:4-126.
+
+    criterion "abs": stop when r.z < tol^2 (the reference's test, :87).
+    criterion "rel": stop when ||r||_2 / ||b||_2 < tol.
+    Returns (x, iterations, final r.z, final relative residual)."""
+    x = x0.copy()
+    r = b - apply_A(x)
+    p = r / diag
+    rz = _seqdot(r, p)
+    bnorm = math.sqrt(_seqdot(b, b)) or 1.0
+    it = 0
+    while it < max_iter:
+        q = apply_A(p)
+        alpha = rz / _seqdot(p, q)
+        x = x + alpha * p
+        r = r - alpha * q
+        s = r / diag
+        rz_old = rz
+        rz = _seqdot(r, s)
+        if criterion == "abs":
+            if rz < tol * tol:
+                break
+        elif math.sqrt(_seqdot(r, r)) / bnorm < tol:
+            break
+        beta = rz / rz_old
+        p = p * beta + s
+        it += 1
+    return x, it, rz, math.sqrt(_seqdot(r, r)) / bnorm
+
+
+def velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode="corrected", jc=None):
+    """UpdateVelocityByPressureGradientVariableDensity (PROJECTION_3D.h:1099-1449).
+
+    Same-side faces: u -= dt*(p_c - p_nb)/rho_c/dx with the sharp rho of the
+    cell on the face's + side.  Faces whose two cells have phi_c*phi_nb <= 0:
+    u -= dt*(p_c - p_nb -/+ jump)/rho_f/dx with rho_f the smeared density
+    (PROJECTION_3D Heaviside, eps = 1.5 dx) of the face-averaged phi.
+
+    faithful: only w is updated (the u and v branches of the reference are
+    gated on pipe-mode flags, :1188,1211,1297,1320) and the bottom face of the
+    first cell is updated against a zero ghost pressure (bc*bc_d >= 0 holds
+    for row index 0).  corrected: u, v and w updated, wall faces untouched."""
+    nz, ny, nx = phi.shape
+    rho_c = np.where(phi <= 0, rho_neg, rho_pos)
+    pg = extrapolate_ghosts(phi, 1)
+    jc = np.zeros_like(phi) if jc is None else jc
+    e = 1.5 * dx
+    inv = 1.0 / dx
+    out = [u.copy(), v.copy(), w.copy()]
+    axes = (2,) if mode == "faithful" else (0, 1, 2)
+    for axis in axes:
+        ax = 2 - axis
+        sl_c = [slice(None)] * 3; sl_n = [slice(None)] * 3
+        sl_c[ax] = slice(1, None); sl_n[ax] = slice(0, -1)
+        sl_c, sl_n = tuple(sl_c), tuple(sl_n)
+        ph_c, ph_n = phi[sl_c], phi[sl_n]
+        # face phi from the extrapolated ghost copy (interior faces only here)
+        face_phi = 0.5 * (ph_c + ph_n)
+        rho_f = mix(rho_neg, rho_pos, heaviside_projection(face_phi, e))
+        inv_rho_f = 1.0 / rho_f
+        inv_rho_c = 1.0 / rho_c[sl_c]
+        with np.errstate(invalid="ignore", divide="ignore"):
+            jump = (jc[sl_c] * np.abs(ph_n) + jc[sl_n] * np.abs(ph_c)) / (np.abs(ph_n) + np.abs(ph_c))
+        dp = p[sl_c] - p[sl_n]
+        same = ph_c * ph_n > 0
+        upd_same = dt * dp * inv_rho_c * inv
+        upd_neg = dt * (dp + jump) * inv_rho_f * inv
+        upd_pos = dt * (dp - jump) * inv_rho_f * inv
+        upd = np.where(same, upd_same, np.where(ph_c <= 0, upd_neg, upd_pos))
+        f = out[axis]
+        fs = [slice(None)] * 3
+        fs[ax] = slice(1, -1)
+        f[tuple(fs)] = f[tuple(fs)] - upd
+        if mode == "faithful" and axis == 2:
+            # the first cell's bottom face against the zero ghost pressure
+            c = phi[0, 0, 0]; g = pg[0, 1, 1]
+            fphi = 0.5 * (c + g)
+            if c * g > 0:
+                f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0) * (1.0 / rho_c[0, 0, 0]) * inv
+            else:
+                rf = mix(rho_neg, rho_pos, heaviside_projection(np.array(fphi), e))
+                jmp = 0.0
+                if c <= 0:
+                    f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0 + jmp) * (1.0 / rf) * inv
+                else:
+                    f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0 - jmp) * (1.0 / rf) * inv
+    return tuple(out)
+
+
+def projection(phi, u, v, w, dx, dt, rho_neg, rho_pos, tol, max_iter, mode="corrected", criterion="abs", p0=None):
+    """PROJECTION_3D::Solve for the air/water box with Neumann walls:
+    divergence, operator, RHS = -div minus its mean (POISSON_SOLVER_3D.h:225-246),
+    Jacobi-PCG, velocity correction.  Returns (u, v, w, p, info)."""
+    div = divergence(u, v, w, dx, dt)
+    op = poisson_operator(phi, dx, rho_neg, rho_pos)
+    b = -div
+    b = b - (1.0 / b.size) * _seqsum(b)
+    x0 = np.zeros_like(b) if p0 is None else p0
+    p, it, rz, rel = pcg(lambda x: apply_poisson(op, x), op[3], b, x0, tol, max_iter, criterion)
+    u2, v2, w2 = velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode)
+    return u2, v2, w2, p, {"iterations": it, "rz": rz, "rel_residual": rel, "b": b, "op": op}
+
+
+# ----------------------------------------------------------------------------
+# Viscosity (VISCOSITY_3D.h)
+# ----------------------------------------------------------------------------
+
+def _cell_ghost(phi):
+    return extrapolate_ghosts(phi, 1)
+
+
+def viscosity_samples(phi, axis):
+    """Level-set samples used by the viscous coefficients of component
+    `axis` (VISCOSITY_3D.h:462-470 for x, 502-510 for y, 541-549 for z):
+    face average (density), the two cells across the face (normal stress)
+    and four edge averages (shear), from a 1-layer extrapolated ghost copy."""
+    pg = _cell_ghost(phi)
+    nz, ny, nx = phi.shape
+    shp = face_shape((nx, ny, nz), axis)
+
+    def P(di, dj, dk):
+        return pg[1 + dk:1 + dk + shp[0], 1 + dj:1 + dj + shp[1], 1 + di:1 + di + shp[2]]
+
+    if axis == 0:
+        half = 0.5 * (P(-1, 0, 0) + P(0, 0, 0))
+        n_hi, n_lo = P(0, 0, 0), P(-1, 0, 0)
+        e1 = 0.25 * (((P(-1, 0, 0) + P(0, 0, 0)) + P(-1, 1, 0)) + P(0, 1, 0))   # cu
+        e2 = 0.25 * (((P(-1, 0, 0) + P(0, 0, 0)) + P(-1, -1, 0)) + P(0, -1, 0))  # cd
+        e3 = 0.25 * (((P(-1, 0, 0) + P(0, 0, 0)) + P(-1, 0, 1)) + P(0, 0, 1))   # ct
+        e4 = 0.25 * (((P(-1, 0, 0) + P(0, 0, 0)) + P(-1, 0, -1)) + P(0, 0, -1))  # cb
+    elif axis == 1:
+        half = 0.5 * (P(0, -1, 0) + P(0, 0, 0))
+        n_hi, n_lo = P(0, 0, 0), P(0, -1, 0)
+        e1 = 0.25 * (((P(0, -1, 0) + P(1, -1, 0)) + P(0, 0, 0)) + P(1, 0, 0))   # cu (x+)
+        e2 = 0.25 * (((P(-1, -1, 0) + P(0, -1, 0)) + P(-1, 0, 0)) + P(0, 0, 0))  # cl (x-)
+        e3 = 0.25 * (((P(0, -1, 1) + P(0, -1, 0)) + P(0, 0, 1)) + P(0, 0, 0))   # ct
+        e4 = 0.25 * (((P(0, -1, -1) + P(0, -1, 0)) + P(0, 0, -1)) + P(0, 0, 0))  # cb
+    else:
+        half = 0.5 * (P(0, 0, -1) + P(0, 0, 0))
+        n_hi, n_lo = P(0, 0, 0), P(0, 0, -1)
+        e1 = 0.25 * (((P(0, 0, -1) + P(1, 0, -1)) + P(0, 0, 0)) + P(1, 0, 0))   # ct (x+)
+        e2 = 0.25 * (((P(0, 0, -1) + P(-1, 0, -1)) + P(0, 0, 0)) + P(-1, 0, 0))  # cb (x-)
+        e3 = 0.25 * (((P(0, 0, -1) + P(0, 1, -1)) + P(0, 0, 0)) + P(0, 1, 0))   # cu (y+)
+        e4 = 0.25 * (((P(0, 0, -1) + P(0, -1, -1)) + P(0, 0, 0)) + P(0, -1, 0))  # cd (y-)
+    return half, n_hi, n_lo, e1, e2, e3, e4
+
+
+DIRECTIONS = ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1))
+
+
+def semi_implicit_coefficients(phi, axis, dx, dt, rho_neg, rho_pos, mu_neg, mu_pos):
+    """Coefficients of the semi-implicit system of component `axis`, in the
+    direction order of the reference's builder (coef_1..coef_6 = +x, -x, +y,
+    -y, +z, -z; POISSON_SOLVER_3D.h:3383-3411): 2 dt mu/rho_f on the two
+    normal arms, dt mu/rho_f on the tangential arms (VISCOSITY_3D.h:603-611,
+    744-749, 811-816, Re = 1).  mu on the normal arms is sampled at the two
+    cells across the face, on the tangential arms at the four-cell edge
+    averages; rho_f from the face-averaged phi.
+    Returns (coefs[6], rho_f, [mu_hi, mu_lo, mu_t1+, mu_t1-, mu_t2+, mu_t2-])."""
+    e = 1.5 * dx
+    half, n_hi, n_lo, e1, e2, e3, e4 = viscosity_samples(phi, axis)
+    rho_f = mix(rho_neg, rho_pos, heaviside_viscosity(half, e))
+    mu = [mix(mu_neg, mu_pos, heaviside_viscosity(a, e)) for a in (n_hi, n_lo, e1, e2, e3, e4)]
+    two = 2.0 * dt / (1.0 * rho_f)
+    one = dt / (1.0 * rho_f)
+    t1, t2 = [a for a in (0, 1, 2) if a != axis]
+    c = [None] * 6
+    c[2 * axis], c[2 * axis + 1] = two * mu[0], two * mu[1]
+    c[2 * t1], c[2 * t1 + 1] = one * mu[2], one * mu[3]
+    c[2 * t2], c[2 * t2 + 1] = one * mu[4], one * mu[5]
+    return c, rho_f, mu
+
+
+def semi_implicit_explicit_term(u, v, w, axis, dx, dt, rho_f, mu):
+    """u* + dt/rho_f * (transpose stress terms), VISCOSITY_3D.h:620-630
+    (x component; y and z by the same pattern), zero velocity ghosts."""
+    inv = 1.0 / dx
+    vel = (u, v, w)
+    g = [zero_ghosts(a, 1) for a in vel]
+    shp = vel[axis].shape
+
+    def F(comp, di, dj, dk):
+        a = g[comp]
+        return a[1 + dk:1 + dk + shp[0], 1 + dj:1 + dj + shp[1], 1 + di:1 + di + shp[2]]
+
+    off = {0: (1, 0, 0), 1: (0, 1, 0), 2: (0, 0, 1)}
+    others = [a for a in (0, 1, 2) if a != axis]
+    total = vel[axis]
+    coef = dt / (1.0 * rho_f)
+    for n, t in enumerate(others):
+        mu_p, mu_m = mu[2 + 2 * n], mu[3 + 2 * n]
+        ot = off[t]; oa = off[axis]
+        # d/dt( mu * d(vel_t)/d(axis) ) at the face of component `axis`
+        hi = mu_p * inv * (F(t, ot[0], ot[1], ot[2]) - F(t, ot[0] - oa[0], ot[1] - oa[1], ot[2] - oa[2]))
+        lo = mu_m * inv * (F(t, 0, 0, 0) - F(t, -oa[0], -oa[1], -oa[2]))
+        total = total + coef * (inv * (hi - lo))
+    return total
+
+
+def semi_implicit_system(coef, explicit_term, comp0, axis, inv2, unknown, dval):
+    """Assemble the semi-implicit system for one component in the
+    reference's row order (k, j, i over unknowns) and entry order
+    (-x, +x, -y, +y, -z, +z, diagonal).  Returns a dense operator closure,
+    the Jacobi diagonal, the RHS and the unknown index map."""
+    shp = comp0.shape
+    # entry order of the reference's rows: -x, +x, -y, +y, -z, +z
+    dirs = [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]
+    arm_of = {o: n for n, o in enumerate(DIRECTIONS)}
+    ug = np.pad(unknown, 1)
+    dg = np.pad(dval, 1)
+    coef_sum = np.zeros(shp)
+    rhs = explicit_term.copy()
+    nb_coef = []
+    for d in dirs:
+        c = coef[arm_of[d]] * 1.0
+        m = ug[1 + d[2]:1 + d[2] + shp[0], 1 + d[1]:1 + d[1] + shp[1], 1 + d[0]:1 + d[0] + shp[2]]
+        coef_sum = coef_sum + np.where(m, c, 0.0)
+        nb_coef.append((d, np.where(m, -c * inv2, 0.0), m))
+    for d in dirs:
+        c = coef[arm_of[d]]
+        m = ug[1 + d[2]:1 + d[2] + shp[0], 1 + d[1]:1 + d[1] + shp[1], 1 + d[0]:1 + d[0] + shp[2]]
+        coef_sum = coef_sum + np.where(~m, c, 0.0)
+    coef_sum = np.where(coef_sum == 0, 1.0, coef_sum)
+    diag = 1.0 + inv2 * coef_sum
+    for d in dirs:
+        c = coef[arm_of[d]]
+        m = ug[1 + d[2]:1 + d[2] + shp[0], 1 + d[1]:1 + d[1] + shp[1], 1 + d[0]:1 + d[0] + shp[2]]
+        val = dg[1 + d[2]:1 + d[2] + shp[0], 1 + d[1]:1 + d[1] + shp[1], 1 + d[0]:1 + d[0] + shp[2]]
+        rhs = rhs + np.where(~m, c * inv2 * val, 0.0)
+
+    def apply(x):
+        xg = np.pad(np.where(unknown, x, 0.0), 1)
+        q = np.zeros(shp)
+        for d, a, m in nb_coef:
+            q = q + a * xg[1 + d[2]:1 + d[2] + shp[0], 1 + d[1]:1 + d[1] + shp[1], 1 + d[0]:1 + d[0] + shp[2]]
+        q = q + diag * x
+        return np.where(unknown, q, 0.0)
+
+    return apply, np.where(unknown, diag, 1.0), np.where(unknown, rhs, 0.0)
+
+
+def solve_semi_implicit(comp0, coef, explicit_term, axis, dx, tol, max_iter, unknown=None, dval=None,
+                        criterion="abs", x0=None):
+    """Jacobi-PCG on the semi-implicit system of one component (the reference
+    solves it with the projection's PCG, VISCOSITY_3D.h:711)."""
+    shp = comp0.shape
+    unknown = np.ones(shp, dtype=bool) if unknown is None else unknown
+    dval = np.zeros(shp) if dval is None else dval
+    inv2 = 1.0 / (dx * dx)
+    apply, diag, rhs = semi_implicit_system(coef, explicit_term, comp0, axis, inv2, unknown, dval)
+    start = np.where(unknown, comp0 if x0 is None else x0, 0.0)
+    x, it, rz, rel = pcg(apply, diag, rhs, start, tol, max_iter, criterion)
+    return np.where(unknown, x, dval), it, rel
+
+
+def wall_normal_mask(n, axis):
+    """Unknown faces of component `axis` in the box: all but the two wall
+    planes normal to the axis."""
+    shp = face_shape(n, axis)
+    m = np.ones(shp, dtype=bool)
+    ax = 2 - axis
+    sl = [slice(None)] * 3
+    sl[ax] = 0; m[tuple(sl)] = False
+    sl[ax] = -1; m[tuple(sl)] = False
+    return m
+
+
+def viscosity_semi_implicit(phi, u, v, w, dx, dt, rho_neg, rho_pos, mu_neg, mu_pos, tol, max_iter, criterion="rel"):
+    """Semi-implicit viscosity for the box: per component, implicit in
+    d/dx_j(mu du_i/dx_j) (factor 2 on the normal arm), explicit transpose
+    terms; wall-normal faces are held at zero, tangential ghosts are zero."""
+    nx = phi.shape[2]; ny = phi.shape[1]; nz = phi.shape[0]
+    n = (nx, ny, nz)
+    out, iters = [], []
+    comps = (u, v, w)
+    for axis in range(3):
+        coef, rho_f, mu = semi_implicit_coefficients(phi, axis, dx, dt, rho_neg, rho_pos, mu_neg, mu_pos)
+        ex = semi_implicit_explicit_term(u, v, w, axis, dx, dt, rho_f, mu)
+        mask = wall_normal_mask(n, axis)
+        x, it, _ = solve_semi_implicit(comps[axis], coef, ex, axis, dx, tol, max_iter, mask, None, criterion)
+        out.append(np.where(mask, x, 0.0)); iters.append(it)
+    return tuple(out), iters
+
+
+# ----------------------------------------------------------------------------
+# CFL (EULERIAN_FLUID_SOLVER_3D.h:2673-2785)
+# ----------------------------------------------------------------------------
+
+def cfl_dt(u, v, w, dx, gravity_y, nu_max=0.0, surface_term=0.0):
+    """1/cfl with cfl = 0.5*(c + v + sqrt((c+v)^2 + 4 g^2 + 4 s^2));
+    c = sum max|u_d|/dx, g = sqrt(|g_y|/dx), v = nu_max*6/dx^2 when the
+    viscosity is explicit (0 when semi-implicit)."""
+    inv = 1.0 / dx
+    c_f = (np.max(np.abs(u)) * inv + np.max(np.abs(v)) * inv) + np.max(np.abs(w)) * inv
+    g_f = math.sqrt(abs(gravity_y) * inv)
+    inv2 = 1.0 / (dx * dx)
+    v_f = nu_max * ((2.0 * inv2 + 2.0 * inv2) + 2.0 * inv2)
+    s_f = surface_term
+    cv = c_f + v_f
+    cfl = 0.5 * (cv + math.sqrt((cv * cv + 4.0 * (g_f * g_f)) + 4.0 * (s_f * s_f)))
+    return 1.0 / cfl

@@ -1,0 +1,259 @@
+// Headless driver around the reference solver, built only to produce golden
+// vectors (test infrastructure, never part of the product path).
+//
+// It builds a SIMULATION_WORLD from a generated air/water .sim script exactly
+// as the reference application does (SIMULATION_WORLD.h:InitializeFormScript),
+// then lets the caller inject seeded interior fields and call single reference
+// operators on them.  Every call runs with number_of_threads = 1 and
+// thread_id 0, so the reference's barriers are no-ops and its ordered partial
+// sums become plain sequential sums.
+//
+// Field ids: 0 phi (cells), 1 u (x faces), 2 v (y faces), 3 w (z faces),
+// 4 pressure (cells).  Arrays are interior values only, x fastest:
+// idx = i + nx*(j + ny*k) with nx the extent of that field (n+1 on its own
+// face axis).
+#include "SIMULATION_WORLD.h"
+
+namespace {
+
+struct RefCase {
+  SIMULATION_WORLD world;
+};
+
+FIELD_STRUCTURE_3D<T>& field_of(RefCase* c, int id) {
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  switch (id) {
+    case 0: return s.water_levelset->signed_distance_field;
+    case 1: return *s.water_velocity_field_mac_x;
+    case 2: return *s.water_velocity_field_mac_y;
+    case 3: return *s.water_velocity_field_mac_z;
+    default: return s.water_projection->pressure_field;
+  }
+}
+
+template <class F>
+void for_interior(FIELD_STRUCTURE_3D<T>& f, F&& body) {
+  const GRID_STRUCTURE_3D& g = f.grid;
+  long idx = 0;
+  for (int k = g.k_start; k <= g.k_end; ++k)
+    for (int j = g.j_start; j <= g.j_end; ++j)
+      for (int i = g.i_start; i <= g.i_end; ++i) body(f.array_for_this(i, j, k), idx++);
+}
+
+// The reference's level set carries two ghost layers that its extrapolating
+// ghost fill reads for layers >= 2 (FIELD_STRUCTURE_3D.h:1776-1830).  Filling
+// them in place first, with the same routine, makes those reads well defined:
+// the loop runs outward, so layer m reads the freshly written layer m-1.
+void extrapolate_levelset_in_place(EULERIAN_FLUID_SOLVER_3D& s) {
+  s.water_levelset->signed_distance_field.FillGhostCellsContinuousDerivativesFrom(0, s.water_levelset->arr, false);
+}
+
+void zero_ghost_velocities(EULERIAN_FLUID_SOLVER_3D& s) {
+  s.vector_field_mac_ghost_x.FillGhostCellsZero(0, s.water_velocity_field_mac_x->array_for_this, true);
+  s.vector_field_mac_ghost_y.FillGhostCellsZero(0, s.water_velocity_field_mac_y->array_for_this, true);
+  s.vector_field_mac_ghost_z.FillGhostCellsZero(0, s.water_velocity_field_mac_z->array_for_this, true);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* fsref_create(const char* sim_path) {
+  RefCase* c = new RefCase;
+  c->world.InitializeFormScript(sim_path);
+  return c;
+}
+
+void fsref_destroy(void* h) { delete static_cast<RefCase*>(h); }
+
+void fsref_dims(void* h, int* out) {
+  const GRID_STRUCTURE_3D& g = static_cast<RefCase*>(h)->world.eulerian_solver.base_grid;
+  out[0] = g.i_res; out[1] = g.j_res; out[2] = g.k_res;
+}
+
+double fsref_dx(void* h) { return static_cast<RefCase*>(h)->world.eulerian_solver.base_grid.dx; }
+
+void fsref_set(void* h, int id, const double* src) {
+  for_interior(field_of(static_cast<RefCase*>(h), id), [&](T& v, long n) { v = src[n]; });
+}
+
+void fsref_get(void* h, int id, double* dst) {
+  for_interior(field_of(static_cast<RefCase*>(h), id), [&](T& v, long n) { dst[n] = v; });
+}
+
+// Extrapolated level-set ghosts (three layers on the faces of the box), as
+// the WENO5 stencil reads them.  Output layout: (n+6)^3, x fastest.
+void fsref_levelset_ghost(void* h, double* dst) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  extrapolate_levelset_in_place(s);
+  s.scalar_field_ghost.FillGhostCellsContinuousDerivativesFrom(0, s.water_levelset->arr, true);
+  const GRID_STRUCTURE_3D& g = s.base_grid;
+  long idx = 0;
+  for (int k = g.k_start - 3; k <= g.k_end + 3; ++k)
+    for (int j = g.j_start - 3; j <= g.j_end + 3; ++j)
+      for (int i = g.i_start - 3; i <= g.i_end + 3; ++i) dst[idx++] = s.scalar_field_ghost.array_for_this(i, j, k);
+}
+
+// One forward-Euler WENO5 level-set update (ADVECTION_METHOD_3D.h:42-279)
+// with the ghost copy filled from the current level set by linear
+// extrapolation and the MAC velocity ghosts zero-filled.
+void fsref_weno5_levelset(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  extrapolate_levelset_in_place(s);
+  s.scalar_field_ghost.FillGhostCellsContinuousDerivativesFrom(0, s.water_levelset->arr, true);
+  zero_ghost_velocities(s);
+  ADVECTION_METHOD_3D<T>::WENO5th(0, s.water_levelset->signed_distance_field, s.scalar_field_ghost,
+                                  s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z,
+                                  dt, *c->world.multithreading, s.advecting_field_variables->epsilon);
+}
+
+// One forward-Euler WENO5 update of the three MAC components.  own_ghost = 0
+// reproduces ADVECTION_3D.h:317-319 (the x-component ghost copy is the
+// stencil source for all three components); own_ghost = 1 gives each
+// component its own ghost copy.
+void fsref_weno5_velocity(void* h, double dt, int own_ghost) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  zero_ghost_velocities(s);
+  MULTITHREADING& mt = *c->world.multithreading;
+  const T eps = s.advecting_field_variables->epsilon_v;
+  FIELD_STRUCTURE_3D<T>& gx = s.vector_field_mac_ghost_x;
+  FIELD_STRUCTURE_3D<T>& gy = own_ghost ? s.vector_field_mac_ghost_y : s.vector_field_mac_ghost_x;
+  FIELD_STRUCTURE_3D<T>& gz = own_ghost ? s.vector_field_mac_ghost_z : s.vector_field_mac_ghost_x;
+  ADVECTION_METHOD_3D<T>::WENO5th(0, *s.water_velocity_field_mac_x, gx, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
+  ADVECTION_METHOD_3D<T>::WENO5th(0, *s.water_velocity_field_mac_y, gy, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
+  ADVECTION_METHOD_3D<T>::WENO5th(0, *s.water_velocity_field_mac_z, gz, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
+}
+
+// One reinitialisation block: S = phi0/sqrt(phi0^2 + dx^2) and
+// iteration_number_for_reinitialization Sussman pseudo-steps of
+// dtau = dx/scaling_number (EULERIAN_FLUID_SOLVER_3D.h Reinitialization).
+// refresh_ghosts = 0 is the reference call as it stands (the level set's own
+// ghost layers keep their value from before the block); refresh_ghosts = 1
+// re-extrapolates them before every pseudo-step.
+void fsref_reinitialization(void* h, double dt, int refresh_ghosts) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  extrapolate_levelset_in_place(s);
+  if (!refresh_ghosts) {
+    s.Reinitialization(0, dt);
+    return;
+  }
+  const T fictious_dt = s.base_grid.dx / s.scaling_number_for_reinitialization;
+  const GRID_STRUCTURE_3D& g = s.base_grid;
+  for (int k = g.k_start; k <= g.k_end; ++k)
+    for (int j = g.j_start; j <= g.j_end; ++j)
+      for (int i = g.i_start; i <= g.i_end; ++i) {
+        const T p = s.water_levelset->signed_distance_field(i, j, k);
+        s.sign_function(i, j, k) = p / sqrt(POW2(p) + POW2(s.water_levelset->grid.dx));
+      }
+  for (int it = 0; it < s.iteration_number_for_reinitialization; ++it) {
+    extrapolate_levelset_in_place(s);
+    s.advecting_field_variables->ReinitializationBySussman(0, fictious_dt, s.sign_function);
+  }
+}
+
+// PROJECTION_3D::Solve (PROJECTION_3D.h:416) on the injected phi and
+// velocities; returns the PCG/CG iteration count of the pressure solve.
+int fsref_projection(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  extrapolate_levelset_in_place(s);
+  s.water_projection->Solve(0, dt);
+  return s.water_projection->poisson_solver.linear_solver->num_iteration;
+}
+
+int fsref_poisson_rows(void* h) { return static_cast<RefCase*>(h)->world.eulerian_solver.water_projection->poisson_solver.A.N; }
+int fsref_poisson_nnz(void* h) { return static_cast<RefCase*>(h)->world.eulerian_solver.water_projection->poisson_solver.A.nz; }
+
+// CSR matrix, right-hand side (after mean removal) and solution of the last
+// pressure solve, in the reference's own row numbering.
+void fsref_poisson_csr(void* h, double* vals, int* cols, int* rowptr, double* b, double* x) {
+  POISSON_SOLVER_3D& ps = static_cast<RefCase*>(h)->world.eulerian_solver.water_projection->poisson_solver;
+  for (int n = 0; n < ps.A.nz; ++n) { vals[n] = ps.A.values[n]; cols[n] = ps.A.column_index[n]; }
+  for (int r = 0; r <= ps.A.N; ++r) rowptr[r] = ps.A.row_ptr[r];
+  for (int r = 0; r < ps.A.N; ++r) { b[r] = ps.b[r]; x[r] = ps.x[r]; }
+}
+
+// Divergence field of the last projection (cells, already divided by dt).
+void fsref_divergence(void* h, double* dst) {
+  PROJECTION_3D& p = *static_cast<RefCase*>(h)->world.eulerian_solver.water_projection;
+  for_interior(p.divergence_field, [&](T& v, long n) { dst[n] = v; });
+}
+
+// Explicit variable-viscosity update (VISCOSITY_3D.h:452-563), in place.
+void fsref_viscosity(void* h, double dt) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  extrapolate_levelset_in_place(s);
+  s.viscosity_solver->ApplyViscosity(0, s.epsilon_for_mollification, dt);
+}
+
+// Semi-implicit viscosity system for one MAC component through the reference
+// builder and linear solver (POISSON_SOLVER_3D.h:3359-3496 + selected solver):
+// (1 + sum c/dx^2) u_c - sum c_nb/dx^2 u_nb = explicit.  comp selects the
+// face field; coef holds 6 interior arrays back to back; every interior face
+// is an unknown, faces outside the component's grid are Dirichlet with the
+// ghost value of the velocity field (zero here).  Returns the iteration count.
+int fsref_semi_implicit_solve(void* h, int comp, const double* coef, const double* explicit_term, double* out) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  FIELD_STRUCTURE_3D<T>& vel = field_of(static_cast<RefCase*>(h), comp);
+  MULTITHREADING* mt = s.multithreading;
+  FIELD_STRUCTURE_3D<T> cf[6], ex;
+  FIELD_STRUCTURE_3D<int> bc;
+  const GRID_STRUCTURE_3D& g = vel.grid;
+  for (int m = 0; m < 6; ++m) {
+    cf[m].Initialize(mt, g.i_res, g.j_res, g.k_res, g.i_start, g.j_start, g.k_start, g.x_min, g.y_min, g.z_min, g.x_max, g.y_max, g.z_max, 1);
+    const long off = (long)m * g.ijk_res;
+    for_interior(cf[m], [&](T& v, long n) { v = coef[off + n]; });
+  }
+  ex.Initialize(mt, g.i_res, g.j_res, g.k_res, g.i_start, g.j_start, g.k_start, g.x_min, g.y_min, g.z_min, g.x_max, g.y_max, g.z_max, 1);
+  for_interior(ex, [&](T& v, long n) { v = explicit_term[n]; });
+  bc.Initialize(mt, g.i_res, g.j_res, g.k_res, g.i_start, g.j_start, g.k_start, g.x_min, g.y_min, g.z_min, g.x_max, g.y_max, g.z_max, 1);
+  for (int k = g.k_start - 1; k <= g.k_end + 1; ++k)
+    for (int j = g.j_start - 1; j <= g.j_end + 1; ++j)
+      for (int i = g.i_start - 1; i <= g.i_end + 1; ++i) {
+        const bool inside = i >= g.i_start && i <= g.i_end && j >= g.j_start && j <= g.j_end && k >= g.k_start && k <= g.k_end;
+        bc.array_for_this(i, j, k) = inside ? BC_FULL : BC_DIR;
+      }
+  POISSON_SOLVER_3D& ps = s.water_projection->poisson_solver;
+  ps.SolveForViscosity(0, vel, cf[0], cf[1], cf[2], cf[3], cf[4], cf[5], bc, ex);
+  for_interior(vel, [&](T& v, long n) { out[n] = v; });
+  return ps.linear_solver->num_iteration;
+}
+
+// dt limit before the CFL factor (EULERIAN_FLUID_SOLVER_3D.h:2673-2785).
+double fsref_cfl(void* h) { return static_cast<RefCase*>(h)->world.eulerian_solver.CFLOneTimeStep(); }
+
+// Mean curvature of the level set (LEVELSET_3D.h ComputeCurvatures).
+void fsref_curvature(void* h, double* dst) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  extrapolate_levelset_in_place(s);
+  s.water_levelset->ComputeCurvatures(0);
+  for_interior(s.water_levelset->curvature, [&](T& v, long n) { dst[n] = v; });
+}
+
+// Plain linear solve through the reference's selected LINEAR_SOLVER on a
+// caller-supplied CSR matrix (LINEAR_SOLVER.h:36).  Returns iterations.
+int fsref_linear_solve(void* h, int n, int nnz, const double* vals, const int* cols, const int* rowptr,
+                       const double* b, double* x) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  MULTITHREADING* mt = s.multithreading;
+  POISSON_SOLVER_3D& ps = s.water_projection->poisson_solver;
+  CSR_MATRIX<T> A;
+  A.Initialize(mt, n, nnz);
+  mt->SplitDomainIndex1D(0, n);
+  A.start_ix[0] = 0; A.end_ix[0] = n - 1; A.prev_row_array[0] = -1; A.values_ix_array[0] = 0;
+  for (int r = 0; r < n; ++r)
+    for (int q = rowptr[r]; q < rowptr[r + 1]; ++q) A.AssignValue(0, r, cols[q], vals[q]);
+  VECTOR_ND<T> xv, bv;
+  xv.Initialize(n, true);
+  bv.Initialize(n);
+  for (int r = 0; r < n; ++r) { xv[r] = x[r]; bv[r] = b[r]; }
+  FIELD_STRUCTURE_3D<int>& bc = s.water_projection->boundary_condition_field;
+  ps.linear_solver->Solve(0, A, xv, bv, bc);
+  for (int r = 0; r < n; ++r) x[r] = xv[r];
+  return ps.linear_solver->num_iteration;
+}
+
+}  // extern "C"

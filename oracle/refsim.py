@@ -1,0 +1,305 @@
+"""ctypes access to the headless reference build (oracle/_ref/libfsref.so).
+
+Test infrastructure only: golden-vector generation, reference-parity checks
+and the timed CPU baseline call into the reference solver through this
+module; the product path never imports it.
+
+The reference is configured the way its own application is, through a `.sim`
+script (SCRIPT_READER block syntax).  `write_sim` emits an air/water box
+scenario whose keys are the ones the reference reads:
+  SIMULATION_WORLD / WORLD_DISCRETIZATION_AIR_WATER / GRID_STRUCTURE_3D_LARGE
+  (SIMULATION_WORLD.h InitializeFormScript, WORLD_DISCRETIZATION_3D.h:73-90),
+  FLUID_SOLVER_UNIFORM_AIR_WATER (EULERIAN_FLUID_SOLVER_3D.h:192-260),
+  LEVELSET_ADVECTION / VELOCITY_ADVECTION (ADVECTION_3D.h InitializeFromBlock),
+  PROJECTION_WATER (PROJECTION_3D.h:178-230).
+The grid is n^3 cells on the unit cube: base_grid_min = 0 and
+base_grid_max = (n-1)/n so that dx = (max-min)/(res-1) = 1/n
+(GRID_STRUCTURE_3D.h:115).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libfsref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def available():
+    return os.path.exists(LIB_PATH)
+
+
+def _lib():
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.fsref_create.restype = ctypes.c_void_p
+    lib.fsref_create.argtypes = [ctypes.c_char_p]
+    lib.fsref_destroy.argtypes = [ctypes.c_void_p]
+    lib.fsref_dims.argtypes = [ctypes.c_void_p, _ip]
+    lib.fsref_dx.restype = ctypes.c_double
+    lib.fsref_dx.argtypes = [ctypes.c_void_p]
+    lib.fsref_set.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+    lib.fsref_get.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+    lib.fsref_levelset_ghost.argtypes = [ctypes.c_void_p, _dp]
+    lib.fsref_weno5_levelset.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.fsref_weno5_velocity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+    lib.fsref_reinitialization.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+    lib.fsref_projection.restype = ctypes.c_int
+    lib.fsref_projection.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.fsref_poisson_rows.restype = ctypes.c_int
+    lib.fsref_poisson_rows.argtypes = [ctypes.c_void_p]
+    lib.fsref_poisson_nnz.restype = ctypes.c_int
+    lib.fsref_poisson_nnz.argtypes = [ctypes.c_void_p]
+    lib.fsref_poisson_csr.argtypes = [ctypes.c_void_p, _dp, _ip, _ip, _dp, _dp]
+    lib.fsref_divergence.argtypes = [ctypes.c_void_p, _dp]
+    lib.fsref_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.fsref_semi_implicit_solve.restype = ctypes.c_int
+    lib.fsref_semi_implicit_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
+    lib.fsref_cfl.restype = ctypes.c_double
+    lib.fsref_cfl.argtypes = [ctypes.c_void_p]
+    lib.fsref_curvature.argtypes = [ctypes.c_void_p, _dp]
+    lib.fsref_linear_solve.restype = ctypes.c_int
+    lib.fsref_linear_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _dp, _dp]
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = _lib()
+    return _LIB
+
+
+def write_sim(path, n, *, water_drop=True, threads=1, tolerance=1e-10, max_iteration=100000,
+              solver="PCG", reinit_iterations=10, reinit_scaling=5, epsilon=1e-6,
+              water_density=1000.0, air_density=1.0, water_viscosity=1e-3, air_viscosity=1.8e-5,
+              gravity=(0.0, -9.8, 0.0), order=3, cfl=0.5, velocity_weno=True, surface_tension=0.0):
+    """Write an air/water box scenario in the reference's .sim syntax."""
+    hi = (n - 1) / n
+    b = lambda v: "true" if v else "false"
+    # The script's number syntax has no exponent (SCRIPT_READER.cpp:8):
+    # every real is written positionally at full double precision.
+    r = lambda x: np.format_float_positional(float(x), unique=True, trim="-")
+    text = f"""SIMULATION_WORLD
+{{
+	dt = 0.001
+	max_dt = 100
+	num_substeps = 1
+	CFL = {r(cfl)}
+	frame_rate = 30
+	use_eulerian_solver = true
+	use_sph_solver = false
+	use_solid_solver = false
+	use_sph_levelset = false
+	number_of_threads = {threads}
+	use_field_boundary = false
+	last_frame = 100000
+	auto_run = false
+	air_water_simulation = true
+	oil_water_simulation = false
+	WORLD_DISCRETIZATION_AIR_WATER
+	{{
+		large_bubble = true
+		small_bubble = false
+		GRID_STRUCTURE_3D_LARGE
+		{{
+			resolution_scale = 1
+			start_indices = (0,0,0)
+			base_grid_resolution = ({n}, {n}, {n})
+			base_grid_min = (0, 0, 0)
+			base_grid_max = ({r(hi)}, {r(hi)}, {r(hi)})
+		}}
+		padding_width = 2
+	}}
+	LOG
+	{{
+		max_log_level = 1
+		use_log_file = false
+		display_accum_time = false
+		use_log_screen = false
+		output_log_file_name = "log.txt"
+	}}
+}}
+
+FLUID_SOLVER_UNIFORM_AIR_WATER
+{{
+	use_water_solver = true
+	is_Levelset_advection_active = true
+	is_Velocity_advection_active = true
+	is_external_force_active = true
+	is_sourcing_active = true
+	is_projection_active = true
+	fastsweeping_reinitialization = false
+	sussmanstyle_reinitialization = true
+	scaling_number_for_reinitialization = {reinit_scaling}
+	iteration_number_for_reinitialization = {reinit_iterations}
+	use_delta_function_formulation = true
+	curvature_by_normal_vector = false
+	curvature_by_levelset = true
+	CSF_model = false
+	order_for_time_advancing = {order}
+	LEVELSET_ADVECTION
+	{{
+		use_csl = false
+		use_5th_weno = true
+		use_3rd_eno = false
+		epsilon = {r(epsilon)}
+	}}
+	VELOCITY_ADVECTION
+	{{
+		use_5th_weno_v = {b(velocity_weno)}
+		use_3rd_eno_v = {b(not velocity_weno)}
+		epsilon = {r(epsilon)}
+	}}
+	PROJECTION_WATER
+	{{
+		tolerance = {r(tolerance)}
+		max_iteration = {max_iteration}
+		air_bubble_rising = {b(not water_drop)}
+		water_drop = {b(water_drop)}
+		use_previous_pressure = false
+		poisson_solver_type = "{solver}"
+		use_2nd_order = false
+		use_variable_density = true
+		Dirichlet_Boundary_Condition = false
+		Neumann_Boundary_Condition = true
+	}}
+	ghost_width = 3
+	use_water_levelset = true
+	gravity = ({r(gravity[0])}, {r(gravity[1])}, {r(gravity[2])})
+	water_viscosity = {r(water_viscosity)}
+	water_density = {r(water_density)}
+	surface_tension = {r(surface_tension)}
+	air_viscosity = {r(air_viscosity)}
+	air_density = {r(air_density)}
+}}
+"""
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+def _ptr(a, ct=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+class RefCase:
+    """One reference solver instance built from a generated script."""
+
+    FIELDS = {"phi": 0, "u": 1, "v": 2, "w": 3, "p": 4}
+
+    def __init__(self, sim_path):
+        self._lib = lib()
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        saved = os.dup(1)
+        os.dup2(devnull, 1)  # the reference prints its configuration on stdout
+        try:
+            self.h = self._lib.fsref_create(sim_path.encode())
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+            os.close(devnull)
+        d = (ctypes.c_int * 3)()
+        self._lib.fsref_dims(self.h, d)
+        self.n = tuple(d)  # (nx, ny, nz)
+        self.dx = self._lib.fsref_dx(self.h)
+
+    def close(self):
+        if self.h:
+            self._lib.fsref_destroy(self.h)
+            self.h = None
+
+    def shape(self, name):
+        nx, ny, nz = self.n
+        return {"phi": (nz, ny, nx), "p": (nz, ny, nx), "u": (nz, ny, nx + 1),
+                "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx)}[name]
+
+    def set(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        assert a.shape == self.shape(name), (name, a.shape)
+        self._lib.fsref_set(self.h, self.FIELDS[name], _ptr(a))
+
+    def get(self, name):
+        a = np.empty(self.shape(name), dtype=np.float64)
+        self._lib.fsref_get(self.h, self.FIELDS[name], _ptr(a))
+        return a
+
+    def _quiet(self, fn, *args):
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        saved = os.dup(1)
+        os.dup2(devnull, 1)
+        try:
+            return fn(*args)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+            os.close(devnull)
+
+    def levelset_ghost(self):
+        nx, ny, nz = self.n
+        a = np.empty((nz + 6, ny + 6, nx + 6))
+        self._lib.fsref_levelset_ghost(self.h, _ptr(a))
+        return a
+
+    def weno5_levelset(self, dt):
+        self._lib.fsref_weno5_levelset(self.h, dt)
+
+    def weno5_velocity(self, dt, own_ghost):
+        self._lib.fsref_weno5_velocity(self.h, dt, int(own_ghost))
+
+    def reinitialization(self, dt, refresh_ghosts):
+        self._lib.fsref_reinitialization(self.h, dt, int(refresh_ghosts))
+
+    def projection(self, dt):
+        return self._quiet(self._lib.fsref_projection, self.h, dt)
+
+    def poisson_csr(self):
+        rows = self._lib.fsref_poisson_rows(self.h)
+        nnz = self._lib.fsref_poisson_nnz(self.h)
+        vals = np.empty(nnz)
+        cols = np.empty(nnz, dtype=np.int32)
+        rowptr = np.empty(rows + 1, dtype=np.int32)
+        b = np.empty(rows)
+        x = np.empty(rows)
+        self._lib.fsref_poisson_csr(self.h, _ptr(vals), _ptr(cols, ctypes.c_int), _ptr(rowptr, ctypes.c_int), _ptr(b), _ptr(x))
+        return vals, cols, rowptr, b, x
+
+    def divergence(self):
+        a = np.empty(self.shape("phi"))
+        self._lib.fsref_divergence(self.h, _ptr(a))
+        return a
+
+    def viscosity(self, dt):
+        self._lib.fsref_viscosity(self.h, dt)
+
+    def semi_implicit_solve(self, comp, coef, explicit_term):
+        name = {1: "u", 2: "v", 3: "w"}[comp]
+        coef = np.ascontiguousarray(coef, dtype=np.float64)
+        ex = np.ascontiguousarray(explicit_term, dtype=np.float64)
+        out = np.empty(self.shape(name))
+        it = self._quiet(self._lib.fsref_semi_implicit_solve, self.h, comp, _ptr(coef), _ptr(ex), _ptr(out))
+        return out, it
+
+    def cfl(self):
+        return self._lib.fsref_cfl(self.h)
+
+    def curvature(self):
+        a = np.empty(self.shape("phi"))
+        self._lib.fsref_curvature(self.h, _ptr(a))
+        return a
+
+    def linear_solve(self, vals, cols, rowptr, b, x0):
+        n = len(b)
+        vals = np.ascontiguousarray(vals, dtype=np.float64)
+        cols = np.ascontiguousarray(cols, dtype=np.int32)
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.array(x0, dtype=np.float64)
+        it = self._quiet(self._lib.fsref_linear_solve, self.h, n, len(vals), _ptr(vals), _ptr(cols, ctypes.c_int),
+                         _ptr(rowptr, ctypes.c_int), _ptr(b), _ptr(x))
+        return x, it

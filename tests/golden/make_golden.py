@@ -1,0 +1,148 @@
+"""Generate the golden vectors in tests/golden/ from the reference's own code.
+
+Runs the reference solver built headlessly (oracle/refbuild -> oracle/_ref/
+libfsref.so) on seeded synthetic inputs and stores inputs and outputs as
+.npz fixtures.  The fixtures travel with the repository; the reference build
+does not have to exist where the tests run.
+
+    python tests/golden/make_golden.py      (from the repository root)
+
+Every case is a single reference operator called with number_of_threads = 1
+on the air/water unit-cube box with Neumann pressure walls:
+  weno5_levelset   ADVECTION_METHOD_3D<T>::WENO5th on the level set
+  weno5_velocity   WENO5th on u, v, w (each with its own ghost copy)
+  reinit           one Reinitialization block (sign function + 10 Sussman
+                   pseudo-steps), ghosts re-extrapolated before each step
+  projection_*     PROJECTION_3D::Solve: divergence, CSR system, PCG, velocity
+                   update (the reference as it runs: only w corrected)
+  semi_implicit_*  POISSON_SOLVER_3D::SolveForViscosity on seeded coefficients
+  cfl              EULERIAN_FLUID_SOLVER_3D::CFLOneTimeStep
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
+sys.path.insert(0, ROOT)
+from oracle import refsim  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+WORK = os.path.join(OUT, "_sim")
+
+
+def sphere(n, c, r):
+    x = (np.arange(n) + 0.5) / n
+    return np.sqrt((x[None, None, :] - c[0]) ** 2 + (x[None, :, None] - c[1]) ** 2 + (x[:, None, None] - c[2]) ** 2) - r
+
+
+def box_sdf(n, hi):
+    """Signed distance to the box [0,hi0]x[0,hi1]x[0,hi2] at cell centres
+    (negative inside); the dam-break initial level set."""
+    x = (np.arange(n) + 0.5) / n
+    X, Y, Z = x[None, None, :], x[None, :, None], x[:, None, None]
+    q = [np.abs(X - hi[0] / 2) - hi[0] / 2, np.abs(Y - hi[1] / 2) - hi[1] / 2, np.abs(Z - hi[2] / 2) - hi[2] / 2]
+    outside = np.sqrt(sum(np.maximum(a, 0.0) ** 2 for a in q))
+    inside = np.minimum(np.maximum(np.maximum(q[0], q[1]), q[2]), 0.0)
+    return outside + inside
+
+
+def case(n, **kw):
+    os.makedirs(WORK, exist_ok=True)
+    path = refsim.write_sim(os.path.join(WORK, f"case_{n}.sim"), n, **kw)
+    return refsim.RefCase(path)
+
+
+def main():
+    rng = np.random.default_rng(20241203)
+    fixtures = {}
+
+    # WENO5 level set, random field and random face velocities, 11^3
+    n = 11
+    c = case(n)
+    phi = rng.normal(size=c.shape("phi")) * 0.1
+    vel = {k: rng.normal(size=c.shape(k)) * 0.3 for k in "uvw"}
+    for k, a in vel.items():
+        c.set(k, a)
+    c.set("phi", phi)
+    c.weno5_levelset(2e-3)
+    fixtures["weno5_levelset"] = dict(n=n, dx=c.dx, dt=2e-3, eps=1e-6, phi=phi, **vel, out=c.get("phi"))
+    c.close()
+
+    # WENO5 MAC self-advection, 10^3
+    n = 10
+    c = case(n)
+    vel = {k: rng.normal(size=c.shape(k)) * 0.3 for k in "uvw"}
+    for k, a in vel.items():
+        c.set(k, a)
+    c.weno5_velocity(2e-3, 1)
+    fixtures["weno5_velocity"] = dict(n=n, dx=c.dx, dt=2e-3, eps=1e-6, **vel,
+                                      out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"))
+    c.close()
+
+    # Sussman reinitialisation block on a noisy field (exercises every branch
+    # of the Godunov case tree), 12^3
+    n = 12
+    c = case(n)
+    phi = rng.normal(size=c.shape("phi")) * 0.1
+    c.set("phi", phi)
+    c.reinitialization(1e-3, 1)
+    fixtures["reinit"] = dict(n=n, dx=c.dx, iterations=10, scaling=5, eps=1e-6, phi=phi, out=c.get("phi"))
+    c.close()
+
+    # Projection, both phase conventions, 10^3.  The reference's curvature
+    # routine (called inside the projection for the jump term) exits the
+    # process where the central-difference gradient vanishes
+    # (LEVELSET_3D.h:1040-1044); the box SDF has such points on its medial
+    # planes, so it gets a small seeded perturbation.
+    n = 10
+    drop_phi = box_sdf(n, (0.4, 0.6, 1.0)) + 1e-3 * rng.normal(size=(n, n, n))
+    for name, water_drop, phi in (("projection_drop", True, drop_phi),
+                                  ("projection_bubble", False, sphere(n, (0.5, 0.4, 0.5), 0.3))):
+        c = case(n, water_drop=water_drop, tolerance=1e-9)
+        vel = {k: rng.normal(size=c.shape(k)) * 0.3 for k in "uvw"}
+        for k, a in vel.items():
+            c.set(k, a)
+        c.set("phi", phi)
+        it = c.projection(2e-3)
+        vals, cols, rowptr, b, x = c.poisson_csr()
+        fixtures[name] = dict(n=n, dx=c.dx, dt=2e-3, tol=1e-9, rho_neg=1000.0 if water_drop else 1.0,
+                              rho_pos=1.0 if water_drop else 1000.0, phi=phi, **vel, iterations=it,
+                              csr_vals=vals, csr_cols=cols, csr_rowptr=rowptr, b=b, x=x,
+                              div=c.divergence(), out_p=c.get("p"), out_u=c.get("u"), out_v=c.get("v"),
+                              out_w=c.get("w"))
+        c.close()
+
+    # Semi-implicit viscosity systems, 8^3
+    n = 8
+    c = case(n, tolerance=1e-9)
+    for axis, k in enumerate("uvw"):
+        shp = c.shape(k)
+        coef = rng.uniform(0.01, 0.3, size=(6,) + shp) * c.dx * c.dx
+        ex = rng.normal(size=shp)
+        comp0 = rng.normal(size=shp) * 0.1
+        c.set(k, comp0)
+        out, it = c.semi_implicit_solve(axis + 1, coef, ex)
+        fixtures[f"semi_implicit_{k}"] = dict(n=n, dx=c.dx, tol=1e-9, axis=axis, coef=coef, explicit=ex,
+                                             comp0=comp0, out=out, iterations=it)
+    c.close()
+
+    # CFL dt, 9^3
+    n = 9
+    c = case(n)
+    vel = {k: rng.normal(size=c.shape(k)) * s for k, s in zip("uvw", (0.5, 1.5, 0.7))}
+    for k, a in vel.items():
+        c.set(k, a)
+    fixtures["cfl"] = dict(n=n, dx=c.dx, gravity_y=-9.8, nu_max=max(1e-3 / 1000.0, 1.8e-5 / 1.0), **vel, out=c.cfl())
+    c.close()
+
+    for name, d in fixtures.items():
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **{k: np.asarray(v) for k, v in d.items()})
+        print("wrote", name)
+    for f in os.listdir(WORK):
+        os.remove(os.path.join(WORK, f))
+    os.rmdir(WORK)
+
+
+if __name__ == "__main__":
+    main()
