@@ -1,0 +1,140 @@
+// Shared device-side definitions of the B200 solver: padded array layout,
+// launch helpers and block reductions.
+//
+// HBM layout.  Every field is a padded 3-D array with a ghost ring of width 3
+// on all six sides (the WENO5 stencil reach), x fastest.  Stencil kernels
+// therefore never branch on the box boundary: ghost values are written by a
+// ghost-fill kernel (level set: linear extrapolation) or are permanently zero
+// (velocity ghosts, pressure-solve vector ghosts, coefficient faces on walls).
+// The reference stores the same x-fastest order (ARRAY_3D.h:98) with ghost
+// widths 2-3 per field (EULERIAN_FLUID_SOLVER_3D.h:405-431).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fsb {
+
+constexpr int GH = 3;  // ghost width
+
+struct Lay {
+  int nx, ny, nz;   // interior extent
+  int px, py;       // padded extent in x and y
+  int64_t slab;     // px*py
+  int64_t total;    // px*py*(nz+2*GH)
+  __host__ __device__ int64_t at(int i, int j, int k) const {
+    return ((int64_t)(k + GH) * py + (j + GH)) * px + (i + GH);
+  }
+};
+
+inline Lay make_lay(int nx, int ny, int nz) {
+  Lay l;
+  l.nx = nx; l.ny = ny; l.nz = nz;
+  l.px = nx + 2 * GH;
+  l.py = ny + 2 * GH;
+  l.slab = (int64_t)l.px * l.py;
+  l.total = l.slab * (nz + 2 * GH);
+  return l;
+}
+
+// Interior launch: one thread per (i, j, k), x fastest.
+struct Launch3 {
+  dim3 grid, block;
+};
+
+inline Launch3 launch3(int nx, int ny, int nz, int bx = 32, int by = 4, int bz = 2) {
+  Launch3 L;
+  L.block = dim3(bx, by, bz);
+  L.grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, (nz + bz - 1) / bz);
+  return L;
+}
+
+#define FS_IJK(L)                                      \
+  const int i = blockIdx.x * blockDim.x + threadIdx.x; \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y; \
+  const int k = blockIdx.z * blockDim.z + threadIdx.z; \
+  if (i >= (L).nx || j >= (L).ny || k >= (L).nz) return;
+
+// Block-wide sum of a double (any block size that is a multiple of 32, up
+// to 1024).  Result valid in thread 0.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double part[32];
+  const int lane = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) & 31;
+  const int warp = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) >> 5;
+  const int nwarps = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) part[warp] = v;
+  __syncthreads();
+  v = 0.0;
+  if (warp == 0) {
+    v = lane < nwarps ? part[lane] : 0.0;
+    v = warp_sum(v);
+  }
+  return v;
+}
+
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double partm[32];
+  const int lane = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) & 31;
+  const int warp = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) >> 5;
+  const int nwarps = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) partm[warp] = v;
+  __syncthreads();
+  v = 0.0;
+  if (warp == 0) {
+    v = lane < nwarps ? partm[lane] : 0.0;
+    v = warp_max(v);
+  }
+  return v;
+}
+
+__device__ __forceinline__ int flat_block() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+__device__ __forceinline__ int num_blocks() { return gridDim.x * gridDim.y * gridDim.z; }
+__device__ __forceinline__ bool thread0() { return threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0; }
+
+// Deterministic grid-wide reduction: every block writes its partial, the last
+// block to finish (counted with an atomic ticket) sums the partials in block
+// order and resets the ticket.  Returns true in the one thread that holds
+// the final value in *out_total (thread 0 of the last block).
+__device__ __forceinline__ bool grid_reduce_sum(double block_value, double* partials, unsigned int* ticket,
+                                                double* out_total) {
+  __shared__ bool is_last;
+  const int b = flat_block();
+  if (thread0()) {
+    partials[b] = block_value;
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == (unsigned int)(num_blocks() - 1));
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  double s = 0.0;
+  for (int q = tid; q < num_blocks(); q += nt) s += ((volatile double*)partials)[q];
+  s = block_sum(s);
+  if (tid == 0) {
+    *out_total = s;
+    *ticket = 0u;
+    return true;
+  }
+  return false;
+}
+
+}  // namespace fsb

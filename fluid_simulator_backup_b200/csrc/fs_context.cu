@@ -1,0 +1,844 @@
+// fs_ctx: device state of one simulation and the C ABI of include/fluid_b200.h.
+//
+// The host side here replaces the reference's thread-pool runtime
+// (MULTITHREADING.h, one fork/join per frame plus a barrier after every grid
+// loop) with one CUDA stream per context: every operator is a short sequence
+// of kernel launches on that stream, and the Krylov loops run as captured
+// CUDA graphs of 16 iterations whose kernels stop themselves once the solve
+// has converged, with one host check of the solver state per graph launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fluid_b200.h"
+#include "fs_kernels.h"
+
+using namespace fsb;
+
+namespace {
+
+thread_local char g_last_error[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof g_last_error, fmt, ap);
+  va_end(ap);
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return FS_CUDA_ERROR;                                                               \
+    }                                                                                     \
+  } while (0)
+
+#define CKS(expr)                  \
+  do {                             \
+    fs_status s_ = (expr);         \
+    if (s_ != FS_OK) return s_;    \
+  } while (0)
+
+constexpr int kGraphIters = 16;
+
+// A device buffer typed at run time (float or double storage).
+struct Buf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct fs_ctx {
+  fs_grid_desc grid{};
+  fs_params prm{};
+  bool fp32 = false;  // storage precision of the fields
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Lay Lc{}, Lu{}, Lv{}, Lw{};
+
+  std::vector<Buf> owned;
+  int64_t bytes = 0;
+
+  // fields (storage type S)
+  void *phi = nullptr, *s1 = nullptr, *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sgn = nullptr;
+  void *u = nullptr, *v = nullptr, *w = nullptr;
+  void *u0 = nullptr, *v0 = nullptr, *w0 = nullptr;
+  void *ua = nullptr, *va = nullptr, *wa = nullptr;
+  // pressure (FP64) and projection work
+  double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *r64 = nullptr;
+  // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
+  void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
+  void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
+  // viscosity systems, one per component (storage type S)
+  void* vs[3][9] = {};  // ax, ay, az, diag, rhs, x, r, p, q
+  // reductions
+  double* partials = nullptr;
+  unsigned int* tickets = nullptr;  // [8]
+  double* scalars = nullptr;        // [16]
+  PcgState* st = nullptr;           // device
+  PcgState* st_host = nullptr;      // pinned
+  double* sc_host = nullptr;        // pinned [16]
+  double* staging = nullptr;        // packed FP64 transfer buffer
+  std::map<int, cudaGraphExec_t> graphs;
+
+  size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
+};
+
+namespace {
+
+fs_status dalloc(fs_ctx* c, void** out, size_t bytes) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    return FS_OOM;
+  }
+  e = cudaMemsetAsync(p, 0, bytes, c->stream);
+  if (e != cudaSuccess) {
+    cudaFree(p);
+    set_error("cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    return FS_CUDA_ERROR;
+  }
+  c->owned.push_back({p, bytes});
+  c->bytes += (int64_t)bytes;
+  *out = p;
+  return FS_OK;
+}
+
+void release(fs_ctx* c) {
+  if (!c) return;
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  c->graphs.clear();
+  for (auto& b : c->owned) cudaFree(b.p);
+  c->owned.clear();
+  if (c->st_host) cudaFreeHost(c->st_host);
+  if (c->sc_host) cudaFreeHost(c->sc_host);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+const Lay& lay_of(const fs_ctx* c, int field) {
+  switch (field) {
+    case FS_FIELD_U: return c->Lu;
+    case FS_FIELD_V: return c->Lv;
+    case FS_FIELD_W: return c->Lw;
+    default: return c->Lc;
+  }
+}
+
+fs_status check_params(const fs_params* p) {
+  if (!p) { set_error("params is NULL"); return FS_INVALID_ARG; }
+  if (!(p->rho_neg > 0) || !(p->rho_pos > 0)) { set_error("densities must be positive"); return FS_INVALID_ARG; }
+  if (p->mu_neg < 0 || p->mu_pos < 0) { set_error("viscosities must be non-negative"); return FS_INVALID_ARG; }
+  if (p->order < 1 || p->order > 3) { set_error("order must be 1, 2 or 3"); return FS_INVALID_ARG; }
+  if (p->precision != FS_PRECISION_FP64 && p->precision != FS_PRECISION_FP32_REFINE) {
+    set_error("unknown precision %d", p->precision);
+    return FS_INVALID_ARG;
+  }
+  if (p->stop != FS_STOP_RELATIVE && p->stop != FS_STOP_ABSOLUTE) { set_error("unknown stop criterion"); return FS_INVALID_ARG; }
+  if (!(p->tolerance >= 0) || p->max_iteration < 0 || p->reinit_iterations < 0 || p->reinit_scaling <= 0) {
+    set_error("bad solver or reinitialisation settings");
+    return FS_INVALID_ARG;
+  }
+  if (p->precision == FS_PRECISION_FP32_REFINE && (!(p->inner_tolerance > 0) || p->max_outer < 1)) {
+    set_error("FP32_REFINE needs inner_tolerance > 0 and max_outer >= 1");
+    return FS_INVALID_ARG;
+  }
+  return FS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Krylov driver
+// ---------------------------------------------------------------------------
+
+template <class V>
+fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V* p, V* q, double tol, int max_iter,
+                  int criterion, int* iterations, double* rel, int* status) {
+  PcgState init{};
+  init.tol = tol;
+  init.max_iter = max_iter;
+  init.criterion = criterion;
+  *c->st_host = init;
+  CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
+  pcg_init<V>(A, b, x, r, p, c->st, c->partials, c->stream);
+  CK(cudaGetLastError());
+  auto it = c->graphs.find(key);
+  if (it == c->graphs.end()) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int n = 0; n < kGraphIters; ++n) pcg_iteration<V>(A, x, r, p, q, c->st, c->partials, c->stream);
+    CK(cudaStreamEndCapture(c->stream, &g));
+    cudaGraphExec_t ge;
+    CK(cudaGraphInstantiate(&ge, g, 0));
+    cudaGraphDestroy(g);
+    it = c->graphs.emplace(key, ge).first;
+  }
+  // one graph per 16 iterations; the kernels of a converged solve return at
+  // once, so the bound below only caps the number of host checks
+  const int max_launches = max_iter / kGraphIters + 2;
+  for (int n = 0; n < max_launches; ++n) {
+    CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->st_host->done) break;
+    CK(cudaGraphLaunch(it->second, c->stream));
+  }
+  CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const PcgState& s = *c->st_host;
+  if (iterations) *iterations = s.iter;
+  if (rel) *rel = s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0;
+  if (status) *status = s.status;
+  if (s.status == PCG_NONFINITE) {
+    set_error("non-finite residual in a PCG solve");
+    return FS_NONFINITE;
+  }
+  return FS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// operators, templated on the storage type S
+// ---------------------------------------------------------------------------
+
+template <class S>
+S* F(void* p) { return static_cast<S*>(p); }
+
+template <class S>
+fs_status advect_levelset_t(fs_ctx* c, double dt) {
+  const fs_params& P = c->prm;
+  const double eps = P.weno_epsilon, dx = c->grid.dx;
+  S *phi = F<S>(c->phi), *t1 = F<S>(c->s1), *t2 = F<S>(c->s2);
+  S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w);
+  cudaStream_t s = c->stream;
+  auto fe = [&](S* src, const S* base, S* out, double c0, double c1) {
+    fill_extrap<S>(src, c->Lc, s);
+    weno5_levelset<S>(src, base, out, u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, eps, dt, c0, c1, s);
+  };
+  if (P.order == 3 && !(P.flags & FS_FLAG_LEVELSET_FORWARD_EULER)) {
+    fe(phi, phi, t1, 0.0, 1.0);                        // phi1 = phi0 + dt L(phi0)
+    fe(t1, phi, t2, 0.75, 0.25);                       // phi2 = 3/4 phi0 + 1/4 (phi1 + dt L(phi1))
+    fe(t2, phi, t1, 1.0 / 3.0, 2.0 / 3.0);             // phi3 = 1/3 phi0 + 2/3 (phi2 + dt L(phi2))
+  } else if (P.order == 3) {
+    fe(phi, phi, t1, 0.0, 1.0);                        // the reference's order-3 level set: one Euler step
+  } else {
+    fe(phi, phi, t1, 0.0, 1.0);                        // Heun: phi1, then 1/2 phi0 + 1/2 (phi1 + dt L(phi1))
+    fe(t1, phi, t2, 0.5, 0.5);
+    std::swap(c->s1, c->s2);
+  }
+  std::swap(c->phi, c->s1);
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+template <class S>
+fs_status advect_velocity_t(fs_ctx* c, double dt) {
+  const double eps = c->prm.weno_epsilon, dx = c->grid.dx;
+  S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w);
+  weno5_mac<S>(u, F<S>(c->ua), u, v, w, c->Lu, c->Lu, c->Lv, c->Lw, 0, dx, eps, dt, c->stream);
+  weno5_mac<S>(v, F<S>(c->va), u, v, w, c->Lv, c->Lu, c->Lv, c->Lw, 1, dx, eps, dt, c->stream);
+  weno5_mac<S>(w, F<S>(c->wa), u, v, w, c->Lw, c->Lu, c->Lv, c->Lw, 2, dx, eps, dt, c->stream);
+  std::swap(c->u, c->ua);
+  std::swap(c->v, c->va);
+  std::swap(c->w, c->wa);
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+// One reinitialisation block from `in` into `out` (out may be `base`):
+// S from `in`, reinit_iterations pseudo-steps, the last one combined as
+// c0*base + c1*result.
+template <class S>
+fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, double c1, void* scrA, void* scrB) {
+  const fs_params& P = c->prm;
+  const double dx = c->grid.dx, dtau = dx / P.reinit_scaling;
+  const int n = P.reinit_iterations;
+  cudaStream_t s = c->stream;
+  if (n == 0) {
+    if (c0 != 0.0) axpby<S>(F<S>(out), F<S>(base), F<S>(in), c0, c1, c->Lc, s);
+    else if (out != in) CK(cudaMemcpyAsync(out, in, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s));
+    return FS_OK;
+  }
+  sign_function<S>(F<S>(in), F<S>(c->sgn), c->Lc, dx, s);
+  void* cur = in;
+  for (int it = 0; it < n; ++it) {
+    const bool last = it == n - 1;
+    void* dst = last ? out : (cur == scrA ? scrB : scrA);
+    fill_extrap<S>(F<S>(cur), c->Lc, s);
+    sussman_step<S>(F<S>(cur), F<S>(c->sgn), F<S>(base), F<S>(dst), c->Lc, dx, P.weno_epsilon, dtau,
+                    last ? c0 : 0.0, last ? c1 : 1.0, (P.flags & FS_FLAG_REINIT_TYPO) ? 1 : 0, s);
+    cur = dst;
+  }
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+template <class S>
+fs_status reinitialize_t(fs_ctx* c) {
+  // RK combination of reinitialisation blocks (EULERIAN_FLUID_SOLVER_3D.h:959-979, 1081-1109)
+  if (c->prm.order == 3) {
+    CKS(reinit_block_t<S>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3));
+    CKS(reinit_block_t<S>(c, c->s1, c->s4, c->phi, 0.75, 0.25, c->s2, c->s3));
+    CKS(reinit_block_t<S>(c, c->s4, c->phi, c->phi, 1.0 / 3.0, 2.0 / 3.0, c->s2, c->s3));
+  } else {
+    CKS(reinit_block_t<S>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3));
+    CKS(reinit_block_t<S>(c, c->s1, c->phi, c->phi, 0.5, 0.5, c->s2, c->s3));
+  }
+  return FS_OK;
+}
+
+template <class S>
+fs_status viscosity_t(fs_ctx* c, double dt, int* iters_out) {
+  const fs_params& P = c->prm;
+  if (!P.viscosity) {
+    if (iters_out) *iters_out = 0;
+    return FS_OK;
+  }
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  void* comps[3] = {c->u, c->v, c->w};
+  // all three systems from the pre-viscosity velocities
+  for (int a = 0; a < 3; ++a) {
+    viscosity_system<S>(F<S>(c->phi), F<S>(c->u), F<S>(c->v), F<S>(c->w), c->Lc, c->Lu, c->Lv, c->Lw, a,
+                        c->grid.dx, dt, P.rho_neg, P.rho_pos, P.mu_neg, P.mu_pos, F<S>(c->vs[a][0]),
+                        F<S>(c->vs[a][1]), F<S>(c->vs[a][2]), F<S>(c->vs[a][3]), F<S>(c->vs[a][4]), c->stream);
+    CK(cudaMemcpyAsync(c->vs[a][5], comps[a], lays[a]->total * c->S(), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  CK(cudaGetLastError());
+  int total = 0;
+  for (int a = 0; a < 3; ++a) {
+    Op7<S> A{F<S>(c->vs[a][0]), F<S>(c->vs[a][1]), F<S>(c->vs[a][2]), F<S>(c->vs[a][3]), *lays[a]};
+    int it = 0, st = 0;
+    CKS(run_pcg<S>(c, 100 + a, A, F<S>(c->vs[a][4]), F<S>(c->vs[a][5]), F<S>(c->vs[a][6]), F<S>(c->vs[a][7]),
+                   F<S>(c->vs[a][8]), P.viscosity_tolerance, P.viscosity_max_iteration, FS_STOP_RELATIVE, &it,
+                   nullptr, &st));
+    total += it;
+  }
+  for (int a = 0; a < 3; ++a) std::swap(c->vs[a][5], a == 0 ? c->u : (a == 1 ? c->v : c->w));
+  if (iters_out) *iters_out = total;
+  return FS_OK;
+}
+
+// PROJECTION_3D::Solve; c0/c1 fuse the RK combination with base (u0, v0, w0)
+template <class S>
+fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report* rep) {
+  const fs_params& P = c->prm;
+  const double dx = c->grid.dx;
+  cudaStream_t s = c->stream;
+  const bool faithful = (P.flags & FS_FLAG_FAITHFUL_PROJECTION) != 0;
+  S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w), *phi = F<S>(c->phi);
+  divergence_rhs<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, dt, c->b64, c->div64, c->partials, c->tickets + 0,
+                    c->scalars + 0, s);
+  subtract_mean(c->b64, c->Lc, c->scalars + 0, c->partials, c->tickets + 1, c->scalars + 1, s);
+  CK(cudaGetLastError());
+  int iters = 0, outer = 0, st = 0;
+  double rel = 0.0;
+  if (!c->fp32) {
+    build_pressure_operator<S, double>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (double*)c->pax, (double*)c->pay,
+                                       (double*)c->paz, (double*)c->pdiag, s);
+    Op7<double> A{(double*)c->pax, (double*)c->pay, (double*)c->paz, (double*)c->pdiag, c->Lc};
+    CKS(run_pcg<double>(c, 1, A, c->b64, c->p64, (double*)c->pr, (double*)c->pp, (double*)c->pq, P.tolerance,
+                        P.max_iteration, P.stop, &iters, &rel, &st));
+    outer = 1;
+  } else {
+    build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
+                                      (float*)c->paz, (float*)c->pdiag, s);
+    Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc};
+    const size_t vbytes = c->Lc.total * sizeof(float);
+    for (outer = 0; outer <= P.max_outer; ++outer) {
+      defect_residual<S>(phi, c->p64, c->b64, c->r64, (float*)c->prhs, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
+                         c->tickets + 2, c->scalars + 2, s);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const double bb = c->sc_host[1], rr = c->sc_host[2];
+      rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+      if (!std::isfinite(rel)) {
+        set_error("non-finite defect residual");
+        return FS_NONFINITE;
+      }
+      if (rel <= P.tolerance || outer == P.max_outer) break;
+      CK(cudaMemsetAsync(c->px, 0, vbytes, s));
+      int it = 0;
+      CKS(run_pcg<float>(c, 2, A, (float*)c->prhs, (float*)c->px, (float*)c->pr, (float*)c->pp, (float*)c->pq,
+                         P.inner_tolerance, P.max_iteration, FS_STOP_RELATIVE, &it, nullptr, &st));
+      iters += it;
+      add_correction(c->p64, (float*)c->px, c->Lc, s);
+    }
+    st = rel <= P.tolerance ? PCG_CONVERGED : PCG_MAXITER;
+  }
+  velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
+  velocity_correct<S>(v, F<S>(c->v0), c->p64, phi, c->Lv, c->Lc, 1, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
+  velocity_correct<S>(w, F<S>(c->w0), c->p64, phi, c->Lw, c->Lc, 2, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
+  CK(cudaGetLastError());
+  if (rep) {
+    divergence_norms<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, c->partials, c->tickets + 3, c->scalars + 4, s);
+    CK(cudaMemcpyAsync(c->sc_host, c->scalars, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    rep->iterations = iters;
+    rep->outer_iterations = outer;
+    rep->rel_residual = rel;
+    rep->rz = c->st_host->rz;
+    rep->div_l2 = std::sqrt(c->sc_host[4]);
+    rep->div_linf = c->sc_host[5];
+  }
+  if (st == PCG_MAXITER) {
+    set_error("pressure solve stopped at its iteration cap (relative residual %.3e)", rel);
+    return FS_NOT_CONVERGED;
+  }
+  return FS_OK;
+}
+
+template <class S>
+fs_status gravity_t(fs_ctx* c, double dt) {
+  const double* g = c->prm.gravity;
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  void* comps[3] = {c->u, c->v, c->w};
+  for (int a = 0; a < 3; ++a)
+    if (g[a] != 0.0) add_const_faces<S>(F<S>(comps[a]), *lays[a], a, dt * g[a], 1, c->stream);
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+// One SolveForRK stage (EULERIAN_FLUID_SOLVER_3D.h:1453-1476): advection,
+// gravity, viscosity, projection; the projection's velocity update also
+// applies the stage's RK combination with the step's initial velocity.
+template <class S>
+fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* rep) {
+  CKS(advect_velocity_t<S>(c, dt));
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  if (!(c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION)) {
+    // no penetration: advection also updates the wall faces, which hold zero
+    zero_walls<S>(F<S>(c->u), *lays[0], 0, c->stream);
+    zero_walls<S>(F<S>(c->v), *lays[1], 1, c->stream);
+    zero_walls<S>(F<S>(c->w), *lays[2], 2, c->stream);
+  }
+  CKS(gravity_t<S>(c, dt));
+  int vit = 0;
+  CKS(viscosity_t<S>(c, dt, &vit));
+  fs_solve_report pr{};
+  fs_status st = project_t<S>(c, dt, c0, c1, &pr);
+  if (st != FS_OK && st != FS_NOT_CONVERGED) return st;
+  if (rep) {
+    rep->pcg_iterations += pr.iterations;
+    rep->outer_iterations += pr.outer_iterations;
+    rep->viscosity_iterations += vit;
+    rep->projections += 1;
+    rep->max_rel_residual = std::max(rep->max_rel_residual, pr.rel_residual);
+    rep->div_l2 = pr.div_l2;
+    rep->div_linf = pr.div_linf;
+  }
+  return st;
+}
+
+template <class S>
+fs_status step_t(fs_ctx* c, double dt, fs_step_report* rep) {
+  const int order = c->prm.order;
+  fs_status worst = FS_OK;
+  CKS(advect_levelset_t<S>(c, dt));
+  const size_t bu = c->Lu.total * c->S(), bv = c->Lv.total * c->S(), bw = c->Lw.total * c->S();
+  if (order > 1) {
+    CK(cudaMemcpyAsync(c->u0, c->u, bu, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->v0, c->v, bv, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->w0, c->w, bw, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  auto stage = [&](double c0, double c1) -> fs_status {
+    fs_status s = stage_t<S>(c, dt, c0, c1, rep);
+    if (s == FS_NOT_CONVERGED) { worst = s; return FS_OK; }
+    return s;
+  };
+  if (order == 1) {
+    CKS(stage(0.0, 1.0));
+  } else if (order == 2) {
+    CKS(stage(0.0, 1.0));
+    CKS(stage(0.5, 0.5));
+  } else {
+    CKS(stage(0.0, 1.0));
+    CKS(stage(0.75, 0.25));
+    CKS(stage(1.0 / 3.0, 2.0 / 3.0));
+  }
+  CKS(reinitialize_t<S>(c));
+  return worst;
+}
+
+template <class S>
+fs_status cfl_t(fs_ctx* c, double* dt) {
+  absmax3<S>(F<S>(c->u), F<S>(c->v), F<S>(c->w), c->Lu, c->Lv, c->Lw, c->scalars + 8, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->sc_host + 8, c->scalars + 8, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const fs_params& P = c->prm;
+  const double inv = 1.0 / c->grid.dx, inv2 = 1.0 / (c->grid.dx * c->grid.dx);
+  const double c_f = (c->sc_host[8] * inv + c->sc_host[9] * inv) + c->sc_host[10] * inv;
+  const double g_f = std::sqrt(std::fabs(P.gravity[1]) * inv);
+  // semi-implicit viscosity imposes no limit; explicit (off) uses the reference's term
+  const double nu = P.viscosity ? 0.0 : std::max(P.mu_neg / P.rho_neg, P.mu_pos / P.rho_pos);
+  const double v_f = nu * ((2.0 * inv2 + 2.0 * inv2) + 2.0 * inv2);
+  const double cv = c_f + v_f;
+  const double cfl = 0.5 * (cv + std::sqrt(cv * cv + 4.0 * (g_f * g_f)));
+  *dt = P.cfl / cfl;
+  return FS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+void fs_params_default(fs_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->rho_neg = 1000.0;
+  p->rho_pos = 1.0;
+  p->mu_neg = 1e-3;
+  p->mu_pos = 1.8e-5;
+  p->gravity[0] = 0.0;
+  p->gravity[1] = -9.8;
+  p->gravity[2] = 0.0;
+  p->weno_epsilon = 1e-6;
+  p->reinit_iterations = 10;
+  p->reinit_scaling = 5;
+  p->order = 3;
+  p->precision = FS_PRECISION_FP64;
+  p->stop = FS_STOP_RELATIVE;
+  p->tolerance = 1e-6;
+  p->max_iteration = 20000;
+  p->inner_tolerance = 1e-2;
+  p->max_outer = 20;
+  p->viscosity = 1;
+  p->viscosity_tolerance = 1e-8;
+  p->viscosity_max_iteration = 1000;
+  p->cfl = 0.5;
+  p->flags = 0;
+}
+
+const char* fs_status_str(fs_status s) {
+  switch (s) {
+    case FS_OK: return "ok";
+    case FS_INVALID_ARG: return "invalid argument";
+    case FS_OOM: return "out of device memory";
+    case FS_NOT_CONVERGED: return "iterative solve not converged";
+    case FS_NONFINITE: return "non-finite value";
+    case FS_CUDA_ERROR: return "CUDA error";
+    case FS_TIMEOUT: return "timeout";
+    case FS_NOT_SUPPORTED: return "not supported";
+  }
+  return "unknown status";
+}
+
+const char* fs_last_error(void) { return g_last_error; }
+
+fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** out) {
+  if (!grid || !out) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  *out = nullptr;
+  if (grid->nx < 3 || grid->ny < 3 || grid->nz < 3 || !(grid->dx > 0)) {
+    set_error("grid must be at least 3^3 cells with dx > 0");
+    return FS_INVALID_ARG;
+  }
+  const int64_t cells = (int64_t)grid->nx * grid->ny * grid->nz;
+  if (grid->nx > 4096 || grid->ny > 4096 || grid->nz > 4096 || cells > (int64_t)1 << 32) {
+    set_error("grid too large for one context");
+    return FS_INVALID_ARG;
+  }
+  fs_params prm;
+  if (params) prm = *params; else fs_params_default(&prm);
+  CKS(check_params(&prm));
+  fs_ctx* c = new (std::nothrow) fs_ctx();
+  if (!c) { set_error("host allocation failed"); return FS_OOM; }
+  c->grid = *grid;
+  c->prm = prm;
+  c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
+  c->Lc = make_lay(grid->nx, grid->ny, grid->nz);
+  c->Lu = make_lay(grid->nx + 1, grid->ny, grid->nz);
+  c->Lv = make_lay(grid->nx, grid->ny + 1, grid->nz);
+  c->Lw = make_lay(grid->nx, grid->ny, grid->nz + 1);
+  auto fail = [&](fs_status s) { release(c); delete c; return s; };
+  if (cudaGetDevice(&c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    set_error("CUDA stream/event creation failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return fail(FS_CUDA_ERROR);
+  }
+  const size_t S = c->S();
+  const size_t cb = c->Lc.total * S, ub = c->Lu.total * S, vb = c->Lv.total * S, wb = c->Lw.total * S;
+  const size_t c8 = c->Lc.total * sizeof(double);
+  const size_t V = c->fp32 ? sizeof(float) : sizeof(double);
+  const size_t cv = c->Lc.total * V;
+  fs_status s = FS_OK;
+  void** cell_s[] = {&c->phi, &c->s1, &c->s2, &c->s3, &c->s4, &c->sgn};
+  for (void** p : cell_s) if ((s = dalloc(c, p, cb)) != FS_OK) return fail(s);
+  void** fu[] = {&c->u, &c->u0, &c->ua};
+  void** fv[] = {&c->v, &c->v0, &c->va};
+  void** fw[] = {&c->w, &c->w0, &c->wa};
+  for (void** p : fu) if ((s = dalloc(c, p, ub)) != FS_OK) return fail(s);
+  for (void** p : fv) if ((s = dalloc(c, p, vb)) != FS_OK) return fail(s);
+  for (void** p : fw) if ((s = dalloc(c, p, wb)) != FS_OK) return fail(s);
+  double** d8[] = {&c->p64, &c->b64, &c->div64};
+  for (double** p : d8) if ((s = dalloc(c, (void**)p, c8)) != FS_OK) return fail(s);
+  if (c->fp32 && (s = dalloc(c, (void**)&c->r64, c8)) != FS_OK) return fail(s);
+  void** pv[] = {&c->pax, &c->pay, &c->paz, &c->pdiag, &c->pr, &c->pp, &c->pq};
+  for (void** p : pv) if ((s = dalloc(c, p, cv)) != FS_OK) return fail(s);
+  if (c->fp32) {
+    if ((s = dalloc(c, &c->px, cv)) != FS_OK) return fail(s);
+    if ((s = dalloc(c, &c->prhs, cv)) != FS_OK) return fail(s);
+  }
+  if (prm.viscosity) {
+    const size_t fb[3] = {ub, vb, wb};
+    for (int a = 0; a < 3; ++a)
+      for (int m = 0; m < 9; ++m)
+        if ((s = dalloc(c, &c->vs[a][m], fb[a])) != FS_OK) return fail(s);
+  }
+  const int nblk = std::max(pcg_blocks(c->Lu), std::max(pcg_blocks(c->Lv), pcg_blocks(c->Lw))) * 2 + 64;
+  if ((s = dalloc(c, (void**)&c->partials, (size_t)nblk * 3 * sizeof(double))) != FS_OK) return fail(s);
+  if ((s = dalloc(c, (void**)&c->tickets, 8 * sizeof(unsigned int))) != FS_OK) return fail(s);
+  if ((s = dalloc(c, (void**)&c->scalars, 16 * sizeof(double))) != FS_OK) return fail(s);
+  if ((s = dalloc(c, (void**)&c->st, sizeof(PcgState))) != FS_OK) return fail(s);
+  const int64_t maxf = std::max(std::max(c->Lu.total, c->Lv.total), std::max(c->Lw.total, c->Lc.total));
+  if ((s = dalloc(c, (void**)&c->staging, (size_t)maxf * sizeof(double))) != FS_OK) return fail(s);
+  if (cudaMallocHost((void**)&c->st_host, sizeof(PcgState)) != cudaSuccess ||
+      cudaMallocHost((void**)&c->sc_host, 16 * sizeof(double)) != cudaSuccess) {
+    set_error("pinned host allocation failed");
+    return fail(FS_OOM);
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error("initialisation failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return fail(FS_CUDA_ERROR);
+  }
+  *out = c;
+  return FS_OK;
+}
+
+fs_status fs_destroy(fs_ctx* c) {
+  if (!c) return FS_OK;
+  cudaStreamSynchronize(c->stream);
+  release(c);
+  delete c;
+  return FS_OK;
+}
+
+fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
+  if (!c || !p) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  CKS(check_params(p));
+  if (p->precision != c->prm.precision) { set_error("precision is fixed at creation"); return FS_INVALID_ARG; }
+  if (p->viscosity && !c->prm.viscosity) { set_error("viscosity buffers were not allocated at creation"); return FS_INVALID_ARG; }
+  c->prm = *p;
+  return FS_OK;
+}
+
+fs_status fs_memory_bytes(const fs_ctx* c, int64_t* bytes) {
+  if (!c || !bytes) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  *bytes = c->bytes;
+  return FS_OK;
+}
+
+static void** field_ptr(fs_ctx* c, int field) {
+  switch (field) {
+    case FS_FIELD_PHI: return &c->phi;
+    case FS_FIELD_U: return &c->u;
+    case FS_FIELD_V: return &c->v;
+    case FS_FIELD_W: return &c->w;
+    default: return nullptr;
+  }
+}
+
+static fs_status upload_from_staging(fs_ctx* c, int field) {
+  const Lay& L = lay_of(c, field);
+  if (field == FS_FIELD_PRESSURE) {
+    unpack_from_double<double>(c->p64, c->staging, L, c->stream);
+  } else {
+    void* dst = *field_ptr(c, field);
+    if (c->fp32) unpack_from_double<float>((float*)dst, c->staging, L, c->stream);
+    else unpack_from_double<double>((double*)dst, c->staging, L, c->stream);
+  }
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+static fs_status download_to_staging(fs_ctx* c, int field) {
+  const Lay& L = lay_of(c, field);
+  if (field == FS_FIELD_PRESSURE) pack_to_double<double>(c->staging, c->p64, L, c->stream);
+  else if (field == FS_FIELD_DIVERGENCE) pack_to_double<double>(c->staging, c->div64, L, c->stream);
+  else {
+    void* src = *field_ptr(c, field);
+    if (c->fp32) pack_to_double<float>(c->staging, (const float*)src, L, c->stream);
+    else pack_to_double<double>(c->staging, (const double*)src, L, c->stream);
+  }
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+static int64_t field_count(const fs_ctx* c, int field) {
+  const Lay& L = lay_of(c, field);
+  return (int64_t)L.nx * L.ny * L.nz;
+}
+
+fs_status fs_upload(fs_ctx* c, int field, const double* host, const int64_t* strides) {
+  if (!c || !host) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  if (field < FS_FIELD_PHI || field > FS_FIELD_PRESSURE) { set_error("field %d cannot be uploaded", field); return FS_INVALID_ARG; }
+  const Lay& L = lay_of(c, field);
+  const int64_t n = field_count(c, field);
+  if (strides) {
+    std::vector<double> tmp((size_t)n);
+    for (int k = 0; k < L.nz; ++k)
+      for (int j = 0; j < L.ny; ++j)
+        for (int i = 0; i < L.nx; ++i)
+          tmp[((size_t)k * L.ny + j) * L.nx + i] = host[i * strides[0] + j * strides[1] + k * strides[2]];
+    CK(cudaMemcpyAsync(c->staging, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CKS(upload_from_staging(c, field));
+    CK(cudaStreamSynchronize(c->stream));
+    return FS_OK;
+  }
+  CK(cudaMemcpyAsync(c->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CKS(upload_from_staging(c, field));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_download(fs_ctx* c, int field, double* host, const int64_t* strides) {
+  if (!c || !host) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  if (field < FS_FIELD_PHI || field > FS_FIELD_DIVERGENCE) { set_error("unknown field %d", field); return FS_INVALID_ARG; }
+  const Lay& L = lay_of(c, field);
+  const int64_t n = field_count(c, field);
+  CKS(download_to_staging(c, field));
+  if (strides) {
+    std::vector<double> tmp((size_t)n);
+    CK(cudaMemcpyAsync(tmp.data(), c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < L.nz; ++k)
+      for (int j = 0; j < L.ny; ++j)
+        for (int i = 0; i < L.nx; ++i)
+          host[i * strides[0] + j * strides[1] + k * strides[2]] = tmp[((size_t)k * L.ny + j) * L.nx + i];
+    return FS_OK;
+  }
+  CK(cudaMemcpyAsync(host, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_upload_device(fs_ctx* c, int field, const double* dev) {
+  if (!c || !dev) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  if (field < FS_FIELD_PHI || field > FS_FIELD_PRESSURE) { set_error("field %d cannot be uploaded", field); return FS_INVALID_ARG; }
+  const Lay& L = lay_of(c, field);
+  if (field == FS_FIELD_PRESSURE) unpack_from_double<double>(c->p64, dev, L, c->stream);
+  else if (c->fp32) unpack_from_double<float>((float*)*field_ptr(c, field), dev, L, c->stream);
+  else unpack_from_double<double>((double*)*field_ptr(c, field), dev, L, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_download_device(fs_ctx* c, int field, double* dev) {
+  if (!c || !dev) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  if (field < FS_FIELD_PHI || field > FS_FIELD_DIVERGENCE) { set_error("unknown field %d", field); return FS_INVALID_ARG; }
+  const Lay& L = lay_of(c, field);
+  if (field == FS_FIELD_PRESSURE) pack_to_double<double>(dev, c->p64, L, c->stream);
+  else if (field == FS_FIELD_DIVERGENCE) pack_to_double<double>(dev, c->div64, L, c->stream);
+  else if (c->fp32) pack_to_double<float>(dev, (const float*)*field_ptr(c, field), L, c->stream);
+  else pack_to_double<double>(dev, (const double*)*field_ptr(c, field), L, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+#define DISPATCH(c, fn, ...) ((c)->fp32 ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))
+
+static fs_status timed_begin(fs_ctx* c) {
+  CK(cudaEventRecord(c->ev0, c->stream));
+  return FS_OK;
+}
+
+static fs_status timed_end(fs_ctx* c, float* ms) {
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  if (ms) CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  return FS_OK;
+}
+
+fs_status fs_step(fs_ctx* c, double dt, fs_step_report* rep) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
+  fs_step_report local{};
+  fs_step_report* r = rep ? rep : &local;
+  *r = fs_step_report{};
+  CKS(timed_begin(c));
+  fs_status s = DISPATCH(c, step_t, c, dt, r);
+  if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
+  CKS(timed_end(c, &r->ms));
+  return s;
+}
+
+fs_status fs_cfl_dt(fs_ctx* c, double* dt) {
+  if (!c || !dt) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  return DISPATCH(c, cfl_t, c, dt);
+}
+
+fs_status fs_project(fs_ctx* c, double dt, fs_solve_report* rep) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
+  fs_solve_report local{};
+  fs_solve_report* r = rep ? rep : &local;
+  CKS(timed_begin(c));
+  fs_status s = DISPATCH(c, project_t, c, dt, 0.0, 1.0, r);
+  if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
+  CKS(timed_end(c, &r->ms));
+  return s;
+}
+
+fs_status fs_advect_levelset(fs_ctx* c, double dt) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  const int order = c->prm.order, flags = c->prm.flags;
+  // a single forward-Euler update, whatever the time order
+  c->prm.order = 3;
+  c->prm.flags |= FS_FLAG_LEVELSET_FORWARD_EULER;
+  fs_status s = DISPATCH(c, advect_levelset_t, c, dt);
+  c->prm.order = order;
+  c->prm.flags = flags;
+  if (s != FS_OK) return s;
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_advect_velocity(fs_ctx* c, double dt) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(DISPATCH(c, advect_velocity_t, c, dt));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_reinitialize(fs_ctx* c) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  // one block: S from the current phi, reinit_iterations pseudo-steps
+  fs_status s = c->fp32 ? reinit_block_t<float>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3)
+                        : reinit_block_t<double>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3);
+  if (s != FS_OK) return s;
+  if (c->prm.reinit_iterations > 0) std::swap(c->phi, c->s1);
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_viscosity(fs_ctx* c, double dt, int* iterations) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (!(dt > 0)) { set_error("dt must be positive"); return FS_INVALID_ARG; }
+  CKS(DISPATCH(c, viscosity_t, c, dt, iterations));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_pcg_csr(fs_ctx* c, int n, int nnz, const double* values, const int* column_index, const int* row_ptr,
+                     const double* b, double* x, double tolerance, int max_iteration, int stop, int* iterations,
+                     double* residual);
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// Host-side declarations of the kernel launchers (one translation unit per
+// kernel family; all are explicitly instantiated for float and double).
+#pragma once
+
+#include "fs_common.cuh"
+
+namespace fsb {
+
+// ---- stencil family (fs_stencil.cu)
+template <class T> void fill_extrap(T* f, const Lay& L, cudaStream_t s);
+template <class T>
+void weno5_levelset(const T* src, const T* base, T* out, const T* u, const T* v, const T* w, const Lay& L,
+                    const Lay& Lu, const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c0, double c1,
+                    cudaStream_t s);
+template <class T>
+void weno5_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+               const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s);
+template <class T> void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s);
+template <class T>
+void sussman_step(const T* src, const T* sgn, const T* base, T* out, const Lay& L, double dx, double eps, double dtau,
+                  double c0, double c1, int typo, cudaStream_t s);
+template <class T> void axpby(T* out, const T* x, const T* y, double a, double b, const Lay& L, cudaStream_t s);
+template <class T> void add_const_faces(T* f, const Lay& L, int axis, double value, int skip_walls, cudaStream_t s);
+template <class T> void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s);
+
+// ---- Krylov solver state shared by the pressure and viscosity solves
+struct PcgState {
+  double rz, pq, rr, bb, beta, tol;
+  int iter, max_iter, done, criterion, status, pad;
+  unsigned int ticket;
+  unsigned int pad2;
+};
+
+enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_MAXITER = 2, PCG_NONFINITE = 3 };
+
+// Seven-point symmetric operator on a padded layout:
+// (A x)_c = diag_c x_c - sum_d (a_d[c] x_{c-e_d} + a_d[c+e_d] x_{c+e_d});
+// a_d[c] couples c-e_d and c.  Couplings across walls are zero, so ghost
+// values of x never contribute.
+template <class V> struct Op7 {
+  const V* ax;
+  const V* ay;
+  const V* az;
+  const V* diag;
+  Lay L;
+};
+
+template <class V>
+void pcg_init(const Op7<V>& A, const V* b, V* x, V* r, V* p, PcgState* st, double* partials, cudaStream_t s);
+template <class V>
+void pcg_iteration(const Op7<V>& A, V* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+int pcg_blocks(const Lay& L);
+
+// ---- projection family (fs_projection.cu)
+struct ProjParams {
+  double dx, dt, rho_neg, rho_pos;
+  int faithful;
+};
+template <class T>
+void divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
+                    double dx, double dt, double* b, double* div_out, double* partials, unsigned int* ticket,
+                    double* scalars, cudaStream_t s);
+void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* partials, unsigned int* ticket,
+                   double* scalars_out, cudaStream_t s);
+template <class T, class V>
+void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
+                             V* diag, cudaStream_t s);
+template <class T>
+void defect_residual(const T* phi, const double* p64, const double* b, double* r64, float* r32, const Lay& Lc, double dx,
+                     double rho_neg, double rho_pos, double* partials, unsigned int* ticket, double* rr_out,
+                     cudaStream_t s);
+void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s);
+template <class T>
+void velocity_correct(T* f, const T* base, const double* p, const T* phi, const Lay& Lf, const Lay& Lc, int axis,
+                      double dx, double dt, double rho_neg, double rho_pos, int faithful, double c0, double c1,
+                      cudaStream_t s);
+template <class T>
+void divergence_norms(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
+                      double dx, double* partials, unsigned int* ticket, double* out2, cudaStream_t s);
+template <class T>
+void absmax3(const T* u, const T* v, const T* w, const Lay& Lu, const Lay& Lv, const Lay& Lw, double* out3,
+             cudaStream_t s);
+template <class S, class D> void convert_copy(D* dst, const S* src, const Lay& L, cudaStream_t s);
+template <class T> void pack_to_double(double* dst, const T* src, const Lay& L, cudaStream_t s);
+template <class T> void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s);
+
+// ---- viscosity family (fs_viscosity.cu)
+template <class T>
+void viscosity_system(const T* phi, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+                      const Lay& Lw, int axis, double dx, double dt, double rho_neg, double rho_pos, double mu_neg,
+                      double mu_pos, T* ax, T* ay, T* az, T* diag, T* rhs, cudaStream_t s);
+
+}  // namespace fsb

@@ -1,0 +1,391 @@
+// Variable-density ghost-fluid pressure projection, matrix free
+// (PROJECTION_3D.h:416-1449, POISSON_SOLVER_3D.h:165-252, 1030-1214).
+//
+//   divergence_rhs   b = -(div u)/dt and sum(b)           (DetermineDivergence, :681-744)
+//   subtract_mean    b -= mean(b), ||b||^2                 (POISSON_SOLVER_3D.h:225-246)
+//   build_pressure_operator  beta on faces and the diagonal from phi
+//                    (POISSON_SOLVER_3D.h:1075-1214; no CSR is ever built)
+//   defect_residual  r64 = b - A64 p64 with A64 evaluated on the fly in FP64
+//                    from phi: the FP64 residual of the FP32_REFINE path
+//   velocity_correct u -= dt grad p / rho (UpdateVelocityByPressureGradient-
+//                    VariableDensity, :1099-1449), fused with the RK combine
+#include "fs_kernels.h"
+
+namespace fsb {
+
+// beta of the face between cells with (1/rho, |phi|) = (vc, ac) and (vn, an),
+// written as the reference's right arm: vc*vn*(an+ac)/(vn*ac + vc*an).
+__device__ __forceinline__ double face_beta(double vc, double vn, double ac, double an) {
+  return vc * vn * (an + ac) / (vn * ac + vc * an);
+}
+
+template <class T>
+__device__ __forceinline__ double inv_rho(T phi, double rn, double rp) {
+  return 1.0 / ((double)phi <= 0.0 ? rn : rp);
+}
+
+template <class T>
+__global__ void k_divergence_rhs(const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, Lay Lc,
+                                 Lay Lu, Lay Lv, Lay Lw, double inv_h, double inv_dt, double* __restrict__ b,
+                                 double* __restrict__ div_out, double* partials, unsigned int* ticket,
+                                 double* scalars) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  double bv = 0.0;
+  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
+    const double d = (inv_h * ((double)u[Lu.at(i + 1, j, k)] - (double)u[Lu.at(i, j, k)]) +
+                      inv_h * ((double)v[Lv.at(i, j + 1, k)] - (double)v[Lv.at(i, j, k)])) +
+                     inv_h * ((double)w[Lw.at(i, j, k + 1)] - (double)w[Lw.at(i, j, k)]);
+    const double dv = d * inv_dt;
+    const int64_t c = Lc.at(i, j, k);
+    div_out[c] = dv;
+    bv = -dv;
+    b[c] = bv;
+  }
+  bv = block_sum(bv);
+  double tot;
+  if (grid_reduce_sum(bv, partials, ticket, &tot)) scalars[0] = tot;
+}
+
+__global__ void k_subtract_mean(double* __restrict__ b, Lay Lc, const double* mean_src, double inv_n,
+                                double* partials, unsigned int* ticket, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const double m = inv_n * mean_src[0];
+  double bb = 0.0;
+  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
+    const int64_t c = Lc.at(i, j, k);
+    const double v = b[c] - m;
+    b[c] = v;
+    bb = v * v;
+  }
+  bb = block_sum(bb);
+  double tot;
+  if (grid_reduce_sum(bb, partials, ticket, &tot)) out[0] = tot;
+}
+
+// Coefficients on the cell layout: ax[c] couples cell c-e_x and c (zero on
+// the walls i = 0 and i = nx, the latter a ghost column), likewise ay, az.
+// Entries are beta/dx^2, the diagonal is inv_dx2 * sum(beta over the six
+// faces) in the reference's order l, r, b, t, d, u; the first cell adds the
+// betas of its bottom and down Neumann ghosts (deflation, :1145-1179), and a
+// zero sum becomes one.
+template <class T, class V>
+__global__ void k_pressure_faces(const T* __restrict__ phi, Lay Lc, double rn, double rp, double inv2,
+                                 V* __restrict__ ax, V* __restrict__ ay, V* __restrict__ az) {
+  // one thread per cell, writing the couplings on its low faces; the
+  // (i = nx, j = ny, k = nz) ghost faces stay zero from allocation
+  FS_IJK(Lc);
+  const int64_t c = Lc.at(i, j, k);
+  const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
+  double bx = 0.0, by = 0.0, bz = 0.0;
+  if (i > 0) {
+    const double pn = (double)phi[c - 1];
+    bx = face_beta(inv_rho(phi[c - 1], rn, rp), vc, fabs(pn), acv);
+  }
+  if (j > 0) {
+    const double pn = (double)phi[c - Lc.px];
+    by = face_beta(inv_rho(phi[c - Lc.px], rn, rp), vc, fabs(pn), acv);
+  }
+  if (k > 0) {
+    const double pn = (double)phi[c - Lc.slab];
+    bz = face_beta(inv_rho(phi[c - Lc.slab], rn, rp), vc, fabs(pn), acv);
+  }
+  ax[c] = (V)(bx * inv2);
+  ay[c] = (V)(by * inv2);
+  az[c] = (V)(bz * inv2);
+}
+
+template <class T, class V>
+__global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, double rp, double inv2,
+                                V* __restrict__ diag) {
+  FS_IJK(Lc);
+  const int64_t c = Lc.at(i, j, k);
+  const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
+  double s = 0.0;
+  if (i > 0) s += face_beta(vc, inv_rho(phi[c - 1], rn, rp), acv, fabs((double)phi[c - 1]));
+  if (i < Lc.nx - 1) s += face_beta(vc, inv_rho(phi[c + 1], rn, rp), acv, fabs((double)phi[c + 1]));
+  if (j > 0) s += face_beta(vc, inv_rho(phi[c - Lc.px], rn, rp), acv, fabs((double)phi[c - Lc.px]));
+  if (j < Lc.ny - 1) s += face_beta(vc, inv_rho(phi[c + Lc.px], rn, rp), acv, fabs((double)phi[c + Lc.px]));
+  if (k > 0) s += face_beta(vc, inv_rho(phi[c - Lc.slab], rn, rp), acv, fabs((double)phi[c - Lc.slab]));
+  if (k < Lc.nz - 1) s += face_beta(vc, inv_rho(phi[c + Lc.slab], rn, rp), acv, fabs((double)phi[c + Lc.slab]));
+  if (i == 0 && j == 0 && k == 0) {
+    // deflation: the ghost 1/rho is the clamped copy of vc and the ghost phi
+    // the linear extrapolation 2 phi0 - phi1 along the axis
+    const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
+    const double gd = fabs(2.0 * pc - (double)phi[c + Lc.slab]);
+    s = (s + vc * vc * (gb + acv) / (vc * gb + vc * acv)) + vc * vc * (gd + acv) / (vc * gd + vc * acv);
+  }
+  if (s == 0.0) s = 1.0;
+  diag[c] = (V)(inv2 * s);
+}
+
+// r64 = b - A p64 with A from phi in FP64 (same formulas as the two kernels
+// above); also r32 = (float) r64 and ||r64||^2.
+template <class T>
+__global__ void k_defect_residual(const T* __restrict__ phi, const double* __restrict__ p, const double* __restrict__ b,
+                                  double* __restrict__ r64, float* __restrict__ r32, Lay Lc, double rn, double rp,
+                                  double inv2, double* partials, unsigned int* ticket, double* rr_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  double rr = 0.0;
+  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
+    const int64_t c = Lc.at(i, j, k);
+    const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc), xc = p[c];
+    double s = 0.0, off = 0.0;
+    const int64_t nb[6] = {c - 1, c + 1, c - Lc.px, c + Lc.px, c - Lc.slab, c + Lc.slab};
+    const bool ok[6] = {i > 0, i < Lc.nx - 1, j > 0, j < Lc.ny - 1, k > 0, k < Lc.nz - 1};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      if (!ok[q]) continue;
+      const double beta = face_beta(vc, inv_rho(phi[nb[q]], rn, rp), acv, fabs((double)phi[nb[q]]));
+      s += beta;
+      off += beta * p[nb[q]];
+    }
+    if (i == 0 && j == 0 && k == 0) {
+      const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
+      const double gd = fabs(2.0 * pc - (double)phi[c + Lc.slab]);
+      s = (s + vc * vc * (gb + acv) / (vc * gb + vc * acv)) + vc * vc * (gd + acv) / (vc * gd + vc * acv);
+    }
+    if (s == 0.0) s = 1.0;
+    const double ax = inv2 * s * xc - inv2 * off;
+    const double rv = b[c] - ax;
+    r64[c] = rv;
+    if (r32) r32[c] = (float)rv;
+    rr = rv * rv;
+  }
+  rr = block_sum(rr);
+  double tot;
+  if (grid_reduce_sum(rr, partials, ticket, &tot)) rr_out[0] = tot;
+}
+
+__global__ void k_add_correction(double* __restrict__ p, const float* __restrict__ e, Lay Lc) {
+  FS_IJK(Lc);
+  const int64_t c = Lc.at(i, j, k);
+  p[c] += (double)e[c];
+}
+
+__device__ __forceinline__ double heaviside_proj(double phi, double e) {
+  // PROJECTION_3D.h:1452-1470
+  const double ooe = 1.0 / e, oop = 1.0 / 3.14159265358979323846;
+  if (phi < -e) return 0.0;
+  if (phi > e) return 1.0;
+  return (0.5 + phi * ooe * 0.5) + 0.5 * oop * sin(3.14159265358979323846 * phi * ooe);
+}
+
+// Pressure-gradient update of one face component.  Face (i,j,k) of
+// component `axis` lies between cell c = (i,j,k) and the cell n one step
+// back along the axis.  Same-side faces use the sharp 1/rho of cell c, faces
+// across the interface the smeared density of the face-averaged phi.  Wall
+// faces are left alone (corrected) - in faithful mode only w is updated and
+// the first cell's bottom face sees the zero ghost pressure.  Then the RK
+// combination out = c0*base + c1*f (skipped when c0 == 0).
+template <class T>
+__global__ void k_velocity_correct(T* __restrict__ f, const T* __restrict__ base, const double* __restrict__ p,
+                                   const T* __restrict__ phi, Lay Lf, Lay Lc, int axis, double inv_h, double dt,
+                                   double rn, double rp, int faithful, double c0, double c1) {
+  FS_IJK(Lf);
+  const int64_t fc = Lf.at(i, j, k);
+  double val = (double)f[fc];
+  const int e = axis == 0 ? i : (axis == 1 ? j : k);
+  const int n = axis == 0 ? Lc.nx : (axis == 1 ? Lc.ny : Lc.nz);
+  const bool update_axis = !faithful || axis == 2;
+  const bool interior = e > 0 && e < n;
+  const bool quirk = faithful && axis == 2 && i == 0 && j == 0 && k == 0;
+  if (update_axis && (interior || quirk)) {
+    const int64_t c = Lc.at(i, j, k);
+    const int64_t step = axis == 0 ? 1 : (axis == 1 ? Lc.px : Lc.slab);
+    const double phc = (double)phi[c];
+    // across the bottom wall the ghost phi is the linear extrapolation and
+    // the ghost pressure is zero
+    const double phn = interior ? (double)phi[c - step] : 2.0 * phc - (double)phi[c + step];
+    const double pn = interior ? p[c - step] : 0.0;
+    const double dp = p[c] - pn;
+    double upd;
+    if (phc * phn > 0.0) {
+      upd = dt * dp * (1.0 / (phc <= 0.0 ? rn : rp)) * inv_h;
+    } else {
+      const double ef = 1.5 / inv_h;
+      const double rho_f = rn + (rp - rn) * heaviside_proj(0.5 * (phc + phn), ef);
+      upd = dt * dp * (1.0 / rho_f) * inv_h;  // jump term: zero without surface tension
+    }
+    val -= upd;
+  }
+  f[fc] = c0 == 0.0 ? (T)val : (T)(c0 * (double)base[fc] + c1 * val);
+}
+
+template <class T>
+__global__ void k_divergence_norms(const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, Lay Lc,
+                                   Lay Lu, Lay Lv, Lay Lw, double inv_h, double* partials, unsigned int* ticket,
+                                   double* out2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  double d2 = 0.0, dm = 0.0;
+  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
+    const double d = (inv_h * ((double)u[Lu.at(i + 1, j, k)] - (double)u[Lu.at(i, j, k)]) +
+                      inv_h * ((double)v[Lv.at(i, j + 1, k)] - (double)v[Lv.at(i, j, k)])) +
+                     inv_h * ((double)w[Lw.at(i, j, k + 1)] - (double)w[Lw.at(i, j, k)]);
+    d2 = d * d;
+    dm = fabs(d);
+  }
+  const double bm = block_max(dm);
+  __syncthreads();
+  if (thread0()) atomicMax((unsigned long long*)&out2[1], (unsigned long long)__double_as_longlong(bm));
+  d2 = block_sum(d2);
+  double tot;
+  if (grid_reduce_sum(d2, partials, ticket, &tot)) out2[0] = tot;
+}
+
+template <class T>
+__global__ void k_absmax(const T* __restrict__ f, Lay L, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  double m = 0.0;
+  if (i < L.nx && j < L.ny && k < L.nz) m = fabs((double)f[L.at(i, j, k)]);
+  m = block_max(m);
+  if (thread0()) atomicMax((unsigned long long*)out, (unsigned long long)__double_as_longlong(m));
+}
+
+template <class S, class D>
+__global__ void k_convert(D* __restrict__ dst, const S* __restrict__ src, Lay L) {
+  FS_IJK(L);
+  const int64_t c = L.at(i, j, k);
+  dst[c] = (D)src[c];
+}
+
+// packed (x fastest, no ghosts) FP64 <-> padded storage
+template <class T>
+__global__ void k_pack(double* __restrict__ dst, const T* __restrict__ src, Lay L) {
+  FS_IJK(L);
+  dst[((int64_t)k * L.ny + j) * L.nx + i] = (double)src[L.at(i, j, k)];
+}
+
+template <class T>
+__global__ void k_unpack(T* __restrict__ dst, const double* __restrict__ src, Lay L) {
+  FS_IJK(L);
+  dst[L.at(i, j, k)] = (T)src[((int64_t)k * L.ny + j) * L.nx + i];
+}
+
+// ---------------------------------------------------------------------------
+
+template <class T>
+void divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
+                    double dx, double dt, double* b, double* div_out, double* partials, unsigned int* ticket,
+                    double* scalars, cudaStream_t s) {
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
+  k_divergence_rhs<T><<<g.grid, g.block, 0, s>>>(u, v, w, Lc, Lu, Lv, Lw, 1.0 / dx, 1.0 / dt, b, div_out, partials,
+                                                  ticket, scalars);
+}
+
+void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* partials, unsigned int* ticket,
+                   double* scalars_out, cudaStream_t s) {
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
+  const double inv_n = 1.0 / ((double)Lc.nx * Lc.ny * Lc.nz);
+  k_subtract_mean<<<g.grid, g.block, 0, s>>>(b, Lc, scalars, inv_n, partials, ticket, scalars_out);
+}
+
+template <class T, class V>
+void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
+                             V* diag, cudaStream_t s) {
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
+  const double inv2 = 1.0 / (dx * dx);
+  k_pressure_faces<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, ax, ay, az);
+  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag);
+}
+
+template <class T>
+void defect_residual(const T* phi, const double* p64, const double* b, double* r64, float* r32, const Lay& Lc, double dx,
+                     double rho_neg, double rho_pos, double* partials, unsigned int* ticket, double* rr_out,
+                     cudaStream_t s) {
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
+  k_defect_residual<T><<<g.grid, g.block, 0, s>>>(phi, p64, b, r64, r32, Lc, rho_neg, rho_pos, 1.0 / (dx * dx),
+                                                   partials, ticket, rr_out);
+}
+
+void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s) {
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
+  k_add_correction<<<g.grid, g.block, 0, s>>>(p64, e, Lc);
+}
+
+template <class T>
+void velocity_correct(T* f, const T* base, const double* p, const T* phi, const Lay& Lf, const Lay& Lc, int axis,
+                      double dx, double dt, double rho_neg, double rho_pos, int faithful, double c0, double c1,
+                      cudaStream_t s) {
+  Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
+  k_velocity_correct<T><<<g.grid, g.block, 0, s>>>(f, base, p, phi, Lf, Lc, axis, 1.0 / dx, dt, rho_neg, rho_pos,
+                                                    faithful, c0, c1);
+}
+
+template <class T>
+void divergence_norms(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
+                      double dx, double* partials, unsigned int* ticket, double* out2, cudaStream_t s) {
+  cudaMemsetAsync(out2 + 1, 0, sizeof(double), s);
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
+  k_divergence_norms<T><<<g.grid, g.block, 0, s>>>(u, v, w, Lc, Lu, Lv, Lw, 1.0 / dx, partials, ticket, out2);
+}
+
+template <class T>
+void absmax3(const T* u, const T* v, const T* w, const Lay& Lu, const Lay& Lv, const Lay& Lw, double* out3,
+             cudaStream_t s) {
+  cudaMemsetAsync(out3, 0, 3 * sizeof(double), s);
+  Launch3 g = launch3(Lu.nx, Lu.ny, Lu.nz);
+  k_absmax<T><<<g.grid, g.block, 0, s>>>(u, Lu, out3);
+  g = launch3(Lv.nx, Lv.ny, Lv.nz);
+  k_absmax<T><<<g.grid, g.block, 0, s>>>(v, Lv, out3 + 1);
+  g = launch3(Lw.nx, Lw.ny, Lw.nz);
+  k_absmax<T><<<g.grid, g.block, 0, s>>>(w, Lw, out3 + 2);
+}
+
+template <class S, class D>
+void convert_copy(D* dst, const S* src, const Lay& L, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_convert<S, D><<<g.grid, g.block, 0, s>>>(dst, src, L);
+}
+
+template <class T>
+void pack_to_double(double* dst, const T* src, const Lay& L, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_pack<T><<<g.grid, g.block, 0, s>>>(dst, src, L);
+}
+
+template <class T>
+void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_unpack<T><<<g.grid, g.block, 0, s>>>(dst, src, L);
+}
+
+#define FS_PINST(T)                                                                                                  \
+  template void divergence_rhs<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,     \
+                                  double, double, double*, double*, double*, unsigned int*, double*, cudaStream_t); \
+  template void defect_residual<T>(const T*, const double*, const double*, double*, float*, const Lay&, double,     \
+                                   double, double, double*, unsigned int*, double*, cudaStream_t);                  \
+  template void velocity_correct<T>(T*, const T*, const double*, const T*, const Lay&, const Lay&, int, double,     \
+                                    double, double, double, int, double, double, cudaStream_t);                     \
+  template void divergence_norms<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,   \
+                                    double, double*, unsigned int*, double*, cudaStream_t);                         \
+  template void absmax3<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, double*, cudaStream_t); \
+  template void pack_to_double<T>(double*, const T*, const Lay&, cudaStream_t);                                     \
+  template void unpack_from_double<T>(T*, const double*, const Lay&, cudaStream_t);
+
+FS_PINST(float)
+FS_PINST(double)
+
+template void build_pressure_operator<float, float>(const float*, const Lay&, double, double, double, float*, float*,
+                                                    float*, float*, cudaStream_t);
+template void build_pressure_operator<double, double>(const double*, const Lay&, double, double, double, double*,
+                                                      double*, double*, double*, cudaStream_t);
+template void build_pressure_operator<double, float>(const double*, const Lay&, double, double, double, float*,
+                                                     float*, float*, float*, cudaStream_t);
+template void build_pressure_operator<float, double>(const float*, const Lay&, double, double, double, double*,
+                                                     double*, double*, double*, cudaStream_t);
+template void convert_copy<float, double>(double*, const float*, const Lay&, cudaStream_t);
+template void convert_copy<double, float>(float*, const double*, const Lay&, cudaStream_t);
+template void convert_copy<double, double>(double*, const double*, const Lay&, cudaStream_t);
+template void convert_copy<float, float>(float*, const float*, const Lay&, cudaStream_t);
+
+}  // namespace fsb

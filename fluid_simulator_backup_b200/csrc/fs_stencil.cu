@@ -1,0 +1,356 @@
+// Level-set and velocity stencil kernels: ghost fills, WENO5 advection
+// (ADVECTION_METHOD_3D.h:42-279), Sussman reinitialisation
+// (ADVECTION_METHOD_3D.h:745-1637) and the RK stage combiners
+// (EULERIAN_FLUID_SOLVER_3D.h:886-1109), templated on the storage/arithmetic
+// type (double for the FP64 path, float for FP32_REFINE).
+//
+// These kernels are FP32/FP64-issue bound rather than HBM bound (about 440
+// flops per cell per WENO5 update), so the WENO weights are evaluated with one
+// division per side: w_k = d_k prod_{j!=k} q_j / sum_m d_m prod_{j!=m} q_j
+// with q = (eps + IS)^2, algebraically equal to the reference's
+// (d_k/q_k)/sum(d_m/q_m).  The substencil constants 1/3, 7/6, ... are applied
+// as multiplications.  Both change results only at the level of rounding.
+#include "fs_kernels.h"
+
+namespace fsb {
+
+// ---------------------------------------------------------------------------
+// ghost fills
+// ---------------------------------------------------------------------------
+
+// m-th ghost layer (m = 1..3) of the outward linear extrapolation
+// ghost(-m) = 2 ghost(-m+1) - ghost(-m+2), evaluated recursively from the
+// two boundary values f0 (on the wall) and f1 (one inside) as the reference
+// does (FIELD_STRUCTURE_3D.h:1776-1895).
+template <class T>
+__device__ __forceinline__ T extrap_layer(T f0, T f1, int m) {
+  T a = f1, b = f0;  // (layer m-2, layer m-1)
+  for (int q = 0; q < m; ++q) {
+    T c = T(2) * b - a;
+    a = b;
+    b = c;
+  }
+  return b;
+}
+
+template <class T>
+struct ExtrapField {
+  const T* f;
+  Lay L;
+  // value at (i, j, k) with i, j, k possibly in the ghost ring: extend x
+  // first, then y, then z (dimension by dimension).
+  __device__ T x_ext(int i, int j, int k) const {
+    if (i < 0) return extrap_layer(f[L.at(0, j, k)], f[L.at(1, j, k)], -i);
+    if (i >= L.nx) return extrap_layer(f[L.at(L.nx - 1, j, k)], f[L.at(L.nx - 2, j, k)], i - L.nx + 1);
+    return f[L.at(i, j, k)];
+  }
+  __device__ T y_ext(int i, int j, int k) const {
+    if (j < 0) return extrap_layer(x_ext(i, 0, k), x_ext(i, 1, k), -j);
+    if (j >= L.ny) return extrap_layer(x_ext(i, L.ny - 1, k), x_ext(i, L.ny - 2, k), j - L.ny + 1);
+    return x_ext(i, j, k);
+  }
+  __device__ T z_ext(int i, int j, int k) const {
+    if (k < 0) return extrap_layer(y_ext(i, j, 0), y_ext(i, j, 1), -k);
+    if (k >= L.nz) return extrap_layer(y_ext(i, j, L.nz - 1), y_ext(i, j, L.nz - 2), k - L.nz + 1);
+    return y_ext(i, j, k);
+  }
+};
+
+// Decode a flat index over the ghost shell: the z slabs (full padded x, y),
+// then the y slabs (interior z, full padded x), then the x slabs (interior
+// y, z).  Returns false past the end.
+__device__ __forceinline__ bool shell_coord(const Lay& L, int64_t t, int& i, int& j, int& k) {
+  const int px = L.px, py = L.py;
+  const int64_t nzs = (int64_t)2 * GH * px * py;
+  if (t < nzs) {
+    const int64_t s = t / ((int64_t)px * py);
+    const int64_t r = t % ((int64_t)px * py);
+    k = s < GH ? (int)(s - GH) : (int)(L.nz + (s - GH));
+    j = (int)(r / px) - GH;
+    i = (int)(r % px) - GH;
+    return true;
+  }
+  t -= nzs;
+  const int64_t nys = (int64_t)2 * GH * px * L.nz;
+  if (t < nys) {
+    const int64_t s = t / ((int64_t)px * L.nz);
+    const int64_t r = t % ((int64_t)px * L.nz);
+    j = s < GH ? (int)(s - GH) : (int)(L.ny + (s - GH));
+    k = (int)(r / px);
+    i = (int)(r % px) - GH;
+    return true;
+  }
+  t -= nys;
+  const int64_t nxs = (int64_t)2 * GH * L.ny * L.nz;
+  if (t < nxs) {
+    const int64_t s = t / ((int64_t)L.ny * L.nz);
+    const int64_t r = t % ((int64_t)L.ny * L.nz);
+    i = s < GH ? (int)(s - GH) : (int)(L.nx + (s - GH));
+    k = (int)(r / L.ny);
+    j = (int)(r % L.ny);
+    return true;
+  }
+  return false;
+}
+
+inline int64_t shell_count(const Lay& L) {
+  return (int64_t)2 * GH * L.px * L.py + (int64_t)2 * GH * L.px * L.nz + (int64_t)2 * GH * L.ny * L.nz;
+}
+
+template <class T>
+__global__ void k_fill_extrap(T* f, Lay L) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (!shell_coord(L, t, i, j, k)) return;
+  ExtrapField<T> e{f, L};
+  f[L.at(i, j, k)] = e.z_ext(i, j, k);
+}
+
+template <class T>
+void fill_extrap(T* f, const Lay& L, cudaStream_t s) {
+  const int64_t n = shell_count(L);
+  k_fill_extrap<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(f, L);
+}
+
+// ---------------------------------------------------------------------------
+// WENO5
+// ---------------------------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ T weno_side(T r1, T r2, T r3, T r4, T r5, T eps) {
+  const T c1312 = T(13.0 / 12.0);
+  T t = (r1 - T(2) * r2) + r3, q = (r1 - T(4) * r2) + T(3) * r3;
+  const T s1 = (c1312 * t) * t + (T(0.25) * q) * q;
+  t = (r2 - T(2) * r3) + r4; q = r2 - r4;
+  const T s2 = (c1312 * t) * t + (T(0.25) * q) * q;
+  t = (r3 - T(2) * r4) + r5; q = (T(3) * r3 - T(4) * r4) + r5;
+  const T s3 = (c1312 * t) * t + (T(0.25) * q) * q;
+  const T e1 = eps + s1, e2 = eps + s2, e3 = eps + s3;
+  const T q1 = e1 * e1, q2 = e2 * e2, q3 = e3 * e3;
+  const T b1 = T(0.1) * (q2 * q3), b2 = T(0.6) * (q1 * q3), b3 = T(0.3) * (q1 * q2);
+  const T inv = T(1) / ((b1 + b2) + b3);
+  const T third = T(1.0 / 3.0), sixth = T(1.0 / 6.0);
+  const T u1 = (r1 * third - r2 * T(7.0 / 6.0)) + r3 * T(11.0 / 6.0);
+  const T u2 = (r2 * (-sixth) + r3 * T(5.0 / 6.0)) + r4 * third;
+  const T u3 = (r3 * third + r4 * T(5.0 / 6.0)) - r5 * sixth;
+  return ((b1 * u1 + b2 * u2) + b3 * u3) * inv;
+}
+
+// D- and D+ along a stride from the 7 samples f[-3..3].
+template <class T>
+__device__ __forceinline__ void weno_pair(const T* __restrict__ f, int64_t c, int64_t st, T inv_h, T eps, T& dm, T& dp) {
+  const T fm3 = f[c - 3 * st], fm2 = f[c - 2 * st], fm1 = f[c - st], f0 = f[c], fp1 = f[c + st], fp2 = f[c + 2 * st],
+          fp3 = f[c + 3 * st];
+  const T d1 = inv_h * (fm2 - fm3), d2 = inv_h * (fm1 - fm2), d3 = inv_h * (f0 - fm1), d4 = inv_h * (fp1 - f0),
+          d5 = inv_h * (fp2 - fp1), d6 = inv_h * (fp3 - fp2);
+  dm = weno_side(d1, d2, d3, d4, d5, eps);
+  dp = weno_side(d6, d5, d4, d3, d2, eps);
+}
+
+// out = c0*base + c1*(src - dt*(u.grad src)), the level-set update at cell
+// centres; u, v, w are the MAC faces (zero ghosts).  With c0 == 0 the
+// combination is skipped and out is the forward-Euler value.
+template <class T>
+__global__ void k_weno5_levelset(const T* __restrict__ src, const T* __restrict__ base, T* __restrict__ out,
+                                 const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, Lay L,
+                                 Lay Lu, Lay Lv, Lay Lw, T inv_h, T eps, T dt, T c0, T c1) {
+  FS_IJK(L);
+  const int64_t c = L.at(i, j, k);
+  T dxm, dxp, dym, dyp, dzm, dzp;
+  weno_pair(src, c, 1, inv_h, eps, dxm, dxp);
+  weno_pair(src, c, L.px, inv_h, eps, dym, dyp);
+  weno_pair(src, c, L.slab, inv_h, eps, dzm, dzp);
+  const T uc = (u[Lu.at(i + 1, j, k)] + u[Lu.at(i, j, k)]) * T(0.5);
+  const T vc = (v[Lv.at(i, j + 1, k)] + v[Lv.at(i, j, k)]) * T(0.5);
+  const T wc = (w[Lw.at(i, j, k + 1)] + w[Lw.at(i, j, k)]) * T(0.5);
+  const T fe = src[c] - dt * ((uc * (uc > T(0) ? dxm : dxp) + vc * (vc > T(0) ? dym : dyp)) + wc * (wc > T(0) ? dzm : dzp));
+  out[c] = c0 == T(0) ? fe : c0 * base[c] + c1 * fe;
+}
+
+// MAC component self-advection on every face of component `axis` (wall
+// faces included, as the reference's loop covers the whole face grid).
+template <class T>
+__global__ void k_weno5_mac(const T* __restrict__ comp, T* __restrict__ out, const T* __restrict__ u,
+                            const T* __restrict__ v, const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw, int axis,
+                            T inv_h, T eps, T dt) {
+  FS_IJK(Lc);
+  const int64_t c = Lc.at(i, j, k);
+  T uvel, vvel, wvel;
+  if (axis == 0) {
+    uvel = u[Lu.at(i, j, k)];
+    vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i - 1, j, k)]) + v[Lv.at(i - 1, j + 1, k)]) * T(0.25);
+    wvel = (((w[Lw.at(i, j, k)] + w[Lw.at(i, j, k + 1)]) + w[Lw.at(i - 1, j, k)]) + w[Lw.at(i - 1, j, k + 1)]) * T(0.25);
+  } else if (axis == 1) {
+    uvel = (((u[Lu.at(i, j, k)] + u[Lu.at(i + 1, j, k)]) + u[Lu.at(i, j - 1, k)]) + u[Lu.at(i + 1, j - 1, k)]) * T(0.25);
+    vvel = v[Lv.at(i, j, k)];
+    wvel = (((w[Lw.at(i, j, k)] + w[Lw.at(i, j, k + 1)]) + w[Lw.at(i, j - 1, k)]) + w[Lw.at(i, j - 1, k + 1)]) * T(0.25);
+  } else {
+    uvel = (((u[Lu.at(i, j, k)] + u[Lu.at(i + 1, j, k)]) + u[Lu.at(i, j, k - 1)]) + u[Lu.at(i + 1, j, k - 1)]) * T(0.25);
+    vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i, j, k - 1)]) + v[Lv.at(i, j + 1, k - 1)]) * T(0.25);
+    wvel = w[Lw.at(i, j, k)];
+  }
+  T dxm, dxp, dym, dyp, dzm, dzp;
+  weno_pair(comp, c, 1, inv_h, eps, dxm, dxp);
+  weno_pair(comp, c, Lc.px, inv_h, eps, dym, dyp);
+  weno_pair(comp, c, Lc.slab, inv_h, eps, dzm, dzp);
+  out[c] = comp[c] - dt * ((uvel * (uvel > T(0) ? dxm : dxp) + vvel * (vvel > T(0) ? dym : dyp)) +
+                           wvel * (wvel > T(0) ? dzm : dzp));
+}
+
+// ---------------------------------------------------------------------------
+// Sussman reinitialisation
+// ---------------------------------------------------------------------------
+
+template <class T>
+__global__ void k_sign(const T* __restrict__ phi, T* __restrict__ s, Lay L, T dx) {
+  FS_IJK(L);
+  const int64_t c = L.at(i, j, k);
+  const T p = phi[c];
+  s[c] = p / sqrt(p * p + dx * dx);
+}
+
+// Per-axis Godunov choice of the reference's case tree.  code: 0 D-, 1 D+,
+// 2 dropped (expansion fan).
+template <class T>
+__device__ __forceinline__ T godunov(T s, T dm, T dp, int& code, bool& shock) {
+  const T sm = s * dm, sp = s * dp;
+  shock = false;
+  if (sp >= T(0) && sm >= T(0)) { code = 0; return dm; }
+  if (sp <= T(0) && sm <= T(0)) { code = 1; return dp; }
+  if (sp > T(0) && sm < T(0)) { code = 2; return T(0); }
+  shock = true;  // sp < 0 < sm
+  const T ss = s * (fabs(dp) - fabs(dm)) / (dp - dm);
+  if (ss > T(0)) { code = 0; return dm; }
+  code = 1;
+  return dp;
+}
+
+// One pseudo-step phi - dtau*S*(|grad phi|_G - 1) with the sign-preserving
+// clamp; out = c0*base + c1*(that) when c0 != 0 (RK block combination).
+template <class T>
+__global__ void k_sussman(const T* __restrict__ src, const T* __restrict__ sgn, const T* __restrict__ base,
+                          T* __restrict__ out, Lay L, T inv_h, T eps, T dtau, T c0, T c1, int typo) {
+  FS_IJK(L);
+  const int64_t c = L.at(i, j, k);
+  T dxm, dxp, dym, dyp, dzm, dzp;
+  weno_pair(src, c, 1, inv_h, eps, dxm, dxp);
+  weno_pair(src, c, L.px, inv_h, eps, dym, dyp);
+  weno_pair(src, c, L.slab, inv_h, eps, dzm, dzp);
+  const T s = sgn[c];
+  int cx, cy, cz;
+  bool shx, shy, shz;
+  const T gx = godunov(s, dxm, dxp, cx, shx);
+  const T gy = godunov(s, dym, dyp, cy, shy);
+  const T gz = godunov(s, dzm, dzp, cz, shz);
+  T mag = sqrt((gx * gx + gy * gy) + gz * gz) - T(1);
+  if (typo && shx && shy && cy == 1 && cz == 2) mag = (sqrt(gx * gx) + gy * gy) - T(1);
+  T r = src[c] - dtau * s * mag;
+  if (s * r < T(0)) {
+    if (s < T(0)) r = -eps;
+    if (s > T(0)) r = eps;
+  }
+  out[c] = c0 == T(0) ? r : c0 * base[c] + c1 * r;
+}
+
+// ---------------------------------------------------------------------------
+// elementwise helpers
+// ---------------------------------------------------------------------------
+
+// out = a*x + b*y over the interior of layout L.
+template <class T>
+__global__ void k_axpby(T* __restrict__ out, const T* __restrict__ x, const T* __restrict__ y, T a, T b, Lay L) {
+  FS_IJK(L);
+  const int64_t c = L.at(i, j, k);
+  out[c] = a * x[c] + b * y[c];
+}
+
+// Add a constant (gravity*dt) to every interior face except the two wall
+// planes normal to the component (which hold the no-penetration zero).
+template <class T>
+__global__ void k_add_const_interior_faces(T* __restrict__ f, Lay L, int axis, T value, int skip_walls) {
+  FS_IJK(L);
+  if (skip_walls) {
+    const int e = axis == 0 ? i : (axis == 1 ? j : k);
+    const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+    if (e == 0 || e == n - 1) return;
+  }
+  f[L.at(i, j, k)] += value;
+}
+
+// Zero the two wall planes normal to a face component.
+template <class T>
+__global__ void k_zero_walls(T* __restrict__ f, Lay L, int axis) {
+  FS_IJK(L);
+  const int e = axis == 0 ? i : (axis == 1 ? j : k);
+  const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+  if (e == 0 || e == n - 1) f[L.at(i, j, k)] = T(0);
+}
+
+// ---------------------------------------------------------------------------
+// host wrappers
+// ---------------------------------------------------------------------------
+
+template <class T>
+void weno5_levelset(const T* src, const T* base, T* out, const T* u, const T* v, const T* w, const Lay& L,
+                    const Lay& Lu, const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c0, double c1,
+                    cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz, 32, 4, 2);
+  k_weno5_levelset<T><<<g.grid, g.block, 0, s>>>(src, base, out, u, v, w, L, Lu, Lv, Lw, T(1.0 / dx), T(eps), T(dt),
+                                                   T(c0), T(c1));
+}
+
+template <class T>
+void weno5_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+               const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s) {
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz, 32, 4, 2);
+  k_weno5_mac<T><<<g.grid, g.block, 0, s>>>(comp, out, u, v, w, Lc, Lu, Lv, Lw, axis, T(1.0 / dx), T(eps), T(dt));
+}
+
+template <class T>
+void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_sign<T><<<g.grid, g.block, 0, s>>>(phi, sgn, L, T(dx));
+}
+
+template <class T>
+void sussman_step(const T* src, const T* sgn, const T* base, T* out, const Lay& L, double dx, double eps, double dtau,
+                  double c0, double c1, int typo, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz, 32, 4, 2);
+  k_sussman<T><<<g.grid, g.block, 0, s>>>(src, sgn, base, out, L, T(1.0 / dx), T(eps), T(dtau), T(c0), T(c1), typo);
+}
+
+template <class T>
+void axpby(T* out, const T* x, const T* y, double a, double b, const Lay& L, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_axpby<T><<<g.grid, g.block, 0, s>>>(out, x, y, T(a), T(b), L);
+}
+
+template <class T>
+void add_const_faces(T* f, const Lay& L, int axis, double value, int skip_walls, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_add_const_interior_faces<T><<<g.grid, g.block, 0, s>>>(f, L, axis, T(value), skip_walls);
+}
+
+template <class T>
+void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s) {
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_zero_walls<T><<<g.grid, g.block, 0, s>>>(f, L, axis);
+}
+
+#define FS_INST(T)                                                                                                    \
+  template void fill_extrap<T>(T*, const Lay&, cudaStream_t);                                                         \
+  template void weno5_levelset<T>(const T*, const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&,       \
+                                  const Lay&, const Lay&, double, double, double, double, double, cudaStream_t);      \
+  template void weno5_mac<T>(const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,          \
+                             const Lay&, int, double, double, double, cudaStream_t);                                  \
+  template void sign_function<T>(const T*, T*, const Lay&, double, cudaStream_t);                                    \
+  template void sussman_step<T>(const T*, const T*, const T*, T*, const Lay&, double, double, double, double, double, \
+                                int, cudaStream_t);                                                                   \
+  template void axpby<T>(T*, const T*, const T*, double, double, const Lay&, cudaStream_t);                          \
+  template void add_const_faces<T>(T*, const Lay&, int, double, int, cudaStream_t);                                  \
+  template void zero_walls<T>(T*, const Lay&, int, cudaStream_t);
+
+FS_INST(float)
+FS_INST(double)
+
+}  // namespace fsb

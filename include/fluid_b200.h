@@ -1,0 +1,165 @@
+/*
+ * fluid_b200.h - C ABI of the B200 (sm_100a) two-phase level-set solver
+ * timestep: WENO5 level-set and velocity advection, Sussman
+ * reinitialisation, semi-implicit viscosity and the variable-density
+ * ghost-fluid pressure projection, all device resident.
+ *
+ * Every entry point returns an fs_status; none calls exit().  After any
+ * status other than FS_CUDA_ERROR the context stays usable.  A context owns
+ * one CUDA stream and all device memory of one simulation; it is not
+ * re-entrant (one host thread at a time, as the reference's head-thread work
+ * is).  Host arrays are borrowed only for the duration of a call.
+ *
+ * Array conventions (the reference's ARRAY_3D order, ARRAY_3D.h:98): x is the
+ * fastest index.  Cell fields hold nx*ny*nz values; MAC face fields carry one
+ * more entry along their own axis: u (nx+1)*ny*nz, v nx*(ny+1)*nz,
+ * w nx*ny*(nz+1).  The grid is uniform with spacing dx on all axes; cell
+ * (i,j,k) is centred at ((i+1/2)dx, (j+1/2)dx, (k+1/2)dx).  The phase with
+ * phi <= 0 is the "negative" phase of fs_params.
+ */
+#ifndef FLUID_B200_H
+#define FLUID_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fs_ctx fs_ctx;
+
+typedef enum {
+  FS_OK = 0,
+  FS_INVALID_ARG = 1,     /* bad size, null pointer, unknown field or option */
+  FS_OOM = 2,             /* device allocation failed; nothing was kept */
+  FS_NOT_CONVERGED = 3,   /* an iterative solve stopped at its iteration cap */
+  FS_NONFINITE = 4,       /* NaN/Inf detected in a residual or input */
+  FS_CUDA_ERROR = 5,      /* a CUDA call failed; the context may be unusable */
+  FS_TIMEOUT = 6,         /* a bounded device-side wait ran out */
+  FS_NOT_SUPPORTED = 7
+} fs_status;
+
+typedef enum {
+  FS_FIELD_PHI = 0,       /* level set, cells */
+  FS_FIELD_U = 1,         /* x-velocity, x faces */
+  FS_FIELD_V = 2,         /* y-velocity, y faces */
+  FS_FIELD_W = 3,         /* z-velocity, z faces */
+  FS_FIELD_PRESSURE = 4,  /* pressure of the last projection, cells */
+  FS_FIELD_DIVERGENCE = 5 /* divergence/dt of the last projection's input, cells (download only) */
+} fs_field;
+
+typedef enum {
+  FS_PRECISION_FP64 = 0,        /* FP64 storage and arithmetic everywhere */
+  FS_PRECISION_FP32_REFINE = 1  /* FP32 storage/stencils/inner PCG + FP64 defect correction */
+} fs_precision;
+
+typedef enum {
+  FS_STOP_RELATIVE = 0,   /* ||b - A p||_2 / ||b||_2 < tolerance */
+  FS_STOP_ABSOLUTE = 1    /* r.z < tolerance^2, the reference's PCG test (PCG_METHOD.cpp:87) */
+} fs_stop;
+
+/* Behaviour switches; 0 is the corrected specification. */
+enum {
+  FS_FLAG_FAITHFUL_PROJECTION = 1 << 0, /* only w corrected + first-cell bottom face quirk (PROJECTION_3D.h:1188-1407) */
+  FS_FLAG_REINIT_TYPO = 1 << 1,         /* reproduce the two sqrt(a^2)+b^2 leaves (ADVECTION_METHOD_3D.h:1463,1605) */
+  FS_FLAG_LEVELSET_FORWARD_EULER = 1 << 2 /* order 3 advances phi by one Euler step (EULERIAN_FLUID_SOLVER_3D.h:1010) */
+};
+
+typedef struct {
+  int nx, ny, nz;
+  double dx;
+} fs_grid_desc;
+
+typedef struct {
+  double rho_neg, rho_pos;          /* density of the phase at phi <= 0 / phi > 0 */
+  double mu_neg, mu_pos;            /* dynamic viscosity, same convention */
+  double gravity[3];                /* gravity (the reference's default is (0,-9.8,0)) */
+  double weno_epsilon;              /* LEVELSET_ADVECTION.epsilon (also the reinit clamp) */
+  int reinit_iterations;            /* iteration_number_for_reinitialization */
+  int reinit_scaling;               /* scaling_number_for_reinitialization: dtau = dx/scaling */
+  int order;                        /* order_for_time_advancing: 1, 2 or 3 */
+  int precision;                    /* fs_precision */
+  int stop;                         /* fs_stop for the pressure solve */
+  double tolerance;                 /* pressure tolerance (relative divergence in FP32_REFINE) */
+  int max_iteration;                /* PCG iteration cap per solve (inner cap in FP32_REFINE) */
+  double inner_tolerance;           /* FP32_REFINE: relative reduction asked of each inner solve */
+  int max_outer;                    /* FP32_REFINE: defect-correction cap */
+  int viscosity;                    /* 0: off, 1: semi-implicit */
+  double viscosity_tolerance;       /* relative residual of each viscosity solve */
+  int viscosity_max_iteration;
+  double cfl;                       /* CFL number used by fs_cfl_dt */
+  int flags;                        /* FS_FLAG_* */
+} fs_params;
+
+typedef struct {
+  int iterations;           /* PCG iterations (sum of inner iterations in FP32_REFINE) */
+  int outer_iterations;     /* FP32_REFINE defect corrections (1 in FP64) */
+  double rel_residual;      /* final ||b - A p||_2/||b||_2 in FP64 */
+  double rz;                /* final r.z of the last PCG */
+  double div_l2, div_linf;  /* divergence of the corrected velocity (cells, not scaled by dt) */
+  float ms;                 /* device time of the call */
+} fs_solve_report;
+
+typedef struct {
+  int pcg_iterations;       /* over all projections of the step */
+  int outer_iterations;
+  int viscosity_iterations;
+  int projections;
+  double max_rel_residual;  /* worst pressure residual of the step */
+  double div_l2, div_linf;  /* divergence after the last projection */
+  float ms;                 /* device time of the step */
+} fs_step_report;
+
+/* Defaults that reproduce the reference's script defaults where it has them
+ * (EULERIAN_FLUID_SOLVER_3D.h:192-260, PROJECTION_3D.h:178-230) and the
+ * configuration's values elsewhere. */
+void fs_params_default(fs_params* p);
+const char* fs_status_str(fs_status s);
+const char* fs_last_error(void);
+
+/* Context life cycle (replaces EULERIAN_FLUID_SOLVER_3D::InitializeFromScriptBlock,
+ * EULERIAN_FLUID_SOLVER_3D.h:192).  Allocates every device buffer up front. */
+fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** out);
+fs_status fs_destroy(fs_ctx* ctx);
+fs_status fs_set_params(fs_ctx* ctx, const fs_params* params);
+fs_status fs_memory_bytes(const fs_ctx* ctx, int64_t* bytes);
+
+/* Host <-> device copies of one field (FP64 host values; converted to the
+ * context's storage precision).  Non-NULL strides give element strides of
+ * the host array in x, y, z (default: packed). */
+fs_status fs_upload(fs_ctx* ctx, int field, const double* host, const int64_t* strides);
+fs_status fs_download(fs_ctx* ctx, int field, double* host, const int64_t* strides);
+/* Same, from/to device memory the caller owns (FP64, packed). */
+fs_status fs_upload_device(fs_ctx* ctx, int field, const double* dev);
+fs_status fs_download_device(fs_ctx* ctx, int field, double* dev);
+
+/* One timestep (EULERIAN_FLUID_SOLVER_3D::AdvanceOneTimeStepThread,
+ * EULERIAN_FLUID_SOLVER_3D.h:803-1111). */
+fs_status fs_step(fs_ctx* ctx, double dt, fs_step_report* report);
+/* CFL-limited dt times params.cfl (CFLOneTimeStep, EULERIAN_FLUID_SOLVER_3D.h:2673-2785). */
+fs_status fs_cfl_dt(fs_ctx* ctx, double* dt);
+
+/* Single operators of the step, on the context's current fields. */
+/* PROJECTION_3D::Solve (PROJECTION_3D.h:416). */
+fs_status fs_project(fs_ctx* ctx, double dt, fs_solve_report* report);
+/* One forward-Euler WENO5 level-set update (ADVECTION_3D::Solve_Levelset, ADVECTION_3D.h:204). */
+fs_status fs_advect_levelset(fs_ctx* ctx, double dt);
+/* One forward-Euler WENO5 update of u, v, w (ADVECTION_3D::Solve_Velocity, ADVECTION_3D.h:244). */
+fs_status fs_advect_velocity(fs_ctx* ctx, double dt);
+/* One reinitialisation block (EULERIAN_FLUID_SOLVER_3D::Reinitialization, :2198). */
+fs_status fs_reinitialize(fs_ctx* ctx);
+/* Semi-implicit viscosity of u, v, w (VISCOSITY_3D::ApplyViscosity, VISCOSITY_3D.h:448). */
+fs_status fs_viscosity(fs_ctx* ctx, double dt, int* iterations);
+
+/* LINEAR_SOLVER::Solve plugin (LINEAR_SOLVER.h:36): Jacobi-PCG on a CSR
+ * matrix given on the host, x in/out (initial guess in).  Runs on the
+ * context's stream with its own temporary device buffers. */
+fs_status fs_pcg_csr(fs_ctx* ctx, int n, int nnz, const double* values, const int* column_index,
+                     const int* row_ptr, const double* b, double* x, double tolerance, int max_iteration,
+                     int stop, int* iterations, double* residual);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLUID_B200_H */

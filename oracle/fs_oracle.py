@@ -685,3 +685,82 @@ def cfl_dt(u, v, w, dx, gravity_y, nu_max=0.0, surface_term=0.0):
     cv = c_f + v_f
     cfl = 0.5 * (cv + math.sqrt((cv * cv + 4.0 * (g_f * g_f)) + 4.0 * (s_f * s_f)))
     return 1.0 / cfl
+
+
+# ----------------------------------------------------------------------------
+# Whole timestep, corrected specification (the GPU path's contract)
+# ----------------------------------------------------------------------------
+
+def add_gravity(u, v, w, g, dt):
+    """u_d += dt*g_d on every face except the two wall planes normal to d
+    (ApplyGravity, EULERIAN_FLUID_SOLVER_3D.h:2237-2269; wall faces hold the
+    no-penetration zero)."""
+    out = []
+    for axis, f in enumerate((u, v, w)):
+        f = f.copy()
+        if g[axis] != 0.0:
+            ax = 2 - axis
+            sl = [slice(None)] * 3
+            sl[ax] = slice(1, -1)
+            f[tuple(sl)] = f[tuple(sl)] + dt * g[axis]
+        out.append(f)
+    return tuple(out)
+
+
+def zero_walls(u, v, w):
+    out = []
+    for axis, f in enumerate((u, v, w)):
+        f = f.copy()
+        ax = 2 - axis
+        sl = [slice(None)] * 3
+        sl[ax] = 0
+        f[tuple(sl)] = 0.0
+        sl[ax] = -1
+        f[tuple(sl)] = 0.0
+        out.append(f)
+    return tuple(out)
+
+
+def step(phi, u, v, w, dx, dt, P, p0=None):
+    """One timestep of the corrected specification, order 3:
+    level set TVD-RK3 (Shu-Osher) with the step's initial velocity; velocity
+    Shu-Osher RK3 over SolveForRK stages (WENO5 self-advection, wall faces
+    zeroed, gravity, semi-implicit viscosity, projection correcting u, v and
+    w); reinitialisation as the reference's RK3 of reinitialisation blocks
+    (EULERIAN_FLUID_SOLVER_3D.h:1081-1109).  P is a dict with rho_neg,
+    rho_pos, mu_neg, mu_pos, gravity, eps, reinit_iterations, reinit_scaling,
+    tol, max_iter, viscosity (bool), visc_tol.  Returns (phi, u, v, w, p, info)."""
+    eps = P["eps"]
+    L = lambda f: weno5_levelset(f, u, v, w, dx, dt, eps)
+    phi1 = L(phi)
+    phi2 = 0.75 * phi + 0.25 * L(phi1)
+    phin = (1.0 / 3.0) * phi + (2.0 / 3.0) * L(phi2)
+    p = np.zeros_like(phi) if p0 is None else p0
+    info = {"iterations": [], "rel_residual": []}
+
+    def stage(vel, c0, c1, base):
+        nonlocal p
+        a = weno5_velocity(*vel, dx, dt, eps)
+        a = zero_walls(*a)
+        a = add_gravity(*a, P["gravity"], dt)
+        if P.get("viscosity", True):
+            a, _ = viscosity_semi_implicit(phin, *a, dx, dt, P["rho_neg"], P["rho_pos"], P["mu_neg"], P["mu_pos"],
+                                           P["visc_tol"], 10000, "rel")
+        uu, vv, ww, p, pi = projection(phin, *a, dx, dt, P["rho_neg"], P["rho_pos"], P["tol"], P["max_iter"],
+                                       mode="corrected", criterion="rel", p0=p)
+        info["iterations"].append(pi["iterations"])
+        info["rel_residual"].append(pi["rel_residual"])
+        out = (uu, vv, ww)
+        if c0 != 0.0:
+            out = tuple(c0 * b + c1 * o for b, o in zip(base, out))
+        return out
+
+    base = (u, v, w)
+    s1 = stage(base, 0.0, 1.0, base)
+    s2 = stage(s1, 0.75, 0.25, base)
+    s3 = stage(s2, 1.0 / 3.0, 2.0 / 3.0, base)
+    it, sc = P["reinit_iterations"], P["reinit_scaling"]
+    r1 = reinitialization_block(phin, dx, it, sc, eps)
+    r2 = 0.75 * phin + 0.25 * reinitialization_block(r1, dx, it, sc, eps)
+    phi_out = (1.0 / 3.0) * phin + (2.0 / 3.0) * reinitialization_block(r2, dx, it, sc, eps)
+    return phi_out, s3[0], s3[1], s3[2], p, info
