@@ -1,0 +1,332 @@
+"""Timestep benchmark: rising air bubble at 256^3 (density ratio 1000).
+
+One "step" is one full timestep of the solver (fs_step: WENO5 TVD-RK3 level
+set, three SolveForRK stages of WENO5 velocity advection + gravity +
+semi-implicit viscosity + pressure projection, RK3 of reinitialisation
+blocks) on the workload of the rising-bubble configuration: 256^3 cells on the
+unit cube, air sphere of radius 0.15 at (0.5, 0.25, 0.5) (rho 1, mu 1.8e-5)
+in water (rho 1000, mu 1e-3), gravity -9.8 y, CFL 0.5, pressure solved to
+1e-6 relative divergence ||b - A p||/||b||.
+
+`value` is the FP32+FP64-refinement timestep in ms (device time, inputs
+resident).  The same steps are also timed in the plain FP64 path
+(`fp64_ms_per_step`).  Inputs are synthetic (the scene above, seeded), the
+fields are far larger than L2 (each FP32 field is 67 MB, a step touches
+several GB), so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n 256] [--impl reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the same
+workload on its own GPU ("replicas only": the path does not shard on one
+GPU's worth of grid); `value` is then the max over ranks of the per-step time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_UNKNOWN_PCG_FP32 = 68  # spmv 24 + update 28 + direction 16 (FP32 storage)
+BYTES_PER_UNKNOWN_PCG_FP64 = 136
+
+
+def scene(n):
+    x = (np.arange(n) + 0.5) / n
+    phi = np.sqrt((x[None, None, :] - 0.5) ** 2 + (x[None, :, None] - 0.25) ** 2 + (x[:, None, None] - 0.5) ** 2) - 0.15
+    u = np.zeros((n, n, n + 1)); v = np.zeros((n, n + 1, n)); w = np.zeros((n + 1, n, n))
+    return phi, u, v, w
+
+
+def params(fs, precision):
+    return fs.default_params(rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0),
+                             precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=20000,
+                             inner_tolerance=1e-2, max_outer=30, viscosity=1, viscosity_tolerance=1e-8, cfl=0.5,
+                             order=3, reinit_iterations=10, reinit_scaling=5, weno_epsilon=1e-6)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in self.rows for q in range(4) if r[3 + q].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def run_steps(fs, n, precision, warmup, steps, barrier):
+    import torch
+    phi, u, v, w = scene(n)
+    s = fs.Solver(n, 1.0 / n, params(fs, precision))
+    for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
+        s.upload(k, a)
+    for _ in range(warmup):
+        s.step(s.cfl_dt(), allow_not_converged=True)
+    barrier()
+    torch.cuda.synchronize()
+    reps = []
+    for _ in range(steps):
+        dt = s.cfl_dt()
+        reps.append(s.step(dt, allow_not_converged=True))
+    torch.cuda.synchronize()
+    barrier()
+    return s, reps
+
+
+def e2e_steps(fs, s, n, steps):
+    """End to end through the public API: per step, the fields are uploaded
+    from pinned host memory, the step runs, and the level set is read back."""
+    import torch
+    shapes = {k: s.shape(k) for k in ("phi", "u", "v", "w")}
+    host = {k: torch.from_numpy(s.download(k)).pin_memory() for k in shapes}
+    out = torch.empty(shapes["phi"], dtype=torch.float64).pin_memory()
+    h2d = sum(int(np.prod(sh)) * 8 for sh in shapes.values())
+    d2h = int(np.prod(shapes["phi"])) * 8
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for k in ("phi", "u", "v", "w"):
+            s.upload_ptr(k, host[k].data_ptr())
+        s.step(s.cfl_dt(), allow_not_converged=True)
+        s.download_ptr("phi", out.data_ptr())
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    return ms, h2d, d2h
+
+
+def reference_sample(n, pcg_iterations_per_projection, threads=1):
+    """Time the reference's own CPU operators (oracle/_ref, built from the
+    reference sources) on the same 256^3 scene and scale them to one
+    timestep: 3 level-set WENO5 updates, 3 WENO5 velocity updates, 3
+    explicit viscosity updates (the reference's air/water viscosity), 3
+    projections (system build + the GPU FP64 path's PCG iteration count per
+    projection at the same tolerance) and 3 reinitialisation blocks of 10
+    pseudo-steps.  Bounded sample: one call of each operator, the projection
+    run at two iteration caps to separate build and per-iteration cost, one
+    Sussman pseudo-step."""
+    import psutil
+
+    from oracle import refsim
+    if not refsim.available():
+        return None, "oracle/_ref/libfsref.so not built"
+    # the reference holds ~150 double fields of n^3; sample at a smaller grid
+    # and scale per cell when the host cannot hold the full one comfortably
+    need_gb = 2300 * n ** 3 / 1e9  # ~2.3 kB of host memory per cell (measured at 64^3)
+    m = n
+    while need_gb * (m / n) ** 3 > 0.5 * psutil.virtual_memory().available / 1e9 and m > 64:
+        m //= 2
+    scale = (n / m) ** 3
+    os.makedirs(os.path.join(ROOT, "_bench_tmp"), exist_ok=True)
+    phi, u, v, w = scene(m)
+    rng = np.random.default_rng(0)
+    u = rng.normal(size=u.shape) * 0.01; v = rng.normal(size=v.shape) * 0.01; w = rng.normal(size=w.shape) * 0.01
+    times = {}
+
+    def case(max_iteration, reinit_iterations=1):
+        path = refsim.write_sim(os.path.join(ROOT, "_bench_tmp", f"ref_{m}.sim"), m, water_drop=False, threads=threads,
+                                tolerance=1e-30, max_iteration=max_iteration, reinit_iterations=reinit_iterations)
+        c = refsim.RefCase(path)
+        for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
+            c.set(k, a)
+        return c
+
+    c = case(5)
+    t = time.perf_counter(); c.weno5_levelset(1e-4); times["weno_levelset"] = time.perf_counter() - t
+    t = time.perf_counter(); c.weno5_velocity(1e-4, 1); times["weno_velocity"] = time.perf_counter() - t
+    t = time.perf_counter(); c.viscosity(1e-4); times["viscosity"] = time.perf_counter() - t
+    for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
+        c.set(k, a)
+    t = time.perf_counter(); c.projection(1e-4); t5 = time.perf_counter() - t
+    t = time.perf_counter(); c.reinitialization(1e-4, 0); times["reinit_pseudo_step"] = time.perf_counter() - t
+    c.close()
+    c = case(15)
+    t = time.perf_counter(); c.projection(1e-4); t15 = time.perf_counter() - t
+    c.close()
+    per_it = max((t15 - t5) / 10.0, 0.0)
+    build = max(t5 - 5 * per_it, 0.0)
+    for f in os.listdir(os.path.join(ROOT, "_bench_tmp")):
+        os.remove(os.path.join(ROOT, "_bench_tmp", f))
+    os.rmdir(os.path.join(ROOT, "_bench_tmp"))
+    step_s = scale * (3 * times["weno_levelset"] + 3 * times["weno_velocity"] + 3 * times["viscosity"] +
+                      3 * (build + pcg_iterations_per_projection * per_it) + 3 * 10 * times["reinit_pseudo_step"])
+    sample = (f"reference operators timed once each at {m}^3 (cells scale x{scale:g} to {n}^3): WENO5 level set "
+              f"{times['weno_levelset']:.2f}s, WENO5 u,v,w {times['weno_velocity']:.2f}s, explicit viscosity "
+              f"{times['viscosity']:.2f}s, projection build {build:.2f}s + {per_it * 1e3:.1f} ms/PCG iteration, "
+              f"Sussman pseudo-step {times['reinit_pseudo_step']:.2f}s; scaled to 3 stages with "
+              f"{pcg_iterations_per_projection:.0f} PCG iterations per projection and 3x10 pseudo-steps")
+    return step_s * 1e3, sample
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.n
+    config = {"workload": f"rising air bubble {n}^3, density ratio 1000, one timestep (TVD-RK3, 3 projections)",
+              "grid": [n, n, n], "precision": "fp32+fp64-refine", "div_tolerance": 1e-6, "cfl": 0.5,
+              "l2": "inputs larger than L2 (67 MB per FP32 field), no flush", "parallelism": f"replicas{world}"}
+    metric = "timestep ms @256^3 (FP32+refine, 1e-6 relative divergence)"
+
+    if args.impl == "reference":
+        if rank != 0:
+            if dist is not None:
+                dist.destroy_process_group()
+            return
+        # the FP64 PCG iteration count of this workload on the GPU path at the
+        # same tolerance (measured in the default run; see profiles/)
+        iters = float(os.environ.get("FS_REF_PCG_ITERATIONS", "400"))
+        threads = 1
+        ms, sample = reference_sample(n, iters, threads)
+        line = {"impl": "reference", "metric": metric, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+                "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference", "sample": sample},
+                "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import fluid_simulator_backup_b200 as fs
+    fs.lib()
+    with ClockSampler(local) as clk:
+        s32, reps = run_steps(fs, n, fs.FS_PRECISION_FP32_REFINE, args.warmup, args.steps, barrier)
+    ms_steps = [r["ms"] for r in reps]
+    ms = max_over_ranks(float(np.mean(ms_steps)))
+    pcg_ms = sum(r["pcg_ms"] for r in reps)
+    pcg_its = sum(r["pcg_launched_iterations"] for r in reps)
+    real_its = sum(r["pcg_iterations"] for r in reps)
+    launches = sum(r["kernel_launches"] for r in reps)
+    N = n ** 3
+    per_iter_s = pcg_ms / 1e3 / max(pcg_its, 1)
+    achieved = BYTES_PER_UNKNOWN_PCG_FP32 * N / per_iter_s / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    e2e_ms, h2d, d2h = e2e_steps(fs, s32, n, args.e2e_steps)
+    e2e_ms = max_over_ranks(e2e_ms)
+    s32.close()
+
+    fp64 = None
+    if not args.no_fp64:
+        s64, reps64 = run_steps(fs, n, fs.FS_PRECISION_FP64, args.warmup, args.steps, barrier)
+        ms64 = max_over_ranks(float(np.mean([r["ms"] for r in reps64])))
+        fp64 = {"ms_per_step": ms64, "pcg_iterations_per_step": float(np.mean([r["pcg_iterations"] for r in reps64])),
+                "speedup_fp32_refine": ms64 / ms, "max_rel_residual": max(r["max_rel_residual"] for r in reps64)}
+        s64.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        iters = fp64["pcg_iterations_per_step"] / 3.0 if fp64 else 400.0
+        ref_ms, sample = reference_sample(n, iters, 1)
+        if ref_ms is not None:
+            cpu = {"value": ref_ms, "unit": "ms", "cores": 1, "kind": "reference", "sample": sample}
+
+    line = {
+        "metric": metric, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic", "config": config,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "FP32 inner PCG iteration (spmv + update + direction, 3 kernels)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "traffic": None,
+                     "bytes_per_iteration": BYTES_PER_UNKNOWN_PCG_FP32 * N,
+                     "pcg_ms": pcg_ms, "pcg_launched_iterations": pcg_its, "pcg_iterations": real_its},
+        "fp64": fp64,
+        "steps_detail": [{k: r[k] for k in ("ms", "pcg_iterations", "outer_iterations", "viscosity_iterations",
+                                             "max_rel_residual", "div_linf", "pcg_ms")} for r in reps],
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

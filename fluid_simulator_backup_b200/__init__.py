@@ -76,7 +76,8 @@ class StepReport(ctypes.Structure):
     _fields_ = [("pcg_iterations", ctypes.c_int), ("outer_iterations", ctypes.c_int),
                 ("viscosity_iterations", ctypes.c_int), ("projections", ctypes.c_int),
                 ("max_rel_residual", ctypes.c_double), ("div_l2", ctypes.c_double), ("div_linf", ctypes.c_double),
-                ("ms", ctypes.c_float)]
+                ("ms", ctypes.c_float), ("pcg_ms", ctypes.c_float), ("pcg_launched_iterations", ctypes.c_int),
+                ("kernel_launches", ctypes.c_int64)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -92,6 +92,11 @@ struct fs_ctx {
   double* sc_host = nullptr;        // pinned [16]
   double* staging = nullptr;        // packed FP64 transfer buffer
   std::map<int, cudaGraphExec_t> graphs;
+  // accounting for fs_step_report
+  int64_t launches = 0;
+  float pcg_ms = 0.0f;
+  int pcg_launched_iterations = 0;
+  cudaEvent_t evp0 = nullptr, evp1 = nullptr;
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -127,6 +132,8 @@ void release(fs_ctx* c) {
   if (c->st_host) cudaFreeHost(c->st_host);
   if (c->sc_host) cudaFreeHost(c->sc_host);
   if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->evp0) cudaEventDestroy(c->evp0);
+  if (c->evp1) cudaEventDestroy(c->evp1);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -173,8 +180,11 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   init.max_iter = max_iter;
   init.criterion = criterion;
   *c->st_host = init;
+  const bool timed = key < 100;  // pressure solves
   CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
+  if (timed) CK(cudaEventRecord(c->evp0, c->stream));
   pcg_init<V>(A, b, x, r, p, c->st, c->partials, c->stream);
+  c->launches += 1;
   CK(cudaGetLastError());
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
@@ -195,6 +205,15 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
     CK(cudaStreamSynchronize(c->stream));
     if (c->st_host->done) break;
     CK(cudaGraphLaunch(it->second, c->stream));
+    c->launches += 3 * kGraphIters;
+    if (timed) c->pcg_launched_iterations += kGraphIters;
+  }
+  if (timed) {
+    CK(cudaEventRecord(c->evp1, c->stream));
+    CK(cudaEventSynchronize(c->evp1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
+    c->pcg_ms += ms;
   }
   CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -226,6 +245,7 @@ fs_status advect_levelset_t(fs_ctx* c, double dt) {
   auto fe = [&](S* src, const S* base, S* out, double c0, double c1) {
     fill_extrap<S>(src, c->Lc, s);
     weno5_levelset<S>(src, base, out, u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, eps, dt, c0, c1, s);
+    c->launches += 2;
   };
   if (P.order == 3 && !(P.flags & FS_FLAG_LEVELSET_FORWARD_EULER)) {
     fe(phi, phi, t1, 0.0, 1.0);                        // phi1 = phi0 + dt L(phi0)
@@ -250,6 +270,7 @@ fs_status advect_velocity_t(fs_ctx* c, double dt) {
   weno5_mac<S>(u, F<S>(c->ua), u, v, w, c->Lu, c->Lu, c->Lv, c->Lw, 0, dx, eps, dt, c->stream);
   weno5_mac<S>(v, F<S>(c->va), u, v, w, c->Lv, c->Lu, c->Lv, c->Lw, 1, dx, eps, dt, c->stream);
   weno5_mac<S>(w, F<S>(c->wa), u, v, w, c->Lw, c->Lu, c->Lv, c->Lw, 2, dx, eps, dt, c->stream);
+  c->launches += 3;
   std::swap(c->u, c->ua);
   std::swap(c->v, c->va);
   std::swap(c->w, c->wa);
@@ -267,11 +288,12 @@ fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, 
   const int n = P.reinit_iterations;
   cudaStream_t s = c->stream;
   if (n == 0) {
-    if (c0 != 0.0) axpby<S>(F<S>(out), F<S>(base), F<S>(in), c0, c1, c->Lc, s);
+    if (c0 != 0.0) { axpby<S>(F<S>(out), F<S>(base), F<S>(in), c0, c1, c->Lc, s); c->launches += 1; }
     else if (out != in) CK(cudaMemcpyAsync(out, in, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s));
     return FS_OK;
   }
   sign_function<S>(F<S>(in), F<S>(c->sgn), c->Lc, dx, s);
+  c->launches += 1 + 2 * n;
   void* cur = in;
   for (int it = 0; it < n; ++it) {
     const bool last = it == n - 1;
@@ -313,6 +335,7 @@ fs_status viscosity_t(fs_ctx* c, double dt, int* iters_out) {
     viscosity_system<S>(F<S>(c->phi), F<S>(c->u), F<S>(c->v), F<S>(c->w), c->Lc, c->Lu, c->Lv, c->Lw, a,
                         c->grid.dx, dt, P.rho_neg, P.rho_pos, P.mu_neg, P.mu_pos, F<S>(c->vs[a][0]),
                         F<S>(c->vs[a][1]), F<S>(c->vs[a][2]), F<S>(c->vs[a][3]), F<S>(c->vs[a][4]), c->stream);
+    c->launches += 1;
     CK(cudaMemcpyAsync(c->vs[a][5], comps[a], lays[a]->total * c->S(), cudaMemcpyDeviceToDevice, c->stream));
   }
   CK(cudaGetLastError());
@@ -341,6 +364,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
   divergence_rhs<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, dt, c->b64, c->div64, c->partials, c->tickets + 0,
                     c->scalars + 0, s);
   subtract_mean(c->b64, c->Lc, c->scalars + 0, c->partials, c->tickets + 1, c->scalars + 1, s);
+  c->launches += 4;  // divergence, mean, pressure faces, pressure diagonal
   CK(cudaGetLastError());
   int iters = 0, outer = 0, st = 0;
   double rel = 0.0;
@@ -359,6 +383,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     for (outer = 0; outer <= P.max_outer; ++outer) {
       defect_residual<S>(phi, c->p64, c->b64, c->r64, (float*)c->prhs, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
                          c->tickets + 2, c->scalars + 2, s);
+      c->launches += 1;
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
@@ -375,15 +400,18 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
                          P.inner_tolerance, P.max_iteration, FS_STOP_RELATIVE, &it, nullptr, &st));
       iters += it;
       add_correction(c->p64, (float*)c->px, c->Lc, s);
+      c->launches += 1;
     }
     st = rel <= P.tolerance ? PCG_CONVERGED : PCG_MAXITER;
   }
   velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
   velocity_correct<S>(v, F<S>(c->v0), c->p64, phi, c->Lv, c->Lc, 1, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
   velocity_correct<S>(w, F<S>(c->w0), c->p64, phi, c->Lw, c->Lc, 2, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
+  c->launches += 3;
   CK(cudaGetLastError());
   if (rep) {
     divergence_norms<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, c->partials, c->tickets + 3, c->scalars + 4, s);
+    c->launches += 1;
     CK(cudaMemcpyAsync(c->sc_host, c->scalars, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     rep->iterations = iters;
@@ -406,7 +434,7 @@ fs_status gravity_t(fs_ctx* c, double dt) {
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   void* comps[3] = {c->u, c->v, c->w};
   for (int a = 0; a < 3; ++a)
-    if (g[a] != 0.0) add_const_faces<S>(F<S>(comps[a]), *lays[a], a, dt * g[a], 1, c->stream);
+    if (g[a] != 0.0) { add_const_faces<S>(F<S>(comps[a]), *lays[a], a, dt * g[a], 1, c->stream); c->launches += 1; }
   CK(cudaGetLastError());
   return FS_OK;
 }
@@ -423,6 +451,7 @@ fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* re
     zero_walls<S>(F<S>(c->u), *lays[0], 0, c->stream);
     zero_walls<S>(F<S>(c->v), *lays[1], 1, c->stream);
     zero_walls<S>(F<S>(c->w), *lays[2], 2, c->stream);
+    c->launches += 3;
   }
   CKS(gravity_t<S>(c, dt));
   int vit = 0;
@@ -475,6 +504,7 @@ fs_status step_t(fs_ctx* c, double dt, fs_step_report* rep) {
 template <class S>
 fs_status cfl_t(fs_ctx* c, double* dt) {
   absmax3<S>(F<S>(c->u), F<S>(c->v), F<S>(c->w), c->Lu, c->Lv, c->Lw, c->scalars + 8, c->stream);
+  c->launches += 3;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->sc_host + 8, c->scalars + 8, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -568,7 +598,8 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->Lw = make_lay(grid->nx, grid->ny, grid->nz + 1);
   auto fail = [&](fs_status s) { release(c); delete c; return s; };
   if (cudaGetDevice(&c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->evp0) != cudaSuccess || cudaEventCreate(&c->evp1) != cudaSuccess) {
     set_error("CUDA stream/event creation failed: %s", cudaGetErrorString(cudaGetLastError()));
     return fail(FS_CUDA_ERROR);
   }
@@ -773,10 +804,16 @@ fs_status fs_step(fs_ctx* c, double dt, fs_step_report* rep) {
   fs_step_report local{};
   fs_step_report* r = rep ? rep : &local;
   *r = fs_step_report{};
+  c->launches = 0;
+  c->pcg_ms = 0.0f;
+  c->pcg_launched_iterations = 0;
   CKS(timed_begin(c));
   fs_status s = DISPATCH(c, step_t, c, dt, r);
   if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
   CKS(timed_end(c, &r->ms));
+  r->pcg_ms = c->pcg_ms;
+  r->pcg_launched_iterations = c->pcg_launched_iterations;
+  r->kernel_launches = c->launches;
   return s;
 }
 

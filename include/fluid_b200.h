@@ -108,6 +108,9 @@ typedef struct {
   double max_rel_residual;  /* worst pressure residual of the step */
   double div_l2, div_linf;  /* divergence after the last projection */
   float ms;                 /* device time of the step */
+  float pcg_ms;             /* device time inside the pressure PCG loops (FP32 inner loops in FP32_REFINE) */
+  int pcg_launched_iterations; /* PCG iterations whose kernels ran in those loops (incl. the idle tail of the last batch) */
+  int64_t kernel_launches;  /* kernels launched by the step (graph nodes counted individually) */
 } fs_step_report;
 
 /* Defaults that reproduce the reference's script defaults where it has them

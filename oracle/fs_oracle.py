@@ -393,8 +393,11 @@ def pcg(apply_A, diag, b, x0, tol, max_iter, criterion="abs"):
     r = b - apply_A(x)
     p = r / diag
     rz = _seqdot(r, p)
-    bnorm = math.sqrt(_seqdot(b, b)) or 1.0
+    bb = _seqdot(b, b)
+    bnorm = math.sqrt(bb) or 1.0
     it = 0
+    if criterion != "abs" and (bb == 0.0 or math.sqrt(_seqdot(r, r)) / bnorm <= tol):
+        return x, 0, rz, math.sqrt(_seqdot(r, r)) / bnorm
     while it < max_iter:
         q = apply_A(p)
         alpha = rz / _seqdot(p, q)
