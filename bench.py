@@ -202,6 +202,20 @@ def reference_sample(n, pcg_iterations_per_projection, threads=1):
     return step_s * 1e3, sample
 
 
+def reference_sample_isolated(n, iters, threads=1):
+    """reference_sample in a child process: the reference calls exit() on
+    some inputs (LEVELSET_3D.h:1040-1044) and holds tens of GB of host
+    memory at 256^3; neither should touch the benchmark process."""
+    code = ("import json, sys; sys.path.insert(0, %r); import bench; "
+            "ms, sample = bench.reference_sample(%d, %r, %d); print('REFJSON' + json.dumps([ms, sample]))"
+            % (ROOT, n, float(iters), threads))
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, timeout=1200)
+    for line in p.stdout.splitlines():
+        if line.startswith("REFJSON"):
+            return tuple(json.loads(line[7:]))
+    return None, f"reference sample failed (rc={p.returncode}): {p.stderr.strip()[-300:]}"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,7 +268,7 @@ def main():
         # same tolerance (measured in the default run; see profiles/)
         iters = float(os.environ.get("FS_REF_PCG_ITERATIONS", "400"))
         threads = 1
-        ms, sample = reference_sample(n, iters, threads)
+        ms, sample = reference_sample_isolated(n, iters, threads)
         line = {"impl": "reference", "metric": metric, "value": ms, "unit": "ms", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
                 "dtype": "f64", "data": "synthetic", "config": config,
@@ -300,7 +314,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         iters = fp64["pcg_iterations_per_step"] / 3.0 if fp64 else 400.0
-        ref_ms, sample = reference_sample(n, iters, 1)
+        ref_ms, sample = reference_sample_isolated(n, iters, 1)
         if ref_ms is not None:
             cpu = {"value": ref_ms, "unit": "ms", "cores": 1, "kind": "reference", "sample": sample}
 
