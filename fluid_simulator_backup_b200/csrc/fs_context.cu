@@ -348,7 +348,10 @@ fs_status viscosity_t(fs_ctx* c, double dt, int* iters_out) {
                    nullptr, &st));
     total += it;
   }
-  for (int a = 0; a < 3; ++a) std::swap(c->vs[a][5], a == 0 ? c->u : (a == 1 ? c->v : c->w));
+  // the solution buffers stay where the captured solver graphs expect them;
+  // copy the result back into the velocity fields
+  for (int a = 0; a < 3; ++a)
+    CK(cudaMemcpyAsync(comps[a], c->vs[a][5], lays[a]->total * c->S(), cudaMemcpyDeviceToDevice, c->stream));
   if (iters_out) *iters_out = total;
   return FS_OK;
 }

@@ -724,7 +724,7 @@ def zero_walls(u, v, w):
     return tuple(out)
 
 
-def step(phi, u, v, w, dx, dt, P, p0=None):
+def step(phi, u, v, w, dx, dt, P, p0=None, order=3):
     """One timestep of the corrected specification, order 3:
     level set TVD-RK3 (Shu-Osher) with the step's initial velocity; velocity
     Shu-Osher RK3 over SolveForRK stages (WENO5 self-advection, wall faces
@@ -736,8 +736,11 @@ def step(phi, u, v, w, dx, dt, P, p0=None):
     eps = P["eps"]
     L = lambda f: weno5_levelset(f, u, v, w, dx, dt, eps)
     phi1 = L(phi)
-    phi2 = 0.75 * phi + 0.25 * L(phi1)
-    phin = (1.0 / 3.0) * phi + (2.0 / 3.0) * L(phi2)
+    if order == 3:
+        phi2 = 0.75 * phi + 0.25 * L(phi1)
+        phin = (1.0 / 3.0) * phi + (2.0 / 3.0) * L(phi2)
+    else:  # Heun (EULERIAN_FLUID_SOLVER_3D.h:809-832, 888-911)
+        phin = 0.5 * phi + 0.5 * L(phi1)
     p = np.zeros_like(phi) if p0 is None else p0
     info = {"iterations": [], "rel_residual": []}
 
@@ -759,11 +762,18 @@ def step(phi, u, v, w, dx, dt, P, p0=None):
         return out
 
     base = (u, v, w)
-    s1 = stage(base, 0.0, 1.0, base)
-    s2 = stage(s1, 0.75, 0.25, base)
-    s3 = stage(s2, 1.0 / 3.0, 2.0 / 3.0, base)
     it, sc = P["reinit_iterations"], P["reinit_scaling"]
-    r1 = reinitialization_block(phin, dx, it, sc, eps)
-    r2 = 0.75 * phin + 0.25 * reinitialization_block(r1, dx, it, sc, eps)
-    phi_out = (1.0 / 3.0) * phin + (2.0 / 3.0) * reinitialization_block(r2, dx, it, sc, eps)
+    if order == 3:
+        s1 = stage(base, 0.0, 1.0, base)
+        s2 = stage(s1, 0.75, 0.25, base)
+        s3 = stage(s2, 1.0 / 3.0, 2.0 / 3.0, base)
+        r1 = reinitialization_block(phin, dx, it, sc, eps)
+        r2 = 0.75 * phin + 0.25 * reinitialization_block(r1, dx, it, sc, eps)
+        phi_out = (1.0 / 3.0) * phin + (2.0 / 3.0) * reinitialization_block(r2, dx, it, sc, eps)
+    else:
+        s3 = stage(base, 0.0, 1.0, base)
+        if order == 2:
+            s3 = stage(s3, 0.5, 0.5, base)
+        r1 = reinitialization_block(phin, dx, it, sc, eps)
+        phi_out = 0.5 * phin + 0.5 * reinitialization_block(r1, dx, it, sc, eps)
     return phi_out, s3[0], s3[1], s3[2], p, info

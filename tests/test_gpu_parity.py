@@ -190,16 +190,21 @@ def test_cfl_matches_reference_formula():
         assert abs(s.cfl_dt() - float(g["out"])) < 1e-14 * float(g["out"])
 
 
-@pytest.mark.parametrize("precision,tol", [(fs.FS_PRECISION_FP64, 1e-6), (fs.FS_PRECISION_FP32_REFINE, 5e-4)])
-def test_whole_step_matches_oracle(precision, tol):
+@pytest.mark.parametrize("order", [1, 3])
+@pytest.mark.parametrize("precision,tol", [(fs.FS_PRECISION_FP64, 1e-8), (fs.FS_PRECISION_FP32_REFINE, 5e-4)])
+def test_whole_step_matches_oracle(precision, tol, order):
+    """Two full timesteps (with semi-implicit viscosity) against the oracle's
+    corrected step, both pressure solves stopped at a 1e-12 relative
+    residual; fields compared relative to their maximum: 1e-8 in FP64, 5e-4
+    with FP32 storage."""
     n = 16
     dx = 1.0 / n
     phi = sphere(n, (0.5, 0.35, 0.5), 0.2)
     u = np.zeros((n, n, n + 1)); v = np.zeros((n, n + 1, n)); w = np.zeros((n + 1, n, n))
     P = dict(rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0), eps=1e-6,
-             reinit_iterations=10, reinit_scaling=5, tol=1e-10, max_iter=20000, viscosity=True, visc_tol=1e-12)
-    with make(n, precision, rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, tolerance=1e-10,
-              viscosity_tolerance=1e-12) as s:
+             reinit_iterations=10, reinit_scaling=5, tol=1e-12, max_iter=20000, viscosity=True, visc_tol=1e-12)
+    with make(n, precision, rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, tolerance=1e-12,
+              viscosity_tolerance=1e-12, order=order) as s:
         upload_all(s, phi, u, v, w)
         dt = s.cfl_dt()
         states = []
@@ -207,11 +212,11 @@ def test_whole_step_matches_oracle(precision, tol):
         ph, uu, vv, ww = phi, u, v, w
         for _ in range(2):
             rep = s.step(dt)
-            assert rep["projections"] == 3
-            ph, uu, vv, ww, p0, info = O.step(ph, uu, vv, ww, dx, dt, P, p0)
+            assert rep["projections"] == order
+            ph, uu, vv, ww, p0, info = O.step(ph, uu, vv, ww, dx, dt, P, p0, order=order)
             states.append(([s.download(k) for k in ("phi", "u", "v", "w")], (ph, uu, vv, ww)))
     for got, ref in states:
-        assert rel_err(got[0], ref[0]) < tol
+        assert rel_err(got[0], ref[0]) < max(tol / 10, 1e-6)
         for a, b in zip(got[1:], ref[1:]):
             assert np.abs(a - b).max() < tol * max(np.abs(b).max(), 1e-3)
 
