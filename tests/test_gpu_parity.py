@@ -203,7 +203,9 @@ def test_whole_step_matches_oracle(precision, tol, order):
     u = np.zeros((n, n, n + 1)); v = np.zeros((n, n + 1, n)); w = np.zeros((n + 1, n, n))
     P = dict(rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0), eps=1e-6,
              reinit_iterations=10, reinit_scaling=5, tol=1e-12, max_iter=20000, viscosity=True, visc_tol=1e-12)
-    with make(n, precision, rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, tolerance=1e-12,
+    # the FP64 defect residual of the FP32 path floors near 1e-11 here
+    ptol = 1e-12 if precision == fs.FS_PRECISION_FP64 else 1e-10
+    with make(n, precision, rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, tolerance=ptol,
               viscosity_tolerance=1e-12, order=order) as s:
         upload_all(s, phi, u, v, w)
         dt = s.cfl_dt()
