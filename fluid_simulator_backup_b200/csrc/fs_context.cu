@@ -399,8 +399,12 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       if (rel <= P.tolerance || outer == P.max_outer) break;
       CK(cudaMemsetAsync(c->px, 0, vbytes, s));
       int it = 0;
+      // ask the FP32 solve for the reduction that would reach the target
+      // (with a safety factor), but never below what FP32 arithmetic can
+      // deliver (inner_tolerance); the FP64 defect then decides
+      const double inner = std::min(0.5, std::max(0.3 * P.tolerance / rel, P.inner_tolerance));
       CKS(run_pcg<float>(c, 2, A, (float*)c->prhs, (float*)c->px, (float*)c->pr, (float*)c->pp, (float*)c->pq,
-                         P.inner_tolerance, P.max_iteration, FS_STOP_RELATIVE, &it, nullptr, &st));
+                         inner, P.max_iteration, FS_STOP_RELATIVE, &it, nullptr, &st));
       iters += it;
       add_correction(c->p64, (float*)c->px, c->Lc, s);
       c->launches += 1;
@@ -550,7 +554,7 @@ void fs_params_default(fs_params* p) {
   p->stop = FS_STOP_RELATIVE;
   p->tolerance = 1e-6;
   p->max_iteration = 20000;
-  p->inner_tolerance = 1e-2;
+  p->inner_tolerance = 1e-5;
   p->max_outer = 20;
   p->viscosity = 1;
   p->viscosity_tolerance = 1e-8;

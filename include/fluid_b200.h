@@ -82,7 +82,8 @@ typedef struct {
   int stop;                         /* fs_stop for the pressure solve */
   double tolerance;                 /* pressure tolerance (relative divergence in FP32_REFINE) */
   int max_iteration;                /* PCG iteration cap per solve (inner cap in FP32_REFINE) */
-  double inner_tolerance;           /* FP32_REFINE: relative reduction asked of each inner solve */
+  double inner_tolerance;           /* FP32_REFINE: smallest relative reduction asked of one inner FP32
+                                       solve; each inner solve targets 0.3*tolerance/current residual */
   int max_outer;                    /* FP32_REFINE: defect-correction cap */
   int viscosity;                    /* 0: off, 1: semi-implicit */
   double viscosity_tolerance;       /* relative residual of each viscosity solve */
