@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -97,6 +98,7 @@ struct fs_ctx {
   float pcg_ms = 0.0f;
   int pcg_launched_iterations = 0;
   cudaEvent_t evp0 = nullptr, evp1 = nullptr;
+  bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -179,6 +181,7 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   init.tol = tol;
   init.max_iter = max_iter;
   init.criterion = criterion;
+  init.stall_limit = c->fp32 ? 400 : 0;  // FP32 iterations can stall at their rounding floor
   *c->st_host = init;
   const bool timed = key < 100;  // pressure solves
   CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
@@ -221,8 +224,11 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   if (iterations) *iterations = s.iter;
   if (rel) *rel = s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0;
   if (status) *status = s.status;
+  if (c->debug)
+    std::fprintf(stderr, "[fs] pcg key %d: %d iterations, status %d, rel %.3e\n", key, s.iter, s.status,
+                 s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0);
   if (s.status == PCG_NONFINITE) {
-    set_error("non-finite residual in a PCG solve");
+    set_error("non-finite residual in a PCG solve (key %d, iteration %d)", key, s.iter);
     return FS_NONFINITE;
   }
   return FS_OK;
@@ -403,8 +409,12 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       // (with a safety factor), but never below what FP32 arithmetic can
       // deliver (inner_tolerance); the FP64 defect then decides
       const double inner = std::min(0.5, std::max(0.3 * P.tolerance / rel, P.inner_tolerance));
+      double inner_rel = 0.0;
       CKS(run_pcg<float>(c, 2, A, (float*)c->prhs, (float*)c->px, (float*)c->pr, (float*)c->pp, (float*)c->pq,
-                         inner, P.max_iteration, FS_STOP_RELATIVE, &it, nullptr, &st));
+                         inner, P.max_iteration, FS_STOP_RELATIVE, &it, &inner_rel, &st));
+      if (c->debug)
+        std::fprintf(stderr, "[fs] outer %d: defect %.3e, inner target %.1e -> %d iterations (status %d, %.3e)\n",
+                     outer, rel, inner, it, st, inner_rel);
       iters += it;
       add_correction(c->p64, (float*)c->px, c->Lc, s);
       c->launches += 1;
@@ -599,6 +609,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->grid = *grid;
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
+  c->debug = std::getenv("FS_DEBUG") != nullptr;
   c->Lc = make_lay(grid->nx, grid->ny, grid->nz);
   c->Lu = make_lay(grid->nx + 1, grid->ny, grid->nz);
   c->Lv = make_lay(grid->nx, grid->ny + 1, grid->nz);

@@ -26,12 +26,16 @@ template <class T> void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s)
 // ---- Krylov solver state shared by the pressure and viscosity solves
 struct PcgState {
   double rz, pq, rr, bb, beta, tol;
-  int iter, max_iter, done, criterion, status, pad;
+  double best_rr;   // smallest r.r seen
+  int iter, max_iter, done, criterion, status, stall;
+  int stall_limit;  // iterations without a 1% improvement of best_rr before giving up
   unsigned int ticket;
-  unsigned int pad2;
 };
 
-enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_MAXITER = 2, PCG_NONFINITE = 3 };
+// STAGNATED: the iteration can make no further progress in its arithmetic
+// (p.Ap <= 0 or no improvement for stall_limit iterations); the iterate is
+// kept and the caller decides (the FP64 defect correction continues).
+enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_MAXITER = 2, PCG_NONFINITE = 3, PCG_STAGNATED = 4 };
 
 // Seven-point symmetric operator on a padded layout:
 // (A x)_c = diag_c x_c - sum_d (a_d[c] x_{c-e_d} + a_d[c+e_d] x_{c+e_d});

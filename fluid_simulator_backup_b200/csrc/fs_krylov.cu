@@ -99,6 +99,8 @@ __global__ void __launch_bounds__(256) k_pcg_init(Op7<V> A, const V* __restrict_
     st->bb = tot[2];
     st->iter = 0;
     st->beta = 0.0;
+    st->best_rr = tot[1];
+    st->stall = 0;
     st->status = PCG_RUNNING;
     st->done = 0;
     const bool nonfinite = !isfinite(tot[0]) || !isfinite(tot[1]);
@@ -142,13 +144,17 @@ __global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x,
                                                     const V* __restrict__ p, const V* __restrict__ q, PcgState* st,
                                                     double* partials) {
   if (((volatile PcgState*)st)->done) return;
-  const double alpha = ((volatile PcgState*)st)->rz / ((volatile PcgState*)st)->pq;
+  const double pq_all = ((volatile PcgState*)st)->pq;
+  const double alpha = ((volatile PcgState*)st)->rz / pq_all;
+  // a non-positive p.Ap (or an infinite step) means the iteration has lost
+  // its footing in this arithmetic: keep the iterate, stop (uniform branch)
+  const bool breakdown = !(pq_all > 0.0) || !isfinite(alpha);
   const V a = (V)alpha;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   double rz = 0.0, rr = 0.0;
-  if (i < A.L.nx && j < A.L.ny && k < A.L.nz) {
+  if (!breakdown && i < A.L.nx && j < A.L.ny && k < A.L.nz) {
     const int64_t c = A.L.at(i, j, k);
     x[c] += a * p[c];
     const V rv = r[c] - a * q[c];
@@ -158,12 +164,23 @@ __global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x,
   }
   double tot[3];
   if (grid_reduce3(rz, rr, 0.0, partials, &st->ticket, tot)) {
+    if (breakdown) {
+      st->status = PCG_STAGNATED;
+      st->done = 1;
+      return;
+    }
     const double rz_old = st->rz;
     st->rr = tot[1];
-    const bool nonfinite = !isfinite(tot[0]) || !isfinite(tot[1]) || !isfinite(alpha);
+    const bool nonfinite = !isfinite(tot[0]) || !isfinite(tot[1]);
     const bool converged = st->criterion == 1 ? (tot[0] < st->tol * st->tol)
                                               : (sqrt(tot[1]) <= st->tol * sqrt(st->bb));
     st->rz = tot[0];
+    if (tot[1] < 0.99 * st->best_rr) {
+      st->best_rr = tot[1];
+      st->stall = 0;
+    } else {
+      st->stall += 1;
+    }
     if (nonfinite) {
       st->status = PCG_NONFINITE;
       st->done = 1;
@@ -175,6 +192,9 @@ __global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x,
       st->iter += 1;
       if (st->iter >= st->max_iter) {
         st->status = PCG_MAXITER;
+        st->done = 1;
+      } else if (st->stall_limit > 0 && st->stall >= st->stall_limit) {
+        st->status = PCG_STAGNATED;
         st->done = 1;
       }
     }
