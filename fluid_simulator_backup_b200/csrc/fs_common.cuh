@@ -55,6 +55,41 @@ inline Launch3 launch3(int nx, int ny, int nz, int bx = 32, int by = 4, int bz =
   const int k = blockIdx.z * blockDim.z + threadIdx.z; \
   if (i >= (L).nx || j >= (L).ny || k >= (L).nz) return;
 
+// Grid-stride traversal of the interior of a layout, x fastest, for the
+// reduction kernels: they run on a grid of a few blocks per SM (set by
+// reduction_blocks), so the per-block partial sums and the one atomic
+// ticket per block stay few.  The cursor advances (i, j, k) by the grid
+// stride with carries instead of dividing every linear index.
+struct Cursor {
+  int i, j, k, si, sj, sk;
+  __device__ __forceinline__ void init(const Lay& L) {
+    const int64_t start = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t row = start / L.nx;
+    i = (int)(start % L.nx);
+    j = (int)(row % L.ny);
+    k = (int)(row / L.ny);
+    const int64_t srow = stride / L.nx;
+    si = (int)(stride % L.nx);
+    sj = (int)(srow % L.ny);
+    sk = (int)(srow / L.ny);
+  }
+  __device__ __forceinline__ bool valid(const Lay& L) const { return k < L.nz; }
+  __device__ __forceinline__ void next(const Lay& L) {
+    i += si;
+    int c = i >= L.nx;
+    i -= c ? L.nx : 0;
+    j += sj + c;
+    c = j >= L.ny;
+    j -= c ? L.ny : 0;
+    k += sk + c;
+  }
+};
+
+// Blocks for a grid-stride reduction kernel of 256 threads over n items.
+int reduction_blocks(int64_t n);
+constexpr int kRedThreads = 256;
+
 // Block-wide sum of a double (any block size that is a multiple of 32, up
 // to 1024).  Result valid in thread 0.
 __device__ __forceinline__ double warp_sum(double v) {

@@ -174,21 +174,10 @@ fs_status check_params(const fs_params* p) {
 // Krylov driver
 // ---------------------------------------------------------------------------
 
+// Launch captured batches of kGraphIters iterations until the solver state
+// says stop (done != 0); one host check of the state per batch.
 template <class V>
-fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V* p, V* q, double tol, int max_iter,
-                  int criterion, int* iterations, double* rel, int* status) {
-  PcgState init{};
-  init.tol = tol;
-  init.max_iter = max_iter;
-  init.criterion = criterion;
-  init.stall_limit = c->fp32 ? 400 : 0;  // FP32 iterations can stall at their rounding floor
-  *c->st_host = init;
-  const bool timed = key < 100;  // pressure solves
-  CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
-  if (timed) CK(cudaEventRecord(c->evp0, c->stream));
-  pcg_init<V>(A, b, x, r, p, c->st, c->partials, c->stream);
-  c->launches += 1;
-  CK(cudaGetLastError());
+fs_status drive_pcg(fs_ctx* c, int key, const Op7<V>& A, V* x, V* r, V* p, V* q, int max_iter, bool timed) {
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
@@ -200,17 +189,39 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
     cudaGraphDestroy(g);
     it = c->graphs.emplace(key, ge).first;
   }
-  // one graph per 16 iterations; the kernels of a converged solve return at
-  // once, so the bound below only caps the number of host checks
+  // the kernels of a stopped solve return at once, so the bound below only
+  // caps the number of host checks
   const int max_launches = max_iter / kGraphIters + 2;
   for (int n = 0; n < max_launches; ++n) {
     CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    if (c->st_host->done) break;
+    if (c->st_host->done) return FS_OK;
     CK(cudaGraphLaunch(it->second, c->stream));
     c->launches += 3 * kGraphIters;
     if (timed) c->pcg_launched_iterations += kGraphIters;
   }
+  CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+template <class V>
+fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V* p, V* q, double tol, int max_iter,
+                  int criterion, int* iterations, double* rel, int* status) {
+  PcgState init{};
+  init.tol = tol;
+  init.max_iter = max_iter;
+  init.criterion = criterion;
+  // FP32 viscosity solves can stall at their rounding floor before a tight tolerance
+  init.stall_limit = (c->fp32 && key >= 100) ? 400 : 0;
+  *c->st_host = init;
+  const bool timed = key < 100;  // pressure solves
+  CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
+  if (timed) CK(cudaEventRecord(c->evp0, c->stream));
+  pcg_init<V>(A, b, x, r, p, c->st, c->partials, c->stream);
+  c->launches += 1;
+  CK(cudaGetLastError());
+  CKS(drive_pcg<V>(c, key, A, x, r, p, q, max_iter, timed));
   if (timed) {
     CK(cudaEventRecord(c->evp1, c->stream));
     CK(cudaEventSynchronize(c->evp1));
@@ -218,8 +229,6 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
     CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
     c->pcg_ms += ms;
   }
-  CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
   const PcgState& s = *c->st_host;
   if (iterations) *iterations = s.iter;
   if (rel) *rel = s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0;
@@ -389,37 +398,72 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
                                       (float*)c->paz, (float*)c->pdiag, s);
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc};
     const size_t vbytes = c->Lc.total * sizeof(float);
-    for (outer = 0; outer <= P.max_outer; ++outer) {
-      defect_residual<S>(phi, c->p64, c->b64, c->r64, (float*)c->prhs, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
+    double bb = 0.0;
+    // true FP64 residual of the current pressure (b - A64 p64, A64 from phi
+    // in FP64); its FP32 image lands in the Krylov residual buffer
+    auto defect = [&]() -> fs_status {
+      defect_residual<S>(phi, c->p64, c->b64, c->r64, (float*)c->pr, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
                          c->tickets + 2, c->scalars + 2, s);
       c->launches += 1;
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      const double bb = c->sc_host[1], rr = c->sc_host[2];
+      bb = c->sc_host[1];
+      const double rr = c->sc_host[2];
       rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+      outer += 1;
       if (!std::isfinite(rel)) {
         set_error("non-finite defect residual");
         return FS_NONFINITE;
       }
-      if (rel <= P.tolerance || outer == P.max_outer) break;
+      return FS_OK;
+    };
+    CKS(defect());
+    st = PCG_CONVERGED;
+    if (rel > P.tolerance) {
       CK(cudaMemsetAsync(c->px, 0, vbytes, s));
-      int it = 0;
-      // ask the FP32 solve for the reduction that would reach the target
-      // (with a safety factor), but never below what FP32 arithmetic can
-      // deliver (inner_tolerance); the FP64 defect then decides
-      const double inner = std::min(0.5, std::max(0.3 * P.tolerance / rel, P.inner_tolerance));
-      double inner_rel = 0.0;
-      CKS(run_pcg<float>(c, 2, A, (float*)c->prhs, (float*)c->px, (float*)c->pr, (float*)c->pp, (float*)c->pq,
-                         inner, P.max_iteration, FS_STOP_RELATIVE, &it, &inner_rel, &st));
-      if (c->debug)
-        std::fprintf(stderr, "[fs] outer %d: defect %.3e, inner target %.1e -> %d iterations (status %d, %.3e)\n",
-                     outer, rel, inner, it, st, inner_rel);
-      iters += it;
-      add_correction(c->p64, (float*)c->px, c->Lc, s);
+      PcgState init{};
+      init.criterion = 2;  // absolute 2-norm of the FP32 residual, in b's units
+      init.tol = 0.5 * P.tolerance * std::sqrt(bb);
+      init.max_iter = P.max_iteration;
+      init.reliable_delta = 0.1;
+      *c->st_host = init;
+      CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
+      CK(cudaEventRecord(c->evp0, s));
+      pcg_init<float>(A, (float*)c->pr, (float*)c->px, (float*)c->pr, (float*)c->pp, c->st, c->partials, s);
       c->launches += 1;
+      int restarts = 0;
+      for (;;) {
+        CKS(drive_pcg<float>(c, 2, A, (float*)c->px, (float*)c->pr, (float*)c->pp, (float*)c->pq, P.max_iteration,
+                             true));
+        const int status = c->st_host->status;
+        iters = c->st_host->iter;
+        if (status == PCG_NONFINITE) {
+          set_error("non-finite residual in the FP32 pressure iteration (iteration %d)", iters);
+          return FS_NONFINITE;
+        }
+        // fold the FP32 correction into the FP64 pressure and take the true residual
+        add_correction(c->p64, (float*)c->px, c->Lc, s);
+        c->launches += 1;
+        CK(cudaMemsetAsync(c->px, 0, vbytes, s));
+        CKS(defect());
+        if (c->debug)
+          std::fprintf(stderr, "[fs] reliable update %d: iteration %d, status %d, true residual %.3e\n", outer - 1,
+                       iters, status, rel);
+        if (rel <= P.tolerance) { st = PCG_CONVERGED; break; }
+        if (iters >= P.max_iteration) { st = PCG_MAXITER; break; }
+        const bool restart = status == PCG_STAGNATED;
+        if (restart && ++restarts > 5) { st = PCG_MAXITER; break; }
+        pcg_resume<float>(A, (float*)c->pr, (float*)c->pp, c->st, c->partials, restart ? 1 : 0, s);
+        c->launches += 2;
+        CK(cudaGetLastError());
+      }
+      CK(cudaEventRecord(c->evp1, s));
+      CK(cudaEventSynchronize(c->evp1));
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
+      c->pcg_ms += ms;
     }
-    st = rel <= P.tolerance ? PCG_CONVERGED : PCG_MAXITER;
   }
   velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
   velocity_correct<S>(v, F<S>(c->v0), c->p64, phi, c->Lv, c->Lc, 1, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);

@@ -26,16 +26,21 @@ template <class T> void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s)
 // ---- Krylov solver state shared by the pressure and viscosity solves
 struct PcgState {
   double rz, pq, rr, bb, beta, tol;
-  double best_rr;   // smallest r.r seen
+  double best_rr;         // smallest r.r seen
+  double max_rr;          // largest r.r since the last true residual (reliable updates)
+  double rz_prev;         // r.z at the start of the last accepted step
+  double reliable_delta;  // pause for a true residual when ||r|| < delta*max||r|| (0: never)
   int iter, max_iter, done, criterion, status, stall;
-  int stall_limit;  // iterations without a 1% improvement of best_rr before giving up
+  int stall_limit;  // iterations without a 1% improvement of best_rr before giving up (0: never)
   unsigned int ticket;
 };
 
 // STAGNATED: the iteration can make no further progress in its arithmetic
 // (p.Ap <= 0 or no improvement for stall_limit iterations); the iterate is
-// kept and the caller decides (the FP64 defect correction continues).
-enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_MAXITER = 2, PCG_NONFINITE = 3, PCG_STAGNATED = 4 };
+// kept and the caller decides.  RELIABLE_UPDATE: paused (done = 2) for the
+// caller to replace the recursive residual by the true one.
+enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_MAXITER = 2, PCG_NONFINITE = 3, PCG_STAGNATED = 4,
+       PCG_RELIABLE_UPDATE = 5 };
 
 // Seven-point symmetric operator on a padded layout:
 // (A x)_c = diag_c x_c - sum_d (a_d[c] x_{c-e_d} + a_d[c+e_d] x_{c+e_d});
@@ -53,6 +58,8 @@ template <class V>
 void pcg_init(const Op7<V>& A, const V* b, V* x, V* r, V* p, PcgState* st, double* partials, cudaStream_t s);
 template <class V>
 void pcg_iteration(const Op7<V>& A, V* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+template <class V>
+void pcg_resume(const Op7<V>& A, const V* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);
 int pcg_blocks(const Lay& L);
 
 // ---- projection family (fs_projection.cu)

@@ -1,39 +1,57 @@
 // Jacobi-preconditioned conjugate gradients on a matrix-free seven-point
-// operator (PCG_METHOD.cpp:4-126 restated for the GPU).
+// operator (PCG_METHOD.cpp:4-126 restated for the GPU), with optional
+// reliable updates for the mixed-precision pressure solve.
 //
 // One iteration is three kernels:
 //   spmv    q = A p and p.q                      (reads p, ax, ay, az, diag; writes q)
 //   update  x += alpha p, r -= alpha q, r.z, r.r (reads x, p, r, q, diag; writes x, r)
 //   pupdate p = r/diag + beta p                  (reads r, diag, p; writes p)
-// z = r/diag is never stored.  Dot products are block-reduced in FP64 and
-// finished by the last block of the grid (deterministic for a given launch
-// shape), which also takes the scalar decisions (alpha, beta, convergence,
-// iteration cap, NaN) and writes them to the PcgState in device memory.
-// Every kernel starts by reading `done`, so batches of iterations captured
-// in a CUDA graph cost a few microseconds per launch once converged.
+// z = r/diag is never stored: 68 bytes per unknown and iteration in FP32,
+// 136 in FP64.  The kernels run grid-stride over a grid of a few blocks per
+// SM; dot products are reduced in FP64 per block and finished by the last
+// block (deterministic for a given grid), which also takes the scalar
+// decisions (alpha, beta, convergence, caps, breakdown) and writes them to
+// the PcgState in device memory.  Every kernel starts by reading `done`, so
+// iterations captured in a CUDA graph cost microseconds once a solve stops.
+//
+// Reliable updates (Clark et al., "Solving lattice QCD systems of equations
+// using mixed precision solvers on GPUs", 2010): in the FP32 pressure solve
+// the update kernel pauses the iteration (done = 2) whenever the recursive
+// residual has dropped by `reliable_delta` since the last true residual; the
+// host then folds x into the FP64 pressure, recomputes the true residual in
+// FP64 and resumes the same Krylov iteration (pcg_resume) with that residual,
+// keeping the search direction.  The FP32 iteration therefore converges like
+// one long CG instead of a sequence of restarted ones.
 #include "fs_kernels.h"
 
 namespace fsb {
 
-constexpr int KB_X = 32, KB_Y = 4, KB_Z = 2;  // 256 threads
+static int g_sm_count = 0;
 
-int pcg_blocks(const Lay& L) {
-  return ((L.nx + KB_X - 1) / KB_X) * ((L.ny + KB_Y - 1) / KB_Y) * ((L.nz + KB_Z - 1) / KB_Z);
+int reduction_blocks(int64_t n) {
+  if (g_sm_count <= 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) g_sm_count = 148;
+  }
+  const int64_t want = (n + kRedThreads - 1) / kRedThreads;
+  const int64_t cap = (int64_t)4 * g_sm_count;
+  return (int)(want < cap ? (want > 0 ? want : 1) : cap);
 }
 
-static inline Launch3 kl(const Lay& L) { return launch3(L.nx, L.ny, L.nz, KB_X, KB_Y, KB_Z); }
+int pcg_blocks(const Lay& L) { return reduction_blocks((int64_t)L.nx * L.ny * L.nz); }
 
 template <class V>
 __device__ __forceinline__ V apply7(const Op7<V>& A, const V* __restrict__ x, int64_t c) {
-  const int64_t sx = 1, sy = A.L.px, sz = A.L.slab;
+  const int64_t sy = A.L.px, sz = A.L.slab;
   V acc = A.diag[c] * x[c];
-  acc -= A.ax[c] * x[c - sx] + A.ax[c + sx] * x[c + sx];
+  acc -= A.ax[c] * x[c - 1] + A.ax[c + 1] * x[c + 1];
   acc -= A.ay[c] * x[c - sy] + A.ay[c + sy] * x[c + sy];
   acc -= A.az[c] * x[c - sz] + A.az[c + sz] * x[c + sz];
   return acc;
 }
 
-// Three FP64 sums through one grid reduction.
+// Three FP64 sums through one grid reduction (1-D grids).
 __device__ __forceinline__ bool grid_reduce3(double a, double b, double c, double* partials, unsigned int* ticket,
                                              double out[3]) {
   __shared__ bool is_last;
@@ -43,12 +61,11 @@ __device__ __forceinline__ bool grid_reduce3(double a, double b, double c, doubl
   b = block_sum(b);
   __syncthreads();
   c = block_sum(c);
-  const int nb = num_blocks();
-  const int blk = flat_block();
-  if (thread0()) {
-    partials[blk] = a;
-    partials[nb + blk] = b;
-    partials[2 * nb + blk] = c;
+  const int nb = gridDim.x;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = a;
+    partials[nb + blockIdx.x] = b;
+    partials[2 * nb + blockIdx.x] = c;
     __threadfence();
     const unsigned int t = atomicAdd(ticket, 1u);
     is_last = (t == (unsigned int)(nb - 1));
@@ -56,41 +73,45 @@ __device__ __forceinline__ bool grid_reduce3(double a, double b, double c, doubl
   __syncthreads();
   if (!is_last) return false;
   __threadfence();
-  const int nt = blockDim.x * blockDim.y * blockDim.z;
-  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   for (int m = 0; m < 3; ++m) {
     double s = 0.0;
-    for (int q = tid; q < nb; q += nt) s += ((volatile double*)partials)[m * nb + q];
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) s += ((volatile double*)partials)[m * nb + q];
     s = block_sum(s);
-    if (tid == 0) tot[m] = s;
+    if (threadIdx.x == 0) tot[m] = s;
     __syncthreads();
   }
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     out[0] = tot[0];
     out[1] = tot[1];
     out[2] = tot[2];
     *ticket = 0u;
   }
-  return tid == 0;
+  return threadIdx.x == 0;
+}
+
+__device__ __forceinline__ bool stop_test(const PcgState* st, double rz, double rr) {
+  switch (st->criterion) {
+    case 1: return rz < st->tol * st->tol;                 // the reference's r.z < tol^2
+    case 2: return rr < st->tol * st->tol;                 // absolute 2-norm
+    default: return sqrt(rr) <= st->tol * sqrt(st->bb);    // relative 2-norm
+  }
 }
 
 template <class V>
-__global__ void __launch_bounds__(256) k_pcg_init(Op7<V> A, const V* __restrict__ b, V* __restrict__ x,
-                                                  V* __restrict__ r, V* __restrict__ p, PcgState* st,
-                                                  double* partials) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__global__ void __launch_bounds__(kRedThreads) k_pcg_init(Op7<V> A, const V* b, V* x, V* r, V* __restrict__ p,
+                                                          PcgState* st, double* partials) {
   double rz = 0.0, rr = 0.0, bb = 0.0;
-  if (i < A.L.nx && j < A.L.ny && k < A.L.nz) {
-    const int64_t c = A.L.at(i, j, k);
-    const V rv = b[c] - apply7(A, x, c);
+  Cursor cur;
+  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
+    const int64_t c = A.L.at(cur.i, cur.j, cur.k);
+    const V bv = b[c];
+    const V rv = bv - apply7(A, x, c);
     const V z = rv / A.diag[c];
-    r[c] = rv;
+    r[c] = rv;  // b may alias r: each element is read before it is written
     p[c] = z;
-    rz = (double)rv * (double)z;
-    rr = (double)rv * (double)rv;
-    bb = (double)b[c] * (double)b[c];
+    rz += (double)rv * (double)z;
+    rr += (double)rv * (double)rv;
+    bb += (double)bv * (double)bv;
   }
   double tot[3];
   if (grid_reduce3(rz, rr, bb, partials, &st->ticket, tot)) {
@@ -100,17 +121,16 @@ __global__ void __launch_bounds__(256) k_pcg_init(Op7<V> A, const V* __restrict_
     st->iter = 0;
     st->beta = 0.0;
     st->best_rr = tot[1];
+    st->max_rr = tot[1];
+    st->rz_prev = tot[0];
     st->stall = 0;
     st->status = PCG_RUNNING;
     st->done = 0;
-    const bool nonfinite = !isfinite(tot[0]) || !isfinite(tot[1]);
-    const bool converged = st->criterion == 1 ? (tot[0] < st->tol * st->tol)
-                                              : (sqrt(tot[1]) <= st->tol * sqrt(tot[2]));
-    if (nonfinite) {
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) {
       st->status = PCG_NONFINITE;
       st->done = 1;
-    } else if (tot[2] == 0.0 || tot[1] == 0.0 || (converged && st->criterion == 0)) {
-      // zero right-hand side or an exact initial guess: nothing to do
+    } else if (tot[2] == 0.0 || tot[1] == 0.0 || (st->criterion != 1 && stop_test(st, tot[0], tot[1]))) {
+      // zero right-hand side or an initial guess that already satisfies the test
       st->status = PCG_CONVERGED;
       st->done = 1;
     } else if (st->max_iter <= 0) {
@@ -121,18 +141,16 @@ __global__ void __launch_bounds__(256) k_pcg_init(Op7<V> A, const V* __restrict_
 }
 
 template <class V>
-__global__ void __launch_bounds__(256) k_pcg_spmv(Op7<V> A, const V* __restrict__ p, V* __restrict__ q, PcgState* st,
-                                                  double* partials) {
+__global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(Op7<V> A, const V* __restrict__ p, V* __restrict__ q,
+                                                          PcgState* st, double* partials) {
   if (((volatile PcgState*)st)->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   double pq = 0.0;
-  if (i < A.L.nx && j < A.L.ny && k < A.L.nz) {
-    const int64_t c = A.L.at(i, j, k);
+  Cursor cur;
+  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
+    const int64_t c = A.L.at(cur.i, cur.j, cur.k);
     const V qv = apply7(A, p, c);
     q[c] = qv;
-    pq = (double)p[c] * (double)qv;
+    pq += (double)p[c] * (double)qv;
   }
   pq = block_sum(pq);
   double tot;
@@ -140,9 +158,9 @@ __global__ void __launch_bounds__(256) k_pcg_spmv(Op7<V> A, const V* __restrict_
 }
 
 template <class V>
-__global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x, V* __restrict__ r,
-                                                    const V* __restrict__ p, const V* __restrict__ q, PcgState* st,
-                                                    double* partials) {
+__global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, V* __restrict__ x, V* __restrict__ r,
+                                                            const V* __restrict__ p, const V* __restrict__ q,
+                                                            PcgState* st, double* partials) {
   if (((volatile PcgState*)st)->done) return;
   const double pq_all = ((volatile PcgState*)st)->pq;
   const double alpha = ((volatile PcgState*)st)->rz / pq_all;
@@ -150,17 +168,17 @@ __global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x,
   // its footing in this arithmetic: keep the iterate, stop (uniform branch)
   const bool breakdown = !(pq_all > 0.0) || !isfinite(alpha);
   const V a = (V)alpha;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   double rz = 0.0, rr = 0.0;
-  if (!breakdown && i < A.L.nx && j < A.L.ny && k < A.L.nz) {
-    const int64_t c = A.L.at(i, j, k);
-    x[c] += a * p[c];
-    const V rv = r[c] - a * q[c];
-    r[c] = rv;
-    rz = (double)rv * (double)(rv / A.diag[c]);
-    rr = (double)rv * (double)rv;
+  if (!breakdown) {
+    Cursor cur;
+    for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
+      const int64_t c = A.L.at(cur.i, cur.j, cur.k);
+      x[c] += a * p[c];
+      const V rv = r[c] - a * q[c];
+      r[c] = rv;
+      rz += (double)rv * (double)(rv / A.diag[c]);
+      rr += (double)rv * (double)rv;
+    }
   }
   double tot[3];
   if (grid_reduce3(rz, rr, 0.0, partials, &st->ticket, tot)) {
@@ -171,9 +189,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x,
     }
     const double rz_old = st->rz;
     st->rr = tot[1];
-    const bool nonfinite = !isfinite(tot[0]) || !isfinite(tot[1]);
-    const bool converged = st->criterion == 1 ? (tot[0] < st->tol * st->tol)
-                                              : (sqrt(tot[1]) <= st->tol * sqrt(st->bb));
+    st->rz_prev = rz_old;
     st->rz = tot[0];
     if (tot[1] < 0.99 * st->best_rr) {
       st->best_rr = tot[1];
@@ -181,10 +197,11 @@ __global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x,
     } else {
       st->stall += 1;
     }
-    if (nonfinite) {
+    if (tot[1] > st->max_rr) st->max_rr = tot[1];
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) {
       st->status = PCG_NONFINITE;
       st->done = 1;
-    } else if (converged) {
+    } else if (stop_test(st, tot[0], tot[1])) {
       st->status = PCG_CONVERGED;
       st->done = 1;
     } else {
@@ -196,42 +213,85 @@ __global__ void __launch_bounds__(256) k_pcg_update(Op7<V> A, V* __restrict__ x,
       } else if (st->stall_limit > 0 && st->stall >= st->stall_limit) {
         st->status = PCG_STAGNATED;
         st->done = 1;
+      } else if (st->reliable_delta > 0.0 && tot[1] < st->reliable_delta * st->reliable_delta * st->max_rr) {
+        st->status = PCG_RELIABLE_UPDATE;  // pause before the direction update
+        st->done = 2;
       }
     }
   }
 }
 
 template <class V>
-__global__ void __launch_bounds__(256) k_pcg_pupdate(Op7<V> A, const V* __restrict__ r, V* __restrict__ p,
-                                                     PcgState* st) {
+__global__ void __launch_bounds__(kRedThreads) k_pcg_pupdate(Op7<V> A, const V* __restrict__ r, V* __restrict__ p,
+                                                             PcgState* st) {
   if (((volatile PcgState*)st)->done) return;
   const V beta = (V)((volatile PcgState*)st)->beta;
-  FS_IJK(A.L);
-  const int64_t c = A.L.at(i, j, k);
-  p[c] = p[c] * beta + r[c] / A.diag[c];
+  Cursor cur;
+  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
+    const int64_t c = A.L.at(cur.i, cur.j, cur.k);
+    p[c] = p[c] * beta + r[c] / A.diag[c];
+  }
+}
+
+// After the caller replaced r by the true residual: r.z and r.r of the new
+// residual, beta for the direction update (0 on a restart), and the
+// iteration resumes (done = 0).
+template <class V>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_resume(Op7<V> A, const V* __restrict__ r, PcgState* st,
+                                                            double* partials, int restart) {
+  double rz = 0.0, rr = 0.0;
+  Cursor cur;
+  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
+    const int64_t c = A.L.at(cur.i, cur.j, cur.k);
+    const V rv = r[c];
+    rz += (double)rv * (double)(rv / A.diag[c]);
+    rr += (double)rv * (double)rv;
+  }
+  double tot[3];
+  if (grid_reduce3(rz, rr, 0.0, partials, &st->ticket, tot)) {
+    // the direction update continues from the last accepted step: beta
+    // relates the new r.z to the r.z that step started from
+    st->beta = restart ? 0.0 : tot[0] / st->rz_prev;
+    st->rz = tot[0];
+    st->rr = tot[1];
+    st->max_rr = tot[1];
+    st->best_rr = tot[1];
+    st->stall = 0;
+    st->status = PCG_RUNNING;
+    st->done = 0;
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) {
+      st->status = PCG_NONFINITE;
+      st->done = 1;
+    }
+  }
 }
 
 template <class V>
 void pcg_init(const Op7<V>& A, const V* b, V* x, V* r, V* p, PcgState* st, double* partials, cudaStream_t s) {
-  Launch3 g = kl(A.L);
-  k_pcg_init<V><<<g.grid, g.block, 0, s>>>(A, b, x, r, p, st, partials);
+  k_pcg_init<V><<<pcg_blocks(A.L), kRedThreads, 0, s>>>(A, b, x, r, p, st, partials);
 }
 
 template <class V>
 void pcg_iteration(const Op7<V>& A, V* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
-  Launch3 g = kl(A.L);
-  k_pcg_spmv<V><<<g.grid, g.block, 0, s>>>(A, p, q, st, partials);
-  k_pcg_update<V><<<g.grid, g.block, 0, s>>>(A, x, r, p, q, st, partials);
-  k_pcg_pupdate<V><<<g.grid, g.block, 0, s>>>(A, r, p, st);
+  const int nb = pcg_blocks(A.L);
+  k_pcg_spmv<V><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
+  k_pcg_update<V><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
+  k_pcg_pupdate<V><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
 }
 
-template void pcg_init<float>(const Op7<float>&, const float*, float*, float*, float*, PcgState*, double*,
-                              cudaStream_t);
-template void pcg_init<double>(const Op7<double>&, const double*, double*, double*, double*, PcgState*, double*,
-                               cudaStream_t);
-template void pcg_iteration<float>(const Op7<float>&, float*, float*, float*, float*, PcgState*, double*,
-                                   cudaStream_t);
-template void pcg_iteration<double>(const Op7<double>&, double*, double*, double*, double*, PcgState*, double*,
-                                    cudaStream_t);
+template <class V>
+void pcg_resume(const Op7<V>& A, const V* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s) {
+  const int nb = pcg_blocks(A.L);
+  k_pcg_resume<V><<<nb, kRedThreads, 0, s>>>(A, r, st, partials, restart);
+  k_pcg_pupdate<V><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
+}
+
+#define FS_KINST(V)                                                                                               \
+  template void pcg_init<V>(const Op7<V>&, const V*, V*, V*, V*, PcgState*, double*, cudaStream_t);              \
+  template void pcg_iteration<V>(const Op7<V>&, V*, V*, V*, V*, PcgState*, double*, cudaStream_t);               \
+  template void pcg_resume<V>(const Op7<V>&, const V*, V*, PcgState*, double*, int, cudaStream_t);
+
+FS_KINST(float)
+FS_KINST(double)
 
 }  // namespace fsb

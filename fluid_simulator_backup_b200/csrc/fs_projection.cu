@@ -29,19 +29,18 @@ __global__ void k_divergence_rhs(const T* __restrict__ u, const T* __restrict__ 
                                  Lay Lu, Lay Lv, Lay Lw, double inv_h, double inv_dt, double* __restrict__ b,
                                  double* __restrict__ div_out, double* partials, unsigned int* ticket,
                                  double* scalars) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   double bv = 0.0;
-  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
+  Cursor cur;
+  for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
+    const int i = cur.i, j = cur.j, k = cur.k;
     const double d = (inv_h * ((double)u[Lu.at(i + 1, j, k)] - (double)u[Lu.at(i, j, k)]) +
                       inv_h * ((double)v[Lv.at(i, j + 1, k)] - (double)v[Lv.at(i, j, k)])) +
                      inv_h * ((double)w[Lw.at(i, j, k + 1)] - (double)w[Lw.at(i, j, k)]);
     const double dv = d * inv_dt;
     const int64_t c = Lc.at(i, j, k);
     div_out[c] = dv;
-    bv = -dv;
-    b[c] = bv;
+    b[c] = -dv;
+    bv += -dv;
   }
   bv = block_sum(bv);
   double tot;
@@ -50,16 +49,14 @@ __global__ void k_divergence_rhs(const T* __restrict__ u, const T* __restrict__ 
 
 __global__ void k_subtract_mean(double* __restrict__ b, Lay Lc, const double* mean_src, double inv_n,
                                 double* partials, unsigned int* ticket, double* out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   const double m = inv_n * mean_src[0];
   double bb = 0.0;
-  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
-    const int64_t c = Lc.at(i, j, k);
+  Cursor cur;
+  for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
+    const int64_t c = Lc.at(cur.i, cur.j, cur.k);
     const double v = b[c] - m;
     b[c] = v;
-    bb = v * v;
+    bb += v * v;
   }
   bb = block_sum(bb);
   double tot;
@@ -128,11 +125,10 @@ template <class T>
 __global__ void k_defect_residual(const T* __restrict__ phi, const double* __restrict__ p, const double* __restrict__ b,
                                   double* __restrict__ r64, float* __restrict__ r32, Lay Lc, double rn, double rp,
                                   double inv2, double* partials, unsigned int* ticket, double* rr_out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   double rr = 0.0;
-  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
+  Cursor cur;
+  for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
+    const int i = cur.i, j = cur.j, k = cur.k;
     const int64_t c = Lc.at(i, j, k);
     const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc), xc = p[c];
     double s = 0.0, off = 0.0;
@@ -155,7 +151,7 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
     const double rv = b[c] - ax;
     r64[c] = rv;
     if (r32) r32[c] = (float)rv;
-    rr = rv * rv;
+    rr += rv * rv;
   }
   rr = block_sum(rr);
   double tot;
@@ -221,16 +217,15 @@ template <class T>
 __global__ void k_divergence_norms(const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, Lay Lc,
                                    Lay Lu, Lay Lv, Lay Lw, double inv_h, double* partials, unsigned int* ticket,
                                    double* out2) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   double d2 = 0.0, dm = 0.0;
-  if (i < Lc.nx && j < Lc.ny && k < Lc.nz) {
+  Cursor cur;
+  for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
+    const int i = cur.i, j = cur.j, k = cur.k;
     const double d = (inv_h * ((double)u[Lu.at(i + 1, j, k)] - (double)u[Lu.at(i, j, k)]) +
                       inv_h * ((double)v[Lv.at(i, j + 1, k)] - (double)v[Lv.at(i, j, k)])) +
                      inv_h * ((double)w[Lw.at(i, j, k + 1)] - (double)w[Lw.at(i, j, k)]);
-    d2 = d * d;
-    dm = fabs(d);
+    d2 += d * d;
+    dm = fmax(dm, fabs(d));
   }
   const double bm = block_max(dm);
   __syncthreads();
@@ -242,11 +237,9 @@ __global__ void k_divergence_norms(const T* __restrict__ u, const T* __restrict_
 
 template <class T>
 __global__ void k_absmax(const T* __restrict__ f, Lay L, double* out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   double m = 0.0;
-  if (i < L.nx && j < L.ny && k < L.nz) m = fabs((double)f[L.at(i, j, k)]);
+  Cursor cur;
+  for (cur.init(L); cur.valid(L); cur.next(L)) m = fmax(m, fabs((double)f[L.at(cur.i, cur.j, cur.k)]));
   m = block_max(m);
   if (thread0()) atomicMax((unsigned long long*)out, (unsigned long long)__double_as_longlong(m));
 }
@@ -277,16 +270,14 @@ template <class T>
 void divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
                     double dx, double dt, double* b, double* div_out, double* partials, unsigned int* ticket,
                     double* scalars, cudaStream_t s) {
-  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
-  k_divergence_rhs<T><<<g.grid, g.block, 0, s>>>(u, v, w, Lc, Lu, Lv, Lw, 1.0 / dx, 1.0 / dt, b, div_out, partials,
+  k_divergence_rhs<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(u, v, w, Lc, Lu, Lv, Lw, 1.0 / dx, 1.0 / dt, b, div_out, partials,
                                                   ticket, scalars);
 }
 
 void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* partials, unsigned int* ticket,
                    double* scalars_out, cudaStream_t s) {
-  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
   const double inv_n = 1.0 / ((double)Lc.nx * Lc.ny * Lc.nz);
-  k_subtract_mean<<<g.grid, g.block, 0, s>>>(b, Lc, scalars, inv_n, partials, ticket, scalars_out);
+  k_subtract_mean<<<pcg_blocks(Lc), kRedThreads, 0, s>>>(b, Lc, scalars, inv_n, partials, ticket, scalars_out);
 }
 
 template <class T, class V>
@@ -302,8 +293,7 @@ template <class T>
 void defect_residual(const T* phi, const double* p64, const double* b, double* r64, float* r32, const Lay& Lc, double dx,
                      double rho_neg, double rho_pos, double* partials, unsigned int* ticket, double* rr_out,
                      cudaStream_t s) {
-  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
-  k_defect_residual<T><<<g.grid, g.block, 0, s>>>(phi, p64, b, r64, r32, Lc, rho_neg, rho_pos, 1.0 / (dx * dx),
+  k_defect_residual<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, p64, b, r64, r32, Lc, rho_neg, rho_pos, 1.0 / (dx * dx),
                                                    partials, ticket, rr_out);
 }
 
@@ -325,20 +315,16 @@ template <class T>
 void divergence_norms(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
                       double dx, double* partials, unsigned int* ticket, double* out2, cudaStream_t s) {
   cudaMemsetAsync(out2 + 1, 0, sizeof(double), s);
-  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
-  k_divergence_norms<T><<<g.grid, g.block, 0, s>>>(u, v, w, Lc, Lu, Lv, Lw, 1.0 / dx, partials, ticket, out2);
+  k_divergence_norms<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(u, v, w, Lc, Lu, Lv, Lw, 1.0 / dx, partials, ticket, out2);
 }
 
 template <class T>
 void absmax3(const T* u, const T* v, const T* w, const Lay& Lu, const Lay& Lv, const Lay& Lw, double* out3,
              cudaStream_t s) {
   cudaMemsetAsync(out3, 0, 3 * sizeof(double), s);
-  Launch3 g = launch3(Lu.nx, Lu.ny, Lu.nz);
-  k_absmax<T><<<g.grid, g.block, 0, s>>>(u, Lu, out3);
-  g = launch3(Lv.nx, Lv.ny, Lv.nz);
-  k_absmax<T><<<g.grid, g.block, 0, s>>>(v, Lv, out3 + 1);
-  g = launch3(Lw.nx, Lw.ny, Lw.nz);
-  k_absmax<T><<<g.grid, g.block, 0, s>>>(w, Lw, out3 + 2);
+  k_absmax<T><<<pcg_blocks(Lu), kRedThreads, 0, s>>>(u, Lu, out3);
+  k_absmax<T><<<pcg_blocks(Lv), kRedThreads, 0, s>>>(v, Lv, out3 + 1);
+  k_absmax<T><<<pcg_blocks(Lw), kRedThreads, 0, s>>>(w, Lw, out3 + 2);
 }
 
 template <class S, class D>
