@@ -44,9 +44,9 @@ void set_error(const char* fmt, ...) {
     }                                                                                     \
   } while (0)
 
-#define CKS(expr)                  \
+#define CKS(...)                   \
   do {                             \
-    fs_status s_ = (expr);         \
+    fs_status s_ = (__VA_ARGS__);  \
     if (s_ != FS_OK) return s_;    \
   } while (0)
 
@@ -176,13 +176,13 @@ fs_status check_params(const fs_params* p) {
 
 // Launch captured batches of kGraphIters iterations until the solver state
 // says stop (done != 0); one host check of the state per batch.
-template <class V>
-fs_status drive_pcg(fs_ctx* c, int key, const Op7<V>& A, V* x, V* r, V* p, V* q, int max_iter, bool timed) {
+template <class V, class RV = V>
+fs_status drive_pcg(fs_ctx* c, int key, const Op7<V>& A, V* x, RV* r, V* p, V* q, int max_iter, bool timed) {
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    for (int n = 0; n < kGraphIters; ++n) pcg_iteration<V>(A, x, r, p, q, c->st, c->partials, c->stream);
+    for (int n = 0; n < kGraphIters; ++n) pcg_iteration<V, RV>(A, x, r, p, q, c->st, c->partials, c->stream);
     CK(cudaStreamEndCapture(c->stream, &g));
     cudaGraphExec_t ge;
     CK(cudaGraphInstantiate(&ge, g, 0));
@@ -221,7 +221,7 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   pcg_init<V>(A, b, x, r, p, c->st, c->partials, c->stream);
   c->launches += 1;
   CK(cudaGetLastError());
-  CKS(drive_pcg<V>(c, key, A, x, r, p, q, max_iter, timed));
+  CKS(drive_pcg<V, V>(c, key, A, x, r, p, q, max_iter, timed));
   if (timed) {
     CK(cudaEventRecord(c->evp1, c->stream));
     CK(cudaEventSynchronize(c->evp1));
@@ -402,7 +402,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     // true FP64 residual of the current pressure (b - A64 p64, A64 from phi
     // in FP64); its FP32 image lands in the Krylov residual buffer
     auto defect = [&]() -> fs_status {
-      defect_residual<S>(phi, c->p64, c->b64, c->r64, (float*)c->pr, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
+      defect_residual<S>(phi, c->p64, c->b64, c->r64, nullptr, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
                          c->tickets + 2, c->scalars + 2, s);
       c->launches += 1;
       CK(cudaGetLastError());
@@ -430,12 +430,15 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       *c->st_host = init;
       CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
       CK(cudaEventRecord(c->evp0, s));
-      pcg_init<float>(A, (float*)c->pr, (float*)c->px, (float*)c->pr, (float*)c->pp, c->st, c->partials, s);
+      // the FP64 true residual is the Krylov residual: r stays FP64, the
+      // operator, p, q and the partial solution x are FP32
+      pcg_init<float, double>(A, c->r64, (float*)c->px, c->r64, (float*)c->pp, c->st, c->partials, s);
       c->launches += 1;
       int restarts = 0;
+      double last_rel = rel;
       for (;;) {
-        CKS(drive_pcg<float>(c, 2, A, (float*)c->px, (float*)c->pr, (float*)c->pp, (float*)c->pq, P.max_iteration,
-                             true));
+        CKS(drive_pcg<float, double>(c, 2, A, (float*)c->px, c->r64, (float*)c->pp, (float*)c->pq, P.max_iteration,
+                                     true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
         if (status == PCG_NONFINITE) {
@@ -452,9 +455,12 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
                        iters, status, rel);
         if (rel <= P.tolerance) { st = PCG_CONVERGED; break; }
         if (iters >= P.max_iteration) { st = PCG_MAXITER; break; }
-        const bool restart = status == PCG_STAGNATED;
-        if (restart && ++restarts > 5) { st = PCG_MAXITER; break; }
-        pcg_resume<float>(A, (float*)c->pr, (float*)c->pp, c->st, c->partials, restart ? 1 : 0, s);
+        // a breakdown, or a true residual that grew since the last one,
+        // restarts the direction from the preconditioned residual
+        const bool restart = status == PCG_STAGNATED || rel > last_rel;
+        last_rel = std::min(last_rel, rel);
+        if (restart && ++restarts > 8) { st = PCG_MAXITER; break; }
+        pcg_resume<float, double>(A, c->r64, (float*)c->pp, c->st, c->partials, restart ? 1 : 0, s);
         c->launches += 2;
         CK(cudaGetLastError());
       }

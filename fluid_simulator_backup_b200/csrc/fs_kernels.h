@@ -54,12 +54,12 @@ template <class V> struct Op7 {
   Lay L;
 };
 
-template <class V>
-void pcg_init(const Op7<V>& A, const V* b, V* x, V* r, V* p, PcgState* st, double* partials, cudaStream_t s);
-template <class V>
-void pcg_iteration(const Op7<V>& A, V* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
-template <class V>
-void pcg_resume(const Op7<V>& A, const V* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);
+template <class V, class R = V>
+void pcg_init(const Op7<V>& A, const R* b, V* x, R* r, V* p, PcgState* st, double* partials, cudaStream_t s);
+template <class V, class R = V>
+void pcg_iteration(const Op7<V>& A, V* x, R* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+template <class V, class R = V>
+void pcg_resume(const Op7<V>& A, const R* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);
 int pcg_blocks(const Lay& L);
 
 // ---- projection family (fs_projection.cu)

@@ -2,6 +2,13 @@
 // operator (PCG_METHOD.cpp:4-126 restated for the GPU), with optional
 // reliable updates for the mixed-precision pressure solve.
 //
+// Vector types: V for the operator, the search direction p, q = A p and the
+// iterate x; R for the residual r and right-hand side b.  V = R = double is
+// the FP64 path, V = R = float the viscosity solves in FP32 storage, and
+// V = float, R = double the mixed-precision pressure solve: the residual
+// recurrence r -= alpha q and all scalars stay in FP64 while every
+// operator application streams FP32.
+//
 // One iteration is three kernels:
 //   spmv    q = A p and p.q                      (reads p, ax, ay, az, diag; writes q)
 //   update  x += alpha p, r -= alpha q, r.z, r.r (reads x, p, r, q, diag; writes x, r)
@@ -97,18 +104,18 @@ __device__ __forceinline__ bool stop_test(const PcgState* st, double rz, double 
   }
 }
 
-template <class V>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_init(Op7<V> A, const V* b, V* x, V* r, V* __restrict__ p,
+template <class V, class RT>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_init(Op7<V> A, const RT* b, V* x, RT* r, V* __restrict__ p,
                                                           PcgState* st, double* partials) {
   double rz = 0.0, rr = 0.0, bb = 0.0;
   Cursor cur;
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-    const V bv = b[c];
-    const V rv = bv - apply7(A, x, c);
-    const V z = rv / A.diag[c];
+    const RT bv = b[c];
+    const RT rv = bv - (RT)apply7(A, x, c);
+    const RT z = rv / (RT)A.diag[c];
     r[c] = rv;  // b may alias r: each element is read before it is written
-    p[c] = z;
+    p[c] = (V)z;
     rz += (double)rv * (double)z;
     rr += (double)rv * (double)rv;
     bb += (double)bv * (double)bv;
@@ -157,8 +164,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(Op7<V> A, const V* __r
   if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) st->pq = tot;
 }
 
-template <class V>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, V* __restrict__ x, V* __restrict__ r,
+template <class V, class RT>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, V* __restrict__ x, RT* __restrict__ r,
                                                             const V* __restrict__ p, const V* __restrict__ q,
                                                             PcgState* st, double* partials) {
   if (((volatile PcgState*)st)->done) return;
@@ -168,15 +175,16 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, V* __restr
   // its footing in this arithmetic: keep the iterate, stop (uniform branch)
   const bool breakdown = !(pq_all > 0.0) || !isfinite(alpha);
   const V a = (V)alpha;
+  const RT ar = (RT)alpha;
   double rz = 0.0, rr = 0.0;
   if (!breakdown) {
     Cursor cur;
     for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
       const int64_t c = A.L.at(cur.i, cur.j, cur.k);
       x[c] += a * p[c];
-      const V rv = r[c] - a * q[c];
+      const RT rv = r[c] - ar * (RT)q[c];
       r[c] = rv;
-      rz += (double)rv * (double)(rv / A.diag[c]);
+      rz += (double)rv * (double)(rv / (RT)A.diag[c]);
       rr += (double)rv * (double)rv;
     }
   }
@@ -221,30 +229,30 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, V* __restr
   }
 }
 
-template <class V>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_pupdate(Op7<V> A, const V* __restrict__ r, V* __restrict__ p,
+template <class V, class RT>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_pupdate(Op7<V> A, const RT* __restrict__ r, V* __restrict__ p,
                                                              PcgState* st) {
   if (((volatile PcgState*)st)->done) return;
-  const V beta = (V)((volatile PcgState*)st)->beta;
+  const RT beta = (RT)((volatile PcgState*)st)->beta;
   Cursor cur;
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-    p[c] = p[c] * beta + r[c] / A.diag[c];
+    p[c] = (V)((RT)p[c] * beta + r[c] / (RT)A.diag[c]);
   }
 }
 
 // After the caller replaced r by the true residual: r.z and r.r of the new
 // residual, beta for the direction update (0 on a restart), and the
 // iteration resumes (done = 0).
-template <class V>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_resume(Op7<V> A, const V* __restrict__ r, PcgState* st,
+template <class V, class RT>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_resume(Op7<V> A, const RT* __restrict__ r, PcgState* st,
                                                             double* partials, int restart) {
   double rz = 0.0, rr = 0.0;
   Cursor cur;
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-    const V rv = r[c];
-    rz += (double)rv * (double)(rv / A.diag[c]);
+    const RT rv = r[c];
+    rz += (double)rv * (double)(rv / (RT)A.diag[c]);
     rr += (double)rv * (double)rv;
   }
   double tot[3];
@@ -266,32 +274,33 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_resume(Op7<V> A, const V* _
   }
 }
 
-template <class V>
-void pcg_init(const Op7<V>& A, const V* b, V* x, V* r, V* p, PcgState* st, double* partials, cudaStream_t s) {
-  k_pcg_init<V><<<pcg_blocks(A.L), kRedThreads, 0, s>>>(A, b, x, r, p, st, partials);
+template <class V, class RT>
+void pcg_init(const Op7<V>& A, const RT* b, V* x, RT* r, V* p, PcgState* st, double* partials, cudaStream_t s) {
+  k_pcg_init<V, RT><<<pcg_blocks(A.L), kRedThreads, 0, s>>>(A, b, x, r, p, st, partials);
 }
 
-template <class V>
-void pcg_iteration(const Op7<V>& A, V* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
+template <class V, class RT>
+void pcg_iteration(const Op7<V>& A, V* x, RT* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
   const int nb = pcg_blocks(A.L);
   k_pcg_spmv<V><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
-  k_pcg_update<V><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
-  k_pcg_pupdate<V><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
+  k_pcg_update<V, RT><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
+  k_pcg_pupdate<V, RT><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
 }
 
-template <class V>
-void pcg_resume(const Op7<V>& A, const V* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s) {
+template <class V, class RT>
+void pcg_resume(const Op7<V>& A, const RT* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s) {
   const int nb = pcg_blocks(A.L);
-  k_pcg_resume<V><<<nb, kRedThreads, 0, s>>>(A, r, st, partials, restart);
-  k_pcg_pupdate<V><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
+  k_pcg_resume<V, RT><<<nb, kRedThreads, 0, s>>>(A, r, st, partials, restart);
+  k_pcg_pupdate<V, RT><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
 }
 
-#define FS_KINST(V)                                                                                               \
-  template void pcg_init<V>(const Op7<V>&, const V*, V*, V*, V*, PcgState*, double*, cudaStream_t);              \
-  template void pcg_iteration<V>(const Op7<V>&, V*, V*, V*, V*, PcgState*, double*, cudaStream_t);               \
-  template void pcg_resume<V>(const Op7<V>&, const V*, V*, PcgState*, double*, int, cudaStream_t);
+#define FS_KINST(V, RT)                                                                                           \
+  template void pcg_init<V, RT>(const Op7<V>&, const RT*, V*, RT*, V*, PcgState*, double*, cudaStream_t);        \
+  template void pcg_iteration<V, RT>(const Op7<V>&, V*, RT*, V*, V*, PcgState*, double*, cudaStream_t);         \
+  template void pcg_resume<V, RT>(const Op7<V>&, const RT*, V*, PcgState*, double*, int, cudaStream_t);
 
-FS_KINST(float)
-FS_KINST(double)
+FS_KINST(float, float)
+FS_KINST(double, double)
+FS_KINST(float, double)
 
 }  // namespace fsb
