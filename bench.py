@@ -47,7 +47,7 @@ def scene(n):
 def params(fs, precision):
     return fs.default_params(rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0),
                              precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=20000,
-                             inner_tolerance=1e-5, max_outer=30, viscosity=1, viscosity_tolerance=1e-8, cfl=0.5,
+                             inner_tolerance=1e-3, max_outer=30, viscosity=1, viscosity_tolerance=1e-8, cfl=0.5,
                              order=3, reinit_iterations=10, reinit_scaling=5, weno_epsilon=1e-6)
 
 

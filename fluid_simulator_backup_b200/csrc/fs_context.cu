@@ -399,10 +399,10 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc};
     const size_t vbytes = c->Lc.total * sizeof(float);
     double bb = 0.0;
-    // true FP64 residual of the current pressure (b - A64 p64, A64 from phi
-    // in FP64); its FP32 image lands in the Krylov residual buffer
-    auto defect = [&]() -> fs_status {
-      defect_residual<S>(phi, c->p64, c->b64, c->r64, nullptr, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
+    // true FP64 residual b - A64 (p64 [+ x32]) with A64 evaluated from phi in
+    // FP64; it lands in r64, the Krylov residual of the mixed solve
+    auto defect = [&](const float* x32, double* rel_out) -> fs_status {
+      defect_residual<S>(phi, c->p64, x32, c->b64, c->r64, nullptr, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
                          c->tickets + 2, c->scalars + 2, s);
       c->launches += 1;
       CK(cudaGetLastError());
@@ -410,56 +410,62 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       CK(cudaStreamSynchronize(s));
       bb = c->sc_host[1];
       const double rr = c->sc_host[2];
-      rel = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+      *rel_out = bb > 0 ? std::sqrt(rr / bb) : 0.0;
       outer += 1;
-      if (!std::isfinite(rel)) {
+      if (!std::isfinite(*rel_out) && !x32) {
         set_error("non-finite defect residual");
         return FS_NONFINITE;
       }
       return FS_OK;
     };
-    CKS(defect());
+    CKS(defect(nullptr, &rel));
     st = PCG_CONVERGED;
     if (rel > P.tolerance) {
+      // Restarted mixed-precision CG: each Krylov sequence runs in FP32
+      // (operator, p, q, partial solution x32) with an FP64 residual
+      // recurrence and reliable updates every decade; a sequence is trusted
+      // for a reduction of inner_tolerance (the reach of FP32 arithmetic on
+      // this operator), then restarted from the true residual.  A candidate
+      // p64 + x32 is folded only if its true FP64 residual improved.
       CK(cudaMemsetAsync(c->px, 0, vbytes, s));
       PcgState init{};
-      init.criterion = 2;  // absolute 2-norm of the FP32 residual, in b's units
+      init.criterion = 2;  // absolute 2-norm of the recursive residual, in b's units
       init.tol = 0.5 * P.tolerance * std::sqrt(bb);
       init.max_iter = P.max_iteration;
       init.reliable_delta = 0.1;
       *c->st_host = init;
       CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
       CK(cudaEventRecord(c->evp0, s));
-      // the FP64 true residual is the Krylov residual: r stays FP64, the
-      // operator, p, q and the partial solution x are FP32
       pcg_init<float, double>(A, c->r64, (float*)c->px, c->r64, (float*)c->pp, c->st, c->partials, s);
       c->launches += 1;
-      int restarts = 0;
-      double last_rel = rel;
+      int failures = 0;
+      double best = rel, seq_start = rel;
       for (;;) {
         CKS(drive_pcg<float, double>(c, 2, A, (float*)c->px, c->r64, (float*)c->pp, (float*)c->pq, P.max_iteration,
                                      true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
-        if (status == PCG_NONFINITE) {
-          set_error("non-finite residual in the FP32 pressure iteration (iteration %d)", iters);
-          return FS_NONFINITE;
+        double cand = 0.0;
+        CKS(defect((float*)c->px, &cand));  // r64 <- residual of p64 + x32
+        bool restart;
+        if (std::isfinite(cand) && cand < best) {
+          add_correction(c->p64, (float*)c->px, c->Lc, s);
+          c->launches += 1;
+          best = rel = cand;
+          restart = status == PCG_STAGNATED || cand <= seq_start * P.inner_tolerance;
+        } else {
+          // the sequence lost its way in FP32: drop it, restore r64
+          CKS(defect(nullptr, &rel));
+          restart = true;
+          ++failures;
         }
-        // fold the FP32 correction into the FP64 pressure and take the true residual
-        add_correction(c->p64, (float*)c->px, c->Lc, s);
-        c->launches += 1;
         CK(cudaMemsetAsync(c->px, 0, vbytes, s));
-        CKS(defect());
         if (c->debug)
-          std::fprintf(stderr, "[fs] reliable update %d: iteration %d, status %d, true residual %.3e\n", outer - 1,
-                       iters, status, rel);
-        if (rel <= P.tolerance) { st = PCG_CONVERGED; break; }
-        if (iters >= P.max_iteration) { st = PCG_MAXITER; break; }
-        // a breakdown, or a true residual that grew since the last one,
-        // restarts the direction from the preconditioned residual
-        const bool restart = status == PCG_STAGNATED || rel > last_rel;
-        last_rel = std::min(last_rel, rel);
-        if (restart && ++restarts > 8) { st = PCG_MAXITER; break; }
+          std::fprintf(stderr, "[fs] mixed solve: iteration %d, status %d, candidate %.3e, best %.3e%s\n", iters,
+                       status, cand, best, restart ? ", restart" : "");
+        if (best <= P.tolerance) { st = PCG_CONVERGED; break; }
+        if (iters >= P.max_iteration || failures > 8) { st = PCG_MAXITER; break; }
+        if (restart) seq_start = best;
         pcg_resume<float, double>(A, c->r64, (float*)c->pp, c->st, c->partials, restart ? 1 : 0, s);
         c->launches += 2;
         CK(cudaGetLastError());
@@ -614,7 +620,7 @@ void fs_params_default(fs_params* p) {
   p->stop = FS_STOP_RELATIVE;
   p->tolerance = 1e-6;
   p->max_iteration = 20000;
-  p->inner_tolerance = 1e-5;
+  p->inner_tolerance = 1e-3;
   p->max_outer = 20;
   p->viscosity = 1;
   p->viscosity_tolerance = 1e-8;

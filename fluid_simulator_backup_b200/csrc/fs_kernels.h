@@ -77,9 +77,9 @@ template <class T, class V>
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
                              V* diag, cudaStream_t s);
 template <class T>
-void defect_residual(const T* phi, const double* p64, const double* b, double* r64, float* r32, const Lay& Lc, double dx,
-                     double rho_neg, double rho_pos, double* partials, unsigned int* ticket, double* rr_out,
-                     cudaStream_t s);
+void defect_residual(const T* phi, const double* p64, const float* x32, const double* b, double* r64, float* r32,
+                     const Lay& Lc, double dx, double rho_neg, double rho_pos, double* partials, unsigned int* ticket,
+                     double* rr_out, cudaStream_t s);
 void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s);
 template <class T>
 void velocity_correct(T* f, const T* base, const double* p, const T* phi, const Lay& Lf, const Lay& Lc, int axis,

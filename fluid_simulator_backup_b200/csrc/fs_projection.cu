@@ -121,16 +121,20 @@ __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, do
 
 // r64 = b - A p64 with A from phi in FP64 (same formulas as the two kernels
 // above); also r32 = (float) r64 and ||r64||^2.
+// With x32 != nullptr the residual is that of the candidate pressure
+// p64 + x32 (the mixed-precision solve's uncommitted correction).
 template <class T>
-__global__ void k_defect_residual(const T* __restrict__ phi, const double* __restrict__ p, const double* __restrict__ b,
-                                  double* __restrict__ r64, float* __restrict__ r32, Lay Lc, double rn, double rp,
-                                  double inv2, double* partials, unsigned int* ticket, double* rr_out) {
+__global__ void k_defect_residual(const T* __restrict__ phi, const double* __restrict__ p, const float* __restrict__ x32,
+                                  const double* __restrict__ b, double* __restrict__ r64, float* __restrict__ r32,
+                                  Lay Lc, double rn, double rp, double inv2, double* partials, unsigned int* ticket,
+                                  double* rr_out) {
   double rr = 0.0;
   Cursor cur;
   for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
     const int i = cur.i, j = cur.j, k = cur.k;
     const int64_t c = Lc.at(i, j, k);
-    const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc), xc = p[c];
+    const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
+    const double xc = x32 ? p[c] + (double)x32[c] : p[c];
     double s = 0.0, off = 0.0;
     const int64_t nb[6] = {c - 1, c + 1, c - Lc.px, c + Lc.px, c - Lc.slab, c + Lc.slab};
     const bool ok[6] = {i > 0, i < Lc.nx - 1, j > 0, j < Lc.ny - 1, k > 0, k < Lc.nz - 1};
@@ -139,7 +143,7 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
       if (!ok[q]) continue;
       const double beta = face_beta(vc, inv_rho(phi[nb[q]], rn, rp), acv, fabs((double)phi[nb[q]]));
       s += beta;
-      off += beta * p[nb[q]];
+      off += beta * (x32 ? p[nb[q]] + (double)x32[nb[q]] : p[nb[q]]);
     }
     if (i == 0 && j == 0 && k == 0) {
       const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
@@ -290,11 +294,11 @@ void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_
 }
 
 template <class T>
-void defect_residual(const T* phi, const double* p64, const double* b, double* r64, float* r32, const Lay& Lc, double dx,
-                     double rho_neg, double rho_pos, double* partials, unsigned int* ticket, double* rr_out,
-                     cudaStream_t s) {
-  k_defect_residual<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, p64, b, r64, r32, Lc, rho_neg, rho_pos, 1.0 / (dx * dx),
-                                                   partials, ticket, rr_out);
+void defect_residual(const T* phi, const double* p64, const float* x32, const double* b, double* r64, float* r32,
+                     const Lay& Lc, double dx, double rho_neg, double rho_pos, double* partials, unsigned int* ticket,
+                     double* rr_out, cudaStream_t s) {
+  k_defect_residual<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, p64, x32, b, r64, r32, Lc, rho_neg, rho_pos,
+                                                              1.0 / (dx * dx), partials, ticket, rr_out);
 }
 
 void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s) {
@@ -348,8 +352,9 @@ void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s)
 #define FS_PINST(T)                                                                                                  \
   template void divergence_rhs<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,     \
                                   double, double, double*, double*, double*, unsigned int*, double*, cudaStream_t); \
-  template void defect_residual<T>(const T*, const double*, const double*, double*, float*, const Lay&, double,     \
-                                   double, double, double*, unsigned int*, double*, cudaStream_t);                  \
+  template void defect_residual<T>(const T*, const double*, const float*, const double*, double*, float*,         \
+                                   const Lay&, double, double, double, double*, unsigned int*, double*,             \
+                                   cudaStream_t);                                                                   \
   template void velocity_correct<T>(T*, const T*, const double*, const T*, const Lay&, const Lay&, int, double,     \
                                     double, double, double, int, double, double, cudaStream_t);                     \
   template void divergence_norms<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,   \

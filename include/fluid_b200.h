@@ -82,9 +82,9 @@ typedef struct {
   int stop;                         /* fs_stop for the pressure solve */
   double tolerance;                 /* pressure tolerance (relative divergence in FP32_REFINE) */
   int max_iteration;                /* PCG iteration cap per solve (inner cap in FP32_REFINE) */
-  double inner_tolerance;           /* FP32_REFINE: smallest relative reduction asked of one inner FP32
-                                       solve; each inner solve targets 0.3*tolerance/current residual */
-  int max_outer;                    /* FP32_REFINE: defect-correction cap */
+  double inner_tolerance;           /* FP32_REFINE: residual reduction one FP32 Krylov sequence is trusted
+                                       for before it restarts from the FP64 residual (default 1e-3) */
+  int max_outer;                    /* FP32_REFINE: unused (kept for layout); the iteration cap applies */
   int viscosity;                    /* 0: off, 1: semi-implicit */
   double viscosity_tolerance;       /* relative residual of each viscosity solve */
   int viscosity_max_iteration;
