@@ -388,15 +388,15 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
   double rel = 0.0;
   if (!c->fp32) {
     build_pressure_operator<S, double>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (double*)c->pax, (double*)c->pay,
-                                       (double*)c->paz, (double*)c->pdiag, s);
-    Op7<double> A{(double*)c->pax, (double*)c->pay, (double*)c->paz, (double*)c->pdiag, c->Lc};
+                                       (double*)c->paz, (double*)c->pdiag, c->scalars + 12, s);
+    Op7<double> A{(double*)c->pax, (double*)c->pay, (double*)c->paz, (double*)c->pdiag, c->Lc, 1, c->scalars + 12};
     CKS(run_pcg<double>(c, 1, A, c->b64, c->p64, (double*)c->pr, (double*)c->pp, (double*)c->pq, P.tolerance,
                         P.max_iteration, P.stop, &iters, &rel, &st));
     outer = 1;
   } else {
     build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
-                                      (float*)c->paz, (float*)c->pdiag, s);
-    Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc};
+                                      (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s);
+    Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
     const size_t vbytes = c->Lc.total * sizeof(float);
     double bb = 0.0;
     // true FP64 residual b - A64 (p64 [+ x32]) with A64 evaluated from phi in

@@ -46,12 +46,21 @@ enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_MAXITER = 2, PCG_NONFINITE = 3, P
 // (A x)_c = diag_c x_c - sum_d (a_d[c] x_{c-e_d} + a_d[c+e_d] x_{c+e_d});
 // a_d[c] couples c-e_d and c.  Couplings across walls are zero, so ghost
 // values of x never contribute.
+// flux_form != 0 applies the operator as a sum of face fluxes,
+// (A x)_c = sum_faces a_f (x_c - x_nb) + extra0 x_c (extra0 only at the first
+// cell, the deflation term), which avoids the catastrophic cancellation of
+// diag*x_c - sum a x_nb for smooth x: in FP32 the relative error of A x then
+// grows like eps*n instead of eps*cond(A).  The diagonal is still used for
+// the Jacobi preconditioner.  flux_form requires diag = sum of the face
+// couplings everywhere except the first cell (true for the pressure matrix).
 template <class V> struct Op7 {
   const V* ax;
   const V* ay;
   const V* az;
   const V* diag;
   Lay L;
+  int flux_form = 0;
+  const double* extra0 = nullptr;  // device scalar: diag - sum of couplings at cell (0,0,0)
 };
 
 template <class V, class R = V>
@@ -75,7 +84,7 @@ void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* part
                    double* scalars_out, cudaStream_t s);
 template <class T, class V>
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
-                             V* diag, cudaStream_t s);
+                             V* diag, double* extra0, cudaStream_t s);
 template <class T>
 void defect_residual(const T* phi, const double* p64, const float* x32, const double* b, double* r64, float* r32,
                      const Lay& Lc, double dx, double rho_neg, double rho_pos, double* partials, unsigned int* ticket,

@@ -51,7 +51,15 @@ int pcg_blocks(const Lay& L) { return reduction_blocks((int64_t)L.nx * L.ny * L.
 template <class V>
 __device__ __forceinline__ V apply7(const Op7<V>& A, const V* __restrict__ x, int64_t c) {
   const int64_t sy = A.L.px, sz = A.L.slab;
-  V acc = A.diag[c] * x[c];
+  const V xc = x[c];
+  if (A.flux_form) {
+    V acc = A.ax[c] * (xc - x[c - 1]) + A.ax[c + 1] * (xc - x[c + 1]);
+    acc += A.ay[c] * (xc - x[c - sy]) + A.ay[c + sy] * (xc - x[c + sy]);
+    acc += A.az[c] * (xc - x[c - sz]) + A.az[c + sz] * (xc - x[c + sz]);
+    if (c == A.L.at(0, 0, 0)) acc += (V)(*A.extra0) * xc;
+    return acc;
+  }
+  V acc = A.diag[c] * xc;
   acc -= A.ax[c] * x[c - 1] + A.ax[c + 1] * x[c + 1];
   acc -= A.ay[c] * x[c - sy] + A.ay[c + sy] * x[c + sy];
   acc -= A.az[c] * x[c - sz] + A.az[c + sz] * x[c + sz];

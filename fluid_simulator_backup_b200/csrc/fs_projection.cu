@@ -97,7 +97,7 @@ __global__ void k_pressure_faces(const T* __restrict__ phi, Lay Lc, double rn, d
 
 template <class T, class V>
 __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, double rp, double inv2,
-                                V* __restrict__ diag) {
+                                V* __restrict__ diag, double* __restrict__ extra0) {
   FS_IJK(Lc);
   const int64_t c = Lc.at(i, j, k);
   const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
@@ -113,7 +113,9 @@ __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, do
     // the linear extrapolation 2 phi0 - phi1 along the axis
     const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
     const double gd = fabs(2.0 * pc - (double)phi[c + Lc.slab]);
-    s = (s + vc * vc * (gb + acv) / (vc * gb + vc * acv)) + vc * vc * (gd + acv) / (vc * gd + vc * acv);
+    const double e_b = vc * vc * (gb + acv) / (vc * gb + vc * acv), e_d = vc * vc * (gd + acv) / (vc * gd + vc * acv);
+    s = (s + e_b) + e_d;
+    if (extra0) *extra0 = inv2 * (e_b + e_d);
   }
   if (s == 0.0) s = 1.0;
   diag[c] = (V)(inv2 * s);
@@ -151,7 +153,22 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
       s = (s + vc * vc * (gb + acv) / (vc * gb + vc * acv)) + vc * vc * (gd + acv) / (vc * gd + vc * acv);
     }
     if (s == 0.0) s = 1.0;
-    const double ax = inv2 * s * xc - inv2 * off;
+    (void)off;
+    // flux form (no cancellation): sum beta (x_c - x_nb) + deflation term
+    double flux = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      if (!ok[q]) continue;
+      const double beta = face_beta(vc, inv_rho(phi[nb[q]], rn, rp), acv, fabs((double)phi[nb[q]]));
+      const double xn = x32 ? p[nb[q]] + (double)x32[nb[q]] : p[nb[q]];
+      flux += beta * (xc - xn);
+    }
+    double sum_faces = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      if (ok[q]) sum_faces += face_beta(vc, inv_rho(phi[nb[q]], rn, rp), acv, fabs((double)phi[nb[q]]));
+    const double extra = (i == 0 && j == 0 && k == 0) ? s - sum_faces : 0.0;
+    const double ax = inv2 * (flux + extra * xc);
     const double rv = b[c] - ax;
     r64[c] = rv;
     if (r32) r32[c] = (float)rv;
@@ -286,11 +303,11 @@ void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* part
 
 template <class T, class V>
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
-                             V* diag, cudaStream_t s) {
+                             V* diag, double* extra0, cudaStream_t s) {
   Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
   const double inv2 = 1.0 / (dx * dx);
   k_pressure_faces<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, ax, ay, az);
-  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag);
+  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag, extra0);
 }
 
 template <class T>
@@ -366,14 +383,13 @@ void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s)
 FS_PINST(float)
 FS_PINST(double)
 
-template void build_pressure_operator<float, float>(const float*, const Lay&, double, double, double, float*, float*,
-                                                    float*, float*, cudaStream_t);
-template void build_pressure_operator<double, double>(const double*, const Lay&, double, double, double, double*,
-                                                      double*, double*, double*, cudaStream_t);
-template void build_pressure_operator<double, float>(const double*, const Lay&, double, double, double, float*,
-                                                     float*, float*, float*, cudaStream_t);
-template void build_pressure_operator<float, double>(const float*, const Lay&, double, double, double, double*,
-                                                     double*, double*, double*, cudaStream_t);
+#define FS_BINST(T, V)                                                                                        \
+  template void build_pressure_operator<T, V>(const T*, const Lay&, double, double, double, V*, V*, V*, V*, double*, \
+                                              cudaStream_t);
+FS_BINST(float, float)
+FS_BINST(double, double)
+FS_BINST(double, float)
+FS_BINST(float, double)
 template void convert_copy<float, double>(double*, const float*, const Lay&, cudaStream_t);
 template void convert_copy<double, float>(float*, const double*, const Lay&, cudaStream_t);
 template void convert_copy<double, double>(double*, const double*, const Lay&, cudaStream_t);
