@@ -78,7 +78,7 @@ struct fs_ctx {
   void *u0 = nullptr, *v0 = nullptr, *w0 = nullptr;
   void *ua = nullptr, *va = nullptr, *wa = nullptr;
   // pressure (FP64) and projection work
-  double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *r64 = nullptr;
+  double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *r64 = nullptr, *p64bak = nullptr;
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
@@ -177,7 +177,7 @@ fs_status check_params(const fs_params* p) {
 // Launch captured batches of kGraphIters iterations until the solver state
 // says stop (done != 0); one host check of the state per batch.
 template <class V, class RV = V>
-fs_status drive_pcg(fs_ctx* c, int key, const Op7<V>& A, V* x, RV* r, V* p, V* q, int max_iter, bool timed) {
+fs_status drive_pcg(fs_ctx* c, int key, const Op7<V>& A, RV* x, RV* r, V* p, V* q, int max_iter, bool timed) {
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
@@ -421,13 +421,15 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     CKS(defect(nullptr, &rel));
     st = PCG_CONVERGED;
     if (rel > P.tolerance) {
-      // Restarted mixed-precision CG: each Krylov sequence runs in FP32
-      // (operator, p, q, partial solution x32) with an FP64 residual
-      // recurrence and reliable updates every decade; a sequence is trusted
-      // for a reduction of inner_tolerance (the reach of FP32 arithmetic on
-      // this operator), then restarted from the true residual.  A candidate
-      // p64 + x32 is folded only if its true FP64 residual improved.
-      CK(cudaMemsetAsync(c->px, 0, vbytes, s));
+      // Mixed-precision CG: the FP64 pressure p64 is the iterate and r64 the
+      // residual (FP64 recurrences); operator, p and q are FP32.  Every time
+      // the recursive residual drops a decade the true FP64 residual replaces
+      // it (reliable update).  A sequence is trusted for a reduction of
+      // inner_tolerance, then restarted from the true residual; a sequence
+      // whose true residual got worse is rolled back to the last accepted
+      // pressure and restarted.
+      const size_t pbytes = c->Lc.total * sizeof(double);
+      CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
       PcgState init{};
       init.criterion = 2;  // absolute 2-norm of the recursive residual, in b's units
       init.tol = 0.5 * P.tolerance * std::sqrt(bb);
@@ -436,32 +438,32 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       *c->st_host = init;
       CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
       CK(cudaEventRecord(c->evp0, s));
-      pcg_init<float, double>(A, c->r64, (float*)c->px, c->r64, (float*)c->pp, c->st, c->partials, s);
-      c->launches += 1;
+      // r64 already holds b - A p64; with x = p64 the init recomputes it in
+      // the FP32 operator, so start from the true one instead: x = 0 image
+      pcg_resume<float, double>(A, c->r64, (float*)c->pp, c->st, c->partials, 1, s);
+      c->launches += 2;
       int failures = 0;
       double best = rel, seq_start = rel;
       for (;;) {
-        CKS(drive_pcg<float, double>(c, 2, A, (float*)c->px, c->r64, (float*)c->pp, (float*)c->pq, P.max_iteration,
-                                     true));
+        CKS(drive_pcg<float, double>(c, 2, A, c->p64, c->r64, (float*)c->pp, (float*)c->pq, P.max_iteration, true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
         double cand = 0.0;
-        CKS(defect((float*)c->px, &cand));  // r64 <- residual of p64 + x32
+        CKS(defect(nullptr, &cand));  // r64 <- true residual of the updated p64
         bool restart;
         if (std::isfinite(cand) && cand < best) {
-          add_correction(c->p64, (float*)c->px, c->Lc, s);
-          c->launches += 1;
+          CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
           best = rel = cand;
           restart = status == PCG_STAGNATED || cand <= seq_start * P.inner_tolerance;
         } else {
-          // the sequence lost its way in FP32: drop it, restore r64
+          // the sequence lost its way: roll back and restart
+          CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
           CKS(defect(nullptr, &rel));
           restart = true;
           ++failures;
         }
-        CK(cudaMemsetAsync(c->px, 0, vbytes, s));
         if (c->debug)
-          std::fprintf(stderr, "[fs] mixed solve: iteration %d, status %d, candidate %.3e, best %.3e%s\n", iters,
+          std::fprintf(stderr, "[fs] mixed solve: iteration %d, status %d, true residual %.3e, best %.3e%s\n", iters,
                        status, cand, best, restart ? ", restart" : "");
         if (best <= P.tolerance) { st = PCG_CONVERGED; break; }
         if (iters >= P.max_iteration || failures > 8) { st = PCG_MAXITER; break; }
@@ -694,6 +696,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   double** d8[] = {&c->p64, &c->b64, &c->div64};
   for (double** p : d8) if ((s = dalloc(c, (void**)p, c8)) != FS_OK) return fail(s);
   if (c->fp32 && (s = dalloc(c, (void**)&c->r64, c8)) != FS_OK) return fail(s);
+  if (c->fp32 && (s = dalloc(c, (void**)&c->p64bak, c8)) != FS_OK) return fail(s);
   void** pv[] = {&c->pax, &c->pay, &c->paz, &c->pdiag, &c->pr, &c->pp, &c->pq};
   for (void** p : pv) if ((s = dalloc(c, p, cv)) != FS_OK) return fail(s);
   if (c->fp32) {

@@ -64,9 +64,9 @@ template <class V> struct Op7 {
 };
 
 template <class V, class R = V>
-void pcg_init(const Op7<V>& A, const R* b, V* x, R* r, V* p, PcgState* st, double* partials, cudaStream_t s);
+void pcg_init(const Op7<V>& A, const R* b, R* x, R* r, V* p, PcgState* st, double* partials, cudaStream_t s);
 template <class V, class R = V>
-void pcg_iteration(const Op7<V>& A, V* x, R* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+void pcg_iteration(const Op7<V>& A, R* x, R* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
 template <class V, class R = V>
 void pcg_resume(const Op7<V>& A, const R* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);
 int pcg_blocks(const Lay& L);

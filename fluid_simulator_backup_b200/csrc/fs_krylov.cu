@@ -2,12 +2,15 @@
 // operator (PCG_METHOD.cpp:4-126 restated for the GPU), with optional
 // reliable updates for the mixed-precision pressure solve.
 //
-// Vector types: V for the operator, the search direction p, q = A p and the
-// iterate x; R for the residual r and right-hand side b.  V = R = double is
+// Vector types: V for the operator, the search direction p and q = A p; R
+// for the iterate x, the residual r and the right-hand side b.  V = R = double is
 // the FP64 path, V = R = float the viscosity solves in FP32 storage, and
 // V = float, R = double the mixed-precision pressure solve: the residual
-// recurrence r -= alpha q and all scalars stay in FP64 while every
-// operator application streams FP32.
+// recurrences x += alpha p, r -= alpha q and all scalars stay in FP64
+// while every operator application streams FP32 (88 bytes per unknown and
+// iteration).  FP32 rounding of x or r would be amplified by ||A|| (up to
+// 6 beta/dx^2) in the true residual; rounding of p only perturbs the search
+// direction, and q is computed from the rounded p itself.
 //
 // One iteration is three kernels:
 //   spmv    q = A p and p.q                      (reads p, ax, ay, az, diag; writes q)
@@ -48,21 +51,23 @@ int reduction_blocks(int64_t n) {
 
 int pcg_blocks(const Lay& L) { return reduction_blocks((int64_t)L.nx * L.ny * L.nz); }
 
-template <class V>
-__device__ __forceinline__ V apply7(const Op7<V>& A, const V* __restrict__ x, int64_t c) {
+// (A x)_c evaluated in the type X of x (the operator's coefficients are
+// converted): FP32 iterates get FP32 arithmetic, FP64 iterates FP64.
+template <class V, class X>
+__device__ __forceinline__ X apply7(const Op7<V>& A, const X* __restrict__ x, int64_t c) {
   const int64_t sy = A.L.px, sz = A.L.slab;
-  const V xc = x[c];
+  const X xc = x[c];
   if (A.flux_form) {
-    V acc = A.ax[c] * (xc - x[c - 1]) + A.ax[c + 1] * (xc - x[c + 1]);
-    acc += A.ay[c] * (xc - x[c - sy]) + A.ay[c + sy] * (xc - x[c + sy]);
-    acc += A.az[c] * (xc - x[c - sz]) + A.az[c + sz] * (xc - x[c + sz]);
-    if (c == A.L.at(0, 0, 0)) acc += (V)(*A.extra0) * xc;
+    X acc = (X)A.ax[c] * (xc - x[c - 1]) + (X)A.ax[c + 1] * (xc - x[c + 1]);
+    acc += (X)A.ay[c] * (xc - x[c - sy]) + (X)A.ay[c + sy] * (xc - x[c + sy]);
+    acc += (X)A.az[c] * (xc - x[c - sz]) + (X)A.az[c + sz] * (xc - x[c + sz]);
+    if (c == A.L.at(0, 0, 0)) acc += (X)(*A.extra0) * xc;
     return acc;
   }
-  V acc = A.diag[c] * xc;
-  acc -= A.ax[c] * x[c - 1] + A.ax[c + 1] * x[c + 1];
-  acc -= A.ay[c] * x[c - sy] + A.ay[c + sy] * x[c + sy];
-  acc -= A.az[c] * x[c - sz] + A.az[c + sz] * x[c + sz];
+  X acc = (X)A.diag[c] * xc;
+  acc -= (X)A.ax[c] * x[c - 1] + (X)A.ax[c + 1] * x[c + 1];
+  acc -= (X)A.ay[c] * x[c - sy] + (X)A.ay[c + sy] * x[c + sy];
+  acc -= (X)A.az[c] * x[c - sz] + (X)A.az[c + sz] * x[c + sz];
   return acc;
 }
 
@@ -113,14 +118,14 @@ __device__ __forceinline__ bool stop_test(const PcgState* st, double rz, double 
 }
 
 template <class V, class RT>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_init(Op7<V> A, const RT* b, V* x, RT* r, V* __restrict__ p,
+__global__ void __launch_bounds__(kRedThreads) k_pcg_init(Op7<V> A, const RT* b, RT* x, RT* r, V* __restrict__ p,
                                                           PcgState* st, double* partials) {
   double rz = 0.0, rr = 0.0, bb = 0.0;
   Cursor cur;
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
     const RT bv = b[c];
-    const RT rv = bv - (RT)apply7(A, x, c);
+    const RT rv = bv - apply7<V, RT>(A, x, c);
     const RT z = rv / (RT)A.diag[c];
     r[c] = rv;  // b may alias r: each element is read before it is written
     p[c] = (V)z;
@@ -163,7 +168,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(Op7<V> A, const V* __r
   Cursor cur;
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-    const V qv = apply7(A, p, c);
+    const V qv = apply7<V, V>(A, p, c);
     q[c] = qv;
     pq += (double)p[c] * (double)qv;
   }
@@ -173,7 +178,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(Op7<V> A, const V* __r
 }
 
 template <class V, class RT>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, V* __restrict__ x, RT* __restrict__ r,
+__global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, RT* __restrict__ x, RT* __restrict__ r,
                                                             const V* __restrict__ p, const V* __restrict__ q,
                                                             PcgState* st, double* partials) {
   if (((volatile PcgState*)st)->done) return;
@@ -182,14 +187,13 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, V* __restr
   // a non-positive p.Ap (or an infinite step) means the iteration has lost
   // its footing in this arithmetic: keep the iterate, stop (uniform branch)
   const bool breakdown = !(pq_all > 0.0) || !isfinite(alpha);
-  const V a = (V)alpha;
   const RT ar = (RT)alpha;
   double rz = 0.0, rr = 0.0;
   if (!breakdown) {
     Cursor cur;
     for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
       const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-      x[c] += a * p[c];
+      x[c] += ar * (RT)p[c];
       const RT rv = r[c] - ar * (RT)q[c];
       r[c] = rv;
       rz += (double)rv * (double)(rv / (RT)A.diag[c]);
@@ -283,12 +287,12 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_resume(Op7<V> A, const RT* 
 }
 
 template <class V, class RT>
-void pcg_init(const Op7<V>& A, const RT* b, V* x, RT* r, V* p, PcgState* st, double* partials, cudaStream_t s) {
+void pcg_init(const Op7<V>& A, const RT* b, RT* x, RT* r, V* p, PcgState* st, double* partials, cudaStream_t s) {
   k_pcg_init<V, RT><<<pcg_blocks(A.L), kRedThreads, 0, s>>>(A, b, x, r, p, st, partials);
 }
 
 template <class V, class RT>
-void pcg_iteration(const Op7<V>& A, V* x, RT* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
+void pcg_iteration(const Op7<V>& A, RT* x, RT* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
   const int nb = pcg_blocks(A.L);
   k_pcg_spmv<V><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
   k_pcg_update<V, RT><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
@@ -303,8 +307,8 @@ void pcg_resume(const Op7<V>& A, const RT* r, V* p, PcgState* st, double* partia
 }
 
 #define FS_KINST(V, RT)                                                                                           \
-  template void pcg_init<V, RT>(const Op7<V>&, const RT*, V*, RT*, V*, PcgState*, double*, cudaStream_t);        \
-  template void pcg_iteration<V, RT>(const Op7<V>&, V*, RT*, V*, V*, PcgState*, double*, cudaStream_t);         \
+  template void pcg_init<V, RT>(const Op7<V>&, const RT*, RT*, RT*, V*, PcgState*, double*, cudaStream_t);       \
+  template void pcg_iteration<V, RT>(const Op7<V>&, RT*, RT*, V*, V*, PcgState*, double*, cudaStream_t);        \
   template void pcg_resume<V, RT>(const Op7<V>&, const RT*, V*, PcgState*, double*, int, cudaStream_t);
 
 FS_KINST(float, float)
