@@ -53,16 +53,21 @@ int pcg_blocks(const Lay& L) { return reduction_blocks((int64_t)L.nx * L.ny * L.
 
 // (A x)_c evaluated in the type X of x (the operator's coefficients are
 // converted): FP32 iterates get FP32 arithmetic, FP64 iterates FP64.
+// The flux form is always evaluated in FP64 (loads in their storage type):
+// for smooth x the six fluxes nearly cancel, and FP32 arithmetic would lose
+// about log10(n) digits of q to that cancellation; FP64 arithmetic costs no
+// memory traffic and the SpMV stays bandwidth bound.
 template <class V, class X>
 __device__ __forceinline__ X apply7(const Op7<V>& A, const X* __restrict__ x, int64_t c) {
   const int64_t sy = A.L.px, sz = A.L.slab;
   const X xc = x[c];
   if (A.flux_form) {
-    X acc = (X)A.ax[c] * (xc - x[c - 1]) + (X)A.ax[c + 1] * (xc - x[c + 1]);
-    acc += (X)A.ay[c] * (xc - x[c - sy]) + (X)A.ay[c + sy] * (xc - x[c + sy]);
-    acc += (X)A.az[c] * (xc - x[c - sz]) + (X)A.az[c + sz] * (xc - x[c + sz]);
-    if (c == A.L.at(0, 0, 0)) acc += (X)(*A.extra0) * xc;
-    return acc;
+    const double d = (double)xc;
+    double acc = (double)A.ax[c] * (d - (double)x[c - 1]) + (double)A.ax[c + 1] * (d - (double)x[c + 1]);
+    acc += (double)A.ay[c] * (d - (double)x[c - sy]) + (double)A.ay[c + sy] * (d - (double)x[c + sy]);
+    acc += (double)A.az[c] * (d - (double)x[c - sz]) + (double)A.az[c + sz] * (d - (double)x[c + sz]);
+    if (c == A.L.at(0, 0, 0)) acc += (*A.extra0) * d;
+    return (X)acc;
   }
   X acc = (X)A.diag[c] * xc;
   acc -= (X)A.ax[c] * x[c - 1] + (X)A.ax[c + 1] * x[c + 1];
@@ -170,7 +175,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(Op7<V> A, const V* __r
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
     const V qv = apply7<V, V>(A, p, c);
     q[c] = qv;
-    pq += (double)p[c] * (double)qv;
+    pq += (double)p[c] * (double)qv;  // p.q of the stored (rounded) q, as the update uses it
   }
   pq = block_sum(pq);
   double tot;
