@@ -90,6 +90,19 @@ struct Cursor {
 int reduction_blocks(int64_t n);
 constexpr int kRedThreads = 256;
 
+// Ghost-fluid face coefficient of the pressure operator between cells with
+// level sets pc, pn (POISSON_SOLVER_3D.h:1080-1085): with b = 1/rho of each
+// cell's phase, beta = b_c b_n (|phi_n| + |phi_c|) / (b_n |phi_c| + b_c |phi_n|),
+// which is b itself when both cells are in the same phase (evaluated as b
+// there: the reference's expression gives b up to rounding).
+__device__ __forceinline__ double face_coef(double pc, double pn, double rn, double rp) {
+  const bool nc = pc <= 0.0, nn = pn <= 0.0;
+  if (nc == nn) return 1.0 / (nc ? rn : rp);
+  const double vc = 1.0 / (nc ? rn : rp), vn = 1.0 / (nn ? rn : rp);
+  const double ac = fabs(pc), an = fabs(pn);
+  return vc * vn * (an + ac) / (vn * ac + vc * an);
+}
+
 // Block-wide sum of a double (any block size that is a multiple of 32, up
 // to 1024).  Result valid in thread 0.
 __device__ __forceinline__ double warp_sum(double v) {

@@ -176,13 +176,13 @@ fs_status check_params(const fs_params* p) {
 
 // Launch captured batches of kGraphIters iterations until the solver state
 // says stop (done != 0); one host check of the state per batch.
-template <class V, class RV = V>
-fs_status drive_pcg(fs_ctx* c, int key, const Op7<V>& A, RV* x, RV* r, V* p, V* q, int max_iter, bool timed) {
+template <class F>
+fs_status drive_pcg(fs_ctx* c, int key, F&& enqueue_iteration, int max_iter, bool timed) {
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    for (int n = 0; n < kGraphIters; ++n) pcg_iteration<V, RV>(A, x, r, p, q, c->st, c->partials, c->stream);
+    for (int n = 0; n < kGraphIters; ++n) enqueue_iteration();
     CK(cudaStreamEndCapture(c->stream, &g));
     cudaGraphExec_t ge;
     CK(cudaGraphInstantiate(&ge, g, 0));
@@ -221,7 +221,7 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   pcg_init<V>(A, b, x, r, p, c->st, c->partials, c->stream);
   c->launches += 1;
   CK(cudaGetLastError());
-  CKS(drive_pcg<V, V>(c, key, A, x, r, p, q, max_iter, timed));
+  CKS(drive_pcg(c, key, [&] { pcg_iteration<V, V>(A, x, r, p, q, c->st, c->partials, c->stream); }, max_iter, timed));
   if (timed) {
     CK(cudaEventRecord(c->evp1, c->stream));
     CK(cudaEventSynchronize(c->evp1));
@@ -397,6 +397,9 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
                                       (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s);
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
+    // the Krylov sequence applies the operator from phi in FP64 (the same
+    // operator as the FP64 defect); only the Jacobi diagonal is stored
+    const OpPhi<S> Aphi{phi, (float*)c->pdiag, c->Lc, P.rho_neg, P.rho_pos, 1.0 / (dx * dx)};
     const size_t vbytes = c->Lc.total * sizeof(float);
     double bb = 0.0;
     // true FP64 residual b - A64 (p64 [+ x32]) with A64 evaluated from phi in
@@ -445,7 +448,12 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       int failures = 0;
       double best = rel, seq_start = rel;
       for (;;) {
-        CKS(drive_pcg<float, double>(c, 2, A, c->p64, c->r64, (float*)c->pp, (float*)c->pq, P.max_iteration, true));
+        CKS(drive_pcg(c, 2,
+                      [&] {
+                        pcg_iteration_phi<S>(Aphi, c->p64, c->r64, (float*)c->pp, (float*)c->pq, c->st, c->partials,
+                                             s);
+                      },
+                      P.max_iteration, true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
         double cand = 0.0;

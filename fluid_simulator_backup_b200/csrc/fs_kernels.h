@@ -67,6 +67,20 @@ template <class V, class R = V>
 void pcg_init(const Op7<V>& A, const R* b, R* x, R* r, V* p, PcgState* st, double* partials, cudaStream_t s);
 template <class V, class R = V>
 void pcg_iteration(const Op7<V>& A, R* x, R* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+// Pressure operator evaluated from phi on the fly (mixed-precision solve):
+// face coefficients beta_f in FP64 from the stored level set, so the FP32
+// Krylov sequence applies exactly the operator of the FP64 defect residual.
+// diag (FP32) is used only by the Jacobi preconditioner.
+template <class T> struct OpPhi {
+  const T* phi;
+  const float* diag;
+  Lay L;
+  double rn, rp, inv2;
+};
+template <class T>
+void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, float* q, PcgState* st, double* partials,
+                       cudaStream_t s);
+
 template <class V, class R = V>
 void pcg_resume(const Op7<V>& A, const R* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);
 int pcg_blocks(const Lay& L);

@@ -135,40 +135,25 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
   for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
     const int i = cur.i, j = cur.j, k = cur.k;
     const int64_t c = Lc.at(i, j, k);
-    const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
+    const double pc = (double)phi[c];
     const double xc = x32 ? p[c] + (double)x32[c] : p[c];
-    double s = 0.0, off = 0.0;
     const int64_t nb[6] = {c - 1, c + 1, c - Lc.px, c + Lc.px, c - Lc.slab, c + Lc.slab};
     const bool ok[6] = {i > 0, i < Lc.nx - 1, j > 0, j < Lc.ny - 1, k > 0, k < Lc.nz - 1};
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      if (!ok[q]) continue;
-      const double beta = face_beta(vc, inv_rho(phi[nb[q]], rn, rp), acv, fabs((double)phi[nb[q]]));
-      s += beta;
-      off += beta * (x32 ? p[nb[q]] + (double)x32[nb[q]] : p[nb[q]]);
-    }
-    if (i == 0 && j == 0 && k == 0) {
-      const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
-      const double gd = fabs(2.0 * pc - (double)phi[c + Lc.slab]);
-      s = (s + vc * vc * (gb + acv) / (vc * gb + vc * acv)) + vc * vc * (gd + acv) / (vc * gd + vc * acv);
-    }
-    if (s == 0.0) s = 1.0;
-    (void)off;
-    // flux form (no cancellation): sum beta (x_c - x_nb) + deflation term
+    // flux form with the same face coefficients as the on-the-fly SpMV
     double flux = 0.0;
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       if (!ok[q]) continue;
-      const double beta = face_beta(vc, inv_rho(phi[nb[q]], rn, rp), acv, fabs((double)phi[nb[q]]));
       const double xn = x32 ? p[nb[q]] + (double)x32[nb[q]] : p[nb[q]];
-      flux += beta * (xc - xn);
+      flux += face_coef(pc, (double)phi[nb[q]], rn, rp) * (xc - xn);
     }
-    double sum_faces = 0.0;
-#pragma unroll
-    for (int q = 0; q < 6; ++q)
-      if (ok[q]) sum_faces += face_beta(vc, inv_rho(phi[nb[q]], rn, rp), acv, fabs((double)phi[nb[q]]));
-    const double extra = (i == 0 && j == 0 && k == 0) ? s - sum_faces : 0.0;
-    const double ax = inv2 * (flux + extra * xc);
+    if (i == 0 && j == 0 && k == 0) {
+      const double vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
+      const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
+      const double gd = fabs(2.0 * pc - (double)phi[c + Lc.slab]);
+      flux += (vc * vc * (gb + acv) / (vc * gb + vc * acv) + vc * vc * (gd + acv) / (vc * gd + vc * acv)) * xc;
+    }
+    const double ax = inv2 * flux;
     const double rv = b[c] - ax;
     r64[c] = rv;
     if (r32) r32[c] = (float)rv;
