@@ -438,6 +438,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       init.tol = 0.5 * P.tolerance * std::sqrt(bb);
       init.max_iter = P.max_iteration;
       init.reliable_delta = 0.1;
+      init.bb = bb;  // ||b||^2 of the pressure system, for the recursive relative residual
       *c->st_host = init;
       CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
       CK(cudaEventRecord(c->evp0, s));
@@ -446,7 +447,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       pcg_resume<float, double>(A, c->r64, (float*)c->pp, c->st, c->partials, 1, s);
       c->launches += 2;
       int failures = 0;
-      double best = rel, seq_start = rel;
+      double best = rel;
       for (;;) {
         CKS(drive_pcg(c, 2,
                       [&] {
@@ -456,26 +457,37 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
                       P.max_iteration, true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
-        double cand = 0.0;
-        CKS(defect(nullptr, &cand));  // r64 <- true residual of the updated p64
-        bool restart;
-        if (std::isfinite(cand) && cand < best) {
-          CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
-          best = rel = cand;
-          restart = status == PCG_STAGNATED || cand <= seq_start * P.inner_tolerance;
-        } else {
-          // the sequence lost its way: roll back and restart
+        const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
+        double now = 0.0;
+        CKS(defect(nullptr, &now));  // r64 <- true residual of the current pressure
+        bool restart = false;
+        if (!std::isfinite(now) || now > 100.0 * best) {
+          // diverged (not a CG residual oscillation): back to the best pressure
           CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
-          CKS(defect(nullptr, &rel));
+          CKS(defect(nullptr, &now));
           restart = true;
           ++failures;
+        } else {
+          if (now < best) {
+            best = now;
+            CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
+          }
+          // restart the direction after a breakdown or when the recursion
+          // has drifted far from the true residual
+          restart = status == PCG_STAGNATED || now > 10.0 * recursive;
         }
+        rel = now;
         if (c->debug)
-          std::fprintf(stderr, "[fs] mixed solve: iteration %d, status %d, true residual %.3e, best %.3e%s\n", iters,
-                       status, cand, best, restart ? ", restart" : "");
-        if (best <= P.tolerance) { st = PCG_CONVERGED; break; }
-        if (iters >= P.max_iteration || failures > 8) { st = PCG_MAXITER; break; }
-        if (restart) seq_start = best;
+          std::fprintf(stderr, "[fs] mixed solve: iteration %d, status %d, recursive %.3e, true %.3e, best %.3e%s\n",
+                       iters, status, recursive, now, best, restart ? ", restart" : "");
+        if (now <= P.tolerance) { st = PCG_CONVERGED; break; }
+        if (iters >= P.max_iteration || failures > 8) {
+          // leave the best pressure found
+          CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
+          rel = best;
+          st = PCG_MAXITER;
+          break;
+        }
         pcg_resume<float, double>(A, c->r64, (float*)c->pp, c->st, c->partials, restart ? 1 : 0, s);
         c->launches += 2;
         CK(cudaGetLastError());

@@ -27,7 +27,7 @@ template <class T> void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s)
 struct PcgState {
   double rz, pq, rr, bb, beta, tol;
   double best_rr;         // smallest r.r seen
-  double max_rr;          // largest r.r since the last true residual (reliable updates)
+  double max_rr;          // r.r of the last true residual (reference of the reliable-update trigger)
   double rz_prev;         // r.z at the start of the last accepted step
   double reliable_delta;  // pause for a true residual when ||r|| < delta*max||r|| (0: never)
   int iter, max_iter, done, criterion, status, stall;

@@ -222,7 +222,6 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, RT* __rest
     } else {
       st->stall += 1;
     }
-    if (tot[1] > st->max_rr) st->max_rr = tot[1];
     if (!isfinite(tot[0]) || !isfinite(tot[1])) {
       st->status = PCG_NONFINITE;
       st->done = 1;
