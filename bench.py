@@ -33,7 +33,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_UNKNOWN_PCG_FP32 = 76  # spmv 12 (p, phi, q) + update 44 (x64, r64 rw; p, q, diag) + direction 20
+BYTES_PER_UNKNOWN_PCG_FP32 = 84  # spmv 16 (p, phi; q64) + update 48 (x64, r64 rw; p, q64, diag) + direction 20
 BYTES_PER_UNKNOWN_PCG_FP64 = 136
 
 

@@ -95,10 +95,12 @@ constexpr int kRedThreads = 256;
 // cell's phase, beta = b_c b_n (|phi_n| + |phi_c|) / (b_n |phi_c| + b_c |phi_n|),
 // which is b itself when both cells are in the same phase (evaluated as b
 // there: the reference's expression gives b up to rounding).
-__device__ __forceinline__ double face_coef(double pc, double pn, double rn, double rp) {
+// (vneg, vpos are 1/rho of the two phases, precomputed by the caller.)
+__device__ __forceinline__ double face_coef(double pc, double pn, double vneg, double vpos) {
   const bool nc = pc <= 0.0, nn = pn <= 0.0;
-  if (nc == nn) return 1.0 / (nc ? rn : rp);
-  const double vc = 1.0 / (nc ? rn : rp), vn = 1.0 / (nn ? rn : rp);
+  const double vc = nc ? vneg : vpos;
+  if (nc == nn) return vc;
+  const double vn = nn ? vneg : vpos;
   const double ac = fabs(pc), an = fabs(pn);
   return vc * vn * (an + ac) / (vn * ac + vc * an);
 }

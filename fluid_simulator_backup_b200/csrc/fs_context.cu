@@ -78,7 +78,7 @@ struct fs_ctx {
   void *u0 = nullptr, *v0 = nullptr, *w0 = nullptr;
   void *ua = nullptr, *va = nullptr, *wa = nullptr;
   // pressure (FP64) and projection work
-  double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *r64 = nullptr, *p64bak = nullptr;
+  double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *r64 = nullptr, *p64bak = nullptr, *qd = nullptr;
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
@@ -451,8 +451,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       for (;;) {
         CKS(drive_pcg(c, 2,
                       [&] {
-                        pcg_iteration_phi<S>(Aphi, c->p64, c->r64, (float*)c->pp, (float*)c->pq, c->st, c->partials,
-                                             s);
+                        pcg_iteration_phi<S>(Aphi, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s);
                       },
                       P.max_iteration, true));
         const int status = c->st_host->status;
@@ -717,6 +716,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   for (double** p : d8) if ((s = dalloc(c, (void**)p, c8)) != FS_OK) return fail(s);
   if (c->fp32 && (s = dalloc(c, (void**)&c->r64, c8)) != FS_OK) return fail(s);
   if (c->fp32 && (s = dalloc(c, (void**)&c->p64bak, c8)) != FS_OK) return fail(s);
+  if (c->fp32 && (s = dalloc(c, (void**)&c->qd, c8)) != FS_OK) return fail(s);
   void** pv[] = {&c->pax, &c->pay, &c->paz, &c->pdiag, &c->pr, &c->pp, &c->pq};
   for (void** p : pv) if ((s = dalloc(c, p, cv)) != FS_OK) return fail(s);
   if (c->fp32) {

@@ -75,10 +75,10 @@ template <class T> struct OpPhi {
   const T* phi;
   const float* diag;
   Lay L;
-  double rn, rp, inv2;
+  double rn, rp, inv2;  // densities of the phi <= 0 / phi > 0 phases, 1/dx^2
 };
 template <class T>
-void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, float* q, PcgState* st, double* partials,
+void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, double* q, PcgState* st, double* partials,
                        cudaStream_t s);
 
 template <class V, class R = V>

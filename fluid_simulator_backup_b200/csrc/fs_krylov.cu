@@ -8,9 +8,9 @@
 // V = float, R = double the mixed-precision pressure solve: the residual
 // recurrences x += alpha p, r -= alpha q and all scalars stay in FP64
 // while every operator application streams FP32 (88 bytes per unknown and
-// iteration).  FP32 rounding of x or r would be amplified by ||A|| (up to
-// 6 beta/dx^2) in the true residual; rounding of p only perturbs the search
-// direction, and q is computed from the rounded p itself.
+// iteration).  FP32 rounding of x, r or q would be amplified by ||A|| or
+// by the transient growth of the CG residual; rounding of p only perturbs
+// the search direction, and q is computed from the rounded p itself.
 //
 // One iteration is three kernels:
 //   spmv    q = A p and p.q                      (reads p, ax, ay, az, diag; writes q)
@@ -182,9 +182,9 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(Op7<V> A, const V* __r
   if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) st->pq = tot;
 }
 
-template <class V, class RT>
+template <class V, class RT, class Q = V>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, RT* __restrict__ x, RT* __restrict__ r,
-                                                            const V* __restrict__ p, const V* __restrict__ q,
+                                                            const V* __restrict__ p, const Q* __restrict__ q,
                                                             PcgState* st, double* partials) {
   if (((volatile PcgState*)st)->done) return;
   const double pq_all = ((volatile PcgState*)st)->pq;
@@ -305,9 +305,10 @@ void pcg_iteration(const Op7<V>& A, RT* x, RT* r, V* p, V* q, PcgState* st, doub
 
 template <class T>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv_phi(OpPhi<T> A, const float* __restrict__ p,
-                                                              float* __restrict__ q, PcgState* st, double* partials) {
+                                                              double* __restrict__ q, PcgState* st, double* partials) {
   if (((volatile PcgState*)st)->done) return;
   const int64_t sy = A.L.px, sz = A.L.slab;
+  const double vn = 1.0 / A.rn, vp = 1.0 / A.rp;
   double pq = 0.0;
   Cursor cur;
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
@@ -315,21 +316,21 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv_phi(OpPhi<T> A, const 
     const int64_t c = A.L.at(i, j, k);
     const double pc = (double)A.phi[c], xc = (double)p[c];
     double acc = 0.0;
-    if (i > 0) acc += face_coef(pc, (double)A.phi[c - 1], A.rn, A.rp) * (xc - (double)p[c - 1]);
-    if (i < A.L.nx - 1) acc += face_coef(pc, (double)A.phi[c + 1], A.rn, A.rp) * (xc - (double)p[c + 1]);
-    if (j > 0) acc += face_coef(pc, (double)A.phi[c - sy], A.rn, A.rp) * (xc - (double)p[c - sy]);
-    if (j < A.L.ny - 1) acc += face_coef(pc, (double)A.phi[c + sy], A.rn, A.rp) * (xc - (double)p[c + sy]);
-    if (k > 0) acc += face_coef(pc, (double)A.phi[c - sz], A.rn, A.rp) * (xc - (double)p[c - sz]);
-    if (k < A.L.nz - 1) acc += face_coef(pc, (double)A.phi[c + sz], A.rn, A.rp) * (xc - (double)p[c + sz]);
+    if (i > 0) acc += face_coef(pc, (double)A.phi[c - 1], vn, vp) * (xc - (double)p[c - 1]);
+    if (i < A.L.nx - 1) acc += face_coef(pc, (double)A.phi[c + 1], vn, vp) * (xc - (double)p[c + 1]);
+    if (j > 0) acc += face_coef(pc, (double)A.phi[c - sy], vn, vp) * (xc - (double)p[c - sy]);
+    if (j < A.L.ny - 1) acc += face_coef(pc, (double)A.phi[c + sy], vn, vp) * (xc - (double)p[c + sy]);
+    if (k > 0) acc += face_coef(pc, (double)A.phi[c - sz], vn, vp) * (xc - (double)p[c - sz]);
+    if (k < A.L.nz - 1) acc += face_coef(pc, (double)A.phi[c + sz], vn, vp) * (xc - (double)p[c + sz]);
     if (i == 0 && j == 0 && k == 0) {
       // deflation: the first cell's bottom and down Neumann ghosts
-      const double vc = 1.0 / (pc <= 0.0 ? A.rn : A.rp), ac = fabs(pc);
+      const double vc = pc <= 0.0 ? vn : vp, ac = fabs(pc);
       const double gb = fabs(2.0 * pc - (double)A.phi[c + sy]), gd = fabs(2.0 * pc - (double)A.phi[c + sz]);
       acc += (vc * vc * (gb + ac) / (vc * gb + vc * ac) + vc * vc * (gd + ac) / (vc * gd + vc * ac)) * xc;
     }
-    const float qv = (float)(A.inv2 * acc);
+    const double qv = A.inv2 * acc;
     q[c] = qv;
-    pq += xc * (double)qv;
+    pq += xc * qv;
   }
   pq = block_sum(pq);
   double tot;
@@ -337,18 +338,18 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv_phi(OpPhi<T> A, const 
 }
 
 template <class T>
-void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, float* q, PcgState* st, double* partials,
+void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, double* q, PcgState* st, double* partials,
                        cudaStream_t s) {
   const int nb = pcg_blocks(A.L);
   Op7<float> D{nullptr, nullptr, nullptr, A.diag, A.L};
   k_pcg_spmv_phi<T><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
-  k_pcg_update<float, double><<<nb, kRedThreads, 0, s>>>(D, x, r, p, q, st, partials);
+  k_pcg_update<float, double, double><<<nb, kRedThreads, 0, s>>>(D, x, r, p, q, st, partials);
   k_pcg_pupdate<float, double><<<nb, kRedThreads, 0, s>>>(D, r, p, st);
 }
 
-template void pcg_iteration_phi<float>(const OpPhi<float>&, double*, double*, float*, float*, PcgState*, double*,
+template void pcg_iteration_phi<float>(const OpPhi<float>&, double*, double*, float*, double*, PcgState*, double*,
                                        cudaStream_t);
-template void pcg_iteration_phi<double>(const OpPhi<double>&, double*, double*, float*, float*, PcgState*, double*,
+template void pcg_iteration_phi<double>(const OpPhi<double>&, double*, double*, float*, double*, PcgState*, double*,
                                         cudaStream_t);
 
 template <class V, class RT>

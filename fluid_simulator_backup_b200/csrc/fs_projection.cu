@@ -145,7 +145,7 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
     for (int q = 0; q < 6; ++q) {
       if (!ok[q]) continue;
       const double xn = x32 ? p[nb[q]] + (double)x32[nb[q]] : p[nb[q]];
-      flux += face_coef(pc, (double)phi[nb[q]], rn, rp) * (xc - xn);
+      flux += face_coef(pc, (double)phi[nb[q]], 1.0 / rn, 1.0 / rp) * (xc - xn);
     }
     if (i == 0 && j == 0 && k == 0) {
       const double vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
