@@ -92,7 +92,10 @@ struct fs_ctx {
   PcgState* st_host = nullptr;      // pinned
   double* sc_host = nullptr;        // pinned [16]
   double* staging = nullptr;        // packed FP64 transfer buffer
-  std::map<int, cudaGraphExec_t> graphs;
+  // captured solver graphs keyed by solve kind and the one operand whose
+  // buffer rotates between calls (the level set); kernel arguments are
+  // baked into a graph, so a different buffer needs its own graph
+  std::map<std::pair<int, const void*>, cudaGraphExec_t> graphs;
   // accounting for fs_step_report
   int64_t launches = 0;
   float pcg_ms = 0.0f;
@@ -177,7 +180,7 @@ fs_status check_params(const fs_params* p) {
 // Launch captured batches of kGraphIters iterations until the solver state
 // says stop (done != 0); one host check of the state per batch.
 template <class F>
-fs_status drive_pcg(fs_ctx* c, int key, F&& enqueue_iteration, int max_iter, bool timed) {
+fs_status drive_pcg(fs_ctx* c, std::pair<int, const void*> key, F&& enqueue_iteration, int max_iter, bool timed) {
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
@@ -221,7 +224,8 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   pcg_init<V>(A, b, x, r, p, c->st, c->partials, c->stream);
   c->launches += 1;
   CK(cudaGetLastError());
-  CKS(drive_pcg(c, key, [&] { pcg_iteration<V, V>(A, x, r, p, q, c->st, c->partials, c->stream); }, max_iter, timed));
+  CKS(drive_pcg(c, std::make_pair(key, (const void*)nullptr),
+                [&] { pcg_iteration<V, V>(A, x, r, p, q, c->st, c->partials, c->stream); }, max_iter, timed));
   if (timed) {
     CK(cudaEventRecord(c->evp1, c->stream));
     CK(cudaEventSynchronize(c->evp1));
@@ -449,7 +453,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       int failures = 0;
       double best = rel;
       for (;;) {
-        CKS(drive_pcg(c, 2,
+        CKS(drive_pcg(c, std::make_pair(2, (const void*)phi),
                       [&] {
                         pcg_iteration_phi<S>(Aphi, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s);
                       },
