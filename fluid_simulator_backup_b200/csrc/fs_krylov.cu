@@ -32,20 +32,27 @@
 // FP64 and resumes the same Krylov iteration (pcg_resume) with that residual,
 // keeping the search direction.  The FP32 iteration therefore converges like
 // one long CG instead of a sequence of restarted ones.
+#include <cstdlib>
+
 #include "fs_kernels.h"
 
 namespace fsb {
 
 static int g_sm_count = 0;
+static int g_blocks_per_sm = 6;  // 6 x 256 threads: fully resident for kernels up to 40 registers
 
 int reduction_blocks(int64_t n) {
   if (g_sm_count <= 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) g_sm_count = 148;
+    if (const char* e = std::getenv("FS_BLOCKS_PER_SM")) {  // tuning knob for launch-shape sweeps
+      const int v = std::atoi(e);
+      if (v >= 1 && v <= 16) g_blocks_per_sm = v;
+    }
   }
   const int64_t want = (n + kRedThreads - 1) / kRedThreads;
-  const int64_t cap = (int64_t)4 * g_sm_count;
+  const int64_t cap = (int64_t)g_blocks_per_sm * g_sm_count;
   return (int)(want < cap ? (want > 0 ? want : 1) : cap);
 }
 
