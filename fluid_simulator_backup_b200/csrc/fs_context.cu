@@ -102,6 +102,7 @@ struct fs_ctx {
   int pcg_launched_iterations = 0;
   cudaEvent_t evp0 = nullptr, evp1 = nullptr;
   bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
+  bool stored32 = false;  // FS_STORED32=1: mixed solve with stored FP32 couplings instead of phi
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -453,11 +454,16 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       int failures = 0;
       double best = rel;
       for (;;) {
-        CKS(drive_pcg(c, std::make_pair(2, (const void*)phi),
-                      [&] {
-                        pcg_iteration_phi<S>(Aphi, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s);
-                      },
-                      P.max_iteration, true));
+        if (c->stored32)
+          CKS(drive_pcg(c, std::make_pair(3, (const void*)nullptr),
+                        [&] { pcg_iteration_stored32(A, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s); },
+                        P.max_iteration, true));
+        else
+          CKS(drive_pcg(c, std::make_pair(2, (const void*)phi),
+                        [&] {
+                          pcg_iteration_phi<S>(Aphi, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s);
+                        },
+                        P.max_iteration, true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
         const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
@@ -691,6 +697,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
   c->debug = std::getenv("FS_DEBUG") != nullptr;
+  c->stored32 = std::getenv("FS_STORED32") != nullptr;
   c->Lc = make_lay(grid->nx, grid->ny, grid->nz);
   c->Lu = make_lay(grid->nx + 1, grid->ny, grid->nz);
   c->Lv = make_lay(grid->nx, grid->ny + 1, grid->nz);

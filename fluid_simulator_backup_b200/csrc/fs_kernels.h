@@ -81,6 +81,9 @@ template <class T>
 void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, double* q, PcgState* st, double* partials,
                        cudaStream_t s);
 
+void pcg_iteration_stored32(const Op7<float>& A, double* x, double* r, float* p, double* q, PcgState* st,
+                            double* partials, cudaStream_t s);
+
 template <class V, class R = V>
 void pcg_resume(const Op7<V>& A, const R* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);
 int pcg_blocks(const Lay& L);

@@ -32,6 +32,7 @@
 // FP64 and resumes the same Krylov iteration (pcg_resume) with that residual,
 // keeping the search direction.  The FP32 iteration therefore converges like
 // one long CG instead of a sequence of restarted ones.
+#include <algorithm>
 #include <cstdlib>
 
 #include "fs_kernels.h"
@@ -344,12 +345,45 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv_phi(OpPhi<T> A, const 
   if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) st->pq = tot;
 }
 
+// Stored-coefficient variant of the mixed iteration: FP32 face couplings in
+// flux form, evaluated in FP64, q in FP64.
+template <class V>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_spmv_q64(Op7<V> A, const V* __restrict__ p, double* __restrict__ q,
+                                                              PcgState* st, double* partials) {
+  if (((volatile PcgState*)st)->done) return;
+  const int64_t sy = A.L.px, sz = A.L.slab;
+  double pq = 0.0;
+  Cursor cur;
+  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
+    const int64_t c = A.L.at(cur.i, cur.j, cur.k);
+    const double d = (double)p[c];
+    double acc = (double)A.ax[c] * (d - (double)p[c - 1]) + (double)A.ax[c + 1] * (d - (double)p[c + 1]);
+    acc += (double)A.ay[c] * (d - (double)p[c - sy]) + (double)A.ay[c + sy] * (d - (double)p[c + sy]);
+    acc += (double)A.az[c] * (d - (double)p[c - sz]) + (double)A.az[c + sz] * (d - (double)p[c + sz]);
+    if (c == A.L.at(0, 0, 0)) acc += (*A.extra0) * d;
+    q[c] = acc;
+    pq += d * acc;
+  }
+  pq = block_sum(pq);
+  double tot;
+  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) st->pq = tot;
+}
+
+void pcg_iteration_stored32(const Op7<float>& A, double* x, double* r, float* p, double* q, PcgState* st,
+                            double* partials, cudaStream_t s) {
+  const int nb = pcg_blocks(A.L);
+  k_pcg_spmv_q64<float><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
+  k_pcg_update<float, double, double><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
+  k_pcg_pupdate<float, double><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
+}
+
 template <class T>
 void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, double* q, PcgState* st, double* partials,
                        cudaStream_t s) {
   const int nb = pcg_blocks(A.L);
   Op7<float> D{nullptr, nullptr, nullptr, A.diag, A.L};
-  k_pcg_spmv_phi<T><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
+  // the on-the-fly operator needs 58 registers: 4 resident blocks per SM
+  k_pcg_spmv_phi<T><<<std::min(nb, 4 * g_sm_count), kRedThreads, 0, s>>>(A, p, q, st, partials);
   k_pcg_update<float, double, double><<<nb, kRedThreads, 0, s>>>(D, x, r, p, q, st, partials);
   k_pcg_pupdate<float, double><<<nb, kRedThreads, 0, s>>>(D, r, p, st);
 }
