@@ -33,7 +33,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_UNKNOWN_PCG_FP32 = 84  # spmv 16 (p, phi; q64) + update 48 (x64, r64 rw; p, q64, diag) + direction 20
+BYTES_PER_UNKNOWN_PCG_FP32 = 92  # spmv 24 (p32, 3 couplings32; q64) + update 48 (x64, r64 rw; p32, q64, diag32) + direction 20
 BYTES_PER_UNKNOWN_PCG_FP64 = 136
 
 
@@ -219,11 +219,13 @@ def reference_sample_isolated(n, iters, threads=1):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"],
+                    help="precision of the timed path (the headline is fp32_refine)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     args = ap.parse_args()
@@ -281,8 +283,12 @@ def main():
 
     import fluid_simulator_backup_b200 as fs
     fs.lib()
+    main_prec = fs.FS_PRECISION_FP32_REFINE if args.precision == "fp32_refine" else fs.FS_PRECISION_FP64
+    if main_prec == fs.FS_PRECISION_FP64:
+        args.no_fp64 = True
+        config["precision"] = "fp64"
     with ClockSampler(local) as clk:
-        s32, reps = run_steps(fs, n, fs.FS_PRECISION_FP32_REFINE, args.warmup, args.steps, barrier)
+        s32, reps = run_steps(fs, n, main_prec, args.warmup, args.steps, barrier)
     ms_steps = [r["ms"] for r in reps]
     ms = max_over_ranks(float(np.mean(ms_steps)))
     pcg_ms = sum(r["pcg_ms"] for r in reps)
@@ -291,7 +297,8 @@ def main():
     launches = sum(r["kernel_launches"] for r in reps)
     N = n ** 3
     per_iter_s = pcg_ms / 1e3 / max(pcg_its, 1)
-    achieved = BYTES_PER_UNKNOWN_PCG_FP32 * N / per_iter_s / 1e9
+    bpu = BYTES_PER_UNKNOWN_PCG_FP32 if main_prec == fs.FS_PRECISION_FP32_REFINE else BYTES_PER_UNKNOWN_PCG_FP64
+    achieved = bpu * N / per_iter_s / 1e9
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -320,14 +327,15 @@ def main():
 
     line = {
         "metric": metric, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if main_prec == fs.FS_PRECISION_FP32_REFINE else "f64",
         "data": "synthetic", "config": config,
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "FP32 inner PCG iteration (spmv + update + direction, 3 kernels)",
+        "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (spmv + update + direction, 3 kernels)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "traffic": None,
-                     "bytes_per_iteration": BYTES_PER_UNKNOWN_PCG_FP32 * N,
+                     "bytes_per_iteration": bpu * N,
                      "pcg_ms": pcg_ms, "pcg_launched_iterations": pcg_its, "pcg_iterations": real_its},
         "fp64": fp64,
         "steps_detail": [{k: r[k] for k in ("ms", "pcg_iterations", "outer_iterations", "viscosity_iterations",

@@ -102,8 +102,6 @@ struct fs_ctx {
   int pcg_launched_iterations = 0;
   cudaEvent_t evp0 = nullptr, evp1 = nullptr;
   bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
-  bool stored32 = false;  // FS_STORED32=1: mixed solve with stored FP32 couplings instead of phi
-  bool pure32 = false;    // FS_PURE32=1: FP32 Krylov vectors, FP64 only in the true residual and the pressure
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -403,9 +401,6 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
                                       (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s);
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
-    // the Krylov sequence applies the operator from phi in FP64 (the same
-    // operator as the FP64 defect); only the Jacobi diagonal is stored
-    const OpPhi<S> Aphi{phi, (float*)c->pdiag, c->Lc, P.rho_neg, P.rho_pos, 1.0 / (dx * dx)};
     const size_t vbytes = c->Lc.total * sizeof(float);
     double bb = 0.0;
     // true FP64 residual b - A64 (p64 [+ x32]) with A64 evaluated from phi in
@@ -429,93 +424,12 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     };
     CKS(defect(nullptr, &rel));
     st = PCG_CONVERGED;
-    if (rel > P.tolerance && c->pure32) {
-      // FP32 CG (x32, r32, p, q and the couplings in FP32, flux form evaluated
-      // in FP64) with reliable updates: every decade of the recursive
-      // residual, x32 is folded into the FP64 pressure and r32 replaced by the
-      // FP32 image of the true FP64 residual.
-      const size_t pbytes = c->Lc.total * sizeof(double);
-      float *x32 = (float*)c->px, *r32 = (float*)c->pr, *p32 = (float*)c->pp, *q32 = (float*)c->pq;
-      CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
-      CK(cudaMemsetAsync(x32, 0, vbytes, s));
-      // r32 <- image of the true residual
-      defect_residual<S>(phi, c->p64, nullptr, c->b64, c->r64, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
-                         c->tickets + 2, c->scalars + 2, s);
-      c->launches += 1;
-      PcgState init{};
-      init.criterion = 2;
-      init.tol = 0.5 * P.tolerance * std::sqrt(bb);
-      init.max_iter = P.max_iteration;
-      init.reliable_delta = 0.1;
-      init.bb = bb;
-      *c->st_host = init;
-      CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
-      CK(cudaEventRecord(c->evp0, s));
-      pcg_resume<float, float>(A, r32, p32, c->st, c->partials, 1, s);
-      c->launches += 2;
-      int failures = 0;
-      double best = rel;
-      for (;;) {
-        CKS(drive_pcg(c, std::make_pair(4, (const void*)nullptr),
-                      [&] { pcg_iteration<float, float>(A, x32, r32, p32, q32, c->st, c->partials, s); },
-                      P.max_iteration, true));
-        const int status = c->st_host->status;
-        iters = c->st_host->iter;
-        const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
-        double now = 0.0;
-        // true residual of p64 + x32; r32 receives its FP32 image
-        defect_residual<S>(phi, c->p64, x32, c->b64, c->r64, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
-                           c->tickets + 2, c->scalars + 2, s);
-        c->launches += 1;
-        CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        now = c->sc_host[1] > 0 ? std::sqrt(c->sc_host[2] / c->sc_host[1]) : 0.0;
-        outer += 1;
-        bool restart = false;
-        if (!std::isfinite(now) || now > 100.0 * best) {
-          CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
-          CK(cudaMemsetAsync(x32, 0, vbytes, s));
-          defect_residual<S>(phi, c->p64, nullptr, c->b64, c->r64, r32, c->Lc, dx, P.rho_neg, P.rho_pos,
-                             c->partials, c->tickets + 2, c->scalars + 2, s);
-          c->launches += 1;
-          CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-          CK(cudaStreamSynchronize(s));
-          now = std::sqrt(c->sc_host[2] / c->sc_host[1]);
-          restart = true;
-          ++failures;
-        } else {
-          add_correction(c->p64, x32, c->Lc, s);
-          c->launches += 1;
-          CK(cudaMemsetAsync(x32, 0, vbytes, s));
-          if (now < best) {
-            best = now;
-            CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
-          }
-          restart = status == PCG_STAGNATED || now > 10.0 * recursive;
-        }
-        rel = now;
-        if (c->debug)
-          std::fprintf(stderr, "[fs] fp32 solve: iteration %d, status %d, recursive %.3e, true %.3e, best %.3e%s\n",
-                       iters, status, recursive, now, best, restart ? ", restart" : "");
-        if (now <= P.tolerance) { st = PCG_CONVERGED; break; }
-        if (iters >= P.max_iteration || failures > 8) {
-          CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
-          rel = best;
-          st = PCG_MAXITER;
-          break;
-        }
-        pcg_resume<float, float>(A, r32, p32, c->st, c->partials, restart ? 1 : 0, s);
-        c->launches += 2;
-        CK(cudaGetLastError());
-      }
-      CK(cudaEventRecord(c->evp1, s));
-      CK(cudaEventSynchronize(c->evp1));
-      float ms = 0.0f;
-      CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
-      c->pcg_ms += ms;
-    } else if (rel > P.tolerance) {
-      // Mixed-precision CG: the FP64 pressure p64 is the iterate and r64 the
-      // residual (FP64 recurrences); operator, p and q are FP32.  Every time
+    if (rel > P.tolerance) {
+      // Mixed-precision CG: the FP64 pressure p64 is the iterate, r64 the
+      // residual and q = A p is kept in FP64 (FP64 recurrences); the face
+      // couplings and the search direction p are FP32 (the flux-form
+      // operator is evaluated in FP64 from them: 92 bytes per unknown and
+      // iteration against 136 for the FP64 solve).  Every time
       // the recursive residual drops a decade the true FP64 residual replaces
       // it (reliable update).  A sequence is trusted for a reduction of
       // inner_tolerance, then restarted from the true residual; a sequence
@@ -539,16 +453,9 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       int failures = 0;
       double best = rel;
       for (;;) {
-        if (c->stored32)
-          CKS(drive_pcg(c, std::make_pair(3, (const void*)nullptr),
-                        [&] { pcg_iteration_stored32(A, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s); },
-                        P.max_iteration, true));
-        else
-          CKS(drive_pcg(c, std::make_pair(2, (const void*)phi),
-                        [&] {
-                          pcg_iteration_phi<S>(Aphi, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s);
-                        },
-                        P.max_iteration, true));
+        CKS(drive_pcg(c, std::make_pair(2, (const void*)nullptr),
+                      [&] { pcg_iteration_stored32(A, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s); },
+                      P.max_iteration, true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
         const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
@@ -782,8 +689,6 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
   c->debug = std::getenv("FS_DEBUG") != nullptr;
-  c->stored32 = std::getenv("FS_STORED32") != nullptr;
-  c->pure32 = std::getenv("FS_PURE32") != nullptr;
   c->Lc = make_lay(grid->nx, grid->ny, grid->nz);
   c->Lu = make_lay(grid->nx + 1, grid->ny, grid->nz);
   c->Lv = make_lay(grid->nx, grid->ny + 1, grid->nz);

@@ -67,20 +67,8 @@ template <class V, class R = V>
 void pcg_init(const Op7<V>& A, const R* b, R* x, R* r, V* p, PcgState* st, double* partials, cudaStream_t s);
 template <class V, class R = V>
 void pcg_iteration(const Op7<V>& A, R* x, R* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
-// Pressure operator evaluated from phi on the fly (mixed-precision solve):
-// face coefficients beta_f in FP64 from the stored level set, so the FP32
-// Krylov sequence applies exactly the operator of the FP64 defect residual.
-// diag (FP32) is used only by the Jacobi preconditioner.
-template <class T> struct OpPhi {
-  const T* phi;
-  const float* diag;
-  Lay L;
-  double rn, rp, inv2;  // densities of the phi <= 0 / phi > 0 phases, 1/dx^2
-};
-template <class T>
-void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, double* q, PcgState* st, double* partials,
-                       cudaStream_t s);
-
+// Mixed-precision iteration: FP32 couplings and search direction, FP64
+// iterate x, residual r and q = A p.
 void pcg_iteration_stored32(const Op7<float>& A, double* x, double* r, float* p, double* q, PcgState* st,
                             double* partials, cudaStream_t s);
 

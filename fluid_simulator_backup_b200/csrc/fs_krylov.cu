@@ -311,40 +311,6 @@ void pcg_iteration(const Op7<V>& A, RT* x, RT* r, V* p, V* q, PcgState* st, doub
   k_pcg_pupdate<V, RT><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
 }
 
-template <class T>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_spmv_phi(OpPhi<T> A, const float* __restrict__ p,
-                                                              double* __restrict__ q, PcgState* st, double* partials) {
-  if (((volatile PcgState*)st)->done) return;
-  const int64_t sy = A.L.px, sz = A.L.slab;
-  const double vn = 1.0 / A.rn, vp = 1.0 / A.rp;
-  double pq = 0.0;
-  Cursor cur;
-  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
-    const int i = cur.i, j = cur.j, k = cur.k;
-    const int64_t c = A.L.at(i, j, k);
-    const double pc = (double)A.phi[c], xc = (double)p[c];
-    double acc = 0.0;
-    if (i > 0) acc += face_coef(pc, (double)A.phi[c - 1], vn, vp) * (xc - (double)p[c - 1]);
-    if (i < A.L.nx - 1) acc += face_coef(pc, (double)A.phi[c + 1], vn, vp) * (xc - (double)p[c + 1]);
-    if (j > 0) acc += face_coef(pc, (double)A.phi[c - sy], vn, vp) * (xc - (double)p[c - sy]);
-    if (j < A.L.ny - 1) acc += face_coef(pc, (double)A.phi[c + sy], vn, vp) * (xc - (double)p[c + sy]);
-    if (k > 0) acc += face_coef(pc, (double)A.phi[c - sz], vn, vp) * (xc - (double)p[c - sz]);
-    if (k < A.L.nz - 1) acc += face_coef(pc, (double)A.phi[c + sz], vn, vp) * (xc - (double)p[c + sz]);
-    if (i == 0 && j == 0 && k == 0) {
-      // deflation: the first cell's bottom and down Neumann ghosts
-      const double vc = pc <= 0.0 ? vn : vp, ac = fabs(pc);
-      const double gb = fabs(2.0 * pc - (double)A.phi[c + sy]), gd = fabs(2.0 * pc - (double)A.phi[c + sz]);
-      acc += (vc * vc * (gb + ac) / (vc * gb + vc * ac) + vc * vc * (gd + ac) / (vc * gd + vc * ac)) * xc;
-    }
-    const double qv = A.inv2 * acc;
-    q[c] = qv;
-    pq += xc * qv;
-  }
-  pq = block_sum(pq);
-  double tot;
-  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) st->pq = tot;
-}
-
 // Stored-coefficient variant of the mixed iteration: FP32 face couplings in
 // flux form, evaluated in FP64, q in FP64.
 template <class V>
@@ -376,22 +342,6 @@ void pcg_iteration_stored32(const Op7<float>& A, double* x, double* r, float* p,
   k_pcg_update<float, double, double><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
   k_pcg_pupdate<float, double><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
 }
-
-template <class T>
-void pcg_iteration_phi(const OpPhi<T>& A, double* x, double* r, float* p, double* q, PcgState* st, double* partials,
-                       cudaStream_t s) {
-  const int nb = pcg_blocks(A.L);
-  Op7<float> D{nullptr, nullptr, nullptr, A.diag, A.L};
-  // the on-the-fly operator needs 58 registers: 4 resident blocks per SM
-  k_pcg_spmv_phi<T><<<std::min(nb, 4 * g_sm_count), kRedThreads, 0, s>>>(A, p, q, st, partials);
-  k_pcg_update<float, double, double><<<nb, kRedThreads, 0, s>>>(D, x, r, p, q, st, partials);
-  k_pcg_pupdate<float, double><<<nb, kRedThreads, 0, s>>>(D, r, p, st);
-}
-
-template void pcg_iteration_phi<float>(const OpPhi<float>&, double*, double*, float*, double*, PcgState*, double*,
-                                       cudaStream_t);
-template void pcg_iteration_phi<double>(const OpPhi<double>&, double*, double*, float*, double*, PcgState*, double*,
-                                        cudaStream_t);
 
 template <class V, class RT>
 void pcg_resume(const Op7<V>& A, const RT* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s) {
