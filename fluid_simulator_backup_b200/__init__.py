@@ -33,7 +33,7 @@ FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
             "fs_memory_bytes", "fs_upload", "fs_download", "fs_upload_device", "fs_download_device", "fs_step",
             "fs_cfl_dt", "fs_project", "fs_advect_levelset", "fs_advect_velocity", "fs_reinitialize",
-            "fs_viscosity", "fs_pcg_csr")
+            "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc")
 
 
 class FsError(RuntimeError):
@@ -118,6 +118,8 @@ def lib():
         L.fs_viscosity.argtypes = [vp, ctypes.c_double, ip]
         L.fs_pcg_csr.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
                                  ctypes.c_int, ip, dp]
+        L.fs_pcg_csr_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_int, vp, ip, dp]
         for name in EXPORTED:
             if name not in ("fs_params_default", "fs_status_str", "fs_last_error"):
                 getattr(L, name).restype = ctypes.c_int

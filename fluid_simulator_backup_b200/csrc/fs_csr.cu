@@ -8,6 +8,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/fluid_b200.h"
@@ -207,6 +208,110 @@ extern "C" fs_status fs_pcg_csr(fs_ctx* ctx, int n, int nnz, const double* value
   cudaFree(dq); cudaFree(dd); cudaFree(part); cudaFree(st);
   cudaStreamDestroy(s);
   if (result != FS_OK) return result;
+  if (iterations) *iterations = host.iter;
+  if (residual) *residual = stop == FS_STOP_ABSOLUTE ? std::sqrt(host.rz) : (host.bb > 0 ? std::sqrt(host.rr / host.bb) : 0.0);
+  if (host.status == 3) return FS_NONFINITE;
+  if (host.status == 2) return FS_NOT_CONVERGED;
+  return FS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.
+//
+// Some callers cannot allocate device memory when they solve: a host that
+// owns a fixed device memory pool (an FFI/JNI embedding whose allocator is
+// not ours), a real-time loop that must not take cudaMalloc's implicit
+// device synchronisation, or code that runs the solve between other work it
+// has already sized.  fs_pcg_csr_noalloc gives them the same Jacobi-PCG as
+// fs_pcg_csr on matrices and vectors they already hold in device memory; its
+// working vectors live in one file-scope __device__ array of fixed size
+// (kNoAllocMaxRows rows, about 8.4 MB), held by every GPU that loads the
+// library until the process exits.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kNoAllocMaxRows = 1 << 18;  // 262144 rows: a 64^3 pressure system
+
+struct NoAllocScratch {
+  double r[kNoAllocMaxRows];
+  double p[kNoAllocMaxRows];
+  double q[kNoAllocMaxRows];
+  double dinv[kNoAllocMaxRows];
+  double partials[8];
+  CsrState st;
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+NoAllocScratch* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array for the current device.  In host code
+// the symbol is only a host-side stand-in, so the address is looked up once
+// per device (with that device current) and cached.
+fs_status noalloc_scratch(NoAllocScratch** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FS_CUDA_ERROR;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return FS_CUDA_ERROR;
+    g_noalloc_ptr[dev] = static_cast<NoAllocScratch*>(ptr);
+  }
+  *out = g_noalloc_ptr[dev];
+  return FS_OK;
+}
+
+}  // namespace
+
+extern "C" fs_status fs_pcg_csr_noalloc(int n, int nnz, const double* values, const int* column_index,
+                                        const int* row_ptr, const double* b, double* x, double tolerance,
+                                        int max_iteration, int stop, void* stream, int* iterations,
+                                        double* residual) {
+  if (n <= 0 || nnz <= 0 || !values || !column_index || !row_ptr || !b || !x || max_iteration < 0 ||
+      (stop != FS_STOP_RELATIVE && stop != FS_STOP_ABSOLUTE)) {
+    return FS_INVALID_ARG;
+  }
+  if (n > kNoAllocMaxRows) return FS_INVALID_ARG;  // beyond the fixed scratch: use fs_pcg_csr
+  NoAllocScratch* sc = nullptr;
+  fs_status st0 = noalloc_scratch(&sc);
+  if (st0 != FS_OK) return st0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CsrState host{};
+  host.tol = tolerance;
+  host.max_iter = max_iteration;
+  host.criterion = stop;
+  auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+  // the scratch keeps the previous call's contents: clear the accumulators
+  if (!ok(cudaMemsetAsync(sc->partials, 0, sizeof(sc->partials), s)) ||
+      !ok(cudaMemcpyAsync(&sc->st, &host, sizeof(CsrState), cudaMemcpyHostToDevice, s))) {
+    return FS_CUDA_ERROR;
+  }
+  const int T = 256, B = (n + T - 1) / T;
+  k_csr_init<<<B, T, 0, s>>>(n, values, column_index, row_ptr, b, x, sc->r, sc->p, sc->dinv, sc->partials, &sc->st);
+  k_csr_start<<<1, 1, 0, s>>>(sc->partials, &sc->st);
+  if (!ok(cudaGetLastError())) return FS_CUDA_ERROR;
+  const int batches = max_iteration / 16 + 2;
+  for (int bt = 0; bt < batches; ++bt) {
+    if (!ok(cudaMemcpyAsync(&host, &sc->st, sizeof(CsrState), cudaMemcpyDeviceToHost, s)) ||
+        !ok(cudaStreamSynchronize(s))) {
+      return FS_CUDA_ERROR;
+    }
+    if (host.done) break;
+    for (int it = 0; it < 16; ++it) {
+      k_csr_spmv<<<B, T, 0, s>>>(n, values, column_index, row_ptr, sc->p, sc->q, sc->partials, &sc->st);
+      k_csr_update<<<B, T, 0, s>>>(n, x, sc->r, sc->p, sc->q, sc->dinv, sc->partials, &sc->st);
+      k_csr_decide<<<1, 1, 0, s>>>(sc->partials, &sc->st);
+      k_csr_pupdate<<<B, T, 0, s>>>(n, sc->p, sc->r, sc->dinv, sc->partials, &sc->st);
+    }
+    if (!ok(cudaGetLastError())) return FS_CUDA_ERROR;
+  }
+  if (!ok(cudaMemcpyAsync(&host, &sc->st, sizeof(CsrState), cudaMemcpyDeviceToHost, s)) ||
+      !ok(cudaStreamSynchronize(s))) {
+    return FS_CUDA_ERROR;
+  }
   if (iterations) *iterations = host.iter;
   if (residual) *residual = stop == FS_STOP_ABSOLUTE ? std::sqrt(host.rz) : (host.bb > 0 ? std::sqrt(host.rr / host.bb) : 0.0);
   if (host.status == 3) return FS_NONFINITE;

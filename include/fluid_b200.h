@@ -162,6 +162,25 @@ fs_status fs_pcg_csr(fs_ctx* ctx, int n, int nnz, const double* values, const in
                      const int* row_ptr, const double* b, double* x, double tolerance, int max_iteration,
                      int stop, int* iterations, double* residual);
 
+/* Allocation-free fs_pcg_csr, for callers that cannot allocate device
+ * memory during a solve (a host whose device memory pool is owned by another
+ * runtime, a real-time loop that must not take cudaMalloc's implicit
+ * synchronisation).  No counterpart in the reference: it is an addition of
+ * this library.  Every pointer is DEVICE memory the caller owns: the CSR
+ * matrix (values, column_index, row_ptr), b, and x (initial guess in, result
+ * out); stream may be NULL (the legacy default stream).  The working vectors
+ * live in one fixed device array of the library (n <= 262144 rows, about
+ * 8.4 MB on every GPU that loads the library, kept until the process exits);
+ * larger systems are rejected with FS_INVALID_ARG.  The first call on a
+ * device looks up that array's device address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (from
+ * several host threads or streams) race and must not be issued.  Every row
+ * needs a nonzero diagonal (not checked here; a zero diagonal ends the solve
+ * with FS_NONFINITE).  No device or host memory is allocated. */
+fs_status fs_pcg_csr_noalloc(int n, int nnz, const double* values, const int* column_index, const int* row_ptr,
+                             const double* b, double* x, double tolerance, int max_iteration, int stop,
+                             void* stream, int* iterations, double* residual);
+
 #ifdef __cplusplus
 }
 #endif

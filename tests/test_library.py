@@ -66,6 +66,18 @@ def test_pcg_csr_validates_the_matrix_on_the_host():
     assert s == fs.FS_INVALID_ARG
 
 
+def test_pcg_csr_noalloc_rejects_bad_arguments_on_the_host():
+    # argument checks and the fixed-scratch row limit come before any device
+    # work, so they answer without a GPU (the pointers are never dereferenced)
+    L = fs.lib()
+    fake = 256
+    args = (fake, fake, fake, fake, fake, 1e-8, 10, fs.FS_STOP_RELATIVE, None, None, None)
+    assert L.fs_pcg_csr_noalloc((1 << 18) + 1, 7, *args) == fs.FS_INVALID_ARG
+    assert L.fs_pcg_csr_noalloc(0, 7, *args) == fs.FS_INVALID_ARG
+    assert L.fs_pcg_csr_noalloc(8, 7, None, *args[1:]) == fs.FS_INVALID_ARG
+    assert L.fs_pcg_csr_noalloc(8, 7, *args[:7], 5, None, None, None) == fs.FS_INVALID_ARG
+
+
 @pytest.mark.parametrize("name", ["3D_script.sim", "3D_script_1.sim"])
 def test_script_reader_reads_reference_scripts(name):
     path = "/root/reference/" + name
