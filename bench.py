@@ -33,8 +33,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_UNKNOWN_PCG_FP32 = 92  # spmv 24 (p32, 3 couplings32; q64) + update 48 (x64, r64 rw; p32, q64, diag32) + direction 20
-BYTES_PER_UNKNOWN_PCG_FP64 = 136
+# algorithmic bytes per unknown and PCG iteration (each array element once per pass)
+# FP32+refine: spmv 20 (p, ax, ay, az read; q write) + residual update 16 (r, q, diag read; r write)
+#              + direction update 32 (x64 read/write, p read/write, r, diag read)
+BYTES_PER_UNKNOWN_PCG_FP32 = 68
+# FP64: spmv 40 + residual update 32 + direction update 48
+BYTES_PER_UNKNOWN_PCG_FP64 = 120
 
 
 def scene(n):

@@ -6,6 +6,11 @@
 // therefore never branch on the box boundary: ghost values are written by a
 // ghost-fill kernel (level set: linear extrapolation) or are permanently zero
 // (velocity ghosts, pressure-solve vector ghosts, coefficient faces on walls).
+// In x the interior starts at column 4 (one unused column before the three
+// ghosts) and the row pitch px is a multiple of 4, so every interior row
+// starts on a 16-byte boundary for FP32 and a 32-byte boundary for FP64:
+// the streaming kernels move x-aligned groups of four cells with vector
+// loads and stores.
 // The reference stores the same x-fastest order (ARRAY_3D.h:98) with ghost
 // widths 2-3 per field (EULERIAN_FLUID_SOLVER_3D.h:405-431).
 #pragma once
@@ -16,21 +21,22 @@
 namespace fsb {
 
 constexpr int GH = 3;  // ghost width
+constexpr int GX = 4;  // column of i = 0 within a row (ghosts at GX-3 .. GX-1)
 
 struct Lay {
   int nx, ny, nz;   // interior extent
-  int px, py;       // padded extent in x and y
+  int px, py;       // padded extent in x (a multiple of 4) and y
   int64_t slab;     // px*py
   int64_t total;    // px*py*(nz+2*GH)
   __host__ __device__ int64_t at(int i, int j, int k) const {
-    return ((int64_t)(k + GH) * py + (j + GH)) * px + (i + GH);
+    return ((int64_t)(k + GH) * py + (j + GH)) * px + (i + GX);
   }
 };
 
 inline Lay make_lay(int nx, int ny, int nz) {
   Lay l;
   l.nx = nx; l.ny = ny; l.nz = nz;
-  l.px = nx + 2 * GH;
+  l.px = (nx + GX + GH + 3) / 4 * 4;
   l.py = ny + 2 * GH;
   l.slab = (int64_t)l.px * l.py;
   l.total = l.slab * (nz + 2 * GH);

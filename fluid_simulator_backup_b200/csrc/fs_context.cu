@@ -78,7 +78,7 @@ struct fs_ctx {
   void *u0 = nullptr, *v0 = nullptr, *w0 = nullptr;
   void *ua = nullptr, *va = nullptr, *wa = nullptr;
   // pressure (FP64) and projection work
-  double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *r64 = nullptr, *p64bak = nullptr, *qd = nullptr;
+  double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *p64bak = nullptr;
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
@@ -102,6 +102,7 @@ struct fs_ctx {
   int pcg_launched_iterations = 0;
   cudaEvent_t evp0 = nullptr, evp1 = nullptr;
   bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
+  double reliable_delta = 0.1;  // residual drop between reliable updates (FS_RELIABLE_DELTA to sweep)
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -225,7 +226,7 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   c->launches += 1;
   CK(cudaGetLastError());
   CKS(drive_pcg(c, std::make_pair(key, (const void*)nullptr),
-                [&] { pcg_iteration<V, V>(A, x, r, p, q, c->st, c->partials, c->stream); }, max_iter, timed));
+                [&] { cg_iteration<V, V>(A, x, r, p, q, c->st, c->partials, c->stream); }, max_iter, timed));
   if (timed) {
     CK(cudaEventRecord(c->evp1, c->stream));
     CK(cudaEventSynchronize(c->evp1));
@@ -403,10 +404,11 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
     const size_t vbytes = c->Lc.total * sizeof(float);
     double bb = 0.0;
-    // true FP64 residual b - A64 (p64 [+ x32]) with A64 evaluated from phi in
-    // FP64; it lands in r64, the Krylov residual of the mixed solve
+    float *r32 = (float*)c->pr, *p32 = (float*)c->pp, *q32 = (float*)c->pq;
+    // true FP64 residual b - A64 p64 with A64 evaluated from phi in FP64; its
+    // FP32 image lands in r32, the Krylov residual of the mixed solve
     auto defect = [&](const float* x32, double* rel_out) -> fs_status {
-      defect_residual<S>(phi, c->p64, x32, c->b64, c->r64, nullptr, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
+      defect_residual<S>(phi, c->p64, x32, c->b64, nullptr, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
                          c->tickets + 2, c->scalars + 2, s);
       c->launches += 1;
       CK(cudaGetLastError());
@@ -425,42 +427,40 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     CKS(defect(nullptr, &rel));
     st = PCG_CONVERGED;
     if (rel > P.tolerance) {
-      // Mixed-precision CG: the FP64 pressure p64 is the iterate, r64 the
-      // residual and q = A p is kept in FP64 (FP64 recurrences); the face
-      // couplings and the search direction p are FP32 (the flux-form
-      // operator is evaluated in FP64 from them: 92 bytes per unknown and
-      // iteration against 136 for the FP64 solve).  Every time
-      // the recursive residual drops a decade the true FP64 residual replaces
-      // it (reliable update).  A sequence is trusted for a reduction of
-      // inner_tolerance, then restarted from the true residual; a sequence
-      // whose true residual got worse is rolled back to the last accepted
-      // pressure and restarted.
+      // Mixed-precision CG: the FP64 pressure p64 is the iterate; the face
+      // couplings, the residual r, the search direction p and q = A p are
+      // FP32 (the flux-form operator is evaluated in FP64 arithmetic from
+      // them): 68 bytes per unknown and iteration against 120 for the FP64
+      // solve.  Every time the recursive residual drops by reliable_delta
+      // the true FP64 residual of p64 replaces it (reliable update), keeping
+      // the search direction; the recursion stops at the tolerance itself
+      // and the true residual decides.  A sequence whose true residual got
+      // worse is rolled back to the last accepted pressure and restarted.
       const size_t pbytes = c->Lc.total * sizeof(double);
       CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
       PcgState init{};
       init.criterion = 2;  // absolute 2-norm of the recursive residual, in b's units
-      init.tol = 0.5 * P.tolerance * std::sqrt(bb);
+      init.tol = P.tolerance * std::sqrt(bb);
       init.max_iter = P.max_iteration;
-      init.reliable_delta = 0.1;
+      init.reliable_delta = c->reliable_delta;
       init.bb = bb;  // ||b||^2 of the pressure system, for the recursive relative residual
       *c->st_host = init;
       CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
       CK(cudaEventRecord(c->evp0, s));
-      // r64 already holds b - A p64; with x = p64 the init recomputes it in
-      // the FP32 operator, so start from the true one instead: x = 0 image
-      pcg_resume<float, double>(A, c->r64, (float*)c->pp, c->st, c->partials, 1, s);
+      // r32 already holds the image of b - A p64: start the recursion from it
+      pcg_resume<float, float>(A, r32, p32, c->st, c->partials, 1, s);
       c->launches += 2;
       int failures = 0;
       double best = rel;
       for (;;) {
         CKS(drive_pcg(c, std::make_pair(2, (const void*)nullptr),
-                      [&] { pcg_iteration_stored32(A, c->p64, c->r64, (float*)c->pp, c->qd, c->st, c->partials, s); },
+                      [&] { cg_iteration<float, double>(A, c->p64, r32, p32, q32, c->st, c->partials, s); },
                       P.max_iteration, true));
         const int status = c->st_host->status;
         iters = c->st_host->iter;
         const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
         double now = 0.0;
-        CKS(defect(nullptr, &now));  // r64 <- true residual of the current pressure
+        CKS(defect(nullptr, &now));  // r32 <- true residual of the current pressure
         bool restart = false;
         if (!std::isfinite(now) || now > 100.0 * best) {
           // diverged (not a CG residual oscillation): back to the best pressure
@@ -489,7 +489,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
           st = PCG_MAXITER;
           break;
         }
-        pcg_resume<float, double>(A, c->r64, (float*)c->pp, c->st, c->partials, restart ? 1 : 0, s);
+        pcg_resume<float, float>(A, r32, p32, c->st, c->partials, restart ? 1 : 0, s);
         c->launches += 2;
         CK(cudaGetLastError());
       }
@@ -689,6 +689,10 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
   c->debug = std::getenv("FS_DEBUG") != nullptr;
+  if (const char* e = std::getenv("FS_RELIABLE_DELTA")) {  // tuning knob for sweeps
+    const double v = std::atof(e);
+    if (v > 0.0 && v < 1.0) c->reliable_delta = v;
+  }
   c->Lc = make_lay(grid->nx, grid->ny, grid->nz);
   c->Lu = make_lay(grid->nx + 1, grid->ny, grid->nz);
   c->Lv = make_lay(grid->nx, grid->ny + 1, grid->nz);
@@ -716,9 +720,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   for (void** p : fw) if ((s = dalloc(c, p, wb)) != FS_OK) return fail(s);
   double** d8[] = {&c->p64, &c->b64, &c->div64};
   for (double** p : d8) if ((s = dalloc(c, (void**)p, c8)) != FS_OK) return fail(s);
-  if (c->fp32 && (s = dalloc(c, (void**)&c->r64, c8)) != FS_OK) return fail(s);
   if (c->fp32 && (s = dalloc(c, (void**)&c->p64bak, c8)) != FS_OK) return fail(s);
-  if (c->fp32 && (s = dalloc(c, (void**)&c->qd, c8)) != FS_OK) return fail(s);
   void** pv[] = {&c->pax, &c->pay, &c->paz, &c->pdiag, &c->pr, &c->pp, &c->pq};
   for (void** p : pv) if ((s = dalloc(c, p, cv)) != FS_OK) return fail(s);
   if (c->fp32) {
@@ -731,7 +733,12 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
       for (int m = 0; m < 9; ++m)
         if ((s = dalloc(c, &c->vs[a][m], fb[a])) != FS_OK) return fail(s);
   }
-  const int nblk = std::max(pcg_blocks(c->Lu), std::max(pcg_blocks(c->Lv), pcg_blocks(c->Lw))) * 2 + 64;
+  // grid sizes of the Krylov kernels (occupancy queries; never under capture)
+  cg_prepare<double, double>();
+  cg_prepare<float, double>();
+  cg_prepare<float, float>();
+  int nblk = std::max(pcg_blocks(c->Lu), std::max(pcg_blocks(c->Lv), pcg_blocks(c->Lw))) * 2 + 64;
+  for (const Lay* L : {&c->Lc, &c->Lu, &c->Lv, &c->Lw}) nblk = std::max(nblk, cg_max_blocks(*L));
   if ((s = dalloc(c, (void**)&c->partials, (size_t)nblk * 3 * sizeof(double))) != FS_OK) return fail(s);
   if ((s = dalloc(c, (void**)&c->tickets, 8 * sizeof(unsigned int))) != FS_OK) return fail(s);
   if ((s = dalloc(c, (void**)&c->scalars, 16 * sizeof(double))) != FS_OK) return fail(s);

@@ -30,9 +30,12 @@ struct PcgState {
   double max_rr;          // r.r of the last true residual (reference of the reliable-update trigger)
   double rz_prev;         // r.z at the start of the last accepted step
   double reliable_delta;  // pause for a true residual when ||r|| < delta*max||r|| (0: never)
+  double alpha;           // step length of the current iteration (set by the SpMV)
   int iter, max_iter, done, criterion, status, stall;
   int stall_limit;  // iterations without a 1% improvement of best_rr before giving up (0: never)
+  int x_pending;    // alpha is set and x += alpha p is still due (applied by the direction update)
   unsigned int ticket;
+  unsigned int ticket2;  // completion count of the direction update
 };
 
 // STAGNATED: the iteration can make no further progress in its arithmetic
@@ -65,12 +68,16 @@ template <class V> struct Op7 {
 
 template <class V, class R = V>
 void pcg_init(const Op7<V>& A, const R* b, R* x, R* r, V* p, PcgState* st, double* partials, cudaStream_t s);
-template <class V, class R = V>
-void pcg_iteration(const Op7<V>& A, R* x, R* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
-// Mixed-precision iteration: FP32 couplings and search direction, FP64
-// iterate x, residual r and q = A p.
-void pcg_iteration_stored32(const Op7<float>& A, double* x, double* r, float* p, double* q, PcgState* st,
-                            double* partials, cudaStream_t s);
+// One iteration with the iterate update deferred into the direction update
+// (x of type X, r, p, q and the operator of type V): SpMV + alpha, residual
+// update + beta, then x += alpha p and p = z + beta p in one pass over p.
+template <class V, class X>
+void cg_iteration(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+// Occupancy queries that size cg_iteration's grids: call once per (V, X)
+// before the first iteration (outside stream capture).
+template <class V, class X> void cg_prepare();
+// Largest block count of the cg_iteration kernels on a layout (partial sums).
+int cg_max_blocks(const Lay& L);
 
 template <class V, class R = V>
 void pcg_resume(const Op7<V>& A, const R* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);

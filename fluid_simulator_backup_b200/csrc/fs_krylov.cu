@@ -2,35 +2,31 @@
 // operator (PCG_METHOD.cpp:4-126 restated for the GPU), with optional
 // reliable updates for the mixed-precision pressure solve.
 //
-// Vector types: V for the operator, the search direction p and q = A p; R
-// for the iterate x, the residual r and the right-hand side b.  V = R = double is
-// the FP64 path, V = R = float the viscosity solves in FP32 storage, and
-// V = float, R = double the mixed-precision pressure solve: the residual
-// recurrences x += alpha p, r -= alpha q and all scalars stay in FP64
-// while every operator application streams FP32 (88 bytes per unknown and
-// iteration).  FP32 rounding of x, r or q would be amplified by ||A|| or
-// by the transient growth of the CG residual; rounding of p only perturbs
-// the search direction, and q is computed from the rounded p itself.
+// Vector types: V for the operator, the residual r, the search direction p
+// and q = A p; X for the iterate x.  V = X = double is the FP64 path,
+// V = X = float the viscosity solves in FP32 storage, and V = float,
+// X = double the mixed-precision pressure solve, whose iterate is the FP64
+// pressure itself.  The scalars (alpha, beta, r.z, r.r) are FP64 always.
 //
-// One iteration is three kernels:
-//   spmv    q = A p and p.q                      (reads p, ax, ay, az, diag; writes q)
-//   update  x += alpha p, r -= alpha q, r.z, r.r (reads x, p, r, q, diag; writes x, r)
-//   pupdate p = r/diag + beta p                  (reads r, diag, p; writes p)
-// z = r/diag is never stored: 68 bytes per unknown and iteration in FP32,
-// 136 in FP64.  The kernels run grid-stride over a grid of a few blocks per
-// SM; dot products are reduced in FP64 per block and finished by the last
-// block (deterministic for a given grid), which also takes the scalar
-// decisions (alpha, beta, convergence, caps, breakdown) and writes them to
-// the PcgState in device memory.  Every kernel starts by reading `done`, so
-// iterations captured in a CUDA graph cost microseconds once a solve stops.
+// One iteration is three kernels (details at k_cg_spmv below):
+//   spmv    q = A p, p.q, alpha                (reads p, ax, ay, az; writes q)
+//   update  r -= alpha q, r.z, r.r, beta       (reads r, q, diag; writes r)
+//   pupdate x += alpha p, p = r/diag + beta p  (reads x, p, r, diag; writes x, p)
+// z = r/diag is never stored: 68 bytes per unknown and iteration with FP32
+// vectors and an FP64 iterate, 120 in FP64.  Dot products are reduced in
+// FP64 per block and finished by the last block (deterministic for a given
+// grid), which also takes the scalar decisions (alpha, beta, convergence,
+// caps, breakdown) and writes them to the PcgState in device memory.  Every
+// kernel starts by reading `done`, so iterations captured in a CUDA graph
+// cost microseconds once a solve stops.
 //
 // Reliable updates (Clark et al., "Solving lattice QCD systems of equations
 // using mixed precision solvers on GPUs", 2010): in the FP32 pressure solve
 // the update kernel pauses the iteration (done = 2) whenever the recursive
 // residual has dropped by `reliable_delta` since the last true residual; the
-// host then folds x into the FP64 pressure, recomputes the true residual in
-// FP64 and resumes the same Krylov iteration (pcg_resume) with that residual,
-// keeping the search direction.  The FP32 iteration therefore converges like
+// host then recomputes the true residual of the FP64 pressure in FP64 and
+// resumes the same Krylov iteration (pcg_resume) with that residual, keeping
+// the search direction.  The FP32 iteration therefore converges like
 // one long CG instead of a sequence of restarted ones.
 #include <algorithm>
 #include <cstdlib>
@@ -173,86 +169,6 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_init(Op7<V> A, const RT* b,
   }
 }
 
-template <class V>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(Op7<V> A, const V* __restrict__ p, V* __restrict__ q,
-                                                          PcgState* st, double* partials) {
-  if (((volatile PcgState*)st)->done) return;
-  double pq = 0.0;
-  Cursor cur;
-  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
-    const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-    const V qv = apply7<V, V>(A, p, c);
-    q[c] = qv;
-    pq += (double)p[c] * (double)qv;  // p.q of the stored (rounded) q, as the update uses it
-  }
-  pq = block_sum(pq);
-  double tot;
-  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) st->pq = tot;
-}
-
-template <class V, class RT, class Q = V>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_update(Op7<V> A, RT* __restrict__ x, RT* __restrict__ r,
-                                                            const V* __restrict__ p, const Q* __restrict__ q,
-                                                            PcgState* st, double* partials) {
-  if (((volatile PcgState*)st)->done) return;
-  const double pq_all = ((volatile PcgState*)st)->pq;
-  const double alpha = ((volatile PcgState*)st)->rz / pq_all;
-  // a non-positive p.Ap (or an infinite step) means the iteration has lost
-  // its footing in this arithmetic: keep the iterate, stop (uniform branch)
-  const bool breakdown = !(pq_all > 0.0) || !isfinite(alpha);
-  const RT ar = (RT)alpha;
-  double rz = 0.0, rr = 0.0;
-  if (!breakdown) {
-    Cursor cur;
-    for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
-      const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-      x[c] += ar * (RT)p[c];
-      const RT rv = r[c] - ar * (RT)q[c];
-      r[c] = rv;
-      rz += (double)rv * (double)(rv / (RT)A.diag[c]);
-      rr += (double)rv * (double)rv;
-    }
-  }
-  double tot[3];
-  if (grid_reduce3(rz, rr, 0.0, partials, &st->ticket, tot)) {
-    if (breakdown) {
-      st->status = PCG_STAGNATED;
-      st->done = 1;
-      return;
-    }
-    const double rz_old = st->rz;
-    st->rr = tot[1];
-    st->rz_prev = rz_old;
-    st->rz = tot[0];
-    if (tot[1] < 0.99 * st->best_rr) {
-      st->best_rr = tot[1];
-      st->stall = 0;
-    } else {
-      st->stall += 1;
-    }
-    if (!isfinite(tot[0]) || !isfinite(tot[1])) {
-      st->status = PCG_NONFINITE;
-      st->done = 1;
-    } else if (stop_test(st, tot[0], tot[1])) {
-      st->status = PCG_CONVERGED;
-      st->done = 1;
-    } else {
-      st->beta = tot[0] / rz_old;
-      st->iter += 1;
-      if (st->iter >= st->max_iter) {
-        st->status = PCG_MAXITER;
-        st->done = 1;
-      } else if (st->stall_limit > 0 && st->stall >= st->stall_limit) {
-        st->status = PCG_STAGNATED;
-        st->done = 1;
-      } else if (st->reliable_delta > 0.0 && tot[1] < st->reliable_delta * st->reliable_delta * st->max_rr) {
-        st->status = PCG_RELIABLE_UPDATE;  // pause before the direction update
-        st->done = 2;
-      }
-    }
-  }
-}
-
 template <class V, class RT>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_pupdate(Op7<V> A, const RT* __restrict__ r, V* __restrict__ p,
                                                              PcgState* st) {
@@ -304,55 +220,359 @@ void pcg_init(const Op7<V>& A, const RT* b, RT* x, RT* r, V* p, PcgState* st, do
 }
 
 template <class V, class RT>
-void pcg_iteration(const Op7<V>& A, RT* x, RT* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
-  const int nb = pcg_blocks(A.L);
-  k_pcg_spmv<V><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
-  k_pcg_update<V, RT><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
-  k_pcg_pupdate<V, RT><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
-}
-
-// Stored-coefficient variant of the mixed iteration: FP32 face couplings in
-// flux form, evaluated in FP64, q in FP64.
-template <class V>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_spmv_q64(Op7<V> A, const V* __restrict__ p, double* __restrict__ q,
-                                                              PcgState* st, double* partials) {
-  if (((volatile PcgState*)st)->done) return;
-  const int64_t sy = A.L.px, sz = A.L.slab;
-  double pq = 0.0;
-  Cursor cur;
-  for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
-    const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-    const double d = (double)p[c];
-    double acc = (double)A.ax[c] * (d - (double)p[c - 1]) + (double)A.ax[c + 1] * (d - (double)p[c + 1]);
-    acc += (double)A.ay[c] * (d - (double)p[c - sy]) + (double)A.ay[c + sy] * (d - (double)p[c + sy]);
-    acc += (double)A.az[c] * (d - (double)p[c - sz]) + (double)A.az[c + sz] * (d - (double)p[c + sz]);
-    if (c == A.L.at(0, 0, 0)) acc += (*A.extra0) * d;
-    q[c] = acc;
-    pq += d * acc;
-  }
-  pq = block_sum(pq);
-  double tot;
-  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) st->pq = tot;
-}
-
-void pcg_iteration_stored32(const Op7<float>& A, double* x, double* r, float* p, double* q, PcgState* st,
-                            double* partials, cudaStream_t s) {
-  const int nb = pcg_blocks(A.L);
-  k_pcg_spmv_q64<float><<<nb, kRedThreads, 0, s>>>(A, p, q, st, partials);
-  k_pcg_update<float, double, double><<<nb, kRedThreads, 0, s>>>(A, x, r, p, q, st, partials);
-  k_pcg_pupdate<float, double><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
-}
-
-template <class V, class RT>
 void pcg_resume(const Op7<V>& A, const RT* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s) {
   const int nb = pcg_blocks(A.L);
   k_pcg_resume<V, RT><<<nb, kRedThreads, 0, s>>>(A, r, st, partials, restart);
   k_pcg_pupdate<V, RT><<<nb, kRedThreads, 0, s>>>(A, r, p, st);
 }
 
+// ---------------------------------------------------------------------------
+// The iteration with a deferred iterate update.
+//
+// The iterate is touched once per iteration, in the direction update that
+// reads p anyway, so the residual update streams neither p nor x.  When an
+// iteration stops in the residual update (converged, capped, paused for a
+// reliable update) the direction update still applies the pending
+// x += alpha p and leaves p alone; x_pending is cleared by the last block of
+// the direction update so that later launches of a captured batch do not
+// apply it twice.
+//
+// In the pressure solve the iterate must stay FP64: FP32 rounding of x is
+// amplified by ||A|| ||x|| / ||b||, which is of the order of the condition
+// number at density ratio 1000.  FP32 rounding of r and q only perturbs the
+// recursion by eps32 ||r|| per step (reliable updates bound what
+// accumulates), and FP32 rounding of p is harmless because q is computed
+// from the rounded p itself.
+// ---------------------------------------------------------------------------
+
+// ---- four-cell vectors along x (rows start 16/32-byte aligned, see Lay)
+template <class T> struct V4 { T a, b, c, d; };
+
+__device__ __forceinline__ V4<float> ld4(const float* p) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ V4<double> ld4(const double* p) {
+  const double2 v0 = reinterpret_cast<const double2*>(p)[0];
+  const double2 v1 = reinterpret_cast<const double2*>(p)[1];
+  return {v0.x, v0.y, v1.x, v1.y};
+}
+// stores the lanes below `valid` (4: one vector store)
+__device__ __forceinline__ void st4(float* p, const V4<float>& v, int valid) {
+  if (valid >= 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v.a, v.b, v.c, v.d);
+  } else {
+    if (valid > 0) p[0] = v.a;
+    if (valid > 1) p[1] = v.b;
+    if (valid > 2) p[2] = v.c;
+  }
+}
+__device__ __forceinline__ void st4(double* p, const V4<double>& v, int valid) {
+  if (valid >= 4) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v.a, v.b);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v.c, v.d);
+  } else {
+    if (valid > 0) p[0] = v.a;
+    if (valid > 1) p[1] = v.b;
+    if (valid > 2) p[2] = v.c;
+  }
+}
+template <class T> __device__ __forceinline__ T lane(const V4<T>& v, int m) {
+  return m == 0 ? v.a : (m == 1 ? v.b : (m == 2 ? v.c : v.d));
+}
+template <class T> __device__ __forceinline__ void set_lane(V4<T>& v, int m, T x) {
+  if (m == 0) v.a = x; else if (m == 1) v.b = x; else if (m == 2) v.c = x; else v.d = x;
+}
+
+// Grid-stride cursor over (vector, j, k): vector w covers i = 4w .. 4w+3.
+struct VecCursor {
+  Lay Lv;  // the layout with nx replaced by the number of vectors per row
+  Cursor cur;
+  __device__ __forceinline__ void init(const Lay& L) {
+    Lv = L;
+    Lv.nx = (L.nx + 3) >> 2;
+    cur.init(Lv);
+  }
+  __device__ __forceinline__ bool valid() const { return cur.valid(Lv); }
+  __device__ __forceinline__ void next() { cur.next(Lv); }
+};
+
+// ---- SpMV: q = A p with the p.q reduction and the step length.
+//
+// One thread owns four consecutive cells of a row (i = 4w .. 4w+3, j) and
+// marches up a chunk of planes k0 .. k1-1.  The z neighbours of p and the
+// upper z coupling stay in registers from one plane to the next (each plane
+// of p and az is loaded once), the x neighbours come from the adjacent lanes
+// of the warp by shuffle (global loads only at the two ends of a warp or of
+// a row) and the y neighbours are rows that the neighbouring threads of the
+// block load in the same plane (L1 hits).  Blocks are 32 x 8 threads
+// (128 x 8 cells); the grid is the xy tiles times as many z chunks as fill
+// the resident blocks of the GPU.
+template <class V>
+__device__ __forceinline__ void spmv_row4(const Op7<V>& A, const V* __restrict__ p, int64_t c, int i0,
+                                          const V4<V>& pc, const V4<V>& pdn, const V4<V>& pup, const V4<V>& azc,
+                                          const V4<V>& azu, V4<V>& q) {
+  const int64_t sy = A.L.px;
+  const int lane_id = threadIdx.x & 31;
+  const V4<V> ps = ld4(p + c - sy), pn = ld4(p + c + sy);
+  const V4<V> ayc = ld4(A.ay + c), ayn = ld4(A.ay + c + sy);
+  const V4<V> axc = ld4(A.ax + c);
+  // x neighbours: p[i0-1], p[i0+4] and ax[i0+4] from the adjacent lanes
+  V pl = __shfl_up_sync(0xffffffffu, pc.d, 1);
+  V pr = __shfl_down_sync(0xffffffffu, pc.a, 1);
+  V axr = __shfl_down_sync(0xffffffffu, axc.a, 1);
+  if (lane_id == 0) pl = p[c - 1];
+  if (lane_id == 31 || i0 + 4 >= A.L.nx) {  // warp end, or the row ends in this vector
+    pr = p[c + 4];
+    axr = A.ax[c + 4];
+  }
+  const int64_t c00 = A.L.at(0, 0, 0);
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const V xc = lane(pc, m);
+    const V xl = m == 0 ? pl : lane(pc, m - 1);
+    const V xr = m == 3 ? pr : lane(pc, m + 1);
+    const V ar = m == 3 ? axr : lane(axc, m + 1);
+    V out;
+    if (A.flux_form) {
+      // flux form in FP64 arithmetic (see apply7)
+      const double d = (double)xc;
+      double acc = (double)lane(axc, m) * (d - (double)xl) + (double)ar * (d - (double)xr);
+      acc += (double)lane(ayc, m) * (d - (double)lane(ps, m)) + (double)lane(ayn, m) * (d - (double)lane(pn, m));
+      acc += (double)lane(azc, m) * (d - (double)lane(pdn, m)) + (double)lane(azu, m) * (d - (double)lane(pup, m));
+      if (c + m == c00) acc += (*A.extra0) * d;
+      out = (V)acc;
+    } else {
+      V acc = A.diag[c + m] * xc;
+      acc -= lane(axc, m) * xl + ar * xr;
+      acc -= lane(ayc, m) * lane(ps, m) + lane(ayn, m) * lane(pn, m);
+      acc -= lane(azc, m) * lane(pdn, m) + lane(azu, m) * lane(pup, m);
+      out = acc;
+    }
+    set_lane(q, m, out);
+  }
+}
+
+template <class V>
+__global__ void __launch_bounds__(256) k_cg_spmv(Op7<V> A, const V* __restrict__ p, V* __restrict__ q,
+                                                 PcgState* st, double* partials, int kchunk) {
+  if (((volatile PcgState*)st)->done) return;
+  const Lay& L = A.L;
+  const int w = blockIdx.x * 32 + threadIdx.x;  // vector index along x
+  const int j = blockIdx.y * 8 + threadIdx.y;
+  const int i0 = 4 * w;
+  const int k0 = blockIdx.z * kchunk;
+  const int k1 = min(L.nz, k0 + kchunk);
+  // threads past the end of a row or of the box compute on a clamped row and
+  // store nothing; every thread of the warp takes part in the shuffles
+  const bool row_ok = j < L.ny && i0 < L.nx;
+  const int nvalid = row_ok ? min(4, L.nx - i0) : 0;
+  const int jj = min(j, L.ny - 1), ii = min(i0, 4 * ((L.nx - 1) >> 2));
+  const int64_t sz = L.slab;
+  double pq = 0.0;
+  if (k0 < k1) {
+    int64_t c = L.at(ii, jj, k0);
+    V4<V> pdn = ld4(p + c - sz), pc = ld4(p + c), azc = ld4(A.az + c);
+#pragma unroll 2
+    for (int k = k0; k < k1; ++k, c += sz) {
+      const V4<V> pup = ld4(p + c + sz), azu = ld4(A.az + c + sz);
+      V4<V> qv;
+      spmv_row4<V>(A, p, c, ii, pc, pdn, pup, azc, azu, qv);
+      if (nvalid > 0) {
+        st4(q + c, qv, nvalid);
+        pq += (double)pc.a * (double)qv.a;  // p.q of the stored q, as the residual update uses it
+        if (nvalid > 1) pq += (double)pc.b * (double)qv.b;
+        if (nvalid > 2) pq += (double)pc.c * (double)qv.c;
+        if (nvalid > 3) pq += (double)pc.d * (double)qv.d;
+      }
+      pdn = pc;
+      pc = pup;
+      azc = azu;
+    }
+  }
+  pq = block_sum(pq);
+  double tot;
+  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) {
+    st->pq = tot;
+    const double alpha = st->rz / tot;
+    if (!(tot > 0.0) || !isfinite(alpha)) {
+      // a non-positive p.Ap (or an infinite step): the iteration has lost its
+      // footing in this arithmetic; keep the iterate and stop
+      st->status = PCG_STAGNATED;
+      st->done = 1;
+      st->x_pending = 0;
+    } else {
+      st->alpha = alpha;
+      st->x_pending = 1;
+    }
+  }
+}
+
+// ---- residual update: r -= alpha q, r.z and r.r, beta and the decisions
+template <class V>
+__global__ void __launch_bounds__(kRedThreads) k_cg_update(Op7<V> A, V* __restrict__ r, const V* __restrict__ q,
+                                                           PcgState* st, double* partials) {
+  if (((volatile PcgState*)st)->done) return;
+  const V alpha = (V)((volatile PcgState*)st)->alpha;
+  double rz = 0.0, rr = 0.0;
+  VecCursor vc;
+  for (vc.init(A.L); vc.valid(); vc.next()) {
+    const int i0 = 4 * vc.cur.i;
+    const int64_t c = A.L.at(i0, vc.cur.j, vc.cur.k);
+    const int nvalid = min(4, A.L.nx - i0);
+    V4<V> rv = ld4(r + c);
+    const V4<V> qv = ld4(q + c), dv = ld4(A.diag + c);
+    rv.a -= alpha * qv.a;
+    rv.b -= alpha * qv.b;
+    rv.c -= alpha * qv.c;
+    rv.d -= alpha * qv.d;
+    st4(r + c, rv, nvalid);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (m < nvalid) {
+        const double rd = (double)lane(rv, m);
+        rz += rd * (rd / (double)lane(dv, m));
+        rr += rd * rd;
+      }
+    }
+  }
+  double tot[3];
+  if (grid_reduce3(rz, rr, 0.0, partials, &st->ticket, tot)) {
+    const double rz_old = st->rz;
+    st->rr = tot[1];
+    st->rz_prev = rz_old;
+    st->rz = tot[0];
+    if (tot[1] < 0.99 * st->best_rr) {
+      st->best_rr = tot[1];
+      st->stall = 0;
+    } else {
+      st->stall += 1;
+    }
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) {
+      st->status = PCG_NONFINITE;
+      st->done = 1;
+      st->x_pending = 0;  // do not move the iterate along a step that produced non-finite values
+    } else if (stop_test(st, tot[0], tot[1])) {
+      st->status = PCG_CONVERGED;
+      st->done = 1;
+    } else {
+      st->beta = tot[0] / rz_old;
+      st->iter += 1;
+      if (st->iter >= st->max_iter) {
+        st->status = PCG_MAXITER;
+        st->done = 1;
+      } else if (st->stall_limit > 0 && st->stall >= st->stall_limit) {
+        st->status = PCG_STAGNATED;
+        st->done = 1;
+      } else if (st->reliable_delta > 0.0 && tot[1] < st->reliable_delta * st->reliable_delta * st->max_rr) {
+        st->status = PCG_RELIABLE_UPDATE;  // pause before the direction update
+        st->done = 2;
+      }
+    }
+  }
+}
+
+// ---- direction update: x += alpha p (when pending), p = r/diag + beta p
+template <class V, class X>
+__global__ void __launch_bounds__(kRedThreads) k_cg_pupdate(Op7<V> A, X* __restrict__ x, const V* __restrict__ r,
+                                                            V* __restrict__ p, PcgState* st) {
+  const volatile PcgState* vs = (volatile PcgState*)st;
+  const bool move_x = vs->x_pending != 0;
+  const bool move_p = vs->done == 0;
+  if (!move_x && !move_p) return;  // uniform: every block reads the same state
+  const double alpha = vs->alpha;
+  const V beta = (V)vs->beta;
+  VecCursor vc;
+  for (vc.init(A.L); vc.valid(); vc.next()) {
+    const int i0 = 4 * vc.cur.i;
+    const int64_t c = A.L.at(i0, vc.cur.j, vc.cur.k);
+    const int nvalid = min(4, A.L.nx - i0);
+    V4<V> pv = ld4(p + c);
+    if (move_x) {
+      V4<X> xv = ld4(x + c);
+      xv.a += (X)(alpha * (double)pv.a);
+      xv.b += (X)(alpha * (double)pv.b);
+      xv.c += (X)(alpha * (double)pv.c);
+      xv.d += (X)(alpha * (double)pv.d);
+      st4(x + c, xv, nvalid);
+    }
+    if (move_p) {
+      const V4<V> rv = ld4(r + c), dv = ld4(A.diag + c);
+      pv.a = pv.a * beta + rv.a / dv.a;
+      pv.b = pv.b * beta + rv.b / dv.b;
+      pv.c = pv.c * beta + rv.c / dv.c;
+      pv.d = pv.d * beta + rv.d / dv.d;
+      st4(p + c, pv, nvalid);
+    }
+  }
+  if (move_x) {
+    // every thread of this block has read x_pending before it is counted
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned int t = atomicAdd(&st->ticket2, 1u);
+      if (t == gridDim.x - 1) {
+        st->x_pending = 0;
+        st->ticket2 = 0u;
+      }
+    }
+  }
+}
+
+namespace {
+int g_cg_blocks[2][2][3];  // [X double?][V double?][spmv, update, pupdate]: resident blocks per SM
+}
+
+template <class V, class X>
+void cg_prepare() {
+  reduction_blocks(1);  // SM count and the FS_BLOCKS_PER_SM knob
+  int* slot = g_cg_blocks[sizeof(X) == 8][sizeof(V) == 8];
+  const void* ks[3] = {(const void*)k_cg_spmv<V>, (const void*)k_cg_update<V>, (const void*)k_cg_pupdate<V, X>};
+  for (int m = 0; m < 3; ++m) {
+    if (slot[m]) continue;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ks[m], 256, 0) != cudaSuccess || nb <= 0) nb = 1;
+    slot[m] = std::min(nb, g_blocks_per_sm);
+  }
+}
+
+int cg_max_blocks(const Lay& L) {
+  const int tiles = ((L.nx + 127) / 128) * ((L.ny + 7) / 8);
+  return std::max(tiles, reduction_blocks((int64_t)1 << 40));  // the resident-block cap
+}
+
+template <class V, class X>
+void cg_iteration(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
+  const int* slot = g_cg_blocks[sizeof(X) == 8][sizeof(V) == 8];
+  const Lay& L = A.L;
+  // SpMV grid: xy tiles of 128 x 8 cells times z chunks filling the resident blocks
+  const int tx = (L.nx + 127) / 128, ty = (L.ny + 7) / 8;
+  const int want = std::max(1, slot[0]) * g_sm_count;
+  const int chunks = std::max(1, std::min(L.nz, want / (tx * ty)));
+  const int kchunk = (L.nz + chunks - 1) / chunks;
+  const dim3 sg(tx, ty, (L.nz + kchunk - 1) / kchunk);
+  k_cg_spmv<V><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
+  // pointwise kernels: grid-stride over the vectors, resident blocks only
+  const int64_t nvec = (int64_t)((L.nx + 3) >> 2) * L.ny * L.nz;
+  auto grid = [&](int per_sm) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((nvec + kRedThreads - 1) / kRedThreads,
+                                                       (int64_t)std::max(per_sm, 1) * g_sm_count));
+  };
+  k_cg_update<V><<<grid(slot[1]), kRedThreads, 0, s>>>(A, r, q, st, partials);
+  k_cg_pupdate<V, X><<<grid(slot[2]), kRedThreads, 0, s>>>(A, x, r, p, st);
+}
+
+template void cg_prepare<float, double>();
+template void cg_prepare<double, double>();
+template void cg_prepare<float, float>();
+template void cg_iteration<float, double>(const Op7<float>&, double*, float*, float*, float*, PcgState*, double*,
+                                          cudaStream_t);
+template void cg_iteration<double, double>(const Op7<double>&, double*, double*, double*, double*, PcgState*,
+                                           double*, cudaStream_t);
+template void cg_iteration<float, float>(const Op7<float>&, float*, float*, float*, float*, PcgState*, double*,
+                                         cudaStream_t);
+
 #define FS_KINST(V, RT)                                                                                           \
   template void pcg_init<V, RT>(const Op7<V>&, const RT*, RT*, RT*, V*, PcgState*, double*, cudaStream_t);       \
-  template void pcg_iteration<V, RT>(const Op7<V>&, RT*, RT*, V*, V*, PcgState*, double*, cudaStream_t);        \
   template void pcg_resume<V, RT>(const Op7<V>&, const RT*, V*, PcgState*, double*, int, cudaStream_t);
 
 FS_KINST(float, float)

@@ -155,7 +155,7 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
     }
     const double ax = inv2 * flux;
     const double rv = b[c] - ax;
-    r64[c] = rv;
+    if (r64) r64[c] = rv;
     if (r32) r32[c] = (float)rv;
     rr += rv * rv;
   }

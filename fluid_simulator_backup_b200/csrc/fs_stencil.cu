@@ -60,7 +60,7 @@ struct ExtrapField {
 // then the y slabs (interior z, full padded x), then the x slabs (interior
 // y, z).  Returns false past the end.
 __device__ __forceinline__ bool shell_coord(const Lay& L, int64_t t, int& i, int& j, int& k) {
-  const int px = L.px, py = L.py;
+  const int px = L.nx + 2 * GH, py = L.py;  // logical extents: the alignment columns are not part of the shell
   const int64_t nzs = (int64_t)2 * GH * px * py;
   if (t < nzs) {
     const int64_t s = t / ((int64_t)px * py);
@@ -94,7 +94,8 @@ __device__ __forceinline__ bool shell_coord(const Lay& L, int64_t t, int& i, int
 }
 
 inline int64_t shell_count(const Lay& L) {
-  return (int64_t)2 * GH * L.px * L.py + (int64_t)2 * GH * L.px * L.nz + (int64_t)2 * GH * L.ny * L.nz;
+  const int64_t wx = L.nx + 2 * GH;
+  return (int64_t)2 * GH * wx * L.py + (int64_t)2 * GH * wx * L.nz + (int64_t)2 * GH * L.ny * L.nz;
 }
 
 template <class T>
