@@ -39,6 +39,10 @@ sys.path.insert(0, ROOT)
 BYTES_PER_UNKNOWN_PCG_FP32 = 68
 # FP64: spmv 40 + residual update 32 + direction update 48
 BYTES_PER_UNKNOWN_PCG_FP64 = 120
+# PCG iterations per projection of the FP64 GPU path on this workload at 256^3
+# (6725 per timestep of 3 projections over steps 4-6, measured by the default
+# run's fp64 block); the reference arm prices its projection with it
+REF_PCG_ITERATIONS_256 = 2242
 
 
 def scene(n):
@@ -103,7 +107,11 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def run_steps(fs, n, precision, warmup, steps, barrier):
+def run_steps(fs, n, precision, warmup, steps, barrier, record=0):
+    """W untimed steps, then K steps timed by the library (CUDA events on its
+    stream).  With record > 0 the state before each of the first `record`
+    timed steps and its dt are kept in pinned host memory, so that the
+    end-to-end run can replay exactly the same steps."""
     import torch
     phi, u, v, w = scene(n)
     s = fs.Solver(n, 1.0 / n, params(fs, precision))
@@ -113,33 +121,36 @@ def run_steps(fs, n, precision, warmup, steps, barrier):
         s.step(s.cfl_dt(), allow_not_converged=True)
     barrier()
     torch.cuda.synchronize()
-    reps = []
-    for _ in range(steps):
+    reps, states = [], []
+    for m in range(steps):
         dt = s.cfl_dt()
+        if m < record:
+            states.append(({k: torch.from_numpy(s.download(k)).pin_memory() for k in ("phi", "u", "v", "w")}, dt))
         reps.append(s.step(dt, allow_not_converged=True))
     torch.cuda.synchronize()
     barrier()
-    return s, reps
+    return s, reps, states
 
 
-def e2e_steps(fs, s, n, steps):
-    """End to end through the public API: per step, the fields are uploaded
-    from pinned host memory, the step runs, and the level set is read back."""
+def e2e_steps(fs, s, states):
+    """End to end through the public API, on the same steps as the timed run:
+    per step, the state before it is uploaded from pinned host memory, the
+    step runs with the same dt, and the level set is read back to pinned host
+    memory.  Wall clock around the whole sequence, synchronised on both sides."""
     import torch
     shapes = {k: s.shape(k) for k in ("phi", "u", "v", "w")}
-    host = {k: torch.from_numpy(s.download(k)).pin_memory() for k in shapes}
     out = torch.empty(shapes["phi"], dtype=torch.float64).pin_memory()
     h2d = sum(int(np.prod(sh)) * 8 for sh in shapes.values())
     d2h = int(np.prod(shapes["phi"])) * 8
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(steps):
+    for host, dt in states:
         for k in ("phi", "u", "v", "w"):
             s.upload_ptr(k, host[k].data_ptr())
-        s.step(s.cfl_dt(), allow_not_converged=True)
+        s.step(dt, allow_not_converged=True)
         s.download_ptr("phi", out.data_ptr())
     torch.cuda.synchronize()
-    ms = (time.perf_counter() - t0) * 1e3 / steps
+    ms = (time.perf_counter() - t0) * 1e3 / max(len(states), 1)
     return ms, h2d, d2h
 
 
@@ -231,7 +242,7 @@ def main():
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"],
                     help="precision of the timed path (the headline is fp32_refine)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -272,7 +283,8 @@ def main():
             return
         # the FP64 PCG iteration count of this workload on the GPU path at the
         # same tolerance (measured in the default run; see profiles/)
-        iters = float(os.environ.get("FS_REF_PCG_ITERATIONS", "400"))
+        # (Jacobi-PCG iteration counts grow about linearly with n)
+        iters = float(os.environ.get("FS_REF_PCG_ITERATIONS", str(REF_PCG_ITERATIONS_256 * n / 256.0)))
         threads = 1
         ms, sample = reference_sample_isolated(n, iters, threads)
         line = {"impl": "reference", "metric": metric, "value": ms, "unit": "ms", "n_gpus": args.gpus,
@@ -292,7 +304,8 @@ def main():
         args.no_fp64 = True
         config["precision"] = "fp64"
     with ClockSampler(local) as clk:
-        s32, reps = run_steps(fs, n, main_prec, args.warmup, args.steps, barrier)
+        s32, reps, states = run_steps(fs, n, main_prec, args.warmup, args.steps, barrier,
+                                      record=min(args.e2e_steps, args.steps))
     ms_steps = [r["ms"] for r in reps]
     ms = max_over_ranks(float(np.mean(ms_steps)))
     pcg_ms = sum(r["pcg_ms"] for r in reps)
@@ -310,13 +323,16 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    e2e_ms, h2d, d2h = e2e_steps(fs, s32, n, args.e2e_steps)
+    e2e_ms, h2d, d2h = e2e_steps(fs, s32, states)
     e2e_ms = max_over_ranks(e2e_ms)
+    # the device time of the same steps, for comparison with the end-to-end figure
+    e2e_device_ms = float(np.mean([r["ms"] for r in reps[:len(states)]])) if states else None
+    del states
     s32.close()
 
     fp64 = None
     if not args.no_fp64:
-        s64, reps64 = run_steps(fs, n, fs.FS_PRECISION_FP64, args.warmup, args.steps, barrier)
+        s64, reps64, _ = run_steps(fs, n, fs.FS_PRECISION_FP64, args.warmup, args.steps, barrier)
         ms64 = max_over_ranks(float(np.mean([r["ms"] for r in reps64])))
         fp64 = {"ms_per_step": ms64, "pcg_iterations_per_step": float(np.mean([r["pcg_iterations"] for r in reps64])),
                 "speedup_fp32_refine": ms64 / ms, "max_rel_residual": max(r["max_rel_residual"] for r in reps64)}
@@ -334,7 +350,9 @@ def main():
         "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if main_prec == fs.FS_PRECISION_FP32_REFINE else "f64",
         "data": "synthetic", "config": config,
-        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": "the first %d timed steps replayed from their saved states" % min(args.e2e_steps, args.steps),
+                "device_ms_same_steps": e2e_device_ms},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (spmv + update + direction, 3 kernels)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

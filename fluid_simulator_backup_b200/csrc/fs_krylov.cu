@@ -353,8 +353,8 @@ __device__ __forceinline__ void spmv_row4(const Op7<V>& A, const V* __restrict__
   }
 }
 
-template <class V>
-__global__ void __launch_bounds__(256) k_cg_spmv(Op7<V> A, const V* __restrict__ p, V* __restrict__ q,
+template <class V, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cg_spmv(Op7<V> A, const V* __restrict__ p, V* __restrict__ q,
                                                  PcgState* st, double* partials, int kchunk) {
   if (((volatile PcgState*)st)->done) return;
   const Lay& L = A.L;
@@ -520,13 +520,26 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_pupdate(Op7<V> A, X* __restr
 
 namespace {
 int g_cg_blocks[2][2][3];  // [X double?][V double?][spmv, update, pupdate]: resident blocks per SM
+// SpMV blocks per SM the compiler must fit (FS_SPMV_MINB = 2, 3 or 4 to
+// sweep); measured best at 256^3: 4 for FP32 vectors (64 registers, no
+// spills to speak of), 2 for FP64 (128 registers; fewer spill)
+int g_spmv_minb_env = 0;
+template <class V> int spmv_minb() { return g_spmv_minb_env ? g_spmv_minb_env : (sizeof(V) == 4 ? 4 : 2); }
 }
 
 template <class V, class X>
 void cg_prepare() {
   reduction_blocks(1);  // SM count and the FS_BLOCKS_PER_SM knob
   int* slot = g_cg_blocks[sizeof(X) == 8][sizeof(V) == 8];
-  const void* ks[3] = {(const void*)k_cg_spmv<V>, (const void*)k_cg_update<V>, (const void*)k_cg_pupdate<V, X>};
+  if (const char* e = std::getenv("FS_SPMV_MINB")) {
+    const int v = std::atoi(e);
+    if (v >= 2 && v <= 4) g_spmv_minb_env = v;
+  }
+  const int minb = spmv_minb<V>();
+  const void* spmv = minb == 4   ? (const void*)k_cg_spmv<V, 4>
+                     : minb == 3 ? (const void*)k_cg_spmv<V, 3>
+                                 : (const void*)k_cg_spmv<V, 2>;
+  const void* ks[3] = {spmv, (const void*)k_cg_update<V>, (const void*)k_cg_pupdate<V, X>};
   for (int m = 0; m < 3; ++m) {
     if (slot[m]) continue;
     int nb = 0;
@@ -550,7 +563,13 @@ void cg_iteration(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double*
   const int chunks = std::max(1, std::min(L.nz, want / (tx * ty)));
   const int kchunk = (L.nz + chunks - 1) / chunks;
   const dim3 sg(tx, ty, (L.nz + kchunk - 1) / kchunk);
-  k_cg_spmv<V><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
+  const int minb = spmv_minb<V>();
+  if (minb == 4)
+    k_cg_spmv<V, 4><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
+  else if (minb == 3)
+    k_cg_spmv<V, 3><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
+  else
+    k_cg_spmv<V, 2><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
   // pointwise kernels: grid-stride over the vectors, resident blocks only
   const int64_t nvec = (int64_t)((L.nx + 3) >> 2) * L.ny * L.nz;
   auto grid = [&](int per_sm) {
