@@ -25,7 +25,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfluidb200.so")
 
 FS_OK, FS_INVALID_ARG, FS_OOM, FS_NOT_CONVERGED, FS_NONFINITE, FS_CUDA_ERROR, FS_TIMEOUT, FS_NOT_SUPPORTED = range(8)
-FIELD = {"phi": 0, "u": 1, "v": 2, "w": 3, "pressure": 4, "p": 4, "divergence": 5}
+FIELD = {"phi": 0, "u": 1, "v": 2, "w": 3, "pressure": 4, "p": 4, "divergence": 5,
+         "adj_phi": 6, "adj_u": 7, "adj_v": 8, "adj_w": 9}
 FS_PRECISION_FP64, FS_PRECISION_FP32_REFINE = 0, 1
 FS_STOP_RELATIVE, FS_STOP_ABSOLUTE = 0, 1
 FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER = 1, 2, 4
@@ -33,7 +34,9 @@ FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
             "fs_memory_bytes", "fs_upload", "fs_download", "fs_upload_device", "fs_download_device", "fs_step",
             "fs_cfl_dt", "fs_project", "fs_advect_levelset", "fs_advect_velocity", "fs_reinitialize",
-            "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc")
+            "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc", "fs_adjoint_reset", "fs_adjoint_density_bars",
+            "fs_step_adjoint", "fs_advect_levelset_adjoint", "fs_advect_velocity_adjoint", "fs_reinitialize_adjoint",
+            "fs_viscosity_adjoint", "fs_project_adjoint")
 
 
 class FsError(RuntimeError):
@@ -120,6 +123,14 @@ def lib():
                                  ctypes.c_int, ip, dp]
         L.fs_pcg_csr_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_int, vp, ip, dp]
+        L.fs_adjoint_reset.argtypes = [vp]
+        L.fs_adjoint_density_bars.argtypes = [vp, dp, dp]
+        L.fs_step_adjoint.argtypes = [vp, ctypes.c_double, ctypes.POINTER(StepReport)]
+        L.fs_advect_levelset_adjoint.argtypes = [vp, ctypes.c_double]
+        L.fs_advect_velocity_adjoint.argtypes = [vp, ctypes.c_double]
+        L.fs_reinitialize_adjoint.argtypes = [vp]
+        L.fs_viscosity_adjoint.argtypes = [vp, ctypes.c_double]
+        L.fs_project_adjoint.argtypes = [vp, ctypes.c_double]
         for name in EXPORTED:
             if name not in ("fs_params_default", "fs_status_str", "fs_last_error"):
                 getattr(L, name).restype = ctypes.c_int
@@ -155,6 +166,8 @@ def default_params(**overrides):
 
 def field_shape(n, name):
     nx, ny, nz = n
+    if name.startswith("adj_"):
+        name = name[4:]
     return {"phi": (nz, ny, nx), "pressure": (nz, ny, nx), "p": (nz, ny, nx), "divergence": (nz, ny, nx),
             "u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx)}[name]
 
@@ -272,6 +285,38 @@ class Solver:
         it = ctypes.c_int()
         _check(lib().fs_viscosity(self._h, float(dt), ctypes.byref(it)), "fs_viscosity")
         return it.value
+
+    # ---- adjoints (FP64 contexts): bars live in the adj_* fields
+    def adjoint_reset(self):
+        _check(lib().fs_adjoint_reset(self._h), "fs_adjoint_reset")
+
+    def density_bars(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(lib().fs_adjoint_density_bars(self._h, ctypes.byref(a), ctypes.byref(b)), "fs_adjoint_density_bars")
+        return a.value, b.value
+
+    def step_adjoint(self, dt, allow_not_converged=False):
+        r = StepReport()
+        s = lib().fs_step_adjoint(self._h, float(dt), ctypes.byref(r))
+        _check(s, "fs_step_adjoint", (FS_NOT_CONVERGED,) if allow_not_converged else ())
+        out = r.as_dict()
+        out["status"] = s
+        return out
+
+    def advect_levelset_adjoint(self, dt):
+        _check(lib().fs_advect_levelset_adjoint(self._h, float(dt)), "fs_advect_levelset_adjoint")
+
+    def advect_velocity_adjoint(self, dt):
+        _check(lib().fs_advect_velocity_adjoint(self._h, float(dt)), "fs_advect_velocity_adjoint")
+
+    def reinitialize_adjoint(self):
+        _check(lib().fs_reinitialize_adjoint(self._h), "fs_reinitialize_adjoint")
+
+    def viscosity_adjoint(self, dt):
+        _check(lib().fs_viscosity_adjoint(self._h, float(dt)), "fs_viscosity_adjoint")
+
+    def project_adjoint(self, dt):
+        _check(lib().fs_project_adjoint(self._h, float(dt)), "fs_project_adjoint", (FS_NOT_CONVERGED,))
 
 
 def pcg_csr(values, column_index, row_ptr, b, x0, tolerance, max_iteration, stop=FS_STOP_ABSOLUTE, solver=None):

@@ -101,6 +101,14 @@ struct fs_ctx {
   float pcg_ms = 0.0f;
   int pcg_launched_iterations = 0;
   cudaEvent_t evp0 = nullptr, evp1 = nullptr;
+  // adjoint state (FP64 contexts; allocated on first use)
+  double* abar[4] = {};       // bars of phi, u, v, w (FS_FIELD_ADJ_*)
+  double* awork_c[6] = {};    // cell work bars
+  double* awork_f[4][3] = {}; // face work bar triples
+  double* a_vlam[3] = {};     // viscosity: lambda per component
+  double* a_vxb[3] = {};      // viscosity: x_bar per component
+  double* a_rho = nullptr;    // device [4]: bars of rho_neg, rho_pos
+  std::vector<double*> tape_cells, tape_faces;  // taped forward states, allocated on demand
   bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
   double reliable_delta = 0.1;  // residual drop between reliable updates (FS_RELIABLE_DELTA to sweep)
 
@@ -108,6 +116,15 @@ struct fs_ctx {
 };
 
 namespace {
+
+// Forward states kept for the adjoint of one step (FP64 contexts).  Each
+// pointer is a padded field of the context's layouts.
+struct Tape {
+  double* ls[4] = {};                 // level set: the three RK stage inputs and the advected phi
+  double* vel[3][3][3] = {};          // [stage][0 input, 1 viscosity input, 2 projection input][component]
+  double* p[3] = {};                  // pressure of each stage's projection
+  std::vector<double*> re[3];         // [reinit block][pseudo-step]: input of each Sussman step
+};
 
 fs_status dalloc(fs_ctx* c, void** out, size_t bytes) {
   void* p = nullptr;
@@ -146,12 +163,14 @@ void release(fs_ctx* c) {
 
 const Lay& lay_of(const fs_ctx* c, int field) {
   switch (field) {
-    case FS_FIELD_U: return c->Lu;
-    case FS_FIELD_V: return c->Lv;
-    case FS_FIELD_W: return c->Lw;
+    case FS_FIELD_U: case FS_FIELD_ADJ_U: return c->Lu;
+    case FS_FIELD_V: case FS_FIELD_ADJ_V: return c->Lv;
+    case FS_FIELD_W: case FS_FIELD_ADJ_W: return c->Lw;
     default: return c->Lc;
   }
 }
+
+bool is_adjoint_field(int field) { return field >= FS_FIELD_ADJ_PHI && field <= FS_FIELD_ADJ_W; }
 
 fs_status check_params(const fs_params* p) {
   if (!p) { set_error("params is NULL"); return FS_INVALID_ARG; }
@@ -256,13 +275,17 @@ template <class S>
 S* F(void* p) { return static_cast<S*>(p); }
 
 template <class S>
-fs_status advect_levelset_t(fs_ctx* c, double dt) {
+fs_status advect_levelset_t(fs_ctx* c, double dt, Tape* tp = nullptr) {
   const fs_params& P = c->prm;
   const double eps = P.weno_epsilon, dx = c->grid.dx;
   S *phi = F<S>(c->phi), *t1 = F<S>(c->s1), *t2 = F<S>(c->s2);
   S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w);
   cudaStream_t s = c->stream;
+  int stage = 0;
   auto fe = [&](S* src, const S* base, S* out, double c0, double c1) {
+    if (tp && stage < 3)
+      cudaMemcpyAsync(tp->ls[stage], src, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    ++stage;
     fill_extrap<S>(src, c->Lc, s);
     weno5_levelset<S>(src, base, out, u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, eps, dt, c0, c1, s);
     c->launches += 2;
@@ -279,6 +302,7 @@ fs_status advect_levelset_t(fs_ctx* c, double dt) {
     std::swap(c->s1, c->s2);
   }
   std::swap(c->phi, c->s1);
+  if (tp) CK(cudaMemcpyAsync(tp->ls[3], c->phi, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, s));
   CK(cudaGetLastError());
   return FS_OK;
 }
@@ -302,7 +326,8 @@ fs_status advect_velocity_t(fs_ctx* c, double dt) {
 // S from `in`, reinit_iterations pseudo-steps, the last one combined as
 // c0*base + c1*result.
 template <class S>
-fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, double c1, void* scrA, void* scrB) {
+fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, double c1, void* scrA, void* scrB,
+                         std::vector<double*>* tape = nullptr) {
   const fs_params& P = c->prm;
   const double dx = c->grid.dx, dtau = dx / P.reinit_scaling;
   const int n = P.reinit_iterations;
@@ -318,6 +343,7 @@ fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, 
   for (int it = 0; it < n; ++it) {
     const bool last = it == n - 1;
     void* dst = last ? out : (cur == scrA ? scrB : scrA);
+    if (tape) CK(cudaMemcpyAsync((*tape)[it], cur, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, s));
     fill_extrap<S>(F<S>(cur), c->Lc, s);
     sussman_step<S>(F<S>(cur), F<S>(c->sgn), F<S>(base), F<S>(dst), c->Lc, dx, P.weno_epsilon, dtau,
                     last ? c0 : 0.0, last ? c1 : 1.0, (P.flags & FS_FLAG_REINIT_TYPO) ? 1 : 0, s);
@@ -328,15 +354,15 @@ fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, 
 }
 
 template <class S>
-fs_status reinitialize_t(fs_ctx* c) {
+fs_status reinitialize_t(fs_ctx* c, Tape* tp = nullptr) {
   // RK combination of reinitialisation blocks (EULERIAN_FLUID_SOLVER_3D.h:959-979, 1081-1109)
   if (c->prm.order == 3) {
-    CKS(reinit_block_t<S>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3));
-    CKS(reinit_block_t<S>(c, c->s1, c->s4, c->phi, 0.75, 0.25, c->s2, c->s3));
-    CKS(reinit_block_t<S>(c, c->s4, c->phi, c->phi, 1.0 / 3.0, 2.0 / 3.0, c->s2, c->s3));
+    CKS(reinit_block_t<S>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3, tp ? &tp->re[0] : nullptr));
+    CKS(reinit_block_t<S>(c, c->s1, c->s4, c->phi, 0.75, 0.25, c->s2, c->s3, tp ? &tp->re[1] : nullptr));
+    CKS(reinit_block_t<S>(c, c->s4, c->phi, c->phi, 1.0 / 3.0, 2.0 / 3.0, c->s2, c->s3, tp ? &tp->re[2] : nullptr));
   } else {
-    CKS(reinit_block_t<S>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3));
-    CKS(reinit_block_t<S>(c, c->s1, c->phi, c->phi, 0.5, 0.5, c->s2, c->s3));
+    CKS(reinit_block_t<S>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3, tp ? &tp->re[0] : nullptr));
+    CKS(reinit_block_t<S>(c, c->s1, c->phi, c->phi, 0.5, 0.5, c->s2, c->s3, tp ? &tp->re[1] : nullptr));
   }
   return FS_OK;
 }
@@ -538,8 +564,19 @@ fs_status gravity_t(fs_ctx* c, double dt) {
 // One SolveForRK stage (EULERIAN_FLUID_SOLVER_3D.h:1453-1476): advection,
 // gravity, viscosity, projection; the projection's velocity update also
 // applies the stage's RK combination with the step's initial velocity.
+// copy the three velocity components into a tape slot
+fs_status tape_velocity(fs_ctx* c, double* const dst[3]) {
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  void* comps[3] = {c->u, c->v, c->w};
+  for (int a = 0; a < 3; ++a)
+    CK(cudaMemcpyAsync(dst[a], comps[a], lays[a]->total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  return FS_OK;
+}
+
 template <class S>
-fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* rep) {
+fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* rep, Tape* tp = nullptr,
+                  int stage = 0) {
+  if (tp) CKS(tape_velocity(c, tp->vel[stage][0]));
   CKS(advect_velocity_t<S>(c, dt));
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   if (!(c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION)) {
@@ -550,11 +587,14 @@ fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* re
     c->launches += 3;
   }
   CKS(gravity_t<S>(c, dt));
+  if (tp) CKS(tape_velocity(c, tp->vel[stage][1]));
   int vit = 0;
   CKS(viscosity_t<S>(c, dt, &vit));
+  if (tp) CKS(tape_velocity(c, tp->vel[stage][2]));
   fs_solve_report pr{};
   fs_status st = project_t<S>(c, dt, c0, c1, &pr);
   if (st != FS_OK && st != FS_NOT_CONVERGED) return st;
+  if (tp) CK(cudaMemcpyAsync(tp->p[stage], c->p64, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   if (rep) {
     rep->pcg_iterations += pr.iterations;
     rep->outer_iterations += pr.outer_iterations;
@@ -568,18 +608,19 @@ fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* re
 }
 
 template <class S>
-fs_status step_t(fs_ctx* c, double dt, fs_step_report* rep) {
+fs_status step_t(fs_ctx* c, double dt, fs_step_report* rep, Tape* tp = nullptr) {
   const int order = c->prm.order;
   fs_status worst = FS_OK;
-  CKS(advect_levelset_t<S>(c, dt));
+  CKS(advect_levelset_t<S>(c, dt, tp));
   const size_t bu = c->Lu.total * c->S(), bv = c->Lv.total * c->S(), bw = c->Lw.total * c->S();
   if (order > 1) {
     CK(cudaMemcpyAsync(c->u0, c->u, bu, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->v0, c->v, bv, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->w0, c->w, bw, cudaMemcpyDeviceToDevice, c->stream));
   }
+  int stage_index = 0;
   auto stage = [&](double c0, double c1) -> fs_status {
-    fs_status s = stage_t<S>(c, dt, c0, c1, rep);
+    fs_status s = stage_t<S>(c, dt, c0, c1, rep, tp, stage_index++);
     if (s == FS_NOT_CONVERGED) { worst = s; return FS_OK; }
     return s;
   };
@@ -593,7 +634,7 @@ fs_status step_t(fs_ctx* c, double dt, fs_step_report* rep) {
     CKS(stage(0.75, 0.25));
     CKS(stage(1.0 / 3.0, 2.0 / 3.0));
   }
-  CKS(reinitialize_t<S>(c));
+  CKS(reinitialize_t<S>(c, tp));
   return worst;
 }
 
@@ -615,6 +656,304 @@ fs_status cfl_t(fs_ctx* c, double* dt) {
   const double cfl = 0.5 * (cv + std::sqrt(cv * cv + 4.0 * (g_f * g_f)));
   *dt = P.cfl / cfl;
   return FS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the timestep (FP64 contexts)
+// ---------------------------------------------------------------------------
+
+// Buffers of the adjoint, allocated on first use.
+fs_status adj_alloc(fs_ctx* c) {
+  if (c->abar[0]) return FS_OK;
+  const size_t cb = c->Lc.total * sizeof(double);
+  const size_t fb[3] = {c->Lu.total * sizeof(double), c->Lv.total * sizeof(double), c->Lw.total * sizeof(double)};
+  CKS(dalloc(c, (void**)&c->abar[0], cb));
+  for (int a = 0; a < 3; ++a) CKS(dalloc(c, (void**)&c->abar[1 + a], fb[a]));
+  for (double*& p : c->awork_c) CKS(dalloc(c, (void**)&p, cb));
+  for (auto& t : c->awork_f)
+    for (int a = 0; a < 3; ++a) CKS(dalloc(c, (void**)&t[a], fb[a]));
+  for (int a = 0; a < 3; ++a) {
+    CKS(dalloc(c, (void**)&c->a_vlam[a], fb[a]));
+    CKS(dalloc(c, (void**)&c->a_vxb[a], fb[a]));
+  }
+  CKS(dalloc(c, (void**)&c->a_rho, 4 * sizeof(double)));
+  return FS_OK;
+}
+
+// Tape buffers for one step under the current parameters.
+fs_status tape_bind(fs_ctx* c, Tape* tp) {
+  const size_t cb = c->Lc.total * sizeof(double);
+  const size_t fb[3] = {c->Lu.total * sizeof(double), c->Lv.total * sizeof(double), c->Lw.total * sizeof(double)};
+  const int n = c->prm.reinit_iterations;
+  const size_t ncell = 4 + 3 + 3 * (size_t)n, nface = 27;
+  while (c->tape_cells.size() < ncell) {
+    double* p = nullptr;
+    CKS(dalloc(c, (void**)&p, cb));
+    c->tape_cells.push_back(p);
+  }
+  while (c->tape_faces.size() < nface) {
+    double* p = nullptr;
+    CKS(dalloc(c, (void**)&p, fb[c->tape_faces.size() % 3]));
+    c->tape_faces.push_back(p);
+  }
+  size_t q = 0;
+  for (int m = 0; m < 4; ++m) tp->ls[m] = c->tape_cells[q++];
+  for (int m = 0; m < 3; ++m) tp->p[m] = c->tape_cells[q++];
+  for (int b = 0; b < 3; ++b) {
+    tp->re[b].resize(n);
+    for (int it = 0; it < n; ++it) tp->re[b][it] = c->tape_cells[q++];
+  }
+  size_t f = 0;
+  for (int st = 0; st < 3; ++st)
+    for (int k = 0; k < 3; ++k)
+      for (int a = 0; a < 3; ++a) tp->vel[st][k][a] = c->tape_faces[f++];
+  return FS_OK;
+}
+
+fs_status zero_cell(fs_ctx* c, double* p) {
+  CK(cudaMemsetAsync(p, 0, c->Lc.total * sizeof(double), c->stream));
+  return FS_OK;
+}
+fs_status zero_faces(fs_ctx* c, double* const t[3]) {
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  for (int a = 0; a < 3; ++a) CK(cudaMemsetAsync(t[a], 0, lays[a]->total * sizeof(double), c->stream));
+  return FS_OK;
+}
+fs_status copy_cell(fs_ctx* c, double* dst, const double* src) {
+  CK(cudaMemcpyAsync(dst, src, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  return FS_OK;
+}
+fs_status copy_faces(fs_ctx* c, double* const dst[3], double* const src[3]) {
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  for (int a = 0; a < 3; ++a)
+    CK(cudaMemcpyAsync(dst[a], src[a], lays[a]->total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  return FS_OK;
+}
+void axpy_faces(fs_ctx* c, double* const out[3], double* const x[3], double a) {
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  for (int q = 0; q < 3; ++q) adj_axpy(out[q], x[q], a, *lays[q], c->stream);
+  c->launches += 3;
+}
+
+// One forward-Euler WENO5 level-set update fe = src - dt L(src; vel): given
+// out_bar (bar of c1 * fe), src_bar = its bar w.r.t. src (overwritten) and
+// vel_bar += its bar w.r.t. the velocity.  src is refilled in its ghosts.
+fs_status adj_levelset_fe(fs_ctx* c, double* src, double* const vel[3], const double* out_bar, double c1,
+                          double* src_bar, double* const vel_bar[3], double dt) {
+  CKS(zero_cell(c, src_bar));
+  fill_extrap<double>(src, c->Lc, c->stream);
+  adj_weno_levelset(src, vel[0], vel[1], vel[2], out_bar, src_bar, vel_bar[0], vel_bar[1], vel_bar[2], c->Lc, c->Lu,
+                    c->Lv, c->Lw, c->grid.dx, c->prm.weno_epsilon, dt, c1, c->stream);
+  adj_extrap(src_bar, c->Lc, c->stream);
+  c->launches += 3;
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+// One reinitialisation block B (S from its input, n Sussman steps) given the
+// inputs of its pseudo-steps: x_bar (overwritten) = B'^T z_bar.
+fs_status adj_reinit_block(fs_ctx* c, const std::vector<double*>& ys, const double* z_bar, double* x_bar) {
+  const fs_params& P = c->prm;
+  const int n = (int)ys.size();
+  if (n == 0) return copy_cell(c, x_bar, z_bar);
+  const double dx = c->grid.dx, dtau = dx / P.reinit_scaling;
+  double *A = c->awork_c[2], *B = c->awork_c[3], *sbar = c->awork_c[4];
+  sign_function<double>(ys[0], (double*)c->sgn, c->Lc, dx, c->stream);
+  CKS(zero_cell(c, sbar));
+  CKS(copy_cell(c, A, z_bar));
+  for (int it = n - 1; it >= 0; --it) {
+    CKS(zero_cell(c, B));
+    fill_extrap<double>(ys[it], c->Lc, c->stream);
+    adj_sussman(ys[it], (const double*)c->sgn, A, B, sbar, c->Lc, dx, P.weno_epsilon, dtau, 1.0,
+                (P.flags & FS_FLAG_REINIT_TYPO) ? 1 : 0, c->stream);
+    adj_extrap(B, c->Lc, c->stream);
+    std::swap(A, B);
+  }
+  adj_sign(ys[0], sbar, A, c->Lc, dx, c->stream);
+  c->launches += 2 + 3 * n;
+  CKS(copy_cell(c, x_bar, A));
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+// Projection with the RK combination out = c0 base + c1 val: given out_bar,
+// in_bar (overwritten) = bar of u*, base_bar += c0 out_bar (when base_bar),
+// phi_bar and the density bars accumulate.  ustar, p: the forward's input
+// velocity and pressure; phi the level set it used.
+fs_status adj_projection(fs_ctx* c, double* phi, double* const ustar[3], const double* p, double* const out_bar[3],
+                         double c1, double* const in_bar[3], double* phi_bar, double dt) {
+  const fs_params& P = c->prm;
+  const double dx = c->grid.dx;
+  cudaStream_t s = c->stream;
+  (void)ustar;  // the map is affine in u*: its derivative does not depend on it
+  build_pressure_operator<double, double>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (double*)c->pax, (double*)c->pay,
+                                          (double*)c->paz, (double*)c->pdiag, c->scalars + 12, s);
+  Op7<double> A{(double*)c->pax, (double*)c->pay, (double*)c->paz, (double*)c->pdiag, c->Lc, 1, c->scalars + 12};
+  double *pbar = c->awork_c[0], *lam = c->awork_c[1];
+  CKS(zero_cell(c, pbar));
+  CKS(zero_cell(c, lam));
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  for (int a = 0; a < 3; ++a)
+    adj_velcorr(p, phi, out_bar[a], in_bar[a], pbar, phi_bar, c->a_rho, *lays[a], c->Lc, a, dx, dt, P.rho_neg,
+                P.rho_pos, c1, s);
+  c->launches += 5;
+  CK(cudaGetLastError());
+  // lambda = A^-1 p_bar (A symmetric): the second solve with the same operator
+  int it = 0, st = 0;
+  double rel = 0.0;
+  CKS(run_pcg<double>(c, 3, A, pbar, lam, (double*)c->pr, (double*)c->pp, (double*)c->pq,
+                      std::min(P.tolerance, 1e-10), std::max(P.max_iteration, 1), FS_STOP_RELATIVE, &it, &rel, &st));
+  adj_sum(lam, c->Lc, c->partials, c->tickets + 4, c->scalars + 14, s);
+  for (int a = 0; a < 3; ++a) adj_divergence(lam, c->scalars + 14, in_bar[a], *lays[a], c->Lc, a, dx, dt, s);
+  adj_pressure_operator(phi, lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, s);
+  c->launches += 5;
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+// Semi-implicit viscosity x = M(phi)^-1 r(ug, phi): given out_bar (wall rows
+// cleared here), in_bar (overwritten) = bar of ug; phi and density bars
+// accumulate.  ug, x: the forward's input and output velocities.
+fs_status adj_viscosity(fs_ctx* c, double* phi, double* const ug[3], double* const x[3], double* const out_bar[3],
+                        double* const in_bar[3], double* phi_bar, double dt) {
+  const fs_params& P = c->prm;
+  const double dx = c->grid.dx;
+  cudaStream_t s = c->stream;
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  CKS(zero_faces(c, in_bar));
+  for (int a = 0; a < 3; ++a) {
+    viscosity_system<double>(phi, ug[0], ug[1], ug[2], c->Lc, c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos,
+                             P.mu_neg, P.mu_pos, (double*)c->vs[a][0], (double*)c->vs[a][1], (double*)c->vs[a][2],
+                             (double*)c->vs[a][3], (double*)c->vs[a][4], s);
+    CK(cudaMemcpyAsync(c->a_vxb[a], out_bar[a], lays[a]->total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    adj_zero_walls(c->a_vxb[a], *lays[a], a, s);  // wall rows are the constant zero
+    CK(cudaMemsetAsync(c->a_vlam[a], 0, lays[a]->total * sizeof(double), s));
+    Op7<double> A{(double*)c->vs[a][0], (double*)c->vs[a][1], (double*)c->vs[a][2], (double*)c->vs[a][3], *lays[a]};
+    int it = 0, st = 0;
+    CKS(run_pcg<double>(c, 120 + a, A, c->a_vxb[a], c->a_vlam[a], (double*)c->vs[a][6], (double*)c->vs[a][7],
+                        (double*)c->vs[a][8], std::min(P.viscosity_tolerance, 1e-12),
+                        std::max(P.viscosity_max_iteration, 1), FS_STOP_RELATIVE, &it, nullptr, &st));
+    adj_visc(phi, ug[0], ug[1], ug[2], x[a], c->a_vlam[a], in_bar[0], in_bar[1], in_bar[2], phi_bar, c->a_rho, c->Lc,
+             c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos, P.mu_neg, P.mu_pos, s);
+    c->launches += 3;
+  }
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+// WENO5 self-advection of u, v, w: in_bar (overwritten) from out_bar.
+fs_status adj_velocity_advect(fs_ctx* c, double* const uin[3], double* const out_bar[3], double* const in_bar[3],
+                              double dt) {
+  CKS(zero_faces(c, in_bar));
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  for (int a = 0; a < 3; ++a)
+    adj_weno_mac(uin[a], uin[0], uin[1], uin[2], out_bar[a], in_bar[a], in_bar[0], in_bar[1], in_bar[2], *lays[a],
+                 c->Lu, c->Lv, c->Lw, a, c->grid.dx, c->prm.weno_epsilon, dt, c->stream);
+  c->launches += 3;
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+fs_status adj_check(fs_ctx* c) {
+  if (c->fp32) { set_error("adjoints are built for FP64 contexts"); return FS_NOT_SUPPORTED; }
+  if (c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) {
+    set_error("adjoints follow the corrected projection only");
+    return FS_NOT_SUPPORTED;
+  }
+  return adj_alloc(c);
+}
+
+// The whole step: forward recomputed with a tape from the current state,
+// then the reverse sweep.  On entry abar holds the bars of the step's
+// output; on return the bars of its input (phi, u, v, w) and a_rho has the
+// density bars added.  The fields end in the step's output state.
+fs_status step_adjoint_t(fs_ctx* c, double dt, fs_step_report* rep) {
+  const fs_params& P = c->prm;
+  Tape tp;
+  CKS(tape_bind(c, &tp));
+  double* u0[3];
+  for (int a = 0; a < 3; ++a) u0[a] = tp.vel[0][0][a];  // the step's initial velocity (first stage input)
+  fs_status fw = step_t<double>(c, dt, rep, &tp);
+  if (fw != FS_OK && fw != FS_NOT_CONVERGED) return fw;
+  const int order = P.order;
+  // ---- reinitialisation blocks
+  double* phiA = tp.ls[3];
+  double *phibar = c->abar[0], *phiAbar = c->awork_c[5];
+  CKS(zero_cell(c, phiAbar));
+  {
+    double *zb = c->awork_c[0], *xb = c->awork_c[1];  // free here: the projection adjoint runs later
+    const int nb = order == 3 ? 3 : 2;
+    const double c0s[3] = {0.0, order == 3 ? 0.75 : 0.5, 1.0 / 3.0};
+    const double c1s[3] = {1.0, order == 3 ? 0.25 : 0.5, 2.0 / 3.0};
+    // bar of the last block's output is phibar; walk the blocks backwards
+    CKS(copy_cell(c, zb, phibar));
+    for (int b = nb - 1; b >= 0; --b) {
+      adj_axpy(phiAbar, zb, c0s[b], c->Lc, c->stream);  // base term
+      CK(cudaMemsetAsync(xb, 0, c->Lc.total * sizeof(double), c->stream));
+      // the block's own output is scaled by c1
+      adj_axpy(xb, zb, c1s[b], c->Lc, c->stream);
+      CKS(adj_reinit_block(c, tp.re[b], xb, zb));  // zb <- bar of the block input
+      c->launches += 2;
+    }
+    adj_axpy(phiAbar, zb, 1.0, c->Lc, c->stream);  // the first block's input is phiA
+    c->launches += 1;
+  }
+  // ---- velocity stages, backwards
+  const int ns = order;
+  const double vc0[3] = {0.0, order == 3 ? 0.75 : 0.5, 1.0 / 3.0};
+  const double vc1[3] = {1.0, order == 3 ? 0.25 : 0.5, 2.0 / 3.0};
+  double* const* ubar = &c->abar[1];
+  double* cur[3];   // bar of the current stage's output
+  double* u0bar[3];
+  for (int a = 0; a < 3; ++a) { cur[a] = c->awork_f[0][a]; u0bar[a] = c->awork_f[3][a]; }
+  CKS(copy_faces(c, cur, ubar));
+  CKS(zero_faces(c, u0bar));
+  for (int st = ns - 1; st >= 0; --st) {
+    if (vc0[st] != 0.0) axpy_faces(c, u0bar, cur, vc0[st]);
+    double* pin[3] = {c->awork_f[1][0], c->awork_f[1][1], c->awork_f[1][2]};
+    CKS(adj_projection(c, phiA, tp.vel[st][2], tp.p[st], cur, vc1[st], pin, phiAbar, dt));
+    double* gin[3] = {c->awork_f[2][0], c->awork_f[2][1], c->awork_f[2][2]};
+    if (P.viscosity) {
+      CKS(adj_viscosity(c, phiA, tp.vel[st][1], tp.vel[st][2], pin, gin, phiAbar, dt));
+    } else {
+      CKS(copy_faces(c, gin, pin));
+    }
+    // gravity adds a constant; the no-penetration zeroing clears the wall bars
+    const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+    for (int a = 0; a < 3; ++a) adj_zero_walls(gin[a], *lays[a], a, c->stream);
+    c->launches += 3;
+    CKS(adj_velocity_advect(c, tp.vel[st][0], gin, cur, dt));  // cur <- bar of the stage input
+  }
+  axpy_faces(c, u0bar, cur, 1.0);  // the first stage's input is u0
+  // ---- level set: phiA from phi0 with the initial velocity u0
+  double* b1 = c->awork_c[0];
+  double* b2 = c->awork_c[1];
+  CKS(zero_cell(c, phibar));
+  double* const* u0p = u0;
+  if (order == 3 && !(P.flags & FS_FLAG_LEVELSET_FORWARD_EULER)) {
+    // phiA = 1/3 phi0 + 2/3 FE(phi2); phi2 = 3/4 phi0 + 1/4 FE(phi1); phi1 = FE(phi0)
+    adj_axpy(phibar, phiAbar, 1.0 / 3.0, c->Lc, c->stream);
+    CKS(adj_levelset_fe(c, tp.ls[2], u0p, phiAbar, 2.0 / 3.0, b2, u0bar, dt));  // b2 = bar of phi2
+    adj_axpy(phibar, b2, 0.75, c->Lc, c->stream);
+    CKS(adj_levelset_fe(c, tp.ls[1], u0p, b2, 0.25, b1, u0bar, dt));            // b1 = bar of phi1
+    CKS(adj_levelset_fe(c, tp.ls[0], u0p, b1, 1.0, b2, u0bar, dt));             // b2 = bar of phi0 via FE
+    adj_axpy(phibar, b2, 1.0, c->Lc, c->stream);
+    c->launches += 3;
+  } else if (order == 3) {
+    CKS(adj_levelset_fe(c, tp.ls[0], u0p, phiAbar, 1.0, b2, u0bar, dt));
+    adj_axpy(phibar, b2, 1.0, c->Lc, c->stream);
+    c->launches += 1;
+  } else {
+    // Heun: phiA = 1/2 phi0 + 1/2 FE(phi1), phi1 = FE(phi0)
+    adj_axpy(phibar, phiAbar, 0.5, c->Lc, c->stream);
+    CKS(adj_levelset_fe(c, tp.ls[1], u0p, phiAbar, 0.5, b1, u0bar, dt));
+    CKS(adj_levelset_fe(c, tp.ls[0], u0p, b1, 1.0, b2, u0bar, dt));
+    adj_axpy(phibar, b2, 1.0, c->Lc, c->stream);
+    c->launches += 2;
+  }
+  CKS(copy_faces(c, ubar, u0bar));
+  CK(cudaGetLastError());
+  return fw;
 }
 
 }  // namespace
@@ -793,7 +1132,9 @@ static void** field_ptr(fs_ctx* c, int field) {
 
 static fs_status upload_from_staging(fs_ctx* c, int field) {
   const Lay& L = lay_of(c, field);
-  if (field == FS_FIELD_PRESSURE) {
+  if (is_adjoint_field(field)) {
+    unpack_from_double<double>(c->abar[field - FS_FIELD_ADJ_PHI], c->staging, L, c->stream);
+  } else if (field == FS_FIELD_PRESSURE) {
     unpack_from_double<double>(c->p64, c->staging, L, c->stream);
   } else {
     void* dst = *field_ptr(c, field);
@@ -806,7 +1147,8 @@ static fs_status upload_from_staging(fs_ctx* c, int field) {
 
 static fs_status download_to_staging(fs_ctx* c, int field) {
   const Lay& L = lay_of(c, field);
-  if (field == FS_FIELD_PRESSURE) pack_to_double<double>(c->staging, c->p64, L, c->stream);
+  if (is_adjoint_field(field)) pack_to_double<double>(c->staging, c->abar[field - FS_FIELD_ADJ_PHI], L, c->stream);
+  else if (field == FS_FIELD_PRESSURE) pack_to_double<double>(c->staging, c->p64, L, c->stream);
   else if (field == FS_FIELD_DIVERGENCE) pack_to_double<double>(c->staging, c->div64, L, c->stream);
   else {
     void* src = *field_ptr(c, field);
@@ -822,9 +1164,19 @@ static int64_t field_count(const fs_ctx* c, int field) {
   return (int64_t)L.nx * L.ny * L.nz;
 }
 
+// fields accepted by upload (0..4 and the adjoint fields) and download (0..5 and the adjoint fields)
+static fs_status check_field(fs_ctx* c, int field, bool upload) {
+  if (is_adjoint_field(field)) return adj_check(c);
+  if (field < FS_FIELD_PHI || field > (upload ? FS_FIELD_PRESSURE : FS_FIELD_DIVERGENCE)) {
+    set_error("field %d cannot be %s", field, upload ? "uploaded" : "downloaded");
+    return FS_INVALID_ARG;
+  }
+  return FS_OK;
+}
+
 fs_status fs_upload(fs_ctx* c, int field, const double* host, const int64_t* strides) {
   if (!c || !host) { set_error("NULL argument"); return FS_INVALID_ARG; }
-  if (field < FS_FIELD_PHI || field > FS_FIELD_PRESSURE) { set_error("field %d cannot be uploaded", field); return FS_INVALID_ARG; }
+  CKS(check_field(c, field, true));
   const Lay& L = lay_of(c, field);
   const int64_t n = field_count(c, field);
   if (strides) {
@@ -846,7 +1198,7 @@ fs_status fs_upload(fs_ctx* c, int field, const double* host, const int64_t* str
 
 fs_status fs_download(fs_ctx* c, int field, double* host, const int64_t* strides) {
   if (!c || !host) { set_error("NULL argument"); return FS_INVALID_ARG; }
-  if (field < FS_FIELD_PHI || field > FS_FIELD_DIVERGENCE) { set_error("unknown field %d", field); return FS_INVALID_ARG; }
+  CKS(check_field(c, field, false));
   const Lay& L = lay_of(c, field);
   const int64_t n = field_count(c, field);
   CKS(download_to_staging(c, field));
@@ -867,9 +1219,10 @@ fs_status fs_download(fs_ctx* c, int field, double* host, const int64_t* strides
 
 fs_status fs_upload_device(fs_ctx* c, int field, const double* dev) {
   if (!c || !dev) { set_error("NULL argument"); return FS_INVALID_ARG; }
-  if (field < FS_FIELD_PHI || field > FS_FIELD_PRESSURE) { set_error("field %d cannot be uploaded", field); return FS_INVALID_ARG; }
+  CKS(check_field(c, field, true));
   const Lay& L = lay_of(c, field);
-  if (field == FS_FIELD_PRESSURE) unpack_from_double<double>(c->p64, dev, L, c->stream);
+  if (is_adjoint_field(field)) unpack_from_double<double>(c->abar[field - FS_FIELD_ADJ_PHI], dev, L, c->stream);
+  else if (field == FS_FIELD_PRESSURE) unpack_from_double<double>(c->p64, dev, L, c->stream);
   else if (c->fp32) unpack_from_double<float>((float*)*field_ptr(c, field), dev, L, c->stream);
   else unpack_from_double<double>((double*)*field_ptr(c, field), dev, L, c->stream);
   CK(cudaGetLastError());
@@ -879,9 +1232,10 @@ fs_status fs_upload_device(fs_ctx* c, int field, const double* dev) {
 
 fs_status fs_download_device(fs_ctx* c, int field, double* dev) {
   if (!c || !dev) { set_error("NULL argument"); return FS_INVALID_ARG; }
-  if (field < FS_FIELD_PHI || field > FS_FIELD_DIVERGENCE) { set_error("unknown field %d", field); return FS_INVALID_ARG; }
+  CKS(check_field(c, field, false));
   const Lay& L = lay_of(c, field);
-  if (field == FS_FIELD_PRESSURE) pack_to_double<double>(dev, c->p64, L, c->stream);
+  if (is_adjoint_field(field)) pack_to_double<double>(dev, c->abar[field - FS_FIELD_ADJ_PHI], L, c->stream);
+  else if (field == FS_FIELD_PRESSURE) pack_to_double<double>(dev, c->p64, L, c->stream);
   else if (field == FS_FIELD_DIVERGENCE) pack_to_double<double>(dev, c->div64, L, c->stream);
   else if (c->fp32) pack_to_double<float>(dev, (const float*)*field_ptr(c, field), L, c->stream);
   else pack_to_double<double>(dev, (const double*)*field_ptr(c, field), L, c->stream);
@@ -978,6 +1332,116 @@ fs_status fs_viscosity(fs_ctx* c, double dt, int* iterations) {
   CKS(DISPATCH(c, viscosity_t, c, dt, iterations));
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;
+}
+
+// ---- adjoints (FP64 contexts, corrected projection)
+
+fs_status fs_adjoint_reset(fs_ctx* c) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  CKS(zero_cell(c, c->abar[0]));
+  CKS(zero_faces(c, &c->abar[1]));
+  CK(cudaMemsetAsync(c->a_rho, 0, 4 * sizeof(double), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_adjoint_density_bars(fs_ctx* c, double* rho_neg_bar, double* rho_pos_bar) {
+  if (!c || !rho_neg_bar || !rho_pos_bar) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  CK(cudaMemcpyAsync(c->sc_host, c->a_rho, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *rho_neg_bar = c->sc_host[0];
+  *rho_pos_bar = c->sc_host[1];
+  return FS_OK;
+}
+
+fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  fs_step_report local{};
+  fs_step_report* r = rep ? rep : &local;
+  *r = fs_step_report{};
+  c->launches = 0;
+  c->pcg_ms = 0.0f;
+  c->pcg_launched_iterations = 0;
+  CKS(timed_begin(c));
+  fs_status s = step_adjoint_t(c, dt, r);
+  if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
+  CKS(timed_end(c, &r->ms));
+  r->pcg_ms = c->pcg_ms;
+  r->pcg_launched_iterations = c->pcg_launched_iterations;
+  r->kernel_launches = c->launches;
+  return s;
+}
+
+fs_status fs_advect_levelset_adjoint(fs_ctx* c, double dt) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
+  CKS(adj_levelset_fe(c, (double*)c->phi, vel, c->abar[0], 1.0, c->awork_c[0], &c->abar[1], dt));
+  CKS(copy_cell(c, c->abar[0], c->awork_c[0]));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_advect_velocity_adjoint(fs_ctx* c, double dt) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
+  CKS(adj_velocity_advect(c, vel, &c->abar[1], c->awork_f[0], dt));
+  CKS(copy_faces(c, &c->abar[1], c->awork_f[0]));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_reinitialize_adjoint(fs_ctx* c) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  Tape tp;
+  CKS(tape_bind(c, &tp));
+  CKS(reinit_block_t<double>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3, &tp.re[0]));
+  CKS(adj_reinit_block(c, tp.re[0], c->abar[0], c->awork_c[0]));
+  CKS(copy_cell(c, c->abar[0], c->awork_c[0]));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_viscosity_adjoint(fs_ctx* c, double dt) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (!(dt > 0)) { set_error("dt must be positive"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  if (!c->prm.viscosity) { set_error("viscosity is off"); return FS_INVALID_ARG; }
+  Tape tp;
+  CKS(tape_bind(c, &tp));
+  CKS(tape_velocity(c, tp.vel[0][1]));
+  CKS(viscosity_t<double>(c, dt, nullptr));
+  CKS(tape_velocity(c, tp.vel[0][2]));
+  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
+  CKS(copy_faces(c, vel, tp.vel[0][1]));  // the context keeps the operator's input
+  CKS(adj_viscosity(c, (double*)c->phi, tp.vel[0][1], tp.vel[0][2], &c->abar[1], c->awork_f[1], c->abar[0], dt));
+  CKS(copy_faces(c, &c->abar[1], c->awork_f[1]));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_project_adjoint(fs_ctx* c, double dt) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
+  CKS(adj_check(c));
+  Tape tp;
+  CKS(tape_bind(c, &tp));
+  CKS(tape_velocity(c, tp.vel[0][2]));
+  fs_status s = project_t<double>(c, dt, 0.0, 1.0, nullptr);
+  if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
+  CKS(copy_cell(c, tp.p[0], c->p64));
+  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
+  CKS(copy_faces(c, vel, tp.vel[0][2]));  // the context keeps the operator's input
+  CKS(adj_projection(c, (double*)c->phi, tp.vel[0][2], tp.p[0], &c->abar[1], 1.0, c->awork_f[1], c->abar[0], dt));
+  CKS(copy_faces(c, &c->abar[1], c->awork_f[1]));
+  CK(cudaStreamSynchronize(c->stream));
+  return s;
 }
 
 fs_status fs_pcg_csr(fs_ctx* c, int n, int nnz, const double* values, const int* column_index, const int* row_ptr,

@@ -122,4 +122,30 @@ void viscosity_system(const T* phi, const T* u, const T* v, const T* w, const La
                       const Lay& Lw, int axis, double dx, double dt, double rho_neg, double rho_pos, double mu_neg,
                       double mu_pos, T* ax, T* ay, T* az, T* diag, T* rhs, cudaStream_t s);
 
+// ---- adjoint family (fs_adjoint.cu), FP64 only; all add into the bars
+void adj_weno_levelset(const double* src, const double* u, const double* v, const double* w, const double* out_bar,
+                       double* src_bar, double* u_bar, double* v_bar, double* w_bar, const Lay& L, const Lay& Lu,
+                       const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c1, cudaStream_t s);
+void adj_extrap(double* bar, const Lay& L, cudaStream_t s);
+void adj_weno_mac(const double* comp, const double* u, const double* v, const double* w, const double* out_bar,
+                  double* comp_bar, double* u_bar, double* v_bar, double* w_bar, const Lay& Lc, const Lay& Lu,
+                  const Lay& Lv, const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s);
+void adj_sussman(const double* src, const double* sgn, const double* out_bar, double* src_bar, double* sgn_bar,
+                 const Lay& L, double dx, double eps, double dtau, double c1, int typo, cudaStream_t s);
+void adj_sign(const double* phi, const double* sgn_bar, double* phi_bar, const Lay& L, double dx, cudaStream_t s);
+void adj_velcorr(const double* p, const double* phi, const double* out_bar, double* in_bar, double* p_bar,
+                 double* phi_bar, double* rho_bar, const Lay& Lf, const Lay& Lc, int axis, double dx, double dt,
+                 double rn, double rp, double c1, cudaStream_t s);
+void adj_divergence(const double* lam, const double* sum_lam, double* in_bar, const Lay& Lf, const Lay& Lc, int axis,
+                    double dx, double dt, cudaStream_t s);
+void adj_sum(const double* f, const Lay& L, double* partials, unsigned int* ticket, double* out, cudaStream_t s);
+void adj_pressure_operator(const double* phi, const double* lam, const double* p, double* phi_bar, double* rho_bar,
+                           const Lay& Lc, double dx, double rn, double rp, cudaStream_t s);
+void adj_visc(const double* phi, const double* ug, const double* vg, const double* wg, const double* x,
+              const double* lam, double* u_bar, double* v_bar, double* w_bar, double* phi_bar, double* rho_bar,
+              const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw, int axis, double dx, double dt, double rn,
+              double rp, double mn, double mp, cudaStream_t s);
+void adj_zero_walls(double* f, const Lay& L, int axis, cudaStream_t s);
+void adj_axpy(double* out, const double* x, double a, const Lay& L, cudaStream_t s);
+
 }  // namespace fsb

@@ -45,7 +45,11 @@ typedef enum {
   FS_FIELD_V = 2,         /* y-velocity, y faces */
   FS_FIELD_W = 3,         /* z-velocity, z faces */
   FS_FIELD_PRESSURE = 4,  /* pressure of the last projection, cells */
-  FS_FIELD_DIVERGENCE = 5 /* divergence/dt of the last projection's input, cells (download only) */
+  FS_FIELD_DIVERGENCE = 5, /* divergence/dt of the last projection's input, cells (download only) */
+  FS_FIELD_ADJ_PHI = 6,   /* adjoint (bar) of phi, cells: FP64 contexts, see the adjoint entry points */
+  FS_FIELD_ADJ_U = 7,     /* adjoint of u, x faces */
+  FS_FIELD_ADJ_V = 8,     /* adjoint of v, y faces */
+  FS_FIELD_ADJ_W = 9      /* adjoint of w, z faces */
 } fs_field;
 
 typedef enum {
@@ -161,6 +165,40 @@ fs_status fs_viscosity(fs_ctx* ctx, double dt, int* iterations);
 fs_status fs_pcg_csr(fs_ctx* ctx, int n, int nnz, const double* values, const int* column_index,
                      const int* row_ptr, const double* b, double* x, double tolerance, int max_iteration,
                      int stop, int* iterations, double* residual);
+
+/* Adjoints (vector-Jacobian products) of the step and of its operators.
+ * No counterpart in the reference, which has no derivatives; they are part
+ * of this library's differentiable-simulation interface.
+ *
+ * The context's FS_FIELD_ADJ_* fields hold bars: on entry the bars of an
+ * operator's outputs, on return the bars of its inputs.  A field that is both
+ * input and output has its bar replaced; an input that is not an output has
+ * its bar added to (so compositions accumulate).  The primal fields
+ * (PHI, U, V, W) must hold the operator's INPUT state; the forward is
+ * recomputed inside the call.  The density bars d/d(rho_neg), d/d(rho_pos)
+ * accumulate in the context across calls (fs_adjoint_density_bars reads them,
+ * fs_adjoint_reset clears them and the adjoint fields).
+ *
+ * Derivatives are those of the discrete operators as computed, with the
+ * upwind sides of WENO5, the Godunov branches and sign clamp of the Sussman
+ * step and the phase (sign of phi) of each cell frozen at their forward
+ * values; the pressure and viscosity solves are differentiated as exact
+ * solves (a second solve with the same symmetric operator).  dt is a
+ * constant (not differentiated through the CFL condition).
+ * FP64 contexts with the corrected projection only (FS_NOT_SUPPORTED
+ * otherwise).  The first call allocates the adjoint buffers; fs_step_adjoint
+ * also allocates its tape (about 30 + 3*reinit_iterations fields). */
+fs_status fs_adjoint_reset(fs_ctx* ctx);
+fs_status fs_adjoint_density_bars(fs_ctx* ctx, double* rho_neg_bar, double* rho_pos_bar);
+/* Whole step: ADJ_* = bars of the step's output -> bars of its input.  The
+ * primal fields end in the step's OUTPUT state (the forward ran once). */
+fs_status fs_step_adjoint(fs_ctx* ctx, double dt, fs_step_report* report);
+/* Operator adjoints; the primal fields are left as they were. */
+fs_status fs_advect_levelset_adjoint(fs_ctx* ctx, double dt);  /* phi -> phi (u, v, w bars added) */
+fs_status fs_advect_velocity_adjoint(fs_ctx* ctx, double dt);  /* (u, v, w) -> (u, v, w) */
+fs_status fs_reinitialize_adjoint(fs_ctx* ctx);                /* phi -> phi, one block */
+fs_status fs_viscosity_adjoint(fs_ctx* ctx, double dt);        /* (u, v, w) -> (u, v, w); phi and density bars added */
+fs_status fs_project_adjoint(fs_ctx* ctx, double dt);          /* (u, v, w) -> (u, v, w); phi and density bars added */
 
 /* Allocation-free fs_pcg_csr, for callers that cannot allocate device
  * memory during a solve (a host whose device memory pool is owned by another
