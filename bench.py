@@ -154,6 +154,36 @@ def e2e_steps(fs, s, states):
     return ms, h2d, d2h
 
 
+def adjoint_steps(fs, n, warmup, steps):
+    """FP64 adjoint step (fs_step_adjoint: forward recomputed with its tape,
+    then the reverse sweep with the transposed solves) against the FP64
+    forward step from the same states, both timed by the library with CUDA
+    events.  The bars are those of L = sum(phi^2) + |u|^2 at the step's end
+    (any bar costs the same)."""
+    s = fs.Solver(n, 1.0 / n, params(fs, fs.FS_PRECISION_FP64))
+    phi, u, v, w = scene(n)
+    for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
+        s.upload(k, a)
+    for _ in range(warmup):
+        s.step(s.cfl_dt(), allow_not_converged=True)
+    fwd, adj = [], []
+    for _ in range(steps):
+        dt = s.cfl_dt()
+        st = {k: s.download(k) for k in ("phi", "u", "v", "w", "pressure")}
+        fwd.append(s.step(dt, allow_not_converged=True)["ms"])
+        bars = {k: 2.0 * s.download(k) for k in ("phi", "u", "v", "w")}
+        for k, a in st.items():
+            s.upload(k, a)
+        s.adjoint_reset()
+        for k, a in bars.items():
+            s.upload("adj_" + k, a)
+        adj.append(s.step_adjoint(dt, allow_not_converged=True)["ms"])
+    s.close()
+    f, a = float(np.mean(fwd)), float(np.mean(adj))
+    return {"ms_per_step": a, "forward_fp64_ms_per_step": f, "ratio_to_forward": a / f, "precision": "fp64",
+            "steps": steps}
+
+
 def reference_sample(n, pcg_iterations_per_projection, threads=1):
     """Time the reference's own CPU operators (oracle/_ref, built from the
     reference sources) on the same 256^3 scene and scale them to one
@@ -242,6 +272,7 @@ def main():
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"],
                     help="precision of the timed path (the headline is fp32_refine)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--e2e-steps", type=int, default=3)
     args = ap.parse_args()
 
@@ -274,7 +305,7 @@ def main():
     config = {"workload": f"rising air bubble {n}^3, density ratio 1000, one timestep (TVD-RK3, 3 projections)",
               "grid": [n, n, n], "precision": "fp32+fp64-refine", "div_tolerance": 1e-6, "cfl": 0.5,
               "l2": "inputs larger than L2 (67 MB per FP32 field), no flush", "parallelism": f"replicas{world}"}
-    metric = "timestep ms @256^3 (FP32+refine, 1e-6 relative divergence)"
+    metric = "timestep ms @256^3 (FP32+refine, 1e-6 relative divergence); adjoint/fwd ratio in adjoint"
 
     if args.impl == "reference":
         if rank != 0:
@@ -338,6 +369,11 @@ def main():
                 "speedup_fp32_refine": ms64 / ms, "max_rel_residual": max(r["max_rel_residual"] for r in reps64)}
         s64.close()
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_steps(fs, n, min(args.warmup, 1), min(args.steps, 2))
+        adjoint["ms_per_step"] = max_over_ranks(adjoint["ms_per_step"])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         iters = fp64["pcg_iterations_per_step"] / 3.0 if fp64 else 400.0
@@ -360,6 +396,7 @@ def main():
                      "bytes_per_iteration": bpu * N,
                      "pcg_ms": pcg_ms, "pcg_launched_iterations": pcg_its, "pcg_iterations": real_its},
         "fp64": fp64,
+        "adjoint": adjoint,
         "steps_detail": [{k: r[k] for k in ("ms", "pcg_iterations", "outer_iterations", "viscosity_iterations",
                                              "max_rel_residual", "div_linf", "pcg_ms")} for r in reps],
         "clocks": clk.summary(),

@@ -801,8 +801,9 @@ fs_status adj_projection(fs_ctx* c, double* phi, double* const ustar[3], const d
   // lambda = A^-1 p_bar (A symmetric): the second solve with the same operator
   int it = 0, st = 0;
   double rel = 0.0;
-  CKS(run_pcg<double>(c, 3, A, pbar, lam, (double*)c->pr, (double*)c->pp, (double*)c->pq,
-                      std::min(P.tolerance, 1e-10), std::max(P.max_iteration, 1), FS_STOP_RELATIVE, &it, &rel, &st));
+  // the adjoint solve runs to the forward's tolerance, relative to its own right-hand side
+  CKS(run_pcg<double>(c, 3, A, pbar, lam, (double*)c->pr, (double*)c->pp, (double*)c->pq, P.tolerance,
+                      std::max(P.max_iteration, 1), FS_STOP_RELATIVE, &it, &rel, &st));
   adj_sum(lam, c->Lc, c->partials, c->tickets + 4, c->scalars + 14, s);
   for (int a = 0; a < 3; ++a) adj_divergence(lam, c->scalars + 14, in_bar[a], *lays[a], c->Lc, a, dx, dt, s);
   adj_pressure_operator(phi, lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, s);
@@ -831,8 +832,8 @@ fs_status adj_viscosity(fs_ctx* c, double* phi, double* const ug[3], double* con
     Op7<double> A{(double*)c->vs[a][0], (double*)c->vs[a][1], (double*)c->vs[a][2], (double*)c->vs[a][3], *lays[a]};
     int it = 0, st = 0;
     CKS(run_pcg<double>(c, 120 + a, A, c->a_vxb[a], c->a_vlam[a], (double*)c->vs[a][6], (double*)c->vs[a][7],
-                        (double*)c->vs[a][8], std::min(P.viscosity_tolerance, 1e-12),
-                        std::max(P.viscosity_max_iteration, 1), FS_STOP_RELATIVE, &it, nullptr, &st));
+                        (double*)c->vs[a][8], P.viscosity_tolerance, std::max(P.viscosity_max_iteration, 1),
+                        FS_STOP_RELATIVE, &it, nullptr, &st));
     adj_visc(phi, ug[0], ug[1], ug[2], x[a], c->a_vlam[a], in_bar[0], in_bar[1], in_bar[2], phi_bar, c->a_rho, c->Lc,
              c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos, P.mu_neg, P.mu_pos, s);
     c->launches += 3;

@@ -230,3 +230,47 @@ def test_step_adjoint_matches_oracle_finite_differences():
     hr = 0.5
     fd = (loss_oracle(X, 1000.0 + hr) - loss_oracle(X, 1000.0 - hr)) / (2 * hr)
     assert rel(fd, rho_bar[1]) < 1e-4, (fd, rho_bar)
+
+
+def test_rollout_gradient_with_binomial_checkpointing():
+    """Loss ||phi(T) - target||^2 after 6 steps, differentiated through the
+    torch.autograd rollout (2 snapshots) and checked against central
+    differences of the plain FP64 GPU forward."""
+    import torch
+
+    from rollout import Rollout, Schedule
+    n, T, snaps = 10, 6, 2
+    X = zero_walls(scene(n, 8, vel_scale=0.1))
+    dt = 0.3 / n
+    x = (np.arange(n) + 0.5) / n
+    target = torch.from_numpy(np.broadcast_to(x[None, :, None] - 0.3, (n, n, n)).copy())
+    with solver(n) as s:
+        ts = {k: torch.tensor(X[k], requires_grad=True) for k in ("phi", "u", "v", "w")}
+        rho = torch.tensor(1000.0, dtype=torch.float64, requires_grad=True)
+        sched = Schedule()
+        out = Rollout.apply(ts["phi"], ts["u"], ts["v"], ts["w"], rho, s, dt, T, snaps, sched)
+        loss = torch.sum((out[0] - target) ** 2)
+        loss.backward()
+        assert sched.adjoint_steps == T
+        assert sched.max_live_snapshots <= snaps
+        grad = {k: ts[k].grad.numpy() for k in ("u", "v", "w")}
+        g_rho = float(rho.grad)
+
+        def loss_fd(st, rho_pos):
+            s.set_params(rho_pos=rho_pos)
+            load(s, st)
+            for _ in range(T):
+                s.step(dt)
+            return float(np.sum((s.download("phi") - target.numpy()) ** 2))
+
+        h = 1e-6
+        for d in range(3):
+            dX = zero_walls(rand_like(X, np.random.default_rng(200 + d), FIELDS_VEL))
+            plus = {k: X[k] + h * dX[k] if k in dX else X[k] for k in X}
+            minus = {k: X[k] - h * dX[k] if k in dX else X[k] for k in X}
+            fd = (loss_fd(plus, 1000.0) - loss_fd(minus, 1000.0)) / (2 * h)
+            ad = dot(grad, dX, FIELDS_VEL)
+            assert rel(fd, ad) < 1e-4, (d, fd, ad)
+        hr = 0.5
+        fd = (loss_fd(X, 1000.0 + hr) - loss_fd(X, 1000.0 - hr)) / (2 * hr)
+        assert rel(fd, g_rho) < 1e-3, (fd, g_rho)
