@@ -430,8 +430,10 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update(Op7<V> A, V* __restri
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       if (m < nvalid) {
-        const double rd = (double)lane(rv, m);
-        rz += rd * (rd / (double)lane(dv, m));
+        // z = r/diag in the vector type, as the direction update forms it
+        const V rm = lane(rv, m);
+        const double rd = (double)rm;
+        rz += rd * (double)(rm / lane(dv, m));
         rr += rd * rd;
       }
     }
