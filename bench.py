@@ -261,6 +261,43 @@ def reference_sample_isolated(n, iters, threads=1):
     return None, f"reference sample failed (rc={p.returncode}): {p.stderr.strip()[-300:]}"
 
 
+def init_replicas(backend="nccl"):
+    """One process per GPU, each running an independent replica of the
+    workload ("replicas only": the path has no exchange step).  Returns the
+    rank layout, the process group module (None for one process) and the two
+    collectives the benchmark uses: a barrier around the timed region and the
+    max over ranks of a per-rank time.  With backend "gloo" everything stays
+    on the CPU (used by the multi-process tests)."""
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    device = "cpu" if backend == "gloo" else "cuda"
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        if device == "cuda":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    elif device == "cuda":
+        torch.cuda.set_device(0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return world, rank, local, dist, barrier, max_over_ranks
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -276,30 +313,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     args = ap.parse_args()
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    import torch
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    else:
-        torch.cuda.set_device(0)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    world, rank, local, dist, barrier, max_over_ranks = init_replicas("nccl")
 
     n = args.n
     config = {"workload": f"rising air bubble {n}^3, density ratio 1000, one timestep (TVD-RK3, 3 projections)",
