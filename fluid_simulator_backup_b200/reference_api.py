@@ -23,9 +23,10 @@ class GRID_STRUCTURE_3D:
         self.i_start, self.j_start, self.k_start = (int(a) for a in start)
         self.x_min, self.y_min, self.z_min = (float(a) for a in mn)
         self.x_max, self.y_max, self.z_max = (float(a) for a in mx)
-        self.dx = (self.x_max - self.x_min) / (self.i_res - 1)
-        self.dy = (self.y_max - self.y_min) / (self.j_res - 1)
-        self.dz = (self.z_max - self.z_min) / (self.k_res - 1)
+        # a one-cell axis (the default-constructed grid) has no spacing of its own
+        self.dx = (self.x_max - self.x_min) / max(self.i_res - 1, 1)
+        self.dy = (self.y_max - self.y_min) / max(self.j_res - 1, 1)
+        self.dz = (self.z_max - self.z_min) / max(self.k_res - 1, 1)
 
     def InitializeFromBlock(self, block):
         self.__init__(block.GetVector3("base_grid_resolution", (1, 1, 1)), block.GetVector3("start_indices", (0, 0, 0)),
