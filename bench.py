@@ -39,6 +39,11 @@ sys.path.insert(0, ROOT)
 BYTES_PER_UNKNOWN_PCG_FP32 = 68
 # FP64: spmv 40 + residual update 32 + direction update 48
 BYTES_PER_UNKNOWN_PCG_FP64 = 120
+# DRAM bytes (read + write) of one FP32 PCG iteration at 256^3 measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of k_cg_spmv, k_cg_update,
+# k_cg_pupdate; profiles/pcg_iteration_fp32refine_256.md); scaled by the
+# unknowns for other sizes
+TRAFFIC_PER_ITERATION_256_FP32 = 1089.1e6
 # PCG iterations per projection of the FP64 GPU path on this workload at 256^3
 # (6725 per timestep of 3 projections over steps 4-6, measured by the default
 # run's fp64 block); the reference arm prices its projection with it
@@ -406,7 +411,10 @@ def main():
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (spmv + update + direction, 3 kernels)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_src, "traffic": None,
+                     "peak_source": peak_src,
+                     "traffic": (TRAFFIC_PER_ITERATION_256_FP32 * N / 256 ** 3
+                                 if main_prec == fs.FS_PRECISION_FP32_REFINE else None),
+                     "traffic_unit": "bytes per PCG iteration (ncu capture at 256^3, scaled by unknowns)",
                      "bytes_per_iteration": bpu * N,
                      "pcg_ms": pcg_ms, "pcg_launched_iterations": pcg_its, "pcg_iterations": real_its},
         "fp64": fp64,
