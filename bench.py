@@ -41,8 +41,8 @@ BYTES_PER_UNKNOWN_PCG_FP32 = 68
 BYTES_PER_UNKNOWN_PCG_FP64 = 120
 # DRAM bytes (read + write) of one FP32 PCG iteration at 256^3 measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum of k_cg_spmv, k_cg_update,
-# k_cg_pupdate; profiles/pcg_iteration_fp32refine_256.md); scaled by the
-# unknowns for other sizes
+# k_cg_pupdate, one capture of the bench workload); scaled by the unknowns
+# for other sizes
 TRAFFIC_PER_ITERATION_256_FP32 = 1089.1e6
 # PCG iterations per projection of the FP64 GPU path on this workload at 256^3
 # (6725 per timestep of 3 projections over steps 4-6, measured by the default
