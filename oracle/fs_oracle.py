@@ -417,6 +417,111 @@ def pcg(apply_A, diag, b, x0, tol, max_iter, criterion="abs"):
     return x, it, rz, math.sqrt(_seqdot(r, r)) / bnorm
 
 
+# ----------------------------------------------------------------------------
+# Surface tension (LEVELSET_3D.h:963-1082, PROJECTION_3D.h:746-792,
+# POISSON_SOLVER_3D.h:1216-1328, EULERIAN_FLUID_SOLVER_3D.h:2741-2745)
+# ----------------------------------------------------------------------------
+
+def curvature(phi, dx, typo=False):
+    """LEVELSET_3D::ComputeCurvatures (curvature_by_levelset): kappa from
+    central differences of the level set with one layer of linearly
+    extrapolated ghosts,
+      kappa = -(px^2 pyy - 2 px py pxy + py^2 pxx + px^2 pzz - 2 px pz pxz
+                + pz^2 pxx + py^2 pzz - 2 py pz pyz + pz^2 pyy) / |grad phi|^3,
+    clamped from below at -1/dx (:1061-1068).  typo=True reproduces the
+    reference's two slips: the factor 2 missing on the py pz pyz term
+    (:1033) and, in the zero-gradient fallback of one-sided differences, the
+    z difference multiplied by dz instead of divided (:1037).  Where even the
+    fallback gradient is zero the reference exits the process (:1040-1044);
+    kappa is 0 there.  Returns (kappa, max |kappa| over cells with |phi| < 0.1)."""
+    a = extrapolate_ghosts(phi, 1)
+    nz, ny, nx = phi.shape
+
+    def at(di, dj, dk):
+        return a[1 + dk:1 + dk + nz, 1 + dj:1 + dj + ny, 1 + di:1 + di + nx]
+
+    inv = 1.0 / dx
+    o2 = 0.5 / dx
+    o2sq = 1.0 / (dx * dx)
+    c = at(0, 0, 0)
+    px = (at(1, 0, 0) - at(-1, 0, 0)) * o2
+    py = (at(0, 1, 0) - at(0, -1, 0)) * o2
+    pz = (at(0, 0, 1) - at(0, 0, -1)) * o2
+    pxx = ((at(1, 0, 0) - 2 * c) + at(-1, 0, 0)) * o2sq
+    pyy = ((at(0, 1, 0) - 2 * c) + at(0, -1, 0)) * o2sq
+    pzz = ((at(0, 0, 1) - 2 * c) + at(0, 0, -1)) * o2sq
+    pxy = ((((at(1, 1, 0) - at(1, -1, 0)) - at(-1, 1, 0)) + at(-1, -1, 0)) * o2) * o2
+    pxz = ((((at(1, 0, 1) - at(1, 0, -1)) - at(-1, 0, 1)) + at(-1, 0, -1)) * o2) * o2
+    pyz = ((((at(0, 1, 1) - at(0, 1, -1)) - at(0, -1, 1)) + at(0, -1, -1)) * o2) * o2
+
+    def num(px, py, pz):
+        t = px * px * pyy - 2.0 * px * py * pxy
+        t = t + py * py * pxx
+        t = t + px * px * pzz
+        t = t - 2.0 * px * pz * pxz
+        t = t + pz * pz * pxx
+        t = t + py * py * pzz
+        t = t - (py * pz * pyz if typo else 2.0 * py * pz * pyz)
+        return t + pz * pz * pyy
+
+    mag = np.sqrt((px * px + py * py) + pz * pz)
+    deno = mag * mag * mag
+    with np.errstate(divide="ignore", invalid="ignore"):
+        curv = -num(px, py, pz) * (1.0 / deno)
+        # fallback: one-sided differences where the central gradient vanishes
+        fx = (at(1, 0, 0) - c) * inv
+        fy = (at(0, 1, 0) - c) * inv
+        fz = (at(0, 0, 1) - c) * (dx if typo else inv)
+        fm = np.sqrt((fx * fx + fy * fy) + fz * fz)
+        fd = fm * fm * fm
+        fcurv = np.where(fd != 0, -num(fx, fy, fz) * (1.0 / fd), 0.0)
+    curv = np.where(deno != 0, curv, fcurv)
+    tol = 1.0 / dx
+    kappa = np.where(curv < -tol, -tol, curv)
+    band = np.abs(phi) < 1e-1
+    kmax = float(np.max(np.abs(kappa[band]))) if band.any() else 0.0
+    return kappa, kmax
+
+
+def jump_rhs(phi, jc, dx, rho_neg, rho_pos):
+    """Sum over the six arms of the ghost-fluid jump terms F of the pressure
+    right-hand side b = -div - F_X - F_Y - F_Z (POISSON_SOLVER_3D.h:1216-1328)
+    with jc_on_derivative = 0: an arm whose two cells lie in different phases
+    carries F = +-inv_dx2 * a * beta, a = (jc_c |phi_n| + jc_n |phi_c|) /
+    (|phi_c| + |phi_n|), + when the cell is in the phi <= 0 phase.  Arms to
+    the wall ghosts use the extrapolated ghost phi, jc = 0 and the clamped
+    1/rho.  Returns (F_X, F_Y, F_Z)."""
+    pg = extrapolate_ghosts(phi, 1)
+    var = 1.0 / np.where(phi <= 0, rho_neg, rho_pos)
+    vg = np.pad(var, 1, mode="edge")
+    jg = np.pad(jc, 1)
+    nz, ny, nx = phi.shape
+    inv2 = 1.0 / (dx * dx)
+
+    def nb(arr, di, dj, dk):
+        return arr[1 + dk:1 + dk + nz, 1 + dj:1 + dj + ny, 1 + di:1 + di + nx]
+
+    pc, vc, jcc = phi, var, jc
+    ac = np.abs(pc)
+    out = []
+    for (lo, hi) in (((-1, 0, 0), (1, 0, 0)), ((0, -1, 0), (0, 1, 0)), ((0, 0, -1), (0, 0, 1))):
+        F = []
+        for d, low in ((lo, True), (hi, False)):
+            pn, vn, jn = nb(pg, *d), nb(vg, *d), nb(jg, *d)
+            an = np.abs(pn)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                a = (jcc * an + jn * ac) / (ac + an)
+                if low:   # l, b, d arms
+                    beta = vc * vn * (an + ac) / (vc * an + vn * ac)
+                else:     # r, t, u arms
+                    beta = vc * vn * (an + ac) / (vn * ac + vc * an)
+            f = np.where((pc <= 0) & (pn > 0), inv2 * a * beta,
+                         np.where((pc > 0) & (pn <= 0), -inv2 * a * beta, 0.0))
+            F.append(f)
+        out.append(F[0] + F[1])
+    return tuple(out)
+
+
 def velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode="corrected", jc=None):
     """UpdateVelocityByPressureGradientVariableDensity (PROJECTION_3D.h:1099-1449).
 
@@ -468,7 +573,8 @@ def velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode="correct
                 f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0) * (1.0 / rho_c[0, 0, 0]) * inv
             else:
                 rf = mix(rho_neg, rho_pos, heaviside_projection(np.array(fphi), e))
-                jmp = 0.0
+                # the ghost jump condition is 0 (jc_on_solution is zero outside the box)
+                jmp = (jc[0, 0, 0] * abs(g) + 0.0 * abs(c)) / (abs(g) + abs(c))
                 if c <= 0:
                     f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0 + jmp) * (1.0 / rf) * inv
                 else:
@@ -476,18 +582,28 @@ def velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode="correct
     return tuple(out)
 
 
-def projection(phi, u, v, w, dx, dt, rho_neg, rho_pos, tol, max_iter, mode="corrected", criterion="abs", p0=None):
+def projection(phi, u, v, w, dx, dt, rho_neg, rho_pos, tol, max_iter, mode="corrected", criterion="abs", p0=None,
+               sigma=0.0, curvature_typo=False):
     """PROJECTION_3D::Solve for the air/water box with Neumann walls:
-    divergence, operator, RHS = -div minus its mean (POISSON_SOLVER_3D.h:225-246),
-    Jacobi-PCG, velocity correction.  Returns (u, v, w, p, info)."""
+    divergence, jump condition jc = sigma*kappa (DetermineJumpConditionField,
+    PROJECTION_3D.h:746-792), operator, RHS = -div - F (jump terms) minus its
+    mean (POISSON_SOLVER_3D.h:225-246), Jacobi-PCG, velocity correction with
+    the jump.  Returns (u, v, w, p, info)."""
     div = divergence(u, v, w, dx, dt)
     op = poisson_operator(phi, dx, rho_neg, rho_pos)
-    b = -div
+    jc = None
+    if sigma != 0.0:
+        kappa, _ = curvature(phi, dx, curvature_typo)
+        jc = sigma * kappa
+        FX, FY, FZ = jump_rhs(phi, jc, dx, rho_neg, rho_pos)
+        b = ((-div - FX) - FY) - FZ
+    else:
+        b = -div
     b = b - (1.0 / b.size) * _seqsum(b)
     x0 = np.zeros_like(b) if p0 is None else p0
     p, it, rz, rel = pcg(lambda x: apply_poisson(op, x), op[3], b, x0, tol, max_iter, criterion)
-    u2, v2, w2 = velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode)
-    return u2, v2, w2, p, {"iterations": it, "rz": rz, "rel_residual": rel, "b": b, "op": op}
+    u2, v2, w2 = velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode, jc=jc)
+    return u2, v2, w2, p, {"iterations": it, "rz": rz, "rel_residual": rel, "b": b, "op": op, "jc": jc}
 
 
 # ----------------------------------------------------------------------------
@@ -753,7 +869,8 @@ def step(phi, u, v, w, dx, dt, P, p0=None, order=3):
             a, _ = viscosity_semi_implicit(phin, *a, dx, dt, P["rho_neg"], P["rho_pos"], P["mu_neg"], P["mu_pos"],
                                            P["visc_tol"], 10000, "rel")
         uu, vv, ww, p, pi = projection(phin, *a, dx, dt, P["rho_neg"], P["rho_pos"], P["tol"], P["max_iter"],
-                                       mode="corrected", criterion="rel", p0=p)
+                                       mode="corrected", criterion="rel", p0=p, sigma=P.get("sigma", 0.0),
+                                       curvature_typo=P.get("curvature_typo", False))
         info["iterations"].append(pi["iterations"])
         info["rel_residual"].append(pi["rel_residual"])
         out = (uu, vv, ww)

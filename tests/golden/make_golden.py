@@ -17,6 +17,8 @@ on the air/water unit-cube box with Neumann pressure walls:
                    update (the reference as it runs: only w corrected)
   semi_implicit_*  POISSON_SOLVER_3D::SolveForViscosity on seeded coefficients
   cfl              EULERIAN_FLUID_SOLVER_3D::CFLOneTimeStep
+  projection_tension  curvature (LEVELSET_3D::ComputeCurvatures) and
+                   PROJECTION_3D::Solve with a surface tension jump condition
 """
 import os
 import sys
@@ -134,6 +136,26 @@ def main():
     for k, a in vel.items():
         c.set(k, a)
     fixtures["cfl"] = dict(n=n, dx=c.dx, gravity_y=-9.8, nu_max=max(1e-3 / 1000.0, 1.8e-5 / 1.0), **vel, out=c.cfl())
+    c.close()
+
+    # Surface tension (sigma = 0.0728, air bubble in water), 10^3: the
+    # curvature of a perturbed sphere (LEVELSET_3D::ComputeCurvatures) and a
+    # projection whose right-hand side and velocity update carry the jump
+    # condition sigma*kappa
+    n = 10
+    c = case(n, water_drop=False, tolerance=1e-9, surface_tension=0.0728)
+    phi = sphere(n, (0.5, 0.4, 0.5), 0.3) + 1e-3 * rng.normal(size=(n, n, n))
+    vel = {k: rng.normal(size=c.shape(k)) * 0.3 for k in "uvw"}
+    for k, a in vel.items():
+        c.set(k, a)
+    c.set("phi", phi)
+    kappa = c.curvature()
+    it = c.projection(2e-3)
+    vals, cols, rowptr, b, x = c.poisson_csr()
+    fixtures["projection_tension"] = dict(n=n, dx=c.dx, dt=2e-3, tol=1e-9, rho_neg=1.0, rho_pos=1000.0, sigma=0.0728,
+                                          phi=phi, **vel, kappa=kappa, iterations=it, csr_vals=vals, csr_cols=cols,
+                                          csr_rowptr=rowptr, b=b, x=x, out_p=c.get("p"), out_u=c.get("u"),
+                                          out_v=c.get("v"), out_w=c.get("w"))
     c.close()
 
     for name, d in fixtures.items():
