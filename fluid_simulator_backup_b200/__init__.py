@@ -26,17 +26,17 @@ LIB_PATH = os.path.join(HERE, "libfluidb200.so")
 
 FS_OK, FS_INVALID_ARG, FS_OOM, FS_NOT_CONVERGED, FS_NONFINITE, FS_CUDA_ERROR, FS_TIMEOUT, FS_NOT_SUPPORTED = range(8)
 FIELD = {"phi": 0, "u": 1, "v": 2, "w": 3, "pressure": 4, "p": 4, "divergence": 5,
-         "adj_phi": 6, "adj_u": 7, "adj_v": 8, "adj_w": 9}
+         "adj_phi": 6, "adj_u": 7, "adj_v": 8, "adj_w": 9, "curvature": 10}
 FS_PRECISION_FP64, FS_PRECISION_FP32_REFINE = 0, 1
 FS_STOP_RELATIVE, FS_STOP_ABSOLUTE = 0, 1
-FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER = 1, 2, 4
+FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER, FS_FLAG_CURVATURE_TYPO = 1, 2, 4, 8
 
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
             "fs_memory_bytes", "fs_upload", "fs_download", "fs_upload_device", "fs_download_device", "fs_step",
             "fs_cfl_dt", "fs_project", "fs_advect_levelset", "fs_advect_velocity", "fs_reinitialize",
             "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc", "fs_adjoint_reset", "fs_adjoint_density_bars",
             "fs_step_adjoint", "fs_advect_levelset_adjoint", "fs_advect_velocity_adjoint", "fs_reinitialize_adjoint",
-            "fs_viscosity_adjoint", "fs_project_adjoint")
+            "fs_viscosity_adjoint", "fs_project_adjoint", "fs_curvature")
 
 
 class FsError(RuntimeError):
@@ -56,7 +56,8 @@ class Params(ctypes.Structure):
                 ("precision", ctypes.c_int), ("stop", ctypes.c_int), ("tolerance", ctypes.c_double),
                 ("max_iteration", ctypes.c_int), ("inner_tolerance", ctypes.c_double), ("max_outer", ctypes.c_int),
                 ("viscosity", ctypes.c_int), ("viscosity_tolerance", ctypes.c_double),
-                ("viscosity_max_iteration", ctypes.c_int), ("cfl", ctypes.c_double), ("flags", ctypes.c_int)]
+                ("viscosity_max_iteration", ctypes.c_int), ("cfl", ctypes.c_double), ("flags", ctypes.c_int),
+                ("surface_tension", ctypes.c_double)]
 
     def as_dict(self):
         d = {}
@@ -123,6 +124,7 @@ def lib():
                                  ctypes.c_int, ip, dp]
         L.fs_pcg_csr_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_int, vp, ip, dp]
+        L.fs_curvature.argtypes = [vp, dp]
         L.fs_adjoint_reset.argtypes = [vp]
         L.fs_adjoint_density_bars.argtypes = [vp, dp, dp]
         L.fs_step_adjoint.argtypes = [vp, ctypes.c_double, ctypes.POINTER(StepReport)]
@@ -169,7 +171,7 @@ def field_shape(n, name):
     if name.startswith("adj_"):
         name = name[4:]
     return {"phi": (nz, ny, nx), "pressure": (nz, ny, nx), "p": (nz, ny, nx), "divergence": (nz, ny, nx),
-            "u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx)}[name]
+            "curvature": (nz, ny, nx), "u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx)}[name]
 
 
 class Solver:
@@ -285,6 +287,12 @@ class Solver:
         it = ctypes.c_int()
         _check(lib().fs_viscosity(self._h, float(dt), ctypes.byref(it)), "fs_viscosity")
         return it.value
+
+    def curvature(self):
+        """Mean curvature of the current level set and max |kappa| over |phi| < 0.1."""
+        m = ctypes.c_double()
+        _check(lib().fs_curvature(self._h, ctypes.byref(m)), "fs_curvature")
+        return self.download("curvature"), m.value
 
     # ---- adjoints (FP64 contexts): bars live in the adj_* fields
     def adjoint_reset(self):

@@ -79,6 +79,7 @@ struct fs_ctx {
   void *ua = nullptr, *va = nullptr, *wa = nullptr;
   // pressure (FP64) and projection work
   double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *p64bak = nullptr;
+  double* kappa = nullptr;  // mean curvature (surface tension)
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
@@ -182,6 +183,10 @@ fs_status check_params(const fs_params* p) {
     return FS_INVALID_ARG;
   }
   if (p->stop != FS_STOP_RELATIVE && p->stop != FS_STOP_ABSOLUTE) { set_error("unknown stop criterion"); return FS_INVALID_ARG; }
+  if (!(p->surface_tension >= 0) || !std::isfinite(p->surface_tension)) {
+    set_error("surface_tension must be finite and non-negative");
+    return FS_INVALID_ARG;
+  }
   if (!(p->tolerance >= 0) || p->max_iteration < 0 || p->reinit_iterations < 0 || p->reinit_scaling <= 0) {
     set_error("bad solver or reinitialisation settings");
     return FS_INVALID_ARG;
@@ -412,6 +417,18 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
   S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w), *phi = F<S>(c->phi);
   divergence_rhs<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, dt, c->b64, c->div64, c->partials, c->tickets + 0,
                     c->scalars + 0, s);
+  // surface tension: curvature, jc = sigma kappa, and the jump terms of the
+  // right-hand side (DetermineJumpConditionField, PROJECTION_3D.h:746-792)
+  const double sigma = P.surface_tension;
+  const double* kap = nullptr;
+  if (sigma != 0.0) {
+    fill_extrap<S>(phi, c->Lc, s);
+    curvature<S>(phi, c->kappa, c->Lc, dx, (P.flags & FS_FLAG_CURVATURE_TYPO) ? 1 : 0, c->scalars + 13, s);
+    jump_rhs<S>(phi, c->kappa, sigma, c->b64, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials, c->tickets + 5,
+                c->scalars + 0, s);
+    kap = c->kappa;
+    c->launches += 3;
+  }
   subtract_mean(c->b64, c->Lc, c->scalars + 0, c->partials, c->tickets + 1, c->scalars + 1, s);
   c->launches += 4;  // divergence, mean, pressure faces, pressure diagonal
   CK(cudaGetLastError());
@@ -526,9 +543,12 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       c->pcg_ms += ms;
     }
   }
-  velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
-  velocity_correct<S>(v, F<S>(c->v0), c->p64, phi, c->Lv, c->Lc, 1, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
-  velocity_correct<S>(w, F<S>(c->w0), c->p64, phi, c->Lw, c->Lc, 2, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1, s);
+  velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
+                      kap, sigma, s);
+  velocity_correct<S>(v, F<S>(c->v0), c->p64, phi, c->Lv, c->Lc, 1, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
+                      kap, sigma, s);
+  velocity_correct<S>(w, F<S>(c->w0), c->p64, phi, c->Lw, c->Lc, 2, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
+                      kap, sigma, s);
   c->launches += 3;
   CK(cudaGetLastError());
   if (rep) {
@@ -639,11 +659,23 @@ fs_status step_t(fs_ctx* c, double dt, fs_step_report* rep, Tape* tp = nullptr) 
 }
 
 template <class S>
+fs_status curvature_t(fs_ctx* c) {
+  const fs_params& P = c->prm;
+  fill_extrap<S>(F<S>(c->phi), c->Lc, c->stream);
+  curvature<S>(F<S>(c->phi), c->kappa, c->Lc, c->grid.dx, (P.flags & FS_FLAG_CURVATURE_TYPO) ? 1 : 0,
+               c->scalars + 13, c->stream);
+  c->launches += 2;
+  CK(cudaGetLastError());
+  return FS_OK;
+}
+
+template <class S>
 fs_status cfl_t(fs_ctx* c, double* dt) {
   absmax3<S>(F<S>(c->u), F<S>(c->v), F<S>(c->w), c->Lu, c->Lv, c->Lw, c->scalars + 8, c->stream);
   c->launches += 3;
+  if (c->prm.surface_tension != 0.0) CKS(curvature_t<S>(c));
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c->sc_host + 8, c->scalars + 8, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->sc_host + 8, c->scalars + 8, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   const fs_params& P = c->prm;
   const double inv = 1.0 / c->grid.dx, inv2 = 1.0 / (c->grid.dx * c->grid.dx);
@@ -652,8 +684,13 @@ fs_status cfl_t(fs_ctx* c, double* dt) {
   // semi-implicit viscosity imposes no limit; explicit (off) uses the reference's term
   const double nu = P.viscosity ? 0.0 : std::max(P.mu_neg / P.rho_neg, P.mu_pos / P.rho_pos);
   const double v_f = nu * ((2.0 * inv2 + 2.0 * inv2) + 2.0 * inv2);
+  // surface tension (EULERIAN_FLUID_SOLVER_3D.h:2741-2745): sqrt(sigma kappa_max / (min rho dx^2))
+  const double s_f = P.surface_tension != 0.0
+                         ? std::sqrt((P.surface_tension * c->sc_host[13]) /
+                                     (std::min(P.rho_neg, P.rho_pos) * (c->grid.dx * c->grid.dx)))
+                         : 0.0;
   const double cv = c_f + v_f;
-  const double cfl = 0.5 * (cv + std::sqrt(cv * cv + 4.0 * (g_f * g_f)));
+  const double cfl = 0.5 * (cv + std::sqrt((cv * cv + 4.0 * (g_f * g_f)) + 4.0 * (s_f * s_f)));
   *dt = P.cfl / cfl;
   return FS_OK;
 }
@@ -857,6 +894,10 @@ fs_status adj_velocity_advect(fs_ctx* c, double* const uin[3], double* const out
 
 fs_status adj_check(fs_ctx* c) {
   if (c->fp32) { set_error("adjoints are built for FP64 contexts"); return FS_NOT_SUPPORTED; }
+  if (c->prm.surface_tension != 0.0) {
+    set_error("adjoints do not cover the surface-tension jump terms");
+    return FS_NOT_SUPPORTED;
+  }
   if (c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) {
     set_error("adjoints follow the corrected projection only");
     return FS_NOT_SUPPORTED;
@@ -1058,7 +1099,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   for (void** p : fu) if ((s = dalloc(c, p, ub)) != FS_OK) return fail(s);
   for (void** p : fv) if ((s = dalloc(c, p, vb)) != FS_OK) return fail(s);
   for (void** p : fw) if ((s = dalloc(c, p, wb)) != FS_OK) return fail(s);
-  double** d8[] = {&c->p64, &c->b64, &c->div64};
+  double** d8[] = {&c->p64, &c->b64, &c->div64, &c->kappa};
   for (double** p : d8) if ((s = dalloc(c, (void**)p, c8)) != FS_OK) return fail(s);
   if (c->fp32 && (s = dalloc(c, (void**)&c->p64bak, c8)) != FS_OK) return fail(s);
   void** pv[] = {&c->pax, &c->pay, &c->paz, &c->pdiag, &c->pr, &c->pp, &c->pq};
@@ -1149,6 +1190,7 @@ static fs_status upload_from_staging(fs_ctx* c, int field) {
 static fs_status download_to_staging(fs_ctx* c, int field) {
   const Lay& L = lay_of(c, field);
   if (is_adjoint_field(field)) pack_to_double<double>(c->staging, c->abar[field - FS_FIELD_ADJ_PHI], L, c->stream);
+  else if (field == FS_FIELD_CURVATURE) pack_to_double<double>(c->staging, c->kappa, L, c->stream);
   else if (field == FS_FIELD_PRESSURE) pack_to_double<double>(c->staging, c->p64, L, c->stream);
   else if (field == FS_FIELD_DIVERGENCE) pack_to_double<double>(c->staging, c->div64, L, c->stream);
   else {
@@ -1168,6 +1210,7 @@ static int64_t field_count(const fs_ctx* c, int field) {
 // fields accepted by upload (0..4 and the adjoint fields) and download (0..5 and the adjoint fields)
 static fs_status check_field(fs_ctx* c, int field, bool upload) {
   if (is_adjoint_field(field)) return adj_check(c);
+  if (field == FS_FIELD_CURVATURE && !upload) return FS_OK;
   if (field < FS_FIELD_PHI || field > (upload ? FS_FIELD_PRESSURE : FS_FIELD_DIVERGENCE)) {
     set_error("field %d cannot be %s", field, upload ? "uploaded" : "downloaded");
     return FS_INVALID_ARG;
@@ -1236,6 +1279,7 @@ fs_status fs_download_device(fs_ctx* c, int field, double* dev) {
   CKS(check_field(c, field, false));
   const Lay& L = lay_of(c, field);
   if (is_adjoint_field(field)) pack_to_double<double>(dev, c->abar[field - FS_FIELD_ADJ_PHI], L, c->stream);
+  else if (field == FS_FIELD_CURVATURE) pack_to_double<double>(dev, c->kappa, L, c->stream);
   else if (field == FS_FIELD_PRESSURE) pack_to_double<double>(dev, c->p64, L, c->stream);
   else if (field == FS_FIELD_DIVERGENCE) pack_to_double<double>(dev, c->div64, L, c->stream);
   else if (c->fp32) pack_to_double<float>(dev, (const float*)*field_ptr(c, field), L, c->stream);
@@ -1276,6 +1320,15 @@ fs_status fs_step(fs_ctx* c, double dt, fs_step_report* rep) {
   r->pcg_launched_iterations = c->pcg_launched_iterations;
   r->kernel_launches = c->launches;
   return s;
+}
+
+fs_status fs_curvature(fs_ctx* c, double* kappa_max) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(DISPATCH(c, curvature_t, c));
+  CK(cudaMemcpyAsync(c->sc_host + 13, c->scalars + 13, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (kappa_max) *kappa_max = c->sc_host[13];
+  return FS_OK;
 }
 
 fs_status fs_cfl_dt(fs_ctx* c, double* dt) {

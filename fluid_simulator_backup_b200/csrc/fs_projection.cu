@@ -188,7 +188,8 @@ __device__ __forceinline__ double heaviside_proj(double phi, double e) {
 template <class T>
 __global__ void k_velocity_correct(T* __restrict__ f, const T* __restrict__ base, const double* __restrict__ p,
                                    const T* __restrict__ phi, Lay Lf, Lay Lc, int axis, double inv_h, double dt,
-                                   double rn, double rp, int faithful, double c0, double c1) {
+                                   double rn, double rp, int faithful, double c0, double c1,
+                                   const double* __restrict__ kappa, double sigma) {
   FS_IJK(Lf);
   const int64_t fc = Lf.at(i, j, k);
   double val = (double)f[fc];
@@ -212,11 +213,128 @@ __global__ void k_velocity_correct(T* __restrict__ f, const T* __restrict__ base
     } else {
       const double ef = 1.5 / inv_h;
       const double rho_f = rn + (rp - rn) * heaviside_proj(0.5 * (phc + phn), ef);
-      upd = dt * dp * (1.0 / rho_f) * inv_h;  // jump term: zero without surface tension
+      double jump = 0.0;
+      if (kappa) {
+        // jc interpolated to the interface (PROJECTION_3D.h:1181); the ghost jc is 0
+        const double jcc = sigma * kappa[c], jcn = interior ? sigma * kappa[c - step] : 0.0;
+        jump = (jcc * fabs(phn) + jcn * fabs(phc)) / (fabs(phn) + fabs(phc));
+      }
+      upd = dt * (phc <= 0.0 ? dp + jump : dp - jump) * (1.0 / rho_f) * inv_h;
     }
     val -= upd;
   }
   f[fc] = c0 == 0.0 ? (T)val : (T)(c0 * (double)base[fc] + c1 * val);
+}
+
+// ---------------------------------------------------------------------------
+// Surface tension (LEVELSET_3D.h:963-1082, POISSON_SOLVER_3D.h:1216-1328)
+// ---------------------------------------------------------------------------
+
+// Mean curvature from central differences of phi (ghosts extrapolated):
+// kappa = -(px^2 pyy - 2 px py pxy + py^2 pxx + px^2 pzz - 2 px pz pxz
+//           + pz^2 pxx + py^2 pzz - 2 py pz pyz + pz^2 pyy) / |grad phi|^3,
+// clamped below at -1/dx.  typo reproduces the reference's missing factor 2
+// on the py pz pyz term and its dz (not 1/dz) in the zero-gradient
+// fallback; where the fallback gradient is zero too (the reference exits
+// there) kappa is 0.  kmax: max |kappa| over cells with |phi| < 0.1.
+__device__ __forceinline__ double curv_num(double px, double py, double pz, double pxx, double pyy, double pzz,
+                                           double pxy, double pxz, double pyz, int typo) {
+  double t = px * px * pyy - 2.0 * px * py * pxy;
+  t = t + py * py * pxx;
+  t = t + px * px * pzz;
+  t = t - 2.0 * px * pz * pxz;
+  t = t + pz * pz * pxx;
+  t = t + py * py * pzz;
+  t = t - (typo ? py * pz * pyz : 2.0 * py * pz * pyz);
+  return t + pz * pz * pyy;
+}
+
+template <class T>
+__global__ void k_curvature(const T* __restrict__ phi, double* __restrict__ kappa, Lay L, double dx, int typo,
+                            double* kmax) {
+  double m = 0.0;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i < L.nx && j < L.ny && k < L.nz) {
+    const int64_t c = L.at(i, j, k), sy = L.px, sz = L.slab;
+    auto f = [&](int64_t o) { return (double)phi[c + o]; };
+    const double inv = 1.0 / dx, o2 = 0.5 / dx, o2sq = 1.0 / (dx * dx);
+    const double pc = f(0);
+    const double px = (f(1) - f(-1)) * o2, py = (f(sy) - f(-sy)) * o2, pz = (f(sz) - f(-sz)) * o2;
+    const double pxx = ((f(1) - 2.0 * pc) + f(-1)) * o2sq;
+    const double pyy = ((f(sy) - 2.0 * pc) + f(-sy)) * o2sq;
+    const double pzz = ((f(sz) - 2.0 * pc) + f(-sz)) * o2sq;
+    const double pxy = ((((f(1 + sy) - f(1 - sy)) - f(-1 + sy)) + f(-1 - sy)) * o2) * o2;
+    const double pxz = ((((f(1 + sz) - f(1 - sz)) - f(-1 + sz)) + f(-1 - sz)) * o2) * o2;
+    const double pyz = ((((f(sy + sz) - f(sy - sz)) - f(-sy + sz)) + f(-sy - sz)) * o2) * o2;
+    const double mag = sqrt((px * px + py * py) + pz * pz);
+    const double deno = mag * mag * mag;
+    double curv;
+    if (deno != 0.0) {
+      curv = -curv_num(px, py, pz, pxx, pyy, pzz, pxy, pxz, pyz, typo) * (1.0 / deno);
+    } else {
+      const double fx = (f(1) - pc) * inv, fy = (f(sy) - pc) * inv, fz = (f(sz) - pc) * (typo ? dx : inv);
+      const double fm = sqrt((fx * fx + fy * fy) + fz * fz), fd = fm * fm * fm;
+      curv = fd != 0.0 ? -curv_num(fx, fy, fz, pxx, pyy, pzz, pxy, pxz, pyz, typo) * (1.0 / fd) : 0.0;
+    }
+    const double tol = 1.0 / dx;
+    const double kv = curv < -tol ? -tol : curv;
+    kappa[c] = kv;
+    if (fabs(pc) < 1e-1) m = fabs(kv);
+  }
+  m = block_max(m);
+  if (thread0() && m > 0.0) atomicMax((unsigned long long*)kmax, (unsigned long long)__double_as_longlong(m));
+}
+
+// b_c = ((b_c - F_X) - F_Y) - F_Z with the ghost-fluid jump terms of the six
+// arms (jc_on_derivative = 0): an arm across the interface carries
+// +-inv_dx2 * a * beta, a = (jc_c |phi_n| + jc_n |phi_c|)/(|phi_c| + |phi_n|),
+// jc = sigma * kappa, + when the cell is in the phi <= 0 phase.  Arms to the
+// wall ghosts use the extrapolated ghost phi (the ghosts of phi must be
+// filled), jc = 0 and the cell's own 1/rho.  The last block stores sum(b) in
+// sum_out for the mean removal.
+template <class T>
+__global__ void k_jump_rhs(const T* __restrict__ phi, const double* __restrict__ kappa, double sigma,
+                           double* __restrict__ b, Lay Lc, double rn, double rp, double inv2, double* partials,
+                           unsigned int* ticket, double* sum_out) {
+  double bs = 0.0;
+  Cursor cur;
+  for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
+    const int i = cur.i, j = cur.j, k = cur.k;
+    const int64_t c = Lc.at(i, j, k);
+    const double pc = (double)phi[c], ac = fabs(pc);
+    const double vc = 1.0 / (pc <= 0.0 ? rn : rp);
+    const double jcc = sigma * kappa[c];
+    const int64_t step[3] = {1, Lc.px, Lc.slab};
+    const int e[3] = {i, j, k};
+    const int n[3] = {Lc.nx, Lc.ny, Lc.nz};
+    double bv = b[c];
+    for (int a = 0; a < 3; ++a) {
+      double F = 0.0;
+      for (int side = 0; side < 2; ++side) {
+        const int64_t nb = side == 0 ? c - step[a] : c + step[a];
+        const bool ghost = side == 0 ? e[a] == 0 : e[a] == n[a] - 1;
+        const double pn = (double)phi[nb], an = fabs(pn);
+        const double vn = ghost ? vc : 1.0 / (pn <= 0.0 ? rn : rp);
+        const double jn = ghost ? 0.0 : sigma * kappa[nb];
+        double f = 0.0;
+        if ((pc <= 0.0) != (pn <= 0.0)) {
+          const double av = (jcc * an + jn * ac) / (ac + an);
+          const double beta = side == 0 ? vc * vn * (an + ac) / (vc * an + vn * ac)
+                                        : vc * vn * (an + ac) / (vn * ac + vc * an);
+          f = pc <= 0.0 ? inv2 * av * beta : -inv2 * av * beta;
+        }
+        F = side == 0 ? f : F + f;
+      }
+      bv = bv - F;
+    }
+    b[c] = bv;
+    bs += bv;
+  }
+  bs = block_sum(bs);
+  double tot;
+  if (grid_reduce_sum(bs, partials, ticket, &tot)) sum_out[0] = tot;
 }
 
 template <class T>
@@ -311,10 +429,24 @@ void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s) 
 template <class T>
 void velocity_correct(T* f, const T* base, const double* p, const T* phi, const Lay& Lf, const Lay& Lc, int axis,
                       double dx, double dt, double rho_neg, double rho_pos, int faithful, double c0, double c1,
-                      cudaStream_t s) {
+                      const double* kappa, double sigma, cudaStream_t s) {
   Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
   k_velocity_correct<T><<<g.grid, g.block, 0, s>>>(f, base, p, phi, Lf, Lc, axis, 1.0 / dx, dt, rho_neg, rho_pos,
-                                                    faithful, c0, c1);
+                                                    faithful, c0, c1, kappa, sigma);
+}
+
+template <class T>
+void curvature(const T* phi, double* kappa, const Lay& L, double dx, int typo, double* kmax, cudaStream_t s) {
+  cudaMemsetAsync(kmax, 0, sizeof(double), s);
+  Launch3 g = launch3(L.nx, L.ny, L.nz);
+  k_curvature<T><<<g.grid, g.block, 0, s>>>(phi, kappa, L, dx, typo, kmax);
+}
+
+template <class T>
+void jump_rhs(const T* phi, const double* kappa, double sigma, double* b, const Lay& Lc, double dx, double rho_neg,
+              double rho_pos, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s) {
+  k_jump_rhs<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, kappa, sigma, b, Lc, rho_neg, rho_pos, 1.0 / (dx * dx),
+                                                       partials, ticket, sum_out);
 }
 
 template <class T>
@@ -358,7 +490,11 @@ void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s)
                                    const Lay&, double, double, double, double*, unsigned int*, double*,             \
                                    cudaStream_t);                                                                   \
   template void velocity_correct<T>(T*, const T*, const double*, const T*, const Lay&, const Lay&, int, double,     \
-                                    double, double, double, int, double, double, cudaStream_t);                     \
+                                    double, double, double, int, double, double, const double*, double,            \
+                                    cudaStream_t);                                                                  \
+  template void curvature<T>(const T*, double*, const Lay&, double, int, double*, cudaStream_t);                   \
+  template void jump_rhs<T>(const T*, const double*, double, double*, const Lay&, double, double, double, double*, \
+                            unsigned int*, double*, cudaStream_t);                                                  \
   template void divergence_norms<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,   \
                                     double, double*, unsigned int*, double*, cudaStream_t);                         \
   template void absmax3<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, double*, cudaStream_t); \

@@ -124,6 +124,7 @@ def params_from_block(block, base_grid):
         viscosity=1 if block.GetBoolean("semi_implicit_approach", True) else 0,
         viscosity_tolerance=block.GetFloat("viscosity_tolerance", 1e-8),
         flags=0 if block.GetBoolean("corrected_projection", True) else FS_FLAG_FAITHFUL_PROJECTION,
+        surface_tension=block.GetFloat("surface_tension", 0.0),
     )
     if p.precision == FS_PRECISION_FP32_REFINE:
         p.stop = FS_STOP_RELATIVE

@@ -49,7 +49,8 @@ typedef enum {
   FS_FIELD_ADJ_PHI = 6,   /* adjoint (bar) of phi, cells: FP64 contexts, see the adjoint entry points */
   FS_FIELD_ADJ_U = 7,     /* adjoint of u, x faces */
   FS_FIELD_ADJ_V = 8,     /* adjoint of v, y faces */
-  FS_FIELD_ADJ_W = 9      /* adjoint of w, z faces */
+  FS_FIELD_ADJ_W = 9,     /* adjoint of w, z faces */
+  FS_FIELD_CURVATURE = 10 /* mean curvature from the last fs_curvature or surface-tension projection (download only) */
 } fs_field;
 
 typedef enum {
@@ -66,7 +67,9 @@ typedef enum {
 enum {
   FS_FLAG_FAITHFUL_PROJECTION = 1 << 0, /* only w corrected + first-cell bottom face quirk (PROJECTION_3D.h:1188-1407) */
   FS_FLAG_REINIT_TYPO = 1 << 1,         /* reproduce the two sqrt(a^2)+b^2 leaves (ADVECTION_METHOD_3D.h:1463,1605) */
-  FS_FLAG_LEVELSET_FORWARD_EULER = 1 << 2 /* order 3 advances phi by one Euler step (EULERIAN_FLUID_SOLVER_3D.h:1010) */
+  FS_FLAG_LEVELSET_FORWARD_EULER = 1 << 2, /* order 3 advances phi by one Euler step (EULERIAN_FLUID_SOLVER_3D.h:1010) */
+  FS_FLAG_CURVATURE_TYPO = 1 << 3  /* curvature as the reference computes it: factor 2 missing on py*pz*pyz and dz
+                                      for 1/dz in the zero-gradient fallback (LEVELSET_3D.h:1033,1037) */
 };
 
 typedef struct {
@@ -94,6 +97,7 @@ typedef struct {
   int viscosity_max_iteration;
   double cfl;                       /* CFL number used by fs_cfl_dt */
   int flags;                        /* FS_FLAG_* */
+  double surface_tension;           /* sigma: the pressure jump sigma*kappa across the interface (0: none) */
 } fs_params;
 
 typedef struct {
@@ -146,6 +150,11 @@ fs_status fs_download_device(fs_ctx* ctx, int field, double* dev);
 fs_status fs_step(fs_ctx* ctx, double dt, fs_step_report* report);
 /* CFL-limited dt times params.cfl (CFLOneTimeStep, EULERIAN_FLUID_SOLVER_3D.h:2673-2785). */
 fs_status fs_cfl_dt(fs_ctx* ctx, double* dt);
+
+/* Mean curvature of the current level set (LEVELSET_3D::ComputeCurvatures,
+ * LEVELSET_3D.h:963) into FS_FIELD_CURVATURE; kappa_max (may be NULL) gets
+ * max |kappa| over cells with |phi| < 0.1, the value the CFL condition uses. */
+fs_status fs_curvature(fs_ctx* ctx, double* kappa_max);
 
 /* Single operators of the step, on the context's current fields. */
 /* PROJECTION_3D::Solve (PROJECTION_3D.h:416). */

@@ -332,6 +332,7 @@ inline fs_params params_from_block(const SCRIPT_BLOCK& block, const GRID_STRUCTU
   p.viscosity = block.GetBoolean("semi_implicit_approach", true) ? 1 : 0;
   p.viscosity_tolerance = block.GetFloat("viscosity_tolerance", 1e-8);
   p.flags = block.GetBoolean("corrected_projection", true) ? 0 : FS_FLAG_FAITHFUL_PROJECTION;
+  p.surface_tension = block.GetFloat("surface_tension", 0.0);
   if (p.precision == FS_PRECISION_FP32_REFINE) p.stop = FS_STOP_RELATIVE;
   if (std::abs(grid.dx - grid.dy) > 1e-12 * grid.dx || std::abs(grid.dx - grid.dz) > 1e-12 * grid.dx)
     throw std::invalid_argument("the solver needs a uniform grid (dx = dy = dz)");
