@@ -36,7 +36,8 @@ EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", 
             "fs_cfl_dt", "fs_project", "fs_advect_levelset", "fs_advect_velocity", "fs_reinitialize",
             "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc", "fs_adjoint_reset", "fs_adjoint_density_bars",
             "fs_step_adjoint", "fs_advect_levelset_adjoint", "fs_advect_velocity_adjoint", "fs_reinitialize_adjoint",
-            "fs_viscosity_adjoint", "fs_project_adjoint", "fs_curvature")
+            "fs_viscosity_adjoint", "fs_project_adjoint", "fs_curvature", "fs_write_levelset", "fs_read_levelset",
+            "fs_write_state", "fs_read_state")
 
 
 class FsError(RuntimeError):
@@ -125,6 +126,10 @@ def lib():
         L.fs_pcg_csr_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_int, vp, ip, dp]
         L.fs_curvature.argtypes = [vp, dp]
+        L.fs_write_levelset.argtypes = [vp, ctypes.c_char_p, dp]
+        L.fs_read_levelset.argtypes = [vp, ctypes.c_char_p, dp]
+        L.fs_write_state.argtypes = [vp, ctypes.c_char_p]
+        L.fs_read_state.argtypes = [vp, ctypes.c_char_p]
         L.fs_adjoint_reset.argtypes = [vp]
         L.fs_adjoint_density_bars.argtypes = [vp, dp, dp]
         L.fs_step_adjoint.argtypes = [vp, ctypes.c_double, ctypes.POINTER(StepReport)]
@@ -287,6 +292,23 @@ class Solver:
         it = ctypes.c_int()
         _check(lib().fs_viscosity(self._h, float(dt), ctypes.byref(it)), "fs_viscosity")
         return it.value
+
+    def write_levelset(self, path, grid_min=(0.0, 0.0, 0.0)):
+        """The level set in the reference's LEVELSET_3D binary format."""
+        mn = (ctypes.c_double * 3)(*grid_min)
+        _check(lib().fs_write_levelset(self._h, str(path).encode(), mn), "fs_write_levelset")
+
+    def read_levelset(self, path):
+        """Load a LEVELSET_3D file; returns the grid minimum it records."""
+        mn = (ctypes.c_double * 3)()
+        _check(lib().fs_read_levelset(self._h, str(path).encode(), mn), "fs_read_levelset")
+        return tuple(mn)
+
+    def write_state(self, path):
+        _check(lib().fs_write_state(self._h, str(path).encode()), "fs_write_state")
+
+    def read_state(self, path):
+        _check(lib().fs_read_state(self._h, str(path).encode()), "fs_read_state")
 
     def curvature(self):
         """Mean curvature of the current level set and max |kappa| over |phi| < 0.1."""

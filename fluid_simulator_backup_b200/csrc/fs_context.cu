@@ -1388,6 +1388,123 @@ fs_status fs_viscosity(fs_ctx* c, double dt, int* iterations) {
   return FS_OK;
 }
 
+// ---- state I/O
+
+// LEVELSET_3D::Write/Read (LEVELSET_3D.h:1132-1200): int32 i_start, j_start,
+// k_start, i_res, j_res, k_res; float64 x_min, y_min, z_min, x_max, y_max,
+// z_max; int32 ghost_width; then phi(i, j, k) as float64 with i fastest,
+// k slowest.  No padding between the fields.
+fs_status fs_write_levelset(fs_ctx* c, const char* path, const double* grid_min) {
+  if (!c || !path) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  const int nx = c->grid.nx, ny = c->grid.ny, nz = c->grid.nz;
+  std::vector<double> phi((size_t)nx * ny * nz);
+  CKS(fs_download(c, FS_FIELD_PHI, phi.data(), nullptr));
+  FILE* f = std::fopen(path, "wb");
+  if (!f) { set_error("cannot open %s for writing", path); return FS_INVALID_ARG; }
+  const int32_t hdr_i[6] = {0, 0, 0, nx, ny, nz};
+  const double mn[3] = {grid_min ? grid_min[0] : 0.0, grid_min ? grid_min[1] : 0.0, grid_min ? grid_min[2] : 0.0};
+  const double hdr_d[6] = {mn[0], mn[1], mn[2], mn[0] + (nx - 1) * c->grid.dx, mn[1] + (ny - 1) * c->grid.dx,
+                           mn[2] + (nz - 1) * c->grid.dx};
+  const int32_t ghost = GH;
+  bool ok = std::fwrite(hdr_i, sizeof hdr_i, 1, f) == 1 && std::fwrite(hdr_d, sizeof hdr_d, 1, f) == 1 &&
+            std::fwrite(&ghost, sizeof ghost, 1, f) == 1 &&
+            std::fwrite(phi.data(), sizeof(double), phi.size(), f) == phi.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) { set_error("short write to %s", path); return FS_INVALID_ARG; }
+  return FS_OK;
+}
+
+fs_status fs_read_levelset(fs_ctx* c, const char* path, double* grid_min) {
+  if (!c || !path) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  FILE* f = std::fopen(path, "rb");
+  if (!f) { set_error("cannot open %s", path); return FS_INVALID_ARG; }
+  int32_t hdr_i[6];
+  double hdr_d[6];
+  int32_t ghost = 0;
+  bool ok = std::fread(hdr_i, sizeof hdr_i, 1, f) == 1 && std::fread(hdr_d, sizeof hdr_d, 1, f) == 1 &&
+            std::fread(&ghost, sizeof ghost, 1, f) == 1;
+  const int nx = c->grid.nx, ny = c->grid.ny, nz = c->grid.nz;
+  if (ok && (hdr_i[3] != nx || hdr_i[4] != ny || hdr_i[5] != nz)) {
+    std::fclose(f);
+    set_error("%s holds a %d x %d x %d level set, the context is %d x %d x %d", path, hdr_i[3], hdr_i[4], hdr_i[5], nx,
+              ny, nz);
+    return FS_INVALID_ARG;
+  }
+  if (ok) {
+    const double dx = (hdr_d[3] - hdr_d[0]) / (nx > 1 ? nx - 1 : 1);
+    if (std::fabs(dx - c->grid.dx) > 1e-12 * c->grid.dx) {
+      std::fclose(f);
+      set_error("%s has grid spacing %.17g, the context %.17g", path, dx, c->grid.dx);
+      return FS_INVALID_ARG;
+    }
+  }
+  std::vector<double> phi((size_t)nx * ny * nz);
+  ok = ok && std::fread(phi.data(), sizeof(double), phi.size(), f) == phi.size();
+  std::fclose(f);
+  if (!ok) { set_error("%s is truncated or not a level-set file", path); return FS_INVALID_ARG; }
+  if (grid_min) {
+    grid_min[0] = hdr_d[0];
+    grid_min[1] = hdr_d[1];
+    grid_min[2] = hdr_d[2];
+  }
+  return fs_upload(c, FS_FIELD_PHI, phi.data(), nullptr);
+}
+
+// Checkpoint of the step state: "FSB200ST", uint32 version 1, int32 nx, ny,
+// nz, float64 dx, then phi, u, v, w, pressure as float64 interior values
+// (x fastest), each field in the layout of fs_download.
+static const char kStateMagic[8] = {'F', 'S', 'B', '2', '0', '0', 'S', 'T'};
+
+fs_status fs_write_state(fs_ctx* c, const char* path) {
+  if (!c || !path) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  FILE* f = std::fopen(path, "wb");
+  if (!f) { set_error("cannot open %s for writing", path); return FS_INVALID_ARG; }
+  const uint32_t version = 1;
+  const int32_t dims[3] = {c->grid.nx, c->grid.ny, c->grid.nz};
+  bool ok = std::fwrite(kStateMagic, 8, 1, f) == 1 && std::fwrite(&version, 4, 1, f) == 1 &&
+            std::fwrite(dims, sizeof dims, 1, f) == 1 && std::fwrite(&c->grid.dx, 8, 1, f) == 1;
+  const int fields[5] = {FS_FIELD_PHI, FS_FIELD_U, FS_FIELD_V, FS_FIELD_W, FS_FIELD_PRESSURE};
+  for (int fld : fields) {
+    if (!ok) break;
+    std::vector<double> a((size_t)field_count(c, fld));
+    fs_status st = fs_download(c, fld, a.data(), nullptr);
+    if (st != FS_OK) { std::fclose(f); return st; }
+    ok = std::fwrite(a.data(), sizeof(double), a.size(), f) == a.size();
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) { set_error("short write to %s", path); return FS_INVALID_ARG; }
+  return FS_OK;
+}
+
+fs_status fs_read_state(fs_ctx* c, const char* path) {
+  if (!c || !path) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  FILE* f = std::fopen(path, "rb");
+  if (!f) { set_error("cannot open %s", path); return FS_INVALID_ARG; }
+  char magic[8];
+  uint32_t version = 0;
+  int32_t dims[3];
+  double dx = 0.0;
+  bool ok = std::fread(magic, 8, 1, f) == 1 && std::memcmp(magic, kStateMagic, 8) == 0 &&
+            std::fread(&version, 4, 1, f) == 1 && version == 1 && std::fread(dims, sizeof dims, 1, f) == 1 &&
+            std::fread(&dx, 8, 1, f) == 1;
+  if (!ok) { std::fclose(f); set_error("%s is not a state file of this library", path); return FS_INVALID_ARG; }
+  if (dims[0] != c->grid.nx || dims[1] != c->grid.ny || dims[2] != c->grid.nz || dx != c->grid.dx) {
+    std::fclose(f);
+    set_error("%s holds a %d x %d x %d grid with dx %.17g, not the context's", path, dims[0], dims[1], dims[2], dx);
+    return FS_INVALID_ARG;
+  }
+  const int fields[5] = {FS_FIELD_PHI, FS_FIELD_U, FS_FIELD_V, FS_FIELD_W, FS_FIELD_PRESSURE};
+  std::vector<std::vector<double>> data(5);
+  for (int q = 0; q < 5 && ok; ++q) {
+    data[q].resize((size_t)field_count(c, fields[q]));
+    ok = std::fread(data[q].data(), sizeof(double), data[q].size(), f) == data[q].size();
+  }
+  std::fclose(f);
+  if (!ok) { set_error("%s is truncated", path); return FS_INVALID_ARG; }
+  for (int q = 0; q < 5; ++q) CKS(fs_upload(c, fields[q], data[q].data(), nullptr));
+  return FS_OK;
+}
+
 // ---- adjoints (FP64 contexts, corrected projection)
 
 fs_status fs_adjoint_reset(fs_ctx* c) {

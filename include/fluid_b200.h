@@ -175,6 +175,20 @@ fs_status fs_pcg_csr(fs_ctx* ctx, int n, int nnz, const double* values, const in
                      const int* row_ptr, const double* b, double* x, double tolerance, int max_iteration,
                      int stop, int* iterations, double* residual);
 
+/* State I/O.  The level set in the reference's binary format
+ * (LEVELSET_3D::Write / Read, LEVELSET_3D.h:1132-1200): int32 i_start,
+ * j_start, k_start, i_res, j_res, k_res, float64 x_min, y_min, z_min, x_max,
+ * y_max, z_max, int32 ghost_width, then phi as float64, x fastest.  grid_min
+ * (may be NULL: the origin) is the position of cell (0,0,0); reading checks
+ * the resolution and the spacing against the context and returns grid_min. */
+fs_status fs_write_levelset(fs_ctx* ctx, const char* path, const double* grid_min);
+fs_status fs_read_levelset(fs_ctx* ctx, const char* path, double* grid_min);
+/* Checkpoint and resume of the step state (phi, u, v, w, pressure) in this
+ * library's own format (magic "FSB200ST", version 1, grid, then the fields
+ * as float64).  No counterpart in the reference, which has no restart. */
+fs_status fs_write_state(fs_ctx* ctx, const char* path);
+fs_status fs_read_state(fs_ctx* ctx, const char* path);
+
 /* Adjoints (vector-Jacobian products) of the step and of its operators.
  * No counterpart in the reference, which has no derivatives; they are part
  * of this library's differentiable-simulation interface.

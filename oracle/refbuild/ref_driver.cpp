@@ -256,4 +256,11 @@ int fsref_linear_solve(void* h, int n, int nnz, const double* vals, const int* c
   return ps.linear_solver->num_iteration;
 }
 
+// The level set in the reference's binary format (LEVELSET_3D::Write,
+// LEVELSET_3D.h:1132-1160).
+void fsref_write_levelset(void* h, const char* path) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  s.water_levelset->Write(path);
+}
+
 }  // extern "C"

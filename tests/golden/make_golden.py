@@ -19,6 +19,7 @@ on the air/water unit-cube box with Neumann pressure walls:
   cfl              EULERIAN_FLUID_SOLVER_3D::CFLOneTimeStep
   projection_tension  curvature (LEVELSET_3D::ComputeCurvatures) and
                    PROJECTION_3D::Solve with a surface tension jump condition
+  levelset_file    the bytes LEVELSET_3D::Write produces for a level set
 """
 import os
 import sys
@@ -156,6 +157,18 @@ def main():
                                           phi=phi, **vel, kappa=kappa, iterations=it, csr_vals=vals, csr_cols=cols,
                                           csr_rowptr=rowptr, b=b, x=x, out_p=c.get("p"), out_u=c.get("u"),
                                           out_v=c.get("v"), out_w=c.get("w"))
+    c.close()
+
+    # A level set written by LEVELSET_3D::Write (the bytes of the file), 9^3
+    n = 9
+    c = case(n)
+    phi = rng.normal(size=c.shape("phi"))
+    c.set("phi", phi)
+    path = os.path.join(WORK, "levelset.bin")
+    c.write_levelset(path)
+    with open(path, "rb") as f:
+        raw = np.frombuffer(f.read(), dtype=np.uint8).copy()
+    fixtures["levelset_file"] = dict(n=n, dx=c.dx, phi=phi, raw=raw)
     c.close()
 
     for name, d in fixtures.items():
