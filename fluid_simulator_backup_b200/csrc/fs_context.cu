@@ -112,6 +112,7 @@ struct fs_ctx {
   std::vector<double*> tape_cells, tape_faces;  // taped forward states, allocated on demand
   bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
   double reliable_delta = 0.1;  // residual drop between reliable updates (FS_RELIABLE_DELTA to sweep)
+  int flux32 = 2;               // arithmetic of the FP32 flux SpMV (Op7::flux32; FS_FLUX32 to sweep)
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -445,6 +446,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
                                       (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s);
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
+    A.flux32 = c->flux32;
     const size_t vbytes = c->Lc.total * sizeof(float);
     double bb = 0.0;
     float *r32 = (float*)c->pr, *p32 = (float*)c->pp, *q32 = (float*)c->pq;
@@ -1070,6 +1072,10 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
   c->debug = std::getenv("FS_DEBUG") != nullptr;
+  if (const char* e = std::getenv("FS_FLUX32")) {
+    const int v = std::atoi(e);
+    if (v >= 0 && v <= 2) c->flux32 = v;
+  }
   if (const char* e = std::getenv("FS_RELIABLE_DELTA")) {  // tuning knob for sweeps
     const double v = std::atof(e);
     if (v > 0.0 && v < 1.0) c->reliable_delta = v;

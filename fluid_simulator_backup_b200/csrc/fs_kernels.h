@@ -64,6 +64,16 @@ template <class V> struct Op7 {
   Lay L;
   int flux_form = 0;
   const double* extra0 = nullptr;  // device scalar: diag - sum of couplings at cell (0,0,0)
+  // flux form with FP32 vectors: 0 sums FP64 fluxes formed from exact FP64
+  // differences and products; 1 forms each flux in FP32 (difference and
+  // product correctly rounded) and sums them in FP64; 2 does all in FP32.
+  // Each FP32 flux a (x_c - x_n) is exact to 2 eps32 of itself (the stored x
+  // are exact inputs, so the difference is correctly rounded); the sum of six
+  // loses eps32 * sum|flux| to cancellation, an inexact matrix-vector product
+  // that the mixed solve's reliable updates (true residual in FP64) absorb:
+  // at 256^3 mode 2 needs the same iterations as mode 0 and avoids the
+  // FP32->FP64 conversions that bound the SpMV's issue rate.
+  int flux32 = 0;
 };
 
 template <class V, class R = V>

@@ -57,10 +57,10 @@ int pcg_blocks(const Lay& L) { return reduction_blocks((int64_t)L.nx * L.ny * L.
 
 // (A x)_c evaluated in the type X of x (the operator's coefficients are
 // converted): FP32 iterates get FP32 arithmetic, FP64 iterates FP64.
-// The flux form is always evaluated in FP64 (loads in their storage type):
-// for smooth x the six fluxes nearly cancel, and FP32 arithmetic would lose
-// about log10(n) digits of q to that cancellation; FP64 arithmetic costs no
-// memory traffic and the SpMV stays bandwidth bound.
+// The flux form is evaluated here in FP64 (loads in their storage type):
+// for smooth x the six fluxes nearly cancel, and FP64 keeps q exact to
+// rounding.  (The iteration's own SpMV, k_cg_spmv, may form FP32 fluxes in
+// FP32: see Op7::flux32.)
 template <class V, class X>
 __device__ __forceinline__ X apply7(const Op7<V>& A, const X* __restrict__ x, int64_t c) {
   const int64_t sy = A.L.px, sz = A.L.slab;
@@ -334,7 +334,19 @@ __device__ __forceinline__ void spmv_row4(const Op7<V>& A, const V* __restrict__
     const V xr = m == 3 ? pr : lane(pc, m + 1);
     const V ar = m == 3 ? axr : lane(axc, m + 1);
     V out;
-    if (A.flux_form) {
+    if (A.flux_form && A.flux32 == 2) {
+      V acc = lane(axc, m) * (xc - xl) + ar * (xc - xr);
+      acc += lane(ayc, m) * (xc - lane(ps, m)) + lane(ayn, m) * (xc - lane(pn, m));
+      acc += lane(azc, m) * (xc - lane(pdn, m)) + lane(azu, m) * (xc - lane(pup, m));
+      if (c + m == c00) acc += (V)(*A.extra0) * xc;
+      out = acc;
+    } else if (A.flux_form && A.flux32 == 1) {
+      double acc = (double)(lane(axc, m) * (xc - xl)) + (double)(ar * (xc - xr));
+      acc += (double)(lane(ayc, m) * (xc - lane(ps, m))) + (double)(lane(ayn, m) * (xc - lane(pn, m)));
+      acc += (double)(lane(azc, m) * (xc - lane(pdn, m))) + (double)(lane(azu, m) * (xc - lane(pup, m)));
+      if (c + m == c00) acc += (*A.extra0) * (double)xc;
+      out = (V)acc;
+    } else if (A.flux_form) {
       // flux form in FP64 arithmetic (see apply7)
       const double d = (double)xc;
       double acc = (double)lane(axc, m) * (d - (double)xl) + (double)ar * (d - (double)xr);
