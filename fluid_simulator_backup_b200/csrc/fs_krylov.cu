@@ -439,16 +439,19 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update(Op7<V> A, V* __restri
     rv.c -= alpha * qv.c;
     rv.d -= alpha * qv.d;
     st4(r + c, rv, nvalid);
+    // r.z and r.r of the vector's cells in the vector type (z = r/diag as the
+    // direction update forms it), accumulated in FP64 across vectors
+    V rz4 = V(0), rr4 = V(0);
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       if (m < nvalid) {
-        // z = r/diag in the vector type, as the direction update forms it
         const V rm = lane(rv, m);
-        const double rd = (double)rm;
-        rz += rd * (double)(rm / lane(dv, m));
-        rr += rd * rd;
+        rz4 += rm * (rm / lane(dv, m));
+        rr4 += rm * rm;
       }
     }
+    rz += (double)rz4;
+    rr += (double)rr4;
   }
   double tot[3];
   if (grid_reduce3(rz, rr, 0.0, partials, &st->ticket, tot)) {
