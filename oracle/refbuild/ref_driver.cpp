@@ -4,14 +4,20 @@
 // It builds a SIMULATION_WORLD from a generated air/water .sim script exactly
 // as the reference application does (SIMULATION_WORLD.h:InitializeFormScript),
 // then lets the caller inject seeded interior fields and call single reference
-// operators on them.  Every call runs with number_of_threads = 1 and
-// thread_id 0, so the reference's barriers are no-ops and its ordered partial
-// sums become plain sequential sums.
+// operators on them.  The golden vectors are made with number_of_threads = 1
+// (thread_id 0: the reference's barriers are no-ops and its ordered partial
+// sums plain sequential sums).  With number_of_threads = T in the script the
+// timed operators run on T threads, each calling the reference routine with
+// its thread_id, as MULTITHREADING::RunThreads does (used to time the
+// reference's CPU path with every host thread).
 //
 // Field ids: 0 phi (cells), 1 u (x faces), 2 v (y faces), 3 w (z faces),
 // 4 pressure (cells).  Arrays are interior values only, x fastest:
 // idx = i + nx*(j + ny*k) with nx the extent of that field (n+1 on its own
 // face axis).
+#include <thread>
+#include <vector>
+
 #include "SIMULATION_WORLD.h"
 
 namespace {
@@ -44,14 +50,28 @@ void for_interior(FIELD_STRUCTURE_3D<T>& f, F&& body) {
 // ghost fill reads for layers >= 2 (FIELD_STRUCTURE_3D.h:1776-1830).  Filling
 // them in place first, with the same routine, makes those reads well defined:
 // the loop runs outward, so layer m reads the freshly written layer m-1.
-void extrapolate_levelset_in_place(EULERIAN_FLUID_SOLVER_3D& s) {
-  s.water_levelset->signed_distance_field.FillGhostCellsContinuousDerivativesFrom(0, s.water_levelset->arr, false);
+void extrapolate_levelset_in_place(EULERIAN_FLUID_SOLVER_3D& s, int t = 0) {
+  s.water_levelset->signed_distance_field.FillGhostCellsContinuousDerivativesFrom(t, s.water_levelset->arr, false);
 }
 
-void zero_ghost_velocities(EULERIAN_FLUID_SOLVER_3D& s) {
-  s.vector_field_mac_ghost_x.FillGhostCellsZero(0, s.water_velocity_field_mac_x->array_for_this, true);
-  s.vector_field_mac_ghost_y.FillGhostCellsZero(0, s.water_velocity_field_mac_y->array_for_this, true);
-  s.vector_field_mac_ghost_z.FillGhostCellsZero(0, s.water_velocity_field_mac_z->array_for_this, true);
+void zero_ghost_velocities(EULERIAN_FLUID_SOLVER_3D& s, int t = 0) {
+  s.vector_field_mac_ghost_x.FillGhostCellsZero(t, s.water_velocity_field_mac_x->array_for_this, true);
+  s.vector_field_mac_ghost_y.FillGhostCellsZero(t, s.water_velocity_field_mac_y->array_for_this, true);
+  s.vector_field_mac_ghost_z.FillGhostCellsZero(t, s.water_velocity_field_mac_z->array_for_this, true);
+}
+
+// body(thread_id) on every thread of the world's MULTITHREADING, as its
+// RunThreads does; one thread runs inline.
+template <class F>
+void run_threads(RefCase* c, F&& body) {
+  const int T = c->world.multithreading->num_threads;
+  if (T <= 1) {
+    body(0);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < T; ++t) th.emplace_back([&body, t] { body(t); });
+  for (auto& x : th) x.join();
 }
 
 }  // namespace
@@ -100,12 +120,15 @@ void fsref_levelset_ghost(void* h, double* dst) {
 void fsref_weno5_levelset(void* h, double dt) {
   RefCase* c = static_cast<RefCase*>(h);
   EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
-  extrapolate_levelset_in_place(s);
-  s.scalar_field_ghost.FillGhostCellsContinuousDerivativesFrom(0, s.water_levelset->arr, true);
-  zero_ghost_velocities(s);
-  ADVECTION_METHOD_3D<T>::WENO5th(0, s.water_levelset->signed_distance_field, s.scalar_field_ghost,
-                                  s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z,
-                                  dt, *c->world.multithreading, s.advecting_field_variables->epsilon);
+  run_threads(c, [&](int t) {
+    extrapolate_levelset_in_place(s, t);
+    s.scalar_field_ghost.FillGhostCellsContinuousDerivativesFrom(t, s.water_levelset->arr, true);
+    zero_ghost_velocities(s, t);
+    ADVECTION_METHOD_3D<T>::WENO5th(t, s.water_levelset->signed_distance_field, s.scalar_field_ghost,
+                                    s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y,
+                                    s.vector_field_mac_ghost_z, dt, *c->world.multithreading,
+                                    s.advecting_field_variables->epsilon);
+  });
 }
 
 // One forward-Euler WENO5 update of the three MAC components.  own_ghost = 0
@@ -115,15 +138,17 @@ void fsref_weno5_levelset(void* h, double dt) {
 void fsref_weno5_velocity(void* h, double dt, int own_ghost) {
   RefCase* c = static_cast<RefCase*>(h);
   EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
-  zero_ghost_velocities(s);
   MULTITHREADING& mt = *c->world.multithreading;
   const T eps = s.advecting_field_variables->epsilon_v;
   FIELD_STRUCTURE_3D<T>& gx = s.vector_field_mac_ghost_x;
   FIELD_STRUCTURE_3D<T>& gy = own_ghost ? s.vector_field_mac_ghost_y : s.vector_field_mac_ghost_x;
   FIELD_STRUCTURE_3D<T>& gz = own_ghost ? s.vector_field_mac_ghost_z : s.vector_field_mac_ghost_x;
-  ADVECTION_METHOD_3D<T>::WENO5th(0, *s.water_velocity_field_mac_x, gx, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
-  ADVECTION_METHOD_3D<T>::WENO5th(0, *s.water_velocity_field_mac_y, gy, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
-  ADVECTION_METHOD_3D<T>::WENO5th(0, *s.water_velocity_field_mac_z, gz, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
+  run_threads(c, [&](int t) {
+    zero_ghost_velocities(s, t);
+    ADVECTION_METHOD_3D<T>::WENO5th(t, *s.water_velocity_field_mac_x, gx, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
+    ADVECTION_METHOD_3D<T>::WENO5th(t, *s.water_velocity_field_mac_y, gy, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
+    ADVECTION_METHOD_3D<T>::WENO5th(t, *s.water_velocity_field_mac_z, gz, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt, eps);
+  });
 }
 
 // One reinitialisation block: S = phi0/sqrt(phi0^2 + dx^2) and
@@ -135,11 +160,14 @@ void fsref_weno5_velocity(void* h, double dt, int own_ghost) {
 void fsref_reinitialization(void* h, double dt, int refresh_ghosts) {
   RefCase* c = static_cast<RefCase*>(h);
   EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
-  extrapolate_levelset_in_place(s);
   if (!refresh_ghosts) {
-    s.Reinitialization(0, dt);
+    run_threads(c, [&](int t) {
+      extrapolate_levelset_in_place(s, t);
+      s.Reinitialization(t, dt);
+    });
     return;
   }
+  extrapolate_levelset_in_place(s);
   const T fictious_dt = s.base_grid.dx / s.scaling_number_for_reinitialization;
   const GRID_STRUCTURE_3D& g = s.base_grid;
   for (int k = g.k_start; k <= g.k_end; ++k)
@@ -159,8 +187,10 @@ void fsref_reinitialization(void* h, double dt, int refresh_ghosts) {
 int fsref_projection(void* h, double dt) {
   RefCase* c = static_cast<RefCase*>(h);
   EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
-  extrapolate_levelset_in_place(s);
-  s.water_projection->Solve(0, dt);
+  run_threads(c, [&](int t) {
+    extrapolate_levelset_in_place(s, t);
+    s.water_projection->Solve(t, dt);
+  });
   return s.water_projection->poisson_solver.linear_solver->num_iteration;
 }
 
@@ -184,9 +214,12 @@ void fsref_divergence(void* h, double* dst) {
 
 // Explicit variable-viscosity update (VISCOSITY_3D.h:452-563), in place.
 void fsref_viscosity(void* h, double dt) {
-  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
-  extrapolate_levelset_in_place(s);
-  s.viscosity_solver->ApplyViscosity(0, s.epsilon_for_mollification, dt);
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  run_threads(c, [&](int t) {
+    extrapolate_levelset_in_place(s, t);
+    s.viscosity_solver->ApplyViscosity(t, s.epsilon_for_mollification, dt);
+  });
 }
 
 // Semi-implicit viscosity system for one MAC component through the reference
