@@ -30,6 +30,7 @@ FIELD = {"phi": 0, "u": 1, "v": 2, "w": 3, "pressure": 4, "p": 4, "divergence": 
 FS_PRECISION_FP64, FS_PRECISION_FP32_REFINE = 0, 1
 FS_STOP_RELATIVE, FS_STOP_ABSOLUTE = 0, 1
 FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER, FS_FLAG_CURVATURE_TYPO = 1, 2, 4, 8
+FS_VELOCITY_WENO5, FS_VELOCITY_ENO3 = 0, 1
 
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
             "fs_memory_bytes", "fs_upload", "fs_download", "fs_upload_device", "fs_download_device", "fs_step",
@@ -58,7 +59,8 @@ class Params(ctypes.Structure):
                 ("max_iteration", ctypes.c_int), ("inner_tolerance", ctypes.c_double), ("max_outer", ctypes.c_int),
                 ("viscosity", ctypes.c_int), ("viscosity_tolerance", ctypes.c_double),
                 ("viscosity_max_iteration", ctypes.c_int), ("cfl", ctypes.c_double), ("flags", ctypes.c_int),
-                ("surface_tension", ctypes.c_double)]
+                ("surface_tension", ctypes.c_double), ("velocity_scheme", ctypes.c_int),
+                ("velocity_epsilon", ctypes.c_double)]
 
     def as_dict(self):
         d = {}

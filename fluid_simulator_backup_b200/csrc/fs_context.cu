@@ -184,6 +184,14 @@ fs_status check_params(const fs_params* p) {
     return FS_INVALID_ARG;
   }
   if (p->stop != FS_STOP_RELATIVE && p->stop != FS_STOP_ABSOLUTE) { set_error("unknown stop criterion"); return FS_INVALID_ARG; }
+  if (!(p->velocity_epsilon >= 0) || !std::isfinite(p->velocity_epsilon)) {
+    set_error("velocity_epsilon must be finite and >= 0");
+    return FS_INVALID_ARG;
+  }
+  if (p->velocity_scheme != FS_VELOCITY_WENO5 && p->velocity_scheme != FS_VELOCITY_ENO3) {
+    set_error("unknown velocity scheme %d", p->velocity_scheme);
+    return FS_INVALID_ARG;
+  }
   if (!(p->surface_tension >= 0) || !std::isfinite(p->surface_tension)) {
     set_error("surface_tension must be finite and non-negative");
     return FS_INVALID_ARG;
@@ -313,13 +321,25 @@ fs_status advect_levelset_t(fs_ctx* c, double dt, Tape* tp = nullptr) {
   return FS_OK;
 }
 
+// The WENO5 epsilon of the velocity advection (VELOCITY_ADVECTION.epsilon,
+// ADVECTION_3D.h:112), which falls back to the level-set one when unset.
+static double velocity_epsilon(const fs_ctx* c) {
+  return c->prm.velocity_epsilon > 0.0 ? c->prm.velocity_epsilon : c->prm.weno_epsilon;
+}
+
 template <class S>
 fs_status advect_velocity_t(fs_ctx* c, double dt) {
-  const double eps = c->prm.weno_epsilon, dx = c->grid.dx;
+  const double eps = velocity_epsilon(c), dx = c->grid.dx;
   S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w);
-  weno5_mac<S>(u, F<S>(c->ua), u, v, w, c->Lu, c->Lu, c->Lv, c->Lw, 0, dx, eps, dt, c->stream);
-  weno5_mac<S>(v, F<S>(c->va), u, v, w, c->Lv, c->Lu, c->Lv, c->Lw, 1, dx, eps, dt, c->stream);
-  weno5_mac<S>(w, F<S>(c->wa), u, v, w, c->Lw, c->Lu, c->Lv, c->Lw, 2, dx, eps, dt, c->stream);
+  if (c->prm.velocity_scheme == FS_VELOCITY_ENO3) {
+    eno3_mac<S>(u, F<S>(c->ua), u, v, w, c->Lu, c->Lu, c->Lv, c->Lw, 0, dx, dt, c->stream);
+    eno3_mac<S>(v, F<S>(c->va), u, v, w, c->Lv, c->Lu, c->Lv, c->Lw, 1, dx, dt, c->stream);
+    eno3_mac<S>(w, F<S>(c->wa), u, v, w, c->Lw, c->Lu, c->Lv, c->Lw, 2, dx, dt, c->stream);
+  } else {
+    weno5_mac<S>(u, F<S>(c->ua), u, v, w, c->Lu, c->Lu, c->Lv, c->Lw, 0, dx, eps, dt, c->stream);
+    weno5_mac<S>(v, F<S>(c->va), u, v, w, c->Lv, c->Lu, c->Lv, c->Lw, 1, dx, eps, dt, c->stream);
+    weno5_mac<S>(w, F<S>(c->wa), u, v, w, c->Lw, c->Lu, c->Lv, c->Lw, 2, dx, eps, dt, c->stream);
+  }
   c->launches += 3;
   std::swap(c->u, c->ua);
   std::swap(c->v, c->va);
@@ -888,7 +908,7 @@ fs_status adj_velocity_advect(fs_ctx* c, double* const uin[3], double* const out
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   for (int a = 0; a < 3; ++a)
     adj_weno_mac(uin[a], uin[0], uin[1], uin[2], out_bar[a], in_bar[a], in_bar[0], in_bar[1], in_bar[2], *lays[a],
-                 c->Lu, c->Lv, c->Lw, a, c->grid.dx, c->prm.weno_epsilon, dt, c->stream);
+                 c->Lu, c->Lv, c->Lw, a, c->grid.dx, velocity_epsilon(c), dt, c->stream);
   c->launches += 3;
   CK(cudaGetLastError());
   return FS_OK;
@@ -898,6 +918,10 @@ fs_status adj_check(fs_ctx* c) {
   if (c->fp32) { set_error("adjoints are built for FP64 contexts"); return FS_NOT_SUPPORTED; }
   if (c->prm.surface_tension != 0.0) {
     set_error("adjoints do not cover the surface-tension jump terms");
+    return FS_NOT_SUPPORTED;
+  }
+  if (c->prm.velocity_scheme != FS_VELOCITY_WENO5) {
+    set_error("adjoints cover the WENO5 velocity advection only");
     return FS_NOT_SUPPORTED;
   }
   if (c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) {

@@ -15,6 +15,9 @@ void weno5_levelset(const T* src, const T* base, T* out, const T* u, const T* v,
 template <class T>
 void weno5_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
                const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s);
+template <class T>
+void eno3_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+              const Lay& Lw, int axis, double dx, double dt, cudaStream_t s);
 template <class T> void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s);
 template <class T>
 void sussman_step(const T* src, const T* sgn, const T* base, T* out, const Lay& L, double dx, double eps, double dtau,

@@ -199,6 +199,72 @@ __global__ void k_weno5_mac(const T* __restrict__ comp, T* __restrict__ out, con
 }
 
 // ---------------------------------------------------------------------------
+// ENO3 (ADVECTION_METHOD_3D.h:1639-1934)
+// ---------------------------------------------------------------------------
+
+// D- and D+ along a stride from the 7 samples f[-3..3]: divided differences
+// d1 (scaled 1/dx), d2 (1/(2dx)), d3 ((1/dx)/3); each side takes the stencil
+// with the smaller |d2|, then the smaller |d3|.
+template <class T>
+__device__ __forceinline__ void eno3_pair(const T* __restrict__ f, int64_t c, int64_t st, T h, T inv, T o2, T o3,
+                                          T& dm, T& dp) {
+  T v[7];
+#pragma unroll
+  for (int s = 0; s < 7; ++s) v[s] = f[c + (s - 3) * st];
+  T d1[6], d2[5], d3[4];  // d1[q]: samples q+1 - q (s = q-3); d2[q] from d1[q+1], d1[q]; d3[q] from d2[q+1], d2[q]
+#pragma unroll
+  for (int q = 0; q < 6; ++q) d1[q] = inv * (v[q + 1] - v[q]);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) d2[q] = o2 * (d1[q + 1] - d1[q]);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) d3[q] = o3 * (d2[q + 1] - d2[q]);
+  // in the reference's names: d1_n1 = d1[2], d1_0 = d1[3]; d2_n1 = d2[1],
+  // d2_0 = d2[2], d2_p1 = d2[3]; d3_n2 = d3[0], d3_n1 = d3[1], d3_0 = d3[2], d3_p1 = d3[3]
+  const T two = T(2);
+  if (fabs(d2[1]) <= fabs(d2[2])) {
+    dm = fabs(d3[0]) <= fabs(d3[1]) ? (d1[2] + d2[1] * h) + two * d3[0] * h * h : (d1[2] + d2[1] * h) + two * d3[1] * h * h;
+  } else {
+    dm = fabs(d3[1]) <= fabs(d3[2]) ? (d1[2] + d2[2] * h) - d3[1] * h * h : (d1[2] + d2[2] * h) - d3[2] * h * h;
+  }
+  if (fabs(d2[2]) <= fabs(d2[3])) {
+    dp = fabs(d3[1]) <= fabs(d3[2]) ? (d1[3] - d2[2] * h) - d3[1] * h * h : (d1[3] - d2[2] * h) - d3[2] * h * h;
+  } else {
+    dp = fabs(d3[2]) <= fabs(d3[3]) ? (d1[3] - d2[3] * h) + two * d3[2] * h * h : (d1[3] - d2[3] * h) + two * d3[3] * h * h;
+  }
+}
+
+// MAC component self-advection with ENO3 (the reference's use_3rd_eno_v,
+// ADVECTION_3D.h:323-325), every face of component `axis`.
+template <class T>
+__global__ void k_eno3_mac(const T* __restrict__ comp, T* __restrict__ out, const T* __restrict__ u,
+                           const T* __restrict__ v, const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw, int axis,
+                           T h, T dt) {
+  FS_IJK(Lc);
+  const int64_t c = Lc.at(i, j, k);
+  T uvel, vvel, wvel;
+  if (axis == 0) {
+    uvel = u[Lu.at(i, j, k)];
+    vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i - 1, j, k)]) + v[Lv.at(i - 1, j + 1, k)]) * T(0.25);
+    wvel = (((w[Lw.at(i, j, k)] + w[Lw.at(i, j, k + 1)]) + w[Lw.at(i - 1, j, k)]) + w[Lw.at(i - 1, j, k + 1)]) * T(0.25);
+  } else if (axis == 1) {
+    uvel = (((u[Lu.at(i, j, k)] + u[Lu.at(i + 1, j, k)]) + u[Lu.at(i, j - 1, k)]) + u[Lu.at(i + 1, j - 1, k)]) * T(0.25);
+    vvel = v[Lv.at(i, j, k)];
+    wvel = (((w[Lw.at(i, j, k)] + w[Lw.at(i, j, k + 1)]) + w[Lw.at(i, j - 1, k)]) + w[Lw.at(i, j - 1, k + 1)]) * T(0.25);
+  } else {
+    uvel = (((u[Lu.at(i, j, k)] + u[Lu.at(i + 1, j, k)]) + u[Lu.at(i, j, k - 1)]) + u[Lu.at(i + 1, j, k - 1)]) * T(0.25);
+    vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i, j, k - 1)]) + v[Lv.at(i, j + 1, k - 1)]) * T(0.25);
+    wvel = w[Lw.at(i, j, k)];
+  }
+  const T inv = T(1) / h, o2 = T(0.5) / h, o3 = inv * T(1) / T(3);
+  T dxm, dxp, dym, dyp, dzm, dzp;
+  eno3_pair(comp, c, 1, h, inv, o2, o3, dxm, dxp);
+  eno3_pair(comp, c, Lc.px, h, inv, o2, o3, dym, dyp);
+  eno3_pair(comp, c, Lc.slab, h, inv, o2, o3, dzm, dzp);
+  out[c] = comp[c] - dt * ((uvel * (uvel > T(0) ? dxm : dxp) + vvel * (vvel > T(0) ? dym : dyp)) +
+                           wvel * (wvel > T(0) ? dzm : dzp));
+}
+
+// ---------------------------------------------------------------------------
 // Sussman reinitialisation
 // ---------------------------------------------------------------------------
 
@@ -308,6 +374,13 @@ void weno5_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const 
 }
 
 template <class T>
+void eno3_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+              const Lay& Lw, int axis, double dx, double dt, cudaStream_t s) {
+  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz, 32, 4, 2);
+  k_eno3_mac<T><<<g.grid, g.block, 0, s>>>(comp, out, u, v, w, Lc, Lu, Lv, Lw, axis, T(dx), T(dt));
+}
+
+template <class T>
 void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s) {
   Launch3 g = launch3(L.nx, L.ny, L.nz);
   k_sign<T><<<g.grid, g.block, 0, s>>>(phi, sgn, L, T(dx));
@@ -344,6 +417,8 @@ void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s) {
                                   const Lay&, const Lay&, double, double, double, double, double, cudaStream_t);      \
   template void weno5_mac<T>(const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,          \
                              const Lay&, int, double, double, double, cudaStream_t);                                  \
+  template void eno3_mac<T>(const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,           \
+                            const Lay&, int, double, double, cudaStream_t);                                          \
   template void sign_function<T>(const T*, T*, const Lay&, double, cudaStream_t);                                    \
   template void sussman_step<T>(const T*, const T*, const T*, T*, const Lay&, double, double, double, double, double, \
                                 int, cudaStream_t);                                                                   \

@@ -10,7 +10,7 @@ thread ids return without doing anything.
 import numpy as np
 
 from . import (FS_FLAG_FAITHFUL_PROJECTION, FS_PRECISION_FP32_REFINE, FS_PRECISION_FP64, FS_STOP_ABSOLUTE,
-               FS_STOP_RELATIVE, FsError, Solver, default_params, pcg_csr)
+               FS_STOP_RELATIVE, FS_VELOCITY_ENO3, FS_VELOCITY_WENO5, FsError, Solver, default_params, pcg_csr)
 from .script import SCRIPT_BLOCK, SCRIPT_READER
 
 
@@ -89,6 +89,18 @@ class CUDA_PCG_METHOD(LINEAR_SOLVER):
         self.residual = res
 
 
+def velocity_scheme(vel_block):
+    """VELOCITY_ADVECTION { use_5th_weno_v, use_3rd_eno_v } (ADVECTION_3D.h:109-112,
+    317-328): ENO3 when only use_3rd_eno_v is set, else WENO5.  With both set the
+    reference applies WENO5 and then ENO3 to the same fields in one stage; that
+    double advection is refused."""
+    weno = vel_block.GetBoolean("use_5th_weno_v", False)
+    eno = vel_block.GetBoolean("use_3rd_eno_v", False)
+    if weno and eno:
+        raise ValueError("VELOCITY_ADVECTION selects both use_5th_weno_v and use_3rd_eno_v")
+    return FS_VELOCITY_ENO3 if eno else FS_VELOCITY_WENO5
+
+
 def params_from_block(block, base_grid):
     """fs_params from a FLUID_SOLVER_UNIFORM_AIR_WATER block; keys and
     defaults as EULERIAN_FLUID_SOLVER_3D.h:192-260, ADVECTION_3D and
@@ -125,6 +137,8 @@ def params_from_block(block, base_grid):
         viscosity_tolerance=block.GetFloat("viscosity_tolerance", 1e-8),
         flags=0 if block.GetBoolean("corrected_projection", True) else FS_FLAG_FAITHFUL_PROJECTION,
         surface_tension=block.GetFloat("surface_tension", 0.0),
+        velocity_scheme=velocity_scheme(block.FindBlock("VELOCITY_ADVECTION")),
+        velocity_epsilon=block.FindBlock("VELOCITY_ADVECTION").GetFloat("epsilon", 10e-6),
     )
     if p.precision == FS_PRECISION_FP32_REFINE:
         p.stop = FS_STOP_RELATIVE

@@ -59,6 +59,11 @@ typedef enum {
 } fs_precision;
 
 typedef enum {
+  FS_VELOCITY_WENO5 = 0,  /* VELOCITY_ADVECTION use_5th_weno_v (ADVECTION_METHOD_3D.h:42-279) */
+  FS_VELOCITY_ENO3 = 1    /* use_3rd_eno_v, the reference scripts' choice (ADVECTION_METHOD_3D.h:1639-1934) */
+} fs_velocity_scheme;
+
+typedef enum {
   FS_STOP_RELATIVE = 0,   /* ||b - A p||_2 / ||b||_2 < tolerance */
   FS_STOP_ABSOLUTE = 1    /* r.z < tolerance^2, the reference's PCG test (PCG_METHOD.cpp:87) */
 } fs_stop;
@@ -98,6 +103,8 @@ typedef struct {
   double cfl;                       /* CFL number used by fs_cfl_dt */
   int flags;                        /* FS_FLAG_* */
   double surface_tension;           /* sigma: the pressure jump sigma*kappa across the interface (0: none) */
+  int velocity_scheme;              /* fs_velocity_scheme of the velocity self-advection */
+  double velocity_epsilon;          /* VELOCITY_ADVECTION.epsilon of the WENO5 weights (0: weno_epsilon) */
 } fs_params;
 
 typedef struct {

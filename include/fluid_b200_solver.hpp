@@ -333,6 +333,14 @@ inline fs_params params_from_block(const SCRIPT_BLOCK& block, const GRID_STRUCTU
   p.viscosity_tolerance = block.GetFloat("viscosity_tolerance", 1e-8);
   p.flags = block.GetBoolean("corrected_projection", true) ? 0 : FS_FLAG_FAITHFUL_PROJECTION;
   p.surface_tension = block.GetFloat("surface_tension", 0.0);
+  // VELOCITY_ADVECTION (ADVECTION_3D.h:109-112, 317-328): ENO3 when only
+  // use_3rd_eno_v is set, else WENO5; with both set the reference applies both
+  // in one stage, which is refused.
+  const SCRIPT_BLOCK& vel = block.FindBlock("VELOCITY_ADVECTION");
+  const bool weno_v = vel.GetBoolean("use_5th_weno_v", false), eno_v = vel.GetBoolean("use_3rd_eno_v", false);
+  if (weno_v && eno_v) throw std::invalid_argument("VELOCITY_ADVECTION selects both use_5th_weno_v and use_3rd_eno_v");
+  p.velocity_scheme = eno_v ? FS_VELOCITY_ENO3 : FS_VELOCITY_WENO5;
+  p.velocity_epsilon = vel.GetFloat("epsilon", 10e-6);
   if (p.precision == FS_PRECISION_FP32_REFINE) p.stop = FS_STOP_RELATIVE;
   if (std::abs(grid.dx - grid.dy) > 1e-12 * grid.dx || std::abs(grid.dx - grid.dz) > 1e-12 * grid.dx)
     throw std::invalid_argument("the solver needs a uniform grid (dx = dy = dz)");

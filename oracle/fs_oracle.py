@@ -207,6 +207,56 @@ def weno5_velocity(u, v, w, dx, dt, eps):
 
 
 # ----------------------------------------------------------------------------
+# ENO3 (ADVECTION_METHOD_3D.h:1639-1934, the box variant)
+# ----------------------------------------------------------------------------
+
+def eno3_derivatives(fg, axis, dx, g=G):
+    """One-sided third-order ENO derivatives D-, D+ along `axis` of a
+    ghosted field: divided differences of orders 1-3 (the second scaled by
+    1/(2dx), the third by (1/dx)/3), each side choosing its stencil by the
+    smaller second difference and then the smaller third difference."""
+    f = lambda s: _shift(fg, axis, s, g)
+    inv = 1.0 / dx
+    o2 = 0.5 / dx
+    o3 = inv * 1.0 / 3.0
+    d1 = {s: inv * (f(s + 1) - f(s)) for s in range(-3, 3)}
+    d2 = {s: o2 * (d1[s] - d1[s - 1]) for s in range(-2, 3)}
+    d3 = {s: o3 * (d2[s + 1] - d2[s]) for s in range(-2, 2)}
+    a = np.abs
+    dm = np.where(a(d2[-1]) <= a(d2[0]),
+                  np.where(a(d3[-2]) <= a(d3[-1]),
+                           (d1[-1] + d2[-1] * dx) + 2.0 * d3[-2] * dx * dx,
+                           (d1[-1] + d2[-1] * dx) + 2.0 * d3[-1] * dx * dx),
+                  np.where(a(d3[-1]) <= a(d3[0]),
+                           (d1[-1] + d2[0] * dx) - d3[-1] * dx * dx,
+                           (d1[-1] + d2[0] * dx) - d3[0] * dx * dx))
+    dp = np.where(a(d2[0]) <= a(d2[1]),
+                  np.where(a(d3[-1]) <= a(d3[0]),
+                           (d1[0] - d2[0] * dx) - d3[-1] * dx * dx,
+                           (d1[0] - d2[0] * dx) - d3[0] * dx * dx),
+                  np.where(a(d3[0]) <= a(d3[1]),
+                           (d1[0] - d2[1] * dx) + 2.0 * d3[0] * dx * dx,
+                           (d1[0] - d2[1] * dx) + 2.0 * d3[1] * dx * dx))
+    return dm, dp
+
+
+def eno3_velocity(u, v, w, dx, dt):
+    """Forward-Euler ENO3 self-advection of the three MAC components
+    (ADVECTION_3D.h:323-325: each component with its own zero-ghosted copy,
+    the advecting velocity as in the WENO5 path)."""
+    ug, vg, wg = zero_ghosts(u), zero_ghosts(v), zero_ghosts(w)
+    out = []
+    for axis, comp in enumerate((u, v, w)):
+        src = (ug, vg, wg)[axis]
+        uvel, vvel, wvel = _face_velocities(axis, ug, vg, wg)
+        dxm, dxp = eno3_derivatives(src, 0, dx)
+        dym, dyp = eno3_derivatives(src, 1, dx)
+        dzm, dzp = eno3_derivatives(src, 2, dx)
+        out.append(_upwind_update(comp, dt, uvel, vvel, wvel, dxm, dxp, dym, dyp, dzm, dzp))
+    return tuple(out)
+
+
+# ----------------------------------------------------------------------------
 # Sussman reinitialisation (ADVECTION_METHOD_3D.h:745-1637,
 # EULERIAN_FLUID_SOLVER_3D.h Reinitialization)
 # ----------------------------------------------------------------------------
@@ -862,7 +912,7 @@ def step(phi, u, v, w, dx, dt, P, p0=None, order=3):
 
     def stage(vel, c0, c1, base):
         nonlocal p
-        a = weno5_velocity(*vel, dx, dt, eps)
+        a = eno3_velocity(*vel, dx, dt) if P.get("velocity_eno3", False) else weno5_velocity(*vel, dx, dt, eps)
         a = zero_walls(*a)
         a = add_gravity(*a, P["gravity"], dt)
         if P.get("viscosity", True):

@@ -151,6 +151,20 @@ void fsref_weno5_velocity(void* h, double dt, int own_ghost) {
   });
 }
 
+// One forward-Euler ENO3 update of the three MAC components, each with its
+// own zero-filled ghost copy (ADVECTION_3D.h:323-325).
+void fsref_eno3_velocity(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  MULTITHREADING& mt = *c->world.multithreading;
+  run_threads(c, [&](int t) {
+    zero_ghost_velocities(s, t);
+    ADVECTION_METHOD_3D<T>::ENO3rd(t, *s.water_velocity_field_mac_x, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt);
+    ADVECTION_METHOD_3D<T>::ENO3rd(t, *s.water_velocity_field_mac_y, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt);
+    ADVECTION_METHOD_3D<T>::ENO3rd(t, *s.water_velocity_field_mac_z, s.vector_field_mac_ghost_z, s.vector_field_mac_ghost_x, s.vector_field_mac_ghost_y, s.vector_field_mac_ghost_z, dt, mt);
+  });
+}
+
 // One reinitialisation block: S = phi0/sqrt(phi0^2 + dx^2) and
 // iteration_number_for_reinitialization Sussman pseudo-steps of
 // dtau = dx/scaling_number (EULERIAN_FLUID_SOLVER_3D.h Reinitialization).

@@ -61,6 +61,7 @@ def _lib():
     lib.fsref_cfl.argtypes = [ctypes.c_void_p]
     lib.fsref_curvature.argtypes = [ctypes.c_void_p, _dp]
     lib.fsref_write_levelset.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    lib.fsref_eno3_velocity.argtypes = [ctypes.c_void_p, ctypes.c_double]
     lib.fsref_linear_solve.restype = ctypes.c_int
     lib.fsref_linear_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _dp, _dp]
     return lib
@@ -288,6 +289,9 @@ class RefCase:
 
     def cfl(self):
         return self._lib.fsref_cfl(self.h)
+
+    def eno3_velocity(self, dt):
+        return self._quiet(self._lib.fsref_eno3_velocity, self.h, dt)
 
     def write_levelset(self, path):
         """LEVELSET_3D::Write of the current level set to `path`."""

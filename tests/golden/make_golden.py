@@ -20,6 +20,7 @@ on the air/water unit-cube box with Neumann pressure walls:
   projection_tension  curvature (LEVELSET_3D::ComputeCurvatures) and
                    PROJECTION_3D::Solve with a surface tension jump condition
   levelset_file    the bytes LEVELSET_3D::Write produces for a level set
+  eno3_velocity    ADVECTION_METHOD_3D<T>::ENO3rd on u, v, w
 """
 import os
 import sys
@@ -169,6 +170,18 @@ def main():
     with open(path, "rb") as f:
         raw = np.frombuffer(f.read(), dtype=np.uint8).copy()
     fixtures["levelset_file"] = dict(n=n, dx=c.dx, phi=phi, raw=raw)
+    c.close()
+
+    # ENO3 MAC self-advection (the scheme the reference's own scripts select
+    # for velocity, use_3rd_eno_v), 10^3
+    n = 10
+    c = case(n, velocity_weno=False)
+    vel = {k: rng.normal(size=c.shape(k)) * 0.3 for k in "uvw"}
+    for k, a in vel.items():
+        c.set(k, a)
+    c.eno3_velocity(2e-3)
+    fixtures["eno3_velocity"] = dict(n=n, dx=c.dx, dt=2e-3, **vel, out_u=c.get("u"), out_v=c.get("v"),
+                                     out_w=c.get("w"))
     c.close()
 
     for name, d in fixtures.items():

@@ -98,3 +98,10 @@ def test_projection_with_surface_tension_matches_reference():
     np.testing.assert_array_equal(p, g["out_p"])
     for k, a in zip("uvw", (u, v, w)):
         np.testing.assert_array_equal(a, g["out_" + k])
+
+
+def test_eno3_velocity_matches_reference():
+    g = load("eno3_velocity")
+    out = O.eno3_velocity(g["u"], g["v"], g["w"], float(g["dx"]), float(g["dt"]))
+    for k, a in zip("uvw", out):
+        np.testing.assert_array_equal(a, g["out_" + k])
