@@ -34,9 +34,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # algorithmic bytes per unknown and PCG iteration (each array element once per pass)
-# FP32+refine: spmv 20 (p, ax, ay, az read; q write) + residual update 16 (r, q, diag read; r write)
-#              + direction update 32 (x64 read/write, p read/write, r, diag read)
-BYTES_PER_UNKNOWN_PCG_FP32 = 68
+# FP32+refine: spmv 20 (p, ax, ay, az read; q write) + residual update 14 (r, q read, bf16 1/diag read;
+#              r write) + direction update 30 (x64 read/write, p read/write, r read, bf16 1/diag read)
+BYTES_PER_UNKNOWN_PCG_FP32 = 64
 # FP64: spmv 40 + residual update 32 + direction update 48
 BYTES_PER_UNKNOWN_PCG_FP64 = 120
 # DRAM bytes (read + write) of one FP32 PCG iteration at 256^3 measured by ncu

@@ -82,6 +82,7 @@ struct fs_ctx {
   double* kappa = nullptr;  // mean curvature (surface tension)
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
+  unsigned short* pdinv = nullptr;  // bf16 1/diag: the Jacobi preconditioner of the FP32 pressure solve
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
   // viscosity systems, one per component (storage type S)
   void* vs[3][9] = {};  // ax, ay, az, diag, rhs, x, r, p, q
@@ -113,6 +114,7 @@ struct fs_ctx {
   bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
   double reliable_delta = 0.1;  // residual drop between reliable updates (FS_RELIABLE_DELTA to sweep)
   int flux32 = 2;               // arithmetic of the FP32 flux SpMV (Op7::flux32; FS_FLUX32 to sweep)
+  int lean = 1;  // FP32 pressure solve preconditioned by the bf16 inverse diagonal (Op7::dinv16; FS_LEAN=0 off)
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -464,9 +466,11 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     outer = 1;
   } else {
     build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
-                                      (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s);
+                                      (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s,
+                                      c->lean ? c->pdinv : nullptr);
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
     A.flux32 = c->flux32;
+    if (c->lean) A.dinv16 = c->pdinv;
     const size_t vbytes = c->Lc.total * sizeof(float);
     double bb = 0.0;
     float *r32 = (float*)c->pr, *p32 = (float*)c->pp, *q32 = (float*)c->pq;
@@ -494,9 +498,9 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
     if (rel > P.tolerance) {
       // Mixed-precision CG: the FP64 pressure p64 is the iterate; the face
       // couplings, the residual r, the search direction p and q = A p are
-      // FP32 (the flux-form operator is evaluated in FP64 arithmetic from
-      // them): 68 bytes per unknown and iteration against 120 for the FP64
-      // solve.  Every time the recursive residual drops by reliable_delta
+      // FP32 (the flux-form operator in FP32 arithmetic, Op7::flux32) and the
+      // Jacobi preconditioner is 1/diag in bf16: 64 bytes per unknown and
+      // iteration against 120 for the FP64 solve.  Every time the recursive residual drops by reliable_delta
       // the true FP64 residual of p64 replaces it (reliable update), keeping
       // the search direction; the recursion stops at the tolerance itself
       // and the true residual decides.  A sequence whose true residual got
@@ -1096,6 +1100,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
   c->debug = std::getenv("FS_DEBUG") != nullptr;
+  if (const char* e = std::getenv("FS_LEAN")) c->lean = std::atoi(e) != 0;
   if (const char* e = std::getenv("FS_FLUX32")) {
     const int v = std::atoi(e);
     if (v >= 0 && v <= 2) c->flux32 = v;
@@ -1137,6 +1142,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   if (c->fp32) {
     if ((s = dalloc(c, &c->px, cv)) != FS_OK) return fail(s);
     if ((s = dalloc(c, &c->prhs, cv)) != FS_OK) return fail(s);
+    if ((s = dalloc(c, (void**)&c->pdinv, c->Lc.total * sizeof(unsigned short))) != FS_OK) return fail(s);
   }
   if (prm.viscosity) {
     const size_t fb[3] = {ub, vb, wb};

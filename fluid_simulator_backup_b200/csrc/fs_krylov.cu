@@ -12,8 +12,9 @@
 //   spmv    q = A p, p.q, alpha                (reads p, ax, ay, az; writes q)
 //   update  r -= alpha q, r.z, r.r, beta       (reads r, q, diag; writes r)
 //   pupdate x += alpha p, p = r/diag + beta p  (reads x, p, r, diag; writes x, p)
-// z = r/diag is never stored: 68 bytes per unknown and iteration with FP32
-// vectors and an FP64 iterate, 120 in FP64.  Dot products are reduced in
+// z = r/diag is never stored: 64 bytes per unknown and iteration with FP32
+// vectors, an FP64 iterate and the bf16 inverse diagonal (Op7::dinv16), 120
+// in FP64.  Dot products are reduced in
 // FP64 per block and finished by the last block (deterministic for a given
 // grid), which also takes the scalar decisions (alpha, beta, convergence,
 // caps, breakdown) and writes them to the PcgState in device memory.  Every
@@ -54,6 +55,14 @@ int reduction_blocks(int64_t n) {
 }
 
 int pcg_blocks(const Lay& L) { return reduction_blocks((int64_t)L.nx * L.ny * L.nz); }
+
+// The Jacobi preconditioner z = M^-1 r: r / diag, or r * dinv16 when the
+// operator carries the bf16 inverse diagonal (Op7::dinv16).
+__device__ __forceinline__ float bf16_to_float(unsigned short b) { return __uint_as_float((unsigned)b << 16); }
+template <class V, class R>
+__device__ __forceinline__ R precond1(const Op7<V>& A, R r, int64_t c) {
+  return A.dinv16 ? r * (R)bf16_to_float(A.dinv16[c]) : r / (R)A.diag[c];
+}
 
 // (A x)_c evaluated in the type X of x (the operator's coefficients are
 // converted): FP32 iterates get FP32 arithmetic, FP64 iterates FP64.
@@ -135,7 +144,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_init(Op7<V> A, const RT* b,
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
     const RT bv = b[c];
     const RT rv = bv - apply7<V, RT>(A, x, c);
-    const RT z = rv / (RT)A.diag[c];
+    const RT z = precond1<V, RT>(A, rv, c);
     r[c] = rv;  // b may alias r: each element is read before it is written
     p[c] = (V)z;
     rz += (double)rv * (double)z;
@@ -177,7 +186,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_pupdate(Op7<V> A, const RT*
   Cursor cur;
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
-    p[c] = (V)((RT)p[c] * beta + r[c] / (RT)A.diag[c]);
+    p[c] = (V)((RT)p[c] * beta + precond1<V, RT>(A, r[c], c));
   }
 }
 
@@ -192,7 +201,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_resume(Op7<V> A, const RT* 
   for (cur.init(A.L); cur.valid(A.L); cur.next(A.L)) {
     const int64_t c = A.L.at(cur.i, cur.j, cur.k);
     const RT rv = r[c];
-    rz += (double)rv * (double)(rv / (RT)A.diag[c]);
+    rz += (double)rv * (double)precond1<V, RT>(A, rv, c);
     rr += (double)rv * (double)rv;
   }
   double tot[3];
@@ -284,6 +293,18 @@ template <class T> __device__ __forceinline__ void set_lane(V4<T>& v, int m, T x
   if (m == 0) v.a = x; else if (m == 1) v.b = x; else if (m == 2) v.c = x; else v.d = x;
 }
 
+// ---- the Jacobi preconditioner z = M^-1 r on four cells (precond1 above)
+template <class V>
+__device__ __forceinline__ V4<V> precond4(const Op7<V>& A, const V4<V>& r, int64_t c) {
+  if (A.dinv16) {
+    const uint2 u = *reinterpret_cast<const uint2*>(A.dinv16 + c);  // 4 bf16, 8-byte aligned (c % 4 == 0)
+    return {r.a * (V)__uint_as_float(u.x << 16), r.b * (V)__uint_as_float(u.x & 0xffff0000u),
+            r.c * (V)__uint_as_float(u.y << 16), r.d * (V)__uint_as_float(u.y & 0xffff0000u)};
+  }
+  const V4<V> d = ld4(A.diag + c);
+  return {r.a / d.a, r.b / d.b, r.c / d.c, r.d / d.d};
+}
+
 // Grid-stride cursor over (vector, j, k): vector w covers i = 4w .. 4w+3.
 struct VecCursor {
   Lay Lv;  // the layout with nx replaced by the number of vectors per row
@@ -365,6 +386,26 @@ __device__ __forceinline__ void spmv_row4(const Op7<V>& A, const V* __restrict__
   }
 }
 
+// p.q over the grid and the step length alpha = r.z / p.q (last block).
+__device__ __forceinline__ void spmv_alpha(double pq, PcgState* st, double* partials) {
+  pq = block_sum(pq);
+  double tot;
+  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) {
+    st->pq = tot;
+    const double alpha = st->rz / tot;
+    if (!(tot > 0.0) || !isfinite(alpha)) {
+      // a non-positive p.Ap (or an infinite step): the iteration has lost its
+      // footing in this arithmetic; keep the iterate and stop
+      st->status = PCG_STAGNATED;
+      st->done = 1;
+      st->x_pending = 0;
+    } else {
+      st->alpha = alpha;
+      st->x_pending = 1;
+    }
+  }
+}
+
 template <class V, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cg_spmv(Op7<V> A, const V* __restrict__ p, V* __restrict__ q,
                                                  PcgState* st, double* partials, int kchunk) {
@@ -402,22 +443,7 @@ __global__ void __launch_bounds__(256, MINB) k_cg_spmv(Op7<V> A, const V* __rest
       azc = azu;
     }
   }
-  pq = block_sum(pq);
-  double tot;
-  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) {
-    st->pq = tot;
-    const double alpha = st->rz / tot;
-    if (!(tot > 0.0) || !isfinite(alpha)) {
-      // a non-positive p.Ap (or an infinite step): the iteration has lost its
-      // footing in this arithmetic; keep the iterate and stop
-      st->status = PCG_STAGNATED;
-      st->done = 1;
-      st->x_pending = 0;
-    } else {
-      st->alpha = alpha;
-      st->x_pending = 1;
-    }
-  }
+  spmv_alpha(pq, st, partials);
 }
 
 // ---- residual update: r -= alpha q, r.z and r.r, beta and the decisions
@@ -433,20 +459,21 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update(Op7<V> A, V* __restri
     const int64_t c = A.L.at(i0, vc.cur.j, vc.cur.k);
     const int nvalid = min(4, A.L.nx - i0);
     V4<V> rv = ld4(r + c);
-    const V4<V> qv = ld4(q + c), dv = ld4(A.diag + c);
+    const V4<V> qv = ld4(q + c);
     rv.a -= alpha * qv.a;
     rv.b -= alpha * qv.b;
     rv.c -= alpha * qv.c;
     rv.d -= alpha * qv.d;
     st4(r + c, rv, nvalid);
-    // r.z and r.r of the vector's cells in the vector type (z = r/diag as the
+    // r.z and r.r of the vector's cells in the vector type (z formed as the
     // direction update forms it), accumulated in FP64 across vectors
+    const V4<V> zv = precond4(A, rv, c);
     V rz4 = V(0), rr4 = V(0);
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       if (m < nvalid) {
         const V rm = lane(rv, m);
-        rz4 += rm * (rm / lane(dv, m));
+        rz4 += rm * lane(zv, m);
         rr4 += rm * rm;
       }
     }
@@ -514,11 +541,11 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_pupdate(Op7<V> A, X* __restr
       st4(x + c, xv, nvalid);
     }
     if (move_p) {
-      const V4<V> rv = ld4(r + c), dv = ld4(A.diag + c);
-      pv.a = pv.a * beta + rv.a / dv.a;
-      pv.b = pv.b * beta + rv.b / dv.b;
-      pv.c = pv.c * beta + rv.c / dv.c;
-      pv.d = pv.d * beta + rv.d / dv.d;
+      const V4<V> zv = precond4(A, ld4(r + c), c);
+      pv.a = pv.a * beta + zv.a;
+      pv.b = pv.b * beta + zv.b;
+      pv.c = pv.c * beta + zv.c;
+      pv.d = pv.d * beta + zv.d;
       st4(p + c, pv, nvalid);
     }
   }
@@ -542,7 +569,7 @@ int g_cg_blocks[2][2][3];  // [X double?][V double?][spmv, update, pupdate]: res
 // spills to speak of), 2 for FP64 (128 registers; fewer spill)
 int g_spmv_minb_env = 0;
 template <class V> int spmv_minb() { return g_spmv_minb_env ? g_spmv_minb_env : (sizeof(V) == 4 ? 4 : 2); }
-}
+}  // namespace
 
 template <class V, class X>
 void cg_prepare() {

@@ -9,6 +9,8 @@
 //                    from phi: the FP64 residual of the FP32_REFINE path
 //   velocity_correct u -= dt grad p / rho (UpdateVelocityByPressureGradient-
 //                    VariableDensity, :1099-1449), fused with the RK combine
+#include <cuda_bf16.h>
+
 #include "fs_kernels.h"
 
 namespace fsb {
@@ -97,7 +99,7 @@ __global__ void k_pressure_faces(const T* __restrict__ phi, Lay Lc, double rn, d
 
 template <class T, class V>
 __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, double rp, double inv2,
-                                V* __restrict__ diag, double* __restrict__ extra0) {
+                                V* __restrict__ diag, double* __restrict__ extra0, unsigned short* __restrict__ dinv16) {
   FS_IJK(Lc);
   const int64_t c = Lc.at(i, j, k);
   const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
@@ -119,6 +121,7 @@ __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, do
   }
   if (s == 0.0) s = 1.0;
   diag[c] = (V)(inv2 * s);
+  if (dinv16) dinv16[c] = __bfloat16_as_ushort(__float2bfloat16_rn((float)(1.0 / (inv2 * s))));
 }
 
 // r64 = b - A p64 with A from phi in FP64 (same formulas as the two kernels
@@ -406,11 +409,11 @@ void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* part
 
 template <class T, class V>
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
-                             V* diag, double* extra0, cudaStream_t s) {
+                             V* diag, double* extra0, cudaStream_t s, unsigned short* dinv16) {
   Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
   const double inv2 = 1.0 / (dx * dx);
   k_pressure_faces<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, ax, ay, az);
-  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag, extra0);
+  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag, extra0, dinv16);
 }
 
 template <class T>
@@ -506,7 +509,7 @@ FS_PINST(double)
 
 #define FS_BINST(T, V)                                                                                        \
   template void build_pressure_operator<T, V>(const T*, const Lay&, double, double, double, V*, V*, V*, V*, double*, \
-                                              cudaStream_t);
+                                              cudaStream_t, unsigned short*);
 FS_BINST(float, float)
 FS_BINST(double, double)
 FS_BINST(double, float)
