@@ -43,7 +43,7 @@ BYTES_PER_UNKNOWN_PCG_FP64 = 120
 # (dram__bytes_read.sum + dram__bytes_write.sum of k_cg_spmv, k_cg_update,
 # k_cg_pupdate, one capture of the bench workload); scaled by the unknowns
 # for other sizes
-TRAFFIC_PER_ITERATION_256_FP32 = 1089.1e6
+TRAFFIC_PER_ITERATION_256_FP32 = 1006.4e6
 # PCG iterations per projection of the FP64 GPU path on this workload at 256^3
 # (6725 per timestep of 3 projections over steps 4-6, measured by the default
 # run's fp64 block); the reference arm prices its projection with it
