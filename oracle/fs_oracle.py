@@ -257,6 +257,148 @@ def eno3_velocity(u, v, w, dx, dt):
 
 
 # ----------------------------------------------------------------------------
+# Fast sweeping reinitialisation (LEVELSET_3D.h:601-610, 734-918)
+# ----------------------------------------------------------------------------
+
+# The two sweeps of each call, by sweep_direction % 4 (LEVELSET_3D.h:789-818):
+# traversal signs (x, y, z) of the first and the second sweep.
+FAST_SWEEP_ORDERS = (((1, 1, 1), (-1, -1, -1)), ((-1, 1, -1), (1, -1, 1)),
+                     ((1, -1, -1), (-1, 1, 1)), ((-1, -1, 1), (1, 1, -1)))
+
+
+def fast_sweeping_prepare(phi, dx):
+    """The set-up of LEVELSET_3D::FastSweepingMethod (LEVELSET_3D.h:736-781):
+    cells farther than 20 dx from the interface and cells with a face
+    neighbour of the other sign (ghosts: copies of the boundary cell,
+    FillGhostCellsFrom) are fixed; the other cells get +-20 dx.  The
+    reference marks neighbours while it scans, but a marked neighbour always
+    has a neighbour of the other sign itself, so the fixed set does not
+    depend on the scan order.  Returns (phi, fixed)."""
+    nb = 20.0 * dx
+    g = np.pad(phi, 1, mode="edge")
+    pos = g > 0.0
+    c = pos[1:-1, 1:-1, 1:-1]
+    other = np.zeros(phi.shape, dtype=bool)
+    for sl in ((slice(1, -1), slice(1, -1), slice(2, None)), (slice(1, -1), slice(1, -1), slice(0, -2)),
+               (slice(1, -1), slice(2, None), slice(1, -1)), (slice(1, -1), slice(0, -2), slice(1, -1)),
+               (slice(2, None), slice(1, -1), slice(1, -1)), (slice(0, -2), slice(1, -1), slice(1, -1))):
+        other |= pos[sl] != c
+    far = np.where(phi > 0, phi, -phi) > nb
+    fixed = far | other
+    out = np.where(fixed, phi, np.where(phi > 0.0, nb, -nb))
+    return out, fixed
+
+
+def _csqrt(x):
+    """C's sqrt: NaN for a negative argument."""
+    return math.sqrt(x) if x >= 0.0 else math.nan
+
+
+def fast_sweep(g, fixed, dx, signs, typo=False):
+    """One Gauss-Seidel sweep (LEVELSET_3D.h:837-918) over the interior, z
+    outermost and x innermost, in the traversal signs given, in place on the
+    ghosted nested list g ([nz+2][ny+2][nx+2]); the ghosts are not touched.
+
+    The reference's INCREASING_SORT3 (MACROS.h:61-68) assigns a3 twice and
+    leaves a2 untouched when c < b < a; with `typo` a2 then keeps the value
+    of the cell updated before it in the sweep (a2 is a local of Sweep, so
+    an input whose first such cell comes before any other update raises:
+    the reference reads an uninitialised value there); without it a2 = b."""
+    nz, ny, nx = len(g) - 2, len(g[0]) - 2, len(g[0][0]) - 2
+    h = dx
+    hh = h * h
+    hh2 = hh * 2.0
+    third = 1.0 / 3.0
+    fx = fixed.tolist()
+    sx, sy, sz = signs
+    a2 = None
+    ks = range(nz) if sz > 0 else range(nz - 1, -1, -1)
+    js = range(ny) if sy > 0 else range(ny - 1, -1, -1)
+    iss = range(nx) if sx > 0 else range(nx - 1, -1, -1)
+    for k in ks:
+        gk, gkm, gkp = g[k + 1], g[k], g[k + 2]
+        for j in js:
+            row, rowm, rowp = gk[j + 1], gk[j], gk[j + 2]
+            zm, zp = gkm[j + 1], gkp[j + 1]
+            fxr = fx[k][j]
+            for i in iss:
+                if fxr[i]:
+                    continue
+                pc = row[i + 1]
+                if pc > 0.0:
+                    l, r = row[i], row[i + 2]
+                    a = r if l > r else l
+                    l, r = rowm[i + 1], rowp[i + 1]
+                    b = r if l > r else l
+                    l, r = zm[i + 1], zp[i + 1]
+                    c = r if l > r else l
+                else:
+                    l, r = row[i], row[i + 2]
+                    a = l if l > r else r
+                    l, r = rowm[i + 1], rowp[i + 1]
+                    b = l if l > r else r
+                    l, r = zm[i + 1], zp[i + 1]
+                    c = l if l > r else r
+                if a <= b:
+                    if b <= c:
+                        a1, a2, a3 = a, b, c
+                    elif a <= c:
+                        a1, a2, a3 = a, c, b
+                    else:
+                        a1, a2, a3 = c, a, b
+                else:
+                    if a <= c:
+                        a1, a2, a3 = b, a, c
+                    elif b <= c:
+                        a1, a2, a3 = b, c, a
+                    else:
+                        a1, a3 = c, a
+                        if typo:
+                            if a2 is None:
+                                raise ValueError("the reference reads an uninitialised a2 here")
+                        else:
+                            a2 = b
+                if pc > 0.0:
+                    upd = a1 + h
+                    if upd > a2:
+                        d = a1 - a2
+                        upd = 0.5 * ((a1 + a2) + _csqrt(hh2 - d * d))
+                        if upd > a3:
+                            t = (a1 + a2) + a3
+                            upd = third * (t + _csqrt(t * t - 3.0 * (((a1 * a1 + a2 * a2) + a3 * a3) - hh)))
+                    row[i + 1] = pc if upd > pc else upd
+                else:
+                    upd = a3 - h
+                    if upd < a2:
+                        d = a3 - a2
+                        upd = 0.5 * ((a3 + a2) - _csqrt(hh2 - d * d))
+                        if upd < a1:
+                            t = (a1 + a2) + a3
+                            upd = third * (t - _csqrt(t * t - 3.0 * (((a1 * a1 + a2 * a2) + a3 * a3) - hh)))
+                    row[i + 1] = upd if upd > pc else pc
+
+
+def fast_sweeping(phi, dx, direction, typo=False, pairs=1):
+    """LEVELSET_3D::ReinitializeByFastSweeping on one thread (LEVELSET_3D.h:
+    601-610): the set-up, one ghost fill from its result, and the two sweeps
+    of sweep_direction % 4 (no ghost fill between them).  `typo`: see
+    fast_sweep.
+
+    Every call of the reference starts with the set-up, which resets all
+    cells off the interface to +-20 dx, so only the two sweeps of that call
+    reach the result, also in FullFastSweepingMethodThreaded's four calls
+    (LEVELSET_3D.h:828-835): distances along the six other sweep octants
+    are not propagated.  pairs = 4 is the corrected full method: one set-up,
+    then the sweep pairs of direction, direction+1, ... (all eight sweeps)."""
+    cur, fixed = fast_sweeping_prepare(phi, dx)
+    g = np.pad(cur, 1, mode="edge").tolist()
+    for p in range(pairs):
+        for signs in FAST_SWEEP_ORDERS[(direction + p) % 4]:
+            fast_sweep(g, fixed, dx, signs, typo=typo)
+    return np.array(g)[1:-1, 1:-1, 1:-1]
+
+
+# ----------------------------------------------------------------------------
 # Sussman reinitialisation (ADVECTION_METHOD_3D.h:745-1637,
 # EULERIAN_FLUID_SOLVER_3D.h Reinitialization)
 # ----------------------------------------------------------------------------

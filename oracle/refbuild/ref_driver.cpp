@@ -305,6 +305,20 @@ int fsref_linear_solve(void* h, int n, int nnz, const double* vals, const int* c
 
 // The level set in the reference's binary format (LEVELSET_3D::Write,
 // LEVELSET_3D.h:1132-1160).
+// LEVELSET_3D::ReinitializeByFastSweeping without its closing Update
+// (normals and curvature, which can exit() on flat regions): a ghost fill,
+// then FastSweepingMethod with sweep_direction = direction
+// (LEVELSET_3D.h:601-610, 734-821).
+void fsref_fast_sweeping(void* h, int direction) {
+  RefCase* c = static_cast<RefCase*>(h);
+  LEVELSET_3D& ls = *c->world.eulerian_solver.water_levelset;
+  ls.sweep_direction = direction;
+  run_threads(c, [&](int t) {
+    ls.FillGhostCellsFrom(t, ls.phi, false);
+    ls.FastSweepingMethod(t);
+  });
+}
+
 void fsref_write_levelset(void* h, const char* path) {
   EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
   s.water_levelset->Write(path);

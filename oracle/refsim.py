@@ -62,6 +62,7 @@ def _lib():
     lib.fsref_curvature.argtypes = [ctypes.c_void_p, _dp]
     lib.fsref_write_levelset.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
     lib.fsref_eno3_velocity.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.fsref_fast_sweeping.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.fsref_linear_solve.restype = ctypes.c_int
     lib.fsref_linear_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _dp, _dp]
     return lib
@@ -292,6 +293,11 @@ class RefCase:
 
     def eno3_velocity(self, dt):
         return self._quiet(self._lib.fsref_eno3_velocity, self.h, dt)
+
+    def fast_sweeping(self, direction):
+        """LEVELSET_3D::ReinitializeByFastSweeping (without its Update) with
+        sweep_direction = direction, on the injected level set."""
+        return self._quiet(self._lib.fsref_fast_sweeping, self.h, int(direction))
 
     def write_levelset(self, path):
         """LEVELSET_3D::Write of the current level set to `path`."""

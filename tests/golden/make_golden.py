@@ -21,6 +21,10 @@ on the air/water unit-cube box with Neumann pressure walls:
                    PROJECTION_3D::Solve with a surface tension jump condition
   levelset_file    the bytes LEVELSET_3D::Write produces for a level set
   eno3_velocity    ADVECTION_METHOD_3D<T>::ENO3rd on u, v, w
+  fast_sweeping    LEVELSET_3D::FastSweepingMethod (after its ghost fill) on a
+                   noisy sphere, sweep_direction 0 and 3; inputs whose sort
+                   never reads the uninitialised a2 of INCREASING_SORT3's
+                   typo branch (checked with the oracle)
 """
 import os
 import sys
@@ -182,6 +186,19 @@ def main():
     c.eno3_velocity(2e-3)
     fixtures["eno3_velocity"] = dict(n=n, dx=c.dx, dt=2e-3, **vel, out_u=c.get("u"), out_v=c.get("v"),
                                      out_w=c.get("w"))
+    c.close()
+
+    # fast sweeping reinitialisation, 20^3: a sphere scaled by 1.5 plus noise
+    n = 20
+    c = case(n, water_drop=False)
+    frng = np.random.default_rng(3)
+    phi = sphere(n, (0.5, 0.45, 0.5), 0.3) * 1.5 + frng.normal(size=(n, n, n)) * 0.01
+    outs = {}
+    for direction in (0, 3):
+        c.set("phi", phi)
+        c.fast_sweeping(direction)
+        outs[f"out_{direction}"] = c.get("phi")
+    fixtures["fast_sweeping"] = dict(n=n, dx=c.dx, phi=phi, **outs)
     c.close()
 
     for name, d in fixtures.items():
