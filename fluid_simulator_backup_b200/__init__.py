@@ -30,6 +30,7 @@ FIELD = {"phi": 0, "u": 1, "v": 2, "w": 3, "pressure": 4, "p": 4, "divergence": 
 FS_PRECISION_FP64, FS_PRECISION_FP32_REFINE = 0, 1
 FS_STOP_RELATIVE, FS_STOP_ABSOLUTE = 0, 1
 FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER, FS_FLAG_CURVATURE_TYPO = 1, 2, 4, 8
+FS_FLAG_SORT_TYPO = 16
 FS_VELOCITY_WENO5, FS_VELOCITY_ENO3 = 0, 1
 
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
@@ -38,7 +39,7 @@ EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", 
             "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc", "fs_adjoint_reset", "fs_adjoint_density_bars",
             "fs_step_adjoint", "fs_advect_levelset_adjoint", "fs_advect_velocity_adjoint", "fs_reinitialize_adjoint",
             "fs_viscosity_adjoint", "fs_project_adjoint", "fs_curvature", "fs_write_levelset", "fs_read_levelset",
-            "fs_write_state", "fs_read_state")
+            "fs_write_state", "fs_read_state", "fs_fast_sweeping")
 
 
 class FsError(RuntimeError):
@@ -60,7 +61,7 @@ class Params(ctypes.Structure):
                 ("viscosity", ctypes.c_int), ("viscosity_tolerance", ctypes.c_double),
                 ("viscosity_max_iteration", ctypes.c_int), ("cfl", ctypes.c_double), ("flags", ctypes.c_int),
                 ("surface_tension", ctypes.c_double), ("velocity_scheme", ctypes.c_int),
-                ("velocity_epsilon", ctypes.c_double)]
+                ("velocity_epsilon", ctypes.c_double), ("fast_sweeping", ctypes.c_int)]
 
     def as_dict(self):
         d = {}
@@ -122,6 +123,7 @@ def lib():
         L.fs_advect_levelset.argtypes = [vp, ctypes.c_double]
         L.fs_advect_velocity.argtypes = [vp, ctypes.c_double]
         L.fs_reinitialize.argtypes = [vp]
+        L.fs_fast_sweeping.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.fs_viscosity.argtypes = [vp, ctypes.c_double, ip]
         L.fs_pcg_csr.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
                                  ctypes.c_int, ip, dp]
@@ -289,6 +291,11 @@ class Solver:
 
     def reinitialize(self):
         _check(lib().fs_reinitialize(self._h), "fs_reinitialize")
+
+    def fast_sweeping(self, direction=-1, pairs=1):
+        """LEVELSET_3D::ReinitializeByFastSweeping on phi (direction -1: the
+        context's sweep counter, which advances)."""
+        _check(lib().fs_fast_sweeping(self._h, int(direction), int(pairs)), "fs_fast_sweeping")
 
     def viscosity(self, dt):
         it = ctypes.c_int()

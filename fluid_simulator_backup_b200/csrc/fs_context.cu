@@ -80,6 +80,9 @@ struct fs_ctx {
   // pressure (FP64) and projection work
   double *p64 = nullptr, *b64 = nullptr, *div64 = nullptr, *p64bak = nullptr;
   double* kappa = nullptr;  // mean curvature (surface tension)
+  unsigned char* fsfixed = nullptr;  // fast sweeping: cells the sweeps leave alone
+  int* fsflag = nullptr;             // fast sweeping: the reference's sort read its uninitialised a2
+  int sweep_direction = 0;           // LEVELSET_3D::sweep_direction
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
   unsigned short* pdinv = nullptr;  // bf16 1/diag: the Jacobi preconditioner of the FP32 pressure solve
@@ -353,6 +356,29 @@ fs_status advect_velocity_t(fs_ctx* c, double dt) {
 // One reinitialisation block from `in` into `out` (out may be `base`):
 // S from `in`, reinit_iterations pseudo-steps, the last one combined as
 // c0*base + c1*result.
+// Fast sweeping of `in` into `out` (EULERIAN_FLUID_SOLVER_3D.h:2202-2205:
+// LEVELSET_3D::ReinitializeByFastSweeping); direction < 0 takes the
+// context's counter and advances it.
+template <class S>
+fs_status fast_sweeping_t(fs_ctx* c, const void* in, void* out, int direction, int pairs) {
+  const bool typo = (c->prm.flags & FS_FLAG_SORT_TYPO) != 0;
+  if (direction < 0) direction = c->sweep_direction++;
+  if (typo) CK(cudaMemsetAsync(c->fsflag, 0, sizeof(int), c->stream));
+  c->launches += fast_sweeping<S>(F<S>(const_cast<void*>(in)), F<S>(out), c->fsfixed, c->Lc, c->grid.dx, direction,
+                                  pairs, typo ? 1 : 0, c->fsflag, c->stream);
+  CK(cudaGetLastError());
+  if (typo) {
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, c->fsflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (flag) {
+      set_error("the reference's sort reads its uninitialised a2 on this input (FS_FLAG_SORT_TYPO)");
+      return FS_NONFINITE;
+    }
+  }
+  return FS_OK;
+}
+
 template <class S>
 fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, double c1, void* scrA, void* scrB,
                          std::vector<double*>* tape = nullptr) {
@@ -360,6 +386,11 @@ fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, 
   const double dx = c->grid.dx, dtau = dx / P.reinit_scaling;
   const int n = P.reinit_iterations;
   cudaStream_t s = c->stream;
+  if (P.fast_sweeping) {
+    // the sweeps first, into scratch (in may be the RK base)
+    CKS(fast_sweeping_t<S>(c, in, scrA, -1, 1));
+    in = scrA;
+  }
   if (n == 0) {
     if (c0 != 0.0) { axpby<S>(F<S>(out), F<S>(base), F<S>(in), c0, c1, c->Lc, s); c->launches += 1; }
     else if (out != in) CK(cudaMemcpyAsync(out, in, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s));
@@ -928,6 +959,10 @@ fs_status adj_check(fs_ctx* c) {
     set_error("adjoints cover the WENO5 velocity advection only");
     return FS_NOT_SUPPORTED;
   }
+  if (c->prm.fast_sweeping) {
+    set_error("adjoints cover the Sussman reinitialisation only");
+    return FS_NOT_SUPPORTED;
+  }
   if (c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) {
     set_error("adjoints follow the corrected projection only");
     return FS_NOT_SUPPORTED;
@@ -1136,6 +1171,8 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   for (void** p : fw) if ((s = dalloc(c, p, wb)) != FS_OK) return fail(s);
   double** d8[] = {&c->p64, &c->b64, &c->div64, &c->kappa};
   for (double** p : d8) if ((s = dalloc(c, (void**)p, c8)) != FS_OK) return fail(s);
+  if ((s = dalloc(c, (void**)&c->fsfixed, c->Lc.total)) != FS_OK) return fail(s);
+  if ((s = dalloc(c, (void**)&c->fsflag, sizeof(int))) != FS_OK) return fail(s);
   if (c->fp32 && (s = dalloc(c, (void**)&c->p64bak, c8)) != FS_OK) return fail(s);
   void** pv[] = {&c->pax, &c->pay, &c->paz, &c->pdiag, &c->pr, &c->pp, &c->pq};
   for (void** p : pv) if ((s = dalloc(c, p, cv)) != FS_OK) return fail(s);
@@ -1412,6 +1449,20 @@ fs_status fs_reinitialize(fs_ctx* c) {
                         : reinit_block_t<double>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3);
   if (s != FS_OK) return s;
   if (c->prm.reinit_iterations > 0) std::swap(c->phi, c->s1);
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_fast_sweeping(fs_ctx* c, int direction, int pairs) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (direction < -1 || direction > 3 || pairs < 1 || pairs > 4) {
+    set_error("direction must be -1..3 and pairs 1..4");
+    return FS_INVALID_ARG;
+  }
+  fs_status s = c->fp32 ? fast_sweeping_t<float>(c, c->phi, c->s1, direction, pairs)
+                        : fast_sweeping_t<double>(c, c->phi, c->s1, direction, pairs);
+  if (s != FS_OK) return s;
+  std::swap(c->phi, c->s1);
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;
 }

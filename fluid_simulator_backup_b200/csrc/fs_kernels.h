@@ -19,6 +19,15 @@ template <class T>
 void eno3_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
               const Lay& Lw, int axis, double dx, double dt, cudaStream_t s);
 template <class T> void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s);
+// LEVELSET_3D::ReinitializeByFastSweeping from `in` into `out` (interior
+// and face ghosts; `in` is not written): the set-up, then `pairs` sweep
+// pairs starting at sweep direction `direction` (the reference runs one per
+// call).  typo: the reference's sort with its stale a2, sequentially;
+// *stale_read is set when that sort reads a2 before the sweep wrote it.
+// Returns the number of kernels launched.
+template <class T>
+int fast_sweeping(const T* in, T* out, unsigned char* fixed, const Lay& L, double dx, int direction, int pairs,
+                  int typo, int* stale_read, cudaStream_t s);
 template <class T>
 void sussman_step(const T* src, const T* sgn, const T* base, T* out, const Lay& L, double dx, double eps, double dtau,
                   double c0, double c1, int typo, cudaStream_t s);

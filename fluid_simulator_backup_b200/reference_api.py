@@ -124,7 +124,12 @@ def params_from_block(block, base_grid):
         rho_neg=neg[0], rho_pos=pos[0], mu_neg=neg[1], mu_pos=pos[1],
         gravity=block.GetVector3("gravity", (0.0, -9.8, 0.0)),
         weno_epsilon=adv.GetFloat("epsilon", 10e-6),
-        reinit_iterations=block.GetInteger("iteration_number_for_reinitialization", 10),
+        # EULERIAN_FLUID_SOLVER_3D.h:201-202, 2198-2225: Sussman pseudo-steps only
+        # with sussmanstyle_reinitialization, fast sweeping before them with
+        # fastsweeping_reinitialization (both default false)
+        reinit_iterations=(block.GetInteger("iteration_number_for_reinitialization", 10)
+                           if block.GetBoolean("sussmanstyle_reinitialization", False) else 0),
+        fast_sweeping=1 if block.GetBoolean("fastsweeping_reinitialization", False) else 0,
         reinit_scaling=block.GetInteger("scaling_number_for_reinitialization", 5),
         order=block.GetInteger("order_for_time_advancing", 1),
         precision=FS_PRECISION_FP32_REFINE if precision == "fp32_refine" else FS_PRECISION_FP64,

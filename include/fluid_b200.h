@@ -73,8 +73,10 @@ enum {
   FS_FLAG_FAITHFUL_PROJECTION = 1 << 0, /* only w corrected + first-cell bottom face quirk (PROJECTION_3D.h:1188-1407) */
   FS_FLAG_REINIT_TYPO = 1 << 1,         /* reproduce the two sqrt(a^2)+b^2 leaves (ADVECTION_METHOD_3D.h:1463,1605) */
   FS_FLAG_LEVELSET_FORWARD_EULER = 1 << 2, /* order 3 advances phi by one Euler step (EULERIAN_FLUID_SOLVER_3D.h:1010) */
-  FS_FLAG_CURVATURE_TYPO = 1 << 3  /* curvature as the reference computes it: factor 2 missing on py*pz*pyz and dz
+  FS_FLAG_CURVATURE_TYPO = 1 << 3, /* curvature as the reference computes it: factor 2 missing on py*pz*pyz and dz
                                       for 1/dz in the zero-gradient fallback (LEVELSET_3D.h:1033,1037) */
+  FS_FLAG_SORT_TYPO = 1 << 4       /* fast sweeping with the reference's INCREASING_SORT3, whose c < b < a branch
+                                      leaves a2 stale (MACROS.h:61-68); sweeps then run sequentially */
 };
 
 typedef struct {
@@ -105,6 +107,8 @@ typedef struct {
   double surface_tension;           /* sigma: the pressure jump sigma*kappa across the interface (0: none) */
   int velocity_scheme;              /* fs_velocity_scheme of the velocity self-advection */
   double velocity_epsilon;          /* VELOCITY_ADVECTION.epsilon of the WENO5 weights (0: weno_epsilon) */
+  int fast_sweeping;                /* fastsweeping_reinitialization: each reinitialisation block starts with
+                                       fs_fast_sweeping(ctx, -1, 1) (EULERIAN_FLUID_SOLVER_3D.h:2202-2205) */
 } fs_params;
 
 typedef struct {
@@ -172,6 +176,16 @@ fs_status fs_advect_levelset(fs_ctx* ctx, double dt);
 fs_status fs_advect_velocity(fs_ctx* ctx, double dt);
 /* One reinitialisation block (EULERIAN_FLUID_SOLVER_3D::Reinitialization, :2198). */
 fs_status fs_reinitialize(fs_ctx* ctx);
+/* LEVELSET_3D::ReinitializeByFastSweeping (LEVELSET_3D.h:601-610) on phi,
+ * without the closing normals and curvature: the set-up (cells beyond
+ * 20 dx and cells next to the interface fixed, the others reset to
+ * +-20 dx), then `pairs` pairs of Gauss-Seidel sweeps, the first in sweep
+ * direction `direction` (0..3; -1: the context's counter, which then
+ * advances by one as the reference's sweep_direction does).  pairs = 1 is
+ * the reference's call; pairs = 4 sweeps all eight octants after one
+ * set-up.  FS_NONFINITE with FS_FLAG_SORT_TYPO when the reference's sort
+ * reads its uninitialised a2 on this input. */
+fs_status fs_fast_sweeping(fs_ctx* ctx, int direction, int pairs);
 /* Semi-implicit viscosity of u, v, w (VISCOSITY_3D::ApplyViscosity, VISCOSITY_3D.h:448). */
 fs_status fs_viscosity(fs_ctx* ctx, double dt, int* iterations);
 

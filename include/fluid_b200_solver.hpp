@@ -318,7 +318,13 @@ inline fs_params params_from_block(const SCRIPT_BLOCK& block, const GRID_STRUCTU
   const double g_def[3] = {0.0, -9.8, 0.0};
   block.GetVector3("gravity", p.gravity, g_def);
   p.weno_epsilon = adv.GetFloat("epsilon", 10e-6);
-  p.reinit_iterations = block.GetInteger("iteration_number_for_reinitialization", 10);
+  // EULERIAN_FLUID_SOLVER_3D.h:201-202, 2198-2225: Sussman pseudo-steps only with
+  // sussmanstyle_reinitialization, fast sweeping before them with
+  // fastsweeping_reinitialization (both default false)
+  p.reinit_iterations = block.GetBoolean("sussmanstyle_reinitialization", false)
+                            ? block.GetInteger("iteration_number_for_reinitialization", 10)
+                            : 0;
+  p.fast_sweeping = block.GetBoolean("fastsweeping_reinitialization", false) ? 1 : 0;
   p.reinit_scaling = block.GetInteger("scaling_number_for_reinitialization", 5);
   p.order = block.GetInteger("order_for_time_advancing", 1);
   const std::string prec = block.GetString("precision", "fp64");

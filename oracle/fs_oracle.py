@@ -1072,17 +1072,28 @@ def step(phi, u, v, w, dx, dt, P, p0=None, order=3):
 
     base = (u, v, w)
     it, sc = P["reinit_iterations"], P["reinit_scaling"]
+    sweep = [P.get("sweep_direction", 0)]
+
+    def reinit(f):
+        # EULERIAN_FLUID_SOLVER_3D::Reinitialization: fast sweeping (its
+        # sweep_direction advancing per call), then the Sussman block
+        if P.get("fast_sweeping", False):
+            f = fast_sweeping(f, dx, sweep[0])
+            sweep[0] += 1
+        return reinitialization_block(f, dx, it, sc, eps) if it > 0 else f
+
     if order == 3:
         s1 = stage(base, 0.0, 1.0, base)
         s2 = stage(s1, 0.75, 0.25, base)
         s3 = stage(s2, 1.0 / 3.0, 2.0 / 3.0, base)
-        r1 = reinitialization_block(phin, dx, it, sc, eps)
-        r2 = 0.75 * phin + 0.25 * reinitialization_block(r1, dx, it, sc, eps)
-        phi_out = (1.0 / 3.0) * phin + (2.0 / 3.0) * reinitialization_block(r2, dx, it, sc, eps)
+        r1 = reinit(phin)
+        r2 = 0.75 * phin + 0.25 * reinit(r1)
+        phi_out = (1.0 / 3.0) * phin + (2.0 / 3.0) * reinit(r2)
     else:
         s3 = stage(base, 0.0, 1.0, base)
         if order == 2:
             s3 = stage(s3, 0.5, 0.5, base)
-        r1 = reinitialization_block(phin, dx, it, sc, eps)
-        phi_out = 0.5 * phin + 0.5 * reinitialization_block(r1, dx, it, sc, eps)
+        r1 = reinit(phin)
+        phi_out = 0.5 * phin + 0.5 * reinit(r1)
+    info["sweep_direction"] = sweep[0]
     return phi_out, s3[0], s3[1], s3[2], p, info

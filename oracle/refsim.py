@@ -81,7 +81,8 @@ def lib():
 def write_sim(path, n, *, water_drop=True, threads=1, tolerance=1e-10, max_iteration=100000,
               solver="PCG", reinit_iterations=10, reinit_scaling=5, epsilon=1e-6,
               water_density=1000.0, air_density=1.0, water_viscosity=1e-3, air_viscosity=1.8e-5,
-              gravity=(0.0, -9.8, 0.0), order=3, cfl=0.5, velocity_weno=True, surface_tension=0.0):
+              gravity=(0.0, -9.8, 0.0), order=3, cfl=0.5, velocity_weno=True, surface_tension=0.0,
+              fast_sweeping=False, sussman=True):
     """Write an air/water box scenario in the reference's .sim syntax."""
     hi = (n - 1) / n
     b = lambda v: "true" if v else "false"
@@ -137,8 +138,8 @@ FLUID_SOLVER_UNIFORM_AIR_WATER
 	is_external_force_active = true
 	is_sourcing_active = true
 	is_projection_active = true
-	fastsweeping_reinitialization = false
-	sussmanstyle_reinitialization = true
+	fastsweeping_reinitialization = {b(fast_sweeping)}
+	sussmanstyle_reinitialization = {b(sussman)}
 	scaling_number_for_reinitialization = {reinit_scaling}
 	iteration_number_for_reinitialization = {reinit_iterations}
 	use_delta_function_formulation = true

@@ -41,6 +41,7 @@ int main(int argc, char** argv) {
       std::printf("tol %.17g maxit %d stop %d order %d reinit %d %d cfl %.17g\n", p.tolerance, p.max_iteration,
                   p.stop, p.order, p.reinit_iterations, p.reinit_scaling, world.GetFloat("CFL", 0.5));
       std::printf("velocity_scheme %d velocity_epsilon %.17g\n", p.velocity_scheme, p.velocity_epsilon);
+      std::printf("fast_sweeping %d reinit_iterations %d\n", p.fast_sweeping, p.reinit_iterations);
       return 0;
     }
     if (mode == "csr" && argc >= 4) {
