@@ -39,7 +39,8 @@ EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", 
             "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc", "fs_adjoint_reset", "fs_adjoint_density_bars",
             "fs_step_adjoint", "fs_advect_levelset_adjoint", "fs_advect_velocity_adjoint", "fs_reinitialize_adjoint",
             "fs_viscosity_adjoint", "fs_project_adjoint", "fs_curvature", "fs_write_levelset", "fs_read_levelset",
-            "fs_write_state", "fs_read_state", "fs_fast_sweeping")
+            "fs_write_state", "fs_read_state", "fs_fast_sweeping", "fs_surface", "fs_surface_download",
+            "fs_write_obj")
 
 
 class FsError(RuntimeError):
@@ -124,6 +125,9 @@ def lib():
         L.fs_advect_velocity.argtypes = [vp, ctypes.c_double]
         L.fs_reinitialize.argtypes = [vp]
         L.fs_fast_sweeping.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.fs_surface.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+        L.fs_surface_download.argtypes = [vp, vp, vp, vp]
+        L.fs_write_obj.argtypes = [vp, ctypes.c_char_p]
         L.fs_viscosity.argtypes = [vp, ctypes.c_double, ip]
         L.fs_pcg_csr.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
                                  ctypes.c_int, ip, dp]
@@ -291,6 +295,23 @@ class Solver:
 
     def reinitialize(self):
         _check(lib().fs_reinitialize(self._h), "fs_reinitialize")
+
+    def surface(self):
+        """The zero level set as a closed triangle mesh (marching cubes):
+        vertices [nv, 3] (x, y, z), vertex normals [nv, 3], triangles
+        [nt, 3] of 1-based vertex numbers."""
+        nv, nt = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().fs_surface(self._h, ctypes.byref(nv), ctypes.byref(nt)), "fs_surface")
+        xyz = np.empty((nv.value, 3))
+        nrm = np.empty((nv.value, 3))
+        tri = np.empty((nt.value, 3), dtype=np.int32)
+        _check(lib().fs_surface_download(self._h, xyz.ctypes.data, nrm.ctypes.data, tri.ctypes.data),
+               "fs_surface_download")
+        return xyz, nrm, tri
+
+    def write_obj(self, path):
+        """The surface as a Wavefront OBJ file (WRITE_LEVELSET::WriteOBJ)."""
+        _check(lib().fs_write_obj(self._h, os.fsencode(path)), "fs_write_obj")
 
     def fast_sweeping(self, direction=-1, pairs=1):
         """LEVELSET_3D::ReinitializeByFastSweeping on phi (direction -1: the

@@ -83,6 +83,7 @@ struct fs_ctx {
   unsigned char* fsfixed = nullptr;  // fast sweeping: cells the sweeps leave alone
   int* fsflag = nullptr;             // fast sweeping: the reference's sort read its uninitialised a2
   int sweep_direction = 0;           // LEVELSET_3D::sweep_direction
+  SurfaceMesh mesh;                  // the last fs_surface
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
   unsigned short* pdinv = nullptr;  // bf16 1/diag: the Jacobi preconditioner of the FP32 pressure solve
@@ -159,6 +160,7 @@ void release(fs_ctx* c) {
   c->graphs.clear();
   for (auto& b : c->owned) cudaFree(b.p);
   c->owned.clear();
+  c->mesh.release();
   if (c->st_host) cudaFreeHost(c->st_host);
   if (c->sc_host) cudaFreeHost(c->sc_host);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1464,6 +1466,56 @@ fs_status fs_fast_sweeping(fs_ctx* c, int direction, int pairs) {
   if (s != FS_OK) return s;
   std::swap(c->phi, c->s1);
   CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
+fs_status fs_surface(fs_ctx* c, int64_t* n_vertices, int64_t* n_triangles) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  const cudaError_t e = c->fp32 ? polygonize<float>(F<float>(c->phi), c->Lc, c->grid.dx, &c->mesh, c->stream)
+                                : polygonize<double>(F<double>(c->phi), c->Lc, c->grid.dx, &c->mesh, c->stream);
+  if (e == cudaErrorInvalidValue) {
+    set_error("grid too large for the surface extraction's 32-bit vertex numbers");
+    return FS_INVALID_ARG;
+  }
+  if (e == cudaErrorMemoryAllocation) {
+    set_error("device memory for the surface mesh");
+    return FS_OOM;
+  }
+  CK(e);
+  c->launches += 9;
+  if (n_vertices) *n_vertices = c->mesh.nv;
+  if (n_triangles) *n_triangles = c->mesh.nt;
+  return FS_OK;
+}
+
+fs_status fs_surface_download(fs_ctx* c, double* xyz, double* normals, int32_t* triangles) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  const SurfaceMesh& m = c->mesh;
+  if (xyz && m.nv) CK(cudaMemcpy(xyz, m.xyz, m.nv * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (normals && m.nv) CK(cudaMemcpy(normals, m.normals, m.nv * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (triangles && m.nt) CK(cudaMemcpy(triangles, m.tri, m.nt * 3 * sizeof(int), cudaMemcpyDeviceToHost));
+  return FS_OK;
+}
+
+fs_status fs_write_obj(fs_ctx* c, const char* path) {
+  if (!c || !path) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  int64_t nv = 0, nt = 0;
+  CKS(fs_surface(c, &nv, &nt));
+  std::vector<double> xyz(3 * nv), nrm(3 * nv);
+  std::vector<int32_t> tri(3 * nt);
+  CKS(fs_surface_download(c, xyz.data(), nrm.data(), tri.data()));
+  FILE* f = std::fopen(path, "w");
+  if (!f) { set_error("cannot open %s", path); return FS_INVALID_ARG; }
+  bool ok = true;
+  for (int64_t v = 0; v < nv && ok; ++v)
+    ok = std::fprintf(f, "v %.9g %.9g %.9g\n", xyz[3 * v], xyz[3 * v + 1], xyz[3 * v + 2]) > 0;
+  for (int64_t v = 0; v < nv && ok; ++v)
+    ok = std::fprintf(f, "vn %.9g %.9g %.9g\n", nrm[3 * v], nrm[3 * v + 1], nrm[3 * v + 2]) > 0;
+  for (int64_t t = 0; t < nt && ok; ++t)
+    ok = std::fprintf(f, "f %d//%d %d//%d %d//%d\n", tri[3 * t], tri[3 * t], tri[3 * t + 1], tri[3 * t + 1],
+                      tri[3 * t + 2], tri[3 * t + 2]) > 0;
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) { set_error("writing %s failed", path); return FS_INVALID_ARG; }
   return FS_OK;
 }
 

@@ -19,6 +19,16 @@ template <class T>
 void eno3_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
               const Lay& Lw, int axis, double dx, double dt, cudaStream_t s);
 template <class T> void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s);
+// The zero level set as a triangle mesh in device memory (fs_surface.cu).
+struct SurfaceMesh {
+  double* xyz = nullptr;      // [nv][3]
+  double* normals = nullptr;  // [nv][3]
+  int* tri = nullptr;         // [nt][3], 1-based vertex numbers
+  int64_t nv = 0, nt = 0;
+  void release();
+};
+template <class T>
+cudaError_t polygonize(const T* phi, const Lay& L, double dx, SurfaceMesh* mesh, cudaStream_t s);
 // LEVELSET_3D::ReinitializeByFastSweeping from `in` into `out` (interior
 // and face ghosts; `in` is not written): the set-up, then `pairs` sweep
 // pairs starting at sweep direction `direction` (the reference runs one per

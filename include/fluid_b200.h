@@ -186,6 +186,20 @@ fs_status fs_reinitialize(fs_ctx* ctx);
  * set-up.  FS_NONFINITE with FS_FLAG_SORT_TYPO when the reference's sort
  * reads its uninitialised a2 on this input. */
 fs_status fs_fast_sweeping(fs_ctx* ctx, int direction, int pairs);
+
+/* The zero level set of phi as a closed triangle mesh: the surface that
+ * WRITE_LEVELSET::WriteOBJ writes (WRITE_LEVELSET.h:22-84), by marching
+ * cubes over the cells with corners sampled as the reference samples them
+ * (MARCHING_CUBES_ALGORITHM.h:146-166, 497-757).  Polygonises on the device
+ * and keeps the mesh in the context; returns its vertex and triangle
+ * counts. */
+fs_status fs_surface(fs_ctx* ctx, int64_t* n_vertices, int64_t* n_triangles);
+/* The mesh of the last fs_surface into host buffers sized from its counts:
+ * xyz [3 nv] and normals [3 nv] (x, y, z per vertex; either may be NULL),
+ * triangles [3 nt] with 1-based vertex numbers (may be NULL). */
+fs_status fs_surface_download(fs_ctx* ctx, double* xyz, double* normals, int32_t* triangles);
+/* fs_surface, then a Wavefront OBJ file: v and vn lines, faces "f a//a b//b c//c". */
+fs_status fs_write_obj(fs_ctx* ctx, const char* path);
 /* Semi-implicit viscosity of u, v, w (VISCOSITY_3D::ApplyViscosity, VISCOSITY_3D.h:448). */
 fs_status fs_viscosity(fs_ctx* ctx, double dt, int* iterations);
 

@@ -1097,3 +1097,207 @@ def step(phi, u, v, w, dx, dt, P, p0=None, order=3):
         phi_out = 0.5 * phin + 0.5 * reinit(r1)
     info["sweep_direction"] = sweep[0]
     return phi_out, s3[0], s3[1], s3[2], p, info
+
+
+# ----------------------------------------------------------------------------
+# Surface output: marching cubes (WRITE_LEVELSET.h:22-84,
+# MARCHING_CUBES_ALGORITHM.h:146-166, 497-757, FIELD_STRUCTURE_3D.h:225-251)
+# ----------------------------------------------------------------------------
+
+# Cube corners: bit 0 the x offset, bit 1 y, bit 2 z from the cube's low
+# corner.  Edges 0-3 run along x, 4-7 along y, 8-11 along z; faces list
+# their corners in cyclic order.
+MC_EDGES = ((0, 1), (2, 3), (4, 5), (6, 7), (0, 2), (1, 3), (4, 6), (5, 7), (0, 4), (1, 5), (2, 6), (3, 7))
+MC_FACES = ((0, 2, 6, 4), (1, 3, 7, 5), (0, 1, 5, 4), (2, 3, 7, 6), (0, 1, 3, 2), (4, 5, 7, 6))
+
+
+def marching_cubes_table():
+    """For each of the 256 inside/outside patterns of a cube (bit c set when
+    corner c has phi <= 0), the triangles as triples of cube edges.
+
+    The surface crosses each face along segments between its sign-changing
+    edges; a face whose diagonal corners share a sign (four crossings) cuts
+    off each inside corner, a rule that both cubes of the face apply alike,
+    so the mesh is closed.  The segments of the six faces close into loops,
+    each loop is fanned from its lowest edge.  The reference's own table
+    (MARCHING_CUBES_ALGORITHM_TABLE.h) gives the same crossings and the
+    same loops on the unambiguous patterns; its triangles differ."""
+    edge_of = {frozenset(e): k for k, e in enumerate(MC_EDGES)}
+    table = []
+    for mask in range(256):
+        inside = [(mask >> c) & 1 for c in range(8)]
+        partner = {}
+        for f in MC_FACES:
+            ring = [edge_of[frozenset((f[q], f[(q + 1) % 4]))] for q in range(4)]
+            active = [inside[f[q]] != inside[f[(q + 1) % 4]] for q in range(4)]
+            if sum(active) == 2:
+                segs = [tuple(ring[q] for q in range(4) if active[q])]
+            elif sum(active) == 4:
+                segs = [(ring[(q - 1) % 4], ring[q]) for q in range(4) if inside[f[q]]]
+            else:
+                segs = []
+            for a, b in segs:
+                partner.setdefault(a, []).append(b)
+                partner.setdefault(b, []).append(a)
+        tris, seen = [], set()
+        for start in sorted(partner):
+            if start in seen:
+                continue
+            loop, prev, cur = [start], None, start
+            seen.add(start)
+            while True:
+                a, b = partner[cur]
+                nxt = b if a == prev else a
+                if nxt == start:
+                    break
+                loop.append(nxt)
+                seen.add(nxt)
+                prev, cur = cur, nxt
+            tris += [(loop[0], loop[q], loop[q + 1]) for q in range(1, len(loop) - 1)]
+        table.append(tris)
+    return table
+
+
+def mc_node_coordinate(I, n, dx):
+    """A cube corner's coordinate along one axis as the reference forms it
+    (MARCHING_CUBES_ALGORITHM.h:151-166): the centre of cube i = min(I, n-1)
+    from the domain's low end 0, then -+ half a cell."""
+    half = dx * 0.5
+    i = min(I, n - 1)
+    centre = (0.0 + half) + dx * float(i)
+    return centre - half if I < n else centre + half
+
+
+def mc_node_values(phi, dx):
+    """phi at the cube corners: FIELD_STRUCTURE_3D::TriLinearInterpolation
+    (FIELD_STRUCTURE_3D.h:225-251) with its indices clamped to the cells
+    (the reference reads copied ghosts there), and phi == 0 moved to -1e-8
+    (MARCHING_CUBES_ALGORITHM.h:308).  Returns the values [nz+1, ny+1, nx+1]
+    and the corner coordinates per axis."""
+    nz, ny, nx = phi.shape
+    inv = 1.0 / dx
+    xs = [mc_node_coordinate(I, nx, dx) for I in range(nx + 1)]
+    ys = [mc_node_coordinate(J, ny, dx) for J in range(ny + 1)]
+    zs = [mc_node_coordinate(K, nz, dx) for K in range(nz + 1)]
+
+    def axis(pos, n):
+        i0 = math.floor((pos - 0.0) * inv - 0.5)
+        a = (pos - (0.0 + (0.5 + float(i0)) * dx)) * inv
+        return min(max(i0, 0), n - 1), min(max(i0 + 1, 0), n - 1), a
+
+    ax = [axis(p, nx) for p in xs]
+    ay = [axis(p, ny) for p in ys]
+    az = [axis(p, nz) for p in zs]
+    f = phi.tolist()
+    out = np.empty((nz + 1, ny + 1, nx + 1))
+    for K, (k0, k1, c) in enumerate(az):
+        for J, (j0, j1, b) in enumerate(ay):
+            mamb_rows = None
+            for I, (i0, i1, a) in enumerate(ax):
+                v000, v100, v010, v001 = f[k0][j0][i0], f[k0][j0][i1], f[k0][j1][i0], f[k1][j0][i0]
+                v110, v101, v011, v111 = f[k0][j1][i1], f[k1][j0][i1], f[k1][j1][i0], f[k1][j1][i1]
+                mamb = (1.0 - a) * (1.0 - b)
+                bc = b * c
+                val = (v000 * (mamb * (1.0 - c)) + (a * (1.0 - b) * (1.0 - c)) * v100 + ((1.0 - a) * b * (1.0 - c)) * v010
+                       + (mamb * c) * v001 + (a * b * (1.0 - c)) * v110 + (a * (1.0 - b) * c) * v101
+                       + ((1.0 - a) * bc) * v011 + (a * bc) * v111)
+                out[K, J, I] = -1e-8 if val == 0.0 else val
+    return out, (np.array(xs), np.array(ys), np.array(zs))
+
+
+def marching_cubes(phi, dx, table=None):
+    """The zero level set as a closed triangle mesh, the form
+    WRITE_LEVELSET::WriteOBJ writes: cube corners sampled as in
+    mc_node_values; cubes with a corner at 4 dx or more skipped
+    (MARCHING_CUBES_ALGORITHM.h:310-316); one vertex per crossed edge used by
+    a kept cube, at (|phi1| P0 + |phi0| P1) * (1/(|phi0| + |phi1|)) (the
+    reference's expression, VECTOR_3D.h:130-135 dividing by a reciprocal);
+    triangles from marching_cubes_table, each turned so its normal
+    (v1 - v0) x (v2 - v0) has a non-negative dot product with the gradient
+    of the cube's trilinear phi at its centre; vertex normals the
+    normalised sum of the unit normals of their triangles
+    (VERTEX::DetermineNormal, TRIANGULAR_SURFACE.cpp:99-121).
+
+    Vertices are numbered by edge: all x edges, then y, then z edges, each
+    set in (k, j, i) order; triangles by cube in (k, j, i) order.  Returns
+    (vertices [nv, 3] as (x, y, z), normals [nv, 3], triangles [nt, 3] with
+    1-based vertex numbers)."""
+    if table is None:
+        table = marching_cubes_table()
+    nz, ny, nx = phi.shape
+    node, (xs, ys, zs) = mc_node_values(phi, dx)
+    big = 4.0 * dx
+    kept = np.ones((nz, ny, nx), dtype=bool)
+    for dk in (0, 1):
+        for dj in (0, 1):
+            for di in (0, 1):
+                kept &= node[dk:nz + dk, dj:ny + dj, di:nx + di] < big
+    neg = node <= 0.0
+    # edges: x edges [nz+1, ny+1, nx], y [nz+1, ny, nx+1], z [nz, ny+1, nx+1]
+    cross = [neg[:, :, 1:] != neg[:, :, :-1], neg[:, 1:, :] != neg[:, :-1, :], neg[1:, :, :] != neg[:-1, :, :]]
+    usedc = [np.zeros_like(c) for c in cross]
+    for dk in (0, 1):
+        for dj in (0, 1):
+            # cubes touching x edge (k, j, i): cube (k-dk, j-dj, i)
+            u = usedc[0]
+            sub = np.zeros_like(u)
+            sub[dk:dk + nz, dj:dj + ny, :] |= kept
+            u |= sub
+            sub = np.zeros_like(usedc[1])
+            sub[dk:dk + nz, :, dj:dj + nx] |= kept
+            usedc[1] |= sub
+            sub = np.zeros_like(usedc[2])
+            sub[:, dk:dk + ny, dj:dj + nx] |= kept
+            usedc[2] |= sub
+    used = [c & u for c, u in zip(cross, usedc)]
+    ids, verts, base = [], [], 0
+    for axis, u in enumerate(used):
+        idx = np.full(u.shape, -1, dtype=np.int64)
+        n = int(u.sum())
+        idx[u] = base + np.arange(n)
+        ids.append(idx)
+        for (k, j, i) in zip(*np.nonzero(u)):
+            k0, j0, i0 = k, j, i
+            k1, j1, i1 = k + (axis == 2), j + (axis == 1), i + (axis == 0)
+            p0, p1 = node[k0, j0, i0], node[k1, j1, i1]
+            a0, a1 = (p0 if p0 > 0 else -p0), (p1 if p1 > 0 else -p1)
+            inv = 1.0 / (a0 + a1)
+            P0 = (xs[i0], ys[j0], zs[k0])
+            P1 = (xs[i1], ys[j1], zs[k1])
+            verts.append([(a1 * P0[q] + a0 * P1[q]) * inv for q in range(3)])
+        base += n
+    verts = np.array(verts, dtype=float).reshape(-1, 3)
+
+    def edge_vertex(e, k, j, i):
+        c0, c1 = MC_EDGES[e]
+        kk, jj, ii = k + (c0 >> 2 & 1), j + (c0 >> 1 & 1), i + (c0 & 1)
+        return int(ids[0 if e < 4 else (1 if e < 8 else 2)][kk, jj, ii])
+
+    tris = []
+    for (k, j, i) in zip(*np.nonzero(kept)):
+        c = [node[k + (q >> 2 & 1), j + (q >> 1 & 1), i + (q & 1)] for q in range(8)]
+        mask = sum(1 << q for q in range(8) if c[q] <= 0.0)
+        if not table[mask]:
+            continue
+        g = np.array([((c[1] + c[3]) + (c[5] + c[7])) - ((c[0] + c[2]) + (c[4] + c[6])),
+                      ((c[2] + c[3]) + (c[6] + c[7])) - ((c[0] + c[1]) + (c[4] + c[5])),
+                      ((c[4] + c[5]) + (c[6] + c[7])) - ((c[0] + c[1]) + (c[2] + c[3]))])
+        for (e0, e1, e2) in table[mask]:
+            v0, v1, v2 = edge_vertex(e0, k, j, i), edge_vertex(e1, k, j, i), edge_vertex(e2, k, j, i)
+            P0, P1, P2 = verts[v0], verts[v1], verts[v2]
+            nrm = np.cross(P1 - P0, P2 - P0)
+            if nrm[0] * g[0] + nrm[1] * g[1] + nrm[2] * g[2] < 0.0:
+                v1, v2 = v2, v1
+            tris.append((v0, v1, v2))
+    tris = np.array(tris, dtype=np.int64).reshape(-1, 3)
+    normals = np.zeros_like(verts)
+    if len(tris):
+        P = verts[tris]
+        fn = np.cross(P[:, 1] - P[:, 0], P[:, 2] - P[:, 0])
+        ln = np.linalg.norm(fn, axis=1)
+        fn = np.where(ln[:, None] > 0, fn / np.where(ln > 0, ln, 1.0)[:, None], 0.0)
+        for q in range(3):
+            np.add.at(normals, tris[:, q], fn)
+        ln = np.linalg.norm(normals, axis=1)
+        normals = np.where(ln[:, None] > 0, normals / np.where(ln > 0, ln, 1.0)[:, None], 0.0)
+    return verts, normals, tris + 1

@@ -40,6 +40,14 @@ EDITS = [
     ("SCRIPT_READER.cpp", "values.swap(vector<SCRIPT_VALUE*>());", "vector<SCRIPT_VALUE*>().swap(values);", 1),
     ("TRIANGULAR_SURFACE.cpp", "if(ist == NULL)", "if(ist.fail())", 1),
     ("TRIANGULAR_SURFACE.cpp", "if(file == 0)", "if(file.fail())", 1),
+    # std::thread passes its arguments as rvalues, which GCC will not bind to
+    # the int& thread ids of the polygonizer's thread functions (MSVC does)
+    ("MARCHING_CUBES_ALGORITHM.h", "void PolygonizeThread(int& thread_id, LEVELSET_OBJECT* levelset)",
+     "void PolygonizeThread(int thread_id, LEVELSET_OBJECT* levelset)", 1),
+    ("MARCHING_CUBES_ALGORITHM.h", "void PolygonizeUseFillGhostCellsFromThread(int& thread_id, LEVELSET_3D* levelset)",
+     "void PolygonizeUseFillGhostCellsFromThread(int thread_id, LEVELSET_3D* levelset)", 1),
+    ("MARCHING_CUBES_ALGORITHM.h", "void PolygonizeThreadPeriodic(int& thread_id, LEVELSET_OBJECT* levelset",
+     "void PolygonizeThreadPeriodic(int thread_id, LEVELSET_OBJECT* levelset", 1),
 ]
 
 

@@ -18,6 +18,7 @@
 #include <thread>
 #include <vector>
 
+#include "MARCHING_CUBES_ALGORITHM.h"
 #include "SIMULATION_WORLD.h"
 
 namespace {
@@ -317,6 +318,43 @@ void fsref_fast_sweeping(void* h, int direction) {
     ls.FillGhostCellsFrom(t, ls.phi, false);
     ls.FastSweepingMethod(t);
   });
+}
+
+// The level set's surface as WRITE_LEVELSET::WriteOBJ makes it
+// (WRITE_LEVELSET.h:22-84): LEVELSET_3D::ComputeNormals (its UnitNormal
+// orients the triangles), then MARCHING_CUBES_ALGORITHM::Polygonize.  Fills
+// at most cap_v vertices (position xyz, normal nrm) and cap_t triangles
+// (the OBJ's 1-based vertex indices); returns the vertex count and sets
+// *ntri to the triangle count.
+int fsref_marching_cubes(void* h, double* xyz, double* nrm, int cap_v, int* tri, int cap_t, int* ntri) {
+  RefCase* c = static_cast<RefCase*>(h);
+  LEVELSET_3D& ls = *c->world.eulerian_solver.water_levelset;
+  run_threads(c, [&](int t) { ls.ComputeNormals(t); });
+  MARCHING_CUBES_ALGORITHM mc;
+  mc.Initialize(ls.multithreading, ls.grid);
+  mc.Polygonize(static_cast<LEVELSET_OBJECT&>(ls));
+  int nv = 0, nt = 0;
+  for (int s = 0; s < mc.surfaces.num_elements; ++s) {
+    TRIANGULAR_SURFACE* surf = mc.surfaces.values[s];
+    for (VERTEX* v : surf->vertices) {
+      if (nv < cap_v)
+        for (int a = 0; a < 3; ++a) {
+          xyz[3 * nv + a] = v->x[a];
+          nrm[3 * nv + a] = v->n[a];
+        }
+      ++nv;
+    }
+  }
+  for (int s = 0; s < mc.surfaces.num_elements; ++s) {
+    TRIANGULAR_SURFACE* surf = mc.surfaces.values[s];
+    for (TRIANGLE* t : surf->triangles) {
+      if (nt < cap_t)
+        for (int a = 0; a < 3; ++a) tri[3 * nt + a] = t->vertices[a]->index;
+      ++nt;
+    }
+  }
+  *ntri = nt;
+  return nv;
 }
 
 void fsref_write_levelset(void* h, const char* path) {

@@ -63,6 +63,8 @@ def _lib():
     lib.fsref_write_levelset.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
     lib.fsref_eno3_velocity.argtypes = [ctypes.c_void_p, ctypes.c_double]
     lib.fsref_fast_sweeping.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.fsref_marching_cubes.restype = ctypes.c_int
+    lib.fsref_marching_cubes.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip]
     lib.fsref_linear_solve.restype = ctypes.c_int
     lib.fsref_linear_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _dp, _dp]
     return lib
@@ -299,6 +301,18 @@ class RefCase:
         """LEVELSET_3D::ReinitializeByFastSweeping (without its Update) with
         sweep_direction = direction, on the injected level set."""
         return self._quiet(self._lib.fsref_fast_sweeping, self.h, int(direction))
+
+    def marching_cubes(self, cap=200000):
+        """WRITE_LEVELSET::WriteOBJ's surface of the injected level set:
+        (vertices [nv, 3], vertex normals [nv, 3], triangles [nt, 3] of 1-based
+        vertex indices)."""
+        xyz = np.zeros((cap, 3)); nrm = np.zeros((cap, 3)); tri = np.zeros((cap, 3), np.int32)
+        nt = ctypes.c_int()
+        nv = self._quiet(self._lib.fsref_marching_cubes, self.h, _ptr(xyz), _ptr(nrm), cap, _ptr(tri, ctypes.c_int),
+                         cap, ctypes.byref(nt))
+        if nv > cap or nt.value > cap:
+            raise ValueError("surface larger than the buffers")
+        return xyz[:nv].copy(), nrm[:nv].copy(), tri[:nt.value].copy()
 
     def write_levelset(self, path):
         """LEVELSET_3D::Write of the current level set to `path`."""

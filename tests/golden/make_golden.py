@@ -25,6 +25,10 @@ on the air/water unit-cube box with Neumann pressure walls:
                    noisy sphere, sweep_direction 0 and 3; inputs whose sort
                    never reads the uninitialised a2 of INCREASING_SORT3's
                    typo branch (checked with the oracle)
+  surface_*        MARCHING_CUBES_ALGORITHM::Polygonize as WRITE_LEVELSET::
+                   WriteOBJ runs it (after ComputeNormals): vertices, vertex
+                   normals, triangles (1-based) of a sphere (16^3) and a
+                   noisy scaled sphere (24^3)
 """
 import os
 import sys
@@ -200,6 +204,16 @@ def main():
         outs[f"out_{direction}"] = c.get("phi")
     fixtures["fast_sweeping"] = dict(n=n, dx=c.dx, phi=phi, **outs)
     c.close()
+
+    # the level set's surface as the OBJ writer makes it
+    for name, n, scale, noise in (("surface_sphere", 16, 1.0, 0.0), ("surface_noisy", 24, 1.3, 0.002)):
+        c = case(n, water_drop=False)
+        srng = np.random.default_rng(1)
+        phi = sphere(n, (0.5, 0.45, 0.5), 0.3) * scale + srng.normal(size=(n, n, n)) * noise
+        c.set("phi", phi)
+        xyz, nrm, tri = c.marching_cubes()
+        fixtures[name] = dict(n=n, dx=c.dx, phi=phi, xyz=xyz, normals=nrm, tri=tri)
+        c.close()
 
     for name, d in fixtures.items():
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **{k: np.asarray(v) for k, v in d.items()})
