@@ -229,7 +229,34 @@ class EULERIAN_FLUID_SOLVER_3D:
         SIMULATION_WORLD)."""
         return self.solver.cfl_dt() / self.solver.params.cfl
 
+    # level set ----------------------------------------------------------------
+    def ReinitializeByFastSweeping(self, thread_id):
+        """water_levelset->ReinitializeByFastSweeping (LEVELSET_3D.h:601): the
+        solver's sweep direction, which then advances."""
+        if thread_id == 0:
+            self.solver.fast_sweeping(-1, 1)
+
+    def FullFastSweepingMethodThreaded(self, corrected=False):
+        """LEVELSET_3D.h:828-835: four calls in sweep directions 0..3, each
+        from its own set-up; corrected: one set-up, then all eight sweeps."""
+        if corrected:
+            self.solver.fast_sweeping(0, 4)
+        else:
+            for d in range(4):
+                self.solver.fast_sweeping(d, 1)
+
+
+class WRITE_LEVELSET:
+    """WRITE_LEVELSET (WRITE_LEVELSET.h:8-84) over a solver mirror: the water
+    level set's surface as an OBJ file named by the caller."""
+
+    def __init__(self, solver):
+        self.solver = solver
+
+    def WriteOBJ(self, path):
+        self.solver.solver.write_obj(path)
+
 
 __all__ = ["GRID_STRUCTURE_3D", "CSR_MATRIX", "LINEAR_SOLVER", "CUDA_PCG_METHOD", "PROJECTION_3D",
-           "EULERIAN_FLUID_SOLVER_3D", "params_from_block", "SCRIPT_BLOCK", "SCRIPT_READER", "FsError",
+           "EULERIAN_FLUID_SOLVER_3D", "WRITE_LEVELSET", "params_from_block", "SCRIPT_BLOCK", "SCRIPT_READER", "FsError",
            "FS_PRECISION_FP64"]

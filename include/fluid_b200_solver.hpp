@@ -455,9 +455,40 @@ class EULERIAN_FLUID_SOLVER_3D {  // EULERIAN_FLUID_SOLVER_3D.h
   double CFL() const { return params_.cfl; }
   fs_ctx* context() const { return ctx_; }
 
+  // water_levelset->ReinitializeByFastSweeping (LEVELSET_3D.h:601): the
+  // context's sweep direction, which then advances
+  void ReinitializeByFastSweeping(const int& thread_id) {
+    if (thread_id != 0) return;
+    check(fs_fast_sweeping(ctx_, -1, 1), "fs_fast_sweeping");
+  }
+  // water_levelset->FullFastSweepingMethodThreaded (LEVELSET_3D.h:828-835):
+  // four calls in sweep directions 0..3, each starting from its own set-up
+  // (corrected = true: one set-up, then all eight sweeps)
+  void FullFastSweepingMethodThreaded(bool corrected = false) {
+    if (corrected) {
+      check(fs_fast_sweeping(ctx_, 0, 4), "fs_fast_sweeping");
+      return;
+    }
+    for (int d = 0; d < 4; ++d) check(fs_fast_sweeping(ctx_, d, 1), "fs_fast_sweeping");
+  }
+
  private:
   fs_ctx* ctx_ = nullptr;
   fs_params params_{};
+};
+
+// WRITE_LEVELSET (WRITE_LEVELSET.h:8-84): the water level set's surface as
+// an OBJ file; the caller names the file (the reference derives it from the
+// frame number and its output directory).
+class WRITE_LEVELSET {
+ public:
+  explicit WRITE_LEVELSET(const EULERIAN_FLUID_SOLVER_3D& solver) : solver_(solver) {}
+  void WriteOBJ(const std::string& path) const {
+    check(fs_write_obj(solver_.context(), path.c_str()), "fs_write_obj");
+  }
+
+ private:
+  const EULERIAN_FLUID_SOLVER_3D& solver_;
 };
 
 inline std::vector<double> PROJECTION_3D::download(int field) const {

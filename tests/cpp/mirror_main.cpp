@@ -83,6 +83,21 @@ int main(int argc, char** argv) {
       std::printf("dt %.17g pcg %d status %d\n", dt, s.last_report.pcg_iterations, (int)s.last_status);
       return 0;
     }
+    if (mode == "levelset" && argc >= 6) {
+      // levelset <sim> <phi.bin> <phi_out.bin> <surface.obj>: the reference's
+      // full fast sweeping, then the OBJ writer
+      EULERIAN_FLUID_SOLVER_3D s;
+      s.InitializeFromScript(argv[2]);
+      std::ifstream f(argv[3], std::ios::binary);
+      s.SetField(FS_FIELD_PHI, read_vec<double>(f, (size_t)s.Count(FS_FIELD_PHI)));
+      s.FullFastSweepingMethodThreaded();
+      s.ReinitializeByFastSweeping(1);  // not the head thread: no work
+      std::ofstream o(argv[4], std::ios::binary);
+      write_vec(o, s.GetField(FS_FIELD_PHI));
+      WRITE_LEVELSET(s).WriteOBJ(argv[5]);
+      std::printf("ok\n");
+      return 0;
+    }
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());
     return 1;

@@ -107,3 +107,31 @@ def test_cpp_solver_steps_like_the_python_mirror(mirror, tmp_path):
     s.solver.close()
     assert int(res[5]) in (fs.FS_OK, fs.FS_NOT_CONVERGED)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_cpp_levelset_mirror_sweeps_and_writes_obj_like_python(mirror, tmp_path):
+    """FullFastSweepingMethodThreaded and WRITE_LEVELSET::WriteOBJ through the
+    C++ mirror give the Python mirror's level set and the same OBJ bytes."""
+    from fluid_simulator_backup_b200.reference_api import WRITE_LEVELSET
+    n = 16
+    path = write_script(str(tmp_path / "ls.sim"), n)
+    x = (np.arange(n) + 0.5) / n
+    phi = 1.4 * (np.sqrt((x[None, None, :] - 0.5) ** 2 + (x[None, :, None] - 0.4) ** 2
+                         + (x[:, None, None] - 0.5) ** 2) - 0.25)
+    phi_in = tmp_path / "phi.bin"
+    phi.astype(np.float64).tofile(phi_in)
+    out_phi, out_obj = tmp_path / "phi_out.bin", tmp_path / "cpp.obj"
+    subprocess.run([mirror, "levelset", path, str(phi_in), str(out_phi), str(out_obj)], check=True,
+                   capture_output=True, text=True)
+    s = EULERIAN_FLUID_SOLVER_3D.FromScript(path)
+    s.water_levelset = phi
+    s.FullFastSweepingMethodThreaded()
+    py_obj = tmp_path / "py.obj"
+    WRITE_LEVELSET(s).WriteOBJ(str(py_obj))
+    want = s.water_levelset
+    s.solver.close()
+    assert np.array_equal(np.fromfile(out_phi, np.float64).reshape(n, n, n), want)
+    assert open(out_obj).read() == open(py_obj).read()
+    from oracle import fs_oracle as O
+    assert np.array_equal(want, O.fast_sweeping(phi, s.base_grid.dx, 3))  # each call starts from its own set-up
