@@ -15,7 +15,7 @@
 //   normals    the normalised sum of the unit normals of a vertex's triangles
 // Every stage uses correctly rounded operations without contraction, so the
 // vertices and triangles are the bits of the CPU restatement of the same
-// rules; vertex normals sum with atomics (order-dependent last bits).
+// rules; vertex normals sum in fixed point, independent of the order.
 //
 // The triangle table is built here from the pattern, not copied: the surface
 // crosses each face along segments between its sign-changing edges (a face
@@ -306,9 +306,13 @@ __global__ void k_mc_triangles(const double* __restrict__ node, const int* __res
 }
 
 // VERTEX::DetermineNormal (TRIANGULAR_SURFACE.cpp:99-121): the unit normals
-// of a vertex's triangles, summed, then normalised.
+// of a vertex's triangles, summed, then normalised.  The sums are taken in
+// 2^-40 fixed point with 64-bit integer atomics: integer addition does not
+// depend on the order the triangles arrive in, so the normals (and the OBJ
+// text) are the same from run to run; the quantisation is below 1e-12.
+constexpr double kNormalScale = 1099511627776.0;  // 2^40
 __global__ void k_mc_face_normals(const int* __restrict__ tri, int64_t nt, const double* __restrict__ xyz,
-                                  double* __restrict__ nrm) {
+                                  unsigned long long* __restrict__ acc) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   const int a = tri[3 * t] - 1, b = tri[3 * t + 1] - 1, c = tri[3 * t + 2] - 1;
@@ -318,23 +322,23 @@ __global__ void k_mc_face_normals(const int* __restrict__ tri, int64_t nt, const
   if (!(len > 0.0)) return;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
-    const double u = n[q] / len;
-    atomicAdd(nrm + 3 * (int64_t)a + q, u);
-    atomicAdd(nrm + 3 * (int64_t)b + q, u);
-    atomicAdd(nrm + 3 * (int64_t)c + q, u);
+    // two's complement: adding the unsigned image of a negative count subtracts it
+    const unsigned long long u = (unsigned long long)__double2ll_rn(n[q] / len * kNormalScale);
+    atomicAdd(acc + 3 * (int64_t)a + q, u);
+    atomicAdd(acc + 3 * (int64_t)b + q, u);
+    atomicAdd(acc + 3 * (int64_t)c + q, u);
   }
 }
 
-__global__ void k_mc_normalize(double* __restrict__ nrm, int64_t nv) {
+__global__ void k_mc_normalize(const unsigned long long* __restrict__ acc, double* __restrict__ nrm, int64_t nv) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
-  double* n = nrm + 3 * v;
+  double n[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) n[q] = (double)(long long)acc[3 * v + q] / kNormalScale;
   const double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-  if (len > 0.0) {
-    n[0] /= len;
-    n[1] /= len;
-    n[2] /= len;
-  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) nrm[3 * v + q] = len > 0.0 ? n[q] / len : 0.0;
 }
 
 bool g_table_ready = false;
@@ -379,6 +383,7 @@ cudaError_t polygonize(const T* phi, const Lay& L, double dx, SurfaceMesh* mesh,
   if (nedge > 0x7fffffff) return cudaErrorInvalidValue;  // 32-bit scans and vertex numbers
   double* node = nullptr;
   int *pattern = nullptr, *count = nullptr, *toff = nullptr, *used = nullptr, *vid = nullptr;
+  unsigned long long* nacc = nullptr;
   auto cleanup = [&] {
     cudaFree(node);
     cudaFree(pattern);
@@ -386,6 +391,7 @@ cudaError_t polygonize(const T* phi, const Lay& L, double dx, SurfaceMesh* mesh,
     cudaFree(toff);
     cudaFree(used);
     cudaFree(vid);
+    cudaFree(nacc);
   };
 #define MC_TRY(x)             \
   do {                        \
@@ -424,9 +430,10 @@ cudaError_t polygonize(const T* phi, const Lay& L, double dx, SurfaceMesh* mesh,
   }
   k_mc_triangles<<<dim3((L.nx + 31) / 32, (L.ny + 7) / 8, L.nz), b, 0, s>>>(node, pattern, toff, vid, mesh->xyz, G,
                                                                           mesh->tri);
-  MC_TRY(cudaMemsetAsync(mesh->normals, 0, std::max<int64_t>(nv, 1) * 3 * sizeof(double), s));
-  if (nt > 0) k_mc_face_normals<<<(int)((nt + 255) / 256), 256, 0, s>>>(mesh->tri, nt, mesh->xyz, mesh->normals);
-  if (nv > 0) k_mc_normalize<<<(int)((nv + 255) / 256), 256, 0, s>>>(mesh->normals, nv);
+  MC_TRY(cudaMalloc(&nacc, std::max<int64_t>(nv, 1) * 3 * sizeof(unsigned long long)));
+  MC_TRY(cudaMemsetAsync(nacc, 0, std::max<int64_t>(nv, 1) * 3 * sizeof(unsigned long long), s));
+  if (nt > 0) k_mc_face_normals<<<(int)((nt + 255) / 256), 256, 0, s>>>(mesh->tri, nt, mesh->xyz, nacc);
+  if (nv > 0) k_mc_normalize<<<(int)((nv + 255) / 256), 256, 0, s>>>(nacc, mesh->normals, nv);
   MC_TRY(cudaGetLastError());
   MC_TRY(cudaStreamSynchronize(s));
   cleanup();
