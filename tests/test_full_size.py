@@ -1,0 +1,158 @@
+"""The benchmark scenes at their full sizes, checked through properties that
+do not depend on the size (the oracle is too slow there):
+
+- 64^3 dam break, FP64, 100 steps: every projection converges to the 1e-8
+  relative residual, the water volume stays within 5 % and the flow stays
+  bounded;
+- 128^3 dam break: FP64 and FP32+refine from the same state reach the same
+  1e-6 relative residual, pressures within 1e-2 and level sets within 1e-4
+  after two steps (the differences are printed);
+- 256^3 rising bubble, FP32+refine: one step converges and keeps the bubble
+  volume;
+- 512^3 oil/water Rayleigh-Taylor (134 M cells), FP32+refine with
+  semi-implicit viscosity: one step converges, fits the device with room to
+  spare, and keeps the oil volume.
+
+Volumes are sum H(-phi) dx^3 with the reference's smeared Heaviside,
+eps = 1.5 dx (EULERIAN_FLUID_SOLVER_3D.h:2459-2479)."""
+import math
+
+import numpy as np
+import pytest
+
+import fluid_simulator_backup_b200 as fs
+
+pytestmark = pytest.mark.gpu
+
+
+def heaviside_volume(phi, dx):
+    eps = 1.5 * dx
+    x = -phi
+    h = np.where(x < -eps, 0.0, np.where(x > eps, 1.0, 0.5 + x / (2 * eps) + np.sin(np.pi * x / eps) / (2 * np.pi)))
+    return float(h.sum()) * dx ** 3
+
+
+def axes(n):
+    x = (np.arange(n) + 0.5) / n
+    return x[None, None, :], x[None, :, None], x[:, None, None]
+
+
+def dam_break(n):
+    """Signed distance to the water box [0,0.4] x [0,0.6] x [0,1], negative inside."""
+    x, y, z = axes(n)
+    lo, hi = np.array([0.0, 0.0, 0.0]), np.array([0.4, 0.6, 1.0])
+    d = [np.maximum(lo[a] - c, c - hi[a]) for a, c in enumerate((x, y, z))]
+    d = np.broadcast_arrays(*d)
+    outside = np.sqrt(sum(np.maximum(q, 0.0) ** 2 for q in d))
+    inside = np.minimum(np.maximum(np.maximum(d[0], d[1]), d[2]), 0.0)
+    return outside + inside
+
+
+def water_params(precision, tol):
+    return dict(rho_neg=1000.0, rho_pos=1.0, mu_neg=1e-3, mu_pos=1.8e-5, precision=precision, tolerance=tol,
+                stop=fs.FS_STOP_RELATIVE, max_iteration=20000, cfl=0.5, order=3)
+
+
+def zero_velocity(s, n):
+    s.upload("u", np.zeros((n, n, n + 1)))
+    s.upload("v", np.zeros((n, n + 1, n)))
+    s.upload("w", np.zeros((n + 1, n, n)))
+
+
+def test_dam_break_64_fp64_100_steps():
+    n = 64
+    dx = 1.0 / n
+    phi = dam_break(n)
+    v0 = heaviside_volume(phi, dx)
+    with fs.Solver(n, dx, **water_params(fs.FS_PRECISION_FP64, 1e-8)) as s:
+        s.upload("phi", phi)
+        zero_velocity(s, n)
+        for _ in range(100):
+            rep = s.step(s.cfl_dt())
+            assert rep["status"] == fs.FS_OK and rep["max_rel_residual"] <= 1e-8
+        phi_t = s.download("phi")
+        umax = max(np.abs(s.download(k)).max() for k in "uvw")
+    drift = heaviside_volume(phi_t, dx) / v0 - 1
+    print(f"64^3 dam break, 100 steps: water volume drift {drift:+.3e}, max |u| {umax:.3f}")
+    assert np.isfinite(phi_t).all()
+    assert abs(drift) < 0.05
+    assert umax < 5 * math.sqrt(2 * 9.8 * 0.6)  # bounded: a few times the free-fall speed of the column
+
+
+def test_dam_break_128_fp32_refine_matches_fp64():
+    n = 128
+    dx = 1.0 / n
+    phi = dam_break(n)
+    out = {}
+    for prec in (fs.FS_PRECISION_FP64, fs.FS_PRECISION_FP32_REFINE):
+        with fs.Solver(n, dx, **water_params(prec, 1e-6)) as s:
+            s.upload("phi", phi)
+            zero_velocity(s, n)
+            dt = s.cfl_dt()
+            reps = [s.step(dt) for _ in range(2)]
+            out[prec] = (reps, s.download("phi"), s.download("pressure"), dt)
+    (r64, phi64, p64, dt64), (r32, phi32, p32, dt32) = out[fs.FS_PRECISION_FP64], out[fs.FS_PRECISION_FP32_REFINE]
+    assert dt64 == dt32
+    for r in r64 + r32:
+        assert r["status"] == fs.FS_OK and r["max_rel_residual"] <= 1e-6
+    p64 = p64 - p64.mean()
+    p32 = p32 - p32.mean()
+    perr = np.linalg.norm(p32 - p64) / np.linalg.norm(p64)
+    print(f"128^3 dam break, 2 steps: pressure rel. difference {perr:.2e}, "
+          f"phi max difference {np.abs(phi32 - phi64).max():.2e}, "
+          f"div L2 {r64[-1]['div_l2']:.3e} (fp64) / {r32[-1]['div_l2']:.3e} (fp32+refine)")
+    assert perr < 1e-2
+    assert np.abs(phi32 - phi64).max() < 1e-4
+
+
+def test_rising_bubble_256_fp32_refine_step():
+    n = 256
+    dx = 1.0 / n
+    x, y, z = axes(n)
+    phi = np.sqrt((x - 0.5) ** 2 + (y - 0.25) ** 2 + (z - 0.5) ** 2) - 0.15
+    v0 = heaviside_volume(phi, dx)
+    with fs.Solver(n, dx, rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3,
+                   precision=fs.FS_PRECISION_FP32_REFINE, tolerance=1e-6, stop=fs.FS_STOP_RELATIVE,
+                   max_iteration=20000, cfl=0.5, order=3) as s:
+        s.upload("phi", phi)
+        zero_velocity(s, n)
+        rep = s.step(s.cfl_dt())
+        phi_t = s.download("phi")
+    assert rep["status"] == fs.FS_OK and rep["max_rel_residual"] <= 1e-6
+    assert abs(heaviside_volume(phi_t, dx) / v0 - 1) < 1e-3
+
+
+def rayleigh_taylor(n, seed=0):
+    """y - 0.5 - 0.01-amplitude sum of modes kx, kz in 1..8 with seeded
+    amplitudes and phases; negative below the interface (oil)."""
+    rng = np.random.default_rng(seed)
+    a = rng.normal(size=(8, 8))
+    px, pz = rng.uniform(0, 1, size=(8, 8)), rng.uniform(0, 1, size=(8, 8))
+    xs = (np.arange(n) + 0.5) / n
+    pert = np.zeros((n, n))  # [z, x]
+    for kx in range(8):
+        for kz in range(8):
+            pert += a[kx, kz] * np.cos(2 * np.pi * ((kx + 1) * xs[None, :] + px[kx, kz])) * \
+                np.cos(2 * np.pi * ((kz + 1) * xs[:, None] + pz[kx, kz]))
+    pert *= 0.01 / np.abs(pert).max()
+    return (xs[None, :, None] - 0.5) - pert[:, None, :]
+
+
+def test_rayleigh_taylor_512_fp32_refine_step():
+    n = 512
+    dx = 1.0 / n
+    phi = rayleigh_taylor(n)
+    v0 = heaviside_volume(phi, dx)
+    with fs.Solver(n, dx, rho_neg=850.0, rho_pos=1000.0, mu_neg=5e-2, mu_pos=1e-3,
+                   precision=fs.FS_PRECISION_FP32_REFINE, tolerance=1e-6, stop=fs.FS_STOP_RELATIVE,
+                   max_iteration=20000, cfl=0.5, order=3, viscosity=1) as s:
+        mem = s.memory_bytes()
+        s.upload("phi", phi)
+        zero_velocity(s, n)
+        rep = s.step(s.cfl_dt())
+        phi_t = s.download("phi")
+    print(f"512^3 Rayleigh-Taylor: device memory {mem / 2**30:.1f} GiB, pcg {rep['pcg_iterations']}, "
+          f"viscosity CG {rep['viscosity_iterations']}, {rep['ms']:.0f} ms")
+    assert mem < 64 * 2**30
+    assert rep["status"] == fs.FS_OK and rep["max_rel_residual"] <= 1e-6
+    assert abs(heaviside_volume(phi_t, dx) / v0 - 1) < 1e-3
