@@ -193,9 +193,14 @@ class EULERIAN_FLUID_SOLVER_3D:
 
     @classmethod
     def FromScript(cls, path, cfl=None):
-        """Build from a reference .sim file (air/water box mode)."""
+        """Build from a reference .sim file (air/water box mode).  A script
+        in the reference's oil/water pipe mode (SIMULATION_WORLD.h:119-122,
+        the mode its own four scripts select) is refused: this solver has no
+        pipe geometry, so running it as a box would be silently wrong."""
         r = SCRIPT_READER(path)
         world = r.FindBlock("SIMULATION_WORLD")
+        if world.GetBoolean("oil_water_simulation", False):
+            raise ValueError("oil_water_simulation (the pipe mode) is not supported; use air_water_simulation")
         grid = GRID_STRUCTURE_3D().InitializeFromBlock(
             world.FindBlock("WORLD_DISCRETIZATION_AIR_WATER").FindBlock("GRID_STRUCTURE_3D_LARGE"))
         s = cls().InitializeFromScriptBlock(None, grid, r.FindBlock("FLUID_SOLVER_UNIFORM_AIR_WATER"))

@@ -413,6 +413,10 @@ class EULERIAN_FLUID_SOLVER_3D {  // EULERIAN_FLUID_SOLVER_3D.h
   void InitializeFromScript(const std::string& path) {
     SCRIPT_READER r(path);
     const SCRIPT_BLOCK& world = r.FindBlock("SIMULATION_WORLD");
+    // the reference's oil/water pipe mode (SIMULATION_WORLD.h:119-122) has no
+    // counterpart here: refuse it rather than run the script as a box
+    if (world.GetBoolean("oil_water_simulation", false))
+      throw std::invalid_argument("oil_water_simulation (the pipe mode) is not supported; use air_water_simulation");
     GRID_STRUCTURE_3D g;
     g.InitializeFromBlock(world.FindBlock("WORLD_DISCRETIZATION_AIR_WATER").FindBlock("GRID_STRUCTURE_3D_LARGE"));
     InitializeFromScriptBlock(g, r.FindBlock("FLUID_SOLVER_UNIFORM_AIR_WATER"));

@@ -135,3 +135,19 @@ def test_cpp_levelset_mirror_sweeps_and_writes_obj_like_python(mirror, tmp_path)
     assert open(out_obj).read() == open(py_obj).read()
     from oracle import fs_oracle as O
     assert np.array_equal(want, O.fast_sweeping(phi, s.base_grid.dx, 3))  # each call starts from its own set-up
+
+
+def test_pipe_mode_scripts_are_refused(mirror, tmp_path):
+    """A script in the reference's oil/water pipe mode is refused by both
+    script readers instead of being run as a box."""
+    path = write_script(str(tmp_path / "pipe.sim"), 16)
+    text = open(path).read()
+    assert "oil_water_simulation = false" in text
+    with open(path, "w") as f:
+        f.write(text.replace("air_water_simulation = true", "air_water_simulation = false")
+                .replace("oil_water_simulation = false", "oil_water_simulation = true"))
+    with pytest.raises(ValueError):
+        EULERIAN_FLUID_SOLVER_3D.FromScript(path)
+    res = subprocess.run([mirror, "step", path, "/dev/null", str(tmp_path / "out.bin")], capture_output=True,
+                         text=True)
+    assert res.returncode != 0 and "pipe mode" in res.stderr
