@@ -341,14 +341,20 @@ __global__ void k_mc_normalize(const unsigned long long* __restrict__ acc, doubl
   for (int q = 0; q < 3; ++q) nrm[3 * v + q] = len > 0.0 ? n[q] / len : 0.0;
 }
 
-bool g_table_ready = false;
+// __constant__ memory is per device: the table is copied once to each device
+// that polygonises (the current device at the call)
+constexpr int kMaxDevices = 64;
+bool g_table_ready[kMaxDevices] = {false};
 
 cudaError_t ensure_table() {
-  if (g_table_ready) return cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kMaxDevices && g_table_ready[dev]) return cudaSuccess;
   McTable t;
   if (!build_table(t)) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemcpyToSymbol(c_table, &t, sizeof t);
-  if (e == cudaSuccess) g_table_ready = true;
+  e = cudaMemcpyToSymbol(c_table, &t, sizeof t);
+  if (e == cudaSuccess && dev >= 0 && dev < kMaxDevices) g_table_ready[dev] = true;
   return e;
 }
 

@@ -54,6 +54,17 @@ def test_create_rejects_bad_arguments_before_touching_the_device():
     assert "densities" in fs.last_error()
     assert L.fs_step(None, ctypes.c_double(0.1), None) == fs.FS_INVALID_ARG
     assert L.fs_destroy(None) == fs.FS_OK
+    p = fs.default_params(velocity_scheme=7)
+    assert L.fs_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == fs.FS_INVALID_ARG
+    assert "velocity scheme" in fs.last_error()
+    p = fs.default_params(velocity_epsilon=-1.0)
+    assert L.fs_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == fs.FS_INVALID_ARG
+    # the reinitialisation and surface entry points refuse a missing context
+    assert L.fs_fast_sweeping(None, 0, 1) == fs.FS_INVALID_ARG
+    n64 = ctypes.c_int64()
+    assert L.fs_surface(None, ctypes.byref(n64), ctypes.byref(n64)) == fs.FS_INVALID_ARG
+    assert L.fs_surface_download(None, None, None, None) == fs.FS_INVALID_ARG
+    assert L.fs_write_obj(None, b"x.obj") == fs.FS_INVALID_ARG
 
 
 def test_pcg_csr_validates_the_matrix_on_the_host():
