@@ -339,7 +339,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     args = ap.parse_args()
 
-    world, rank, local, dist, barrier, max_over_ranks = init_replicas("nccl")
+    # the reference arm is host work: its ranks meet over gloo and touch no GPU
+    world, rank, local, dist, barrier, max_over_ranks = init_replicas("gloo" if args.impl == "reference" else "nccl")
 
     n = args.n
     config = {"workload": f"rising air bubble {n}^3, density ratio 1000, one timestep (TVD-RK3, 3 projections)",
