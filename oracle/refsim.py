@@ -22,7 +22,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_ref", "libfsref.so")
+# FSREF_LIB selects another build of the same sources in oracle/_ref/ (the
+# timed CPU baseline also tries libfsref_o3.so); goldens use libfsref.so
+LIB_PATH = os.path.join(HERE, "_ref", os.environ.get("FSREF_LIB", "libfsref.so"))
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
