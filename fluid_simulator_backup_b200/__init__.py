@@ -32,6 +32,7 @@ FS_STOP_RELATIVE, FS_STOP_ABSOLUTE = 0, 1
 FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER, FS_FLAG_CURVATURE_TYPO = 1, 2, 4, 8
 FS_FLAG_SORT_TYPO = 16
 FS_VELOCITY_WENO5, FS_VELOCITY_ENO3 = 0, 1
+FS_PRECOND_DEFAULT, FS_PRECOND_JACOBI, FS_PRECOND_JACOBI_BF16, FS_PRECOND_RED_BLACK = 0, 1, 2, 3
 
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
             "fs_memory_bytes", "fs_upload", "fs_download", "fs_upload_device", "fs_download_device", "fs_step",
@@ -62,7 +63,9 @@ class Params(ctypes.Structure):
                 ("viscosity", ctypes.c_int), ("viscosity_tolerance", ctypes.c_double),
                 ("viscosity_max_iteration", ctypes.c_int), ("cfl", ctypes.c_double), ("flags", ctypes.c_int),
                 ("surface_tension", ctypes.c_double), ("velocity_scheme", ctypes.c_int),
-                ("velocity_epsilon", ctypes.c_double), ("fast_sweeping", ctypes.c_int)]
+                ("velocity_epsilon", ctypes.c_double), ("fast_sweeping", ctypes.c_int),
+                ("pressure_preconditioner", ctypes.c_int), ("reliable_delta", ctypes.c_double),
+                ("flux_arithmetic", ctypes.c_int), ("verbose", ctypes.c_int)]
 
     def as_dict(self):
         d = {}

@@ -115,10 +115,12 @@ struct fs_ctx {
   double* a_vxb[3] = {};      // viscosity: x_bar per component
   double* a_rho = nullptr;    // device [4]: bars of rho_neg, rho_pos
   std::vector<double*> tape_cells, tape_faces;  // taped forward states, allocated on demand
-  bool debug = false;  // FS_DEBUG=1 in the environment: solver progress on stderr
-  double reliable_delta = 0.1;  // residual drop between reliable updates (FS_RELIABLE_DELTA to sweep)
-  int flux32 = 2;               // arithmetic of the FP32 flux SpMV (Op7::flux32; FS_FLUX32 to sweep)
-  int lean = 1;  // FP32 pressure solve preconditioned by the bf16 inverse diagonal (Op7::dinv16; FS_LEAN=0 off)
+  // derived from fs_params by apply_params
+  bool debug = false;           // params.verbose: solver progress on stderr
+  double reliable_delta = 0.1;  // params.reliable_delta
+  int flux32 = 2;               // params.flux_arithmetic (Op7::flux32)
+  int lean = 1;                 // FP32 pressure solve preconditioned by the bf16 inverse diagonal (Op7::dinv16)
+  bool red_black = false;       // FP32 pressure solve on the red-black Schur complement
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -207,11 +209,34 @@ fs_status check_params(const fs_params* p) {
     set_error("bad solver or reinitialisation settings");
     return FS_INVALID_ARG;
   }
+  if (p->pressure_preconditioner < FS_PRECOND_DEFAULT || p->pressure_preconditioner > FS_PRECOND_RED_BLACK ||
+      (p->pressure_preconditioner >= FS_PRECOND_JACOBI_BF16 && p->precision != FS_PRECISION_FP32_REFINE)) {
+    set_error("unknown pressure preconditioner %d for this precision", p->pressure_preconditioner);
+    return FS_INVALID_ARG;
+  }
+  if (!(p->reliable_delta >= 0.0 && p->reliable_delta < 1.0)) {
+    set_error("reliable_delta must be in [0, 1)");
+    return FS_INVALID_ARG;
+  }
+  if (p->flux_arithmetic < 0 || p->flux_arithmetic > 2) {
+    set_error("flux_arithmetic must be 0, 1 or 2");
+    return FS_INVALID_ARG;
+  }
   if (p->precision == FS_PRECISION_FP32_REFINE && (!(p->inner_tolerance > 0) || p->max_outer < 1)) {
     set_error("FP32_REFINE needs inner_tolerance > 0 and max_outer >= 1");
     return FS_INVALID_ARG;
   }
   return FS_OK;
+}
+
+// The solver settings of the context that follow from its parameters.
+void apply_params(fs_ctx* c) {
+  const fs_params& p = c->prm;
+  c->debug = p.verbose != 0;
+  c->reliable_delta = p.reliable_delta > 0.0 ? p.reliable_delta : 0.1;
+  c->flux32 = p.flux_arithmetic;
+  c->lean = p.pressure_preconditioner != FS_PRECOND_JACOBI;
+  c->red_black = c->fp32 && p.pressure_preconditioner == FS_PRECOND_RED_BLACK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1098,6 +1123,10 @@ void fs_params_default(fs_params* p) {
   p->viscosity_max_iteration = 1000;
   p->cfl = 0.5;
   p->flags = 0;
+  p->pressure_preconditioner = FS_PRECOND_DEFAULT;
+  p->reliable_delta = 0.1;
+  p->flux_arithmetic = 2;
+  p->verbose = 0;
 }
 
 const char* fs_status_str(fs_status s) {
@@ -1136,16 +1165,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->grid = *grid;
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
-  c->debug = std::getenv("FS_DEBUG") != nullptr;
-  if (const char* e = std::getenv("FS_LEAN")) c->lean = std::atoi(e) != 0;
-  if (const char* e = std::getenv("FS_FLUX32")) {
-    const int v = std::atoi(e);
-    if (v >= 0 && v <= 2) c->flux32 = v;
-  }
-  if (const char* e = std::getenv("FS_RELIABLE_DELTA")) {  // tuning knob for sweeps
-    const double v = std::atof(e);
-    if (v > 0.0 && v < 1.0) c->reliable_delta = v;
-  }
+  apply_params(c);
   c->Lc = make_lay(grid->nx, grid->ny, grid->nz);
   c->Lu = make_lay(grid->nx + 1, grid->ny, grid->nz);
   c->Lv = make_lay(grid->nx, grid->ny + 1, grid->nz);
@@ -1228,6 +1248,11 @@ fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
   if (p->precision != c->prm.precision) { set_error("precision is fixed at creation"); return FS_INVALID_ARG; }
   if (p->viscosity && !c->prm.viscosity) { set_error("viscosity buffers were not allocated at creation"); return FS_INVALID_ARG; }
   c->prm = *p;
+  apply_params(c);
+  // captured solver graphs hold the operator's arithmetic and preconditioner
+  // as kernel arguments: capture them again under the new settings
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  c->graphs.clear();
   return FS_OK;
 }
 

@@ -37,17 +37,13 @@
 namespace fsb {
 
 static int g_sm_count = 0;
-static int g_blocks_per_sm = 6;  // 6 x 256 threads: fully resident for kernels up to 40 registers
+constexpr int g_blocks_per_sm = 6;  // 6 x 256 threads: fully resident for kernels up to 40 registers
 
 int reduction_blocks(int64_t n) {
   if (g_sm_count <= 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) g_sm_count = 148;
-    if (const char* e = std::getenv("FS_BLOCKS_PER_SM")) {  // tuning knob for launch-shape sweeps
-      const int v = std::atoi(e);
-      if (v >= 1 && v <= 16) g_blocks_per_sm = v;
-    }
   }
   const int64_t want = (n + kRedThreads - 1) / kRedThreads;
   const int64_t cap = (int64_t)g_blocks_per_sm * g_sm_count;
@@ -564,25 +560,17 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_pupdate(Op7<V> A, X* __restr
 
 namespace {
 int g_cg_blocks[2][2][3];  // [X double?][V double?][spmv, update, pupdate]: resident blocks per SM
-// SpMV blocks per SM the compiler must fit (FS_SPMV_MINB = 2, 3 or 4 to
-// sweep); measured best at 256^3: 4 for FP32 vectors (64 registers, no
-// spills to speak of), 2 for FP64 (128 registers; fewer spill)
-int g_spmv_minb_env = 0;
-template <class V> int spmv_minb() { return g_spmv_minb_env ? g_spmv_minb_env : (sizeof(V) == 4 ? 4 : 2); }
+// SpMV blocks per SM the compiler must fit; measured best at 256^3 (sweeps
+// of 2, 3 and 4): 4 for FP32 vectors (64 registers, no spills to speak
+// of), 2 for FP64 (128 registers; fewer spill)
+template <class V> constexpr int spmv_minb() { return sizeof(V) == 4 ? 4 : 2; }
 }  // namespace
 
 template <class V, class X>
 void cg_prepare() {
-  reduction_blocks(1);  // SM count and the FS_BLOCKS_PER_SM knob
+  reduction_blocks(1);  // SM count
   int* slot = g_cg_blocks[sizeof(X) == 8][sizeof(V) == 8];
-  if (const char* e = std::getenv("FS_SPMV_MINB")) {
-    const int v = std::atoi(e);
-    if (v >= 2 && v <= 4) g_spmv_minb_env = v;
-  }
-  const int minb = spmv_minb<V>();
-  const void* spmv = minb == 4   ? (const void*)k_cg_spmv<V, 4>
-                     : minb == 3 ? (const void*)k_cg_spmv<V, 3>
-                                 : (const void*)k_cg_spmv<V, 2>;
+  const void* spmv = (const void*)k_cg_spmv<V, spmv_minb<V>()>;
   const void* ks[3] = {spmv, (const void*)k_cg_update<V>, (const void*)k_cg_pupdate<V, X>};
   for (int m = 0; m < 3; ++m) {
     if (slot[m]) continue;
@@ -607,13 +595,7 @@ void cg_iteration(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double*
   const int chunks = std::max(1, std::min(L.nz, want / (tx * ty)));
   const int kchunk = (L.nz + chunks - 1) / chunks;
   const dim3 sg(tx, ty, (L.nz + kchunk - 1) / kchunk);
-  const int minb = spmv_minb<V>();
-  if (minb == 4)
-    k_cg_spmv<V, 4><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
-  else if (minb == 3)
-    k_cg_spmv<V, 3><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
-  else
-    k_cg_spmv<V, 2><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
+  k_cg_spmv<V, spmv_minb<V>()><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
   // pointwise kernels: grid-stride over the vectors, resident blocks only
   const int64_t nvec = (int64_t)((L.nx + 3) >> 2) * L.ny * L.nz;
   auto grid = [&](int per_sm) {

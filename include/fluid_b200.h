@@ -63,6 +63,15 @@ typedef enum {
   FS_VELOCITY_ENO3 = 1    /* use_3rd_eno_v, the reference scripts' choice (ADVECTION_METHOD_3D.h:1639-1934) */
 } fs_velocity_scheme;
 
+/* Preconditioner of the pressure solve. */
+typedef enum {
+  FS_PRECOND_DEFAULT = 0,     /* FP64: Jacobi (the reference's, PCG_METHOD.cpp:128-160); FP32_REFINE: bf16 Jacobi */
+  FS_PRECOND_JACOBI = 1,      /* z = r / diag in the solve precision */
+  FS_PRECOND_JACOBI_BF16 = 2, /* FP32_REFINE: z = r * (1/diag rounded to bf16), 2 bytes per unknown */
+  FS_PRECOND_RED_BLACK = 3    /* FP32_REFINE: the same PCG in red-black order; the red cells are eliminated
+                                 exactly and bf16 Jacobi-PCG runs on the black Schur complement */
+} fs_preconditioner;
+
 typedef enum {
   FS_STOP_RELATIVE = 0,   /* ||b - A p||_2 / ||b||_2 < tolerance */
   FS_STOP_ABSOLUTE = 1    /* r.z < tolerance^2, the reference's PCG test (PCG_METHOD.cpp:87) */
@@ -109,6 +118,12 @@ typedef struct {
   double velocity_epsilon;          /* VELOCITY_ADVECTION.epsilon of the WENO5 weights (0: weno_epsilon) */
   int fast_sweeping;                /* fastsweeping_reinitialization: each reinitialisation block starts with
                                        fs_fast_sweeping(ctx, -1, 1) (EULERIAN_FLUID_SOLVER_3D.h:2202-2205) */
+  int pressure_preconditioner;      /* fs_preconditioner of the pressure solve */
+  double reliable_delta;            /* FP32_REFINE: the true FP64 residual replaces the recursive one each time the
+                                       latter drops by this factor (0: 0.1) */
+  int flux_arithmetic;              /* FP32_REFINE pressure SpMV: each face flux a (x_c - x_n) formed in 0: FP64,
+                                       1: FP32 and summed in FP64, 2: FP32 throughout (default) */
+  int verbose;                      /* 1: solver progress on stderr */
 } fs_params;
 
 typedef struct {

@@ -167,25 +167,24 @@ def test_projection_corrected_matches_oracle(precision):
     assert rep["div_l2"] > 0
 
 
-def test_bf16_jacobi_preconditioner(monkeypatch):
-    """The FP32 pressure solve preconditioned by 1/diag rounded to bf16 (the
-    default) against the exact FP32 diagonal (FS_LEAN=0): any fixed SPD
-    diagonal is a valid Jacobi preconditioner, both reach the same FP64 true
-    residual, so the pressures agree to the solve tolerance and the
-    iteration counts stay close."""
+def test_bf16_jacobi_preconditioner():
+    """The FP32 pressure solve preconditioned by 1/diag rounded to bf16
+    against the exact FP32 diagonal: any fixed SPD diagonal is a valid
+    Jacobi preconditioner, both reach the same FP64 true residual, so the
+    pressures agree to the solve tolerance and the iteration counts stay
+    close."""
     n = 48
     phi = sphere(n, (0.5, 0.4, 0.5), 0.2)
     _, u, v, w = random_state((n, n, n), 9)
     dt = 1e-3
     out = {}
-    for mode in ("0", "1"):
-        monkeypatch.setenv("FS_LEAN", mode)
+    for mode in (fs.FS_PRECOND_JACOBI, fs.FS_PRECOND_JACOBI_BF16):
         with make(n, fs.FS_PRECISION_FP32_REFINE, rho_neg=1.0, rho_pos=1000.0, tolerance=1e-10,
-                  max_iteration=20000) as s:
+                  max_iteration=20000, pressure_preconditioner=mode) as s:
             upload_all(s, phi, u, v, w)
             rep = s.project(dt)
             out[mode] = (rep, s.download("pressure"))
-    (r0, p0), (r1, p1) = out["0"], out["1"]
+    (r0, p0), (r1, p1) = out[fs.FS_PRECOND_JACOBI], out[fs.FS_PRECOND_JACOBI_BF16]
     assert r0["rel_residual"] < 1e-10 and r1["rel_residual"] < 1e-10
     assert abs(r1["iterations"] - r0["iterations"]) <= 0.1 * r0["iterations"] + 16
     p0 = p0 - p0.mean()

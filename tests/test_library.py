@@ -91,9 +91,10 @@ def test_pcg_csr_noalloc_rejects_bad_arguments_on_the_host():
 
 @pytest.mark.parametrize("name", ["3D_script.sim", "3D_script_1.sim"])
 def test_script_reader_reads_reference_scripts(name):
-    path = "/root/reference/" + name
-    if not os.path.exists(path):
-        pytest.skip("reference scripts not present")
+    ref = os.environ.get("FS_REFERENCE_DIR")
+    if not ref or not os.path.exists(os.path.join(ref, name)):
+        pytest.skip("FS_REFERENCE_DIR does not point at the reference's scripts")
+    path = os.path.join(ref, name)
     r = SCRIPT_READER(path)
     b = r.FindBlock("FLUID_SOLVER_UNIFORM_AIR_WATER")
     assert b.GetFloat("water_density") == 1000.0
@@ -128,3 +129,15 @@ def test_params_from_block_maps_reference_keys():
     assert p.order == 3 and p.max_iteration == 500 and abs(p.tolerance - 1e-5) < 1e-20
     assert p.precision == fs.FS_PRECISION_FP32_REFINE and p.stop == fs.FS_STOP_RELATIVE
     assert abs(g.dx - 1 / 16) < 1e-15
+
+
+def test_solver_settings_are_checked_on_the_host():
+    """The pressure preconditioner, reliable-update factor and flux
+    arithmetic are fs_params fields, checked by fs_create before any device
+    work: the red-black and bf16 forms exist only for FP32_REFINE."""
+    for kw in ({"precision": fs.FS_PRECISION_FP64, "pressure_preconditioner": fs.FS_PRECOND_RED_BLACK},
+               {"precision": fs.FS_PRECISION_FP64, "pressure_preconditioner": fs.FS_PRECOND_JACOBI_BF16},
+               {"pressure_preconditioner": 9}, {"reliable_delta": 1.5}, {"flux_arithmetic": 3}):
+        with pytest.raises(fs.FsError) as e:
+            fs.Solver((8, 8, 8), 1.0 / 8, **kw)
+        assert e.value.status == fs.FS_INVALID_ARG
