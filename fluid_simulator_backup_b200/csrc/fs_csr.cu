@@ -8,7 +8,6 @@
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 #include "../../include/fluid_b200.h"
@@ -22,19 +21,37 @@ struct CsrState {
   double rz, pq, rr, bb, tol;
   int iter, max_iter, done, criterion, status;
   unsigned int ticket;
+  int bad_index;  // set by k_csr_init when row_ptr or column_index point outside the matrix
 };
 
-__global__ void k_csr_init(int n, const double* __restrict__ val, const int* __restrict__ col,
+// status values of CsrState (0: running)
+enum { CSR_CONVERGED = 1, CSR_MAXITER = 2, CSR_NONFINITE = 3, CSR_BAD_INDEX = 4 };
+
+// r = b - A x, p = z = r/diag and the three start sums.  Every index is
+// checked before it is used: a row whose row_ptr range leaves [0, nnz] or
+// whose column index leaves [0, n) reads nothing and flags bad_index, which
+// ends the solve before any other kernel reads the matrix (row_ptr must hold
+// n + 1 entries and values/column_index nnz entries).
+__global__ void k_csr_init(int n, int nnz, const double* __restrict__ val, const int* __restrict__ col,
                            const int* __restrict__ rp, const double* __restrict__ b, const double* __restrict__ x,
                            double* __restrict__ r, double* __restrict__ p, double* __restrict__ dinv,
                            double* partials, CsrState* st) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double rz = 0, rr = 0, bb = 0;
   if (row < n) {
+    const int q0 = rp[row], q1 = rp[row + 1];
+    bool ok = 0 <= q0 && q0 <= q1 && q1 <= nnz;
     double acc = 0.0, d = 0.0;
-    for (int q = rp[row]; q < rp[row + 1]; ++q) {
-      acc += val[q] * x[col[q]];
-      if (col[q] == row) d = val[q];
+    for (int q = q0; ok && q < q1; ++q) {
+      const int cq = col[q];
+      if (cq < 0 || cq >= n) { ok = false; break; }
+      acc += val[q] * x[cq];
+      if (cq == row) d = val[q];
+    }
+    if (!ok) {
+      atomicOr(&st->bad_index, 1);
+      d = 1.0;
+      acc = b[row];
     }
     const double rv = b[row] - acc;
     const double di = 1.0 / d;
@@ -110,10 +127,10 @@ __global__ void k_csr_decide(double* partials, CsrState* st) {
   partials[3] = 0.0;
   partials[4] = 0.0;
   partials[5] = 0.0;
-  if (bad) { st->status = 3; st->done = 1; return; }
-  if (conv) { st->status = 1; st->done = 1; return; }
+  if (bad) { st->status = CSR_NONFINITE; st->done = 1; return; }
+  if (conv) { st->status = CSR_CONVERGED; st->done = 1; return; }
   st->iter += 1;
-  if (st->iter >= st->max_iter) { st->status = 2; st->done = 1; }
+  if (st->iter >= st->max_iter) { st->status = CSR_MAXITER; st->done = 1; }
 }
 
 __global__ void k_csr_pupdate(int n, double* __restrict__ p, const double* __restrict__ r,
@@ -124,6 +141,9 @@ __global__ void k_csr_pupdate(int n, double* __restrict__ p, const double* __res
   if (row < n) p[row] = p[row] * beta + r[row] * dinv[row];
 }
 
+// The start decisions.  Like PCG_METHOD::PCGMethod (PCG_METHOD.cpp:4-126,
+// `while (num_iteration < max_iteration)`), a cap of 0 runs no iteration and
+// leaves x as it came.
 __global__ void k_csr_start(double* partials, CsrState* st) {
   st->rz = partials[0];
   st->rr = partials[1];
@@ -132,9 +152,11 @@ __global__ void k_csr_start(double* partials, CsrState* st) {
   st->done = 0;
   st->status = 0;
   partials[3] = partials[4] = partials[5] = partials[6] = 0.0;
-  if (!isfinite(st->rz)) { st->status = 3; st->done = 1; }
-  else if (st->bb == 0.0 || st->rr == 0.0) { st->status = 1; st->done = 1; }
-  else if (st->criterion == 0 && sqrt(st->rr) <= st->tol * sqrt(st->bb)) { st->status = 1; st->done = 1; }
+  if (st->bad_index) { st->status = CSR_BAD_INDEX; st->done = 1; }
+  else if (!isfinite(st->rz)) { st->status = CSR_NONFINITE; st->done = 1; }
+  else if (st->bb == 0.0 || st->rr == 0.0) { st->status = CSR_CONVERGED; st->done = 1; }
+  else if (st->criterion == 0 && sqrt(st->rr) <= st->tol * sqrt(st->bb)) { st->status = CSR_CONVERGED; st->done = 1; }
+  else if (st->max_iter <= 0) { st->status = CSR_MAXITER; st->done = 1; }
 }
 
 }  // namespace
@@ -185,7 +207,7 @@ extern "C" fs_status fs_pcg_csr(fs_ctx* ctx, int n, int nnz, const double* value
     ok(cudaMemsetAsync(part, 0, 8 * sizeof(double), s));
     ok(cudaMemcpyAsync(st, &host, sizeof(CsrState), cudaMemcpyHostToDevice, s));
     const int T = 256, B = (n + T - 1) / T;
-    k_csr_init<<<B, T, 0, s>>>(n, dval, dcol, drp, db, dx, dr, dp, dd, part, st);
+    k_csr_init<<<B, T, 0, s>>>(n, nnz, dval, dcol, drp, db, dx, dr, dp, dd, part, st);
     k_csr_start<<<1, 1, 0, s>>>(part, st);
     const int batches = max_iteration / 16 + 2;
     for (int bt = 0; bt < batches && result == FS_OK; ++bt) {
@@ -210,8 +232,8 @@ extern "C" fs_status fs_pcg_csr(fs_ctx* ctx, int n, int nnz, const double* value
   if (result != FS_OK) return result;
   if (iterations) *iterations = host.iter;
   if (residual) *residual = stop == FS_STOP_ABSOLUTE ? std::sqrt(host.rz) : (host.bb > 0 ? std::sqrt(host.rr / host.bb) : 0.0);
-  if (host.status == 3) return FS_NONFINITE;
-  if (host.status == 2) return FS_NOT_CONVERGED;
+  if (host.status == CSR_NONFINITE) return FS_NONFINITE;
+  if (host.status == CSR_MAXITER) return FS_NOT_CONVERGED;
   return FS_OK;
 }
 
@@ -244,23 +266,17 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-NoAllocScratch* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array for the current device.  In host code
-// the symbol is only a host-side stand-in, so the address is looked up once
-// per device (with that device current) and cached.
+// Device address of the scratch array in the current device's context.  In
+// host code the symbol is only a host-side stand-in, so the address is
+// looked up with the caller's device current.  The lookup allocates nothing
+// and is repeated on every call: a context that was reset and rebuilt since
+// the last call (cudaDeviceReset in the embedding) may hold the array at
+// another address.
 fs_status noalloc_scratch(NoAllocScratch** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FS_CUDA_ERROR;
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return FS_CUDA_ERROR;
-    g_noalloc_ptr[dev] = static_cast<NoAllocScratch*>(ptr);
-  }
-  *out = g_noalloc_ptr[dev];
+  void* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || !ptr) return FS_CUDA_ERROR;
+  *out = static_cast<NoAllocScratch*>(ptr);
   return FS_OK;
 }
 
@@ -275,6 +291,9 @@ extern "C" fs_status fs_pcg_csr_noalloc(int n, int nnz, const double* values, co
     return FS_INVALID_ARG;
   }
   if (n > kNoAllocMaxRows) return FS_INVALID_ARG;  // beyond the fixed scratch: use fs_pcg_csr
+  // an error left behind by the caller's earlier, unrelated work is not this
+  // solve's failure: clear it before the first launch is checked
+  (void)cudaGetLastError();
   NoAllocScratch* sc = nullptr;
   fs_status st0 = noalloc_scratch(&sc);
   if (st0 != FS_OK) return st0;
@@ -285,12 +304,14 @@ extern "C" fs_status fs_pcg_csr_noalloc(int n, int nnz, const double* values, co
   host.criterion = stop;
   auto ok = [](cudaError_t e) { return e == cudaSuccess; };
   // the scratch keeps the previous call's contents: clear the accumulators
+  // and the solver state (bad_index included) before the first kernel
   if (!ok(cudaMemsetAsync(sc->partials, 0, sizeof(sc->partials), s)) ||
       !ok(cudaMemcpyAsync(&sc->st, &host, sizeof(CsrState), cudaMemcpyHostToDevice, s))) {
     return FS_CUDA_ERROR;
   }
   const int T = 256, B = (n + T - 1) / T;
-  k_csr_init<<<B, T, 0, s>>>(n, values, column_index, row_ptr, b, x, sc->r, sc->p, sc->dinv, sc->partials, &sc->st);
+  k_csr_init<<<B, T, 0, s>>>(n, nnz, values, column_index, row_ptr, b, x, sc->r, sc->p, sc->dinv, sc->partials,
+                             &sc->st);
   k_csr_start<<<1, 1, 0, s>>>(sc->partials, &sc->st);
   if (!ok(cudaGetLastError())) return FS_CUDA_ERROR;
   const int batches = max_iteration / 16 + 2;
@@ -314,7 +335,8 @@ extern "C" fs_status fs_pcg_csr_noalloc(int n, int nnz, const double* values, co
   }
   if (iterations) *iterations = host.iter;
   if (residual) *residual = stop == FS_STOP_ABSOLUTE ? std::sqrt(host.rz) : (host.bb > 0 ? std::sqrt(host.rr / host.bb) : 0.0);
-  if (host.status == 3) return FS_NONFINITE;
-  if (host.status == 2) return FS_NOT_CONVERGED;
+  if (host.status == CSR_BAD_INDEX) return FS_INVALID_ARG;
+  if (host.status == CSR_NONFINITE) return FS_NONFINITE;
+  if (host.status == CSR_MAXITER) return FS_NOT_CONVERGED;
   return FS_OK;
 }

@@ -341,21 +341,15 @@ __global__ void k_mc_normalize(const unsigned long long* __restrict__ acc, doubl
   for (int q = 0; q < 3; ++q) nrm[3 * v + q] = len > 0.0 ? n[q] / len : 0.0;
 }
 
-// __constant__ memory is per device: the table is copied once to each device
-// that polygonises (the current device at the call)
-constexpr int kMaxDevices = 64;
-bool g_table_ready[kMaxDevices] = {false};
-
+// __constant__ memory belongs to the device context: the table is copied to
+// the current device on every polygonisation (a few kB, next to the passes
+// over the grid), so a context that was reset and rebuilt since the last
+// call gets it again.  The host copy is built once.
 cudaError_t ensure_table() {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev >= 0 && dev < kMaxDevices && g_table_ready[dev]) return cudaSuccess;
-  McTable t;
-  if (!build_table(t)) return cudaErrorInvalidValue;
-  e = cudaMemcpyToSymbol(c_table, &t, sizeof t);
-  if (e == cudaSuccess && dev >= 0 && dev < kMaxDevices) g_table_ready[dev] = true;
-  return e;
+  static McTable host_table;
+  static bool built = build_table(host_table);
+  if (!built) return cudaErrorInvalidValue;
+  return cudaMemcpyToSymbol(c_table, &host_table, sizeof host_table);
 }
 
 // exclusive prefix sum of n ints into out; returns the total in *total

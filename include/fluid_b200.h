@@ -278,16 +278,26 @@ fs_status fs_project_adjoint(fs_ctx* ctx, double dt);          /* (u, v, w) -> (
  * runtime, a real-time loop that must not take cudaMalloc's implicit
  * synchronisation).  No counterpart in the reference: it is an addition of
  * this library.  Every pointer is DEVICE memory the caller owns: the CSR
- * matrix (values, column_index, row_ptr), b, and x (initial guess in, result
- * out); stream may be NULL (the legacy default stream).  The working vectors
- * live in one fixed device array of the library (n <= 262144 rows, about
- * 8.4 MB on every GPU that loads the library, kept until the process exits);
- * larger systems are rejected with FS_INVALID_ARG.  The first call on a
- * device looks up that array's device address, so make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (from
- * several host threads or streams) race and must not be issued.  Every row
- * needs a nonzero diagonal (not checked here; a zero diagonal ends the solve
- * with FS_NONFINITE).  No device or host memory is allocated. */
+ * matrix (values [nnz], column_index [nnz], row_ptr [n + 1]), b, and x
+ * (initial guess in, result out); stream may be NULL (the legacy default
+ * stream).  The working vectors live in one fixed device array of the
+ * library (n <= 262144 rows, about 8.4 MB on every GPU that loads the
+ * library, kept until the process exits); larger systems are rejected with
+ * FS_INVALID_ARG.  Each call looks up that array's device address with the
+ * caller's device current (no allocation); the first call on a device also
+ * loads the library's device code there, so make it before any stream
+ * capture.  The call waits on `stream` between batches of 16 iterations and
+ * returns when the solve has ended.  All calls share the array: calls that
+ * overlap on the GPU (from several host threads or streams) race and must
+ * not be issued.  The matrix is checked on the device before it is used: a
+ * row_ptr entry outside [0, nnz], a decreasing row_ptr or a column index
+ * outside [0, n) ends the call with FS_INVALID_ARG, reading nothing outside
+ * the arrays and leaving x unchanged.  Every row needs a nonzero diagonal
+ * (a zero diagonal ends the solve with FS_NONFINITE).  max_iteration = 0
+ * runs no iteration (x unchanged, FS_NOT_CONVERGED unless b - A x already
+ * meets the test).  After FS_CUDA_ERROR, kernels of the call may still be
+ * queued on `stream`: synchronise it before reusing x or calling again.
+ * No device or host memory is allocated. */
 fs_status fs_pcg_csr_noalloc(int n, int nnz, const double* values, const int* column_index, const int* row_ptr,
                              const double* b, double* x, double tolerance, int max_iteration, int stop,
                              void* stream, int* iterations, double* residual);

@@ -120,3 +120,39 @@ def test_noalloc_reports_iteration_limit_and_rejects_oversize():
     st = fs.lib().fs_pcg_csr_noalloc(MAX_ROWS + 1, 7 * (MAX_ROWS + 1), d.data_ptr(), d.data_ptr(), d.data_ptr(),
                                      d.data_ptr(), d.data_ptr(), 1e-6, 10, fs.FS_STOP_RELATIVE, None, None, None)
     assert st == fs.FS_INVALID_ARG
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_out_of_range_indices_on_the_device():
+    """A column index outside [0, n) or a row_ptr entry beyond nnz is found by
+    the device-side check before the matrix is used: FS_INVALID_ARG, x left
+    as it came, and the next call on a valid system is unaffected."""
+    import torch
+
+    vals, cols, rowptr, b = variable_poisson_csr(8, 5)
+    bad_col = cols.copy()
+    bad_col[17] = len(b)  # one past the last row
+    bad_ptr = rowptr.copy()
+    bad_ptr[5] = len(vals) + 3  # beyond nnz (and decreasing after it)
+    for c, r in ((bad_col, rowptr), (cols, bad_ptr)):
+        x, it, res, st = noalloc_solve(torch, vals, c, r, b, 1e-10, 100, fs.FS_STOP_RELATIVE)
+        assert st == fs.FS_INVALID_ARG
+        assert not np.any(x)  # the zero initial guess is untouched
+    x, it, res, st = noalloc_solve(torch, vals, cols, rowptr, b, 1e-10, 1000, fs.FS_STOP_RELATIVE)
+    assert st == fs.FS_OK and res <= 1e-10
+
+
+@pytest.mark.gpu
+def test_zero_iteration_cap_runs_no_iteration():
+    """max_iteration = 0 runs no iteration, as PCG_METHOD::PCGMethod's
+    `while (num_iteration < max_iteration)` loop (PCG_METHOD.cpp:4-126): x is
+    unchanged and the solve reports 0 iterations, in both CSR entry points."""
+    import torch
+
+    vals, cols, rowptr, b = variable_poisson_csr(8, 6)
+    x0 = np.full_like(b, 0.25)
+    x, it, res, st = fs.pcg_csr(vals, cols, rowptr, b, x0, 1e-10, 0, fs.FS_STOP_RELATIVE)
+    assert st == fs.FS_NOT_CONVERGED and it == 0
+    np.testing.assert_array_equal(x, x0)
+    x, it, res, st = noalloc_solve(torch, vals, cols, rowptr, b, 1e-10, 0, fs.FS_STOP_RELATIVE)
+    assert st == fs.FS_NOT_CONVERGED and it == 0 and not np.any(x)
