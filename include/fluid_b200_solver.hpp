@@ -254,10 +254,27 @@ struct GRID_STRUCTURE_3D {  // GRID_STRUCTURE_3D.h:91-137: dx = (max - min)/(res
   }
 };
 
-struct CSR_MATRIX {  // CSR_MATRIX.h:10-35
+template <class TT> struct CSR_MATRIX {  // CSR_MATRIX.h:10-35
   int N = 0, nz = 0;
-  std::vector<double> values;
+  std::vector<TT> values;
   std::vector<int> column_index, row_ptr;
+};
+
+template <class TT> struct VECTOR_ND {  // VECTOR_ND.h:7-12: num_dimension values
+  int num_dimension = 0;
+  std::vector<TT> values;
+  VECTOR_ND() = default;
+  explicit VECTOR_ND(int n, TT v = TT(0)) : num_dimension(n), values(n, v) {}
+  TT& operator[](int i) { return values[i]; }
+  const TT& operator[](int i) const { return values[i]; }
+};
+
+// The boundary-condition tags the reference passes to every linear solver
+// (FIELD_STRUCTURE_3D<int> bc, one tag per cell); the Jacobi-PCG does not
+// read them (PCG_METHOD.h: Solve hands A, x, b to PCGMethod).
+template <class TT> struct FIELD_STRUCTURE_3D {
+  GRID_STRUCTURE_3D grid;
+  std::vector<TT> values;
 };
 
 class LINEAR_SOLVER {  // LINEAR_SOLVER.h:36: Solve is the plugin point
@@ -274,8 +291,8 @@ class LINEAR_SOLVER {  // LINEAR_SOLVER.h:36: Solve is the plugin point
     tolerance = tol;
     sqr_tolerance = tol * tol;
   }
-  virtual void Solve(const int& thread_id, const CSR_MATRIX& A, std::vector<double>& x,
-                     const std::vector<double>& b) = 0;
+  virtual void Solve(const int& thread_id, const CSR_MATRIX<double>& A, VECTOR_ND<double>& x,
+                     const VECTOR_ND<double>& b, const FIELD_STRUCTURE_3D<int>& bc) = 0;
 };
 
 // Jacobi-PCG on the GPU with the reference's stopping test r.z < tol^2
@@ -284,13 +301,18 @@ class CUDA_PCG_METHOD : public LINEAR_SOLVER {
  public:
   explicit CUDA_PCG_METHOD(bool rel = false) : relative(rel) {}
   bool relative;
-  void Solve(const int& thread_id, const CSR_MATRIX& A, std::vector<double>& x, const std::vector<double>& b) override {
+  void Solve(const int& thread_id, const CSR_MATRIX<double>& A, VECTOR_ND<double>& x, const VECTOR_ND<double>& b,
+             const FIELD_STRUCTURE_3D<int>& bc) override {
+    (void)bc;  // boundary tags: already folded into A by the system builder
     if (thread_id != 0) return;
-    if ((int)x.size() != A.N || (int)b.size() != A.N) throw std::invalid_argument("CUDA_PCG_METHOD: size mismatch");
+    if (x.num_dimension != A.N || b.num_dimension != A.N || (int)x.values.size() != A.N ||
+        (int)b.values.size() != A.N)
+      throw std::invalid_argument("CUDA_PCG_METHOD: size mismatch");
     int it = 0;
     double res = 0.0;
-    check(fs_pcg_csr(nullptr, A.N, A.nz, A.values.data(), A.column_index.data(), A.row_ptr.data(), b.data(), x.data(),
-                     tolerance, max_iteration, relative ? FS_STOP_RELATIVE : FS_STOP_ABSOLUTE, &it, &res),
+    check(fs_pcg_csr(nullptr, A.N, A.nz, A.values.data(), A.column_index.data(), A.row_ptr.data(), b.values.data(),
+                     x.values.data(), tolerance, max_iteration, relative ? FS_STOP_RELATIVE : FS_STOP_ABSOLUTE, &it,
+                     &res),
           "fs_pcg_csr", true);
     num_iteration = it;
     residual = res;

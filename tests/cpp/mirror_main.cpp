@@ -52,19 +52,22 @@ int main(int argc, char** argv) {
       f.read(reinterpret_cast<char*>(hdr), sizeof hdr);
       f.read(reinterpret_cast<char*>(&tol), sizeof tol);
       f.read(reinterpret_cast<char*>(&maxit), sizeof maxit);
-      CSR_MATRIX A;
+      CSR_MATRIX<double> A;
       A.N = hdr[0];
       A.nz = hdr[1];
       A.values = read_vec<double>(f, A.nz);
       A.column_index = read_vec<int>(f, A.nz);
       A.row_ptr = read_vec<int>(f, A.N + 1);
-      std::vector<double> b = read_vec<double>(f, A.N), x(A.N, 0.0);
+      VECTOR_ND<double> b, x(A.N, 0.0);
+      b.values = read_vec<double>(f, A.N);
+      b.num_dimension = A.N;
+      FIELD_STRUCTURE_3D<int> bc;  // the boundary tags the reference passes along
       CUDA_PCG_METHOD solver;
       LINEAR_SOLVER& ls = solver;  // through the plugin base, as POISSON_SOLVER_3D holds it
       ls.Initialize(tol, maxit);
-      for (int t = 3; t >= 0; --t) ls.Solve(t, A, x, b);  // worker threads 1..3 return at once
+      for (int t = 3; t >= 0; --t) ls.Solve(t, A, x, b, bc);  // worker threads 1..3 return at once
       std::ofstream o(argv[3], std::ios::binary);
-      write_vec(o, x);
+      write_vec(o, x.values);
       std::printf("iterations %d residual %.17g\n", ls.num_iteration, ls.residual);
       return 0;
     }
