@@ -44,10 +44,6 @@ BYTES_PER_UNKNOWN_PCG_FP64 = 120
 # k_cg_pupdate, one capture of the bench workload); scaled by the unknowns
 # for other sizes
 TRAFFIC_PER_ITERATION_256_FP32 = 1006.4e6
-# PCG iterations per projection of the FP64 GPU path on this workload at 256^3
-# (6725 per timestep of 3 projections over steps 4-6, measured by the default
-# run's fp64 block); the reference arm prices its projection with it
-REF_PCG_ITERATIONS_256 = 2242
 
 
 def scene(n):
@@ -57,8 +53,14 @@ def scene(n):
     return phi, u, v, w
 
 
+PRECONDITIONER = {"default": 0, "jacobi": 1, "bf16": 2, "red_black": 3}
+PRECOND_CHOICE = "default"
+
+
 def params(fs, precision):
-    return fs.default_params(rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0),
+    pc = PRECONDITIONER[PRECOND_CHOICE] if precision == fs.FS_PRECISION_FP32_REFINE else 0
+    return fs.default_params(pressure_preconditioner=pc,
+                             rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0),
                              precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=20000,
                              inner_tolerance=1e-3, max_outer=30, viscosity=1, viscosity_tolerance=1e-8, cfl=0.5,
                              order=3, reinit_iterations=10, reinit_scaling=5, weno_epsilon=1e-6)
@@ -189,113 +191,107 @@ def adjoint_steps(fs, n, warmup, steps):
             "steps": steps}
 
 
-def reference_sample(n, pcg_iterations_per_projection, threads=1):
-    """Time the reference's own CPU operators (oracle/_ref, built from the
-    reference sources) on the same 256^3 scene and scale them to one
-    timestep: 3 level-set WENO5 updates, 3 WENO5 velocity updates, 3
-    explicit viscosity updates (the reference's air/water viscosity), 3
-    projections (system build + the GPU FP64 path's PCG iteration count per
-    projection at the same tolerance) and 3 reinitialisation blocks of 10
-    pseudo-steps.  Bounded sample: one call of each operator, the projection
-    run at two iteration caps to separate build and per-iteration cost, one
-    Sussman pseudo-step."""
-    import psutil
+def reference_tolerance(m, rel=1e-6):
+    """The reference's PCG stops on an absolute test, r.z < tol^2
+    (PCG_METHOD.cpp:87).  The tolerance that matches the GPU path's relative
+    test ||r||/||b|| <= rel on the scene's first projection: rel times
+    sqrt(b.D^-1 b) of that system.  The first stage projects u* = (0, g dt,
+    0) on interior faces (zero walls), so b = div(g) does not depend on dt."""
+    from oracle import fs_oracle as O
+    phi, u, v, w = scene(m)
+    dt = 1.0
+    v = v.copy()
+    v[:, 1:-1, :] = -9.8 * dt
+    b = -O.divergence(u, v, w, 1.0 / m, dt)
+    b = b - b.mean()
+    diag = O.poisson_operator(phi, 1.0 / m, 1.0, 1000.0)[3]
+    return rel * float(np.sqrt(np.sum(b * b / diag)))
+
+
+def reference_frames(sizes, frames, budget_s, lib_name="libfsref.so"):
+    """Whole reference timesteps, timed on the host: for each sample grid m
+    the rising-bubble scene is injected into the reference's own solver
+    (oracle/_ref, built from the reference sources) and
+    SIMULATION_WORLD::AdvanceOneFrame (SIMULATION_WORLD.h:320) runs one
+    untimed frame, then up to `frames` timed frames within budget_s seconds:
+    dt from the reference's CFL condition, three RK stages of WENO5 velocity
+    advection, gravity, its air/water viscosity and a projection whose PCG
+    runs to convergence, WENO5 level set and Sussman reinitialisation, all
+    in the reference's FP64 code on one thread.  Runs in a child process
+    (the reference calls exit() on some inputs and holds ~2.3 kB of host
+    memory per cell).  Returns {m: {"ms": [...], "pcg_iterations": [...]}}."""
+    code = ("import json, sys; sys.path.insert(0, %r); import bench; "
+            "print('REFJSON' + json.dumps(bench._reference_frames_here(%r, %d, %r)))"
+            % (ROOT, list(sizes), frames, float(budget_s)))
+    env = dict(os.environ, FSREF_LIB=lib_name)
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, timeout=1800, env=env)
+    for line in p.stdout.splitlines():
+        if line.startswith("REFJSON"):
+            return {int(k): v for k, v in json.loads(line[7:]).items()}
+    raise RuntimeError(f"reference frames failed (rc={p.returncode}): {p.stderr.strip()[-300:]}")
+
+
+def _reference_frames_here(sizes, frames, budget_s):
+    import shutil
+    import tempfile
 
     from oracle import refsim
     if not refsim.available():
-        return None, "oracle/_ref/libfsref.so not built"
-    # the reference holds ~150 double fields of n^3; sample at a smaller grid
-    # and scale per cell when the host cannot hold the full one comfortably
-    need_gb = 2300 * n ** 3 / 1e9  # ~2.3 kB of host memory per cell (measured at 64^3)
-    # at most 128^3 (a bounded sample: per-cell costs scale to n^3; a smaller
-    # grid caches better, so the scaled time errs in the reference's favour)
-    m = min(n, 128)
-    while need_gb * (m / n) ** 3 > 0.5 * psutil.virtual_memory().available / 1e9 and m > 64:
-        m //= 2
-    scale = (n / m) ** 3
-    os.makedirs(os.path.join(ROOT, "_bench_tmp"), exist_ok=True)
-    phi, u, v, w = scene(m)
-    rng = np.random.default_rng(0)
-    u = rng.normal(size=u.shape) * 0.01; v = rng.normal(size=v.shape) * 0.01; w = rng.normal(size=w.shape) * 0.01
-    times = {}
-
-    def case(max_iteration, reinit_iterations=1):
-        path = refsim.write_sim(os.path.join(ROOT, "_bench_tmp", f"ref_{m}.sim"), m, water_drop=False, threads=threads,
-                                tolerance=1e-30, max_iteration=max_iteration, reinit_iterations=reinit_iterations)
-        c = refsim.RefCase(path)
-        for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
-            c.set(k, a)
-        return c
-
-    c = case(5)
-    t = time.perf_counter(); c.weno5_levelset(1e-4); times["weno_levelset"] = time.perf_counter() - t
-    t = time.perf_counter(); c.weno5_velocity(1e-4, 1); times["weno_velocity"] = time.perf_counter() - t
-    t = time.perf_counter(); c.viscosity(1e-4); times["viscosity"] = time.perf_counter() - t
-    for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
-        c.set(k, a)
-    t = time.perf_counter(); c.projection(1e-4); t5 = time.perf_counter() - t
-    t = time.perf_counter(); c.reinitialization(1e-4, 0); times["reinit_pseudo_step"] = time.perf_counter() - t
-    c.close()
-    c = case(15)
-    t = time.perf_counter(); c.projection(1e-4); t15 = time.perf_counter() - t
-    c.close()
-    per_it = max((t15 - t5) / 10.0, 0.0)
-    build = max(t5 - 5 * per_it, 0.0)
-    for f in os.listdir(os.path.join(ROOT, "_bench_tmp")):
-        os.remove(os.path.join(ROOT, "_bench_tmp", f))
-    os.rmdir(os.path.join(ROOT, "_bench_tmp"))
-    step_s = scale * (3 * times["weno_levelset"] + 3 * times["weno_velocity"] + 3 * times["viscosity"] +
-                      3 * (build + pcg_iterations_per_projection * per_it) + 3 * 10 * times["reinit_pseudo_step"])
-    sample = (f"reference operators on {threads} thread(s), timed once each at {m}^3 (cells scale x{scale:g} to {n}^3): WENO5 level set "
-              f"{times['weno_levelset']:.2f}s, WENO5 u,v,w {times['weno_velocity']:.2f}s, explicit viscosity "
-              f"{times['viscosity']:.2f}s, projection build {build:.2f}s + {per_it * 1e3:.1f} ms/PCG iteration, "
-              f"Sussman pseudo-step {times['reinit_pseudo_step']:.2f}s; scaled to 3 stages with "
-              f"{pcg_iterations_per_projection:.0f} PCG iterations per projection and 3x10 pseudo-steps")
-    return step_s * 1e3, sample
+        raise RuntimeError("oracle/_ref is not built")
+    out = {}
+    tmp = tempfile.mkdtemp(prefix="fs_ref_")
+    try:
+        for m in sizes:
+            path = refsim.write_sim(os.path.join(tmp, f"ref_{m}.sim"), m, water_drop=False, threads=1,
+                                    tolerance=reference_tolerance(m), max_iteration=100000)
+            c = refsim.RefCase(path)
+            phi, u, v, w = scene(m)
+            for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
+                c.set(k, a)
+            c.advance_frame()  # untimed
+            ms, its = [], []
+            t_start = time.perf_counter()
+            while len(ms) < frames and (not ms or time.perf_counter() - t_start < budget_s / len(sizes)):
+                t = time.perf_counter()
+                _, it = c.advance_frame()
+                ms.append((time.perf_counter() - t) * 1e3)
+                its.append(it)
+            c.close()
+            out[m] = {"ms": ms, "pcg_iterations": its}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
 
 
-# builds of the reference sources tried for the CPU baseline: the one the
-# goldens come from, and -O3 for x86-64-v3 (AVX2, FMA)
-REF_BUILDS = (("-O2", "libfsref.so"), ("-O3 -march=x86-64-v3", "libfsref_o3.so"))
-
-
-def reference_sample_best(n, iters):
-    """The reference's operators on 1, 2, 4 ... up to every host core (its
-    own MULTITHREADING domain decomposition), from each available build;
-    the fastest is the baseline."""
-    cores = os.cpu_count() or 1
-    cands = sorted({t for t in (1, 2, 4, 8, 16, 32, cores) if t <= cores})
-    best = (None, "reference sample failed", 1)
-    tried = []
-    for flags, name in REF_BUILDS:
-        if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", name)):
-            continue
-        for t in cands:
-            ms, sample = reference_sample_isolated(n, iters, t, name)
-            if ms is None:
-                tried.append(f"{flags} {t}: failed")
-                continue
-            tried.append(f"{flags} {t}: {ms / 1e3:.0f} s")
-            if best[0] is None or ms < best[0]:
-                best = (ms, f"build {flags}: " + sample, t)
-    ms, sample, t = best
-    return ms, (sample + "; step estimate per build and thread count: " + ", ".join(tried)), t
-
-
-def reference_sample_isolated(n, iters, threads=1, lib="libfsref.so"):
-    """reference_sample in a child process: the reference calls exit() on
-    some inputs (LEVELSET_3D.h:1040-1044) and holds tens of GB of host
-    memory at 256^3; neither should touch the benchmark process (nor an
-    instruction the host lacks, for the x86-64-v3 build)."""
-    code = ("import json, sys; sys.path.insert(0, %r); import bench; "
-            "ms, sample = bench.reference_sample(%d, %r, %d); print('REFJSON' + json.dumps([ms, sample]))"
-            % (ROOT, n, float(iters), threads))
-    env = dict(os.environ, FSREF_LIB=lib)
-    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, timeout=1200, env=env)
-    for line in p.stdout.splitlines():
-        if line.startswith("REFJSON"):
-            return tuple(json.loads(line[7:]))
-    return None, f"reference sample failed (rc={p.returncode}): {p.stderr.strip()[-300:]}"
+def reference_estimate(n, sizes, frames, budget_s):
+    """The reference's step time at n^3 from whole reference frames at two
+    sample grids.  Per frame the reference does work proportional to the
+    cells (advection, viscosity, reinitialisation, system build) plus its
+    Jacobi-PCG, whose iteration count grows about linearly with n (714 vs
+    357 iterations at 64^3 and 32^3 on this scene), so t(m) = a m^3 + b m^4
+    is fitted through the two measured means and evaluated at n."""
+    import platform
+    res = reference_frames(sizes, frames, budget_s)
+    (m1, m2) = sizes
+    t1, t2 = float(np.mean(res[m1]["ms"])), float(np.mean(res[m2]["ms"]))
+    A = np.array([[m1 ** 3, m1 ** 4], [m2 ** 3, m2 ** 4]], dtype=float)
+    a, b = np.linalg.solve(A, np.array([t1, t2]))
+    if a < 0 or b < 0:  # noisy sample: fall back to the pure cell-count scaling of the larger grid
+        est, model = t2 * (n / m2) ** 3, f"t({m2}) x ({n}/{m2})^3"
+    else:
+        est, model = a * n ** 3 + b * n ** 4, "t(m) = a m^3 + b m^4 through both grids"
+    try:
+        cpu_model = next(l.split(":", 1)[1].strip() for l in open("/proc/cpuinfo") if l.startswith("model name"))
+    except Exception:
+        cpu_model = platform.processor() or "unknown"
+    frames_run = {m: len(res[m]["ms"]) for m in sizes}
+    sample = (f"whole reference frames (SIMULATION_WORLD::AdvanceOneFrame, FP64, PCG to an absolute tolerance "
+              f"matching 1e-6 relative on the first projection), 1 thread (with more threads a whole frame of the "
+              f"headless build does not finish); one untimed frame then {frames_run[m1]} timed at {m1}^3 "
+              f"(mean {t1:.0f} ms, PCG iterations {res[m1]['pcg_iterations']}) and {frames_run[m2]} timed at "
+              f"{m2}^3 (mean {t2:.0f} ms, PCG iterations {res[m2]['pcg_iterations']}); scaled to {n}^3 by {model}; "
+              f"host: {os.cpu_count()} logical cores, {cpu_model}")
+    return est, sample, frames_run
 
 
 def init_replicas(backend="nccl"):
@@ -348,7 +344,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--preconditioner", default="default", choices=sorted(PRECONDITIONER),
+                    help="pressure preconditioner of the FP32+refine path (the FP64 comparison stays Jacobi)")
     args = ap.parse_args()
+    global PRECOND_CHOICE
+    PRECOND_CHOICE = args.preconditioner
 
     # the reference arm is host work: its ranks meet over gloo and touch no GPU
     world, rank, local, dist, barrier, max_over_ranks = init_replicas("gloo" if args.impl == "reference" else "nccl")
@@ -364,15 +364,16 @@ def main():
             if dist is not None:
                 dist.destroy_process_group()
             return
-        # the FP64 PCG iteration count of this workload on the GPU path at the
-        # same tolerance (measured in the default run; see profiles/)
-        # (Jacobi-PCG iteration counts grow about linearly with n)
-        iters = float(os.environ.get("FS_REF_PCG_ITERATIONS", str(REF_PCG_ITERATIONS_256 * n / 256.0)))
-        ms, sample, threads = reference_sample_best(n, iters)
+        # whole reference frames at 32^3 and 64^3 (about two minutes on one
+        # host thread), scaled to n^3; the steps printed are the frames run
+        ms, sample, frames_run = reference_estimate(n, (32, 64), frames=max(1, args.steps), budget_s=150.0)
+        steps_run = sum(frames_run.values())
         line = {"impl": "reference", "metric": metric, "value": ms, "unit": "ms", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+                "steps": steps_run, "warmup": len(frames_run), "ms_per_step": ms, "higher_is_better": False,
                 "dtype": "f64", "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference", "sample": sample},
+                "steps_note": "timed reference frames per sample grid %s after one untimed frame each" % frames_run,
+                "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference", "sample": sample,
+                                 "host_cores": os.cpu_count()},
                 "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         if dist is not None:
@@ -395,7 +396,9 @@ def main():
     real_its = sum(r["pcg_iterations"] for r in reps)
     launches = sum(r["kernel_launches"] for r in reps)
     N = n ** 3
-    per_iter_s = pcg_ms / 1e3 / max(pcg_its, 1)
+    # device time of the pressure solves per real iteration (the launched
+    # count adds the idle tail of the last graph batch of each solve)
+    per_iter_s = pcg_ms / 1e3 / max(real_its, 1)
     bpu = BYTES_PER_UNKNOWN_PCG_FP32 if main_prec == fs.FS_PRECISION_FP32_REFINE else BYTES_PER_UNKNOWN_PCG_FP64
     achieved = bpu * N / per_iter_s / 1e9
     peaks = {}
@@ -427,10 +430,13 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        iters = fp64["pcg_iterations_per_step"] / 3.0 if fp64 else 400.0
-        ref_ms, sample, threads = reference_sample_best(n, iters)
-        if ref_ms is not None:
-            cpu = {"value": ref_ms, "unit": "ms", "cores": threads, "kind": "reference", "sample": sample}
+        # bounded sample (about 25 s of host work): whole frames at 32^3 and 48^3
+        try:
+            ref_ms, sample, _ = reference_estimate(n, (32, 48), frames=3, budget_s=40.0)
+            cpu = {"value": ref_ms, "unit": "ms", "cores": 1, "kind": "reference", "sample": sample,
+                   "host_cores": os.cpu_count()}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
     line = {
         "metric": metric, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -451,12 +457,16 @@ def main():
                      "pcg_ms": pcg_ms, "pcg_launched_iterations": pcg_its, "pcg_iterations": real_its},
         "fp64": fp64,
         "adjoint": adjoint,
-        "steps_detail": [{k: r[k] for k in ("ms", "pcg_iterations", "outer_iterations", "viscosity_iterations",
-                                             "max_rel_residual", "div_linf", "pcg_ms")} for r in reps],
+        "divergence": {"div_l2_last": reps[-1]["div_l2"], "div_linf_max": max(r["div_linf"] for r in reps),
+                       "max_rel_residual": max(r["max_rel_residual"] for r in reps)},
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
     if rank == 0:
+        # per-step detail on stderr; the one JSON line on stdout stays short
+        detail = [{k: r[k] for k in ("ms", "pcg_iterations", "outer_iterations", "viscosity_iterations",
+                                     "max_rel_residual", "div_l2", "div_linf", "pcg_ms")} for r in reps]
+        print(json.dumps({"steps_detail": detail}), file=sys.stderr)
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -357,6 +357,34 @@ int fsref_marching_cubes(void* h, double* xyz, double* nrm, int cap_v, int* tri,
   return nv;
 }
 
+// One frame of the reference application as its SIMULATION_MANAGER runs it
+// (SIMULATION_WORLD::AdvanceOneFrame, SIMULATION_WORLD.h:320-331): the
+// curvature, dt from the CFL condition on the head thread, then one whole
+// timestep (EULERIAN_FLUID_SOLVER_3D::AdvanceOneTimeStepThread) on every
+// thread of the world's MULTITHREADING, its pressure solves run to the
+// script's tolerance.  The level set's ghost layers are extrapolated in place
+// first so that the ghost fills read defined values.  Returns the PCG
+// iteration count of the frame's last pressure solve; *dt_out gets the dt
+// the frame used.  Used to time the reference's CPU step as a whole, with
+// number_of_threads = 1: with 2 or 4 threads a whole frame of this build
+// made no progress within a minute at 32^3 (the cause was not found; the
+// reference's barrier, MULTITHREADING.h:105-118, waits on its condition
+// without a predicate loop), while single operators run threaded.
+int fsref_advance_frame(void* h, double* dt_out) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  extrapolate_levelset_in_place(s);
+  c->world.AdvanceOneFrame();
+  if (dt_out) *dt_out = c->world.dt;
+  return s.water_projection->poisson_solver.linear_solver->num_iteration;
+}
+
+// The pressure solver's stopping tolerance (LINEAR_SOLVER::SetTolerance):
+// the reference stops its PCG when r.z < tolerance^2 (PCG_METHOD.cpp:87).
+void fsref_set_pressure_tolerance(void* h, double tol) {
+  static_cast<RefCase*>(h)->world.eulerian_solver.water_projection->poisson_solver.linear_solver->SetTolerance(tol);
+}
+
 void fsref_write_levelset(void* h, const char* path) {
   EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
   s.water_levelset->Write(path);

@@ -67,6 +67,9 @@ def _lib():
     lib.fsref_fast_sweeping.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.fsref_marching_cubes.restype = ctypes.c_int
     lib.fsref_marching_cubes.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip]
+    lib.fsref_advance_frame.restype = ctypes.c_int
+    lib.fsref_advance_frame.argtypes = [ctypes.c_void_p, _dp]
+    lib.fsref_set_pressure_tolerance.argtypes = [ctypes.c_void_p, ctypes.c_double]
     lib.fsref_linear_solve.restype = ctypes.c_int
     lib.fsref_linear_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _dp, _dp]
     return lib
@@ -324,6 +327,18 @@ class RefCase:
         a = np.empty(self.shape("phi"))
         self._lib.fsref_curvature(self.h, _ptr(a))
         return a
+
+    def advance_frame(self):
+        """SIMULATION_WORLD::AdvanceOneFrame: one whole reference timestep
+        with dt from its CFL condition.  Returns (dt, PCG iterations of the
+        frame's last pressure solve)."""
+        dt = ctypes.c_double()
+        it = self._quiet(self._lib.fsref_advance_frame, self.h, ctypes.byref(dt))
+        return dt.value, it
+
+    def set_pressure_tolerance(self, tol):
+        """The PCG stops when r.z < tol^2 (PCG_METHOD.cpp:87)."""
+        self._lib.fsref_set_pressure_tolerance(self.h, float(tol))
 
     def linear_solve(self, vals, cols, rowptr, b, x0):
         n = len(b)
