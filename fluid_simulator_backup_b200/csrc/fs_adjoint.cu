@@ -363,13 +363,16 @@ __global__ void k_adj_sign(const double* __restrict__ phi, const double* __restr
 
 // ---------------------------------------------------------------------------
 // Projection.  Forward (corrected mode): b = P0(-div u*/dt), A(phi) p = b,
-// val_f = u*_f - dt (p_c - p_n) / (rho_face dx) on interior faces,
+// val_f = u*_f - dt beta_f (p_c - p_n) / dx on interior faces (beta_f the
+// matrix's face coefficient),
 // out = c1 val (+ c0 base, handled by the caller).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double inv_rho_of(double phi, double rn, double rp) { return 1.0 / (phi <= 0.0 ? rn : rp); }
 
-// Per face: u*_bar = c1 out_bar; p_bar, phi_bar (interface faces) and the
-// density bars rho_bar[0] (negative phase), rho_bar[1] (positive).
+// Transpose of the corrected velocity update u_f -= dt inv_h beta_f (p_c - p_n)
+// (beta_f the pressure matrix's face coefficient, see k_velocity_correct):
+// in_bar = c1 out_bar; p, phi and density bars of the gradient term, beta's
+// derivatives as in k_adj_pressure_operator (the phase of each cell frozen).
 __global__ void k_adj_velcorr(const double* __restrict__ p, const double* __restrict__ phi,
                               const double* __restrict__ out_bar, double* __restrict__ in_bar, double* p_bar,
                               double* phi_bar, double* rho_bar, Lay Lf, Lay Lc, int axis, double inv_h, double dt,
@@ -387,30 +390,29 @@ __global__ void k_adj_velcorr(const double* __restrict__ p, const double* __rest
     if (vb != 0.0 && e > 0 && e < n) {
       const int64_t c = Lc.at(i, j, k);
       const int64_t step = axis == 0 ? 1 : (axis == 1 ? Lc.px : Lc.slab);
-      const double phc = phi[c], phn = phi[c - step];
+      const double pc = phi[c], pn = phi[c - step];
+      const double vc = inv_rho_of(pc, rn, rp), vn = inv_rho_of(pn, rn, rp);
+      const double ac = fabs(pc), an = fabs(pn);
       const double dp = p[c] - p[c - step];
-      // val = u* - dt dp inv_h / rho_face
-      if (phc * phn > 0.0) {
-        const double ir = inv_rho_of(phc, rn, rp);
-        const double g = -dt * inv_h * ir * vb;  // d val / d p_c
-        atomicAdd(&p_bar[c], g);
-        atomicAdd(&p_bar[c - step], -g);
-        // d val / d rho = dt dp inv_h / rho^2
-        const double drho = dt * dp * inv_h * ir * ir * vb;
-        if (phc <= 0.0) rbn += drho; else rbp += drho;
+      const bool same = (pc <= 0.0) == (pn <= 0.0);
+      const double beta = same ? vc : vc * vn * (an + ac) / (vn * ac + vc * an);
+      // val = u* - dt inv_h beta dp
+      const double g = -dt * inv_h * beta * vb;  // d val / d p_c
+      atomicAdd(&p_bar[c], g);
+      atomicAdd(&p_bar[c - step], -g);
+      const double gb = -dt * inv_h * dp * vb;   // d val / d beta
+      if (same) {
+        // beta = v of the common phase, dv/drho = -v^2
+        if (pc <= 0.0) rbn += gb * (-vc * vc); else rbp += gb * (-vc * vc);
       } else {
-        const double ef = 1.5 / inv_h, m = 0.5 * (phc + phn);
-        const double H = heaviside(m, ef);
-        const double rho_f = rn + (rp - rn) * H;
-        const double g = -dt * inv_h / rho_f * vb;
-        atomicAdd(&p_bar[c], g);
-        atomicAdd(&p_bar[c - step], -g);
-        const double drho_f = dt * dp * inv_h / (rho_f * rho_f) * vb;  // d val / d rho_f
-        const double dm = drho_f * (rp - rn) * heaviside_d(m, ef) * 0.5;
-        atomicAdd(&phi_bar[c], dm);
-        atomicAdd(&phi_bar[c - step], dm);
-        rbn += drho_f * (1.0 - H);
-        rbp += drho_f * H;
+        const double S = an + ac, D = vn * ac + vc * an, D2 = D * D;
+        const double dac = vc * vn * an * (vc - vn) / D2, dan = vc * vn * ac * (vn - vc) / D2;
+        atomicAdd(&phi_bar[c], gb * dac * (pc > 0.0 ? 1.0 : (pc < 0.0 ? -1.0 : 0.0)));
+        atomicAdd(&phi_bar[c - step], gb * dan * (pn > 0.0 ? 1.0 : (pn < 0.0 ? -1.0 : 0.0)));
+        const double dvc = vn * vn * S * ac / D2, dvn = vc * vc * S * an / D2;
+        const double bvc = gb * dvc * (-vc * vc), bvn = gb * dvn * (-vn * vn);
+        if (pc <= 0.0) rbn += bvc; else rbp += bvc;
+        if (pn <= 0.0) rbn += bvn; else rbp += bvn;
       }
     }
   }

@@ -505,7 +505,8 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
   if (sigma != 0.0) {
     fill_extrap<S>(phi, c->Lc, s);
     curvature<S>(phi, c->kappa, c->Lc, dx, (P.flags & FS_FLAG_CURVATURE_TYPO) ? 1 : 0, c->scalars + 13, s);
-    jump_rhs<S>(phi, c->kappa, sigma, c->b64, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials, c->tickets + 5,
+    jump_rhs<S>(phi, c->kappa, sigma, c->b64, c->Lc, dx, P.rho_neg, P.rho_pos, faithful ? 1 : 0, c->partials,
+                c->tickets + 5,
                 c->scalars + 0, s);
     kap = c->kappa;
     c->launches += 3;

@@ -148,10 +148,11 @@ void velocity_correct(T* f, const T* base, const double* p, const T* phi, const 
 template <class T>
 void curvature(const T* phi, double* kappa, const Lay& L, double dx, int typo, double* kmax, cudaStream_t s);
 // ghost-fluid jump terms of the pressure right-hand side (ghosts of phi filled);
+// walls: arms to the wall ghosts carry jumps too (the reference's system);
 // sum(b) of the result lands in sum_out
 template <class T>
 void jump_rhs(const T* phi, const double* kappa, double sigma, double* b, const Lay& Lc, double dx, double rho_neg,
-              double rho_pos, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s);
+              double rho_pos, int walls, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s);
 template <class T>
 void divergence_norms(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
                       double dx, double* partials, unsigned int* ticket, double* out2, cudaStream_t s);

@@ -183,11 +183,23 @@ __device__ __forceinline__ double heaviside_proj(double phi, double e) {
 
 // Pressure-gradient update of one face component.  Face (i,j,k) of
 // component `axis` lies between cell c = (i,j,k) and the cell n one step
-// back along the axis.  Same-side faces use the sharp 1/rho of cell c, faces
-// across the interface the smeared density of the face-averaged phi.  Wall
-// faces are left alone (corrected) - in faithful mode only w is updated and
-// the first cell's bottom face sees the zero ghost pressure.  Then the RK
-// combination out = c0*base + c1*f (skipped when c0 == 0).
+// back along the axis; wall faces are left alone.  Then the RK combination
+// out = c0*base + c1*f (skipped when c0 == 0).
+//
+// Corrected (the default): u_f -= dt beta_f (p_c - p_n +- a_f)/dx with the
+// pressure matrix's own face coefficient beta_f (POISSON_SOLVER_3D.h:1080-1085,
+// the same expression and operand order as k_pressure_faces) and, on faces
+// whose cells lie in different phases, the same interface jump a_f that the
+// right-hand side carries (+ when c is in the phi <= 0 phase).  The update
+// is then the discrete gradient the matrix was built from: the corrected
+// velocity's divergence is dt times the solve's residual, so it is
+// divergence free to the solve tolerance at the interface too.
+//
+// Faithful (FS_FLAG_FAITHFUL_PROJECTION, PROJECTION_3D.h:1099-1449): same-side
+// faces use the sharp 1/rho of cell c, faces with phi_c phi_n <= 0 the
+// smeared density of the face-averaged phi, only w is updated, and the first
+// cell's bottom face sees the zero ghost pressure.  This is not consistent
+// with the matrix, so the interface keeps a divergence residual there.
 template <class T>
 __global__ void k_velocity_correct(T* __restrict__ f, const T* __restrict__ base, const double* __restrict__ p,
                                    const T* __restrict__ phi, Lay Lf, Lay Lc, int axis, double inv_h, double dt,
@@ -198,12 +210,23 @@ __global__ void k_velocity_correct(T* __restrict__ f, const T* __restrict__ base
   double val = (double)f[fc];
   const int e = axis == 0 ? i : (axis == 1 ? j : k);
   const int n = axis == 0 ? Lc.nx : (axis == 1 ? Lc.ny : Lc.nz);
-  const bool update_axis = !faithful || axis == 2;
   const bool interior = e > 0 && e < n;
-  const bool quirk = faithful && axis == 2 && i == 0 && j == 0 && k == 0;
-  if (update_axis && (interior || quirk)) {
-    const int64_t c = Lc.at(i, j, k);
-    const int64_t step = axis == 0 ? 1 : (axis == 1 ? Lc.px : Lc.slab);
+  const int64_t c = Lc.at(i, j, k);
+  const int64_t step = axis == 0 ? 1 : (axis == 1 ? Lc.px : Lc.slab);
+  if (!faithful) {
+    if (interior) {
+      const double phc = (double)phi[c], phn = (double)phi[c - step];
+      const double vc = inv_rho(phi[c], rn, rp), vn = inv_rho(phi[c - step], rn, rp);
+      const double beta = face_beta(vn, vc, fabs(phn), fabs(phc));
+      double dp = p[c] - p[c - step];
+      if (kappa && (phc <= 0.0) != (phn <= 0.0)) {
+        const double jcc = sigma * kappa[c], jcn = sigma * kappa[c - step];
+        const double jump = (jcc * fabs(phn) + jcn * fabs(phc)) / (fabs(phn) + fabs(phc));
+        dp = phc <= 0.0 ? dp + jump : dp - jump;
+      }
+      val -= dt * dp * beta * inv_h;
+    }
+  } else if (axis == 2 && (interior || (i == 0 && j == 0 && k == 0))) {
     const double phc = (double)phi[c];
     // across the bottom wall the ghost phi is the linear extrapolation and
     // the ghost pressure is zero
@@ -293,14 +316,17 @@ __global__ void k_curvature(const T* __restrict__ phi, double* __restrict__ kapp
 // b_c = ((b_c - F_X) - F_Y) - F_Z with the ghost-fluid jump terms of the six
 // arms (jc_on_derivative = 0): an arm across the interface carries
 // +-inv_dx2 * a * beta, a = (jc_c |phi_n| + jc_n |phi_c|)/(|phi_c| + |phi_n|),
-// jc = sigma * kappa, + when the cell is in the phi <= 0 phase.  Arms to the
-// wall ghosts use the extrapolated ghost phi (the ghosts of phi must be
-// filled), jc = 0 and the cell's own 1/rho.  The last block stores sum(b) in
+// jc = sigma * kappa, + when the cell is in the phi <= 0 phase.  With walls
+// (the reference's system, POISSON_SOLVER_3D.h:1216-1328) arms to the wall
+// ghosts count too, with the extrapolated ghost phi (the ghosts of phi must
+// be filled), jc = 0 and the cell's own 1/rho; without (the corrected
+// projection) only arms to interior cells carry a jump, as only they have a
+// face whose velocity the update corrects.  The last block stores sum(b) in
 // sum_out for the mean removal.
 template <class T>
 __global__ void k_jump_rhs(const T* __restrict__ phi, const double* __restrict__ kappa, double sigma,
-                           double* __restrict__ b, Lay Lc, double rn, double rp, double inv2, double* partials,
-                           unsigned int* ticket, double* sum_out) {
+                           double* __restrict__ b, Lay Lc, double rn, double rp, double inv2, int walls,
+                           double* partials, unsigned int* ticket, double* sum_out) {
   double bs = 0.0;
   Cursor cur;
   for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
@@ -318,6 +344,7 @@ __global__ void k_jump_rhs(const T* __restrict__ phi, const double* __restrict__
       for (int side = 0; side < 2; ++side) {
         const int64_t nb = side == 0 ? c - step[a] : c + step[a];
         const bool ghost = side == 0 ? e[a] == 0 : e[a] == n[a] - 1;
+        if (ghost && !walls) continue;
         const double pn = (double)phi[nb], an = fabs(pn);
         const double vn = ghost ? vc : 1.0 / (pn <= 0.0 ? rn : rp);
         const double jn = ghost ? 0.0 : sigma * kappa[nb];
@@ -447,9 +474,9 @@ void curvature(const T* phi, double* kappa, const Lay& L, double dx, int typo, d
 
 template <class T>
 void jump_rhs(const T* phi, const double* kappa, double sigma, double* b, const Lay& Lc, double dx, double rho_neg,
-              double rho_pos, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s) {
+              double rho_pos, int walls, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s) {
   k_jump_rhs<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, kappa, sigma, b, Lc, rho_neg, rho_pos, 1.0 / (dx * dx),
-                                                       partials, ticket, sum_out);
+                                                       walls, partials, ticket, sum_out);
 }
 
 template <class T>
@@ -496,8 +523,8 @@ void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s)
                                     double, double, double, int, double, double, const double*, double,            \
                                     cudaStream_t);                                                                  \
   template void curvature<T>(const T*, double*, const Lay&, double, int, double*, cudaStream_t);                   \
-  template void jump_rhs<T>(const T*, const double*, double, double*, const Lay&, double, double, double, double*, \
-                            unsigned int*, double*, cudaStream_t);                                                  \
+  template void jump_rhs<T>(const T*, const double*, double, double*, const Lay&, double, double, double, int,    \
+                            double*, unsigned int*, double*, cudaStream_t);                                                  \
   template void divergence_norms<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,   \
                                     double, double*, unsigned int*, double*, cudaStream_t);                         \
   template void absmax3<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, double*, cudaStream_t); \

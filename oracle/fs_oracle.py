@@ -675,14 +675,16 @@ def curvature(phi, dx, typo=False):
     return kappa, kmax
 
 
-def jump_rhs(phi, jc, dx, rho_neg, rho_pos):
+def jump_rhs(phi, jc, dx, rho_neg, rho_pos, walls=True):
     """Sum over the six arms of the ghost-fluid jump terms F of the pressure
     right-hand side b = -div - F_X - F_Y - F_Z (POISSON_SOLVER_3D.h:1216-1328)
     with jc_on_derivative = 0: an arm whose two cells lie in different phases
     carries F = +-inv_dx2 * a * beta, a = (jc_c |phi_n| + jc_n |phi_c|) /
-    (|phi_c| + |phi_n|), + when the cell is in the phi <= 0 phase.  Arms to
-    the wall ghosts use the extrapolated ghost phi, jc = 0 and the clamped
-    1/rho.  Returns (F_X, F_Y, F_Z)."""
+    (|phi_c| + |phi_n|), + when the cell is in the phi <= 0 phase.  With
+    walls (the reference), arms to the wall ghosts use the extrapolated ghost
+    phi, jc = 0 and the clamped 1/rho; without (corrected), only arms between
+    two cells of the box carry a jump, as only they have a face the velocity
+    update corrects.  Returns (F_X, F_Y, F_Z)."""
     pg = extrapolate_ghosts(phi, 1)
     var = 1.0 / np.where(phi <= 0, rho_neg, rho_pos)
     vg = np.pad(var, 1, mode="edge")
@@ -709,6 +711,12 @@ def jump_rhs(phi, jc, dx, rho_neg, rho_pos):
                     beta = vc * vn * (an + ac) / (vn * ac + vc * an)
             f = np.where((pc <= 0) & (pn > 0), inv2 * a * beta,
                          np.where((pc > 0) & (pn <= 0), -inv2 * a * beta, 0.0))
+            if not walls:
+                ax = 2 - [i for i in range(3) if d[i] != 0][0]
+                sl = [slice(None)] * 3
+                sl[ax] = 0 if low else -1
+                f = f.copy()
+                f[tuple(sl)] = 0.0
             F.append(f)
         out.append(F[0] + F[1])
     return tuple(out)
@@ -717,15 +725,22 @@ def jump_rhs(phi, jc, dx, rho_neg, rho_pos):
 def velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode="corrected", jc=None):
     """UpdateVelocityByPressureGradientVariableDensity (PROJECTION_3D.h:1099-1449).
 
-    Same-side faces: u -= dt*(p_c - p_nb)/rho_c/dx with the sharp rho of the
-    cell on the face's + side.  Faces whose two cells have phi_c*phi_nb <= 0:
-    u -= dt*(p_c - p_nb -/+ jump)/rho_f/dx with rho_f the smeared density
-    (PROJECTION_3D Heaviside, eps = 1.5 dx) of the face-averaged phi.
+    faithful (the reference as it runs): same-side faces u -= dt*(p_c -
+    p_nb)/rho_c/dx with the sharp rho of the cell on the face's + side; faces
+    whose two cells have phi_c*phi_nb <= 0: u -= dt*(p_c - p_nb -/+ jump)/
+    rho_f/dx with rho_f the smeared density (PROJECTION_3D Heaviside, eps =
+    1.5 dx) of the face-averaged phi.  Only w is updated (the u and v branches
+    of the reference are gated on pipe-mode flags, :1188,1211,1297,1320) and
+    the bottom face of the first cell is updated against a zero ghost
+    pressure (bc*bc_d >= 0 holds for row index 0).
 
-    faithful: only w is updated (the u and v branches of the reference are
-    gated on pipe-mode flags, :1188,1211,1297,1320) and the bottom face of the
-    first cell is updated against a zero ghost pressure (bc*bc_d >= 0 holds
-    for row index 0).  corrected: u, v and w updated, wall faces untouched."""
+    corrected: u, v and w updated, wall faces untouched, every interior face
+    with the pressure matrix's own coefficient, u -= dt*beta_f*(p_c - p_nb
+    -/+ jump)/dx (beta_f of POISSON_SOLVER_3D.h:1080-1085 as face_betas
+    computes it; the jump on faces whose cells lie in different phases, - when
+    the cell on the face's + side has phi > 0).  This is the gradient the
+    matrix was built from, so the corrected velocity is divergence free to
+    the solve's residual, the interface included."""
     nz, ny, nx = phi.shape
     rho_c = np.where(phi <= 0, rho_neg, rho_pos)
     pg = extrapolate_ghosts(phi, 1)
@@ -733,8 +748,27 @@ def velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode="correct
     e = 1.5 * dx
     inv = 1.0 / dx
     out = [u.copy(), v.copy(), w.copy()]
-    axes = (2,) if mode == "faithful" else (0, 1, 2)
-    for axis in axes:
+    if mode != "faithful":
+        betas = face_betas(phi, rho_neg, rho_pos)[:3]
+        for axis in (0, 1, 2):
+            ax = 2 - axis
+            sl_c = [slice(None)] * 3; sl_n = [slice(None)] * 3
+            sl_c[ax] = slice(1, None); sl_n[ax] = slice(0, -1)
+            sl_c, sl_n = tuple(sl_c), tuple(sl_n)
+            ph_c, ph_n = phi[sl_c], phi[sl_n]
+            fs = [slice(None)] * 3
+            fs[ax] = slice(1, -1)
+            fs = tuple(fs)
+            beta = betas[axis][fs]
+            dp = p[sl_c] - p[sl_n]
+            with np.errstate(invalid="ignore", divide="ignore"):
+                jump = (jc[sl_c] * np.abs(ph_n) + jc[sl_n] * np.abs(ph_c)) / (np.abs(ph_n) + np.abs(ph_c))
+            cross = (ph_c <= 0) != (ph_n <= 0)
+            dp = np.where(cross, np.where(ph_c <= 0, dp + jump, dp - jump), dp)
+            f = out[axis]
+            f[fs] = f[fs] - dt * dp * beta * inv
+        return tuple(out)
+    for axis in (2,):
         ax = 2 - axis
         sl_c = [slice(None)] * 3; sl_n = [slice(None)] * 3
         sl_c[ax] = slice(1, None); sl_n[ax] = slice(0, -1)
@@ -757,20 +791,19 @@ def velocity_correction(u, v, w, p, phi, dx, dt, rho_neg, rho_pos, mode="correct
         fs = [slice(None)] * 3
         fs[ax] = slice(1, -1)
         f[tuple(fs)] = f[tuple(fs)] - upd
-        if mode == "faithful" and axis == 2:
-            # the first cell's bottom face against the zero ghost pressure
-            c = phi[0, 0, 0]; g = pg[0, 1, 1]
-            fphi = 0.5 * (c + g)
-            if c * g > 0:
-                f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0) * (1.0 / rho_c[0, 0, 0]) * inv
+        # the first cell's bottom face against the zero ghost pressure
+        c = phi[0, 0, 0]; g = pg[0, 1, 1]
+        fphi = 0.5 * (c + g)
+        if c * g > 0:
+            f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0) * (1.0 / rho_c[0, 0, 0]) * inv
+        else:
+            rf = mix(rho_neg, rho_pos, heaviside_projection(np.array(fphi), e))
+            # the ghost jump condition is 0 (jc_on_solution is zero outside the box)
+            jmp = (jc[0, 0, 0] * abs(g) + 0.0 * abs(c)) / (abs(g) + abs(c))
+            if c <= 0:
+                f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0 + jmp) * (1.0 / rf) * inv
             else:
-                rf = mix(rho_neg, rho_pos, heaviside_projection(np.array(fphi), e))
-                # the ghost jump condition is 0 (jc_on_solution is zero outside the box)
-                jmp = (jc[0, 0, 0] * abs(g) + 0.0 * abs(c)) / (abs(g) + abs(c))
-                if c <= 0:
-                    f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0 + jmp) * (1.0 / rf) * inv
-                else:
-                    f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0 - jmp) * (1.0 / rf) * inv
+                f[0, 0, 0] = f[0, 0, 0] - dt * (p[0, 0, 0] - 0.0 - jmp) * (1.0 / rf) * inv
     return tuple(out)
 
 
@@ -787,7 +820,7 @@ def projection(phi, u, v, w, dx, dt, rho_neg, rho_pos, tol, max_iter, mode="corr
     if sigma != 0.0:
         kappa, _ = curvature(phi, dx, curvature_typo)
         jc = sigma * kappa
-        FX, FY, FZ = jump_rhs(phi, jc, dx, rho_neg, rho_pos)
+        FX, FY, FZ = jump_rhs(phi, jc, dx, rho_neg, rho_pos, walls=(mode == "faithful"))
         b = ((-div - FX) - FY) - FZ
     else:
         b = -div
