@@ -87,6 +87,11 @@ struct fs_ctx {
   // pressure PCG in the solve precision V (double for FP64, float for FP32_REFINE)
   void *pax = nullptr, *pay = nullptr, *paz = nullptr, *pdiag = nullptr;
   unsigned short* pdinv = nullptr;  // bf16 1/diag: the Jacobi preconditioner of the FP32 pressure solve
+  // red-black reduced FP32 pressure solve (packed half layout Lh, fs_redblack.cu)
+  Lay Lh{};
+  double* rb_x = nullptr;          // black FP64 iterate
+  float *rb_r = nullptr, *rb_p = nullptr, *rb_q = nullptr, *rb_tau = nullptr;
+  unsigned short* rb_dinv = nullptr;  // black bf16 1/diag
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
   // viscosity systems, one per component (storage type S)
   void* vs[3][9] = {};  // ax, ay, az, diag, rhs, x, r, p, q
@@ -246,7 +251,8 @@ void apply_params(fs_ctx* c) {
 // Launch captured batches of kGraphIters iterations until the solver state
 // says stop (done != 0); one host check of the state per batch.
 template <class F>
-fs_status drive_pcg(fs_ctx* c, std::pair<int, const void*> key, F&& enqueue_iteration, int max_iter, bool timed) {
+fs_status drive_pcg(fs_ctx* c, std::pair<int, const void*> key, F&& enqueue_iteration, int max_iter, bool timed,
+                    int kernels_per_iteration = 3) {
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
     cudaGraph_t g;
@@ -266,7 +272,7 @@ fs_status drive_pcg(fs_ctx* c, std::pair<int, const void*> key, F&& enqueue_iter
     CK(cudaStreamSynchronize(c->stream));
     if (c->st_host->done) return FS_OK;
     CK(cudaGraphLaunch(it->second, c->stream));
-    c->launches += 3 * kGraphIters;
+    c->launches += (int64_t)kernels_per_iteration * kGraphIters;
     if (timed) c->pcg_launched_iterations += kGraphIters;
   }
   CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
@@ -524,21 +530,46 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
                         P.max_iteration, P.stop, &iters, &rel, &st));
     outer = 1;
   } else {
+    const bool rb = c->red_black;
     build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
                                       (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s,
-                                      c->lean ? c->pdinv : nullptr);
+                                      (c->lean || rb) ? c->pdinv : nullptr);
     Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
     A.flux32 = c->flux32;
     if (c->lean) A.dinv16 = c->pdinv;
-    const size_t vbytes = c->Lc.total * sizeof(float);
+    // red-black: the black Schur complement on the packed half layout, its
+    // Jacobi preconditioner the black cells' bf16 1/diag
+    RbOp R{(float*)c->pax, (float*)c->pay, (float*)c->paz, c->Lc, c->Lh, c->scalars + 12};
+    Op7<float> Ah{nullptr, nullptr, nullptr, nullptr, c->Lh};
+    Ah.dinv16 = c->rb_dinv;
+    if (rb) {
+      rb_gather<unsigned short, unsigned short>(c->pdinv, c->rb_dinv, c->Lc, c->Lh, s);
+      rb_gather<double, double>(c->p64, c->rb_x, c->Lc, c->Lh, s);  // the initial guess's black cells
+      c->launches += 2;
+    }
     double bb = 0.0;
     float *r32 = (float*)c->pr, *p32 = (float*)c->pp, *q32 = (float*)c->pq;
+    // the Krylov vectors of the chosen form
+    float* kr = rb ? c->rb_r : r32;
+    float* kp = rb ? c->rb_p : p32;
+    const Op7<float>& KA = rb ? Ah : A;
+    // red-black: p64 <- the black iterate, red cells eliminated in FP64
+    auto commit = [&]() {
+      if (!rb) return;
+      rb_commit<S>(phi, c->rb_x, c->b64, c->p64, c->Lc, c->Lh, dx, P.rho_neg, P.rho_pos, s);
+      c->launches += 1;
+    };
     // true FP64 residual b - A64 p64 with A64 evaluated from phi in FP64; its
-    // FP32 image lands in r32, the Krylov residual of the mixed solve
+    // FP32 image lands in r32 (red-black: its black cells in the packed
+    // residual), the Krylov residual of the mixed solve
     auto defect = [&](const float* x32, double* rel_out) -> fs_status {
       defect_residual<S>(phi, c->p64, x32, c->b64, nullptr, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
                          c->tickets + 2, c->scalars + 2, s);
       c->launches += 1;
+      if (rb) {
+        rb_gather<float, float>(r32, c->rb_r, c->Lc, c->Lh, s);
+        c->launches += 1;
+      }
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
@@ -552,18 +583,22 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       }
       return FS_OK;
     };
+    commit();
     CKS(defect(nullptr, &rel));
     st = PCG_CONVERGED;
     if (rel > P.tolerance) {
-      // Mixed-precision CG: the FP64 pressure p64 is the iterate; the face
-      // couplings, the residual r, the search direction p and q = A p are
-      // FP32 (the flux-form operator in FP32 arithmetic, Op7::flux32) and the
-      // Jacobi preconditioner is 1/diag in bf16: 64 bytes per unknown and
-      // iteration against 120 for the FP64 solve.  Every time the recursive residual drops by reliable_delta
-      // the true FP64 residual of p64 replaces it (reliable update), keeping
-      // the search direction; the recursion stops at the tolerance itself
-      // and the true residual decides.  A sequence whose true residual got
-      // worse is rolled back to the last accepted pressure and restarted.
+      // Mixed-precision CG: the FP64 pressure p64 (red-black: its black cells,
+      // packed) is the iterate; the face couplings, the residual r, the
+      // search direction p and q = A p are FP32 (the flux-form operator in
+      // FP32 arithmetic, Op7::flux32, or the red-black Schur complement in
+      // its offset form) and the Jacobi preconditioner is 1/diag in bf16: 64
+      // bytes per unknown and iteration (red-black: 56 at half the
+      // iterations) against 120 for the FP64 solve.  Every time the recursive
+      // residual drops by reliable_delta the true FP64 residual of p64
+      // replaces it (reliable update), keeping the search direction; the
+      // recursion stops at the tolerance itself and the true residual
+      // decides.  A sequence whose true residual got worse is rolled back to
+      // the last accepted pressure and restarted.
       const size_t pbytes = c->Lc.total * sizeof(double);
       CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
       PcgState init{};
@@ -575,24 +610,37 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       *c->st_host = init;
       CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
       CK(cudaEventRecord(c->evp0, s));
-      // r32 already holds the image of b - A p64: start the recursion from it
-      pcg_resume<float, float>(A, r32, p32, c->st, c->partials, 1, s);
+      // the residual already holds the image of b - A p64: start the recursion from it
+      pcg_resume<float, float>(KA, kr, kp, c->st, c->partials, 1, s);
       c->launches += 2;
       int failures = 0;
       double best = rel;
       for (;;) {
-        CKS(drive_pcg(c, std::make_pair(2, (const void*)nullptr),
-                      [&] { cg_iteration<float, double>(A, c->p64, r32, p32, q32, c->st, c->partials, s); },
-                      P.max_iteration, true));
+        if (rb) {
+          CKS(drive_pcg(c, std::make_pair(4, (const void*)nullptr),
+                        [&] {
+                          rb_iteration(R, Ah, c->rb_x, c->rb_r, c->rb_p, c->rb_q, c->rb_tau, c->st, c->partials, s);
+                        },
+                        P.max_iteration, true, 4));
+        } else {
+          CKS(drive_pcg(c, std::make_pair(2, (const void*)nullptr),
+                        [&] { cg_iteration<float, double>(A, c->p64, r32, p32, q32, c->st, c->partials, s); },
+                        P.max_iteration, true));
+        }
         const int status = c->st_host->status;
         iters = c->st_host->iter;
         const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
         double now = 0.0;
-        CKS(defect(nullptr, &now));  // r32 <- true residual of the current pressure
+        commit();
+        CKS(defect(nullptr, &now));  // residual <- true residual of the current pressure
         bool restart = false;
         if (!std::isfinite(now) || now > 100.0 * best) {
           // diverged (not a CG residual oscillation): back to the best pressure
           CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
+          if (rb) {
+            rb_gather<double, double>(c->p64, c->rb_x, c->Lc, c->Lh, s);
+            c->launches += 1;
+          }
           CKS(defect(nullptr, &now));
           restart = true;
           ++failures;
@@ -607,8 +655,8 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
         }
         rel = now;
         if (c->debug)
-          std::fprintf(stderr, "[fs] mixed solve: iteration %d, status %d, recursive %.3e, true %.3e, best %.3e%s\n",
-                       iters, status, recursive, now, best, restart ? ", restart" : "");
+          std::fprintf(stderr, "[fs] mixed solve%s: iteration %d, status %d, recursive %.3e, true %.3e, best %.3e%s\n",
+                       rb ? " (red-black)" : "", iters, status, recursive, now, best, restart ? ", restart" : "");
         if (now <= P.tolerance) { st = PCG_CONVERGED; break; }
         if (iters >= P.max_iteration || failures > 8) {
           // leave the best pressure found
@@ -617,7 +665,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
           st = PCG_MAXITER;
           break;
         }
-        pcg_resume<float, float>(A, r32, p32, c->st, c->partials, restart ? 1 : 0, s);
+        pcg_resume<float, float>(KA, kr, kp, c->st, c->partials, restart ? 1 : 0, s);
         c->launches += 2;
         CK(cudaGetLastError());
       }
@@ -1203,6 +1251,12 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
     if ((s = dalloc(c, &c->px, cv)) != FS_OK) return fail(s);
     if ((s = dalloc(c, &c->prhs, cv)) != FS_OK) return fail(s);
     if ((s = dalloc(c, (void**)&c->pdinv, c->Lc.total * sizeof(unsigned short))) != FS_OK) return fail(s);
+    c->Lh = make_half_lay(c->Lc);
+    const size_t hb = c->Lh.total;
+    if ((s = dalloc(c, (void**)&c->rb_x, hb * sizeof(double))) != FS_OK) return fail(s);
+    float** hv[] = {&c->rb_r, &c->rb_p, &c->rb_q, &c->rb_tau};
+    for (float** p : hv) if ((s = dalloc(c, (void**)p, hb * sizeof(float))) != FS_OK) return fail(s);
+    if ((s = dalloc(c, (void**)&c->rb_dinv, hb * sizeof(unsigned short))) != FS_OK) return fail(s);
   }
   if (prm.viscosity) {
     const size_t fb[3] = {ub, vb, wb};
@@ -1216,6 +1270,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   cg_prepare<float, float>();
   int nblk = std::max(pcg_blocks(c->Lu), std::max(pcg_blocks(c->Lv), pcg_blocks(c->Lw))) * 2 + 64;
   for (const Lay* L : {&c->Lc, &c->Lu, &c->Lv, &c->Lw}) nblk = std::max(nblk, cg_max_blocks(*L));
+  if (c->fp32) nblk = std::max(nblk, rb_blocks(c->Lh));
   if ((s = dalloc(c, (void**)&c->partials, (size_t)nblk * 3 * sizeof(double))) != FS_OK) return fail(s);
   if ((s = dalloc(c, (void**)&c->tickets, 8 * sizeof(unsigned int))) != FS_OK) return fail(s);
   if ((s = dalloc(c, (void**)&c->scalars, 16 * sizeof(double))) != FS_OK) return fail(s);

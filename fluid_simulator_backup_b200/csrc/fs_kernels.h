@@ -111,11 +111,43 @@ void pcg_init(const Op7<V>& A, const R* b, R* x, R* r, V* p, PcgState* st, doubl
 // update + beta, then x += alpha p and p = z + beta p in one pass over p.
 template <class V, class X>
 void cg_iteration(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+// The two pointwise kernels of cg_iteration alone (residual update, then the
+// deferred iterate update and the direction update), after a SpMV that set
+// alpha in the state.
+template <class V, class X>
+void cg_vector_updates(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
 // Occupancy queries that size cg_iteration's grids: call once per (V, X)
 // before the first iteration (outside stream capture).
 template <class V, class X> void cg_prepare();
 // Largest block count of the cg_iteration kernels on a layout (partial sums).
 int cg_max_blocks(const Lay& L);
+
+// ---- red-black reduced pressure solve (fs_redblack.cu)
+// The pressure operator's FP32 couplings (cell layout L) seen through the
+// packed half layout Lh of one colour: slot (h, j, k) holds the red cell at
+// i = 2h + ((j+k)&1) and the black cell at i = 2h + ((j+k+1)&1).
+struct RbOp {
+  const float* ax;
+  const float* ay;
+  const float* az;
+  Lay L;                  // cell layout of the couplings
+  Lay Lh;                 // packed layout of the colour vectors
+  const double* extra0;   // deflation term of the first (red) cell
+};
+Lay make_half_lay(const Lay& L);
+int rb_blocks(const Lay& Lh);
+// One CG iteration on the black Schur complement: red stage (tau), black
+// stage (q = S p, p.q, alpha), then cg_vector_updates on the packed black
+// vectors with Ah (layout Lh, dinv16 the packed black bf16 1/diag).
+void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
+                  PcgState* st, double* partials, cudaStream_t s);
+// p64 <- black cells from the packed iterate xh, red cells eliminated in FP64
+// from phi and b (the red rows of b - A p64 vanish)
+template <class T>
+void rb_commit(const T* phi, const double* xh, const double* b, double* p64, const Lay& L, const Lay& Lh, double dx,
+               double rho_neg, double rho_pos, cudaStream_t s);
+// packed black slots <- black cells of a cell-layout field
+template <class S, class D> void rb_gather(const S* full, D* half, const Lay& L, const Lay& Lh, cudaStream_t s);
 
 template <class V, class R = V>
 void pcg_resume(const Op7<V>& A, const R* r, V* p, PcgState* st, double* partials, int restart, cudaStream_t s);

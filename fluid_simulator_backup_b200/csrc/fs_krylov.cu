@@ -596,6 +596,13 @@ void cg_iteration(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double*
   const int kchunk = (L.nz + chunks - 1) / chunks;
   const dim3 sg(tx, ty, (L.nz + kchunk - 1) / kchunk);
   k_cg_spmv<V, spmv_minb<V>()><<<sg, dim3(32, 8, 1), 0, s>>>(A, p, q, st, partials, kchunk);
+  cg_vector_updates<V, X>(A, x, r, p, q, st, partials, s);
+}
+
+template <class V, class X>
+void cg_vector_updates(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s) {
+  const int* slot = g_cg_blocks[sizeof(X) == 8][sizeof(V) == 8];
+  const Lay& L = A.L;
   // pointwise kernels: grid-stride over the vectors, resident blocks only
   const int64_t nvec = (int64_t)((L.nx + 3) >> 2) * L.ny * L.nz;
   auto grid = [&](int per_sm) {
@@ -615,6 +622,8 @@ template void cg_iteration<double, double>(const Op7<double>&, double*, double*,
                                            double*, cudaStream_t);
 template void cg_iteration<float, float>(const Op7<float>&, float*, float*, float*, float*, PcgState*, double*,
                                          cudaStream_t);
+template void cg_vector_updates<float, double>(const Op7<float>&, double*, float*, float*, float*, PcgState*, double*,
+                                               cudaStream_t);
 
 #define FS_KINST(V, RT)                                                                                           \
   template void pcg_init<V, RT>(const Op7<V>&, const RT*, RT*, RT*, V*, PcgState*, double*, cudaStream_t);       \
