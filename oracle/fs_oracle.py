@@ -1012,6 +1012,108 @@ def viscosity_semi_implicit(phi, u, v, w, dx, dt, rho_neg, rho_pos, mu_neg, mu_p
     return tuple(out), iters
 
 
+def _explicit_face_update(axis, vel, rho_h, mu, dx, dt, faces, faithful):
+    """Explicit viscous increment of component `axis` on the faces listed in
+    `faces` (index arrays (k, j, i) into that component's array), from the
+    zero-ghosted velocities `vel` (each padded by one layer).
+
+    faithful: the expressions of VISCOSITY_3D.h:482-486 (x), 521-525 (y),
+    560-564 (z), operand for operand, including their velocity indices: the
+    y update reads w at (i,j,k) and (i,j-1,k) on its z+ edge and one level
+    lower on its z- edge, and the z update reads u at i (not i+1) on its x+
+    edge and v at j (not j+1) on its y+ edge.  corrected: the same
+    discretisation with every transposed-stress term on its own edge, as the
+    x update has it."""
+    K, J, I = faces
+    inv = 1.0 / dx
+    g = [vel[0], vel[1], vel[2]]
+
+    def at(comp, di, dj, dk):
+        return g[comp][K + 1 + dk, J + 1 + dj, I + 1 + di]
+
+    rh = rho_h[K, J, I]
+    m = [a[K, J, I] for a in mu]  # hi, lo, e1, e2, e3, e4 (viscosity_samples order)
+    coef = dt * (1.0 / rh)
+    if axis == 0:
+        u = at(0, 0, 0, 0)
+        first = 2.0 * coef * inv * (m[0] * inv * (at(0, 1, 0, 0) - u) - m[1] * inv * (u - at(0, -1, 0, 0)))
+        second = coef * inv * (m[2] * (inv * (at(0, 0, 1, 0) - u) + inv * (at(1, 0, 1, 0) - at(1, -1, 1, 0)))
+                               - m[3] * (inv * (u - at(0, 0, -1, 0)) + inv * (at(1, 0, 0, 0) - at(1, -1, 0, 0))))
+        third = coef * inv * (m[4] * (inv * (at(0, 0, 0, 1) - u) + inv * (at(2, 0, 0, 1) - at(2, -1, 0, 1)))
+                              - m[5] * (inv * (u - at(0, 0, 0, -1)) + inv * (at(2, 0, 0, 0) - at(2, -1, 0, 0))))
+        return u + ((first + second) + third)
+    if axis == 1:
+        v = at(1, 0, 0, 0)
+        first = coef * inv * (m[2] * (inv * (at(0, 1, 0, 0) - at(0, 1, -1, 0)) + inv * (at(1, 1, 0, 0) - v))
+                              - m[3] * (inv * (at(0, 0, 0, 0) - at(0, 0, -1, 0)) + inv * (v - at(1, -1, 0, 0))))
+        second = 2.0 * coef * inv * (m[0] * inv * (at(1, 0, 1, 0) - v) - m[1] * inv * (v - at(1, 0, -1, 0)))
+        zt = 0 if faithful else 1  # the w level of the z+ edge
+        third = coef * inv * (m[4] * (inv * (at(1, 0, 0, 1) - v) + inv * (at(2, 0, 0, zt) - at(2, 0, -1, zt)))
+                              - m[5] * (inv * (v - at(1, 0, 0, -1)) + inv * (at(2, 0, 0, zt - 1) - at(2, 0, -1, zt - 1))))
+        return v + ((first + second) + third)
+    w = at(2, 0, 0, 0)
+    xt = 0 if faithful else 1  # the u column of the x+ edge
+    yt = 0 if faithful else 1  # the v row of the y+ edge
+    first = coef * inv * (m[2] * (inv * (at(0, xt, 0, 0) - at(0, xt, 0, -1)) + inv * (at(2, 1, 0, 0) - w))
+                          - m[3] * (inv * (at(0, xt - 1, 0, 0) - at(0, xt - 1, 0, -1)) + inv * (w - at(2, -1, 0, 0))))
+    second = coef * inv * (m[4] * (inv * (at(1, 0, yt, 0) - at(1, 0, yt, -1)) + inv * (at(2, 0, 1, 0) - w))
+                           - m[5] * (inv * (at(1, 0, yt - 1, 0) - at(1, 0, yt - 1, -1)) + inv * (w - at(2, 0, -1, 0))))
+    third = 2.0 * coef * inv * (m[0] * inv * (at(2, 0, 0, 1) - w) - m[1] * inv * (w - at(2, 0, 0, -1)))
+    return w + ((first + second) + third)
+
+
+def explicit_viscosity(phi, u, v, w, dx, dt, rho_neg, rho_pos, mu_neg, mu_pos, faithful=False):
+    """The air/water viscosity of VISCOSITY_3D::ApplyViscosity
+    (VISCOSITY_3D.h:452-563): an explicit variable-viscosity stress update
+    with the smeared density of the face-averaged phi and the smeared
+    viscosity at the two cells across the face (normal stress) and at the
+    four edge averages (shear), Heaviside eps = 1.5 dx
+    (EULERIAN_FLUID_SOLVER_3D.h:394, VISCOSITY_3D.h:1234-1253).  Velocity
+    ghosts are zero; phi has one layer of linearly extrapolated ghosts.
+
+    faithful (the reference as it runs, one thread): x, then y, then z, each
+    updated in place in (k, j, i) order, so a face reads the already updated
+    x-1, y-1, z-1 neighbours of its own component and later components read
+    the earlier ones' new values; every face of the component is updated,
+    the wall faces included; the velocity indices of _explicit_face_update.
+    The in-place order is evaluated here by hyperplanes i+j+k = s (a face
+    depends on its own component only through hyperplane s-1), which reads
+    exactly what the sequential loop reads.
+
+    corrected: one explicit Euler step of the stress divergence from the
+    input velocities (no in-place order), transposed terms on their own
+    edges, wall-normal faces left as they are (no penetration)."""
+    nz, ny, nx = phi.shape
+    n = (nx, ny, nz)
+    e = 1.5 * dx
+    out = [np.array(u, dtype=float), np.array(v, dtype=float), np.array(w, dtype=float)]
+    src = [np.pad(a, 1) for a in out]
+    for axis in range(3):
+        half, n_hi, n_lo, e1, e2, e3, e4 = viscosity_samples(phi, axis)
+        rho_h = mix(rho_neg, rho_pos, heaviside_viscosity(half, e))
+        mu = [mix(mu_neg, mu_pos, heaviside_viscosity(a, e)) for a in (n_hi, n_lo, e1, e2, e3, e4)]
+        shp = face_shape(n, axis)
+        Kg, Jg, Ig = np.indices(shp)
+        if faithful:
+            vel = [np.pad(a, 1) for a in out]  # current values, earlier components updated
+            s_of = Kg + Jg + Ig
+            for s_ in range(int(s_of.max()) + 1):
+                sel = s_of == s_
+                faces = (Kg[sel], Jg[sel], Ig[sel])
+                vel[axis][faces[0] + 1, faces[1] + 1, faces[2] + 1] = _explicit_face_update(
+                    axis, vel, rho_h, mu, dx, dt, faces, True)
+            out[axis] = vel[axis][1:-1, 1:-1, 1:-1].copy()
+        else:
+            ax = 2 - axis
+            keep = (Kg, Jg, Ig)[ax]
+            inner = (keep > 0) & (keep < shp[ax] - 1)
+            faces = (Kg[inner], Jg[inner], Ig[inner])
+            res = out[axis].copy()
+            res[faces] = _explicit_face_update(axis, src, rho_h, mu, dx, dt, faces, False)
+            out[axis] = res
+    return tuple(out)
+
+
 # ----------------------------------------------------------------------------
 # CFL (EULERIAN_FLUID_SOLVER_3D.h:2673-2785)
 # ----------------------------------------------------------------------------

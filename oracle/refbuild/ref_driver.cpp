@@ -237,6 +237,35 @@ void fsref_viscosity(void* h, double dt) {
   });
 }
 
+// The same explicit update on fully defined inputs: the level set's first
+// ghost layer (edges and corners included) is set from phi_g, the caller's
+// one-layer ghosted copy ((n+2)^3 values, x fastest), and the first ghost
+// layer of each velocity component is zeroed, so that every value the
+// stencils read is given.  One thread.
+void fsref_viscosity_ghosted(void* h, const double* phi_g, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  FIELD_STRUCTURE_3D<T>& ls = s.water_levelset->signed_distance_field;
+  const GRID_STRUCTURE_3D& g = ls.grid;
+  long idx = 0;
+  for (int k = g.k_start - 1; k <= g.k_end + 1; ++k)
+    for (int j = g.j_start - 1; j <= g.j_end + 1; ++j)
+      for (int i = g.i_start - 1; i <= g.i_end + 1; ++i) ls.array_for_this(i, j, k) = phi_g[idx++];
+  FIELD_STRUCTURE_3D<T>* vel[3] = {s.water_velocity_field_mac_x, s.water_velocity_field_mac_y,
+                                   s.water_velocity_field_mac_z};
+  for (FIELD_STRUCTURE_3D<T>* f : vel) {
+    const GRID_STRUCTURE_3D& fg = f->grid;
+    for (int k = fg.k_start - 1; k <= fg.k_end + 1; ++k)
+      for (int j = fg.j_start - 1; j <= fg.j_end + 1; ++j)
+        for (int i = fg.i_start - 1; i <= fg.i_end + 1; ++i) {
+          const bool inside = i >= fg.i_start && i <= fg.i_end && j >= fg.j_start && j <= fg.j_end &&
+                              k >= fg.k_start && k <= fg.k_end;
+          if (!inside) f->array_for_this(i, j, k) = 0.0;
+        }
+  }
+  s.viscosity_solver->ApplyViscosity(0, s.epsilon_for_mollification, dt);
+}
+
 // Semi-implicit viscosity system for one MAC component through the reference
 // builder and linear solver (POISSON_SOLVER_3D.h:3359-3496 + selected solver):
 // (1 + sum c/dx^2) u_c - sum c_nb/dx^2 u_nb = explicit.  comp selects the

@@ -57,6 +57,7 @@ def _lib():
     lib.fsref_poisson_csr.argtypes = [ctypes.c_void_p, _dp, _ip, _ip, _dp, _dp]
     lib.fsref_divergence.argtypes = [ctypes.c_void_p, _dp]
     lib.fsref_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.fsref_viscosity_ghosted.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double]
     lib.fsref_semi_implicit_solve.restype = ctypes.c_int
     lib.fsref_semi_implicit_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
     lib.fsref_cfl.restype = ctypes.c_double
@@ -287,6 +288,15 @@ class RefCase:
 
     def viscosity(self, dt):
         self._lib.fsref_viscosity(self.h, dt)
+
+    def viscosity_ghosted(self, phi_ghosted, dt):
+        """VISCOSITY_3D::ApplyViscosity (air/water, explicit, in place) with
+        the level set's first ghost layer from phi_ghosted [(nz+2, ny+2,
+        nx+2)] and zero velocity ghosts."""
+        a = np.ascontiguousarray(phi_ghosted, dtype=np.float64)
+        nx, ny, nz = self.n
+        assert a.shape == (nz + 2, ny + 2, nx + 2)
+        self._lib.fsref_viscosity_ghosted(self.h, _ptr(a), float(dt))
 
     def semi_implicit_solve(self, comp, coef, explicit_term):
         name = {1: "u", 2: "v", 3: "w"}[comp]

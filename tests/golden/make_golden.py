@@ -29,6 +29,13 @@ on the air/water unit-cube box with Neumann pressure walls:
                    WriteOBJ runs it (after ComputeNormals): vertices, vertex
                    normals, triangles (1-based) of a sphere (16^3) and a
                    noisy scaled sphere (24^3)
+  explicit_viscosity_*  VISCOSITY_3D::ApplyViscosity, the air/water explicit
+                   in-place update (x, then y, then z), on a noisy sphere with
+                   random velocities, both phase conventions (10^3); the level
+                   set's first ghost layer is the oracle's linear
+                   extrapolation and the velocity ghosts are zero
+
+    python tests/golden/make_golden.py [name ...]   writes only the named fixtures
 """
 import os
 import sys
@@ -37,6 +44,7 @@ import numpy as np
 
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
 sys.path.insert(0, ROOT)
+from oracle import fs_oracle  # noqa: E402
 from oracle import refsim  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
@@ -215,7 +223,27 @@ def main():
         fixtures[name] = dict(n=n, dx=c.dx, phi=phi, xyz=xyz, normals=nrm, tri=tri)
         c.close()
 
+    # explicit air/water viscosity (its own seed: the fixtures above keep their draws)
+    vrng = np.random.default_rng(11)
+    n = 10
+    for name, water_drop in (("explicit_viscosity_drop", True), ("explicit_viscosity_bubble", False)):
+        c = case(n, water_drop=water_drop)
+        phi = sphere(n, (0.5, 0.45, 0.5), 0.3) + vrng.normal(size=(n, n, n)) * 0.02
+        vel = {k: vrng.normal(size=c.shape(k)) * 0.3 for k in "uvw"}
+        for k, a in vel.items():
+            c.set(k, a)
+        c.set("phi", phi)
+        c.viscosity_ghosted(fs_oracle.extrapolate_ghosts(phi, 1), 2e-3)
+        fixtures[name] = dict(n=n, dx=c.dx, dt=2e-3, rho_neg=1000.0 if water_drop else 1.0,
+                              rho_pos=1.0 if water_drop else 1000.0, mu_neg=1e-3 if water_drop else 1.8e-5,
+                              mu_pos=1.8e-5 if water_drop else 1e-3, phi=phi, **vel, out_u=c.get("u"),
+                              out_v=c.get("v"), out_w=c.get("w"))
+        c.close()
+
+    only = set(sys.argv[1:])
     for name, d in fixtures.items():
+        if only and name not in only:
+            continue
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **{k: np.asarray(v) for k, v in d.items()})
         print("wrote", name)
     for f in os.listdir(WORK):
