@@ -30,7 +30,8 @@ FIELD = {"phi": 0, "u": 1, "v": 2, "w": 3, "pressure": 4, "p": 4, "divergence": 
 FS_PRECISION_FP64, FS_PRECISION_FP32_REFINE = 0, 1
 FS_STOP_RELATIVE, FS_STOP_ABSOLUTE = 0, 1
 FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_FLAG_LEVELSET_FORWARD_EULER, FS_FLAG_CURVATURE_TYPO = 1, 2, 4, 8
-FS_FLAG_SORT_TYPO = 16
+FS_FLAG_SORT_TYPO, FS_FLAG_VISCOSITY_IN_PLACE = 16, 32
+FS_VISCOSITY_OFF, FS_VISCOSITY_SEMI_IMPLICIT, FS_VISCOSITY_EXPLICIT = 0, 1, 2
 FS_VELOCITY_WENO5, FS_VELOCITY_ENO3 = 0, 1
 FS_PRECOND_DEFAULT, FS_PRECOND_JACOBI, FS_PRECOND_JACOBI_BF16, FS_PRECOND_RED_BLACK = 0, 1, 2, 3
 

@@ -202,6 +202,10 @@ fs_status check_params(const fs_params* p) {
     set_error("velocity_epsilon must be finite and >= 0");
     return FS_INVALID_ARG;
   }
+  if (p->viscosity < 0 || p->viscosity > 2) {
+    set_error("viscosity must be 0 (off), 1 (semi-implicit) or 2 (explicit)");
+    return FS_INVALID_ARG;
+  }
   if (p->velocity_scheme != FS_VELOCITY_WENO5 && p->velocity_scheme != FS_VELOCITY_ENO3) {
     set_error("unknown velocity scheme %d", p->velocity_scheme);
     return FS_INVALID_ARG;
@@ -463,6 +467,21 @@ template <class S>
 fs_status viscosity_t(fs_ctx* c, double dt, int* iters_out) {
   const fs_params& P = c->prm;
   if (!P.viscosity) {
+    if (iters_out) *iters_out = 0;
+    return FS_OK;
+  }
+  if (P.viscosity == 2) {
+    // the reference's air/water explicit update (VISCOSITY_3D.h:452-563)
+    const int in_place = (P.flags & FS_FLAG_VISCOSITY_IN_PLACE) ? 1 : 0;
+    c->launches += viscosity_explicit<S>(F<S>(c->phi), F<S>(c->u), F<S>(c->v), F<S>(c->w), F<S>(c->ua), F<S>(c->va),
+                                         F<S>(c->wa), c->Lc, c->Lu, c->Lv, c->Lw, c->grid.dx, dt, P.rho_neg,
+                                         P.rho_pos, P.mu_neg, P.mu_pos, in_place, c->stream);
+    if (!in_place) {
+      std::swap(c->u, c->ua);
+      std::swap(c->v, c->va);
+      std::swap(c->w, c->wa);
+    }
+    CK(cudaGetLastError());
     if (iters_out) *iters_out = 0;
     return FS_OK;
   }
@@ -815,7 +834,9 @@ fs_status cfl_t(fs_ctx* c, double* dt) {
   const double c_f = (c->sc_host[8] * inv + c->sc_host[9] * inv) + c->sc_host[10] * inv;
   const double g_f = std::sqrt(std::fabs(P.gravity[1]) * inv);
   // semi-implicit viscosity imposes no limit; explicit (off) uses the reference's term
-  const double nu = P.viscosity ? 0.0 : std::max(P.mu_neg / P.rho_neg, P.mu_pos / P.rho_pos);
+  // semi-implicit viscosity imposes no limit; otherwise the reference's
+  // air/water term (EULERIAN_FLUID_SOLVER_3D.h:2765-2768)
+  const double nu = P.viscosity == 1 ? 0.0 : std::max(P.mu_neg / P.rho_neg, P.mu_pos / P.rho_pos);
   const double v_f = nu * ((2.0 * inv2 + 2.0 * inv2) + 2.0 * inv2);
   // surface tension (EULERIAN_FLUID_SOLVER_3D.h:2741-2745): sqrt(sigma kappa_max / (min rho dx^2))
   const double s_f = P.surface_tension != 0.0
@@ -1043,6 +1064,10 @@ fs_status adj_check(fs_ctx* c) {
     set_error("adjoints follow the corrected projection only");
     return FS_NOT_SUPPORTED;
   }
+  if (c->prm.viscosity == 2) {
+    set_error("adjoints cover the semi-implicit viscosity only");
+    return FS_NOT_SUPPORTED;
+  }
   return adj_alloc(c);
 }
 
@@ -1258,7 +1283,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
     for (float** p : hv) if ((s = dalloc(c, (void**)p, hb * sizeof(float))) != FS_OK) return fail(s);
     if ((s = dalloc(c, (void**)&c->rb_dinv, hb * sizeof(unsigned short))) != FS_OK) return fail(s);
   }
-  if (prm.viscosity) {
+  if (prm.viscosity == 1) {
     const size_t fb[3] = {ub, vb, wb};
     for (int a = 0; a < 3; ++a)
       for (int m = 0; m < 9; ++m)
@@ -1302,7 +1327,10 @@ fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
   if (!c || !p) { set_error("NULL argument"); return FS_INVALID_ARG; }
   CKS(check_params(p));
   if (p->precision != c->prm.precision) { set_error("precision is fixed at creation"); return FS_INVALID_ARG; }
-  if (p->viscosity && !c->prm.viscosity) { set_error("viscosity buffers were not allocated at creation"); return FS_INVALID_ARG; }
+  if (p->viscosity == 1 && !c->vs[0][0]) {
+    set_error("semi-implicit viscosity buffers were not allocated at creation");
+    return FS_INVALID_ARG;
+  }
   c->prm = *p;
   apply_params(c);
   // captured solver graphs hold the operator's arithmetic and preconditioner

@@ -201,6 +201,15 @@ void viscosity_system(const T* phi, const T* u, const T* v, const T* w, const La
                       const Lay& Lw, int axis, double dx, double dt, double rho_neg, double rho_pos, double mu_neg,
                       double mu_pos, T* ax, T* ay, T* az, T* diag, T* rhs, cudaStream_t s);
 
+// The reference's explicit air/water viscosity (VISCOSITY_3D.h:452-563).
+// in_place = 0: (ua, va, wa) <- the update of (u, v, w) (the caller swaps);
+// in_place = 1: u, v, w updated in place in the reference's order.  Returns
+// the number of kernels launched.
+template <class T>
+int viscosity_explicit(const T* phi, T* u, T* v, T* w, T* ua, T* va, T* wa, const Lay& Lc, const Lay& Lu,
+                       const Lay& Lv, const Lay& Lw, double dx, double dt, double rho_neg, double rho_pos,
+                       double mu_neg, double mu_pos, int in_place, cudaStream_t s);
+
 // ---- adjoint family (fs_adjoint.cu), FP64 only; all add into the bars
 void adj_weno_levelset(const double* src, const double* u, const double* v, const double* w, const double* out_bar,
                        double* src_bar, double* u_bar, double* v_bar, double* w_bar, const Lay& L, const Lay& Lu,

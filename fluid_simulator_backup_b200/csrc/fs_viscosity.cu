@@ -129,6 +129,165 @@ __global__ void k_visc_system(const T* __restrict__ phi, const T* __restrict__ u
   rhs[f] = (T)(rho_f * ex);
 }
 
+// ---------------------------------------------------------------------------
+// The reference's air/water viscosity: the explicit variable-viscosity stress
+// update of VISCOSITY_3D::ApplyViscosity (VISCOSITY_3D.h:452-563).  Per face
+// of component a: the smeared density of the face-averaged phi, the smeared
+// viscosity at the two cells across the face (normal stress, factor 2) and
+// at the four edge averages (shear), each sample summed in the reference's
+// operand order (VISCOSITY_3D.h:462-470, 502-510, 541-549).
+//
+// corrected (default): one explicit Euler step of the stress divergence from
+// the input velocities into separate output arrays, every transposed-stress
+// term on its own edge, wall-normal faces unchanged.  in_place
+// (FS_FLAG_VISCOSITY_IN_PLACE): as the reference runs on one thread - x,
+// then y, then z, each updated in place in (k, j, i) order, wall faces
+// included, with the reference's velocity indices (its y update reads w one
+// level low on both z edges, its z update reads u and v on the low edge's
+// column/row for the high edge too).  The in-place order is reproduced by
+// hyperplanes i + j + k = s: a face depends on its own component only through
+// its x-1, y-1, z-1 neighbours (hyperplane s-1, already updated) and x+1,
+// y+1, z+1 neighbours (s+1, not yet), so one launch per hyperplane reads
+// exactly what the sequential loop reads.
+// ---------------------------------------------------------------------------
+
+struct ExplicitViscosity {
+  Lay Lc, Lu, Lv, Lw;
+  int axis;
+  double inv_h, dt, rn, rp, mn, mp;
+};
+
+template <class T, bool IN_PLACE>
+__device__ __forceinline__ double explicit_visc_face(const ExplicitViscosity& X, const PhiX<T>& P, const T* u,
+                                                     const T* v, const T* w, int i, int j, int k) {
+  const double e = 1.5 / X.inv_h, inv = X.inv_h;
+  auto ph = [&](int di, int dj, int dk) { return P.at(i + di, j + dj, k + dk); };
+  double half, hi, lo, e1, e2, e3, e4;
+  if (X.axis == 0) {
+    half = 0.5 * (ph(-1, 0, 0) + ph(0, 0, 0));
+    hi = ph(0, 0, 0);
+    lo = ph(-1, 0, 0);
+    e1 = 0.25 * (((ph(-1, 0, 0) + ph(0, 0, 0)) + ph(-1, 1, 0)) + ph(0, 1, 0));
+    e2 = 0.25 * (((ph(-1, 0, 0) + ph(0, 0, 0)) + ph(-1, -1, 0)) + ph(0, -1, 0));
+    e3 = 0.25 * (((ph(-1, 0, 0) + ph(0, 0, 0)) + ph(-1, 0, 1)) + ph(0, 0, 1));
+    e4 = 0.25 * (((ph(-1, 0, 0) + ph(0, 0, 0)) + ph(-1, 0, -1)) + ph(0, 0, -1));
+  } else if (X.axis == 1) {
+    half = 0.5 * (ph(0, -1, 0) + ph(0, 0, 0));
+    hi = ph(0, 0, 0);
+    lo = ph(0, -1, 0);
+    e1 = 0.25 * (((ph(0, -1, 0) + ph(1, -1, 0)) + ph(0, 0, 0)) + ph(1, 0, 0));
+    e2 = 0.25 * (((ph(-1, -1, 0) + ph(0, -1, 0)) + ph(-1, 0, 0)) + ph(0, 0, 0));
+    e3 = 0.25 * (((ph(0, -1, 1) + ph(0, -1, 0)) + ph(0, 0, 1)) + ph(0, 0, 0));
+    e4 = 0.25 * (((ph(0, -1, -1) + ph(0, -1, 0)) + ph(0, 0, -1)) + ph(0, 0, 0));
+  } else {
+    half = 0.5 * (ph(0, 0, -1) + ph(0, 0, 0));
+    hi = ph(0, 0, 0);
+    lo = ph(0, 0, -1);
+    e1 = 0.25 * (((ph(0, 0, -1) + ph(1, 0, -1)) + ph(0, 0, 0)) + ph(1, 0, 0));
+    e2 = 0.25 * (((ph(0, 0, -1) + ph(-1, 0, -1)) + ph(0, 0, 0)) + ph(-1, 0, 0));
+    e3 = 0.25 * (((ph(0, 0, -1) + ph(0, 1, -1)) + ph(0, 0, 0)) + ph(0, 1, 0));
+    e4 = 0.25 * (((ph(0, 0, -1) + ph(0, -1, -1)) + ph(0, 0, 0)) + ph(0, -1, 0));
+  }
+  auto mu = [&](double p) { return X.mn + (X.mp - X.mn) * heaviside_visc(p, e); };
+  const double rho_h = X.rn + (X.rp - X.rn) * heaviside_visc(half, e);
+  const double m0 = mu(hi), m1 = mu(lo), m2 = mu(e1), m3 = mu(e2), m4 = mu(e3), m5 = mu(e4);
+  const T* comp[3] = {u, v, w};
+  const Lay lay[3] = {X.Lu, X.Lv, X.Lw};
+  auto at = [&](int c, int di, int dj, int dk) { return (double)comp[c][lay[c].at(i + di, j + dj, k + dk)]; };
+  const double coef = X.dt * (1.0 / rho_h);
+  if (X.axis == 0) {
+    const double uc = at(0, 0, 0, 0);
+    const double first = 2.0 * coef * inv * (m0 * inv * (at(0, 1, 0, 0) - uc) - m1 * inv * (uc - at(0, -1, 0, 0)));
+    const double second = coef * inv * (m2 * (inv * (at(0, 0, 1, 0) - uc) + inv * (at(1, 0, 1, 0) - at(1, -1, 1, 0))) -
+                                        m3 * (inv * (uc - at(0, 0, -1, 0)) + inv * (at(1, 0, 0, 0) - at(1, -1, 0, 0))));
+    const double third = coef * inv * (m4 * (inv * (at(0, 0, 0, 1) - uc) + inv * (at(2, 0, 0, 1) - at(2, -1, 0, 1))) -
+                                       m5 * (inv * (uc - at(0, 0, 0, -1)) + inv * (at(2, 0, 0, 0) - at(2, -1, 0, 0))));
+    return uc + ((first + second) + third);
+  }
+  if (X.axis == 1) {
+    const double vc = at(1, 0, 0, 0);
+    const int zt = IN_PLACE ? 0 : 1;  // the w level of the z+ edge
+    const double first = coef * inv * (m2 * (inv * (at(0, 1, 0, 0) - at(0, 1, -1, 0)) + inv * (at(1, 1, 0, 0) - vc)) -
+                                       m3 * (inv * (at(0, 0, 0, 0) - at(0, 0, -1, 0)) + inv * (vc - at(1, -1, 0, 0))));
+    const double second = 2.0 * coef * inv * (m0 * inv * (at(1, 0, 1, 0) - vc) - m1 * inv * (vc - at(1, 0, -1, 0)));
+    const double third =
+        coef * inv * (m4 * (inv * (at(1, 0, 0, 1) - vc) + inv * (at(2, 0, 0, zt) - at(2, 0, -1, zt))) -
+                      m5 * (inv * (vc - at(1, 0, 0, -1)) + inv * (at(2, 0, 0, zt - 1) - at(2, 0, -1, zt - 1))));
+    return vc + ((first + second) + third);
+  }
+  const double wc = at(2, 0, 0, 0);
+  const int xt = IN_PLACE ? 0 : 1, yt = IN_PLACE ? 0 : 1;  // the u column / v row of the high edges
+  const double first =
+      coef * inv * (m2 * (inv * (at(0, xt, 0, 0) - at(0, xt, 0, -1)) + inv * (at(2, 1, 0, 0) - wc)) -
+                    m3 * (inv * (at(0, xt - 1, 0, 0) - at(0, xt - 1, 0, -1)) + inv * (wc - at(2, -1, 0, 0))));
+  const double second =
+      coef * inv * (m4 * (inv * (at(1, 0, yt, 0) - at(1, 0, yt, -1)) + inv * (at(2, 0, 1, 0) - wc)) -
+                    m5 * (inv * (at(1, 0, yt - 1, 0) - at(1, 0, yt - 1, -1)) + inv * (wc - at(2, 0, -1, 0))));
+  const double third = 2.0 * coef * inv * (m0 * inv * (at(2, 0, 0, 1) - wc) - m1 * inv * (wc - at(2, 0, 0, -1)));
+  return wc + ((first + second) + third);
+}
+
+// corrected: out = the updated component from the input velocities
+template <class T>
+__global__ void k_visc_explicit(ExplicitViscosity X, const T* __restrict__ phi, const T* __restrict__ u,
+                                const T* __restrict__ v, const T* __restrict__ w, T* __restrict__ out) {
+  const Lay& Lf = X.axis == 0 ? X.Lu : (X.axis == 1 ? X.Lv : X.Lw);
+  FS_IJK(Lf);
+  const int64_t f = Lf.at(i, j, k);
+  const int e = X.axis == 0 ? i : (X.axis == 1 ? j : k);
+  const int n = X.axis == 0 ? Lf.nx : (X.axis == 1 ? Lf.ny : Lf.nz);
+  const T* comp = X.axis == 0 ? u : (X.axis == 1 ? v : w);
+  if (e == 0 || e == n - 1) {
+    out[f] = comp[f];
+    return;
+  }
+  out[f] = (T)explicit_visc_face<T, false>(X, PhiX<T>{phi, X.Lc}, u, v, w, i, j, k);
+}
+
+// in place: the faces of hyperplane i + j + k = s of component X.axis
+template <class T>
+__global__ void k_visc_explicit_plane(ExplicitViscosity X, const T* __restrict__ phi, T* u, T* v, T* w, int s) {
+  const Lay& Lf = X.axis == 0 ? X.Lu : (X.axis == 1 ? X.Lv : X.Lw);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = s - j - k;
+  if (j >= Lf.ny || k >= Lf.nz || i < 0 || i >= Lf.nx) return;
+  T* comp = X.axis == 0 ? u : (X.axis == 1 ? v : w);
+  comp[Lf.at(i, j, k)] = (T)explicit_visc_face<T, true>(X, PhiX<T>{phi, X.Lc}, u, v, w, i, j, k);
+}
+
+template <class T>
+int viscosity_explicit(const T* phi, T* u, T* v, T* w, T* ua, T* va, T* wa, const Lay& Lc, const Lay& Lu,
+                       const Lay& Lv, const Lay& Lw, double dx, double dt, double rho_neg, double rho_pos,
+                       double mu_neg, double mu_pos, int in_place, cudaStream_t s) {
+  ExplicitViscosity X{Lc, Lu, Lv, Lw, 0, 1.0 / dx, dt, rho_neg, rho_pos, mu_neg, mu_pos};
+  int launches = 0;
+  T* outs[3] = {ua, va, wa};
+  const Lay* lays[3] = {&Lu, &Lv, &Lw};
+  for (int a = 0; a < 3; ++a) {
+    X.axis = a;
+    const Lay& Lf = *lays[a];
+    if (in_place) {
+      const dim3 blk(32, 8, 1), grd((Lf.ny + 31) / 32, (Lf.nz + 7) / 8, 1);
+      const int planes = Lf.nx + Lf.ny + Lf.nz - 2;
+      for (int p = 0; p < planes; ++p) k_visc_explicit_plane<T><<<grd, blk, 0, s>>>(X, phi, u, v, w, p);
+      launches += planes;
+    } else {
+      Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
+      k_visc_explicit<T><<<g.grid, g.block, 0, s>>>(X, phi, u, v, w, outs[a]);
+      launches += 1;
+    }
+  }
+  return launches;
+}
+
+template int viscosity_explicit<float>(const float*, float*, float*, float*, float*, float*, float*, const Lay&,
+                                       const Lay&, const Lay&, const Lay&, double, double, double, double, double,
+                                       double, int, cudaStream_t);
+template int viscosity_explicit<double>(const double*, double*, double*, double*, double*, double*, double*,
+                                        const Lay&, const Lay&, const Lay&, const Lay&, double, double, double, double,
+                                        double, double, int, cudaStream_t);
+
 template <class T>
 void viscosity_system(const T* phi, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
                       const Lay& Lw, int axis, double dx, double dt, double rho_neg, double rho_pos, double mu_neg,

@@ -138,7 +138,8 @@ def params_from_block(block, base_grid):
         max_iteration=proj.GetInteger("max_iteration", 30),
         inner_tolerance=proj.GetFloat("inner_tolerance", 1e-2),
         max_outer=proj.GetInteger("max_outer", 20),
-        viscosity=1 if block.GetBoolean("semi_implicit_approach", True) else 0,
+        # semi_implicit_approach = false: the reference's air/water explicit update
+        viscosity=1 if block.GetBoolean("semi_implicit_approach", True) else 2,
         viscosity_tolerance=block.GetFloat("viscosity_tolerance", 1e-8),
         flags=0 if block.GetBoolean("corrected_projection", True) else FS_FLAG_FAITHFUL_PROJECTION,
         surface_tension=block.GetFloat("surface_tension", 0.0),

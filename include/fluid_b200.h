@@ -84,8 +84,11 @@ enum {
   FS_FLAG_LEVELSET_FORWARD_EULER = 1 << 2, /* order 3 advances phi by one Euler step (EULERIAN_FLUID_SOLVER_3D.h:1010) */
   FS_FLAG_CURVATURE_TYPO = 1 << 3, /* curvature as the reference computes it: factor 2 missing on py*pz*pyz and dz
                                       for 1/dz in the zero-gradient fallback (LEVELSET_3D.h:1033,1037) */
-  FS_FLAG_SORT_TYPO = 1 << 4       /* fast sweeping with the reference's INCREASING_SORT3, whose c < b < a branch
+  FS_FLAG_SORT_TYPO = 1 << 4,      /* fast sweeping with the reference's INCREASING_SORT3, whose c < b < a branch
                                       leaves a2 stale (MACROS.h:61-68); sweeps then run sequentially */
+  FS_FLAG_VISCOSITY_IN_PLACE = 1 << 5 /* explicit viscosity as the reference runs it: x, then y, then z, in place
+                                         in (k, j, i) order, wall faces included, its shear-term velocity indices
+                                         (VISCOSITY_3D.h:452-563) */
 };
 
 typedef struct {
@@ -108,7 +111,8 @@ typedef struct {
   double inner_tolerance;           /* FP32_REFINE: residual reduction one FP32 Krylov sequence is trusted
                                        for before it restarts from the FP64 residual (default 1e-3) */
   int max_outer;                    /* FP32_REFINE: unused (kept for layout); the iteration cap applies */
-  int viscosity;                    /* 0: off, 1: semi-implicit */
+  int viscosity;                    /* 0: off, 1: semi-implicit, 2: explicit (the reference's air/water update,
+                                       VISCOSITY_3D.h:452-563; its dt limit enters fs_cfl_dt) */
   double viscosity_tolerance;       /* relative residual of each viscosity solve */
   int viscosity_max_iteration;
   double cfl;                       /* CFL number used by fs_cfl_dt */

@@ -357,7 +357,8 @@ inline fs_params params_from_block(const SCRIPT_BLOCK& block, const GRID_STRUCTU
   p.max_iteration = proj.GetInteger("max_iteration", 30);
   p.inner_tolerance = proj.GetFloat("inner_tolerance", 1e-2);
   p.max_outer = proj.GetInteger("max_outer", 20);
-  p.viscosity = block.GetBoolean("semi_implicit_approach", true) ? 1 : 0;
+  // semi_implicit_approach = false: the reference's air/water explicit update
+  p.viscosity = block.GetBoolean("semi_implicit_approach", true) ? 1 : 2;
   p.viscosity_tolerance = block.GetFloat("viscosity_tolerance", 1e-8);
   p.flags = block.GetBoolean("corrected_projection", true) ? 0 : FS_FLAG_FAITHFUL_PROJECTION;
   p.surface_tension = block.GetFloat("surface_tension", 0.0);

@@ -1175,7 +1175,8 @@ def step(phi, u, v, w, dx, dt, P, p0=None, order=3):
     w); reinitialisation as the reference's RK3 of reinitialisation blocks
     (EULERIAN_FLUID_SOLVER_3D.h:1081-1109).  P is a dict with rho_neg,
     rho_pos, mu_neg, mu_pos, gravity, eps, reinit_iterations, reinit_scaling,
-    tol, max_iter, viscosity (bool), visc_tol.  Returns (phi, u, v, w, p, info)."""
+    tol, max_iter, viscosity (bool, or "explicit" for the reference's air/water
+    update, with viscosity_in_place for its in-place order), visc_tol.  Returns (phi, u, v, w, p, info)."""
     eps = P["eps"]
     L = lambda f: weno5_levelset(f, u, v, w, dx, dt, eps)
     phi1 = L(phi)
@@ -1192,7 +1193,10 @@ def step(phi, u, v, w, dx, dt, P, p0=None, order=3):
         a = eno3_velocity(*vel, dx, dt) if P.get("velocity_eno3", False) else weno5_velocity(*vel, dx, dt, eps)
         a = zero_walls(*a)
         a = add_gravity(*a, P["gravity"], dt)
-        if P.get("viscosity", True):
+        if P.get("viscosity", True) == "explicit":
+            a = explicit_viscosity(phin, *a, dx, dt, P["rho_neg"], P["rho_pos"], P["mu_neg"], P["mu_pos"],
+                                   faithful=P.get("viscosity_in_place", False))
+        elif P.get("viscosity", True):
             a, _ = viscosity_semi_implicit(phin, *a, dx, dt, P["rho_neg"], P["rho_pos"], P["mu_neg"], P["mu_pos"],
                                            P["visc_tol"], 10000, "rel")
         uu, vv, ww, p, pi = projection(phin, *a, dx, dt, P["rho_neg"], P["rho_pos"], P["tol"], P["max_iter"],
