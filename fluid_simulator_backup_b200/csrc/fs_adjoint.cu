@@ -1,4 +1,7 @@
-// Adjoint (vector-Jacobian) kernels of the timestep's operators, FP64.
+// Adjoint (vector-Jacobian) kernels of the timestep's operators.  The
+// primal fields they read (the forward's states, type T) are FP64 or FP32
+// (the FP32 context's storage); the bars are FP64 always and every
+// derivative is evaluated and accumulated in FP64.
 //
 // Each kernel takes the bar (adjoint) of an operator's output and adds the
 // bars of its inputs.  The discrete operators are differentiated exactly as
@@ -91,7 +94,8 @@ __device__ __forceinline__ void weno_pair_bar(const double f[7], double inv_h, d
   }
 }
 
-__device__ __forceinline__ void load7(const double* f, int64_t c, int64_t st, double out[7]) {
+template <class T>
+__device__ __forceinline__ void load7(const T* f, int64_t c, int64_t st, double out[7]) {
 #pragma unroll
   for (int s = 0; s < 7; ++s) out[s] = f[c + (s - 3) * st];
 }
@@ -124,8 +128,9 @@ __device__ __forceinline__ double heaviside_d(double phi, double e) {
 // Level-set WENO5 update: fe = src - dt (uc D_x + vc D_y + wc D_z), out = c1 fe
 // (the RK base term is handled by the caller).  fe_bar = c1 * out_bar.
 // ---------------------------------------------------------------------------
-__global__ void k_adj_weno_levelset(const double* __restrict__ src, const double* __restrict__ u,
-                                    const double* __restrict__ v, const double* __restrict__ w,
+template <class T>
+__global__ void k_adj_weno_levelset(const T* __restrict__ src, const T* __restrict__ u,
+                                    const T* __restrict__ v, const T* __restrict__ w,
                                     const double* __restrict__ out_bar, double* src_bar, double* u_bar,
                                     double* v_bar, double* w_bar, Lay L, Lay Lu, Lay Lv, Lay Lw, double inv_h,
                                     double eps, double dt, double c1) {
@@ -134,9 +139,10 @@ __global__ void k_adj_weno_levelset(const double* __restrict__ src, const double
   const double fb = c1 * out_bar[c];
   if (fb == 0.0) return;
   atomicAdd(&src_bar[c], fb);
-  const double vel[3] = {(u[Lu.at(i + 1, j, k)] + u[Lu.at(i, j, k)]) * 0.5,
-                         (v[Lv.at(i, j + 1, k)] + v[Lv.at(i, j, k)]) * 0.5,
-                         (w[Lw.at(i, j, k + 1)] + w[Lw.at(i, j, k)]) * 0.5};
+  // the forward's cell velocity, summed in the storage type as the forward does
+  const double vel[3] = {(double)(u[Lu.at(i + 1, j, k)] + u[Lu.at(i, j, k)]) * 0.5,
+                         (double)(v[Lv.at(i, j + 1, k)] + v[Lv.at(i, j, k)]) * 0.5,
+                         (double)(w[Lw.at(i, j, k + 1)] + w[Lw.at(i, j, k)]) * 0.5};
   const int64_t st[3] = {1, L.px, L.slab};
   double* vb[3] = {u_bar, v_bar, w_bar};
   const Lay* lv[3] = {&Lu, &Lv, &Lw};
@@ -221,8 +227,9 @@ __global__ void k_adj_extrap(double* bar, Lay L) {
 // ---------------------------------------------------------------------------
 // MAC component WENO5 self-advection: out = comp - dt (uvel D_x + ...)
 // ---------------------------------------------------------------------------
-__global__ void k_adj_weno_mac(const double* __restrict__ comp, const double* __restrict__ u,
-                               const double* __restrict__ v, const double* __restrict__ w,
+template <class T>
+__global__ void k_adj_weno_mac(const T* __restrict__ comp, const T* __restrict__ u,
+                               const T* __restrict__ v, const T* __restrict__ w,
                                const double* __restrict__ out_bar, double* comp_bar, double* u_bar, double* v_bar,
                                double* w_bar, Lay Lc, Lay Lu, Lay Lv, Lay Lw, int axis, double inv_h, double eps,
                                double dt) {
@@ -232,7 +239,7 @@ __global__ void k_adj_weno_mac(const double* __restrict__ comp, const double* __
   if (ob == 0.0) return;
   atomicAdd(&comp_bar[c], ob);
   // the advecting velocity at this face and the faces it averages
-  const double* comps[3] = {u, v, w};
+  const T* comps[3] = {u, v, w};
   double* bars[3] = {u_bar, v_bar, w_bar};
   const Lay* lays[3] = {&Lu, &Lv, &Lw};
   const int e[3] = {i, j, k};
@@ -301,7 +308,8 @@ __device__ __forceinline__ double godunov_sel(double s, double dm, double dp, in
   return dp;
 }
 
-__global__ void k_adj_sussman(const double* __restrict__ src, const double* __restrict__ sgn,
+template <class T>
+__global__ void k_adj_sussman(const T* __restrict__ src, const T* __restrict__ sgn,
                               const double* __restrict__ out_bar, double* src_bar, double* sgn_bar, Lay L,
                               double inv_h, double eps, double dtau, double c1, int typo) {
   FS_IJK(L);
@@ -353,7 +361,8 @@ __global__ void k_adj_sussman(const double* __restrict__ src, const double* __re
 }
 
 // s = p / sqrt(p^2 + dx^2): p_bar += s_bar dx^2 / (p^2 + dx^2)^(3/2)
-__global__ void k_adj_sign(const double* __restrict__ phi, const double* __restrict__ sgn_bar, double* phi_bar, Lay L,
+template <class T>
+__global__ void k_adj_sign(const T* __restrict__ phi, const double* __restrict__ sgn_bar, double* phi_bar, Lay L,
                            double dx) {
   FS_IJK(L);
   const int64_t c = L.at(i, j, k);
@@ -373,7 +382,8 @@ __device__ __forceinline__ double inv_rho_of(double phi, double rn, double rp) {
 // (beta_f the pressure matrix's face coefficient, see k_velocity_correct):
 // in_bar = c1 out_bar; p, phi and density bars of the gradient term, beta's
 // derivatives as in k_adj_pressure_operator (the phase of each cell frozen).
-__global__ void k_adj_velcorr(const double* __restrict__ p, const double* __restrict__ phi,
+template <class T>
+__global__ void k_adj_velcorr(const double* __restrict__ p, const T* __restrict__ phi,
                               const double* __restrict__ out_bar, double* __restrict__ in_bar, double* p_bar,
                               double* phi_bar, double* rho_bar, Lay Lf, Lay Lc, int axis, double inv_h, double dt,
                               double rn, double rp, double c1) {
@@ -454,7 +464,8 @@ __global__ void k_adj_sum(const double* __restrict__ f, Lay L, double* partials,
 // faces and (cell 0) the deflation term.  A p = sum_f beta_f inv2 (p_c - p_n)
 // per face, beta = vc vn (ac + an) / (vn ac + vc an) with v = 1/rho of the
 // cell's phase and a = |phi|.
-__global__ void k_adj_pressure_operator(const double* __restrict__ phi, const double* __restrict__ lam,
+template <class T>
+__global__ void k_adj_pressure_operator(const T* __restrict__ phi, const double* __restrict__ lam,
                                         const double* __restrict__ p, double* phi_bar, double* rho_bar, Lay Lc,
                                         double rn, double rp, double inv2) {
   double rbn = 0.0, rbp = 0.0;
@@ -512,8 +523,9 @@ __global__ void k_adj_pressure_operator(const double* __restrict__ phi, const do
 //   lambda^T (dr/dtheta) - lambda^T (dM/dtheta) x.
 // ---------------------------------------------------------------------------
 namespace {
+template <class T>
 struct PhiXD {  // the forward kernel's one-layer extrapolated phi, with its transpose
-  const double* phi;
+  const T* phi;
   Lay L;
   __device__ int terms(int x, int n, int idx[2], double wt[2]) const {
     if (x < 0) { idx[0] = 0; idx[1] = 1; wt[0] = 2.0; wt[1] = -1.0; return 2; }
@@ -553,8 +565,9 @@ struct PhiXD {  // the forward kernel's one-layer extrapolated phi, with its tra
 };
 }  // namespace
 
-__global__ void k_adj_visc(const double* __restrict__ phi, const double* __restrict__ ug, const double* __restrict__ vg,
-                           const double* __restrict__ wg, const double* __restrict__ x, const double* __restrict__ lam,
+template <class T>
+__global__ void k_adj_visc(const T* __restrict__ phi, const T* __restrict__ ug, const T* __restrict__ vg,
+                           const T* __restrict__ wg, const T* __restrict__ x, const double* __restrict__ lam,
                            double* u_bar, double* v_bar, double* w_bar, double* phi_bar, double* rho_bar, Lay Lc,
                            Lay Lu, Lay Lv, Lay Lw, Lay Lf, int axis, double inv_h, double dt, double rn, double rp,
                            double mn, double mp) {
@@ -566,12 +579,12 @@ __global__ void k_adj_visc(const double* __restrict__ phi, const double* __restr
   const int n_ax = axis == 0 ? Lf.nx : (axis == 1 ? Lf.ny : Lf.nz);
   if (i < Lf.nx && j < Lf.ny && k < Lf.nz && !(e_ax == 0 || e_ax == n_ax - 1)) {
     const int64_t f = Lf.at(i, j, k);
-    const PhiXD P{phi, Lc};
+    const PhiXD<T> P{phi, Lc};
     const double e = 1.5 / inv_h, inv2 = inv_h * inv_h;
     const int ea[3] = {axis == 0, axis == 1, axis == 2};
     const int li = i - ea[0], lj = j - ea[1], lk = k - ea[2];
     const double lamf = lam[f], xf = x[f];
-    const double* comp[3] = {ug, vg, wg};
+    const T* comp[3] = {ug, vg, wg};
     double* cbar[3] = {u_bar, v_bar, w_bar};
     const Lay lay[3] = {Lu, Lv, Lw};
     // rho_f and its dependence
@@ -641,7 +654,7 @@ __global__ void k_adj_visc(const double* __restrict__ phi, const double* __restr
       }
       // right-hand side: explicit transpose terms for tangential d
       if (d != axis) {
-        const double* vt = comp[d];
+        const T* vt = comp[d];
         const Lay& Lt = lay[d];
         const int ti = di, tj = dj, tk = dk;
         const int64_t ia = Lt.at(i + ti, j + tj, k + tk), ib = Lt.at(i + ti - ea[0], j + tj - ea[1], k + tk - ea[2]);
@@ -695,12 +708,13 @@ __global__ void k_adj_axpy(double* out, const double* x, double a, Lay L) {
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-void adj_weno_levelset(const double* src, const double* u, const double* v, const double* w, const double* out_bar,
-                       double* src_bar, double* u_bar, double* v_bar, double* w_bar, const Lay& L, const Lay& Lu,
-                       const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c1, cudaStream_t s) {
+template <class T>
+void adj_weno_levelset(const T* src, const T* u, const T* v, const T* w, const double* out_bar, double* src_bar,
+                       double* u_bar, double* v_bar, double* w_bar, const Lay& L, const Lay& Lu, const Lay& Lv,
+                       const Lay& Lw, double dx, double eps, double dt, double c1, cudaStream_t s) {
   Launch3 g = launch3(L.nx, L.ny, L.nz, 32, 4, 2);
-  k_adj_weno_levelset<<<g.grid, g.block, 0, s>>>(src, u, v, w, out_bar, src_bar, u_bar, v_bar, w_bar, L, Lu, Lv, Lw,
-                                                 1.0 / dx, eps, dt, c1);
+  k_adj_weno_levelset<T><<<g.grid, g.block, 0, s>>>(src, u, v, w, out_bar, src_bar, u_bar, v_bar, w_bar, L, Lu, Lv,
+                                                    Lw, 1.0 / dx, eps, dt, c1);
 }
 
 void adj_extrap(double* bar, const Lay& L, cudaStream_t s) {
@@ -709,31 +723,35 @@ void adj_extrap(double* bar, const Lay& L, cudaStream_t s) {
   k_adj_extrap<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(bar, L);
 }
 
-void adj_weno_mac(const double* comp, const double* u, const double* v, const double* w, const double* out_bar,
-                  double* comp_bar, double* u_bar, double* v_bar, double* w_bar, const Lay& Lc, const Lay& Lu,
-                  const Lay& Lv, const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s) {
+template <class T>
+void adj_weno_mac(const T* comp, const T* u, const T* v, const T* w, const double* out_bar, double* comp_bar,
+                  double* u_bar, double* v_bar, double* w_bar, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+                  const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s) {
   Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz, 32, 4, 2);
-  k_adj_weno_mac<<<g.grid, g.block, 0, s>>>(comp, u, v, w, out_bar, comp_bar, u_bar, v_bar, w_bar, Lc, Lu, Lv, Lw,
-                                            axis, 1.0 / dx, eps, dt);
+  k_adj_weno_mac<T><<<g.grid, g.block, 0, s>>>(comp, u, v, w, out_bar, comp_bar, u_bar, v_bar, w_bar, Lc, Lu, Lv, Lw,
+                                               axis, 1.0 / dx, eps, dt);
 }
 
-void adj_sussman(const double* src, const double* sgn, const double* out_bar, double* src_bar, double* sgn_bar,
-                 const Lay& L, double dx, double eps, double dtau, double c1, int typo, cudaStream_t s) {
+template <class T>
+void adj_sussman(const T* src, const T* sgn, const double* out_bar, double* src_bar, double* sgn_bar, const Lay& L,
+                 double dx, double eps, double dtau, double c1, int typo, cudaStream_t s) {
   Launch3 g = launch3(L.nx, L.ny, L.nz, 32, 4, 2);
-  k_adj_sussman<<<g.grid, g.block, 0, s>>>(src, sgn, out_bar, src_bar, sgn_bar, L, 1.0 / dx, eps, dtau, c1, typo);
+  k_adj_sussman<T><<<g.grid, g.block, 0, s>>>(src, sgn, out_bar, src_bar, sgn_bar, L, 1.0 / dx, eps, dtau, c1, typo);
 }
 
-void adj_sign(const double* phi, const double* sgn_bar, double* phi_bar, const Lay& L, double dx, cudaStream_t s) {
+template <class T>
+void adj_sign(const T* phi, const double* sgn_bar, double* phi_bar, const Lay& L, double dx, cudaStream_t s) {
   Launch3 g = launch3(L.nx, L.ny, L.nz);
-  k_adj_sign<<<g.grid, g.block, 0, s>>>(phi, sgn_bar, phi_bar, L, dx);
+  k_adj_sign<T><<<g.grid, g.block, 0, s>>>(phi, sgn_bar, phi_bar, L, dx);
 }
 
-void adj_velcorr(const double* p, const double* phi, const double* out_bar, double* in_bar, double* p_bar,
-                 double* phi_bar, double* rho_bar, const Lay& Lf, const Lay& Lc, int axis, double dx, double dt,
-                 double rn, double rp, double c1, cudaStream_t s) {
+template <class T>
+void adj_velcorr(const double* p, const T* phi, const double* out_bar, double* in_bar, double* p_bar, double* phi_bar,
+                 double* rho_bar, const Lay& Lf, const Lay& Lc, int axis, double dx, double dt, double rn, double rp,
+                 double c1, cudaStream_t s) {
   Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
-  k_adj_velcorr<<<g.grid, g.block, 0, s>>>(p, phi, out_bar, in_bar, p_bar, phi_bar, rho_bar, Lf, Lc, axis, 1.0 / dx,
-                                           dt, rn, rp, c1);
+  k_adj_velcorr<T><<<g.grid, g.block, 0, s>>>(p, phi, out_bar, in_bar, p_bar, phi_bar, rho_bar, Lf, Lc, axis,
+                                              1.0 / dx, dt, rn, rp, c1);
 }
 
 void adj_divergence(const double* lam, const double* sum_lam, double* in_bar, const Lay& Lf, const Lay& Lc, int axis,
@@ -747,20 +765,22 @@ void adj_sum(const double* f, const Lay& L, double* partials, unsigned int* tick
   k_adj_sum<<<pcg_blocks(L), kRedThreads, 0, s>>>(f, L, partials, ticket, out);
 }
 
-void adj_pressure_operator(const double* phi, const double* lam, const double* p, double* phi_bar, double* rho_bar,
+template <class T>
+void adj_pressure_operator(const T* phi, const double* lam, const double* p, double* phi_bar, double* rho_bar,
                            const Lay& Lc, double dx, double rn, double rp, cudaStream_t s) {
   Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
-  k_adj_pressure_operator<<<g.grid, g.block, 0, s>>>(phi, lam, p, phi_bar, rho_bar, Lc, rn, rp, 1.0 / (dx * dx));
+  k_adj_pressure_operator<T><<<g.grid, g.block, 0, s>>>(phi, lam, p, phi_bar, rho_bar, Lc, rn, rp, 1.0 / (dx * dx));
 }
 
-void adj_visc(const double* phi, const double* ug, const double* vg, const double* wg, const double* x,
-              const double* lam, double* u_bar, double* v_bar, double* w_bar, double* phi_bar, double* rho_bar,
-              const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw, int axis, double dx, double dt, double rn,
-              double rp, double mn, double mp, cudaStream_t s) {
+template <class T>
+void adj_visc(const T* phi, const T* ug, const T* vg, const T* wg, const T* x, const double* lam, double* u_bar,
+              double* v_bar, double* w_bar, double* phi_bar, double* rho_bar, const Lay& Lc, const Lay& Lu,
+              const Lay& Lv, const Lay& Lw, int axis, double dx, double dt, double rn, double rp, double mn,
+              double mp, cudaStream_t s) {
   const Lay& Lf = axis == 0 ? Lu : (axis == 1 ? Lv : Lw);
   Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
-  k_adj_visc<<<g.grid, g.block, 0, s>>>(phi, ug, vg, wg, x, lam, u_bar, v_bar, w_bar, phi_bar, rho_bar, Lc, Lu, Lv, Lw,
-                                        Lf, axis, 1.0 / dx, dt, rn, rp, mn, mp);
+  k_adj_visc<T><<<g.grid, g.block, 0, s>>>(phi, ug, vg, wg, x, lam, u_bar, v_bar, w_bar, phi_bar, rho_bar, Lc, Lu, Lv,
+                                           Lw, Lf, axis, 1.0 / dx, dt, rn, rp, mn, mp);
 }
 
 void adj_zero_walls(double* f, const Lay& L, int axis, cudaStream_t s) {
@@ -772,5 +792,26 @@ void adj_axpy(double* out, const double* x, double a, const Lay& L, cudaStream_t
   Launch3 g = launch3(L.nx, L.ny, L.nz);
   k_adj_axpy<<<g.grid, g.block, 0, s>>>(out, x, a, L);
 }
+
+#define FS_ADJ_INST(T)                                                                                            \
+  template void adj_weno_levelset<T>(const T*, const T*, const T*, const T*, const double*, double*, double*,      \
+                                     double*, double*, const Lay&, const Lay&, const Lay&, const Lay&, double,       \
+                                     double, double, double, cudaStream_t);                                          \
+  template void adj_weno_mac<T>(const T*, const T*, const T*, const T*, const double*, double*, double*, double*,  \
+                                double*, const Lay&, const Lay&, const Lay&, const Lay&, int, double, double, double, \
+                                cudaStream_t);                                                                       \
+  template void adj_sussman<T>(const T*, const T*, const double*, double*, double*, const Lay&, double, double,     \
+                               double, double, int, cudaStream_t);                                                   \
+  template void adj_sign<T>(const T*, const double*, double*, const Lay&, double, cudaStream_t);                     \
+  template void adj_velcorr<T>(const double*, const T*, const double*, double*, double*, double*, double*,         \
+                               const Lay&, const Lay&, int, double, double, double, double, double, cudaStream_t);   \
+  template void adj_pressure_operator<T>(const T*, const double*, const double*, double*, double*, const Lay&,      \
+                                         double, double, double, cudaStream_t);                                      \
+  template void adj_visc<T>(const T*, const T*, const T*, const T*, const T*, const double*, double*, double*,      \
+                            double*, double*, double*, const Lay&, const Lay&, const Lay&, const Lay&, int, double,  \
+                            double, double, double, double, double, cudaStream_t);
+
+FS_ADJ_INST(float)
+FS_ADJ_INST(double)
 
 }  // namespace fsb

@@ -112,14 +112,21 @@ struct fs_ctx {
   float pcg_ms = 0.0f;
   int pcg_launched_iterations = 0;
   cudaEvent_t evp0 = nullptr, evp1 = nullptr;
-  // adjoint state (FP64 contexts; allocated on first use)
+  // adjoint state (bars FP64 in both precisions; allocated on first use)
   double* abar[4] = {};       // bars of phi, u, v, w (FS_FIELD_ADJ_*)
   double* awork_c[6] = {};    // cell work bars
   double* awork_f[4][3] = {}; // face work bar triples
   double* a_vlam[3] = {};     // viscosity: lambda per component
   double* a_vxb[3] = {};      // viscosity: x_bar per component
   double* a_rho = nullptr;    // device [4]: bars of rho_neg, rho_pos
-  std::vector<double*> tape_cells, tape_faces;  // taped forward states, allocated on demand
+  std::vector<void*> tape_cells, tape_faces;  // taped forward states (storage precision), allocated on demand
+  std::vector<double*> tape_p;                // taped stage pressures (FP64)
+  // FP64 operator and Krylov vectors of the adjoint solves: the forward's own
+  // buffers in FP64 contexts, separate ones in FP32 contexts (one viscosity
+  // system set shared by the three components there)
+  double *a_ax = nullptr, *a_ay = nullptr, *a_az = nullptr, *a_diag = nullptr;
+  double *a_r = nullptr, *a_p = nullptr, *a_q = nullptr;
+  double* a_vs[3][9] = {};
   // derived from fs_params by apply_params
   bool debug = false;           // params.verbose: solver progress on stderr
   double reliable_delta = 0.1;  // params.reliable_delta
@@ -132,13 +139,14 @@ struct fs_ctx {
 
 namespace {
 
-// Forward states kept for the adjoint of one step (FP64 contexts).  Each
-// pointer is a padded field of the context's layouts.
+// Forward states kept for the adjoint of one step.  Each pointer is a
+// padded field of the context's layouts in its storage precision; the
+// pressures are FP64.
 struct Tape {
-  double* ls[4] = {};                 // level set: the three RK stage inputs and the advected phi
-  double* vel[3][3][3] = {};          // [stage][0 input, 1 viscosity input, 2 projection input][component]
+  void* ls[4] = {};                   // level set: the three RK stage inputs and the advected phi
+  void* vel[3][3][3] = {};            // [stage][0 input, 1 viscosity input, 2 projection input][component]
   double* p[3] = {};                  // pressure of each stage's projection
-  std::vector<double*> re[3];         // [reinit block][pseudo-step]: input of each Sussman step
+  std::vector<void*> re[3];           // [reinit block][pseudo-step]: input of each Sussman step
 };
 
 fs_status dalloc(fs_ctx* c, void** out, size_t bytes) {
@@ -340,7 +348,7 @@ fs_status advect_levelset_t(fs_ctx* c, double dt, Tape* tp = nullptr) {
   int stage = 0;
   auto fe = [&](S* src, const S* base, S* out, double c0, double c1) {
     if (tp && stage < 3)
-      cudaMemcpyAsync(tp->ls[stage], src, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(tp->ls[stage], src, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s);
     ++stage;
     fill_extrap<S>(src, c->Lc, s);
     weno5_levelset<S>(src, base, out, u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, eps, dt, c0, c1, s);
@@ -358,7 +366,7 @@ fs_status advect_levelset_t(fs_ctx* c, double dt, Tape* tp = nullptr) {
     std::swap(c->s1, c->s2);
   }
   std::swap(c->phi, c->s1);
-  if (tp) CK(cudaMemcpyAsync(tp->ls[3], c->phi, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (tp) CK(cudaMemcpyAsync(tp->ls[3], c->phi, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s));
   CK(cudaGetLastError());
   return FS_OK;
 }
@@ -418,7 +426,7 @@ fs_status fast_sweeping_t(fs_ctx* c, const void* in, void* out, int direction, i
 
 template <class S>
 fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, double c1, void* scrA, void* scrB,
-                         std::vector<double*>* tape = nullptr) {
+                         std::vector<void*>* tape = nullptr) {
   const fs_params& P = c->prm;
   const double dx = c->grid.dx, dtau = dx / P.reinit_scaling;
   const int n = P.reinit_iterations;
@@ -439,7 +447,7 @@ fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, 
   for (int it = 0; it < n; ++it) {
     const bool last = it == n - 1;
     void* dst = last ? out : (cur == scrA ? scrB : scrA);
-    if (tape) CK(cudaMemcpyAsync((*tape)[it], cur, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (tape) CK(cudaMemcpyAsync((*tape)[it], cur, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s));
     fill_extrap<S>(F<S>(cur), c->Lc, s);
     sussman_step<S>(F<S>(cur), F<S>(c->sgn), F<S>(base), F<S>(dst), c->Lc, dx, P.weno_epsilon, dtau,
                     last ? c0 : 0.0, last ? c1 : 1.0, (P.flags & FS_FLAG_REINIT_TYPO) ? 1 : 0, s);
@@ -737,11 +745,11 @@ fs_status gravity_t(fs_ctx* c, double dt) {
 // gravity, viscosity, projection; the projection's velocity update also
 // applies the stage's RK combination with the step's initial velocity.
 // copy the three velocity components into a tape slot
-fs_status tape_velocity(fs_ctx* c, double* const dst[3]) {
+fs_status tape_velocity(fs_ctx* c, void* const dst[3]) {
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   void* comps[3] = {c->u, c->v, c->w};
   for (int a = 0; a < 3; ++a)
-    CK(cudaMemcpyAsync(dst[a], comps[a], lays[a]->total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst[a], comps[a], lays[a]->total * c->S(), cudaMemcpyDeviceToDevice, c->stream));
   return FS_OK;
 }
 
@@ -868,28 +876,50 @@ fs_status adj_alloc(fs_ctx* c) {
     CKS(dalloc(c, (void**)&c->a_vxb[a], fb[a]));
   }
   CKS(dalloc(c, (void**)&c->a_rho, 4 * sizeof(double)));
+  if (!c->fp32) {
+    c->a_ax = (double*)c->pax; c->a_ay = (double*)c->pay; c->a_az = (double*)c->paz; c->a_diag = (double*)c->pdiag;
+    c->a_r = (double*)c->pr; c->a_p = (double*)c->pp; c->a_q = (double*)c->pq;
+    for (int a = 0; a < 3; ++a)
+      for (int m = 0; m < 9; ++m) c->a_vs[a][m] = (double*)c->vs[a][m];
+  } else {
+    double** ops[] = {&c->a_ax, &c->a_ay, &c->a_az, &c->a_diag, &c->a_r, &c->a_p, &c->a_q};
+    for (double** p : ops) CKS(dalloc(c, (void**)p, cb));
+    if (c->prm.viscosity == 1) {
+      const size_t fmax = std::max(fb[0], std::max(fb[1], fb[2]));
+      for (int m = 0; m < 9; ++m) {
+        CKS(dalloc(c, (void**)&c->a_vs[0][m], fmax));
+        c->a_vs[1][m] = c->a_vs[2][m] = c->a_vs[0][m];
+      }
+    }
+  }
   return FS_OK;
 }
 
-// Tape buffers for one step under the current parameters.
+// Tape buffers for one step under the current parameters (storage
+// precision; the three stage pressures FP64).
 fs_status tape_bind(fs_ctx* c, Tape* tp) {
-  const size_t cb = c->Lc.total * sizeof(double);
-  const size_t fb[3] = {c->Lu.total * sizeof(double), c->Lv.total * sizeof(double), c->Lw.total * sizeof(double)};
+  const size_t cb = c->Lc.total * c->S();
+  const size_t fb[3] = {c->Lu.total * c->S(), c->Lv.total * c->S(), c->Lw.total * c->S()};
   const int n = c->prm.reinit_iterations;
-  const size_t ncell = 4 + 3 + 3 * (size_t)n, nface = 27;
+  const size_t ncell = 4 + 3 * (size_t)n, nface = 27;
   while (c->tape_cells.size() < ncell) {
-    double* p = nullptr;
-    CKS(dalloc(c, (void**)&p, cb));
+    void* p = nullptr;
+    CKS(dalloc(c, &p, cb));
     c->tape_cells.push_back(p);
   }
   while (c->tape_faces.size() < nface) {
-    double* p = nullptr;
-    CKS(dalloc(c, (void**)&p, fb[c->tape_faces.size() % 3]));
+    void* p = nullptr;
+    CKS(dalloc(c, &p, fb[c->tape_faces.size() % 3]));
     c->tape_faces.push_back(p);
+  }
+  while (c->tape_p.size() < 3) {
+    double* p = nullptr;
+    CKS(dalloc(c, (void**)&p, c->Lc.total * sizeof(double)));
+    c->tape_p.push_back(p);
   }
   size_t q = 0;
   for (int m = 0; m < 4; ++m) tp->ls[m] = c->tape_cells[q++];
-  for (int m = 0; m < 3; ++m) tp->p[m] = c->tape_cells[q++];
+  for (int m = 0; m < 3; ++m) tp->p[m] = c->tape_p[m];
   for (int b = 0; b < 3; ++b) {
     tp->re[b].resize(n);
     for (int it = 0; it < n; ++it) tp->re[b][it] = c->tape_cells[q++];
@@ -914,6 +944,13 @@ fs_status copy_cell(fs_ctx* c, double* dst, const double* src) {
   CK(cudaMemcpyAsync(dst, src, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   return FS_OK;
 }
+// copy three face fields of the storage precision (primal states)
+fs_status copy_fields(fs_ctx* c, void* const dst[3], void* const src[3]) {
+  const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+  for (int a = 0; a < 3; ++a)
+    CK(cudaMemcpyAsync(dst[a], src[a], lays[a]->total * c->S(), cudaMemcpyDeviceToDevice, c->stream));
+  return FS_OK;
+}
 fs_status copy_faces(fs_ctx* c, double* const dst[3], double* const src[3]) {
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   for (int a = 0; a < 3; ++a)
@@ -929,11 +966,12 @@ void axpy_faces(fs_ctx* c, double* const out[3], double* const x[3], double a) {
 // One forward-Euler WENO5 level-set update fe = src - dt L(src; vel): given
 // out_bar (bar of c1 * fe), src_bar = its bar w.r.t. src (overwritten) and
 // vel_bar += its bar w.r.t. the velocity.  src is refilled in its ghosts.
-fs_status adj_levelset_fe(fs_ctx* c, double* src, double* const vel[3], const double* out_bar, double c1,
+template <class S>
+fs_status adj_levelset_fe(fs_ctx* c, void* src, void* const vel[3], const double* out_bar, double c1,
                           double* src_bar, double* const vel_bar[3], double dt) {
   CKS(zero_cell(c, src_bar));
-  fill_extrap<double>(src, c->Lc, c->stream);
-  adj_weno_levelset(src, vel[0], vel[1], vel[2], out_bar, src_bar, vel_bar[0], vel_bar[1], vel_bar[2], c->Lc, c->Lu,
+  fill_extrap<S>(F<S>(src), c->Lc, c->stream);
+  adj_weno_levelset<S>(F<S>(src), F<S>(vel[0]), F<S>(vel[1]), F<S>(vel[2]), out_bar, src_bar, vel_bar[0], vel_bar[1], vel_bar[2], c->Lc, c->Lu,
                     c->Lv, c->Lw, c->grid.dx, c->prm.weno_epsilon, dt, c1, c->stream);
   adj_extrap(src_bar, c->Lc, c->stream);
   c->launches += 3;
@@ -943,24 +981,25 @@ fs_status adj_levelset_fe(fs_ctx* c, double* src, double* const vel[3], const do
 
 // One reinitialisation block B (S from its input, n Sussman steps) given the
 // inputs of its pseudo-steps: x_bar (overwritten) = B'^T z_bar.
-fs_status adj_reinit_block(fs_ctx* c, const std::vector<double*>& ys, const double* z_bar, double* x_bar) {
+template <class S>
+fs_status adj_reinit_block(fs_ctx* c, const std::vector<void*>& ys, const double* z_bar, double* x_bar) {
   const fs_params& P = c->prm;
   const int n = (int)ys.size();
   if (n == 0) return copy_cell(c, x_bar, z_bar);
   const double dx = c->grid.dx, dtau = dx / P.reinit_scaling;
   double *A = c->awork_c[2], *B = c->awork_c[3], *sbar = c->awork_c[4];
-  sign_function<double>(ys[0], (double*)c->sgn, c->Lc, dx, c->stream);
+  sign_function<S>(F<S>(ys[0]), F<S>(c->sgn), c->Lc, dx, c->stream);
   CKS(zero_cell(c, sbar));
   CKS(copy_cell(c, A, z_bar));
   for (int it = n - 1; it >= 0; --it) {
     CKS(zero_cell(c, B));
-    fill_extrap<double>(ys[it], c->Lc, c->stream);
-    adj_sussman(ys[it], (const double*)c->sgn, A, B, sbar, c->Lc, dx, P.weno_epsilon, dtau, 1.0,
+    fill_extrap<S>(F<S>(ys[it]), c->Lc, c->stream);
+    adj_sussman<S>(F<S>(ys[it]), F<S>(c->sgn), A, B, sbar, c->Lc, dx, P.weno_epsilon, dtau, 1.0,
                 (P.flags & FS_FLAG_REINIT_TYPO) ? 1 : 0, c->stream);
     adj_extrap(B, c->Lc, c->stream);
     std::swap(A, B);
   }
-  adj_sign(ys[0], sbar, A, c->Lc, dx, c->stream);
+  adj_sign<S>(F<S>(ys[0]), sbar, A, c->Lc, dx, c->stream);
   c->launches += 2 + 3 * n;
   CKS(copy_cell(c, x_bar, A));
   CK(cudaGetLastError());
@@ -971,33 +1010,34 @@ fs_status adj_reinit_block(fs_ctx* c, const std::vector<double*>& ys, const doub
 // in_bar (overwritten) = bar of u*, base_bar += c0 out_bar (when base_bar),
 // phi_bar and the density bars accumulate.  ustar, p: the forward's input
 // velocity and pressure; phi the level set it used.
-fs_status adj_projection(fs_ctx* c, double* phi, double* const ustar[3], const double* p, double* const out_bar[3],
+template <class S>
+fs_status adj_projection(fs_ctx* c, void* phi, void* const ustar[3], const double* p, double* const out_bar[3],
                          double c1, double* const in_bar[3], double* phi_bar, double dt) {
   const fs_params& P = c->prm;
   const double dx = c->grid.dx;
   cudaStream_t s = c->stream;
   (void)ustar;  // the map is affine in u*: its derivative does not depend on it
-  build_pressure_operator<double, double>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (double*)c->pax, (double*)c->pay,
-                                          (double*)c->paz, (double*)c->pdiag, c->scalars + 12, s);
-  Op7<double> A{(double*)c->pax, (double*)c->pay, (double*)c->paz, (double*)c->pdiag, c->Lc, 1, c->scalars + 12};
+  build_pressure_operator<S, double>(F<S>(phi), c->Lc, dx, P.rho_neg, P.rho_pos, c->a_ax, c->a_ay, c->a_az,
+                                     c->a_diag, c->scalars + 12, s);
+  Op7<double> A{c->a_ax, c->a_ay, c->a_az, c->a_diag, c->Lc, 1, c->scalars + 12};
   double *pbar = c->awork_c[0], *lam = c->awork_c[1];
   CKS(zero_cell(c, pbar));
   CKS(zero_cell(c, lam));
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   for (int a = 0; a < 3; ++a)
-    adj_velcorr(p, phi, out_bar[a], in_bar[a], pbar, phi_bar, c->a_rho, *lays[a], c->Lc, a, dx, dt, P.rho_neg,
-                P.rho_pos, c1, s);
+    adj_velcorr<S>(p, F<S>(phi), out_bar[a], in_bar[a], pbar, phi_bar, c->a_rho, *lays[a], c->Lc, a, dx, dt,
+                   P.rho_neg, P.rho_pos, c1, s);
   c->launches += 5;
   CK(cudaGetLastError());
   // lambda = A^-1 p_bar (A symmetric): the second solve with the same operator
   int it = 0, st = 0;
   double rel = 0.0;
   // the adjoint solve runs to the forward's tolerance, relative to its own right-hand side
-  CKS(run_pcg<double>(c, 3, A, pbar, lam, (double*)c->pr, (double*)c->pp, (double*)c->pq, P.tolerance,
-                      std::max(P.max_iteration, 1), FS_STOP_RELATIVE, &it, &rel, &st));
+  CKS(run_pcg<double>(c, 3, A, pbar, lam, c->a_r, c->a_p, c->a_q, P.tolerance, std::max(P.max_iteration, 1),
+                      FS_STOP_RELATIVE, &it, &rel, &st));
   adj_sum(lam, c->Lc, c->partials, c->tickets + 4, c->scalars + 14, s);
   for (int a = 0; a < 3; ++a) adj_divergence(lam, c->scalars + 14, in_bar[a], *lays[a], c->Lc, a, dx, dt, s);
-  adj_pressure_operator(phi, lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, s);
+  adj_pressure_operator<S>(F<S>(phi), lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, s);
   c->launches += 5;
   CK(cudaGetLastError());
   return FS_OK;
@@ -1006,7 +1046,8 @@ fs_status adj_projection(fs_ctx* c, double* phi, double* const ustar[3], const d
 // Semi-implicit viscosity x = M(phi)^-1 r(ug, phi): given out_bar (wall rows
 // cleared here), in_bar (overwritten) = bar of ug; phi and density bars
 // accumulate.  ug, x: the forward's input and output velocities.
-fs_status adj_viscosity(fs_ctx* c, double* phi, double* const ug[3], double* const x[3], double* const out_bar[3],
+template <class S>
+fs_status adj_viscosity(fs_ctx* c, void* phi, void* const ug[3], void* const x[3], double* const out_bar[3],
                         double* const in_bar[3], double* phi_bar, double dt) {
   const fs_params& P = c->prm;
   const double dx = c->grid.dx;
@@ -1014,19 +1055,20 @@ fs_status adj_viscosity(fs_ctx* c, double* phi, double* const ug[3], double* con
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   CKS(zero_faces(c, in_bar));
   for (int a = 0; a < 3; ++a) {
-    viscosity_system<double>(phi, ug[0], ug[1], ug[2], c->Lc, c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos,
-                             P.mu_neg, P.mu_pos, (double*)c->vs[a][0], (double*)c->vs[a][1], (double*)c->vs[a][2],
-                             (double*)c->vs[a][3], (double*)c->vs[a][4], s);
+    viscosity_system<S, double>(F<S>(phi), F<S>(ug[0]), F<S>(ug[1]), F<S>(ug[2]), c->Lc, c->Lu, c->Lv, c->Lw, a, dx,
+                                dt, P.rho_neg, P.rho_pos, P.mu_neg, P.mu_pos, c->a_vs[a][0], c->a_vs[a][1],
+                                c->a_vs[a][2], c->a_vs[a][3], c->a_vs[a][4], s);
     CK(cudaMemcpyAsync(c->a_vxb[a], out_bar[a], lays[a]->total * sizeof(double), cudaMemcpyDeviceToDevice, s));
     adj_zero_walls(c->a_vxb[a], *lays[a], a, s);  // wall rows are the constant zero
     CK(cudaMemsetAsync(c->a_vlam[a], 0, lays[a]->total * sizeof(double), s));
-    Op7<double> A{(double*)c->vs[a][0], (double*)c->vs[a][1], (double*)c->vs[a][2], (double*)c->vs[a][3], *lays[a]};
+    Op7<double> A{c->a_vs[a][0], c->a_vs[a][1], c->a_vs[a][2], c->a_vs[a][3], *lays[a]};
     int it = 0, st = 0;
-    CKS(run_pcg<double>(c, 120 + a, A, c->a_vxb[a], c->a_vlam[a], (double*)c->vs[a][6], (double*)c->vs[a][7],
-                        (double*)c->vs[a][8], P.viscosity_tolerance, std::max(P.viscosity_max_iteration, 1),
-                        FS_STOP_RELATIVE, &it, nullptr, &st));
-    adj_visc(phi, ug[0], ug[1], ug[2], x[a], c->a_vlam[a], in_bar[0], in_bar[1], in_bar[2], phi_bar, c->a_rho, c->Lc,
-             c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos, P.mu_neg, P.mu_pos, s);
+    CKS(run_pcg<double>(c, 120 + a, A, c->a_vxb[a], c->a_vlam[a], c->a_vs[a][6], c->a_vs[a][7], c->a_vs[a][8],
+                        P.viscosity_tolerance, std::max(P.viscosity_max_iteration, 1), FS_STOP_RELATIVE, &it, nullptr,
+                        &st));
+    adj_visc<S>(F<S>(phi), F<S>(ug[0]), F<S>(ug[1]), F<S>(ug[2]), F<S>(x[a]), c->a_vlam[a], in_bar[0], in_bar[1],
+                in_bar[2], phi_bar, c->a_rho, c->Lc, c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos, P.mu_neg,
+                P.mu_pos, s);
     c->launches += 3;
   }
   CK(cudaGetLastError());
@@ -1034,12 +1076,13 @@ fs_status adj_viscosity(fs_ctx* c, double* phi, double* const ug[3], double* con
 }
 
 // WENO5 self-advection of u, v, w: in_bar (overwritten) from out_bar.
-fs_status adj_velocity_advect(fs_ctx* c, double* const uin[3], double* const out_bar[3], double* const in_bar[3],
+template <class S>
+fs_status adj_velocity_advect(fs_ctx* c, void* const uin[3], double* const out_bar[3], double* const in_bar[3],
                               double dt) {
   CKS(zero_faces(c, in_bar));
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   for (int a = 0; a < 3; ++a)
-    adj_weno_mac(uin[a], uin[0], uin[1], uin[2], out_bar[a], in_bar[a], in_bar[0], in_bar[1], in_bar[2], *lays[a],
+    adj_weno_mac<S>(F<S>(uin[a]), F<S>(uin[0]), F<S>(uin[1]), F<S>(uin[2]), out_bar[a], in_bar[a], in_bar[0], in_bar[1], in_bar[2], *lays[a],
                  c->Lu, c->Lv, c->Lw, a, c->grid.dx, velocity_epsilon(c), dt, c->stream);
   c->launches += 3;
   CK(cudaGetLastError());
@@ -1047,7 +1090,6 @@ fs_status adj_velocity_advect(fs_ctx* c, double* const uin[3], double* const out
 }
 
 fs_status adj_check(fs_ctx* c) {
-  if (c->fp32) { set_error("adjoints are built for FP64 contexts"); return FS_NOT_SUPPORTED; }
   if (c->prm.surface_tension != 0.0) {
     set_error("adjoints do not cover the surface-tension jump terms");
     return FS_NOT_SUPPORTED;
@@ -1075,17 +1117,18 @@ fs_status adj_check(fs_ctx* c) {
 // then the reverse sweep.  On entry abar holds the bars of the step's
 // output; on return the bars of its input (phi, u, v, w) and a_rho has the
 // density bars added.  The fields end in the step's output state.
+template <class S>
 fs_status step_adjoint_t(fs_ctx* c, double dt, fs_step_report* rep) {
   const fs_params& P = c->prm;
   Tape tp;
   CKS(tape_bind(c, &tp));
-  double* u0[3];
+  void* u0[3];
   for (int a = 0; a < 3; ++a) u0[a] = tp.vel[0][0][a];  // the step's initial velocity (first stage input)
-  fs_status fw = step_t<double>(c, dt, rep, &tp);
+  fs_status fw = step_t<S>(c, dt, rep, &tp);
   if (fw != FS_OK && fw != FS_NOT_CONVERGED) return fw;
   const int order = P.order;
   // ---- reinitialisation blocks
-  double* phiA = tp.ls[3];
+  void* phiA = tp.ls[3];
   double *phibar = c->abar[0], *phiAbar = c->awork_c[5];
   CKS(zero_cell(c, phiAbar));
   {
@@ -1100,7 +1143,7 @@ fs_status step_adjoint_t(fs_ctx* c, double dt, fs_step_report* rep) {
       CK(cudaMemsetAsync(xb, 0, c->Lc.total * sizeof(double), c->stream));
       // the block's own output is scaled by c1
       adj_axpy(xb, zb, c1s[b], c->Lc, c->stream);
-      CKS(adj_reinit_block(c, tp.re[b], xb, zb));  // zb <- bar of the block input
+      CKS(adj_reinit_block<S>(c, tp.re[b], xb, zb));  // zb <- bar of the block input
       c->launches += 2;
     }
     adj_axpy(phiAbar, zb, 1.0, c->Lc, c->stream);  // the first block's input is phiA
@@ -1119,10 +1162,10 @@ fs_status step_adjoint_t(fs_ctx* c, double dt, fs_step_report* rep) {
   for (int st = ns - 1; st >= 0; --st) {
     if (vc0[st] != 0.0) axpy_faces(c, u0bar, cur, vc0[st]);
     double* pin[3] = {c->awork_f[1][0], c->awork_f[1][1], c->awork_f[1][2]};
-    CKS(adj_projection(c, phiA, tp.vel[st][2], tp.p[st], cur, vc1[st], pin, phiAbar, dt));
+    CKS(adj_projection<S>(c, phiA, tp.vel[st][2], tp.p[st], cur, vc1[st], pin, phiAbar, dt));
     double* gin[3] = {c->awork_f[2][0], c->awork_f[2][1], c->awork_f[2][2]};
     if (P.viscosity) {
-      CKS(adj_viscosity(c, phiA, tp.vel[st][1], tp.vel[st][2], pin, gin, phiAbar, dt));
+      CKS(adj_viscosity<S>(c, phiA, tp.vel[st][1], tp.vel[st][2], pin, gin, phiAbar, dt));
     } else {
       CKS(copy_faces(c, gin, pin));
     }
@@ -1130,32 +1173,32 @@ fs_status step_adjoint_t(fs_ctx* c, double dt, fs_step_report* rep) {
     const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
     for (int a = 0; a < 3; ++a) adj_zero_walls(gin[a], *lays[a], a, c->stream);
     c->launches += 3;
-    CKS(adj_velocity_advect(c, tp.vel[st][0], gin, cur, dt));  // cur <- bar of the stage input
+    CKS(adj_velocity_advect<S>(c, tp.vel[st][0], gin, cur, dt));  // cur <- bar of the stage input
   }
   axpy_faces(c, u0bar, cur, 1.0);  // the first stage's input is u0
   // ---- level set: phiA from phi0 with the initial velocity u0
   double* b1 = c->awork_c[0];
   double* b2 = c->awork_c[1];
   CKS(zero_cell(c, phibar));
-  double* const* u0p = u0;
+  void* const* u0p = u0;
   if (order == 3 && !(P.flags & FS_FLAG_LEVELSET_FORWARD_EULER)) {
     // phiA = 1/3 phi0 + 2/3 FE(phi2); phi2 = 3/4 phi0 + 1/4 FE(phi1); phi1 = FE(phi0)
     adj_axpy(phibar, phiAbar, 1.0 / 3.0, c->Lc, c->stream);
-    CKS(adj_levelset_fe(c, tp.ls[2], u0p, phiAbar, 2.0 / 3.0, b2, u0bar, dt));  // b2 = bar of phi2
+    CKS(adj_levelset_fe<S>(c, tp.ls[2], u0p, phiAbar, 2.0 / 3.0, b2, u0bar, dt));  // b2 = bar of phi2
     adj_axpy(phibar, b2, 0.75, c->Lc, c->stream);
-    CKS(adj_levelset_fe(c, tp.ls[1], u0p, b2, 0.25, b1, u0bar, dt));            // b1 = bar of phi1
-    CKS(adj_levelset_fe(c, tp.ls[0], u0p, b1, 1.0, b2, u0bar, dt));             // b2 = bar of phi0 via FE
+    CKS(adj_levelset_fe<S>(c, tp.ls[1], u0p, b2, 0.25, b1, u0bar, dt));            // b1 = bar of phi1
+    CKS(adj_levelset_fe<S>(c, tp.ls[0], u0p, b1, 1.0, b2, u0bar, dt));             // b2 = bar of phi0 via FE
     adj_axpy(phibar, b2, 1.0, c->Lc, c->stream);
     c->launches += 3;
   } else if (order == 3) {
-    CKS(adj_levelset_fe(c, tp.ls[0], u0p, phiAbar, 1.0, b2, u0bar, dt));
+    CKS(adj_levelset_fe<S>(c, tp.ls[0], u0p, phiAbar, 1.0, b2, u0bar, dt));
     adj_axpy(phibar, b2, 1.0, c->Lc, c->stream);
     c->launches += 1;
   } else {
     // Heun: phiA = 1/2 phi0 + 1/2 FE(phi1), phi1 = FE(phi0)
     adj_axpy(phibar, phiAbar, 0.5, c->Lc, c->stream);
-    CKS(adj_levelset_fe(c, tp.ls[1], u0p, phiAbar, 0.5, b1, u0bar, dt));
-    CKS(adj_levelset_fe(c, tp.ls[0], u0p, b1, 1.0, b2, u0bar, dt));
+    CKS(adj_levelset_fe<S>(c, tp.ls[1], u0p, phiAbar, 0.5, b1, u0bar, dt));
+    CKS(adj_levelset_fe<S>(c, tp.ls[0], u0p, b1, 1.0, b2, u0bar, dt));
     adj_axpy(phibar, b2, 1.0, c->Lc, c->stream);
     c->launches += 2;
   }
@@ -1753,7 +1796,7 @@ fs_status fs_read_state(fs_ctx* c, const char* path) {
   return FS_OK;
 }
 
-// ---- adjoints (FP64 contexts, corrected projection)
+// ---- adjoints (corrected projection; FP64 bars over FP64 or FP32 states)
 
 fs_status fs_adjoint_reset(fs_ctx* c) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
@@ -1786,7 +1829,7 @@ fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {
   c->pcg_ms = 0.0f;
   c->pcg_launched_iterations = 0;
   CKS(timed_begin(c));
-  fs_status s = step_adjoint_t(c, dt, r);
+  fs_status s = c->fp32 ? step_adjoint_t<float>(c, dt, r) : step_adjoint_t<double>(c, dt, r);
   if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
   CKS(timed_end(c, &r->ms));
   r->pcg_ms = c->pcg_ms;
@@ -1798,8 +1841,9 @@ fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {
 fs_status fs_advect_levelset_adjoint(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
   CKS(adj_check(c));
-  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
-  CKS(adj_levelset_fe(c, (double*)c->phi, vel, c->abar[0], 1.0, c->awork_c[0], &c->abar[1], dt));
+  void* vel[3] = {c->u, c->v, c->w};
+  CKS(c->fp32 ? adj_levelset_fe<float>(c, c->phi, vel, c->abar[0], 1.0, c->awork_c[0], &c->abar[1], dt)
+              : adj_levelset_fe<double>(c, c->phi, vel, c->abar[0], 1.0, c->awork_c[0], &c->abar[1], dt));
   CKS(copy_cell(c, c->abar[0], c->awork_c[0]));
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;
@@ -1808,8 +1852,9 @@ fs_status fs_advect_levelset_adjoint(fs_ctx* c, double dt) {
 fs_status fs_advect_velocity_adjoint(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
   CKS(adj_check(c));
-  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
-  CKS(adj_velocity_advect(c, vel, &c->abar[1], c->awork_f[0], dt));
+  void* vel[3] = {c->u, c->v, c->w};
+  CKS(c->fp32 ? adj_velocity_advect<float>(c, vel, &c->abar[1], c->awork_f[0], dt)
+              : adj_velocity_advect<double>(c, vel, &c->abar[1], c->awork_f[0], dt));
   CKS(copy_faces(c, &c->abar[1], c->awork_f[0]));
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;
@@ -1820,8 +1865,13 @@ fs_status fs_reinitialize_adjoint(fs_ctx* c) {
   CKS(adj_check(c));
   Tape tp;
   CKS(tape_bind(c, &tp));
-  CKS(reinit_block_t<double>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3, &tp.re[0]));
-  CKS(adj_reinit_block(c, tp.re[0], c->abar[0], c->awork_c[0]));
+  if (c->fp32) {
+    CKS(reinit_block_t<float>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3, &tp.re[0]));
+    CKS(adj_reinit_block<float>(c, tp.re[0], c->abar[0], c->awork_c[0]));
+  } else {
+    CKS(reinit_block_t<double>(c, c->phi, c->s1, c->phi, 0.0, 1.0, c->s2, c->s3, &tp.re[0]));
+    CKS(adj_reinit_block<double>(c, tp.re[0], c->abar[0], c->awork_c[0]));
+  }
   CKS(copy_cell(c, c->abar[0], c->awork_c[0]));
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;
@@ -1831,15 +1881,17 @@ fs_status fs_viscosity_adjoint(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
   if (!(dt > 0)) { set_error("dt must be positive"); return FS_INVALID_ARG; }
   CKS(adj_check(c));
-  if (!c->prm.viscosity) { set_error("viscosity is off"); return FS_INVALID_ARG; }
+  if (c->prm.viscosity != 1) { set_error("the semi-implicit viscosity is off"); return FS_INVALID_ARG; }
   Tape tp;
   CKS(tape_bind(c, &tp));
   CKS(tape_velocity(c, tp.vel[0][1]));
-  CKS(viscosity_t<double>(c, dt, nullptr));
+  CKS(c->fp32 ? viscosity_t<float>(c, dt, nullptr) : viscosity_t<double>(c, dt, nullptr));
   CKS(tape_velocity(c, tp.vel[0][2]));
-  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
-  CKS(copy_faces(c, vel, tp.vel[0][1]));  // the context keeps the operator's input
-  CKS(adj_viscosity(c, (double*)c->phi, tp.vel[0][1], tp.vel[0][2], &c->abar[1], c->awork_f[1], c->abar[0], dt));
+  void* vel[3] = {c->u, c->v, c->w};
+  CKS(copy_fields(c, vel, tp.vel[0][1]));  // the context keeps the operator's input
+  CKS(c->fp32 ? adj_viscosity<float>(c, c->phi, tp.vel[0][1], tp.vel[0][2], &c->abar[1], c->awork_f[1], c->abar[0], dt)
+              : adj_viscosity<double>(c, c->phi, tp.vel[0][1], tp.vel[0][2], &c->abar[1], c->awork_f[1], c->abar[0],
+                                      dt));
   CKS(copy_faces(c, &c->abar[1], c->awork_f[1]));
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;
@@ -1852,12 +1904,14 @@ fs_status fs_project_adjoint(fs_ctx* c, double dt) {
   Tape tp;
   CKS(tape_bind(c, &tp));
   CKS(tape_velocity(c, tp.vel[0][2]));
-  fs_status s = project_t<double>(c, dt, 0.0, 1.0, nullptr);
+  fs_status s = c->fp32 ? project_t<float>(c, dt, 0.0, 1.0, nullptr) : project_t<double>(c, dt, 0.0, 1.0, nullptr);
   if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
   CKS(copy_cell(c, tp.p[0], c->p64));
-  double* vel[3] = {(double*)c->u, (double*)c->v, (double*)c->w};
-  CKS(copy_faces(c, vel, tp.vel[0][2]));  // the context keeps the operator's input
-  CKS(adj_projection(c, (double*)c->phi, tp.vel[0][2], tp.p[0], &c->abar[1], 1.0, c->awork_f[1], c->abar[0], dt));
+  void* vel[3] = {c->u, c->v, c->w};
+  CKS(copy_fields(c, vel, tp.vel[0][2]));  // the context keeps the operator's input
+  CKS(c->fp32 ? adj_projection<float>(c, c->phi, tp.vel[0][2], tp.p[0], &c->abar[1], 1.0, c->awork_f[1], c->abar[0], dt)
+              : adj_projection<double>(c, c->phi, tp.vel[0][2], tp.p[0], &c->abar[1], 1.0, c->awork_f[1], c->abar[0],
+                                       dt));
   CKS(copy_faces(c, &c->abar[1], c->awork_f[1]));
   CK(cudaStreamSynchronize(c->stream));
   return s;

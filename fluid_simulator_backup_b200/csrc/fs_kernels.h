@@ -196,10 +196,11 @@ template <class T> void pack_to_double(double* dst, const T* src, const Lay& L, 
 template <class T> void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s);
 
 // ---- viscosity family (fs_viscosity.cu)
-template <class T>
+// the system of component `axis` from fields of type T, stored in type V
+template <class T, class V = T>
 void viscosity_system(const T* phi, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
                       const Lay& Lw, int axis, double dx, double dt, double rho_neg, double rho_pos, double mu_neg,
-                      double mu_pos, T* ax, T* ay, T* az, T* diag, T* rhs, cudaStream_t s);
+                      double mu_pos, V* ax, V* ay, V* az, V* diag, V* rhs, cudaStream_t s);
 
 // The reference's explicit air/water viscosity (VISCOSITY_3D.h:452-563).
 // in_place = 0: (ua, va, wa) <- the update of (u, v, w) (the caller swaps);
@@ -210,29 +211,37 @@ int viscosity_explicit(const T* phi, T* u, T* v, T* w, T* ua, T* va, T* wa, cons
                        const Lay& Lv, const Lay& Lw, double dx, double dt, double rho_neg, double rho_pos,
                        double mu_neg, double mu_pos, int in_place, cudaStream_t s);
 
-// ---- adjoint family (fs_adjoint.cu), FP64 only; all add into the bars
-void adj_weno_levelset(const double* src, const double* u, const double* v, const double* w, const double* out_bar,
-                       double* src_bar, double* u_bar, double* v_bar, double* w_bar, const Lay& L, const Lay& Lu,
-                       const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c1, cudaStream_t s);
+// ---- adjoint family (fs_adjoint.cu): primal fields of the storage type T
+// (FP64 or FP32), bars FP64; all add into the bars
+template <class T>
+void adj_weno_levelset(const T* src, const T* u, const T* v, const T* w, const double* out_bar, double* src_bar,
+                       double* u_bar, double* v_bar, double* w_bar, const Lay& L, const Lay& Lu, const Lay& Lv,
+                       const Lay& Lw, double dx, double eps, double dt, double c1, cudaStream_t s);
 void adj_extrap(double* bar, const Lay& L, cudaStream_t s);
-void adj_weno_mac(const double* comp, const double* u, const double* v, const double* w, const double* out_bar,
-                  double* comp_bar, double* u_bar, double* v_bar, double* w_bar, const Lay& Lc, const Lay& Lu,
-                  const Lay& Lv, const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s);
-void adj_sussman(const double* src, const double* sgn, const double* out_bar, double* src_bar, double* sgn_bar,
-                 const Lay& L, double dx, double eps, double dtau, double c1, int typo, cudaStream_t s);
-void adj_sign(const double* phi, const double* sgn_bar, double* phi_bar, const Lay& L, double dx, cudaStream_t s);
-void adj_velcorr(const double* p, const double* phi, const double* out_bar, double* in_bar, double* p_bar,
-                 double* phi_bar, double* rho_bar, const Lay& Lf, const Lay& Lc, int axis, double dx, double dt,
-                 double rn, double rp, double c1, cudaStream_t s);
+template <class T>
+void adj_weno_mac(const T* comp, const T* u, const T* v, const T* w, const double* out_bar, double* comp_bar,
+                  double* u_bar, double* v_bar, double* w_bar, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+                  const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s);
+template <class T>
+void adj_sussman(const T* src, const T* sgn, const double* out_bar, double* src_bar, double* sgn_bar, const Lay& L,
+                 double dx, double eps, double dtau, double c1, int typo, cudaStream_t s);
+template <class T>
+void adj_sign(const T* phi, const double* sgn_bar, double* phi_bar, const Lay& L, double dx, cudaStream_t s);
+template <class T>
+void adj_velcorr(const double* p, const T* phi, const double* out_bar, double* in_bar, double* p_bar, double* phi_bar,
+                 double* rho_bar, const Lay& Lf, const Lay& Lc, int axis, double dx, double dt, double rn, double rp,
+                 double c1, cudaStream_t s);
 void adj_divergence(const double* lam, const double* sum_lam, double* in_bar, const Lay& Lf, const Lay& Lc, int axis,
                     double dx, double dt, cudaStream_t s);
 void adj_sum(const double* f, const Lay& L, double* partials, unsigned int* ticket, double* out, cudaStream_t s);
-void adj_pressure_operator(const double* phi, const double* lam, const double* p, double* phi_bar, double* rho_bar,
+template <class T>
+void adj_pressure_operator(const T* phi, const double* lam, const double* p, double* phi_bar, double* rho_bar,
                            const Lay& Lc, double dx, double rn, double rp, cudaStream_t s);
-void adj_visc(const double* phi, const double* ug, const double* vg, const double* wg, const double* x,
-              const double* lam, double* u_bar, double* v_bar, double* w_bar, double* phi_bar, double* rho_bar,
-              const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw, int axis, double dx, double dt, double rn,
-              double rp, double mn, double mp, cudaStream_t s);
+template <class T>
+void adj_visc(const T* phi, const T* ug, const T* vg, const T* wg, const T* x, const double* lam, double* u_bar,
+              double* v_bar, double* w_bar, double* phi_bar, double* rho_bar, const Lay& Lc, const Lay& Lu,
+              const Lay& Lv, const Lay& Lw, int axis, double dx, double dt, double rn, double rp, double mn,
+              double mp, cudaStream_t s);
 void adj_zero_walls(double* f, const Lay& L, int axis, cudaStream_t s);
 void adj_axpy(double* out, const double* x, double a, const Lay& L, cudaStream_t s);
 

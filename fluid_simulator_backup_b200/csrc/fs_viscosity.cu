@@ -54,11 +54,11 @@ struct PhiX {  // phi with a one-layer linear extrapolation across the walls
 // Face (i,j,k) of component `axis` sits between cell (i,j,k) and the cell
 // one step back along the axis.  Cells around the face are addressed in
 // "face coordinates" relative to that low cell.
-template <class T>
+template <class T, class V>
 __global__ void k_visc_system(const T* __restrict__ phi, const T* __restrict__ u, const T* __restrict__ v,
                               const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw, Lay Lf, int axis, double inv_h,
-                              double dt, double rn, double rp, double mn, double mp, T* __restrict__ ax,
-                              T* __restrict__ ay, T* __restrict__ az, T* __restrict__ diag, T* __restrict__ rhs) {
+                              double dt, double rn, double rp, double mn, double mp, V* __restrict__ ax,
+                              V* __restrict__ ay, V* __restrict__ az, V* __restrict__ diag, V* __restrict__ rhs) {
   FS_IJK(Lf);
   const int64_t f = Lf.at(i, j, k);
   const PhiX<T> P{phi, Lc};
@@ -99,15 +99,15 @@ __global__ void k_visc_system(const T* __restrict__ phi, const T* __restrict__ u
   // couplings stored at this face couple it with the face one step back;
   // couplings that touch a wall face are zeroed (Dirichlet neighbour)
   const bool low_is_wall[3] = {axis == 0 && i == 1, axis == 1 && j == 1, axis == 2 && k == 1};
-  ax[f] = (T)((wall || low_is_wall[0] || i == 0) ? 0.0 : low[0]);
-  ay[f] = (T)((wall || low_is_wall[1] || j == 0) ? 0.0 : low[1]);
-  az[f] = (T)((wall || low_is_wall[2] || k == 0) ? 0.0 : low[2]);
+  ax[f] = (V)((wall || low_is_wall[0] || i == 0) ? 0.0 : low[0]);
+  ay[f] = (V)((wall || low_is_wall[1] || j == 0) ? 0.0 : low[1]);
+  az[f] = (V)((wall || low_is_wall[2] || k == 0) ? 0.0 : low[2]);
   if (wall) {
-    diag[f] = (T)1.0;
-    rhs[f] = (T)0.0;
+    diag[f] = (V)1.0;
+    rhs[f] = (V)0.0;
     return;
   }
-  diag[f] = (T)(rho_f + ((((low[0] + high[0]) + low[1]) + high[1]) + low[2]) + high[2]);
+  diag[f] = (V)(rho_f + ((((low[0] + high[0]) + low[1]) + high[1]) + low[2]) + high[2]);
   // explicit transpose terms (VISCOSITY_3D.h:620-630): for each tangential
   // direction t, d/dt( mu_edge * d(vel_t)/d(axis) ) with zero ghosts
   const T* comp[3] = {u, v, w};
@@ -126,7 +126,7 @@ __global__ void k_visc_system(const T* __restrict__ phi, const T* __restrict__ u
     const double lo_b = (double)vt[Lt.at(i - ea[0], j - ea[1], k - ea[2])];
     ex = ex + coef * (inv_h * (mu_high[t] * inv_h * (hi_a - hi_b) - mu_low[t] * inv_h * (lo_a - lo_b)));
   }
-  rhs[f] = (T)(rho_f * ex);
+  rhs[f] = (V)(rho_f * ex);
 }
 
 // ---------------------------------------------------------------------------
@@ -288,21 +288,22 @@ template int viscosity_explicit<double>(const double*, double*, double*, double*
                                         const Lay&, const Lay&, const Lay&, const Lay&, double, double, double, double,
                                         double, double, int, cudaStream_t);
 
-template <class T>
+template <class T, class V>
 void viscosity_system(const T* phi, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
                       const Lay& Lw, int axis, double dx, double dt, double rho_neg, double rho_pos, double mu_neg,
-                      double mu_pos, T* ax, T* ay, T* az, T* diag, T* rhs, cudaStream_t s) {
+                      double mu_pos, V* ax, V* ay, V* az, V* diag, V* rhs, cudaStream_t s) {
   const Lay& Lf = axis == 0 ? Lu : (axis == 1 ? Lv : Lw);
   Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
-  k_visc_system<T><<<g.grid, g.block, 0, s>>>(phi, u, v, w, Lc, Lu, Lv, Lw, Lf, axis, 1.0 / dx, dt, rho_neg, rho_pos,
-                                               mu_neg, mu_pos, ax, ay, az, diag, rhs);
+  k_visc_system<T, V><<<g.grid, g.block, 0, s>>>(phi, u, v, w, Lc, Lu, Lv, Lw, Lf, axis, 1.0 / dx, dt, rho_neg,
+                                                 rho_pos, mu_neg, mu_pos, ax, ay, az, diag, rhs);
 }
 
-template void viscosity_system<float>(const float*, const float*, const float*, const float*, const Lay&, const Lay&,
-                                      const Lay&, const Lay&, int, double, double, double, double, double, double,
-                                      float*, float*, float*, float*, float*, cudaStream_t);
-template void viscosity_system<double>(const double*, const double*, const double*, const double*, const Lay&,
-                                       const Lay&, const Lay&, const Lay&, int, double, double, double, double, double,
-                                       double, double*, double*, double*, double*, double*, cudaStream_t);
+#define FS_VISC_INST(T, V)                                                                                          \
+  template void viscosity_system<T, V>(const T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, \
+                                       const Lay&, int, double, double, double, double, double, double, V*, V*, V*, \
+                                       V*, V*, cudaStream_t);
+FS_VISC_INST(float, float)
+FS_VISC_INST(double, double)
+FS_VISC_INST(float, double)
 
 }  // namespace fsb

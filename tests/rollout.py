@@ -1,14 +1,17 @@
 """Differentiable multi-step rollout for the tests: a torch.autograd.Function
-over the library's fs_step / fs_step_adjoint (FP64 contexts), with binomial
-checkpointing of the step states.
+over the library's fs_step / fs_step_adjoint (FP64 or FP32 contexts), with
+binomial or uniform checkpointing of the step states.
 
 Forward runs T steps keeping only the initial state.  Backward reverses the
 steps with at most `snapshots` stored states besides the initial one: with s
 snapshots and repetition number t, a segment of up to C(s+t, s) steps is
 reversed by advancing to a split point m, taking a snapshot there, reversing
 [m, end) with s-1 snapshots and then [start, m) with the same s snapshots
-and repetition t-1 (Griewank's binomial schedule).  The adjoint fields of the
-context carry the bars from one reversed step to the one before.
+and repetition t-1 (Griewank's binomial schedule).  With a uniform schedule
+(`every` = m) the forward keeps the states at steps 0, m, 2m, ... and each
+segment is reversed by recomputing its states from its checkpoint.  The
+adjoint fields of the context carry the bars from one reversed step to the
+one before.
 
 Test infrastructure only: the library itself knows nothing of torch.
 """
@@ -82,16 +85,42 @@ def _reverse(s, a, b, st_a, snaps, dt, sched):
     _reverse(s, a, m, st_a, snaps, dt, sched)
 
 
+def _reverse_uniform(s, checkpoints, every, nsteps, dt, sched):
+    """Reverse all steps segment by segment from the stored checkpoints."""
+    for start in range(((nsteps - 1) // every) * every, -1, -every):
+        end = min(start + every, nsteps)
+        states = [checkpoints[start]]
+        for _ in range(start + 1, end):
+            states.append(_advance(s, states[-1], 1, dt, sched))
+        sched.max_live_snapshots = max(sched.max_live_snapshots, len(checkpoints) + len(states))
+        for st in reversed(states):
+            _load(s, st)
+            s.step_adjoint(dt)
+            sched.adjoint_steps += 1
+
+
 class Rollout(torch.autograd.Function):
-    """phi(T), u(T), v(T), w(T) = rollout(phi0, u0, v0, w0, rho_pos) over
-    `nsteps` steps of length dt on the FP64 solver `s`."""
+    """phi(T), u(T), v(T), w(T) = rollout(phi0, u0, v0, w0, rho) over `nsteps`
+    steps of length dt on the solver `s`, rho being the density of the phase
+    `phase` ("pos" for phi > 0, "neg" for phi <= 0).  snapshots > 0: the
+    binomial schedule with that many snapshots; every > 0: uniform
+    checkpoints every `every` steps."""
 
     @staticmethod
-    def forward(ctx, phi0, u0, v0, w0, rho_pos, s, dt, nsteps, snapshots, sched):
+    def forward(ctx, phi0, u0, v0, w0, rho, s, dt, nsteps, snapshots, sched, phase="pos", every=0):
         st0 = {k: t.detach().cpu().numpy().astype(np.float64) for k, t in zip(KEYS, (phi0, u0, v0, w0))}
-        s.set_params(rho_pos=float(rho_pos.item()))
-        out = _advance(s, st0, nsteps, dt, sched)
+        s.set_params(**{"rho_" + phase: float(rho.item())})
+        ctx.checkpoints = {}
+        if every > 0:
+            st = st0
+            for start in range(0, nsteps, every):
+                ctx.checkpoints[start] = st
+                st = _advance(s, st, min(every, nsteps - start), dt, sched)
+            out = st
+        else:
+            out = _advance(s, st0, nsteps, dt, sched)
         ctx.s, ctx.dt, ctx.nsteps, ctx.snapshots, ctx.st0, ctx.sched = s, dt, nsteps, snapshots, st0, sched
+        ctx.phase, ctx.every = phase, every
         return tuple(torch.from_numpy(out[k]) for k in KEYS)
 
     @staticmethod
@@ -100,7 +129,11 @@ class Rollout(torch.autograd.Function):
         s.adjoint_reset()
         for k, g in zip(KEYS, (gphi, gu, gv, gw)):
             s.upload("adj_" + k, (g if g is not None else torch.zeros(s.shape(k), dtype=torch.float64)).numpy())
-        _reverse(s, 0, ctx.nsteps, ctx.st0, ctx.snapshots, ctx.dt, ctx.sched)
+        if ctx.every > 0:
+            _reverse_uniform(s, ctx.checkpoints, ctx.every, ctx.nsteps, ctx.dt, ctx.sched)
+        else:
+            _reverse(s, 0, ctx.nsteps, ctx.st0, ctx.snapshots, ctx.dt, ctx.sched)
         grads = [torch.from_numpy(s.download("adj_" + k)) for k in KEYS]
-        rho_bar = torch.tensor(s.density_bars()[1], dtype=torch.float64)
-        return (*grads, rho_bar, None, None, None, None, None)
+        bars = s.density_bars()
+        rho_bar = torch.tensor(bars[1] if ctx.phase == "pos" else bars[0], dtype=torch.float64)
+        return (*grads, rho_bar, None, None, None, None, None, None, None)
