@@ -4,12 +4,24 @@
 // (EULERIAN_FLUID_SOLVER_3D.h:886-1109), templated on the storage/arithmetic
 // type (double for the FP64 path, float for FP32_REFINE).
 //
+// Staging.  The four seven-point stencil kernels (WENO5 level set, WENO5 and
+// ENO3 MAC components, Sussman) run on 32 x 8 column tiles that march up a
+// chunk of z planes: the stencil field is staged in shared memory as a ring of
+// seven (32+6) x (8+6) planes (the tile and its three-cell halo), one new
+// plane loaded per output plane with row-contiguous (coalesced) loads, and
+// every x, y and z sample of the stencil is read from that ring.  HBM then
+// carries each field element about once per kernel instead of up to 19
+// times through L1/L2.  The ghost ring of the padded layout supplies the halo
+// at the box boundary.
+//
 // These kernels are FP32/FP64-issue bound rather than HBM bound (about 440
 // flops per cell per WENO5 update), so the WENO weights are evaluated with one
 // division per side: w_k = d_k prod_{j!=k} q_j / sum_m d_m prod_{j!=m} q_j
 // with q = (eps + IS)^2, algebraically equal to the reference's
 // (d_k/q_k)/sum(d_m/q_m).  The substencil constants 1/3, 7/6, ... are applied
 // as multiplications.  Both change results only at the level of rounding.
+#include <algorithm>
+
 #include "fs_kernels.h"
 
 namespace fsb {
@@ -137,46 +149,117 @@ __device__ __forceinline__ T weno_side(T r1, T r2, T r3, T r4, T r5, T eps) {
   return ((b1 * u1 + b2 * u2) + b3 * u3) * inv;
 }
 
-// D- and D+ along a stride from the 7 samples f[-3..3].
+// D- and D+ from the 7 samples v[0..6] = f[-3..3] along one axis.
 template <class T>
-__device__ __forceinline__ void weno_pair(const T* __restrict__ f, int64_t c, int64_t st, T inv_h, T eps, T& dm, T& dp) {
-  const T fm3 = f[c - 3 * st], fm2 = f[c - 2 * st], fm1 = f[c - st], f0 = f[c], fp1 = f[c + st], fp2 = f[c + 2 * st],
-          fp3 = f[c + 3 * st];
-  const T d1 = inv_h * (fm2 - fm3), d2 = inv_h * (fm1 - fm2), d3 = inv_h * (f0 - fm1), d4 = inv_h * (fp1 - f0),
-          d5 = inv_h * (fp2 - fp1), d6 = inv_h * (fp3 - fp2);
+__device__ __forceinline__ void weno_pair7(const T v[7], T inv_h, T eps, T& dm, T& dp) {
+  const T d1 = inv_h * (v[1] - v[0]), d2 = inv_h * (v[2] - v[1]), d3 = inv_h * (v[3] - v[2]),
+          d4 = inv_h * (v[4] - v[3]), d5 = inv_h * (v[5] - v[4]), d6 = inv_h * (v[6] - v[5]);
   dm = weno_side(d1, d2, d3, d4, d5, eps);
   dp = weno_side(d6, d5, d4, d3, d2, eps);
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory plane ring of the staged stencil kernels
+// ---------------------------------------------------------------------------
+constexpr int kTX = 32, kTY = 8;                     // tile (threads) in x and y
+constexpr int kRW = kTX + 2 * GH, kRH = kTY + 2 * GH;  // staged plane: tile + halo
+constexpr int kRing = 2 * GH + 1;                    // planes k-3 .. k+3
+
+__device__ __forceinline__ int ring_slot(int k) { return ((k % kRing) + kRing) % kRing; }
+
+// Plane k of f (halo included) into its ring slot: row-contiguous loads of
+// the (32+6) x (8+6) window; halo cells beyond the ghost ring (i >= nx+3 or
+// j >= ny+3, only at the tile past the box edge) are not needed and skipped.
+template <class T>
+__device__ __forceinline__ void stage_plane(T* ring, const T* __restrict__ f, const Lay& L, int i0, int j0, int k) {
+  T* dst = ring + ring_slot(k) * (kRW * kRH);
+  const int tid = threadIdx.x + kTX * threadIdx.y;
+  for (int t = tid; t < kRW * kRH; t += kTX * kTY) {
+    const int x = t % kRW, y = t / kRW;
+    const int gi = i0 - GH + x, gj = j0 - GH + y;
+    if (gi < L.nx + GH && gj < L.ny + GH) dst[t] = f[L.at(gi, gj, k)];
+  }
+}
+
+// The seven samples of (tx, ty) in plane k along x, y and z from the ring.
+template <class T>
+__device__ __forceinline__ void ring_samples(const T* ring, int k, T vx[7], T vy[7], T vz[7]) {
+  const int tx = threadIdx.x + GH, ty = threadIdx.y + GH;
+  const T* pc = ring + ring_slot(k) * (kRW * kRH);
+#pragma unroll
+  for (int o = 0; o < 7; ++o) {
+    vx[o] = pc[ty * kRW + tx + o - GH];
+    vy[o] = pc[(ty + o - GH) * kRW + tx];
+    vz[o] = ring[ring_slot(k + o - GH) * (kRW * kRH) + ty * kRW + tx];
+  }
+}
+
+// Grid of a staged kernel: xy tiles times z chunks, enough blocks to fill
+// the GPU a few times over (each chunk re-stages six halo planes).
+struct StagedGrid {
+  dim3 grid;
+  int kchunk;
+};
+inline StagedGrid staged_grid(const Lay& L) {
+  static int sms = 0;
+  if (sms <= 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  const int tx = (L.nx + kTX - 1) / kTX, ty = (L.ny + kTY - 1) / kTY;
+  const int want = 8 * sms;
+  const int chunks = std::max(1, std::min(L.nz, (want + tx * ty - 1) / (tx * ty)));
+  const int kchunk = (L.nz + chunks - 1) / chunks;
+  StagedGrid g;
+  g.grid = dim3(tx, ty, (L.nz + kchunk - 1) / kchunk);
+  g.kchunk = kchunk;
+  return g;
 }
 
 // out = c0*base + c1*(src - dt*(u.grad src)), the level-set update at cell
 // centres; u, v, w are the MAC faces (zero ghosts).  With c0 == 0 the
 // combination is skipped and out is the forward-Euler value.
 template <class T>
-__global__ void k_weno5_levelset(const T* __restrict__ src, const T* __restrict__ base, T* __restrict__ out,
-                                 const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, Lay L,
-                                 Lay Lu, Lay Lv, Lay Lw, T inv_h, T eps, T dt, T c0, T c1) {
-  FS_IJK(L);
-  const int64_t c = L.at(i, j, k);
-  T dxm, dxp, dym, dyp, dzm, dzp;
-  weno_pair(src, c, 1, inv_h, eps, dxm, dxp);
-  weno_pair(src, c, L.px, inv_h, eps, dym, dyp);
-  weno_pair(src, c, L.slab, inv_h, eps, dzm, dzp);
-  const T uc = (u[Lu.at(i + 1, j, k)] + u[Lu.at(i, j, k)]) * T(0.5);
-  const T vc = (v[Lv.at(i, j + 1, k)] + v[Lv.at(i, j, k)]) * T(0.5);
-  const T wc = (w[Lw.at(i, j, k + 1)] + w[Lw.at(i, j, k)]) * T(0.5);
-  const T fe = src[c] - dt * ((uc * (uc > T(0) ? dxm : dxp) + vc * (vc > T(0) ? dym : dyp)) + wc * (wc > T(0) ? dzm : dzp));
-  out[c] = c0 == T(0) ? fe : c0 * base[c] + c1 * fe;
+__global__ void __launch_bounds__(kTX * kTY) k_weno5_levelset(const T* __restrict__ src, const T* __restrict__ base,
+                                                           T* __restrict__ out, const T* __restrict__ u,
+                                                           const T* __restrict__ v, const T* __restrict__ w, Lay L,
+                                                           Lay Lu, Lay Lv, Lay Lw, T inv_h, T eps, T dt, T c0, T c1,
+                                                           int kchunk) {
+  __shared__ T ring[kRing * kRW * kRH];
+  const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int k0 = blockIdx.z * kchunk, k1 = min(L.nz, k0 + kchunk);
+  const bool valid = i < L.nx && j < L.ny;
+  for (int kk = k0 - GH; kk < k0 + GH; ++kk) stage_plane(ring, src, L, i0, j0, kk);
+  for (int k = k0; k < k1; ++k) {
+    stage_plane(ring, src, L, i0, j0, k + GH);
+    __syncthreads();
+    if (valid) {
+      T vx[7], vy[7], vz[7];
+      ring_samples(ring, k, vx, vy, vz);
+      T dxm, dxp, dym, dyp, dzm, dzp;
+      weno_pair7(vx, inv_h, eps, dxm, dxp);
+      weno_pair7(vy, inv_h, eps, dym, dyp);
+      weno_pair7(vz, inv_h, eps, dzm, dzp);
+      const int64_t c = L.at(i, j, k);
+      const T uc = (u[Lu.at(i + 1, j, k)] + u[Lu.at(i, j, k)]) * T(0.5);
+      const T vc = (v[Lv.at(i, j + 1, k)] + v[Lv.at(i, j, k)]) * T(0.5);
+      const T wc = (w[Lw.at(i, j, k + 1)] + w[Lw.at(i, j, k)]) * T(0.5);
+      const T fe =
+          vx[3] - dt * ((uc * (uc > T(0) ? dxm : dxp) + vc * (vc > T(0) ? dym : dyp)) + wc * (wc > T(0) ? dzm : dzp));
+      out[c] = c0 == T(0) ? fe : c0 * base[c] + c1 * fe;
+    }
+    __syncthreads();
+  }
 }
 
-// MAC component self-advection on every face of component `axis` (wall
-// faces included, as the reference's loop covers the whole face grid).
+// The velocities that advect face (i,j,k) of component `axis`: its own
+// component, the four-face averages of the other two.
 template <class T>
-__global__ void k_weno5_mac(const T* __restrict__ comp, T* __restrict__ out, const T* __restrict__ u,
-                            const T* __restrict__ v, const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw, int axis,
-                            T inv_h, T eps, T dt) {
-  FS_IJK(Lc);
-  const int64_t c = Lc.at(i, j, k);
-  T uvel, vvel, wvel;
+__device__ __forceinline__ void mac_velocity(const T* __restrict__ u, const T* __restrict__ v,
+                                             const T* __restrict__ w, const Lay& Lu, const Lay& Lv, const Lay& Lw,
+                                             int axis, int i, int j, int k, T& uvel, T& vvel, T& wvel) {
   if (axis == 0) {
     uvel = u[Lu.at(i, j, k)];
     vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i - 1, j, k)]) + v[Lv.at(i - 1, j + 1, k)]) * T(0.25);
@@ -190,12 +273,38 @@ __global__ void k_weno5_mac(const T* __restrict__ comp, T* __restrict__ out, con
     vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i, j, k - 1)]) + v[Lv.at(i, j + 1, k - 1)]) * T(0.25);
     wvel = w[Lw.at(i, j, k)];
   }
-  T dxm, dxp, dym, dyp, dzm, dzp;
-  weno_pair(comp, c, 1, inv_h, eps, dxm, dxp);
-  weno_pair(comp, c, Lc.px, inv_h, eps, dym, dyp);
-  weno_pair(comp, c, Lc.slab, inv_h, eps, dzm, dzp);
-  out[c] = comp[c] - dt * ((uvel * (uvel > T(0) ? dxm : dxp) + vvel * (vvel > T(0) ? dym : dyp)) +
-                           wvel * (wvel > T(0) ? dzm : dzp));
+}
+
+// MAC component self-advection on every face of component `axis` (wall
+// faces included, as the reference's loop covers the whole face grid).
+template <class T>
+__global__ void __launch_bounds__(kTX * kTY) k_weno5_mac(const T* __restrict__ comp, T* __restrict__ out,
+                                                      const T* __restrict__ u, const T* __restrict__ v,
+                                                      const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw,
+                                                      int axis, T inv_h, T eps, T dt, int kchunk) {
+  __shared__ T ring[kRing * kRW * kRH];
+  const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int k0 = blockIdx.z * kchunk, k1 = min(Lc.nz, k0 + kchunk);
+  const bool valid = i < Lc.nx && j < Lc.ny;
+  for (int kk = k0 - GH; kk < k0 + GH; ++kk) stage_plane(ring, comp, Lc, i0, j0, kk);
+  for (int k = k0; k < k1; ++k) {
+    stage_plane(ring, comp, Lc, i0, j0, k + GH);
+    __syncthreads();
+    if (valid) {
+      T uvel, vvel, wvel;
+      mac_velocity(u, v, w, Lu, Lv, Lw, axis, i, j, k, uvel, vvel, wvel);
+      T vx[7], vy[7], vz[7];
+      ring_samples(ring, k, vx, vy, vz);
+      T dxm, dxp, dym, dyp, dzm, dzp;
+      weno_pair7(vx, inv_h, eps, dxm, dxp);
+      weno_pair7(vy, inv_h, eps, dym, dyp);
+      weno_pair7(vz, inv_h, eps, dzm, dzp);
+      out[Lc.at(i, j, k)] = vx[3] - dt * ((uvel * (uvel > T(0) ? dxm : dxp) + vvel * (vvel > T(0) ? dym : dyp)) +
+                                          wvel * (wvel > T(0) ? dzm : dzp));
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -206,11 +315,7 @@ __global__ void k_weno5_mac(const T* __restrict__ comp, T* __restrict__ out, con
 // d1 (scaled 1/dx), d2 (1/(2dx)), d3 ((1/dx)/3); each side takes the stencil
 // with the smaller |d2|, then the smaller |d3|.
 template <class T>
-__device__ __forceinline__ void eno3_pair(const T* __restrict__ f, int64_t c, int64_t st, T h, T inv, T o2, T o3,
-                                          T& dm, T& dp) {
-  T v[7];
-#pragma unroll
-  for (int s = 0; s < 7; ++s) v[s] = f[c + (s - 3) * st];
+__device__ __forceinline__ void eno3_pair7(const T v[7], T h, T inv, T o2, T o3, T& dm, T& dp) {
   T d1[6], d2[5], d3[4];  // d1[q]: samples q+1 - q (s = q-3); d2[q] from d1[q+1], d1[q]; d3[q] from d2[q+1], d2[q]
 #pragma unroll
   for (int q = 0; q < 6; ++q) d1[q] = inv * (v[q + 1] - v[q]);
@@ -236,32 +341,34 @@ __device__ __forceinline__ void eno3_pair(const T* __restrict__ f, int64_t c, in
 // MAC component self-advection with ENO3 (the reference's use_3rd_eno_v,
 // ADVECTION_3D.h:323-325), every face of component `axis`.
 template <class T>
-__global__ void k_eno3_mac(const T* __restrict__ comp, T* __restrict__ out, const T* __restrict__ u,
-                           const T* __restrict__ v, const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw, int axis,
-                           T h, T dt) {
-  FS_IJK(Lc);
-  const int64_t c = Lc.at(i, j, k);
-  T uvel, vvel, wvel;
-  if (axis == 0) {
-    uvel = u[Lu.at(i, j, k)];
-    vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i - 1, j, k)]) + v[Lv.at(i - 1, j + 1, k)]) * T(0.25);
-    wvel = (((w[Lw.at(i, j, k)] + w[Lw.at(i, j, k + 1)]) + w[Lw.at(i - 1, j, k)]) + w[Lw.at(i - 1, j, k + 1)]) * T(0.25);
-  } else if (axis == 1) {
-    uvel = (((u[Lu.at(i, j, k)] + u[Lu.at(i + 1, j, k)]) + u[Lu.at(i, j - 1, k)]) + u[Lu.at(i + 1, j - 1, k)]) * T(0.25);
-    vvel = v[Lv.at(i, j, k)];
-    wvel = (((w[Lw.at(i, j, k)] + w[Lw.at(i, j, k + 1)]) + w[Lw.at(i, j - 1, k)]) + w[Lw.at(i, j - 1, k + 1)]) * T(0.25);
-  } else {
-    uvel = (((u[Lu.at(i, j, k)] + u[Lu.at(i + 1, j, k)]) + u[Lu.at(i, j, k - 1)]) + u[Lu.at(i + 1, j, k - 1)]) * T(0.25);
-    vvel = (((v[Lv.at(i, j, k)] + v[Lv.at(i, j + 1, k)]) + v[Lv.at(i, j, k - 1)]) + v[Lv.at(i, j + 1, k - 1)]) * T(0.25);
-    wvel = w[Lw.at(i, j, k)];
-  }
+__global__ void __launch_bounds__(kTX * kTY) k_eno3_mac(const T* __restrict__ comp, T* __restrict__ out,
+                                                     const T* __restrict__ u, const T* __restrict__ v,
+                                                     const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw,
+                                                     int axis, T h, T dt, int kchunk) {
+  __shared__ T ring[kRing * kRW * kRH];
+  const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int k0 = blockIdx.z * kchunk, k1 = min(Lc.nz, k0 + kchunk);
+  const bool valid = i < Lc.nx && j < Lc.ny;
   const T inv = T(1) / h, o2 = T(0.5) / h, o3 = inv * T(1) / T(3);
-  T dxm, dxp, dym, dyp, dzm, dzp;
-  eno3_pair(comp, c, 1, h, inv, o2, o3, dxm, dxp);
-  eno3_pair(comp, c, Lc.px, h, inv, o2, o3, dym, dyp);
-  eno3_pair(comp, c, Lc.slab, h, inv, o2, o3, dzm, dzp);
-  out[c] = comp[c] - dt * ((uvel * (uvel > T(0) ? dxm : dxp) + vvel * (vvel > T(0) ? dym : dyp)) +
-                           wvel * (wvel > T(0) ? dzm : dzp));
+  for (int kk = k0 - GH; kk < k0 + GH; ++kk) stage_plane(ring, comp, Lc, i0, j0, kk);
+  for (int k = k0; k < k1; ++k) {
+    stage_plane(ring, comp, Lc, i0, j0, k + GH);
+    __syncthreads();
+    if (valid) {
+      T uvel, vvel, wvel;
+      mac_velocity(u, v, w, Lu, Lv, Lw, axis, i, j, k, uvel, vvel, wvel);
+      T vx[7], vy[7], vz[7];
+      ring_samples(ring, k, vx, vy, vz);
+      T dxm, dxp, dym, dyp, dzm, dzp;
+      eno3_pair7(vx, h, inv, o2, o3, dxm, dxp);
+      eno3_pair7(vy, h, inv, o2, o3, dym, dyp);
+      eno3_pair7(vz, h, inv, o2, o3, dzm, dzp);
+      out[Lc.at(i, j, k)] = vx[3] - dt * ((uvel * (uvel > T(0) ? dxm : dxp) + vvel * (vvel > T(0) ? dym : dyp)) +
+                                          wvel * (wvel > T(0) ? dzm : dzp));
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -295,28 +402,43 @@ __device__ __forceinline__ T godunov(T s, T dm, T dp, int& code, bool& shock) {
 // One pseudo-step phi - dtau*S*(|grad phi|_G - 1) with the sign-preserving
 // clamp; out = c0*base + c1*(that) when c0 != 0 (RK block combination).
 template <class T>
-__global__ void k_sussman(const T* __restrict__ src, const T* __restrict__ sgn, const T* __restrict__ base,
-                          T* __restrict__ out, Lay L, T inv_h, T eps, T dtau, T c0, T c1, int typo) {
-  FS_IJK(L);
-  const int64_t c = L.at(i, j, k);
-  T dxm, dxp, dym, dyp, dzm, dzp;
-  weno_pair(src, c, 1, inv_h, eps, dxm, dxp);
-  weno_pair(src, c, L.px, inv_h, eps, dym, dyp);
-  weno_pair(src, c, L.slab, inv_h, eps, dzm, dzp);
-  const T s = sgn[c];
-  int cx, cy, cz;
-  bool shx, shy, shz;
-  const T gx = godunov(s, dxm, dxp, cx, shx);
-  const T gy = godunov(s, dym, dyp, cy, shy);
-  const T gz = godunov(s, dzm, dzp, cz, shz);
-  T mag = sqrt((gx * gx + gy * gy) + gz * gz) - T(1);
-  if (typo && shx && shy && cy == 1 && cz == 2) mag = (sqrt(gx * gx) + gy * gy) - T(1);
-  T r = src[c] - dtau * s * mag;
-  if (s * r < T(0)) {
-    if (s < T(0)) r = -eps;
-    if (s > T(0)) r = eps;
+__global__ void __launch_bounds__(kTX * kTY) k_sussman(const T* __restrict__ src, const T* __restrict__ sgn,
+                                                    const T* __restrict__ base, T* __restrict__ out, Lay L, T inv_h,
+                                                    T eps, T dtau, T c0, T c1, int typo, int kchunk) {
+  __shared__ T ring[kRing * kRW * kRH];
+  const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int k0 = blockIdx.z * kchunk, k1 = min(L.nz, k0 + kchunk);
+  const bool valid = i < L.nx && j < L.ny;
+  for (int kk = k0 - GH; kk < k0 + GH; ++kk) stage_plane(ring, src, L, i0, j0, kk);
+  for (int k = k0; k < k1; ++k) {
+    stage_plane(ring, src, L, i0, j0, k + GH);
+    __syncthreads();
+    if (valid) {
+      const int64_t c = L.at(i, j, k);
+      T vx[7], vy[7], vz[7];
+      ring_samples(ring, k, vx, vy, vz);
+      T dxm, dxp, dym, dyp, dzm, dzp;
+      weno_pair7(vx, inv_h, eps, dxm, dxp);
+      weno_pair7(vy, inv_h, eps, dym, dyp);
+      weno_pair7(vz, inv_h, eps, dzm, dzp);
+      const T s = sgn[c];
+      int cx, cy, cz;
+      bool shx, shy, shz;
+      const T gx = godunov(s, dxm, dxp, cx, shx);
+      const T gy = godunov(s, dym, dyp, cy, shy);
+      const T gz = godunov(s, dzm, dzp, cz, shz);
+      T mag = sqrt((gx * gx + gy * gy) + gz * gz) - T(1);
+      if (typo && shx && shy && cy == 1 && cz == 2) mag = (sqrt(gx * gx) + gy * gy) - T(1);
+      T r = vx[3] - dtau * s * mag;
+      if (s * r < T(0)) {
+        if (s < T(0)) r = -eps;
+        if (s > T(0)) r = eps;
+      }
+      out[c] = c0 == T(0) ? r : c0 * base[c] + c1 * r;
+    }
+    __syncthreads();
   }
-  out[c] = c0 == T(0) ? r : c0 * base[c] + c1 * r;
 }
 
 // ---------------------------------------------------------------------------
@@ -361,23 +483,25 @@ template <class T>
 void weno5_levelset(const T* src, const T* base, T* out, const T* u, const T* v, const T* w, const Lay& L,
                     const Lay& Lu, const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c0, double c1,
                     cudaStream_t s) {
-  Launch3 g = launch3(L.nx, L.ny, L.nz, 32, 4, 2);
-  k_weno5_levelset<T><<<g.grid, g.block, 0, s>>>(src, base, out, u, v, w, L, Lu, Lv, Lw, T(1.0 / dx), T(eps), T(dt),
-                                                   T(c0), T(c1));
+  const StagedGrid g = staged_grid(L);
+  k_weno5_levelset<T><<<g.grid, dim3(kTX, kTY, 1), 0, s>>>(src, base, out, u, v, w, L, Lu, Lv, Lw, T(1.0 / dx),
+                                                           T(eps), T(dt), T(c0), T(c1), g.kchunk);
 }
 
 template <class T>
 void weno5_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
                const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s) {
-  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz, 32, 4, 2);
-  k_weno5_mac<T><<<g.grid, g.block, 0, s>>>(comp, out, u, v, w, Lc, Lu, Lv, Lw, axis, T(1.0 / dx), T(eps), T(dt));
+  const StagedGrid g = staged_grid(Lc);
+  k_weno5_mac<T><<<g.grid, dim3(kTX, kTY, 1), 0, s>>>(comp, out, u, v, w, Lc, Lu, Lv, Lw, axis, T(1.0 / dx), T(eps),
+                                                      T(dt), g.kchunk);
 }
 
 template <class T>
 void eno3_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
               const Lay& Lw, int axis, double dx, double dt, cudaStream_t s) {
-  Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz, 32, 4, 2);
-  k_eno3_mac<T><<<g.grid, g.block, 0, s>>>(comp, out, u, v, w, Lc, Lu, Lv, Lw, axis, T(dx), T(dt));
+  const StagedGrid g = staged_grid(Lc);
+  k_eno3_mac<T><<<g.grid, dim3(kTX, kTY, 1), 0, s>>>(comp, out, u, v, w, Lc, Lu, Lv, Lw, axis, T(dx), T(dt),
+                                                     g.kchunk);
 }
 
 template <class T>
@@ -389,8 +513,9 @@ void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s
 template <class T>
 void sussman_step(const T* src, const T* sgn, const T* base, T* out, const Lay& L, double dx, double eps, double dtau,
                   double c0, double c1, int typo, cudaStream_t s) {
-  Launch3 g = launch3(L.nx, L.ny, L.nz, 32, 4, 2);
-  k_sussman<T><<<g.grid, g.block, 0, s>>>(src, sgn, base, out, L, T(1.0 / dx), T(eps), T(dtau), T(c0), T(c1), typo);
+  const StagedGrid g = staged_grid(L);
+  k_sussman<T><<<g.grid, dim3(kTX, kTY, 1), 0, s>>>(src, sgn, base, out, L, T(1.0 / dx), T(eps), T(dtau), T(c0),
+                                                    T(c1), typo, g.kchunk);
 }
 
 template <class T>
