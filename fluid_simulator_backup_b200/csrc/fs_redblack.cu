@@ -89,18 +89,20 @@ __global__ void __launch_bounds__(256) k_rb_red(RbOp A, const float* __restrict_
   tau[s] = t;
 }
 
-// black stage: q = S p on the black cell of slot (h, j, k), p.q, alpha
-__global__ void __launch_bounds__(256) k_rb_black(RbOp A, const float* __restrict__ p,
-                                                  const float* __restrict__ tau, float* __restrict__ q, PcgState* st,
-                                                  double* partials) {
+// black stage: q = S p on the black cells, p.q, alpha.  Grid-stride over the
+// slots on the resident blocks only, so that the p.q reduction has a few
+// hundred partial sums (one atomic ticket per block) rather than one per
+// 256 slots.
+__global__ void __launch_bounds__(kRedThreads) k_rb_black(RbOp A, const float* __restrict__ p,
+                                                          const float* __restrict__ tau, float* __restrict__ q,
+                                                          PcgState* st, double* partials) {
   if (((volatile PcgState*)st)->done) return;
-  const int h = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
   const Lay& L = A.L;
   const Lay& H = A.Lh;
   double pq = 0.0;
-  if (h < H.nx && j < H.ny && k < H.nz) {
+  Cursor cur;
+  for (cur.init(H); cur.valid(H); cur.next(H)) {
+    const int h = cur.i, j = cur.j, k = cur.k;
     const int pb = (j + k + 1) & 1;
     const int i = 2 * h + pb;
     const int64_t s = H.at(h, j, k);
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(256) k_rb_black(RbOp A, const float* __restric
       acc += aym * (dym - tym) + ayp * (dyp - typ);
       acc += azm * (dzm - tzm) + azp * (dzp - tzp);
       qv = acc;
-      pq = (double)pc * (double)qv;
+      pq += (double)pc * (double)qv;
     }
     q[s] = qv;
   }
@@ -206,16 +208,14 @@ const dim3 kRbBlock(32, 4, 2);
 
 }  // namespace
 
-int rb_blocks(const Lay& H) {
-  const dim3 g = rb_grid(H);
-  return (int)(g.x * g.y * g.z);
-}
+int rb_blocks(const Lay& H) { return reduction_blocks((int64_t)H.nx * H.ny * H.nz); }
 
 void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
                   PcgState* st, double* partials, cudaStream_t s) {
   const dim3 grd = rb_grid(A.Lh);
   k_rb_red<<<grd, kRbBlock, 0, s>>>(A, ph, tau);
-  k_rb_black<<<grd, kRbBlock, 0, s>>>(A, ph, tau, qh, st, partials);
+  k_rb_black<<<reduction_blocks((int64_t)A.Lh.nx * A.Lh.ny * A.Lh.nz), kRedThreads, 0, s>>>(A, ph, tau, qh, st,
+                                                                                           partials);
   cg_vector_updates<float, double>(Ah, xh, rh, ph, qh, st, partials, s);
 }
 
