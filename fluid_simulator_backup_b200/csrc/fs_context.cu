@@ -260,35 +260,72 @@ void apply_params(fs_ctx* c) {
 // Krylov driver
 // ---------------------------------------------------------------------------
 
-// Launch captured batches of kGraphIters iterations until the solver state
-// says stop (done != 0); one host check of the state per batch.
+// The loop control of a captured solve: before the loop it clears the batch
+// counter and lets the loop start only if the solve is still running; after
+// each batch of kGraphIters iterations it continues the loop while the solve
+// runs and fewer than max_iter / kGraphIters + 2 batches have run (the
+// bound that guarantees the loop ends whatever the state says).
+__global__ void k_loop_start(cudaGraphConditionalHandle h, const PcgState* st, unsigned int* batches) {
+  *batches = 0u;
+  cudaGraphSetConditional(h, ((volatile const PcgState*)st)->done == 0 ? 1u : 0u);
+}
+__global__ void k_loop_next(cudaGraphConditionalHandle h, const PcgState* st, unsigned int* batches) {
+  const volatile PcgState* vs = (volatile const PcgState*)st;
+  const unsigned int n = *batches + 1u;
+  *batches = n;
+  const unsigned int cap = (unsigned int)(vs->max_iter / kGraphIters + 2);
+  cudaGraphSetConditional(h, (vs->done == 0 && n < cap) ? 1u : 0u);
+}
+
+// Run the iterations of a solve until its state says stop (done != 0), as
+// ONE graph launch: a captured CUDA graph whose conditional while node
+// repeats a body of kGraphIters iterations plus the loop control above, so
+// the host waits once per solve (or per reliable update of the mixed
+// solve) instead of once per batch.  The graph is captured on first use per
+// key (kernel arguments are baked into it).
 template <class F>
 fs_status drive_pcg(fs_ctx* c, std::pair<int, const void*> key, F&& enqueue_iteration, int max_iter, bool timed,
                     int kernels_per_iteration = 3) {
+  (void)max_iter;  // the device-side bound reads max_iter from the solver state
+  unsigned int* batches = c->tickets + 6;
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    for (int n = 0; n < kGraphIters; ++n) enqueue_iteration();
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    // the loop start, then the while node
+    CK(cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    k_loop_start<<<1, 1, 0, c->stream>>>(h, c->st, batches);
     CK(cudaStreamEndCapture(c->stream, &g));
+    cudaGraphNode_t start = nullptr;
+    size_t nroots = 1;
+    CK(cudaGraphGetRootNodes(g, &start, &nroots));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop = nullptr;
+    CK(cudaGraphAddNode(&loop, g, &start, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (int n = 0; n < kGraphIters; ++n) enqueue_iteration();
+    k_loop_next<<<1, 1, 0, c->stream>>>(h, c->st, batches);
+    CK(cudaStreamEndCapture(c->stream, &body));
     cudaGraphExec_t ge;
     CK(cudaGraphInstantiate(&ge, g, 0));
     cudaGraphDestroy(g);
     it = c->graphs.emplace(key, ge).first;
   }
-  // the kernels of a stopped solve return at once, so the bound below only
-  // caps the number of host checks
-  const int max_launches = max_iter / kGraphIters + 2;
-  for (int n = 0; n < max_launches; ++n) {
-    CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    if (c->st_host->done) return FS_OK;
-    CK(cudaGraphLaunch(it->second, c->stream));
-    c->launches += (int64_t)kernels_per_iteration * kGraphIters;
-    if (timed) c->pcg_launched_iterations += kGraphIters;
-  }
+  CK(cudaGraphLaunch(it->second, c->stream));
   CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+  unsigned int nb = 0;
+  CK(cudaMemcpyAsync(c->sc_host + 15, batches, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(&nb, c->sc_host + 15, sizeof nb);
+  c->launches += 1 + (int64_t)nb * (kernels_per_iteration * kGraphIters + 1);
+  if (timed) c->pcg_launched_iterations += (int)nb * kGraphIters;
   return FS_OK;
 }
 
@@ -640,9 +677,10 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
       // the residual already holds the image of b - A p64: start the recursion from it
       pcg_resume<float, float>(KA, kr, kp, c->st, c->partials, 1, s);
       c->launches += 2;
-      int failures = 0;
+      int failures = 0, passes = 0;
       double best = rel;
       for (;;) {
+        ++passes;  // each pass runs at least one iteration or ends the solve; this bounds the host loop too
         if (rb) {
           CKS(drive_pcg(c, std::make_pair(4, (const void*)nullptr),
                         [&] {
@@ -685,7 +723,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
           std::fprintf(stderr, "[fs] mixed solve%s: iteration %d, status %d, recursive %.3e, true %.3e, best %.3e%s\n",
                        rb ? " (red-black)" : "", iters, status, recursive, now, best, restart ? ", restart" : "");
         if (now <= P.tolerance) { st = PCG_CONVERGED; break; }
-        if (iters >= P.max_iteration || failures > 8) {
+        if (iters >= P.max_iteration || failures > 8 || passes > P.max_iteration + 8) {
           // leave the best pressure found
           CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
           rel = best;
