@@ -122,8 +122,9 @@ struct fs_ctx {
   std::vector<void*> tape_cells, tape_faces;  // taped forward states (storage precision), allocated on demand
   std::vector<double*> tape_p;                // taped stage pressures (FP64)
   // FP64 operator and Krylov vectors of the adjoint solves: the forward's own
-  // buffers in FP64 contexts, separate ones in FP32 contexts (one viscosity
-  // system set shared by the three components there)
+  // buffers in FP64 contexts; FP32 contexts solve the pressure adjoint with
+  // the mixed solve and keep one FP64 viscosity system set shared by the
+  // three components
   double *a_ax = nullptr, *a_ay = nullptr, *a_az = nullptr, *a_diag = nullptr;
   double *a_r = nullptr, *a_p = nullptr, *a_q = nullptr;
   double* a_vs[3][9] = {};
@@ -558,6 +559,173 @@ fs_status viscosity_t(fs_ctx* c, double dt, int* iters_out) {
   return FS_OK;
 }
 
+// The FP32 + FP64 defect-correction solve of A(phi) x = b (A the pressure
+// operator evaluated from phi, b and x FP64 cell fields): the projection's
+// solve and, in FP32 contexts, the adjoint's transposed solve with the same
+// symmetric operator.  *iters, *outer, *rel and *st report the Krylov
+// iterations, the defect corrections, the final relative FP64 residual and
+// the PCG status.
+template <class S>
+fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, int* outer_out, double* rel_out,
+                      int* st_out) {
+  const fs_params& P = c->prm;
+  const double dx = c->grid.dx;
+  cudaStream_t s = c->stream;
+  int iters = 0, outer = 0, st = 0;
+  double rel = 0.0;
+  const bool rb = c->red_black;
+  build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
+                                    (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s,
+                                    (c->lean || rb) ? c->pdinv : nullptr);
+  Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
+  A.flux32 = c->flux32;
+  if (c->lean) A.dinv16 = c->pdinv;
+  // red-black: the black Schur complement on the packed half layout, its
+  // Jacobi preconditioner the black cells' bf16 1/diag
+  RbOp R{(float*)c->pax, (float*)c->pay, (float*)c->paz, c->Lc, c->Lh, c->scalars + 12};
+  Op7<float> Ah{nullptr, nullptr, nullptr, nullptr, c->Lh};
+  Ah.dinv16 = c->rb_dinv;
+  if (rb) {
+    rb_gather<unsigned short, unsigned short>(c->pdinv, c->rb_dinv, c->Lc, c->Lh, s);
+    rb_gather<double, double>(x, c->rb_x, c->Lc, c->Lh, s);  // the initial guess's black cells
+    c->launches += 2;
+  }
+  double bb = 0.0;
+  float *r32 = (float*)c->pr, *p32 = (float*)c->pp, *q32 = (float*)c->pq;
+  // the Krylov vectors of the chosen form
+  float* kr = rb ? c->rb_r : r32;
+  float* kp = rb ? c->rb_p : p32;
+  const Op7<float>& KA = rb ? Ah : A;
+  // red-black: p64 <- the black iterate, red cells eliminated in FP64
+  auto commit = [&]() {
+    if (!rb) return;
+    rb_commit<S>(phi, c->rb_x, b, x, c->Lc, c->Lh, dx, P.rho_neg, P.rho_pos, s);
+    c->launches += 1;
+  };
+  // true FP64 residual b - A64 p64 with A64 evaluated from phi in FP64; its
+  // FP32 image lands in r32 (red-black: its black cells in the packed
+  // residual), the Krylov residual of the mixed solve
+  auto defect = [&](const float* x32, double* rel_out) -> fs_status {
+    defect_residual<S>(phi, x, x32, b, nullptr, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
+                       c->tickets + 2, c->scalars + 2, s);
+    c->launches += 1;
+    if (rb) {
+      rb_gather<float, float>(r32, c->rb_r, c->Lc, c->Lh, s);
+      c->launches += 1;
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    bb = c->sc_host[1];
+    const double rr = c->sc_host[2];
+    *rel_out = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+    outer += 1;
+    if (!std::isfinite(*rel_out) && !x32) {
+      set_error("non-finite defect residual");
+      return FS_NONFINITE;
+    }
+    return FS_OK;
+  };
+  commit();
+  CKS(defect(nullptr, &rel));
+  st = PCG_CONVERGED;
+  if (rel > P.tolerance) {
+    // Mixed-precision CG: the FP64 pressure p64 (red-black: its black cells,
+    // packed) is the iterate; the face couplings, the residual r, the
+    // search direction p and q = A p are FP32 (the flux-form operator in
+    // FP32 arithmetic, Op7::flux32, or the red-black Schur complement in
+    // its offset form) and the Jacobi preconditioner is 1/diag in bf16: 64
+    // bytes per unknown and iteration (red-black: 56 at half the
+    // iterations) against 120 for the FP64 solve.  Every time the recursive
+    // residual drops by reliable_delta the true FP64 residual of p64
+    // replaces it (reliable update), keeping the search direction; the
+    // recursion stops at the tolerance itself and the true residual
+    // decides.  A sequence whose true residual got worse is rolled back to
+    // the last accepted pressure and restarted.
+    const size_t pbytes = c->Lc.total * sizeof(double);
+    CK(cudaMemcpyAsync(c->p64bak, x, pbytes, cudaMemcpyDeviceToDevice, s));
+    PcgState init{};
+    init.criterion = 2;  // absolute 2-norm of the recursive residual, in b's units
+    init.tol = P.tolerance * std::sqrt(bb);
+    init.max_iter = P.max_iteration;
+    init.reliable_delta = c->reliable_delta;
+    init.bb = bb;  // ||b||^2 of the pressure system, for the recursive relative residual
+    *c->st_host = init;
+    CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
+    CK(cudaEventRecord(c->evp0, s));
+    // the residual already holds the image of b - A p64: start the recursion from it
+    pcg_resume<float, float>(KA, kr, kp, c->st, c->partials, 1, s);
+    c->launches += 2;
+    int failures = 0, passes = 0;
+    double best = rel;
+    for (;;) {
+      ++passes;  // each pass runs at least one iteration or ends the solve; this bounds the host loop too
+      if (rb) {
+        CKS(drive_pcg(c, std::make_pair(4, (const void*)nullptr),
+                      [&] {
+                        rb_iteration(R, Ah, c->rb_x, c->rb_r, c->rb_p, c->rb_q, c->rb_tau, c->st, c->partials, s);
+                      },
+                      P.max_iteration, true, 4));
+      } else {
+        CKS(drive_pcg(c, std::make_pair(2, (const void*)x),
+                      [&] { cg_iteration<float, double>(A, x, r32, p32, q32, c->st, c->partials, s); },
+                      P.max_iteration, true));
+      }
+      const int status = c->st_host->status;
+      iters = c->st_host->iter;
+      const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
+      double now = 0.0;
+      commit();
+      CKS(defect(nullptr, &now));  // residual <- true residual of the current pressure
+      bool restart = false;
+      if (!std::isfinite(now) || now > 100.0 * best) {
+        // diverged (not a CG residual oscillation): back to the best pressure
+        CK(cudaMemcpyAsync(x, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
+        if (rb) {
+          rb_gather<double, double>(x, c->rb_x, c->Lc, c->Lh, s);
+          c->launches += 1;
+        }
+        CKS(defect(nullptr, &now));
+        restart = true;
+        ++failures;
+      } else {
+        if (now < best) {
+          best = now;
+          CK(cudaMemcpyAsync(c->p64bak, x, pbytes, cudaMemcpyDeviceToDevice, s));
+        }
+        // restart the direction after a breakdown or when the recursion
+        // has drifted far from the true residual
+        restart = status == PCG_STAGNATED || now > 10.0 * recursive;
+      }
+      rel = now;
+      if (c->debug)
+        std::fprintf(stderr, "[fs] mixed solve%s: iteration %d, status %d, recursive %.3e, true %.3e, best %.3e%s\n",
+                     rb ? " (red-black)" : "", iters, status, recursive, now, best, restart ? ", restart" : "");
+      if (now <= P.tolerance) { st = PCG_CONVERGED; break; }
+      if (iters >= P.max_iteration || failures > 8 || passes > P.max_iteration + 8) {
+        // leave the best pressure found
+        CK(cudaMemcpyAsync(x, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
+        rel = best;
+        st = PCG_MAXITER;
+        break;
+      }
+      pcg_resume<float, float>(KA, kr, kp, c->st, c->partials, restart ? 1 : 0, s);
+      c->launches += 2;
+      CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(c->evp1, s));
+    CK(cudaEventSynchronize(c->evp1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
+    c->pcg_ms += ms;
+  }
+  *iters_out = iters;
+  *outer_out = outer;
+  *rel_out = rel;
+  *st_out = st;
+  return FS_OK;
+}
+
 // PROJECTION_3D::Solve; c0/c1 fuse the RK combination with base (u0, v0, w0)
 template <class S>
 fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report* rep) {
@@ -594,152 +762,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
                         P.max_iteration, P.stop, &iters, &rel, &st));
     outer = 1;
   } else {
-    const bool rb = c->red_black;
-    build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
-                                      (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s,
-                                      (c->lean || rb) ? c->pdinv : nullptr);
-    Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
-    A.flux32 = c->flux32;
-    if (c->lean) A.dinv16 = c->pdinv;
-    // red-black: the black Schur complement on the packed half layout, its
-    // Jacobi preconditioner the black cells' bf16 1/diag
-    RbOp R{(float*)c->pax, (float*)c->pay, (float*)c->paz, c->Lc, c->Lh, c->scalars + 12};
-    Op7<float> Ah{nullptr, nullptr, nullptr, nullptr, c->Lh};
-    Ah.dinv16 = c->rb_dinv;
-    if (rb) {
-      rb_gather<unsigned short, unsigned short>(c->pdinv, c->rb_dinv, c->Lc, c->Lh, s);
-      rb_gather<double, double>(c->p64, c->rb_x, c->Lc, c->Lh, s);  // the initial guess's black cells
-      c->launches += 2;
-    }
-    double bb = 0.0;
-    float *r32 = (float*)c->pr, *p32 = (float*)c->pp, *q32 = (float*)c->pq;
-    // the Krylov vectors of the chosen form
-    float* kr = rb ? c->rb_r : r32;
-    float* kp = rb ? c->rb_p : p32;
-    const Op7<float>& KA = rb ? Ah : A;
-    // red-black: p64 <- the black iterate, red cells eliminated in FP64
-    auto commit = [&]() {
-      if (!rb) return;
-      rb_commit<S>(phi, c->rb_x, c->b64, c->p64, c->Lc, c->Lh, dx, P.rho_neg, P.rho_pos, s);
-      c->launches += 1;
-    };
-    // true FP64 residual b - A64 p64 with A64 evaluated from phi in FP64; its
-    // FP32 image lands in r32 (red-black: its black cells in the packed
-    // residual), the Krylov residual of the mixed solve
-    auto defect = [&](const float* x32, double* rel_out) -> fs_status {
-      defect_residual<S>(phi, c->p64, x32, c->b64, nullptr, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
-                         c->tickets + 2, c->scalars + 2, s);
-      c->launches += 1;
-      if (rb) {
-        rb_gather<float, float>(r32, c->rb_r, c->Lc, c->Lh, s);
-        c->launches += 1;
-      }
-      CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(c->sc_host, c->scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      bb = c->sc_host[1];
-      const double rr = c->sc_host[2];
-      *rel_out = bb > 0 ? std::sqrt(rr / bb) : 0.0;
-      outer += 1;
-      if (!std::isfinite(*rel_out) && !x32) {
-        set_error("non-finite defect residual");
-        return FS_NONFINITE;
-      }
-      return FS_OK;
-    };
-    commit();
-    CKS(defect(nullptr, &rel));
-    st = PCG_CONVERGED;
-    if (rel > P.tolerance) {
-      // Mixed-precision CG: the FP64 pressure p64 (red-black: its black cells,
-      // packed) is the iterate; the face couplings, the residual r, the
-      // search direction p and q = A p are FP32 (the flux-form operator in
-      // FP32 arithmetic, Op7::flux32, or the red-black Schur complement in
-      // its offset form) and the Jacobi preconditioner is 1/diag in bf16: 64
-      // bytes per unknown and iteration (red-black: 56 at half the
-      // iterations) against 120 for the FP64 solve.  Every time the recursive
-      // residual drops by reliable_delta the true FP64 residual of p64
-      // replaces it (reliable update), keeping the search direction; the
-      // recursion stops at the tolerance itself and the true residual
-      // decides.  A sequence whose true residual got worse is rolled back to
-      // the last accepted pressure and restarted.
-      const size_t pbytes = c->Lc.total * sizeof(double);
-      CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
-      PcgState init{};
-      init.criterion = 2;  // absolute 2-norm of the recursive residual, in b's units
-      init.tol = P.tolerance * std::sqrt(bb);
-      init.max_iter = P.max_iteration;
-      init.reliable_delta = c->reliable_delta;
-      init.bb = bb;  // ||b||^2 of the pressure system, for the recursive relative residual
-      *c->st_host = init;
-      CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, s));
-      CK(cudaEventRecord(c->evp0, s));
-      // the residual already holds the image of b - A p64: start the recursion from it
-      pcg_resume<float, float>(KA, kr, kp, c->st, c->partials, 1, s);
-      c->launches += 2;
-      int failures = 0, passes = 0;
-      double best = rel;
-      for (;;) {
-        ++passes;  // each pass runs at least one iteration or ends the solve; this bounds the host loop too
-        if (rb) {
-          CKS(drive_pcg(c, std::make_pair(4, (const void*)nullptr),
-                        [&] {
-                          rb_iteration(R, Ah, c->rb_x, c->rb_r, c->rb_p, c->rb_q, c->rb_tau, c->st, c->partials, s);
-                        },
-                        P.max_iteration, true, 4));
-        } else {
-          CKS(drive_pcg(c, std::make_pair(2, (const void*)nullptr),
-                        [&] { cg_iteration<float, double>(A, c->p64, r32, p32, q32, c->st, c->partials, s); },
-                        P.max_iteration, true));
-        }
-        const int status = c->st_host->status;
-        iters = c->st_host->iter;
-        const double recursive = c->st_host->bb > 0 ? std::sqrt(c->st_host->rr / c->st_host->bb) : 0.0;
-        double now = 0.0;
-        commit();
-        CKS(defect(nullptr, &now));  // residual <- true residual of the current pressure
-        bool restart = false;
-        if (!std::isfinite(now) || now > 100.0 * best) {
-          // diverged (not a CG residual oscillation): back to the best pressure
-          CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
-          if (rb) {
-            rb_gather<double, double>(c->p64, c->rb_x, c->Lc, c->Lh, s);
-            c->launches += 1;
-          }
-          CKS(defect(nullptr, &now));
-          restart = true;
-          ++failures;
-        } else {
-          if (now < best) {
-            best = now;
-            CK(cudaMemcpyAsync(c->p64bak, c->p64, pbytes, cudaMemcpyDeviceToDevice, s));
-          }
-          // restart the direction after a breakdown or when the recursion
-          // has drifted far from the true residual
-          restart = status == PCG_STAGNATED || now > 10.0 * recursive;
-        }
-        rel = now;
-        if (c->debug)
-          std::fprintf(stderr, "[fs] mixed solve%s: iteration %d, status %d, recursive %.3e, true %.3e, best %.3e%s\n",
-                       rb ? " (red-black)" : "", iters, status, recursive, now, best, restart ? ", restart" : "");
-        if (now <= P.tolerance) { st = PCG_CONVERGED; break; }
-        if (iters >= P.max_iteration || failures > 8 || passes > P.max_iteration + 8) {
-          // leave the best pressure found
-          CK(cudaMemcpyAsync(c->p64, c->p64bak, pbytes, cudaMemcpyDeviceToDevice, s));
-          rel = best;
-          st = PCG_MAXITER;
-          break;
-        }
-        pcg_resume<float, float>(KA, kr, kp, c->st, c->partials, restart ? 1 : 0, s);
-        c->launches += 2;
-        CK(cudaGetLastError());
-      }
-      CK(cudaEventRecord(c->evp1, s));
-      CK(cudaEventSynchronize(c->evp1));
-      float ms = 0.0f;
-      CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
-      c->pcg_ms += ms;
-    }
+    CKS(mixed_solve<S>(c, phi, c->b64, c->p64, &iters, &outer, &rel, &st));
   }
   velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
                       kap, sigma, s);
@@ -920,8 +943,9 @@ fs_status adj_alloc(fs_ctx* c) {
     for (int a = 0; a < 3; ++a)
       for (int m = 0; m < 9; ++m) c->a_vs[a][m] = (double*)c->vs[a][m];
   } else {
-    double** ops[] = {&c->a_ax, &c->a_ay, &c->a_az, &c->a_diag, &c->a_r, &c->a_p, &c->a_q};
-    for (double** p : ops) CKS(dalloc(c, (void**)p, cb));
+    // FP32 contexts: the transposed pressure solve reuses the forward's
+    // FP32 + FP64 refinement machinery; only the viscosity systems need FP64
+    // buffers of their own
     if (c->prm.viscosity == 1) {
       const size_t fmax = std::max(fb[0], std::max(fb[1], fb[2]));
       for (int m = 0; m < 9; ++m) {
@@ -1055,9 +1079,6 @@ fs_status adj_projection(fs_ctx* c, void* phi, void* const ustar[3], const doubl
   const double dx = c->grid.dx;
   cudaStream_t s = c->stream;
   (void)ustar;  // the map is affine in u*: its derivative does not depend on it
-  build_pressure_operator<S, double>(F<S>(phi), c->Lc, dx, P.rho_neg, P.rho_pos, c->a_ax, c->a_ay, c->a_az,
-                                     c->a_diag, c->scalars + 12, s);
-  Op7<double> A{c->a_ax, c->a_ay, c->a_az, c->a_diag, c->Lc, 1, c->scalars + 12};
   double *pbar = c->awork_c[0], *lam = c->awork_c[1];
   CKS(zero_cell(c, pbar));
   CKS(zero_cell(c, lam));
@@ -1067,12 +1088,22 @@ fs_status adj_projection(fs_ctx* c, void* phi, void* const ustar[3], const doubl
                    P.rho_neg, P.rho_pos, c1, s);
   c->launches += 5;
   CK(cudaGetLastError());
-  // lambda = A^-1 p_bar (A symmetric): the second solve with the same operator
+  // lambda = A^-1 p_bar (A symmetric): the second solve with the same
+  // operator, to the forward's tolerance relative to its own right-hand
+  // side, in the forward's arithmetic: FP64 PCG in FP64 contexts, the FP32
+  // solve with FP64 defect correction in FP32 contexts
   int it = 0, st = 0;
   double rel = 0.0;
-  // the adjoint solve runs to the forward's tolerance, relative to its own right-hand side
-  CKS(run_pcg<double>(c, 3, A, pbar, lam, c->a_r, c->a_p, c->a_q, P.tolerance, std::max(P.max_iteration, 1),
-                      FS_STOP_RELATIVE, &it, &rel, &st));
+  if constexpr (sizeof(S) == sizeof(float)) {
+    int outer = 0;
+    CKS(mixed_solve<S>(c, F<S>(phi), pbar, lam, &it, &outer, &rel, &st));
+  } else {
+    build_pressure_operator<S, double>(F<S>(phi), c->Lc, dx, P.rho_neg, P.rho_pos, c->a_ax, c->a_ay, c->a_az,
+                                       c->a_diag, c->scalars + 12, s);
+    Op7<double> A{c->a_ax, c->a_ay, c->a_az, c->a_diag, c->Lc, 1, c->scalars + 12};
+    CKS(run_pcg<double>(c, 3, A, pbar, lam, c->a_r, c->a_p, c->a_q, P.tolerance, std::max(P.max_iteration, 1),
+                        FS_STOP_RELATIVE, &it, &rel, &st));
+  }
   adj_sum(lam, c->Lc, c->partials, c->tickets + 4, c->scalars + 14, s);
   for (int a = 0; a < 3; ++a) adj_divergence(lam, c->scalars + 14, in_bar[a], *lays[a], c->Lc, a, dx, dt, s);
   adj_pressure_operator<S>(F<S>(phi), lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, s);
