@@ -150,6 +150,121 @@ __global__ void __launch_bounds__(kRedThreads) k_rb_black(RbOp A, const float* _
   }
 }
 
+// q = S p in one pass: both stages fused, z-marching.  A block owns a tile of
+// 32 x 8 packed slots (64 x 8 cells) and walks a chunk of z planes.  At
+// plane k it computes tau of the red cells of plane k+1 for the tile and a
+// one-slot halo in x and y into a three-plane ring in shared memory, then
+// q of the black cells of plane k from the ring (tau of the four in-plane
+// red neighbours and of the two above and below).  The couplings and p are
+// read by both stages within a plane or two of each other, so HBM carries
+// them about once: 12 (couplings) + 2 (p) + 2 (q) bytes per cell instead of
+// the 34 of the two-kernel form.  p.q is reduced per block and finished by
+// the last block (resident blocks only).
+constexpr int kFX = 32, kFY = 8;
+constexpr int kTW = kFX + 2, kTH = kFY + 2;  // tau plane: tile + one-slot halo
+
+__device__ __forceinline__ float rb_tau_at(const RbOp& A, const float* __restrict__ p, int h, int j, int k) {
+  const Lay& L = A.L;
+  const Lay& H = A.Lh;
+  if (h < 0 || j < 0 || k < 0 || h >= H.nx || j >= H.ny || k >= H.nz) return 0.0f;
+  const int pr = (j + k) & 1;
+  const int i = 2 * h + pr;
+  if (i >= L.nx) return 0.0f;
+  const int64_t s = H.at(h, j, k);
+  const int64_t c = L.at(i, j, k);
+  const float pxm = p[s + pr - 1], pxp = p[s + pr];
+  const float pym = p[s - H.px], pyp = p[s + H.px];
+  const float pzm = p[s - H.slab], pzp = p[s + H.slab];
+  const float axm = A.ax[c], axp = A.ax[c + 1];
+  const float aym = A.ay[c], ayp = A.ay[c + L.px];
+  const float azm = A.az[c], azp = A.az[c + L.slab];
+  const float b0 = i > 0 ? pxm : pxp;
+  float num = axm * (pxm - b0) + axp * (pxp - b0);
+  num += aym * (pym - b0) + ayp * (pyp - b0);
+  num += azm * (pzm - b0) + azp * (pzp - b0);
+  float d = ((axm + axp) + (aym + ayp)) + (azm + azp);
+  if (i == 0 && j == 0 && k == 0) {
+    const float e0 = (float)(*A.extra0);
+    num -= e0 * b0;
+    d += e0;
+  }
+  return d > 0.0f ? num / d : 0.0f;
+}
+
+// tau of plane k (tile + halo) into its ring slot
+__device__ __forceinline__ void rb_tau_plane(const RbOp& A, const float* __restrict__ p, float* ring, int h0, int j0,
+                                             int k) {
+  float* dst = ring + ((k % 3 + 3) % 3) * (kTW * kTH);
+  const int tid = threadIdx.x + kFX * threadIdx.y;
+  for (int t = tid; t < kTW * kTH; t += kFX * kFY) {
+    const int x = t % kTW, y = t / kTW;
+    dst[t] = rb_tau_at(A, p, h0 - 1 + x, j0 - 1 + y, k);
+  }
+}
+
+__global__ void __launch_bounds__(kFX * kFY) k_rb_spmv(RbOp A, const float* __restrict__ p, float* __restrict__ q,
+                                                     PcgState* st, double* partials, int kchunk) {
+  if (((volatile PcgState*)st)->done) return;
+  __shared__ float ring[3 * kTW * kTH];
+  const Lay& L = A.L;
+  const Lay& H = A.Lh;
+  const int h0 = blockIdx.x * kFX, j0 = blockIdx.y * kFY;
+  const int h = h0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int k0 = blockIdx.z * kchunk, k1 = min(H.nz, k0 + kchunk);
+  const int tx = threadIdx.x + 1, ty = threadIdx.y + 1;
+  double pq = 0.0;
+  rb_tau_plane(A, p, ring, h0, j0, k0 - 1);
+  rb_tau_plane(A, p, ring, h0, j0, k0);
+  for (int k = k0; k < k1; ++k) {
+    rb_tau_plane(A, p, ring, h0, j0, k + 1);
+    __syncthreads();
+    if (h < H.nx && j < H.ny) {
+      const int pb = (j + k + 1) & 1;
+      const int i = 2 * h + pb;
+      const int64_t s = H.at(h, j, k);
+      float qv = 0.0f;
+      if (i < L.nx) {
+        const int64_t c = L.at(i, j, k);
+        const float pc = p[s];
+        const float axm = A.ax[c], axp = A.ax[c + 1];
+        const float aym = A.ay[c], ayp = A.ay[c + L.px];
+        const float azm = A.az[c], azp = A.az[c + L.slab];
+        const float* t0 = ring + (k % 3) * (kTW * kTH);
+        const float* tm = ring + ((k + 2) % 3) * (kTW * kTH);
+        const float* tp = ring + ((k + 1) % 3) * (kTW * kTH);
+        const float txm = t0[ty * kTW + tx + pb - 1], txp = t0[ty * kTW + tx + pb];
+        const float tym = t0[(ty - 1) * kTW + tx], typ = t0[(ty + 1) * kTW + tx];
+        const float tzm = tm[ty * kTW + tx], tzp = tp[ty * kTW + tx];
+        const int o = i > 0 ? pb - 1 : 0;
+        const float dxm = i > 1 ? pc - p[s - 1] : 0.0f;
+        const float dym = pc - p[s - H.px + o], dyp = pc - p[s + H.px + o];
+        const float dzm = pc - p[s - H.slab + o], dzp = pc - p[s + H.slab + o];
+        float acc = axm * (dxm - txm) + axp * (0.0f - txp);
+        acc += aym * (dym - tym) + ayp * (dyp - typ);
+        acc += azm * (dzm - tzm) + azp * (dzp - tzp);
+        qv = acc;
+        pq += (double)pc * (double)qv;
+      }
+      q[s] = qv;
+    }
+    __syncthreads();
+  }
+  pq = block_sum(pq);
+  double tot;
+  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) {
+    st->pq = tot;
+    const double alpha = st->rz / tot;
+    if (!(tot > 0.0) || !isfinite(alpha)) {
+      st->status = PCG_STAGNATED;
+      st->done = 1;
+      st->x_pending = 0;
+    } else {
+      st->alpha = alpha;
+      st->x_pending = 1;
+    }
+  }
+}
+
 // The FP64 pressure from the packed black iterate: black cells copied, red
 // cells eliminated exactly with the FP64 operator evaluated from phi (the
 // same face coefficients and deflation term as the defect residual), so
@@ -208,14 +323,31 @@ const dim3 kRbBlock(32, 4, 2);
 
 }  // namespace
 
-int rb_blocks(const Lay& H) { return reduction_blocks((int64_t)H.nx * H.ny * H.nz); }
+
+// Grid of the fused SpMV: xy tiles times as many z chunks as fill the
+// resident blocks of the GPU (a chunk re-computes its two halo tau planes).
+struct FusedGrid {
+  dim3 grid;
+  int kchunk;
+};
+FusedGrid fused_grid(const Lay& H) {
+  const int tx = (H.nx + kFX - 1) / kFX, ty = (H.ny + kFY - 1) / kFY;
+  const int want = reduction_blocks((int64_t)1 << 40);  // the resident-block cap of the reductions
+  const int chunks = std::max(1, std::min(H.nz, want / std::max(1, tx * ty)));
+  const int kchunk = (H.nz + chunks - 1) / chunks;
+  return {dim3(tx, ty, (H.nz + kchunk - 1) / kchunk), kchunk};
+}
+
+int rb_blocks(const Lay& H) {
+  const FusedGrid g = fused_grid(H);
+  return std::max((int)(g.grid.x * g.grid.y * g.grid.z), reduction_blocks((int64_t)H.nx * H.ny * H.nz));
+}
 
 void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
                   PcgState* st, double* partials, cudaStream_t s) {
-  const dim3 grd = rb_grid(A.Lh);
-  k_rb_red<<<grd, kRbBlock, 0, s>>>(A, ph, tau);
-  k_rb_black<<<reduction_blocks((int64_t)A.Lh.nx * A.Lh.ny * A.Lh.nz), kRedThreads, 0, s>>>(A, ph, tau, qh, st,
-                                                                                           partials);
+  (void)tau;  // the fused SpMV keeps tau in shared memory
+  const FusedGrid g = fused_grid(A.Lh);
+  k_rb_spmv<<<g.grid, dim3(kFX, kFY, 1), 0, s>>>(A, ph, qh, st, partials, g.kchunk);
   cg_vector_updates<float, double>(Ah, xh, rh, ph, qh, st, partials, s);
 }
 
