@@ -191,6 +191,150 @@ def adjoint_steps(fs, n, warmup, steps):
             "steps": steps}
 
 
+class _TimedSolver:
+    """The solver seen by the checkpoint schedules, keeping the library's
+    device time of every forward and adjoint step."""
+
+    def __init__(self, s):
+        self.s, self.fwd, self.adj = s, [], []
+
+    def step(self, dt):
+        self.fwd.append(self.s.step(dt, allow_not_converged=True)["ms"])
+
+    def step_adjoint(self, dt):
+        self.adj.append(self.s.step_adjoint(dt, allow_not_converged=True)["ms"])
+
+    def upload(self, k, a):
+        self.s.upload(k, a)
+
+    def download(self, k):
+        return self.s.download(k)
+
+
+def scene_params(fs, name, precision):
+    if name == "dam_break":
+        return fs.default_params(rho_neg=1000.0, rho_pos=1.0, mu_neg=1e-3, mu_pos=1.8e-5, gravity=(0.0, -9.8, 0.0),
+                                 precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=20000,
+                                 viscosity=1, viscosity_tolerance=1e-8, cfl=0.5, order=3, reinit_iterations=10,
+                                 reinit_scaling=5,
+                                 pressure_preconditioner=(PRECONDITIONER[PRECOND_CHOICE]
+                                                          if precision == fs.FS_PRECISION_FP32_REFINE else 0))
+    if name == "rayleigh_taylor":
+        return fs.default_params(rho_neg=850.0, rho_pos=1000.0, mu_neg=5e-2, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0),
+                                 precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=40000,
+                                 viscosity=1, viscosity_tolerance=1e-8, cfl=0.5, order=3, reinit_iterations=10,
+                                 reinit_scaling=5, pressure_preconditioner=PRECONDITIONER[PRECOND_CHOICE])
+    return params(fs, precision)
+
+
+def run_scene(fs, name, steps, lead_in, window, snapshots):
+    """The long configurations, one JSON line each (device times from the
+    library's CUDA events; volumes with the reference's smeared Heaviside):
+
+    - dam_break_128: 128^3 dam break, `steps` steps (default 200) in FP64
+      and in FP32+refine from the same state at 1e-6 relative divergence;
+      per-step time, PCG iterations, final divergence and the FP32+refine
+      pressure and level set against the FP64 run's;
+    - rising_bubble_256: `steps` steps (default 300) of the benchmark scene
+      in FP32+refine with the bubble volume drift;
+    - rayleigh_taylor_512_adjoint: 512^3 oil/water Rayleigh-Taylor with
+      semi-implicit viscosity in FP32+refine, `lead_in` forward steps
+      (default 84) then the gradient of L = ||phi(T)||^2 over the last
+      `window` steps (default 16) with binomial checkpointing (`snapshots`
+      snapshots, default 3), with the context's and the device's memory."""
+    import torch
+
+    from fluid_simulator_backup_b200 import checkpoint as ck
+    from fluid_simulator_backup_b200 import scenes as sc
+    out = {"scene": name}
+    if name == "dam_break_128":
+        n = 128
+        steps = steps or 200
+        phi0 = sc.dam_break(n)
+        v0 = sc.heaviside_volume(phi0, 1.0 / n)
+        res = {}
+        for prec, key in ((fs.FS_PRECISION_FP64, "fp64"), (fs.FS_PRECISION_FP32_REFINE, "fp32_refine")):
+            with fs.Solver(n, 1.0 / n, scene_params(fs, "dam_break", prec)) as s:
+                s.upload("phi", phi0)
+                for k, a in zip("uvw", sc.zero_faces(n)):
+                    s.upload(k, a)
+                reps = [s.step(s.cfl_dt(), allow_not_converged=True) for _ in range(steps)]
+                phi, p = s.download("phi"), s.download("pressure")
+            res[key] = (phi, p - p.mean())
+            out[key] = {"ms_per_step": float(np.mean([r["ms"] for r in reps])),
+                        "pcg_iterations_per_step": float(np.mean([r["pcg_iterations"] for r in reps])),
+                        "max_rel_residual": max(r["max_rel_residual"] for r in reps),
+                        "div_l2_final": reps[-1]["div_l2"], "div_linf_final": reps[-1]["div_linf"],
+                        "div_linf_max": max(r["div_linf"] for r in reps),
+                        "volume_drift": sc.heaviside_volume(phi, 1.0 / n) / v0 - 1}
+        (phi64, p64), (phi32, p32) = res["fp64"], res["fp32_refine"]
+        out.update(grid=[n] * 3, steps=steps, speedup_fp32_refine=out["fp64"]["ms_per_step"] /
+                   out["fp32_refine"]["ms_per_step"],
+                   pressure_rel_diff=float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64)),
+                   phi_max_diff=float(np.abs(phi32 - phi64).max()))
+    elif name == "rising_bubble_256":
+        n = 256
+        steps = steps or 300
+        phi0 = sc.rising_bubble(n)
+        v0 = sc.heaviside_volume(phi0, 1.0 / n)
+        with fs.Solver(n, 1.0 / n, params(fs, fs.FS_PRECISION_FP32_REFINE)) as s:
+            s.upload("phi", phi0)
+            for k, a in zip("uvw", sc.zero_faces(n)):
+                s.upload(k, a)
+            reps, t = [], 0.0
+            for _ in range(steps):
+                dt = s.cfl_dt()
+                reps.append(s.step(dt, allow_not_converged=True))
+                t += dt
+            phi = s.download("phi")
+        out.update(grid=[n] * 3, steps=steps, simulated_time=t,
+                   ms_per_step=float(np.mean([r["ms"] for r in reps])),
+                   pcg_iterations_per_step=float(np.mean([r["pcg_iterations"] for r in reps])),
+                   max_rel_residual=max(r["max_rel_residual"] for r in reps),
+                   div_l2_final=reps[-1]["div_l2"], div_linf_max=max(r["div_linf"] for r in reps),
+                   bubble_volume_drift=sc.heaviside_volume(phi, 1.0 / n) / v0 - 1)
+    elif name == "rayleigh_taylor_512_adjoint":
+        n = 512
+        lead_in = 84 if lead_in is None else lead_in
+        free0, total = torch.cuda.mem_get_info()
+        with fs.Solver(n, 1.0 / n, scene_params(fs, "rayleigh_taylor", fs.FS_PRECISION_FP32_REFINE)) as s:
+            s.upload("phi", sc.rayleigh_taylor(n))
+            for k, a in zip("uvw", sc.zero_faces(n)):
+                s.upload(k, a)
+            dt = s.cfl_dt()  # one dt for the whole run, so that the window is one differentiable map
+            lead = [s.step(dt, allow_not_converged=True)["ms"] for _ in range(lead_in)]
+            st0 = ck.save(s)
+            ts, sched = _TimedSolver(s), ck.Schedule()
+            t0 = time.perf_counter()
+            end = ck.advance(ts, st0, window, dt, sched)
+            t_fwd = time.perf_counter() - t0
+            s.adjoint_reset()
+            for k in ck.KEYS:
+                s.upload("adj_" + k, 2.0 * end[k] if k == "phi" else np.zeros_like(end[k]))
+            t0 = time.perf_counter()
+            ck.reverse_binomial(ts, 0, window, st0, snapshots, dt, sched)
+            t_rev = time.perf_counter() - t0
+            free1, _ = torch.cuda.mem_get_info()
+            ctx_bytes = s.memory_bytes()
+            bars = {k: s.download("adj_" + k) for k in ck.KEYS}
+            rho_bar = s.density_bars()[0]
+        fwd_ms = float(np.mean(ts.fwd))
+        adj_ms = float(np.mean(ts.adj))
+        out.update(grid=[n] * 3, dt=dt, lead_in_steps=lead_in, window_steps=window, snapshots=snapshots,
+                   lead_in_ms_per_step=float(np.mean(lead)) if lead else None,
+                   window_forward_ms_per_step=fwd_ms, adjoint_ms_per_step=adj_ms, adjoint_to_forward=adj_ms / fwd_ms,
+                   forward_steps_in_reversal=sched.forward_steps - window, adjoint_steps=sched.adjoint_steps,
+                   max_live_snapshots=sched.max_live_snapshots, window_forward_wall_s=t_fwd,
+                   reversal_wall_s=t_rev, context_gib=ctx_bytes / 2 ** 30,
+                   device_in_use_gib=(total - free1) / 2 ** 30, device_total_gib=total / 2 ** 30,
+                   device_in_use_before_gib=(total - free0) / 2 ** 30,
+                   bars_finite=bool(all(np.isfinite(b).all() for b in bars.values())),
+                   d_loss_d_rho_oil=rho_bar)
+    else:
+        raise ValueError(name)
+    return out
+
+
 def reference_tolerance(m, rel=1e-6):
     """The reference's PCG stops on an absolute test, r.z < tol^2
     (PCG_METHOD.cpp:87).  The tolerance that matches the GPU path's relative
@@ -346,6 +490,13 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--preconditioner", default="default", choices=sorted(PRECONDITIONER),
                     help="pressure preconditioner of the FP32+refine path (the FP64 comparison stays Jacobi)")
+    ap.add_argument("--scene", default=None,
+                    choices=["dam_break_128", "rising_bubble_256", "rayleigh_taylor_512_adjoint"],
+                    help="run one of the long configurations instead of the timestep benchmark (1 GPU)")
+    ap.add_argument("--scene-steps", type=int, default=None)
+    ap.add_argument("--lead-in", type=int, default=None)
+    ap.add_argument("--window", type=int, default=16)
+    ap.add_argument("--snapshots", type=int, default=3)
     args = ap.parse_args()
     global PRECOND_CHOICE
     PRECOND_CHOICE = args.preconditioner
@@ -382,6 +533,15 @@ def main():
 
     import fluid_simulator_backup_b200 as fs
     fs.lib()
+    if args.scene:
+        with ClockSampler(local) as clk:
+            out = run_scene(fs, args.scene, args.scene_steps, args.lead_in, args.window, args.snapshots)
+        out.update(preconditioner=PRECOND_CHOICE, clocks=clk.summary())
+        if rank == 0:
+            print(json.dumps(out))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     main_prec = fs.FS_PRECISION_FP32_REFINE if args.precision == "fp32_refine" else fs.FS_PRECISION_FP64
     if main_prec == fs.FS_PRECISION_FP64:
         args.no_fp64 = True
