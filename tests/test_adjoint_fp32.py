@@ -148,3 +148,35 @@ def test_differentiable_dam_break_96_32_steps():
     assert max(errs[fs.FS_PRECISION_FP32_REFINE]) < 1e-2
     assert rel(grads[fs.FS_PRECISION_FP64][1], fd_rho) < 1e-3
     assert rel(grads[fs.FS_PRECISION_FP32_REFINE][1], fd_rho) < 1e-2
+
+
+@pytest.mark.parametrize("op", ["step", "projection", "viscosity"])
+def test_fp32_adjoint_transpose(op):
+    """Dot-product test in the FP32 + FP64 refinement context: <Ybar, J dX>
+    by central differences of the context's own FP32 forward (h = 1e-3, so
+    that FP32 rounding of the outputs, about 1e-7, stays near 1e-4 of the
+    difference) against <Jt Ybar, dX> from its adjoint.  A transposition
+error shows as an O(1) mismatch; the 1e-2 bound leaves room for the
+rounding and the WENO weights' curvature at this step size."""
+    from test_adjoint import rand_like, rel, scene, transpose_check
+    from test_adjoint import zero_walls as zw
+    n = 10
+    X = zw(scene(n, 7, vel_scale=0.2))
+    rng = np.random.default_rng(40)
+    dX = zw(rand_like(X, rng, KEYS))
+    dX["phi"] = dX["phi"] * 0.01
+    Ybar = rand_like(X, rng, KEYS)
+    dt = 0.3 / n
+    rho, drho = (1.0, 1000.0), (0.2, 50.0)
+    p = dict(rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, precision=fs.FS_PRECISION_FP32_REFINE,
+             tolerance=1e-12, stop=fs.FS_STOP_RELATIVE, max_iteration=100000, viscosity=1,
+             viscosity_tolerance=1e-12, viscosity_max_iteration=100000, order=3)
+    if op == "viscosity":
+        p.update(mu_neg=2e-2, mu_pos=5e-2)  # large enough that the coefficients matter
+    fwd, adj, outs = {"step": (lambda s: s.step(dt), lambda s: s.step_adjoint(dt), KEYS),
+                      "projection": (lambda s: s.project(dt), lambda s: s.project_adjoint(dt), VEL),
+                      "viscosity": (lambda s: s.viscosity(dt), lambda s: s.viscosity_adjoint(dt), VEL)}[op]
+    with fs.Solver(n, 1.0 / n, **p) as s:
+        lhs, rhs = transpose_check(s, fwd, adj, X, dX, Ybar, outs, KEYS, 1e-3, rho, drho)
+    print(f"FP32 context, {op}: <Ybar, J dX> {lhs:.9e}, <Jt Ybar, dX> {rhs:.9e}, relative {rel(lhs, rhs):.2e}")
+    assert rel(lhs, rhs) < 1e-2, (lhs, rhs)
