@@ -53,7 +53,7 @@ def scene(n):
     return phi, u, v, w
 
 
-PRECONDITIONER = {"default": 0, "jacobi": 1, "bf16": 2, "red_black": 3}
+PRECONDITIONER = {"default": 0, "jacobi": 1, "bf16": 2, "red_black": 3, "red_black_jacobi": 4}
 PRECOND_CHOICE = "default"
 
 
@@ -161,13 +161,13 @@ def e2e_steps(fs, s, states):
     return ms, h2d, d2h
 
 
-def adjoint_steps(fs, n, warmup, steps):
-    """FP64 adjoint step (fs_step_adjoint: forward recomputed with its tape,
-    then the reverse sweep with the transposed solves) against the FP64
-    forward step from the same states, both timed by the library with CUDA
-    events.  The bars are those of L = sum(phi^2) + |u|^2 at the step's end
-    (any bar costs the same)."""
-    s = fs.Solver(n, 1.0 / n, params(fs, fs.FS_PRECISION_FP64))
+def adjoint_steps(fs, n, warmup, steps, precision):
+    """Adjoint step (fs_step_adjoint: forward recomputed with its tape, then
+    the reverse sweep with the transposed solves) against the forward step
+    from the same states in the same context, both timed by the library with
+    CUDA events.  The bars are those of L = sum(phi^2) + |u|^2 at the step's
+    end (any bar costs the same)."""
+    s = fs.Solver(n, 1.0 / n, params(fs, precision))
     phi, u, v, w = scene(n)
     for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
         s.upload(k, a)
@@ -185,10 +185,11 @@ def adjoint_steps(fs, n, warmup, steps):
         for k, a in bars.items():
             s.upload("adj_" + k, a)
         adj.append(s.step_adjoint(dt, allow_not_converged=True)["ms"])
+    mem = s.memory_bytes()
     s.close()
     f, a = float(np.mean(fwd)), float(np.mean(adj))
-    return {"ms_per_step": a, "forward_fp64_ms_per_step": f, "ratio_to_forward": a / f, "precision": "fp64",
-            "steps": steps}
+    return {"ms_per_step": a, "forward_ms_per_step": f, "ratio_to_forward": a / f, "steps": steps,
+            "context_gib": mem / 2 ** 30}
 
 
 class _TimedSolver:
@@ -585,8 +586,11 @@ def main():
 
     adjoint = None
     if not args.no_adjoint:
-        adjoint = adjoint_steps(fs, n, min(args.warmup, 1), min(args.steps, 2))
-        adjoint["ms_per_step"] = max_over_ranks(adjoint["ms_per_step"])
+        adjoint = {}
+        for prec, key in ((fs.FS_PRECISION_FP64, "fp64"), (fs.FS_PRECISION_FP32_REFINE, "fp32_refine")):
+            a = adjoint_steps(fs, n, min(args.warmup, 1), min(args.steps, 2), prec)
+            a["ms_per_step"] = max_over_ranks(a["ms_per_step"])
+            adjoint[key] = a
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

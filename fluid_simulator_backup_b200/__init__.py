@@ -34,6 +34,7 @@ FS_FLAG_SORT_TYPO, FS_FLAG_VISCOSITY_IN_PLACE = 16, 32
 FS_VISCOSITY_OFF, FS_VISCOSITY_SEMI_IMPLICIT, FS_VISCOSITY_EXPLICIT = 0, 1, 2
 FS_VELOCITY_WENO5, FS_VELOCITY_ENO3 = 0, 1
 FS_PRECOND_DEFAULT, FS_PRECOND_JACOBI, FS_PRECOND_JACOBI_BF16, FS_PRECOND_RED_BLACK = 0, 1, 2, 3
+FS_PRECOND_RED_BLACK_JACOBI = 4
 
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
             "fs_memory_bytes", "fs_upload", "fs_download", "fs_upload_device", "fs_download_device", "fs_step",

@@ -90,7 +90,7 @@ struct fs_ctx {
   // red-black reduced FP32 pressure solve (packed half layout Lh, fs_redblack.cu)
   Lay Lh{};
   double* rb_x = nullptr;          // black FP64 iterate
-  float *rb_r = nullptr, *rb_p = nullptr, *rb_q = nullptr, *rb_tau = nullptr;
+  float *rb_r = nullptr, *rb_p = nullptr, *rb_q = nullptr;
   unsigned short* rb_dinv = nullptr;  // black bf16 1/diag
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
   // viscosity systems, one per component (storage type S)
@@ -134,6 +134,7 @@ struct fs_ctx {
   int flux32 = 2;               // params.flux_arithmetic (Op7::flux32)
   int lean = 1;                 // FP32 pressure solve preconditioned by the bf16 inverse diagonal (Op7::dinv16)
   bool red_black = false;       // FP32 pressure solve on the red-black Schur complement
+  bool rb_ic0 = true;           // its preconditioner: 1/diag(S) (IC(0) in red-black order), else the black 1/diag
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -227,7 +228,7 @@ fs_status check_params(const fs_params* p) {
     set_error("bad solver or reinitialisation settings");
     return FS_INVALID_ARG;
   }
-  if (p->pressure_preconditioner < FS_PRECOND_DEFAULT || p->pressure_preconditioner > FS_PRECOND_RED_BLACK ||
+  if (p->pressure_preconditioner < FS_PRECOND_DEFAULT || p->pressure_preconditioner > FS_PRECOND_RED_BLACK_JACOBI ||
       (p->pressure_preconditioner >= FS_PRECOND_JACOBI_BF16 && p->precision != FS_PRECISION_FP32_REFINE)) {
     set_error("unknown pressure preconditioner %d for this precision", p->pressure_preconditioner);
     return FS_INVALID_ARG;
@@ -254,7 +255,9 @@ void apply_params(fs_ctx* c) {
   c->reliable_delta = p.reliable_delta > 0.0 ? p.reliable_delta : 0.1;
   c->flux32 = p.flux_arithmetic;
   c->lean = p.pressure_preconditioner != FS_PRECOND_JACOBI;
-  c->red_black = c->fp32 && p.pressure_preconditioner == FS_PRECOND_RED_BLACK;
+  c->red_black = c->fp32 && (p.pressure_preconditioner == FS_PRECOND_RED_BLACK ||
+                              p.pressure_preconditioner == FS_PRECOND_RED_BLACK_JACOBI);
+  c->rb_ic0 = p.pressure_preconditioner == FS_PRECOND_RED_BLACK;
 }
 
 // ---------------------------------------------------------------------------
@@ -581,12 +584,16 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
   A.flux32 = c->flux32;
   if (c->lean) A.dinv16 = c->pdinv;
   // red-black: the black Schur complement on the packed half layout, its
-  // Jacobi preconditioner the black cells' bf16 1/diag
+  // Jacobi preconditioner bf16 1/diag(S) (IC(0) in red-black order) or the
+  // black cells' own bf16 1/diag
   RbOp R{(float*)c->pax, (float*)c->pay, (float*)c->paz, c->Lc, c->Lh, c->scalars + 12};
   Op7<float> Ah{nullptr, nullptr, nullptr, nullptr, c->Lh};
   Ah.dinv16 = c->rb_dinv;
   if (rb) {
-    rb_gather<unsigned short, unsigned short>(c->pdinv, c->rb_dinv, c->Lc, c->Lh, s);
+    if (c->rb_ic0)
+      rb_schur_dinv(R, c->rb_dinv, s);
+    else
+      rb_gather<unsigned short, unsigned short>(c->pdinv, c->rb_dinv, c->Lc, c->Lh, s);
     rb_gather<double, double>(x, c->rb_x, c->Lc, c->Lh, s);  // the initial guess's black cells
     c->launches += 2;
   }
@@ -635,7 +642,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
     // search direction p and q = A p are FP32 (the flux-form operator in
     // FP32 arithmetic, Op7::flux32, or the red-black Schur complement in
     // its offset form) and the Jacobi preconditioner is 1/diag in bf16: 64
-    // bytes per unknown and iteration (red-black: 56 at half the
+    // bytes per unknown and iteration (red-black: 38 per cell at half the
     // iterations) against 120 for the FP64 solve.  Every time the recursive
     // residual drops by reliable_delta the true FP64 residual of p64
     // replaces it (reliable update), keeping the search direction; the
@@ -663,7 +670,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
       if (rb) {
         CKS(drive_pcg(c, std::make_pair(4, (const void*)nullptr),
                       [&] {
-                        rb_iteration(R, Ah, c->rb_x, c->rb_r, c->rb_p, c->rb_q, c->rb_tau, c->st, c->partials, s);
+                        rb_iteration(R, Ah, c->rb_x, c->rb_r, c->rb_p, c->rb_q, c->st, c->partials, s);
                       },
                       P.max_iteration, true, 4));
       } else {
@@ -1391,7 +1398,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
     c->Lh = make_half_lay(c->Lc);
     const size_t hb = c->Lh.total;
     if ((s = dalloc(c, (void**)&c->rb_x, hb * sizeof(double))) != FS_OK) return fail(s);
-    float** hv[] = {&c->rb_r, &c->rb_p, &c->rb_q, &c->rb_tau};
+    float** hv[] = {&c->rb_r, &c->rb_p, &c->rb_q};
     for (float** p : hv) if ((s = dalloc(c, (void**)p, hb * sizeof(float))) != FS_OK) return fail(s);
     if ((s = dalloc(c, (void**)&c->rb_dinv, hb * sizeof(unsigned short))) != FS_OK) return fail(s);
   }

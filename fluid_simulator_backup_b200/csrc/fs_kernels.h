@@ -139,13 +139,16 @@ int rb_blocks(const Lay& Lh);
 // One CG iteration on the black Schur complement: red stage (tau), black
 // stage (q = S p, p.q, alpha), then cg_vector_updates on the packed black
 // vectors with Ah (layout Lh, dinv16 the packed black bf16 1/diag).
-void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
-                  PcgState* st, double* partials, cudaStream_t s);
+void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, PcgState* st,
+                  double* partials, cudaStream_t s);
 // p64 <- black cells from the packed iterate xh, red cells eliminated in FP64
 // from phi and b (the red rows of b - A p64 vanish)
 template <class T>
 void rb_commit(const T* phi, const double* xh, const double* b, double* p64, const Lay& L, const Lay& Lh, double dx,
                double rho_neg, double rho_pos, cudaStream_t s);
+// bf16 1/diag(S) of the black Schur complement per packed black slot: the
+// black pivots of IC(0) in red-black order
+void rb_schur_dinv(const RbOp& A, unsigned short* dinv, cudaStream_t s);
 // packed black slots <- black cells of a cell-layout field
 template <class S, class D> void rb_gather(const S* full, D* half, const Lay& L, const Lay& Lh, cudaStream_t s);
 

@@ -36,13 +36,16 @@
 // (eps32 of the fluxes, not of |p|).  b0(r) is r's x-1 neighbour, or its
 // x+1 neighbour for r at i = 0.
 //
-// Kernels of one iteration (each array element once per kernel):
-//   k_rb_red    tau_r for every red cell          reads ax, ay, az, p     writes tau
-//   k_rb_black  q = S p, p.q and alpha            reads ax, ay, az, p, tau writes q
+// Kernels of one iteration:
+//   k_rb_spmv     q = S p, p.q and alpha: tau of the red cells computed into
+//                 a shared-memory ring of planes and used there (couplings
+//                 12 B, black p 2 B, black q 2 B per cell)
 //   k_cg_update / k_cg_pupdate (fs_krylov.cu) on the packed black vectors
-// = 16 + 18 + 7 + 15 = 56 bytes per cell and iteration (FP32 couplings and
-// vectors, FP64 black iterate, bf16 black 1/diag), at half the iterations of
-// the full Jacobi-PCG's 64.
+//                 (7 + 15 B per cell: FP32 r, p, q, FP64 iterate, bf16 1/diag)
+// = 38 bytes per cell and iteration, at half the iterations of the full
+// Jacobi-PCG's 64.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 
 #include "fs_kernels.h"
@@ -52,103 +55,6 @@ namespace fsb {
 Lay make_half_lay(const Lay& L) { return make_lay((L.nx + 1) / 2, L.ny, L.nz); }
 
 namespace {
-
-// red stage: tau of the red cell in slot (h, j, k)
-__global__ void __launch_bounds__(256) k_rb_red(RbOp A, const float* __restrict__ p, float* __restrict__ tau) {
-  const int h = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
-  const Lay& L = A.L;
-  const Lay& H = A.Lh;
-  if (h >= H.nx || j >= H.ny || k >= H.nz) return;
-  const int pr = (j + k) & 1;
-  const int i = 2 * h + pr;
-  const int64_t s = H.at(h, j, k);
-  float t = 0.0f;
-  if (i < L.nx) {
-    const int64_t c = L.at(i, j, k);
-    // the six black neighbours (packed) and the couplings of the six faces
-    const float pxm = p[s + pr - 1], pxp = p[s + pr];
-    const float pym = p[s - H.px], pyp = p[s + H.px];
-    const float pzm = p[s - H.slab], pzp = p[s + H.slab];
-    const float axm = A.ax[c], axp = A.ax[c + 1];
-    const float aym = A.ay[c], ayp = A.ay[c + L.px];
-    const float azm = A.az[c], azp = A.az[c + L.slab];
-    const float b0 = i > 0 ? pxm : pxp;
-    float num = axm * (pxm - b0) + axp * (pxp - b0);
-    num += aym * (pym - b0) + ayp * (pyp - b0);
-    num += azm * (pzm - b0) + azp * (pzp - b0);
-    float d = ((axm + axp) + (aym + ayp)) + (azm + azp);
-    if (i == 0 && j == 0 && k == 0) {
-      const float e0 = (float)(*A.extra0);
-      num -= e0 * b0;
-      d += e0;
-    }
-    t = d > 0.0f ? num / d : 0.0f;
-  }
-  tau[s] = t;
-}
-
-// black stage: q = S p on the black cells, p.q, alpha.  Grid-stride over the
-// slots on the resident blocks only, so that the p.q reduction has a few
-// hundred partial sums (one atomic ticket per block) rather than one per
-// 256 slots.
-__global__ void __launch_bounds__(kRedThreads) k_rb_black(RbOp A, const float* __restrict__ p,
-                                                          const float* __restrict__ tau, float* __restrict__ q,
-                                                          PcgState* st, double* partials) {
-  if (((volatile PcgState*)st)->done) return;
-  const Lay& L = A.L;
-  const Lay& H = A.Lh;
-  double pq = 0.0;
-  Cursor cur;
-  for (cur.init(H); cur.valid(H); cur.next(H)) {
-    const int h = cur.i, j = cur.j, k = cur.k;
-    const int pb = (j + k + 1) & 1;
-    const int i = 2 * h + pb;
-    const int64_t s = H.at(h, j, k);
-    float qv = 0.0f;
-    if (i < L.nx) {
-      const int64_t c = L.at(i, j, k);
-      const float pc = p[s];
-      const float axm = A.ax[c], axp = A.ax[c + 1];
-      const float aym = A.ay[c], ayp = A.ay[c + L.px];
-      const float azm = A.az[c], azp = A.az[c + L.slab];
-      // tau of the six red neighbours
-      const float txm = tau[s + pb - 1], txp = tau[s + pb];
-      const float tym = tau[s - H.px], typ = tau[s + H.px];
-      const float tzm = tau[s - H.slab], tzp = tau[s + H.slab];
-      // b0 of each red neighbour: its x-1 black neighbour (x+1 at i = 0).
-      // x-1 neighbour (at i-1): b0 is the black cell at i-2, or c itself when
-      // i-1 = 0; x+1 neighbour: b0 is c.  y/z neighbours (at i): b0 is the
-      // black cell at i-1 of their row (slot h + pb - 1), or at i+1 = 1
-      // (slot 0) when i = 0.
-      const int o = i > 0 ? pb - 1 : 0;
-      const float dxm = i > 1 ? pc - p[s - 1] : 0.0f;
-      const float dym = pc - p[s - H.px + o], dyp = pc - p[s + H.px + o];
-      const float dzm = pc - p[s - H.slab + o], dzp = pc - p[s + H.slab + o];
-      float acc = axm * (dxm - txm) + axp * (0.0f - txp);
-      acc += aym * (dym - tym) + ayp * (dyp - typ);
-      acc += azm * (dzm - tzm) + azp * (dzp - tzp);
-      qv = acc;
-      pq += (double)pc * (double)qv;
-    }
-    q[s] = qv;
-  }
-  pq = block_sum(pq);
-  double tot;
-  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) {
-    st->pq = tot;
-    const double alpha = st->rz / tot;
-    if (!(tot > 0.0) || !isfinite(alpha)) {
-      st->status = PCG_STAGNATED;
-      st->done = 1;
-      st->x_pending = 0;
-    } else {
-      st->alpha = alpha;
-      st->x_pending = 1;
-    }
-  }
-}
 
 // q = S p in one pass: both stages fused, z-marching.  A block owns a tile of
 // 32 x 8 packed slots (64 x 8 cells) and walks a chunk of z planes.  At
@@ -318,6 +224,50 @@ __global__ void k_rb_gather(const S* __restrict__ full, D* __restrict__ half, La
   half[H.at(h, j, k)] = ib < L.nx ? (D)full[L.at(ib, j, k)] : D(0);
 }
 
+// The black pivots of IC(0) in red-black order.  Ordered red first, the
+// incomplete Cholesky factor of A keeps the red block's diagonal (no fill
+// there) and drops only the fill inside the black block, so its black
+// pivots are diag(S) = d_c - sum_r a_cr^2 / d_r and PCG on A with that
+// factor is PCG on the Schur complement S with the Jacobi preconditioner
+// 1/diag(S).  Each term a_cr^2 / d_r is subtracted as a_cr (d_r - a_cr)/d_r,
+// with d_r - a_cr the sum of r's other couplings, so nothing cancels.
+// Written as bf16 1/diag(S) per packed black slot (0 for slots without a
+// cell).
+__global__ void k_rb_schur_dinv(RbOp A, unsigned short* __restrict__ dinv) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const Lay& L = A.L;
+  const Lay& H = A.Lh;
+  if (h >= H.nx || j >= H.ny || k >= H.nz) return;
+  const int i = 2 * h + ((j + k + 1) & 1);
+  const int64_t s = H.at(h, j, k);
+  if (i >= L.nx) {
+    dinv[s] = 0;
+    return;
+  }
+  const int64_t c = L.at(i, j, k);
+  const int64_t nb[6] = {c - 1, c + 1, c - L.px, c + L.px, c - L.slab, c + L.slab};
+  const double a[6] = {A.ax[c], A.ax[c + 1], A.ay[c], A.ay[c + L.px], A.az[c], A.az[c + L.slab]};
+  const int64_t c0 = L.at(0, 0, 0);
+  double piv = 0.0;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    if (!(a[q] > 0.0)) continue;  // wall faces carry no coupling
+    const int64_t r = nb[q];
+    const double ar[6] = {A.ax[r], A.ax[r + 1], A.ay[r], A.ay[r + L.px], A.az[r], A.az[r + L.slab]};
+    double other = r == c0 ? (double)*A.extra0 : 0.0;  // the deflation term of the first cell
+    double dr = other;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      dr += ar[m];
+      if (m != (q ^ 1)) other += ar[m];  // r's face toward c is the opposite side of c's face q
+    }
+    piv += a[q] * (other / dr);
+  }
+  dinv[s] = __bfloat16_as_ushort(__float2bfloat16_rn(piv > 0.0 ? (float)(1.0 / piv) : 1.0f));
+}
+
 dim3 rb_grid(const Lay& H) { return dim3((H.nx + 31) / 32, (H.ny + 3) / 4, (H.nz + 1) / 2); }
 const dim3 kRbBlock(32, 4, 2);
 
@@ -343,9 +293,8 @@ int rb_blocks(const Lay& H) {
   return std::max((int)(g.grid.x * g.grid.y * g.grid.z), reduction_blocks((int64_t)H.nx * H.ny * H.nz));
 }
 
-void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
-                  PcgState* st, double* partials, cudaStream_t s) {
-  (void)tau;  // the fused SpMV keeps tau in shared memory
+void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, PcgState* st,
+                  double* partials, cudaStream_t s) {
   const FusedGrid g = fused_grid(A.Lh);
   k_rb_spmv<<<g.grid, dim3(kFX, kFY, 1), 0, s>>>(A, ph, qh, st, partials, g.kchunk);
   cg_vector_updates<float, double>(Ah, xh, rh, ph, qh, st, partials, s);
@@ -355,6 +304,10 @@ template <class T>
 void rb_commit(const T* phi, const double* xh, const double* b, double* p64, const Lay& L, const Lay& H, double dx,
                double rho_neg, double rho_pos, cudaStream_t s) {
   k_rb_commit<T><<<rb_grid(H), kRbBlock, 0, s>>>(phi, xh, b, p64, L, H, rho_neg, rho_pos, dx * dx);
+}
+
+void rb_schur_dinv(const RbOp& A, unsigned short* dinv, cudaStream_t s) {
+  k_rb_schur_dinv<<<rb_grid(A.Lh), kRbBlock, 0, s>>>(A, dinv);
 }
 
 template <class S, class D>

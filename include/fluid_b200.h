@@ -68,8 +68,11 @@ typedef enum {
   FS_PRECOND_DEFAULT = 0,     /* FP64: Jacobi (the reference's, PCG_METHOD.cpp:128-160); FP32_REFINE: bf16 Jacobi */
   FS_PRECOND_JACOBI = 1,      /* z = r / diag in the solve precision */
   FS_PRECOND_JACOBI_BF16 = 2, /* FP32_REFINE: z = r * (1/diag rounded to bf16), 2 bytes per unknown */
-  FS_PRECOND_RED_BLACK = 3    /* FP32_REFINE: the same PCG in red-black order; the red cells are eliminated
-                                 exactly and bf16 Jacobi-PCG runs on the black Schur complement */
+  FS_PRECOND_RED_BLACK = 3,   /* FP32_REFINE: IC(0) in red-black order, i.e. the reference's commented-out
+                                 incomplete Cholesky (PCG_METHOD.cpp:52-54, CSR_MATRIX.h:376) in multicolour
+                                 ordering: the red cells are eliminated exactly and PCG runs on the black Schur
+                                 complement S with the bf16 inverse of diag(S), the factor's black pivots */
+  FS_PRECOND_RED_BLACK_JACOBI = 4 /* FP32_REFINE: the same reduced solve with the black cells' own bf16 1/diag */
 } fs_preconditioner;
 
 typedef enum {

@@ -39,8 +39,9 @@ def solver(n, precond, precision=fs.FS_PRECISION_FP32_REFINE, **kw):
                      pressure_preconditioner=precond, **kw)
 
 
+@pytest.mark.parametrize("precond", ["ic0", "jacobi"])
 @pytest.mark.parametrize("n", [(24, 24, 24), (17, 14, 15), (32, 20, 9)])
-def test_red_black_projection_matches_oracle(n):
+def test_red_black_projection_matches_oracle(n, precond):
     """Even and odd extents (odd nx leaves slots of the packed half layout
     without a cell): pressure and corrected velocities equal the oracle's
     FP64 projection to the tolerance, and the corrected velocity is divergence
@@ -49,7 +50,8 @@ def test_red_black_projection_matches_oracle(n):
     dx, dt = 1.0 / nx, 1e-3
     phi = sphere(n, (0.5, 0.3, 0.25), 0.17)
     u, v, w = velocities(n, 3)
-    with solver(n, fs.FS_PRECOND_RED_BLACK, tolerance=1e-10) as s:
+    pc = fs.FS_PRECOND_RED_BLACK if precond == "ic0" else fs.FS_PRECOND_RED_BLACK_JACOBI
+    with solver(n, pc, tolerance=1e-10) as s:
         for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
             s.upload(k, a)
         rep = s.project(dt)
@@ -72,22 +74,30 @@ def test_red_black_projection_matches_oracle(n):
 def test_red_black_needs_about_half_the_jacobi_iterations():
     """For a two-coloured operator the Schur complement's Jacobi spectrum is
     {1 - l^2} against {1 +- l}: CG needs about half the iterations of the
-    full Jacobi-PCG at the same tolerance, and both reach the same pressure."""
+    full Jacobi-PCG at the same tolerance, and both reach the same pressure.
+    The IC(0) pivots diag(S) are at least as good a scaling of S as the
+    black cells' own diagonal."""
     n = (48, 48, 48)
     phi = sphere(n, (0.5, 0.25, 0.5), 0.15)
     u, v, w = velocities(n, 4, 0.1)
     out = {}
-    for precond in (fs.FS_PRECOND_JACOBI_BF16, fs.FS_PRECOND_RED_BLACK):
+    for precond in (fs.FS_PRECOND_JACOBI_BF16, fs.FS_PRECOND_RED_BLACK, fs.FS_PRECOND_RED_BLACK_JACOBI):
         with solver(n, precond, tolerance=1e-8) as s:
             for k, a in zip(("phi", "u", "v", "w"), (phi, u, v, w)):
                 s.upload(k, a)
             rep = s.project(2e-3)
             out[precond] = (rep, s.download("pressure"))
-    (rj, pj), (rr, pr) = out[fs.FS_PRECOND_JACOBI_BF16], out[fs.FS_PRECOND_RED_BLACK]
-    print(f"48^3 projection to 1e-8: Jacobi {rj['iterations']} iterations, red-black {rr['iterations']}")
-    assert rj["rel_residual"] <= 1e-8 and rr["rel_residual"] <= 1e-8
+    (rj, pj), (rr, pr), (rb, pb) = (out[fs.FS_PRECOND_JACOBI_BF16], out[fs.FS_PRECOND_RED_BLACK],
+                                    out[fs.FS_PRECOND_RED_BLACK_JACOBI])
+    print(f"48^3 projection to 1e-8: Jacobi {rj['iterations']} iterations, red-black IC(0) {rr['iterations']}, "
+          f"red-black with the black diagonal {rb['iterations']}")
+    for r in (rj, rr, rb):
+        assert r["rel_residual"] <= 1e-8
     assert rr["iterations"] < 0.65 * rj["iterations"], (rr["iterations"], rj["iterations"])
+    assert rb["iterations"] < 0.65 * rj["iterations"], (rb["iterations"], rj["iterations"])
+    assert rr["iterations"] <= 1.05 * rb["iterations"], (rr["iterations"], rb["iterations"])
     assert rel_err(pr - pr.mean(), pj - pj.mean()) < 1e-6
+    assert rel_err(pb - pb.mean(), pj - pj.mean()) < 1e-6
 
 
 @pytest.mark.parametrize("order", [1, 3])
