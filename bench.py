@@ -55,11 +55,12 @@ def scene(n):
 
 PRECONDITIONER = {"default": 0, "jacobi": 1, "bf16": 2, "red_black": 3, "red_black_jacobi": 4}
 PRECOND_CHOICE = "default"
+HOST_LOOP = 0  # 1: Krylov batches launched from the host (for profilers), not as one graph per solve
 
 
 def params(fs, precision):
     pc = PRECONDITIONER[PRECOND_CHOICE] if precision == fs.FS_PRECISION_FP32_REFINE else 0
-    return fs.default_params(pressure_preconditioner=pc,
+    return fs.default_params(pressure_preconditioner=pc, host_loop=HOST_LOOP,
                              rho_neg=1.0, rho_pos=1000.0, mu_neg=1.8e-5, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0),
                              precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=20000,
                              inner_tolerance=1e-3, max_outer=30, viscosity=1, viscosity_tolerance=1e-8, cfl=0.5,
@@ -217,14 +218,15 @@ def scene_params(fs, name, precision):
         return fs.default_params(rho_neg=1000.0, rho_pos=1.0, mu_neg=1e-3, mu_pos=1.8e-5, gravity=(0.0, -9.8, 0.0),
                                  precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=20000,
                                  viscosity=1, viscosity_tolerance=1e-8, cfl=0.5, order=3, reinit_iterations=10,
-                                 reinit_scaling=5,
+                                 reinit_scaling=5, host_loop=HOST_LOOP,
                                  pressure_preconditioner=(PRECONDITIONER[PRECOND_CHOICE]
                                                           if precision == fs.FS_PRECISION_FP32_REFINE else 0))
     if name == "rayleigh_taylor":
         return fs.default_params(rho_neg=850.0, rho_pos=1000.0, mu_neg=5e-2, mu_pos=1e-3, gravity=(0.0, -9.8, 0.0),
                                  precision=precision, stop=fs.FS_STOP_RELATIVE, tolerance=1e-6, max_iteration=40000,
                                  viscosity=1, viscosity_tolerance=1e-8, cfl=0.5, order=3, reinit_iterations=10,
-                                 reinit_scaling=5, pressure_preconditioner=PRECONDITIONER[PRECOND_CHOICE])
+                                 reinit_scaling=5, pressure_preconditioner=PRECONDITIONER[PRECOND_CHOICE],
+                                 host_loop=HOST_LOOP)
     return params(fs, precision)
 
 
@@ -491,6 +493,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--preconditioner", default="default", choices=sorted(PRECONDITIONER),
                     help="pressure preconditioner of the FP32+refine path (the FP64 comparison stays Jacobi)")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="launch the Krylov batches from the host instead of one graph per solve (for ncu)")
     ap.add_argument("--scene", default=None,
                     choices=["dam_break_128", "rising_bubble_256", "rayleigh_taylor_512_adjoint"],
                     help="run one of the long configurations instead of the timestep benchmark (1 GPU)")
@@ -499,8 +503,9 @@ def main():
     ap.add_argument("--window", type=int, default=16)
     ap.add_argument("--snapshots", type=int, default=3)
     args = ap.parse_args()
-    global PRECOND_CHOICE
+    global PRECOND_CHOICE, HOST_LOOP
     PRECOND_CHOICE = args.preconditioner
+    HOST_LOOP = 1 if args.host_loop else 0
 
     # the reference arm is host work: its ranks meet over gloo and touch no GPU
     world, rank, local, dist, barrier, max_over_ranks = init_replicas("gloo" if args.impl == "reference" else "nccl")

@@ -67,7 +67,8 @@ class Params(ctypes.Structure):
                 ("surface_tension", ctypes.c_double), ("velocity_scheme", ctypes.c_int),
                 ("velocity_epsilon", ctypes.c_double), ("fast_sweeping", ctypes.c_int),
                 ("pressure_preconditioner", ctypes.c_int), ("reliable_delta", ctypes.c_double),
-                ("flux_arithmetic", ctypes.c_int), ("verbose", ctypes.c_int)]
+                ("flux_arithmetic", ctypes.c_int), ("verbose", ctypes.c_int),
+                ("host_loop", ctypes.c_int)]
 
     def as_dict(self):
         d = {}

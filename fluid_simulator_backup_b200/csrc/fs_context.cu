@@ -134,7 +134,9 @@ struct fs_ctx {
   int flux32 = 2;               // params.flux_arithmetic (Op7::flux32)
   int lean = 1;                 // FP32 pressure solve preconditioned by the bf16 inverse diagonal (Op7::dinv16)
   bool red_black = false;       // FP32 pressure solve on the red-black Schur complement
-  bool rb_ic0 = true;           // its preconditioner: 1/diag(S) (IC(0) in red-black order), else the black 1/diag
+  bool rb_ic0 = true;
+  int adj_unconverged = 0;      // adjoint solves of the current call that stopped before their tolerance
+  double adj_worst_rel = 0.0;   // and the worst relative residual they reached           // its preconditioner: 1/diag(S) (IC(0) in red-black order), else the black 1/diag
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -237,6 +239,10 @@ fs_status check_params(const fs_params* p) {
     set_error("reliable_delta must be in [0, 1)");
     return FS_INVALID_ARG;
   }
+  if (p->host_loop != 0 && p->host_loop != 1) {
+    set_error("host_loop must be 0 or 1");
+    return FS_INVALID_ARG;
+  }
   if (p->flux_arithmetic < 0 || p->flux_arithmetic > 2) {
     set_error("flux_arithmetic must be 0, 1 or 2");
     return FS_INVALID_ARG;
@@ -290,7 +296,24 @@ __global__ void k_loop_next(cudaGraphConditionalHandle h, const PcgState* st, un
 template <class F>
 fs_status drive_pcg(fs_ctx* c, std::pair<int, const void*> key, F&& enqueue_iteration, int max_iter, bool timed,
                     int kernels_per_iteration = 3) {
-  (void)max_iter;  // the device-side bound reads max_iter from the solver state
+  if (c->prm.host_loop) {
+    // the same batches launched from the host, the state polled after each;
+    // bounded like the graph's loop
+    const int cap = max_iter / kGraphIters + 2;
+    int nb = 0;
+    CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    while (!c->st_host->done && nb < cap) {
+      for (int n = 0; n < kGraphIters; ++n) enqueue_iteration();
+      CK(cudaGetLastError());
+      ++nb;
+      CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+    c->launches += (int64_t)nb * kernels_per_iteration * kGraphIters;
+    if (timed) c->pcg_launched_iterations += nb * kGraphIters;
+    return FS_OK;
+  }
   unsigned int* batches = c->tickets + 6;
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
@@ -1111,6 +1134,10 @@ fs_status adj_projection(fs_ctx* c, void* phi, void* const ustar[3], const doubl
     CKS(run_pcg<double>(c, 3, A, pbar, lam, c->a_r, c->a_p, c->a_q, P.tolerance, std::max(P.max_iteration, 1),
                         FS_STOP_RELATIVE, &it, &rel, &st));
   }
+  if (st != PCG_CONVERGED) {
+    c->adj_unconverged += 1;
+    c->adj_worst_rel = std::max(c->adj_worst_rel, rel);
+  }
   adj_sum(lam, c->Lc, c->partials, c->tickets + 4, c->scalars + 14, s);
   for (int a = 0; a < 3; ++a) adj_divergence(lam, c->scalars + 14, in_bar[a], *lays[a], c->Lc, a, dx, dt, s);
   adj_pressure_operator<S>(F<S>(phi), lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, s);
@@ -1142,6 +1169,7 @@ fs_status adj_viscosity(fs_ctx* c, void* phi, void* const ug[3], void* const x[3
     CKS(run_pcg<double>(c, 120 + a, A, c->a_vxb[a], c->a_vlam[a], c->a_vs[a][6], c->a_vs[a][7], c->a_vs[a][8],
                         P.viscosity_tolerance, std::max(P.viscosity_max_iteration, 1), FS_STOP_RELATIVE, &it, nullptr,
                         &st));
+    if (st != PCG_CONVERGED) c->adj_unconverged += 1;
     adj_visc<S>(F<S>(phi), F<S>(ug[0]), F<S>(ug[1]), F<S>(ug[2]), F<S>(x[a]), c->a_vlam[a], in_bar[0], in_bar[1],
                 in_bar[2], phi_bar, c->a_rho, c->Lc, c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos, P.mu_neg,
                 P.mu_pos, s);
@@ -1320,6 +1348,7 @@ void fs_params_default(fs_params* p) {
   p->reliable_delta = 0.1;
   p->flux_arithmetic = 2;
   p->verbose = 0;
+  p->host_loop = 0;
 }
 
 const char* fs_status_str(fs_status s) {
@@ -1894,6 +1923,25 @@ fs_status fs_adjoint_density_bars(fs_ctx* c, double* rho_neg_bar, double* rho_po
   return FS_OK;
 }
 
+// The status of an adjoint entry point: a transposed solve that stopped
+// before its tolerance (iteration cap, stagnation) makes the bars inexact;
+// the call completes and reports FS_NOT_CONVERGED.
+static fs_status adj_finish(fs_ctx* c, fs_status s) {
+  if (s == FS_OK && c->adj_unconverged > 0) {
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "%d adjoint solve(s) stopped before their tolerance (worst pressure residual %.3e)",
+                  c->adj_unconverged, c->adj_worst_rel);
+    set_error(msg);
+    return FS_NOT_CONVERGED;
+  }
+  return s;
+}
+
+static void adj_begin(fs_ctx* c) {
+  c->adj_unconverged = 0;
+  c->adj_worst_rel = 0.0;
+}
+
 fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
   if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
@@ -1905,13 +1953,14 @@ fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {
   c->pcg_ms = 0.0f;
   c->pcg_launched_iterations = 0;
   CKS(timed_begin(c));
+  adj_begin(c);
   fs_status s = c->fp32 ? step_adjoint_t<float>(c, dt, r) : step_adjoint_t<double>(c, dt, r);
   if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
   CKS(timed_end(c, &r->ms));
   r->pcg_ms = c->pcg_ms;
   r->pcg_launched_iterations = c->pcg_launched_iterations;
   r->kernel_launches = c->launches;
-  return s;
+  return adj_finish(c, s);
 }
 
 fs_status fs_advect_levelset_adjoint(fs_ctx* c, double dt) {
@@ -1960,6 +2009,7 @@ fs_status fs_viscosity_adjoint(fs_ctx* c, double dt) {
   if (c->prm.viscosity != 1) { set_error("the semi-implicit viscosity is off"); return FS_INVALID_ARG; }
   Tape tp;
   CKS(tape_bind(c, &tp));
+  adj_begin(c);
   CKS(tape_velocity(c, tp.vel[0][1]));
   CKS(c->fp32 ? viscosity_t<float>(c, dt, nullptr) : viscosity_t<double>(c, dt, nullptr));
   CKS(tape_velocity(c, tp.vel[0][2]));
@@ -1970,7 +2020,7 @@ fs_status fs_viscosity_adjoint(fs_ctx* c, double dt) {
                                       dt));
   CKS(copy_faces(c, &c->abar[1], c->awork_f[1]));
   CK(cudaStreamSynchronize(c->stream));
-  return FS_OK;
+  return adj_finish(c, FS_OK);
 }
 
 fs_status fs_project_adjoint(fs_ctx* c, double dt) {
@@ -1979,6 +2029,7 @@ fs_status fs_project_adjoint(fs_ctx* c, double dt) {
   CKS(adj_check(c));
   Tape tp;
   CKS(tape_bind(c, &tp));
+  adj_begin(c);
   CKS(tape_velocity(c, tp.vel[0][2]));
   fs_status s = c->fp32 ? project_t<float>(c, dt, 0.0, 1.0, nullptr) : project_t<double>(c, dt, 0.0, 1.0, nullptr);
   if (s != FS_OK && s != FS_NOT_CONVERGED) return s;
@@ -1990,7 +2041,7 @@ fs_status fs_project_adjoint(fs_ctx* c, double dt) {
                                        dt));
   CKS(copy_faces(c, &c->abar[1], c->awork_f[1]));
   CK(cudaStreamSynchronize(c->stream));
-  return s;
+  return adj_finish(c, s);
 }
 
 fs_status fs_pcg_csr(fs_ctx* c, int n, int nnz, const double* values, const int* column_index, const int* row_ptr,

@@ -131,6 +131,10 @@ typedef struct {
   int flux_arithmetic;              /* FP32_REFINE pressure SpMV: each face flux a (x_c - x_n) formed in 0: FP64,
                                        1: FP32 and summed in FP64, 2: FP32 throughout (default) */
   int verbose;                      /* 1: solver progress on stderr */
+  int host_loop;                    /* 0 (default): each Krylov solve is one CUDA graph launch (a conditional while
+                                       node repeating 16-iteration batches); 1: the same kernels launched from the
+                                       host, 16 iterations between polls of the solver state (for profilers that do
+                                       not descend into conditional graph nodes) */
 } fs_params;
 
 typedef struct {
