@@ -54,9 +54,11 @@ struct PhiX {  // phi with a one-layer linear extrapolation across the walls
 // Face (i,j,k) of component `axis` sits between cell (i,j,k) and the cell
 // one step back along the axis.  Cells around the face are addressed in
 // "face coordinates" relative to that low cell.
-template <class T, class V>
+// The component's axis is a template parameter so that every per-direction
+// array below is indexed by compile-time constants (registers, no stack).
+template <class T, class V, int axis>
 __global__ void k_visc_system(const T* __restrict__ phi, const T* __restrict__ u, const T* __restrict__ v,
-                              const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw, Lay Lf, int axis, double inv_h,
+                              const T* __restrict__ w, Lay Lc, Lay Lu, Lay Lv, Lay Lw, Lay Lf, double inv_h,
                               double dt, double rn, double rp, double mn, double mp, V* __restrict__ ax,
                               V* __restrict__ ay, V* __restrict__ az, V* __restrict__ diag, V* __restrict__ rhs) {
   FS_IJK(Lf);
@@ -74,6 +76,7 @@ __global__ void k_visc_system(const T* __restrict__ phi, const T* __restrict__ u
   // face one step back along d): normal arm -> the low cell, tangential arm
   // -> the edge shared by the four cells {low, high} x {d-1, d}
   double mu_low[3], mu_high[3], low[3], high[3];
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
     const int di = d == 0, dj = d == 1, dk = d == 2;
     if (d == axis) {
@@ -110,15 +113,15 @@ __global__ void k_visc_system(const T* __restrict__ phi, const T* __restrict__ u
   diag[f] = (V)(rho_f + ((((low[0] + high[0]) + low[1]) + high[1]) + low[2]) + high[2]);
   // explicit transpose terms (VISCOSITY_3D.h:620-630): for each tangential
   // direction t, d/dt( mu_edge * d(vel_t)/d(axis) ) with zero ghosts
-  const T* comp[3] = {u, v, w};
-  const Lay lay[3] = {Lu, Lv, Lw};
-  double ex = (double)comp[axis][f];
+  const T* own = axis == 0 ? u : (axis == 1 ? v : w);
+  double ex = (double)own[f];
   const double coef = dt / rho_f;
+#pragma unroll
   for (int t = 0; t < 3; ++t) {
     if (t == axis) continue;
     const int ti = t == 0, tj = t == 1, tk = t == 2;
-    const T* vt = comp[t];
-    const Lay& Lt = lay[t];
+    const T* vt = t == 0 ? u : (t == 1 ? v : w);
+    const Lay& Lt = t == 0 ? Lu : (t == 1 ? Lv : Lw);
     // vel_t at (face coords) + e_t and at the same place shifted back along axis
     const double hi_a = (double)vt[Lt.at(i + ti, j + tj, k + tk)];
     const double hi_b = (double)vt[Lt.at(i + ti - ea[0], j + tj - ea[1], k + tk - ea[2])];
@@ -294,8 +297,15 @@ void viscosity_system(const T* phi, const T* u, const T* v, const T* w, const La
                       double mu_pos, V* ax, V* ay, V* az, V* diag, V* rhs, cudaStream_t s) {
   const Lay& Lf = axis == 0 ? Lu : (axis == 1 ? Lv : Lw);
   Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
-  k_visc_system<T, V><<<g.grid, g.block, 0, s>>>(phi, u, v, w, Lc, Lu, Lv, Lw, Lf, axis, 1.0 / dx, dt, rho_neg,
-                                                 rho_pos, mu_neg, mu_pos, ax, ay, az, diag, rhs);
+  if (axis == 0)
+    k_visc_system<T, V, 0><<<g.grid, g.block, 0, s>>>(phi, u, v, w, Lc, Lu, Lv, Lw, Lf, 1.0 / dx, dt, rho_neg,
+                                                      rho_pos, mu_neg, mu_pos, ax, ay, az, diag, rhs);
+  else if (axis == 1)
+    k_visc_system<T, V, 1><<<g.grid, g.block, 0, s>>>(phi, u, v, w, Lc, Lu, Lv, Lw, Lf, 1.0 / dx, dt, rho_neg,
+                                                      rho_pos, mu_neg, mu_pos, ax, ay, az, diag, rhs);
+  else
+    k_visc_system<T, V, 2><<<g.grid, g.block, 0, s>>>(phi, u, v, w, Lc, Lu, Lv, Lw, Lf, 1.0 / dx, dt, rho_neg,
+                                                      rho_pos, mu_neg, mu_pos, ax, ay, az, diag, rhs);
 }
 
 #define FS_VISC_INST(T, V)                                                                                          \
