@@ -467,7 +467,7 @@ __global__ void k_adj_sum(const double* __restrict__ f, Lay L, double* partials,
 template <class T>
 __global__ void k_adj_pressure_operator(const T* __restrict__ phi, const double* __restrict__ lam,
                                         const double* __restrict__ p, double* phi_bar, double* rho_bar, Lay Lc,
-                                        double rn, double rp, double inv2) {
+                                        double rn, double rp, double inv2, int deflate) {
   double rbn = 0.0, rbp = 0.0;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -498,7 +498,7 @@ __global__ void k_adj_pressure_operator(const T* __restrict__ phi, const double*
       if (pc <= 0.0) rbn += bvc; else rbp += bvc;
       if (pn <= 0.0) rbn += bvn; else rbp += bvn;
     }
-    if (i == 0 && j == 0 && k == 0) {
+    if (deflate && i == 0 && j == 0 && k == 0) {
       // deflation: extra0 = inv2 (e_b + e_d) = 2 inv2 vc
       const double g = -lam[c] * p[c] * 2.0 * inv2 * (-vc * vc);
       if (pc <= 0.0) rbn += g; else rbp += g;
@@ -767,9 +767,10 @@ void adj_sum(const double* f, const Lay& L, double* partials, unsigned int* tick
 
 template <class T>
 void adj_pressure_operator(const T* phi, const double* lam, const double* p, double* phi_bar, double* rho_bar,
-                           const Lay& Lc, double dx, double rn, double rp, cudaStream_t s) {
+                           const Lay& Lc, double dx, double rn, double rp, int deflate, cudaStream_t s) {
   Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
-  k_adj_pressure_operator<T><<<g.grid, g.block, 0, s>>>(phi, lam, p, phi_bar, rho_bar, Lc, rn, rp, 1.0 / (dx * dx));
+  k_adj_pressure_operator<T><<<g.grid, g.block, 0, s>>>(phi, lam, p, phi_bar, rho_bar, Lc, rn, rp, 1.0 / (dx * dx),
+                                                        deflate);
 }
 
 template <class T>
@@ -806,7 +807,7 @@ void adj_axpy(double* out, const double* x, double a, const Lay& L, cudaStream_t
   template void adj_velcorr<T>(const double*, const T*, const double*, double*, double*, double*, double*,         \
                                const Lay&, const Lay&, int, double, double, double, double, double, cudaStream_t);   \
   template void adj_pressure_operator<T>(const T*, const double*, const double*, double*, double*, const Lay&,      \
-                                         double, double, double, cudaStream_t);                                      \
+                                         double, double, double, int, cudaStream_t);                                      \
   template void adj_visc<T>(const T*, const T*, const T*, const T*, const T*, const double*, double*, double*,      \
                             double*, double*, double*, const Lay&, const Lay&, const Lay&, const Lay&, int, double,  \
                             double, double, double, double, double, cudaStream_t);

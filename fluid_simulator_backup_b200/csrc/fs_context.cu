@@ -266,6 +266,14 @@ void apply_params(fs_ctx* c) {
   c->rb_ic0 = p.pressure_preconditioner == FS_PRECOND_RED_BLACK;
 }
 
+// The pressure system keeps the reference's deflation of the first cell only
+// in the faithful projection.  The corrected projection solves the singular
+// Neumann system as it is (consistent: b has zero mean), so that the
+// corrected velocity's divergence is the solve's residual in every cell;
+// with the deflation the first cell's divergence would carry the sum of the
+// residual, e0 p0 = -sum(r).
+int deflate(const fs_ctx* c) { return (c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) ? 1 : 0; }
+
 // ---------------------------------------------------------------------------
 // Krylov driver
 // ---------------------------------------------------------------------------
@@ -601,7 +609,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
   double rel = 0.0;
   const bool rb = c->red_black;
   build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
-                                    (float*)c->paz, (float*)c->pdiag, c->scalars + 12, s,
+                                    (float*)c->paz, (float*)c->pdiag, c->scalars + 12, deflate(c), s,
                                     (c->lean || rb) ? c->pdinv : nullptr);
   Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
   A.flux32 = c->flux32;
@@ -629,7 +637,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
   // red-black: p64 <- the black iterate, red cells eliminated in FP64
   auto commit = [&]() {
     if (!rb) return;
-    rb_commit<S>(phi, c->rb_x, b, x, c->Lc, c->Lh, dx, P.rho_neg, P.rho_pos, s);
+    rb_commit<S>(phi, c->rb_x, b, x, c->Lc, c->Lh, dx, P.rho_neg, P.rho_pos, deflate(c), s);
     c->launches += 1;
   };
   // true FP64 residual b - A64 p64 with A64 evaluated from phi in FP64; its
@@ -637,7 +645,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
   // residual), the Krylov residual of the mixed solve
   auto defect = [&](const float* x32, double* rel_out) -> fs_status {
     defect_residual<S>(phi, x, x32, b, nullptr, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
-                       c->tickets + 2, c->scalars + 2, s);
+                       c->tickets + 2, c->scalars + 2, deflate(c), s);
     c->launches += 1;
     if (rb) {
       rb_gather<float, float>(r32, c->rb_r, c->Lc, c->Lh, s);
@@ -786,7 +794,7 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
   double rel = 0.0;
   if (!c->fp32) {
     build_pressure_operator<S, double>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (double*)c->pax, (double*)c->pay,
-                                       (double*)c->paz, (double*)c->pdiag, c->scalars + 12, s);
+                                       (double*)c->paz, (double*)c->pdiag, c->scalars + 12, deflate(c), s);
     Op7<double> A{(double*)c->pax, (double*)c->pay, (double*)c->paz, (double*)c->pdiag, c->Lc, 1, c->scalars + 12};
     CKS(run_pcg<double>(c, 1, A, c->b64, c->p64, (double*)c->pr, (double*)c->pp, (double*)c->pq, P.tolerance,
                         P.max_iteration, P.stop, &iters, &rel, &st));
@@ -1129,7 +1137,7 @@ fs_status adj_projection(fs_ctx* c, void* phi, void* const ustar[3], const doubl
     CKS(mixed_solve<S>(c, F<S>(phi), pbar, lam, &it, &outer, &rel, &st));
   } else {
     build_pressure_operator<S, double>(F<S>(phi), c->Lc, dx, P.rho_neg, P.rho_pos, c->a_ax, c->a_ay, c->a_az,
-                                       c->a_diag, c->scalars + 12, s);
+                                       c->a_diag, c->scalars + 12, deflate(c), s);
     Op7<double> A{c->a_ax, c->a_ay, c->a_az, c->a_diag, c->Lc, 1, c->scalars + 12};
     CKS(run_pcg<double>(c, 3, A, pbar, lam, c->a_r, c->a_p, c->a_q, P.tolerance, std::max(P.max_iteration, 1),
                         FS_STOP_RELATIVE, &it, &rel, &st));
@@ -1140,7 +1148,7 @@ fs_status adj_projection(fs_ctx* c, void* phi, void* const ustar[3], const doubl
   }
   adj_sum(lam, c->Lc, c->partials, c->tickets + 4, c->scalars + 14, s);
   for (int a = 0; a < 3; ++a) adj_divergence(lam, c->scalars + 14, in_bar[a], *lays[a], c->Lc, a, dx, dt, s);
-  adj_pressure_operator<S>(F<S>(phi), lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, s);
+  adj_pressure_operator<S>(F<S>(phi), lam, p, phi_bar, c->a_rho, c->Lc, dx, P.rho_neg, P.rho_pos, deflate(c), s);
   c->launches += 5;
   CK(cudaGetLastError());
   return FS_OK;

@@ -145,7 +145,7 @@ void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, fl
 // from phi and b (the red rows of b - A p64 vanish)
 template <class T>
 void rb_commit(const T* phi, const double* xh, const double* b, double* p64, const Lay& L, const Lay& Lh, double dx,
-               double rho_neg, double rho_pos, cudaStream_t s);
+               double rho_neg, double rho_pos, int deflate, cudaStream_t s);
 // bf16 1/diag(S) of the black Schur complement per packed black slot: the
 // black pivots of IC(0) in red-black order
 void rb_schur_dinv(const RbOp& A, unsigned short* dinv, cudaStream_t s);
@@ -168,12 +168,16 @@ void divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay
 void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* partials, unsigned int* ticket,
                    double* scalars_out, cudaStream_t s);
 template <class T, class V>
+// deflate: the reference's fix of the first cell (the betas of its bottom and
+// down Neumann ghosts added to its diagonal, POISSON_SOLVER_3D.h:1145-1179),
+// which makes the Neumann system nonsingular; without it the system is
+// singular and consistent (b has zero mean) and CG solves it as such.
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
-                             V* diag, double* extra0, cudaStream_t s, unsigned short* dinv16 = nullptr);
+                             V* diag, double* extra0, int deflate, cudaStream_t s, unsigned short* dinv16 = nullptr);
 template <class T>
 void defect_residual(const T* phi, const double* p64, const float* x32, const double* b, double* r64, float* r32,
                      const Lay& Lc, double dx, double rho_neg, double rho_pos, double* partials, unsigned int* ticket,
-                     double* rr_out, cudaStream_t s);
+                     double* rr_out, int deflate, cudaStream_t s);
 void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s);
 template <class T>
 void velocity_correct(T* f, const T* base, const double* p, const T* phi, const Lay& Lf, const Lay& Lc, int axis,
@@ -239,7 +243,7 @@ void adj_divergence(const double* lam, const double* sum_lam, double* in_bar, co
 void adj_sum(const double* f, const Lay& L, double* partials, unsigned int* ticket, double* out, cudaStream_t s);
 template <class T>
 void adj_pressure_operator(const T* phi, const double* lam, const double* p, double* phi_bar, double* rho_bar,
-                           const Lay& Lc, double dx, double rn, double rp, cudaStream_t s);
+                           const Lay& Lc, double dx, double rn, double rp, int deflate, cudaStream_t s);
 template <class T>
 void adj_visc(const T* phi, const T* ug, const T* vg, const T* wg, const T* x, const double* lam, double* u_bar,
               double* v_bar, double* w_bar, double* phi_bar, double* rho_bar, const Lay& Lc, const Lay& Lu,

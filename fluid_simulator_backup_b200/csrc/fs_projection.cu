@@ -99,7 +99,8 @@ __global__ void k_pressure_faces(const T* __restrict__ phi, Lay Lc, double rn, d
 
 template <class T, class V>
 __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, double rp, double inv2,
-                                V* __restrict__ diag, double* __restrict__ extra0, unsigned short* __restrict__ dinv16) {
+                                V* __restrict__ diag, double* __restrict__ extra0, unsigned short* __restrict__ dinv16,
+                                int deflate) {
   FS_IJK(Lc);
   const int64_t c = Lc.at(i, j, k);
   const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
@@ -110,7 +111,9 @@ __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, do
   if (j < Lc.ny - 1) s += face_beta(vc, inv_rho(phi[c + Lc.px], rn, rp), acv, fabs((double)phi[c + Lc.px]));
   if (k > 0) s += face_beta(vc, inv_rho(phi[c - Lc.slab], rn, rp), acv, fabs((double)phi[c - Lc.slab]));
   if (k < Lc.nz - 1) s += face_beta(vc, inv_rho(phi[c + Lc.slab], rn, rp), acv, fabs((double)phi[c + Lc.slab]));
-  if (i == 0 && j == 0 && k == 0) {
+  if (i == 0 && j == 0 && k == 0 && !deflate) {
+    if (extra0) *extra0 = 0.0;
+  } else if (i == 0 && j == 0 && k == 0) {
     // deflation: the ghost 1/rho is the clamped copy of vc and the ghost phi
     // the linear extrapolation 2 phi0 - phi1 along the axis
     const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
@@ -132,7 +135,7 @@ template <class T>
 __global__ void k_defect_residual(const T* __restrict__ phi, const double* __restrict__ p, const float* __restrict__ x32,
                                   const double* __restrict__ b, double* __restrict__ r64, float* __restrict__ r32,
                                   Lay Lc, double rn, double rp, double inv2, double* partials, unsigned int* ticket,
-                                  double* rr_out) {
+                                  double* rr_out, int deflate) {
   double rr = 0.0;
   Cursor cur;
   for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
@@ -150,7 +153,7 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
       const double xn = x32 ? p[nb[q]] + (double)x32[nb[q]] : p[nb[q]];
       flux += face_coef(pc, (double)phi[nb[q]], 1.0 / rn, 1.0 / rp) * (xc - xn);
     }
-    if (i == 0 && j == 0 && k == 0) {
+    if (deflate && i == 0 && j == 0 && k == 0) {
       const double vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
       const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
       const double gd = fabs(2.0 * pc - (double)phi[c + Lc.slab]);
@@ -436,19 +439,19 @@ void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* part
 
 template <class T, class V>
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
-                             V* diag, double* extra0, cudaStream_t s, unsigned short* dinv16) {
+                             V* diag, double* extra0, int deflate, cudaStream_t s, unsigned short* dinv16) {
   Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
   const double inv2 = 1.0 / (dx * dx);
   k_pressure_faces<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, ax, ay, az);
-  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag, extra0, dinv16);
+  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag, extra0, dinv16, deflate);
 }
 
 template <class T>
 void defect_residual(const T* phi, const double* p64, const float* x32, const double* b, double* r64, float* r32,
                      const Lay& Lc, double dx, double rho_neg, double rho_pos, double* partials, unsigned int* ticket,
-                     double* rr_out, cudaStream_t s) {
+                     double* rr_out, int deflate, cudaStream_t s) {
   k_defect_residual<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, p64, x32, b, r64, r32, Lc, rho_neg, rho_pos,
-                                                              1.0 / (dx * dx), partials, ticket, rr_out);
+                                                              1.0 / (dx * dx), partials, ticket, rr_out, deflate);
 }
 
 void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s) {
@@ -517,7 +520,7 @@ void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s)
   template void divergence_rhs<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,     \
                                   double, double, double*, double*, double*, unsigned int*, double*, cudaStream_t); \
   template void defect_residual<T>(const T*, const double*, const float*, const double*, double*, float*,         \
-                                   const Lay&, double, double, double, double*, unsigned int*, double*,             \
+                                   const Lay&, double, double, double, double*, unsigned int*, double*, int,        \
                                    cudaStream_t);                                                                   \
   template void velocity_correct<T>(T*, const T*, const double*, const T*, const Lay&, const Lay&, int, double,     \
                                     double, double, double, int, double, double, const double*, double,            \
@@ -536,7 +539,7 @@ FS_PINST(double)
 
 #define FS_BINST(T, V)                                                                                        \
   template void build_pressure_operator<T, V>(const T*, const Lay&, double, double, double, V*, V*, V*, V*, double*, \
-                                              cudaStream_t, unsigned short*);
+                                              int, cudaStream_t, unsigned short*);
 FS_BINST(float, float)
 FS_BINST(double, double)
 FS_BINST(double, float)

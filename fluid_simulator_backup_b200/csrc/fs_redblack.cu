@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kFX * kFY) k_rb_spmv(RbOp A, const float* __re
 // inv_dx2 (den p_c - sum_nb beta p_nb) = b_c  =>  p_c = (dx^2 b_c + sum) / den.
 template <class T>
 __global__ void k_rb_commit(const T* __restrict__ phi, const double* __restrict__ xh, const double* __restrict__ b,
-                            double* __restrict__ p64, Lay L, Lay H, double rn, double rp, double dx2) {
+                            double* __restrict__ p64, Lay L, Lay H, double rn, double rp, double dx2, int deflate) {
   const int h = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -202,7 +202,7 @@ __global__ void k_rb_commit(const T* __restrict__ phi, const double* __restrict_
     sum += beta * xh[nbs[q]];
     den += beta;
   }
-  if (ir == 0 && j == 0 && k == 0) {
+  if (deflate && ir == 0 && j == 0 && k == 0) {
     // deflation: the betas of the bottom and down Neumann ghosts (POISSON_SOLVER_3D.h:1145-1179)
     const double vc = pc <= 0.0 ? vneg : vpos, acv = fabs(pc);
     const double gb = fabs(2.0 * pc - (double)phi[c + L.px]);
@@ -302,8 +302,8 @@ void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, fl
 
 template <class T>
 void rb_commit(const T* phi, const double* xh, const double* b, double* p64, const Lay& L, const Lay& H, double dx,
-               double rho_neg, double rho_pos, cudaStream_t s) {
-  k_rb_commit<T><<<rb_grid(H), kRbBlock, 0, s>>>(phi, xh, b, p64, L, H, rho_neg, rho_pos, dx * dx);
+               double rho_neg, double rho_pos, int deflate, cudaStream_t s) {
+  k_rb_commit<T><<<rb_grid(H), kRbBlock, 0, s>>>(phi, xh, b, p64, L, H, rho_neg, rho_pos, dx * dx, deflate);
 }
 
 void rb_schur_dinv(const RbOp& A, unsigned short* dinv, cudaStream_t s) {
@@ -316,9 +316,9 @@ void rb_gather(const S* full, D* half, const Lay& L, const Lay& H, cudaStream_t 
 }
 
 template void rb_commit<float>(const float*, const double*, const double*, double*, const Lay&, const Lay&, double,
-                               double, double, cudaStream_t);
+                               double, double, int, cudaStream_t);
 template void rb_commit<double>(const double*, const double*, const double*, double*, const Lay&, const Lay&, double,
-                                double, double, cudaStream_t);
+                                double, double, int, cudaStream_t);
 template void rb_gather<double, double>(const double*, double*, const Lay&, const Lay&, cudaStream_t);
 template void rb_gather<float, float>(const float*, float*, const Lay&, const Lay&, cudaStream_t);
 template void rb_gather<unsigned short, unsigned short>(const unsigned short*, unsigned short*, const Lay&,

@@ -815,7 +815,11 @@ def projection(phi, u, v, w, dx, dt, rho_neg, rho_pos, tol, max_iter, mode="corr
     mean (POISSON_SOLVER_3D.h:225-246), Jacobi-PCG, velocity correction with
     the jump.  Returns (u, v, w, p, info)."""
     div = divergence(u, v, w, dx, dt)
-    op = poisson_operator(phi, dx, rho_neg, rho_pos)
+    # faithful: the reference's deflated (nonsingular) system; corrected: the
+    # singular consistent Neumann system, so that the corrected velocity's
+    # divergence is the residual in every cell (the deflation would leave the
+    # residual's sum in the first cell)
+    op = poisson_operator(phi, dx, rho_neg, rho_pos, deflate=(mode == "faithful"))
     jc = None
     if sigma != 0.0:
         kappa, _ = curvature(phi, dx, curvature_typo)
