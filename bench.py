@@ -39,11 +39,16 @@ sys.path.insert(0, ROOT)
 BYTES_PER_UNKNOWN_PCG_FP32 = 64
 # FP64: spmv 40 + residual update 32 + direction update 48
 BYTES_PER_UNKNOWN_PCG_FP64 = 120
-# DRAM bytes (read + write) of one FP32 PCG iteration at 256^3 measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of k_cg_spmv, k_cg_update,
-# k_cg_pupdate, one capture of the bench workload); scaled by the unknowns
-# for other sizes
+# red-black IC(0) (per cell of the grid, the black vectors holding half the
+# cells): SpMV 16 (ax, ay, az 12; black p 2; black q 2) + residual update 7 +
+# direction update 15, at about half the iterations
+BYTES_PER_CELL_PCG_RB = 38
+# DRAM bytes (read + write) of one FP32 Jacobi PCG iteration at 256^3
+# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of
+# k_cg_spmv, k_cg_update, k_cg_pupdate, one capture of the bench workload);
+# scaled by the unknowns for other sizes
 TRAFFIC_PER_ITERATION_256_FP32 = 1006.4e6
+TRAFFIC_PER_ITERATION_256_RB = None
 
 
 def scene(n):
@@ -55,6 +60,12 @@ def scene(n):
 
 PRECONDITIONER = {"default": 0, "jacobi": 1, "bf16": 2, "red_black": 3, "red_black_jacobi": 4}
 PRECOND_CHOICE = "default"
+# what FS_PRECOND_DEFAULT selects in an FP32_REFINE context
+DEFAULT_FP32_PRECONDITIONER = "bf16"
+
+
+def effective_preconditioner(fs):
+    return DEFAULT_FP32_PRECONDITIONER if PRECOND_CHOICE == "default" else PRECOND_CHOICE
 HOST_LOOP = 0  # 1: Krylov batches launched from the host (for profilers), not as one graph per solve
 
 
@@ -137,6 +148,10 @@ def run_steps(fs, n, precision, warmup, steps, barrier, record=0):
         reps.append(s.step(dt, allow_not_converged=True))
     torch.cuda.synchronize()
     barrier()
+    # divergence of the last projection's input (stored as div/dt), for the
+    # relative divergence of the corrected velocity (outside the timed region)
+    if reps:
+        reps[-1]["div_input_l2"] = float(np.linalg.norm(s.download("divergence"))) * dt
     return s, reps, states
 
 
@@ -565,7 +580,17 @@ def main():
     # device time of the pressure solves per real iteration (the launched
     # count adds the idle tail of the last graph batch of each solve)
     per_iter_s = pcg_ms / 1e3 / max(real_its, 1)
-    bpu = BYTES_PER_UNKNOWN_PCG_FP32 if main_prec == fs.FS_PRECISION_FP32_REFINE else BYTES_PER_UNKNOWN_PCG_FP64
+    rb = main_prec == fs.FS_PRECISION_FP32_REFINE and effective_preconditioner(fs) in ("red_black", "red_black_jacobi")
+    if main_prec == fs.FS_PRECISION_FP64:
+        bpu, kernel = BYTES_PER_UNKNOWN_PCG_FP64, "FP64 Jacobi PCG iteration (spmv + update + direction, 3 kernels)"
+        traffic = None
+    elif rb:
+        bpu = BYTES_PER_CELL_PCG_RB
+        kernel = "red-black IC(0) PCG iteration (pipelined Schur-complement spmv + update + direction, 3 kernels)"
+        traffic = TRAFFIC_PER_ITERATION_256_RB * N / 256 ** 3 if TRAFFIC_PER_ITERATION_256_RB else None
+    else:
+        bpu, kernel = BYTES_PER_UNKNOWN_PCG_FP32, "FP32 Jacobi PCG iteration (spmv + update + direction, 3 kernels)"
+        traffic = TRAFFIC_PER_ITERATION_256_FP32 * N / 256 ** 3
     achieved = bpu * N / per_iter_s / 1e9
     peaks = {}
     try:
@@ -616,17 +641,19 @@ def main():
                 "steps": "the first %d timed steps replayed from their saved states" % min(args.e2e_steps, args.steps),
                 "device_ms_same_steps": e2e_device_ms},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "pressure PCG iteration (spmv + update + direction, 3 kernels)",
+        "roofline": {"bound": "hbm", "kernel": kernel, "preconditioner": effective_preconditioner(fs),
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src,
-                     "traffic": (TRAFFIC_PER_ITERATION_256_FP32 * N / 256 ** 3
-                                 if main_prec == fs.FS_PRECISION_FP32_REFINE else None),
+                     "traffic": traffic,
                      "traffic_unit": "bytes per PCG iteration (ncu capture at 256^3, scaled by unknowns)",
                      "bytes_per_iteration": bpu * N,
                      "pcg_ms": pcg_ms, "pcg_launched_iterations": pcg_its, "pcg_iterations": real_its},
         "fp64": fp64,
         "adjoint": adjoint,
         "divergence": {"div_l2_last": reps[-1]["div_l2"], "div_linf_max": max(r["div_linf"] for r in reps),
+                       "div_input_l2_last": reps[-1].get("div_input_l2"),
+                       "relative_l2_last": (reps[-1]["div_l2"] / reps[-1]["div_input_l2"]
+                                            if reps[-1].get("div_input_l2") else None),
                        "max_rel_residual": max(r["max_rel_residual"] for r in reps)},
         "clocks": clk.summary(),
         "cpu_baseline": cpu,

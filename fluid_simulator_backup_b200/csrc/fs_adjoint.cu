@@ -593,13 +593,13 @@ __global__ void k_adj_visc(const T* __restrict__ phi, const T* __restrict__ ug, 
     const double rho_f = rn + (rp - rn) * H;
     // u_bar[a] += rho_f lambda
     atomicAdd(&cbar[axis][f], rho_f * lamf);
-    // rho_f bar: lambda (u_f - x_f)
-    const double rfb = lamf * (comp[axis][f] - xf);
-    rbn += rfb * (1.0 - H);
-    rbp += rfb * H;
-    const double pb_rho = rfb * (rp - rn) * dH * 0.5;
-    P.scatter(phi_bar, li, lj, lk, pb_rho);
-    P.scatter(phi_bar, i, j, k, pb_rho);
+    // The rho_f bar is lambda (u_f - x_f), the viscous change of the face
+    // velocity.  It is formed as (K x - E)/rho_f (K the viscous part of the
+    // matrix, E the explicit transpose terms: rho_f (u - x) = K x - E for the
+    // solved system), accumulated over the arms below, rather than as the
+    // difference of the stored velocities, which in FP32 storage cancels to
+    // a few digits when the viscous change is small.
+    double Kx = 0.0, Ex = 0.0;
     // arms
     for (int d = 0; d < 3; ++d) {
       const int di = d == 0, dj = d == 1, dk = d == 2;
@@ -634,6 +634,7 @@ __global__ void k_adj_visc(const T* __restrict__ phi, const T* __restrict__ ug, 
                       P.at(hi_i[3], hi_j[3], hi_k[3]));
       }
       const double dmu_lo = (mp - mn) * heaviside_d(mlo, e), dmu_hi = (mp - mn) * heaviside_d(mhi, e);
+      const double mu_lo_d = mn + (mp - mn) * heaviside(mlo, e), mu_hi_d = mn + (mp - mn) * heaviside(mhi, e);
       double glo = 0.0, ghi = 0.0;  // bars of mu_low[d], mu_high[d]
       // matrix, low arm: neighbour f - e_d (zero if it is a wall face or beyond)
       {
@@ -643,6 +644,7 @@ __global__ void k_adj_visc(const T* __restrict__ phi, const T* __restrict__ ug, 
         const double xn = nb_wall ? 0.0 : x[Lf.at(ni, nj, nk)];
         const double ln = nb_wall ? 0.0 : lam[Lf.at(ni, nj, nk)];
         glo -= K * (lamf - ln) * (xf - xn);
+        Kx += K * mu_lo_d * (xf - xn);
       }
       // matrix, high arm: only when the neighbour row does not own it (wall or beyond)
       {
@@ -651,6 +653,8 @@ __global__ void k_adj_visc(const T* __restrict__ phi, const T* __restrict__ ug, 
         const int nn = d == 0 ? Lf.nx : (d == 1 ? Lf.ny : Lf.nz);
         const bool nb_wall = (d == axis && en == nn - 1) || en >= nn;
         if (nb_wall) ghi -= K * lamf * xf;
+        const double xn = nb_wall ? 0.0 : x[Lf.at(ni, nj, nk)];
+        Kx += K * mu_hi_d * (xf - xn);
       }
       // right-hand side: explicit transpose terms for tangential d
       if (d != axis) {
@@ -662,10 +666,10 @@ __global__ void k_adj_visc(const T* __restrict__ phi, const T* __restrict__ ug, 
         const double hi_d = vt[ia] - vt[ib], lo_d = vt[ja] - vt[jb];
         ghi += lamf * dt * inv2 * hi_d;
         glo -= lamf * dt * inv2 * lo_d;
+        Ex += dt * inv2 * (mu_hi_d * hi_d - mu_lo_d * lo_d);
         // transpose to the tangential component (its ghosts are zero constants)
         // mu values of the forward
-        const double mu_hi = mn + (mp - mn) * heaviside(mhi, e), mu_lo = mn + (mp - mn) * heaviside(mlo, e);
-        const double ch = lamf * dt * inv2 * mu_hi, cl = lamf * dt * inv2 * mu_lo;
+        const double ch = lamf * dt * inv2 * mu_hi_d, cl = lamf * dt * inv2 * mu_lo_d;
         auto inside = [&](int a, int b, int q) { return a >= 0 && b >= 0 && q >= 0 && a < Lt.nx && b < Lt.ny && q < Lt.nz; };
         if (inside(i + ti, j + tj, k + tk)) atomicAdd(&cbar[d][ia], ch);
         if (inside(i + ti - ea[0], j + tj - ea[1], k + tk - ea[2])) atomicAdd(&cbar[d][ib], -ch);
@@ -679,6 +683,13 @@ __global__ void k_adj_visc(const T* __restrict__ phi, const T* __restrict__ ug, 
         P.scatter(phi_bar, hi_i[q], hi_j[q], hi_k[q], phi_hi);
       }
     }
+    // rho_f bar: lambda (u_f - x_f) = lambda (K x - E)_f / rho_f
+    const double rfb = lamf * (Kx - Ex) / rho_f;
+    rbn += rfb * (1.0 - H);
+    rbp += rfb * H;
+    const double pb_rho = rfb * (rp - rn) * dH * 0.5;
+    P.scatter(phi_bar, li, lj, lk, pb_rho);
+    P.scatter(phi_bar, i, j, k, pb_rho);
   }
   rbn = block_sum(rbn);
   __syncthreads();

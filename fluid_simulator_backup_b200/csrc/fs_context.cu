@@ -90,7 +90,7 @@ struct fs_ctx {
   // red-black reduced FP32 pressure solve (packed half layout Lh, fs_redblack.cu)
   Lay Lh{};
   double* rb_x = nullptr;          // black FP64 iterate
-  float *rb_r = nullptr, *rb_p = nullptr, *rb_q = nullptr;
+  float *rb_r = nullptr, *rb_p = nullptr, *rb_q = nullptr, *rb_tau = nullptr;
   unsigned short* rb_dinv = nullptr;  // black bf16 1/diag
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
   // viscosity systems, one per component (storage type S)
@@ -134,9 +134,10 @@ struct fs_ctx {
   int flux32 = 2;               // params.flux_arithmetic (Op7::flux32)
   int lean = 1;                 // FP32 pressure solve preconditioned by the bf16 inverse diagonal (Op7::dinv16)
   bool red_black = false;       // FP32 pressure solve on the red-black Schur complement
-  bool rb_ic0 = true;
+  bool rb_ic0 = true;           // its preconditioner: 1/diag(S) (IC(0) in red-black order), else the black 1/diag
   int adj_unconverged = 0;      // adjoint solves of the current call that stopped before their tolerance
-  double adj_worst_rel = 0.0;   // and the worst relative residual they reached           // its preconditioner: 1/diag(S) (IC(0) in red-black order), else the black 1/diag
+  double adj_worst_rel = 0.0;   // and the worst relative residual they reached
+  char adj_note[128] = {0};     // the last of them: which solve, its status and iterations
 
   size_t S() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
@@ -372,7 +373,7 @@ fs_status run_pcg(fs_ctx* c, int key, const Op7<V>& A, const V* b, V* x, V* r, V
   init.max_iter = max_iter;
   init.criterion = criterion;
   // FP32 viscosity solves can stall at their rounding floor before a tight tolerance
-  init.stall_limit = (c->fp32 && key >= 100) ? 400 : 0;
+  init.stall_limit = (c->fp32 && key >= 100 && key < 110) ? 400 : 0;  // the FP32 forward viscosity solves
   *c->st_host = init;
   const bool timed = key < 100;  // pressure solves
   CK(cudaMemcpyAsync(c->st, c->st_host, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
@@ -673,7 +674,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
     // search direction p and q = A p are FP32 (the flux-form operator in
     // FP32 arithmetic, Op7::flux32, or the red-black Schur complement in
     // its offset form) and the Jacobi preconditioner is 1/diag in bf16: 64
-    // bytes per unknown and iteration (red-black: 38 per cell at half the
+    // bytes per unknown and iteration (red-black: 56 per cell at half the
     // iterations) against 120 for the FP64 solve.  Every time the recursive
     // residual drops by reliable_delta the true FP64 residual of p64
     // replaces it (reliable update), keeping the search direction; the
@@ -701,7 +702,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
       if (rb) {
         CKS(drive_pcg(c, std::make_pair(4, (const void*)nullptr),
                       [&] {
-                        rb_iteration(R, Ah, c->rb_x, c->rb_r, c->rb_p, c->rb_q, c->st, c->partials, s);
+                        rb_iteration(R, Ah, c->rb_x, c->rb_r, c->rb_p, c->rb_q, c->rb_tau, c->st, c->partials, s);
                       },
                       P.max_iteration, true, 4));
       } else {
@@ -1145,6 +1146,8 @@ fs_status adj_projection(fs_ctx* c, void* phi, void* const ustar[3], const doubl
   if (st != PCG_CONVERGED) {
     c->adj_unconverged += 1;
     c->adj_worst_rel = std::max(c->adj_worst_rel, rel);
+    std::snprintf(c->adj_note, sizeof c->adj_note, "pressure: status %d after %d iterations, residual %.3e", st, it,
+                  rel);
   }
   adj_sum(lam, c->Lc, c->partials, c->tickets + 4, c->scalars + 14, s);
   for (int a = 0; a < 3; ++a) adj_divergence(lam, c->scalars + 14, in_bar[a], *lays[a], c->Lc, a, dx, dt, s);
@@ -1177,7 +1180,10 @@ fs_status adj_viscosity(fs_ctx* c, void* phi, void* const ug[3], void* const x[3
     CKS(run_pcg<double>(c, 120 + a, A, c->a_vxb[a], c->a_vlam[a], c->a_vs[a][6], c->a_vs[a][7], c->a_vs[a][8],
                         P.viscosity_tolerance, std::max(P.viscosity_max_iteration, 1), FS_STOP_RELATIVE, &it, nullptr,
                         &st));
-    if (st != PCG_CONVERGED) c->adj_unconverged += 1;
+    if (st != PCG_CONVERGED) {
+      c->adj_unconverged += 1;
+      std::snprintf(c->adj_note, sizeof c->adj_note, "viscosity component %d: status %d after %d iterations", a, st, it);
+    }
     adj_visc<S>(F<S>(phi), F<S>(ug[0]), F<S>(ug[1]), F<S>(ug[2]), F<S>(x[a]), c->a_vlam[a], in_bar[0], in_bar[1],
                 in_bar[2], phi_bar, c->a_rho, c->Lc, c->Lu, c->Lv, c->Lw, a, dx, dt, P.rho_neg, P.rho_pos, P.mu_neg,
                 P.mu_pos, s);
@@ -1435,7 +1441,7 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
     c->Lh = make_half_lay(c->Lc);
     const size_t hb = c->Lh.total;
     if ((s = dalloc(c, (void**)&c->rb_x, hb * sizeof(double))) != FS_OK) return fail(s);
-    float** hv[] = {&c->rb_r, &c->rb_p, &c->rb_q};
+    float** hv[] = {&c->rb_r, &c->rb_p, &c->rb_q, &c->rb_tau};
     for (float** p : hv) if ((s = dalloc(c, (void**)p, hb * sizeof(float))) != FS_OK) return fail(s);
     if ((s = dalloc(c, (void**)&c->rb_dinv, hb * sizeof(unsigned short))) != FS_OK) return fail(s);
   }
@@ -1936,9 +1942,9 @@ fs_status fs_adjoint_density_bars(fs_ctx* c, double* rho_neg_bar, double* rho_po
 // the call completes and reports FS_NOT_CONVERGED.
 static fs_status adj_finish(fs_ctx* c, fs_status s) {
   if (s == FS_OK && c->adj_unconverged > 0) {
-    char msg[160];
-    std::snprintf(msg, sizeof msg, "%d adjoint solve(s) stopped before their tolerance (worst pressure residual %.3e)",
-                  c->adj_unconverged, c->adj_worst_rel);
+    char msg[320];
+    std::snprintf(msg, sizeof msg, "%d adjoint solve(s) stopped before their tolerance (last: %s)", c->adj_unconverged,
+                  c->adj_note);
     set_error(msg);
     return FS_NOT_CONVERGED;
   }
@@ -1948,6 +1954,7 @@ static fs_status adj_finish(fs_ctx* c, fs_status s) {
 static void adj_begin(fs_ctx* c) {
   c->adj_unconverged = 0;
   c->adj_worst_rel = 0.0;
+  c->adj_note[0] = 0;
 }
 
 fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {

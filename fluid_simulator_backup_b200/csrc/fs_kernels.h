@@ -139,8 +139,8 @@ int rb_blocks(const Lay& Lh);
 // One CG iteration on the black Schur complement: red stage (tau), black
 // stage (q = S p, p.q, alpha), then cg_vector_updates on the packed black
 // vectors with Ah (layout Lh, dinv16 the packed black bf16 1/diag).
-void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, PcgState* st,
-                  double* partials, cudaStream_t s);
+void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
+                  PcgState* st, double* partials, cudaStream_t s);
 // p64 <- black cells from the packed iterate xh, red cells eliminated in FP64
 // from phi and b (the red rows of b - A p64 vanish)
 template <class T>

@@ -36,16 +36,13 @@
 // (eps32 of the fluxes, not of |p|).  b0(r) is r's x-1 neighbour, or its
 // x+1 neighbour for r at i = 0.
 //
-// Kernels of one iteration:
-//   k_rb_spmv_pipe  q = S p, p.q and alpha: the operands staged plane by plane
-//                   in shared memory by cp.async a few planes ahead, tau of
-//                   the red cells computed there into a ring of planes
-//                   (couplings 12 B, black p 2 B, black q 2 B per cell, plus
-//                   the tile halo)
+// Kernels of one iteration (each array element once per kernel):
+//   k_rb_red    tau of every red cell          reads ax, ay, az, p     writes tau
+//   k_rb_black  q = S p, p.q and alpha         reads ax, ay, az, p, tau writes q
 //   k_cg_update / k_cg_pupdate (fs_krylov.cu) on the packed black vectors
-//                   (7 + 15 B per cell: FP32 r, p, q, FP64 iterate, bf16 1/diag)
-// = 38 bytes per cell and iteration, at half the iterations of the full
-// Jacobi-PCG's 64.
+// = 16 + 18 + 7 + 15 = 56 bytes per cell and iteration (FP32 couplings and
+// vectors, FP64 black iterate, bf16 black pivots), at half the iterations of
+// the full Jacobi-PCG's 64.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -58,196 +55,96 @@ Lay make_half_lay(const Lay& L) { return make_lay((L.nx + 1) / 2, L.ny, L.nz); }
 
 namespace {
 
-// ---------------------------------------------------------------------------
-// q = S p, pipelined.  The same two stages and arithmetic as above, with every
-// operand staged in shared memory: a block owns a tile of TX x TY packed
-// slots (2 TX x TY cells) and walks a chunk of z planes; for each plane it
-// copies, 16 bytes per cp.async, the plane's p (tile + 2-slot halo in y,
-// 4 in x) and its three coupling arrays (tile + halo) into one stage of a
-// ring of NS stages, DIST planes ahead of the plane being computed.  The
-// copies of plane k+2+DIST are in flight while tau of plane k+1 and q of
-// plane k are computed from the stages of planes k-1 .. k+2, so the kernel
-// waits on memory once per chunk instead of once per plane.  HBM carries
-// about 21 bytes per cell (the 16 of the operands plus the halo).
-// ---------------------------------------------------------------------------
-namespace rbp {
-constexpr int TX = 32, TY = 8;              // tile of packed slots (threads)
-constexpr int PW = TX + 8, PR = TY + 4;     // p stage: slots h0-4 .. h0+TX+3, rows j0-2 .. j0+TY+1
-constexpr int CW = 2 * TX + 8;              // coupling stages: cells 2h0-4 .. 2h0+2TX+3
-constexpr int XR = TY + 2, YR = TY + 3, ZR = TY + 2;  // rows j0-1 .. j0+TY (ax, az), .. j0+TY+1 (ay)
-constexpr int OFF_X = PR * PW, OFF_Y = OFF_X + XR * CW, OFF_Z = OFF_Y + YR * CW, STAGE = OFF_Z + ZR * CW;
-constexpr int CP = PR * (PW / 4), CX = XR * (CW / 4), CY = YR * (CW / 4), CZ = ZR * (CW / 4);
-constexpr int CHUNKS = CP + CX + CY + CZ;   // 16-byte copies per plane
-constexpr int TW = TX + 2, TH = TY + 2;     // tau plane: tile + one-slot halo
-// DIST planes in flight beyond the four in use; NS = 4 + DIST stages
-constexpr size_t smem_bytes(int dist) { return (size_t)(4 + dist) * STAGE * sizeof(float); }
-static_assert(STAGE % 4 == 0 && OFF_X % 4 == 0 && OFF_Y % 4 == 0 && OFF_Z % 4 == 0, "16-byte aligned stage parts");
-}  // namespace rbp
+// q = S p in two passes.  The red pass writes tau of every red cell (one
+// thread per packed slot, a (32, 8) tile of slots per block and plane); the
+// black pass reads the couplings, p and the six tau of each black cell,
+// writes q and reduces p.q.  Each block of the black pass walks a chunk of
+// z planes so that the p.q reduction has a few hundred partial sums instead
+// of one per plane and tile.  Both passes are plain streaming kernels with
+// few instructions per cell: measured at 256^3 they run faster than fused
+// forms that keep tau on chip (a z-marching shared-memory ring, and a
+// cp.async-staged pipeline), whose per-plane barriers and index arithmetic
+// made them issue- and latency-bound.
+constexpr int kRbBY = 8;
 
-// Source of 16-byte copy t of the stage of plane kk and its offset in the
-// stage (floats); nullptr when the four values lie outside the padded array
-// (the stage gets zeros there, values no computation reads).
-__host__ __device__ inline const float* rb_chunk_src(const RbOp& A, const float* p, int h0, int j0, int kk, int t,
-                                                     int* dst) {
-  using namespace rbp;
-  const float* base;
-  const Lay* Y;
-  int w, off, row0, col0;
-  if (t < CP) {
-    base = p; Y = &A.Lh; w = PW; off = 0; row0 = j0 - 2; col0 = h0 - 4;
-  } else if ((t -= CP) < CX) {
-    base = A.ax; Y = &A.L; w = CW; off = OFF_X; row0 = j0 - 1; col0 = 2 * h0 - 4;
-  } else if ((t -= CX) < CY) {
-    base = A.ay; Y = &A.L; w = CW; off = OFF_Y; row0 = j0 - 1; col0 = 2 * h0 - 4;
-  } else {
-    t -= CY;
-    base = A.az; Y = &A.L; w = CW; off = OFF_Z; row0 = j0 - 1; col0 = 2 * h0 - 4;
-  }
-  const int r = t / (w / 4), c4 = t % (w / 4);
-  *dst = off + r * w + 4 * c4;
-  const int j = row0 + r;
-  const int col = col0 + GX + 4 * c4;  // column within the padded row (a multiple of 4)
-  if (j + GH < 0 || j + GH >= Y->py || kk + GH < 0 || kk + GH >= Y->nz + 2 * GH || col < 0 || col + 3 >= Y->px)
-    return nullptr;
-  return base + ((int64_t)(kk + GH) * Y->py + (j + GH)) * Y->px + col;
-}
-
-// Operand access in a stage (tile origin h0, j0).
-__host__ __device__ inline int rb_sp(int h0, int j0, int h, int j) {
-  return (j - (j0 - 2)) * rbp::PW + (h - (h0 - 4));
-}
-__host__ __device__ inline int rb_sc(int h0, int j0, int i, int j) {
-  return (j - (j0 - 1)) * rbp::CW + (i - (2 * h0 - 4));
-}
-
-// tau of the red cell in slot (h, j, k) from the stages of planes k-1, k, k+1
-// (the expression of rb_tau_at, operand for operand).
-__host__ __device__ inline float rb_tau_s(const RbOp& A, const float* sm, const float* s0, const float* sp, int h0,
-                                          int j0, int h, int j, int k, float e0) {
-  using namespace rbp;
+// tau of the red cell in slot (h, j, k) (in range)
+__device__ __forceinline__ float rb_tau(const RbOp& A, const float* __restrict__ p, int h, int j, int k) {
   const Lay& L = A.L;
   const Lay& H = A.Lh;
-  if (h < 0 || j < 0 || k < 0 || h >= H.nx || j >= H.ny || k >= H.nz) return 0.0f;
   const int pr = (j + k) & 1;
   const int i = 2 * h + pr;
   if (i >= L.nx) return 0.0f;
-  const float pxm = s0[rb_sp(h0, j0, h + pr - 1, j)], pxp = s0[rb_sp(h0, j0, h + pr, j)];
-  const float pym = s0[rb_sp(h0, j0, h, j - 1)], pyp = s0[rb_sp(h0, j0, h, j + 1)];
-  const float pzm = sm[rb_sp(h0, j0, h, j)], pzp = sp[rb_sp(h0, j0, h, j)];
-  const float axm = s0[OFF_X + rb_sc(h0, j0, i, j)], axp = s0[OFF_X + rb_sc(h0, j0, i + 1, j)];
-  const float aym = s0[OFF_Y + rb_sc(h0, j0, i, j)], ayp = s0[OFF_Y + rb_sc(h0, j0, i, j + 1)];
-  const float azm = s0[OFF_Z + rb_sc(h0, j0, i, j)], azp = sp[OFF_Z + rb_sc(h0, j0, i, j)];
+  const int64_t s = H.at(h, j, k);
+  const int64_t c = L.at(i, j, k);
+  // the six black neighbours (packed) and the couplings of the six faces
+  const float pxm = p[s + pr - 1], pxp = p[s + pr];
+  const float pym = p[s - H.px], pyp = p[s + H.px];
+  const float pzm = p[s - H.slab], pzp = p[s + H.slab];
+  const float axm = A.ax[c], axp = A.ax[c + 1];
+  const float aym = A.ay[c], ayp = A.ay[c + L.px];
+  const float azm = A.az[c], azp = A.az[c + L.slab];
   const float b0 = i > 0 ? pxm : pxp;
   float num = axm * (pxm - b0) + axp * (pxp - b0);
   num += aym * (pym - b0) + ayp * (pyp - b0);
   num += azm * (pzm - b0) + azp * (pzp - b0);
   float d = ((axm + axp) + (aym + ayp)) + (azm + azp);
   if (i == 0 && j == 0 && k == 0) {
+    const float e0 = (float)(*A.extra0);
     num -= e0 * b0;
     d += e0;
   }
   return d > 0.0f ? num / d : 0.0f;
 }
 
-// (S p) of the black cell in slot (h, j, k), in-tile slot (tx, ty), from the
-// stages of planes k-1, k, k+1 and the tau planes k-1, k, k+1 (tile + halo).
-__host__ __device__ inline float rb_q_s(const RbOp& A, const float* sm, const float* s0, const float* sp,
-                                        const float* tm, const float* t0, const float* tp, int h0, int j0, int h, int j,
-                                        int k, float* pc_out) {
-  using namespace rbp;
-  const int pb = (j + k + 1) & 1;
-  const int i = 2 * h + pb;
-  *pc_out = 0.0f;
-  if (i >= A.L.nx) return 0.0f;
-  const int tx = h - h0 + 1, ty = j - j0 + 1;
-  const float pc = s0[rb_sp(h0, j0, h, j)];
-  const float axm = s0[OFF_X + rb_sc(h0, j0, i, j)], axp = s0[OFF_X + rb_sc(h0, j0, i + 1, j)];
-  const float aym = s0[OFF_Y + rb_sc(h0, j0, i, j)], ayp = s0[OFF_Y + rb_sc(h0, j0, i, j + 1)];
-  const float azm = s0[OFF_Z + rb_sc(h0, j0, i, j)], azp = sp[OFF_Z + rb_sc(h0, j0, i, j)];
-  const float txm = t0[ty * TW + tx + pb - 1], txp = t0[ty * TW + tx + pb];
-  const float tym = t0[(ty - 1) * TW + tx], typ = t0[(ty + 1) * TW + tx];
-  const float tzm = tm[ty * TW + tx], tzp = tp[ty * TW + tx];
-  const int o = i > 0 ? pb - 1 : 0;
-  const float dxm = i > 1 ? pc - s0[rb_sp(h0, j0, h - 1, j)] : 0.0f;
-  const float dym = pc - s0[rb_sp(h0, j0, h + o, j - 1)], dyp = pc - s0[rb_sp(h0, j0, h + o, j + 1)];
-  const float dzm = pc - sm[rb_sp(h0, j0, h + o, j)], dzp = pc - sp[rb_sp(h0, j0, h + o, j)];
-  float acc = axm * (dxm - txm) + axp * (0.0f - txp);
-  acc += aym * (dym - tym) + ayp * (dyp - typ);
-  acc += azm * (dzm - tzm) + azp * (dzp - tzp);
-  *pc_out = pc;
-  return acc;
+__global__ void __launch_bounds__(32 * kRbBY) k_rb_red(RbOp A, const float* __restrict__ p, float* __restrict__ tau,
+                                                      const PcgState* st) {
+  if (((volatile const PcgState*)st)->done) return;
+  const int h = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * kRbBY + threadIdx.y, k = blockIdx.z;
+  if (h >= A.Lh.nx || j >= A.Lh.ny) return;
+  tau[A.Lh.at(h, j, k)] = rb_tau(A, p, h, j, k);
 }
 
-namespace {
-
-__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-template <int DIST>
-__global__ void __launch_bounds__(rbp::TX * rbp::TY) k_rb_spmv_pipe(RbOp A, const float* __restrict__ p,
-                                                                    float* __restrict__ q, PcgState* st,
-                                                                    double* partials, int kchunk) {
-  using namespace rbp;
-  constexpr int NS = 4 + DIST;
+__global__ void __launch_bounds__(32 * kRbBY) k_rb_black(RbOp A, const float* __restrict__ p,
+                                                        const float* __restrict__ tau, float* __restrict__ q,
+                                                        PcgState* st, double* partials, int kchunk) {
   if (((volatile PcgState*)st)->done) return;
-  extern __shared__ float4 stage_mem[];
-  float* stages = reinterpret_cast<float*>(stage_mem);
-  __shared__ float ring[3 * TW * TH];
+  const Lay& L = A.L;
   const Lay& H = A.Lh;
-  const int h0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  const int k0 = blockIdx.z * kchunk, k1 = min(H.nz, k0 + kchunk);
-  const int tid = threadIdx.x + TX * threadIdx.y;
-  const float e0 = (float)(*A.extra0);
-  auto stage = [&](int kk) { return stages + ((kk % NS + NS) % NS) * STAGE; };
-  auto load = [&](int kk) {
-    if (kk <= k1 + 1) {
-      float* d = stage(kk);
-      for (int t = tid; t < CHUNKS; t += TX * TY) {
-        int off;
-        const float* s = rb_chunk_src(A, p, h0, j0, kk, t, &off);
-        if (s)
-          cp_async16(d + off, s);
-        else
-          *reinterpret_cast<float4*>(d + off) = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-    }
-    cp_async_commit();  // one group per plane, empty past the chunk
-  };
-  auto tau_plane = [&](int kk) {
-    float* dst = ring + ((kk % 3 + 3) % 3) * (TW * TH);
-    const float *sm = stage(kk - 1), *s0 = stage(kk), *sp = stage(kk + 1);
-    for (int t = tid; t < TW * TH; t += TX * TY) {
-      const int x = t % TW, y = t / TW;
-      dst[t] = rb_tau_s(A, sm, s0, sp, h0, j0, h0 - 1 + x, j0 - 1 + y, kk, e0);
-    }
-  };
-  for (int kk = k0 - 2; kk <= k0 + 1 + DIST; ++kk) load(kk);
-  cp_async_wait<DIST>();  // planes k0-2 .. k0+1 landed
-  __syncthreads();
-  tau_plane(k0 - 1);
-  tau_plane(k0);
-  const int h = h0 + threadIdx.x, j = j0 + threadIdx.y;
-  const bool own = h < H.nx && j < H.ny;
+  const int h = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * kRbBY + threadIdx.y;
   double pq = 0.0;
-  for (int k = k0; k < k1; ++k) {
-    cp_async_wait<DIST - 1>();  // plane k+2 landed
-    __syncthreads();            // every thread is past plane k-1: its stage slot and tau slot are free
-    load(k + 2 + DIST);
-    tau_plane(k + 1);
-    __syncthreads();
-    if (own) {
-      float pc;
-      const float qv = rb_q_s(A, stage(k - 1), stage(k), stage(k + 1), ring + ((k + 2) % 3) * (TW * TH),
-                              ring + (k % 3) * (TW * TH), ring + ((k + 1) % 3) * (TW * TH), h0, j0, h, j, k, &pc);
-      q[H.at(h, j, k)] = qv;
-      pq += (double)pc * (double)qv;
+  if (h < H.nx && j < H.ny) {
+    const int k0 = blockIdx.z * kchunk, k1 = min(H.nz, k0 + kchunk);
+    for (int k = k0; k < k1; ++k) {
+      const int pb = (j + k + 1) & 1;
+      const int i = 2 * h + pb;
+      const int64_t s = H.at(h, j, k);
+      float qv = 0.0f;
+      if (i < L.nx) {
+        const int64_t c = L.at(i, j, k);
+        const float pc = p[s];
+        const float axm = A.ax[c], axp = A.ax[c + 1];
+        const float aym = A.ay[c], ayp = A.ay[c + L.px];
+        const float azm = A.az[c], azp = A.az[c + L.slab];
+        // tau of the six red neighbours
+        const float txm = tau[s + pb - 1], txp = tau[s + pb];
+        const float tym = tau[s - H.px], typ = tau[s + H.px];
+        const float tzm = tau[s - H.slab], tzp = tau[s + H.slab];
+        // b0 of each red neighbour: its x-1 black neighbour (x+1 at i = 0).
+        // x-1 neighbour (at i-1): b0 is the black cell at i-2, or c itself when
+        // i-1 = 0; x+1 neighbour: b0 is c.  y/z neighbours (at i): b0 is the
+        // black cell at i-1 of their row (slot h + pb - 1), or at i+1 = 1
+        // (slot 0) when i = 0.
+        const int o = i > 0 ? pb - 1 : 0;
+        const float dxm = i > 1 ? pc - p[s - 1] : 0.0f;
+        const float dym = pc - p[s - H.px + o], dyp = pc - p[s + H.px + o];
+        const float dzm = pc - p[s - H.slab + o], dzp = pc - p[s + H.slab + o];
+        float acc = axm * (dxm - txm) + axp * (0.0f - txp);
+        acc += aym * (dym - tym) + ayp * (dyp - typ);
+        acc += azm * (dzm - tzm) + azp * (dzp - tzp);
+        qv = acc;
+        pq += (double)pc * (double)qv;
+      }
+      q[s] = qv;
     }
   }
   pq = block_sum(pq);
@@ -265,8 +162,6 @@ __global__ void __launch_bounds__(rbp::TX * rbp::TY) k_rb_spmv_pipe(RbOp A, cons
     }
   }
 }
-
-}  // namespace
 
 // The FP64 pressure from the packed black iterate: black cells copied, red
 // cells eliminated exactly with the FP64 operator evaluated from phi (the
@@ -371,47 +266,24 @@ const dim3 kRbBlock(32, 4, 2);
 }  // namespace
 
 
-// Launch shape of the pipelined SpMV: xy tiles times as many z chunks as
-// fill one wave of resident blocks (a chunk costs 4 + DIST plane copies of
-// prologue, so fewer and longer chunks are cheaper once the wave is full).
-constexpr int kRbDist = 2;
-struct RbLaunch {
-  dim3 grid;
-  int kchunk;
-};
-static int g_rb_resident = 0;  // resident blocks of the SpMV on this device (one wave)
+// Launch shape of the black pass: xy tiles times z chunks of kRbChunk
+// planes (the red pass runs one block per tile and plane).
+constexpr int kRbChunk = 16;
 
-void rb_prepare() {
-  if (g_rb_resident > 0) return;
-  cudaFuncSetAttribute(k_rb_spmv_pipe<kRbDist>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)rbp::smem_bytes(kRbDist));
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rb_spmv_pipe<kRbDist>, rbp::TX * rbp::TY,
-                                                rbp::smem_bytes(kRbDist));
-  g_rb_resident = std::max(1, per_sm) * std::max(1, sms);
-}
-
-RbLaunch rb_launch(const Lay& H) {
-  const int tx = (H.nx + rbp::TX - 1) / rbp::TX, ty = (H.ny + rbp::TY - 1) / rbp::TY;
-  const int resident = g_rb_resident > 0 ? g_rb_resident : 148;
-  const int chunks = std::max(1, std::min(H.nz, resident / std::max(1, tx * ty)));
-  const int kchunk = (H.nz + chunks - 1) / chunks;
-  return {dim3(tx, ty, (H.nz + kchunk - 1) / kchunk), kchunk};
+dim3 rb_red_grid(const Lay& H) { return dim3((H.nx + 31) / 32, (H.ny + kRbBY - 1) / kRbBY, H.nz); }
+dim3 rb_black_grid(const Lay& H) {
+  return dim3((H.nx + 31) / 32, (H.ny + kRbBY - 1) / kRbBY, (H.nz + kRbChunk - 1) / kRbChunk);
 }
 
 int rb_blocks(const Lay& H) {
-  rb_prepare();
-  const RbLaunch g = rb_launch(H);
-  return std::max((int)(g.grid.x * g.grid.y * g.grid.z), reduction_blocks((int64_t)H.nx * H.ny * H.nz));
+  const dim3 g = rb_black_grid(H);
+  return std::max((int)(g.x * g.y * g.z), reduction_blocks((int64_t)H.nx * H.ny * H.nz));
 }
 
-void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, PcgState* st,
-                  double* partials, cudaStream_t s) {
-  const RbLaunch g = rb_launch(A.Lh);
-  k_rb_spmv_pipe<kRbDist><<<g.grid, dim3(rbp::TX, rbp::TY, 1), rbp::smem_bytes(kRbDist), s>>>(A, ph, qh, st,
-                                                                                              partials, g.kchunk);
+void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
+                  PcgState* st, double* partials, cudaStream_t s) {
+  k_rb_red<<<rb_red_grid(A.Lh), dim3(32, kRbBY, 1), 0, s>>>(A, ph, tau, st);
+  k_rb_black<<<rb_black_grid(A.Lh), dim3(32, kRbBY, 1), 0, s>>>(A, ph, tau, qh, st, partials, kRbChunk);
   cg_vector_updates<float, double>(Ah, xh, rh, ph, qh, st, partials, s);
 }
 

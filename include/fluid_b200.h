@@ -46,7 +46,7 @@ typedef enum {
   FS_FIELD_W = 3,         /* z-velocity, z faces */
   FS_FIELD_PRESSURE = 4,  /* pressure of the last projection, cells */
   FS_FIELD_DIVERGENCE = 5, /* divergence/dt of the last projection's input, cells (download only) */
-  FS_FIELD_ADJ_PHI = 6,   /* adjoint (bar) of phi, cells: FP64 contexts, see the adjoint entry points */
+  FS_FIELD_ADJ_PHI = 6,   /* adjoint (bar) of phi, cells (FP64 in every context), see the adjoint entry points */
   FS_FIELD_ADJ_U = 7,     /* adjoint of u, x faces */
   FS_FIELD_ADJ_V = 8,     /* adjoint of v, y faces */
   FS_FIELD_ADJ_W = 9,     /* adjoint of w, z faces */
@@ -269,9 +269,16 @@ fs_status fs_read_state(fs_ctx* ctx, const char* path);
  * values; the pressure and viscosity solves are differentiated as exact
  * solves (a second solve with the same symmetric operator).  dt is a
  * constant (not differentiated through the CFL condition).
- * FP64 contexts with the corrected projection only (FS_NOT_SUPPORTED
- * otherwise).  The first call allocates the adjoint buffers; fs_step_adjoint
- * also allocates its tape (about 30 + 3*reinit_iterations fields). */
+ * FP64 and FP32_REFINE contexts: the forward states and the tape are kept in
+ * the context's storage precision, every bar, derivative and sum is FP64,
+ * and the transposed pressure solve uses the context's own solver (FP64
+ * PCG, or the FP32 solve with FP64 defect correction).  The corrected
+ * projection, WENO5 velocity advection, the semi-implicit or no viscosity,
+ * no surface tension and Sussman reinitialisation only (FS_NOT_SUPPORTED
+ * otherwise).  A transposed solve that stops before its tolerance leaves
+ * inexact bars and the call returns FS_NOT_CONVERGED after completing.
+ * The first call allocates the adjoint buffers; fs_step_adjoint also
+ * allocates its tape (about 30 + 3*reinit_iterations fields). */
 fs_status fs_adjoint_reset(fs_ctx* ctx);
 fs_status fs_adjoint_density_bars(fs_ctx* ctx, double* rho_neg_bar, double* rho_pos_bar);
 /* Whole step: ADJ_* = bars of the step's output -> bars of its input.  The
