@@ -164,8 +164,8 @@ __device__ __forceinline__ int num_blocks() { return gridDim.x * gridDim.y * gri
 __device__ __forceinline__ bool thread0() { return threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0; }
 
 // Deterministic grid-wide reduction: every block writes its partial, the last
-// block to finish (counted with an atomic ticket) sums the partials in block
-// order and resets the ticket.  Returns true in the one thread that holds
+// block to finish (counted with an atomic ticket) sums the partials in a
+// fixed order and resets the ticket.  Returns true in the one thread that holds
 // the final value in *out_total (thread 0 of the last block).
 __device__ __forceinline__ bool grid_reduce_sum(double block_value, double* partials, unsigned int* ticket,
                                                 double* out_total) {
@@ -183,7 +183,12 @@ __device__ __forceinline__ bool grid_reduce_sum(double block_value, double* part
   const int nt = blockDim.x * blockDim.y * blockDim.z;
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   double s = 0.0;
-  for (int q = tid; q < num_blocks(); q += nt) s += ((volatile double*)partials)[q];
+  // L2 loads (.cg: the partials of this launch, not stale L1 lines of an
+  // earlier one), not volatile, so that the loop's loads are in flight
+  // together; the additions keep their order, so the sum is deterministic
+  const int nbk = num_blocks();
+#pragma unroll 8
+  for (int q = tid; q < nbk; q += nt) s += __ldcg(partials + q);
   s = block_sum(s);
   if (tid == 0) {
     *out_total = s;

@@ -1168,7 +1168,17 @@ fs_status adj_viscosity(fs_ctx* c, void* phi, void* const ug[3], void* const x[3
   cudaStream_t s = c->stream;
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   CKS(zero_faces(c, in_bar));
+  const bool shared = c->a_vs[1][0] == c->a_vs[0][0];
   for (int a = 0; a < 3; ++a) {
+    if (shared) {
+      // FP32 contexts share one FP64 system for the three components, whose
+      // face layouts differ: clear it, so that the ghost entries the
+      // matrix-free CG reads (couplings and vector values beyond the
+      // component's interior) are zero again and not the previous
+      // component's interior values
+      const size_t fmax = std::max(c->Lu.total, std::max(c->Lv.total, c->Lw.total)) * sizeof(double);
+      for (int m = 0; m < 9; ++m) CK(cudaMemsetAsync(c->a_vs[a][m], 0, fmax, s));
+    }
     viscosity_system<S, double>(F<S>(phi), F<S>(ug[0]), F<S>(ug[1]), F<S>(ug[2]), c->Lc, c->Lu, c->Lv, c->Lw, a, dx,
                                 dt, P.rho_neg, P.rho_pos, P.mu_neg, P.mu_pos, c->a_vs[a][0], c->a_vs[a][1],
                                 c->a_vs[a][2], c->a_vs[a][3], c->a_vs[a][4], s);

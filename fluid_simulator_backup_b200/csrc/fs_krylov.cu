@@ -109,7 +109,8 @@ __device__ __forceinline__ bool grid_reduce3(double a, double b, double c, doubl
   __threadfence();
   for (int m = 0; m < 3; ++m) {
     double s = 0.0;
-    for (int q = threadIdx.x; q < nb; q += blockDim.x) s += ((volatile double*)partials)[m * nb + q];
+#pragma unroll 8
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) s += __ldcg(partials + m * nb + q);  // as in grid_reduce_sum
     s = block_sum(s);
     if (threadIdx.x == 0) tot[m] = s;
     __syncthreads();
