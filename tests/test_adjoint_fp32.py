@@ -107,7 +107,7 @@ def test_differentiable_dam_break_96_32_steps():
     y = (np.arange(n) + 0.5) / n
     target = np.broadcast_to(y[None, :, None] - 0.3, (n, n, n)).copy()
     grads = {}
-    for precision, tol in ((fs.FS_PRECISION_FP32_REFINE, 1e-9), (fs.FS_PRECISION_FP64, 1e-11)):
+    for precision, tol in ((fs.FS_PRECISION_FP32_REFINE, 1e-11), (fs.FS_PRECISION_FP64, 1e-11)):
         with fs.Solver(n, dx, **params(precision, tol)) as s:
             ts = {k: torch.tensor(X[k], requires_grad=True) for k in KEYS}
             rho = torch.tensor(1000.0, dtype=torch.float64, requires_grad=True)
