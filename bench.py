@@ -61,7 +61,7 @@ def scene(n):
 PRECONDITIONER = {"default": 0, "jacobi": 1, "bf16": 2, "red_black": 3, "red_black_jacobi": 4}
 PRECOND_CHOICE = "default"
 # what FS_PRECOND_DEFAULT selects in an FP32_REFINE context
-DEFAULT_FP32_PRECONDITIONER = "bf16"
+DEFAULT_FP32_PRECONDITIONER = "red_black"
 
 
 def effective_preconditioner(fs):

@@ -262,9 +262,12 @@ void apply_params(fs_ctx* c) {
   c->reliable_delta = p.reliable_delta > 0.0 ? p.reliable_delta : 0.1;
   c->flux32 = p.flux_arithmetic;
   c->lean = p.pressure_preconditioner != FS_PRECOND_JACOBI;
-  c->red_black = c->fp32 && (p.pressure_preconditioner == FS_PRECOND_RED_BLACK ||
+  // FP32_REFINE: the default is red-black IC(0), which halves the
+  // iterations of the Jacobi-PCG (FP64 keeps the reference's Jacobi)
+  c->red_black = c->fp32 && (p.pressure_preconditioner == FS_PRECOND_DEFAULT ||
+                              p.pressure_preconditioner == FS_PRECOND_RED_BLACK ||
                               p.pressure_preconditioner == FS_PRECOND_RED_BLACK_JACOBI);
-  c->rb_ic0 = p.pressure_preconditioner == FS_PRECOND_RED_BLACK;
+  c->rb_ic0 = p.pressure_preconditioner != FS_PRECOND_RED_BLACK_JACOBI;
 }
 
 // The pressure system keeps the reference's deflation of the first cell only

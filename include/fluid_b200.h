@@ -65,7 +65,7 @@ typedef enum {
 
 /* Preconditioner of the pressure solve. */
 typedef enum {
-  FS_PRECOND_DEFAULT = 0,     /* FP64: Jacobi (the reference's, PCG_METHOD.cpp:128-160); FP32_REFINE: bf16 Jacobi */
+  FS_PRECOND_DEFAULT = 0,     /* FP64: Jacobi (the reference's, PCG_METHOD.cpp:128-160); FP32_REFINE: red-black IC(0) */
   FS_PRECOND_JACOBI = 1,      /* z = r / diag in the solve precision */
   FS_PRECOND_JACOBI_BF16 = 2, /* FP32_REFINE: z = r * (1/diag rounded to bf16), 2 bytes per unknown */
   FS_PRECOND_RED_BLACK = 3,   /* FP32_REFINE: IC(0) in red-black order, i.e. the reference's commented-out
