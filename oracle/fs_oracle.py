@@ -1444,3 +1444,185 @@ def marching_cubes(phi, dx, table=None):
         ln = np.linalg.norm(normals, axis=1)
         normals = np.where(ln[:, None] > 0, normals / np.where(ln > 0, ln, 1.0)[:, None], 0.0)
     return verts, normals, tris + 1
+
+
+# ----------------------------------------------------------------------------
+# Oil/water pipe mode, vertical pipe (axis y): the level-set path and the
+# dimensionless forcing (ADVECTION_3D.h:204-242, 360-378, 380-430;
+# ADVECTION_METHOD_3D.h:281-523; FIELD_STRUCTURE_3D.h:1328-1431;
+# EULERIAN_FLUID_SOLVER_3D.h:496-514, 2198-2225, 2237-2330)
+# ----------------------------------------------------------------------------
+
+def pipe_grids(n, lo, hi):
+    """The reference's cell grid and the three MAC face grids
+    (GRID_STRUCTURE_3D.h:91-137, EULERIAN_FLUID_SOLVER_3D.h:405-427): per
+    grid (x_min, y_min, z_min, dx, dy, dz).  Positions are x_min + i*dx (the
+    reference's node convention), each face grid spans half a cell beyond the
+    cell grid on its own axis, and every spacing is (max - min)/(res - 1)."""
+    nx, ny, nz = n
+    (x0, y0, z0), (x1, y1, z1) = lo, hi
+    d = ((x1 - x0) / (nx - 1), (y1 - y0) / (ny - 1), (z1 - z0) / (nz - 1))
+    cells = (x0, y0, z0) + d
+    grids = [cells]
+    res = (nx, ny, nz)
+    for axis in range(3):
+        mn, mx, r = [x0, y0, z0], [x1, y1, z1], list(res)
+        mn[axis] = mn[axis] - 0.5 * d[axis]
+        mx[axis] = mx[axis] + 0.5 * d[axis]
+        r[axis] += 1
+        grids.append(tuple(mn) + tuple((mx[q] - mn[q]) / (r[q] - 1) for q in range(3)))
+    return grids
+
+
+def pipe_constants(a, R2, m, eta, K, g, water_density, oil_density, water_viscosity, oil_viscosity,
+                   surface_tension):
+    """The dimensionless constants of the core-annular pipe flow the reference
+    derives from its script (EULERIAN_FLUID_SOLVER_3D.h:496-514)."""
+    R1 = R2 / a
+    f = 1.0 / (K - 1.0) * g * (oil_density - K * water_density)
+    A = (a * a - 1.0) + (m * K + 2.0 * (K - 1) * math.log(a))
+    V0 = (f + water_density * g) * (R1 * R1) / (4.0 * water_viscosity) * A
+    J = surface_tension * R1 * oil_density / (oil_viscosity * oil_viscosity)
+    Re = (oil_density * R1 * abs(V0)) / oil_viscosity
+    We = (1.0 / J) * (Re * Re)
+    return dict(a=a, R1=R1, m=m, eta=eta, K=K, g=g, f=f, A=A, V0=V0, J=J, Re=Re, We=We)
+
+
+def pipe_boundary(grid, shape, a):
+    """Distance to the pipe wall, sqrt(x^2 + z^2) - a, at the points of one
+    grid (vertical pipe; EULERIAN_FLUID_SOLVER_3D.h:2282-2300)."""
+    x0, _, z0, dx, _, dz = grid
+    nz, ny, nx = shape
+    x = x0 + np.arange(nx) * dx
+    z = z0 + np.arange(nz) * dz
+    r = np.sqrt(x[None, :] * x[None, :] + z[:, None] * z[:, None]) - a
+    return np.broadcast_to(r[:, None, :], shape).copy()
+
+
+def periodic_ghosts_y(phi, g=G):
+    """Ghosted copy of a cell field, periodic along y with the reference's
+    node convention (FIELD_STRUCTURE_3D.h:1328-1431): the first and last
+    cells are the same point, so ghost j0 - m is cell j1 - m and ghost j1 + m
+    is cell j0 + m.  Only the y ghosts of interior columns are written: the x
+    and z ghost layers of the reference's ghost copy are never filled in a
+    vertical pipe and hold zero."""
+    nz, ny, nx = phi.shape
+    a = np.zeros((nz + 2 * g, ny + 2 * g, nx + 2 * g))
+    a[g:g + nz, g:g + ny, g:g + nx] = phi
+    for m in range(1, g + 1):
+        a[g:g + nz, g - m, g:g + nx] = phi[:, ny - 1 - m, :]
+        a[g:g + nz, g + ny - 1 + m, g:g + nx] = phi[:, m, :]
+    return a
+
+
+def _wall_extrapolate(vel_ghost, b, along):
+    """Velocity ghost values on faces outside the pipe next to faces inside
+    it (ADVECTION_3D.h:445-485): zero where all four transverse neighbours are
+    outside, else (theta-1)/theta times the inside neighbour along `along`
+    (numpy axis), theta = |b_in|/(|b_in| + |b_out|); the + side wins when both
+    sides are inside.  b outside the face grid counts as 0 (neither side)."""
+    out = vel_ghost.copy()
+    bp = np.pad(b, 1)  # the unfilled ghost layer of the boundary array holds 0
+    c = (slice(1, -1),) * 3
+
+    def nb(ax, s):
+        sl = list(c)
+        sl[ax] = slice(1 + s, bp.shape[ax] - 1 + s)
+        return bp[tuple(sl)]
+
+    vp = np.pad(vel_ghost, 1)
+
+    def vnb(ax, s):
+        sl = list(c)
+        sl[ax] = slice(1 + s, vp.shape[ax] - 1 + s)
+        return vp[tuple(sl)]
+
+    outside = b > 0
+    all4 = (nb(2, -1) > 0) & (nb(2, 1) > 0) & (nb(0, -1) > 0) & (nb(0, 1) > 0)
+    out = np.where(outside & all4, 0.0, out)
+    for s in (-1, 1):
+        bn = nb(along, s)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            theta = np.abs(bn) / (np.abs(bn) + np.abs(b))
+            ext = (theta - 1) / theta * vnb(along, s)
+        out = np.where(outside & (bn < 0), ext, out)
+    return out
+
+
+def pipe_levelset_velocities(u, v, w, grids, a):
+    """SetupBoundaryConditionForVelocity for the level-set advection of a
+    vertical pipe (ADVECTION_3D.h:380-490): the face velocities outside the
+    pipe become 0 in u and w (v is left alone); the ghost copies the WENO5
+    update reads hold the velocities inside the pipe (FIELD_STRUCTURE_3D.h:
+    1432-1460, 0 outside) and, on x and z faces just outside it, the
+    extrapolation across the wall.  Returns (u, v, w, ug, vg, wg)."""
+    bx = pipe_boundary(grids[1], u.shape, a)
+    by = pipe_boundary(grids[2], v.shape, a)
+    bz = pipe_boundary(grids[3], w.shape, a)
+    ug = np.where(bx < 1e-8, u, 0.0)
+    vg = np.where(by < 1e-8, v, 0.0)
+    wg = np.where(bz < 1e-8, w, 0.0)
+    # the y component's periodic fill also rewrites its first and last face
+    # rows (face 0 is face ny-1, face ny is face 1: FIELD_STRUCTURE_3D.h:
+    # 1466-1500), where the face is inside
+    ny = v.shape[1] - 1
+    vg[:, 0, :] = np.where(by[:, 0, :] < 1e-8, v[:, ny - 1, :], vg[:, 0, :])
+    vg[:, ny, :] = np.where(by[:, ny, :] < 1e-8, v[:, 1, :], vg[:, ny, :])
+    ug = _wall_extrapolate(ug, bx, 2)
+    wg = _wall_extrapolate(wg, bz, 0)
+    return np.where(bx > 0, 0.0, u), v.copy(), np.where(bz > 0, 0.0, w), ug, vg, wg
+
+
+def pipe_weno5_levelset(phi, u, v, w, grids, a, dt, eps):
+    """ADVECTION_3D::Solve_Levelset of a vertical pipe: the velocity set-up
+    above, then WENO5th with the boundary level set (ADVECTION_METHOD_3D.h:
+    281-523): cells outside the pipe keep their value, the rest take the
+    WENO5 upwind update on the periodic ghost copy, with the per-axis
+    spacings of the cell grid.  Returns (phi, u, v, w)."""
+    u2, v2, w2, ug, vg, wg = pipe_levelset_velocities(u, v, w, grids, a)
+    cg = grids[0]
+    pg = periodic_ghosts_y(phi)
+    dxm, dxp = weno5_derivatives(pg, 0, 1.0 / cg[3], eps)
+    dym, dyp = weno5_derivatives(pg, 1, 1.0 / cg[4], eps)
+    dzm, dzp = weno5_derivatives(pg, 2, 1.0 / cg[5], eps)
+    uc = (ug[:, :, 1:] + ug[:, :, :-1]) * 0.5
+    vc = (vg[:, 1:, :] + vg[:, :-1, :]) * 0.5
+    wc = (wg[1:, :, :] + wg[:-1, :, :]) * 0.5
+    new = _upwind_update(phi, dt, uc, vc, wc, dxm, dxp, dym, dyp, dzm, dzp)
+    bl = pipe_boundary(cg, phi.shape, a)
+    return np.where(bl > 0, phi, new), u2, v2, w2
+
+
+def pipe_reinitialization(phi, grids, iterations, scaling, eps, typo=True):
+    """EULERIAN_FLUID_SOLVER_3D::Reinitialization of a pipe: S from the
+    block's input, then `iterations` Sussman pseudo-steps of dx/scaling, each
+    reading the periodic ghost copy (ADVECTION_3D.h:360-378).  The reference
+    runs its tree with the two typo leaves (typo=True)."""
+    dx = grids[0][3]
+    s = sign_function(phi, dx)
+    dtau = dx / scaling
+    for _ in range(iterations):
+        phi = sussman_step(phi, s, dx, dtau, eps, typo, ghost_source=periodic_ghosts_y(phi))
+    return phi
+
+
+def pipe_forcing(phi, v, grids, C, gravity_y, oil_density, dt, fixed_v=None):
+    """The dimensionless body force of a vertical pipe (ApplyGravity,
+    EULERIAN_FLUID_SOLVER_3D.h:2304-2326): on y faces inside the pipe that are
+    not fixed, v += R1/V0^2 (dt g_y + dt f/(rho_oil rho_f)), rho_f = 1 +
+    (eta - 1) H(phi_f) the smeared density of the face's level set
+    phi_f = (phi_c + phi_below)/2 from the periodic ghost copy, H with
+    epsilon = 1.5 dy."""
+    cg, vgrid = grids[0], grids[2]
+    pg = periodic_ghosts_y(phi)
+    nz, ny, nx = phi.shape
+    col = pg[G:G + nz, :, G:G + nx]
+    phi_f = 0.5 * (col[:, G:G + ny + 1, :] + col[:, G - 1:G + ny, :])
+    h = heaviside_projection(phi_f, 1.5 * cg[4])
+    rho_f = 1.0 + (C["eta"] - 1.0) * h
+    by = pipe_boundary(vgrid, v.shape, C["a"])
+    add = C["R1"] / (C["V0"] * C["V0"]) * (dt * gravity_y + 1.0 / (oil_density * rho_f) * (dt * C["f"]))
+    mask = by < 0
+    if fixed_v is not None:
+        mask &= ~fixed_v
+    return np.where(mask, v + add, v)

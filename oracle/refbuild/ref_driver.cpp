@@ -82,6 +82,15 @@ extern "C" {
 void* fsref_create(const char* sim_path) {
   RefCase* c = new RefCase;
   c->world.InitializeFormScript(sim_path);
+  // ADVECTION_3D's constructor leaves its two boundary-mode flags
+  // uninitialised (ADVECTION_3D.h:72-73, 87-97), and the first level-set
+  // advection of a pipe run reads velocity_advection before any velocity
+  // advection has set it; both start false here, the value they hold after
+  // the first velocity advection of a run.  The flags matter in pipe mode only.
+  if (ADVECTION_3D* adv = c->world.eulerian_solver.advecting_field_variables) {
+    adv->levelset_advection = false;
+    adv->velocity_advection = false;
+  }
   return c;
 }
 
@@ -417,6 +426,95 @@ void fsref_set_pressure_tolerance(void* h, double tol) {
 void fsref_write_levelset(void* h, const char* path) {
   EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
   s.water_levelset->Write(path);
+}
+
+// ---- oil/water pipe mode (oil_water_simulation = true)
+
+// The constants the reference derives from its pipe script
+// (EULERIAN_FLUID_SOLVER_3D.h:496-514) and the cell grid:
+// out = a, R1, m, eta, K, g, f, A, V0, J, Re, We, water_density, oil_density,
+// water_viscosity, oil_viscosity, surface_tension, is_vertical, is_parallel,
+// x_min, y_min, z_min, dx, dy, dz.
+void fsref_pipe_params(void* h, double* out) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  const GRID_STRUCTURE_3D& g = s.base_grid;
+  const double v[] = {s.a, s.R1, s.m, s.eta, s.K, s.g, s.f, s.A, s.V0, s.J, s.Re, s.We, s.water_density,
+                      s.oil_density, s.water_viscosity, s.oil_viscosity, s.surface_tension,
+                      (double)s.is_vertical, (double)s.is_parallel, g.x_min, g.y_min, g.z_min, g.dx, g.dy, g.dz};
+  for (size_t q = 0; q < sizeof(v) / sizeof(v[0]); ++q) out[q] = v[q];
+}
+
+// The cell-centred boundary level set (interior cells).
+void fsref_boundary_levelset(void* h, double* dst) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  for_interior(s.boundary_levelset->signed_distance_field, [&](T& v, long n) { dst[n] = v; });
+}
+
+// A ghosted copy used by the operators, with its three ghost layers:
+// 0 the level-set ghost copy, 1-3 the MAC velocity ghost copies.
+// Layout (extent + 6) per axis, x fastest.
+void fsref_ghost_copy(void* h, int id, double* dst) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  FIELD_STRUCTURE_3D<T>* f[] = {&s.scalar_field_ghost, &s.vector_field_mac_ghost_x, &s.vector_field_mac_ghost_y,
+                                &s.vector_field_mac_ghost_z};
+  FIELD_STRUCTURE_3D<T>& a = *f[id];
+  const GRID_STRUCTURE_3D& g = a.grid;
+  long idx = 0;
+  for (int k = g.k_start - 3; k <= g.k_end + 3; ++k)
+    for (int j = g.j_start - 3; j <= g.j_end + 3; ++j)
+      for (int i = g.i_start - 3; i <= g.i_end + 3; ++i) dst[idx++] = a.array_for_this(i, j, k);
+}
+
+// The pipe's boundary level set on the faces of one component, as the
+// advection's velocity set-up last computed it (ADVECTION_3D.h:380-430).
+void fsref_boundary_faces(void* h, int comp, double* dst) {
+  ADVECTION_3D& adv = *static_cast<RefCase*>(h)->world.eulerian_solver.advecting_field_variables;
+  FIELD_STRUCTURE_3D<T>* f[] = {&adv.boundary_phi_x, &adv.boundary_phi_y, &adv.boundary_phi_z};
+  for_interior(*f[comp], [&](T& v, long n) { dst[n] = v; });
+}
+
+// The fixed flags of a velocity component (1: the face keeps its value).
+void fsref_fixed(void* h, int comp, unsigned char* dst) {
+  EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;
+  FIELD_STRUCTURE_3D<T>* f[] = {s.water_velocity_field_mac_x, s.water_velocity_field_mac_y,
+                                s.water_velocity_field_mac_z};
+  FIELD_STRUCTURE_3D<T>& a = *f[comp];
+  const GRID_STRUCTURE_3D& g = a.grid;
+  long idx = 0;
+  for (int k = g.k_start; k <= g.k_end; ++k)
+    for (int j = g.j_start; j <= g.j_end; ++j)
+      for (int i = g.i_start; i <= g.i_end; ++i) dst[idx++] = a.fixed(i, j, k) ? 1 : 0;
+}
+
+// ADVECTION_3D::Solve_Levelset in pipe mode (ADVECTION_3D.h:204-242): the
+// velocity boundary set-up of the cylinder, the periodic ghost copy of the
+// level set and the WENO5 update that skips cells outside the pipe.
+void fsref_pipe_levelset_advection(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  run_threads(c, [&](int t) { s.advecting_field_variables->Solve_Levelset(t, dt); });
+}
+
+// ADVECTION_3D::Solve_Velocity in pipe mode (ADVECTION_3D.h:244-358).
+void fsref_pipe_velocity_advection(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  run_threads(c, [&](int t) { s.advecting_field_variables->Solve_Velocity(t, dt); });
+}
+
+// EULERIAN_FLUID_SOLVER_3D::Reinitialization (EULERIAN_FLUID_SOLVER_3D.h:2198-2225).
+void fsref_pipe_reinitialization(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  run_threads(c, [&](int t) { s.Reinitialization(t, dt); });
+}
+
+// EULERIAN_FLUID_SOLVER_3D::ApplyGravity, the dimensionless forcing of the
+// pipe (EULERIAN_FLUID_SOLVER_3D.h:2237-2432).
+void fsref_pipe_gravity(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  run_threads(c, [&](int t) { s.ApplyGravity(t, dt); });
 }
 
 }  // extern "C"

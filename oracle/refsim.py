@@ -73,6 +73,15 @@ def _lib():
     lib.fsref_set_pressure_tolerance.argtypes = [ctypes.c_void_p, ctypes.c_double]
     lib.fsref_linear_solve.restype = ctypes.c_int
     lib.fsref_linear_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _dp, _dp]
+    if hasattr(lib, "fsref_pipe_params"):
+        lib.fsref_pipe_params.argtypes = [ctypes.c_void_p, _dp]
+        lib.fsref_boundary_levelset.argtypes = [ctypes.c_void_p, _dp]
+        lib.fsref_ghost_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        lib.fsref_boundary_faces.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        lib.fsref_fixed.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_ubyte)]
+        for fn in ("fsref_pipe_levelset_advection", "fsref_pipe_velocity_advection", "fsref_pipe_reinitialization",
+                   "fsref_pipe_gravity"):
+            getattr(lib, fn).argtypes = [ctypes.c_void_p, ctypes.c_double]
     return lib
 
 
@@ -194,6 +203,156 @@ FLUID_SOLVER_UNIFORM_AIR_WATER
     with open(path, "w") as f:
         f.write(text)
     return path
+
+
+def write_pipe_sim(path, res, grid_min, grid_max, *, vertical=True, threads=1, a=1.61, R2=0.47625, A_0=0.1,
+                   alpha=2.4, m=0.00166, eta=1.1, K=-2.03030303, g=-980.0, water_density=0.995, oil_density=0.905,
+                   water_viscosity=0.01, oil_viscosity=6.01, surface_tension=8.54, gravity=(0.0, -980.0, 0.0),
+                   order=2, tolerance=1e-6, max_iteration=10000, reinit_iterations=10, reinit_scaling=2,
+                   epsilon=1e-6, periodic_num=5, cfl=0.8):
+    """Write an oil/water pipe scenario in the reference's .sim syntax, with
+    the keys of the reference's own pipe scripts (3D_script_1.sim):
+    SIMULATION_WORLD (a, R2, A_0, alpha; SIMULATION_WORLD.h:120-129),
+    WORLD_DISCRETIZATION_OIL_WATER with PIPE_OPTIONS and the vertical or
+    parallel grid (WORLD_DISCRETIZATION_3D.h:91-107),
+    FLUID_SOLVER_UNIFORM_OIL_WATER (dimensionless form, m, eta, K, g;
+    EULERIAN_FLUID_SOLVER_3D.h:192-560) and an OBJECT_LIST whose WATER object
+    makes the reference seed the core-annular level set and the cylinder's
+    boundary level set (SIMULATION_WORLD.cpp:130-300)."""
+    b = lambda v: "true" if v else "false"
+    r = lambda x: np.format_float_positional(float(x), unique=True, trim="-")
+    v3 = lambda t: f"({r(t[0])}, {r(t[1])}, {r(t[2])})"
+    grid = f"""
+		{{
+			resolution_scale = 1
+			start_indices = (0,0,0)
+			base_grid_resolution = ({res[0]}, {res[1]}, {res[2]})
+			base_grid_min = {v3(grid_min)}
+			base_grid_max = {v3(grid_max)}
+		}}"""
+    text = f"""SIMULATION_WORLD
+{{
+	dt = 0.00001
+	max_dt = 1000000
+	num_substeps = 1
+	CFL = {r(cfl)}
+	frame_rate = 30
+	use_eulerian_solver = true
+	use_sph_solver = false
+	use_solid_solver = false
+	use_sph_levelset = false
+	number_of_threads = {threads}
+	use_field_boundary = false
+	last_frame = 100000
+	auto_run = false
+	air_water_simulation = false
+	oil_water_simulation = true
+	a = {r(a)}
+	R2 = {r(R2)}
+	A_0 = {r(A_0)}
+	alpha = {r(alpha)}
+	WORLD_DISCRETIZATION_OIL_WATER
+	{{
+		PIPE_OPTIONS
+		{{
+			is_vertical = {b(vertical)}
+			is_parallel = {b(not vertical)}
+		}}
+		GRID_STRUCTURE_3D_VERTICAL{grid}
+		GRID_STRUCTURE_3D_PARALLEL{grid}
+		padding_width = 2
+	}}
+	LOG
+	{{
+		max_log_level = 1
+		use_log_file = false
+		display_accum_time = false
+		use_log_screen = false
+		output_log_file_name = "log.txt"
+	}}
+}}
+
+FLUID_SOLVER_UNIFORM_OIL_WATER
+{{
+	use_water_solver = true
+	is_Levelset_advection_active = true
+	is_Velocity_advection_active = true
+	is_external_force_active = true
+	is_sourcing_active = true
+	is_projection_active = true
+	fastsweeping_reinitialization = false
+	sussmanstyle_reinitialization = true
+	scaling_number_for_reinitialization = {reinit_scaling}
+	iteration_number_for_reinitialization = {reinit_iterations}
+	use_delta_function_formulation = true
+	curvature_by_normal_vector = false
+	curvature_by_levelset = true
+	order_for_time_advancing = {order}
+	semi_implicit_approach = true
+	dimensionless_form = true
+	CSF_model = false
+	is_periodic = true
+	periodic_num = {periodic_num}
+	m = {r(m)}
+	eta = {r(eta)}
+	K = {r(K)}
+	g = {r(g)}
+	LEVELSET_ADVECTION
+	{{
+		use_csl = false
+		use_5th_weno = true
+		use_3rd_eno = false
+		epsilon = {r(epsilon)}
+	}}
+	VELOCITY_ADVECTION
+	{{
+		use_5th_weno_v = false
+		use_3rd_eno_v = true
+		epsilon = {r(epsilon)}
+	}}
+	PROJECTION_WATER
+	{{
+		tolerance = {r(tolerance)}
+		max_iteration = {max_iteration}
+		use_previous_pressure = true
+		poisson_solver_type = "PCG"
+		use_2nd_order = false
+		use_variable_density = true
+		Dirichlet_Boundary_Condition = false
+		Neumann_Boundary_Condition = true
+		regular_boundary = false
+		cylindrical_boundary = true
+	}}
+	ghost_width = 3
+	use_water_levelset = true
+	gravity = {v3(gravity)}
+	water_viscosity = {r(water_viscosity)}
+	water_density = {r(water_density)}
+	surface_tension = {r(surface_tension)}
+	oil_density = {r(oil_density)}
+	oil_viscosity = {r(oil_viscosity)}
+}}
+
+OBJECT_LIST
+{{
+	WATER
+	{{
+		object_type = "FLUID"
+		shape_type = "WATER"
+		use_sea_surface = false
+		use_sphere_bubble = false
+		user_defined = false
+	}}
+}}
+"""
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+PIPE_PARAMS = ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We", "water_density", "oil_density",
+               "water_viscosity", "oil_viscosity", "surface_tension", "is_vertical", "is_parallel", "x_min", "y_min",
+               "z_min", "dx", "dy", "dz")
 
 
 def _ptr(a, ct=ctypes.c_double):
@@ -360,3 +519,46 @@ class RefCase:
         it = self._quiet(self._lib.fsref_linear_solve, self.h, n, len(vals), _ptr(vals), _ptr(cols, ctypes.c_int),
                          _ptr(rowptr, ctypes.c_int), _ptr(b), _ptr(x))
         return x, it
+
+    # ---- oil/water pipe mode
+    def pipe_params(self):
+        out = np.zeros(len(PIPE_PARAMS))
+        self._lib.fsref_pipe_params(self.h, _ptr(out))
+        return dict(zip(PIPE_PARAMS, out.tolist()))
+
+    def boundary_levelset(self):
+        a = np.empty(self.shape("phi"))
+        self._lib.fsref_boundary_levelset(self.h, _ptr(a))
+        return a
+
+    def ghost_copy(self, name):
+        """The ghosted copy (three ghost layers) the operators read: "phi" or a
+        velocity component."""
+        sh = tuple(d + 6 for d in self.shape(name))
+        a = np.empty(sh)
+        self._lib.fsref_ghost_copy(self.h, {"phi": 0, "u": 1, "v": 2, "w": 3}[name], _ptr(a))
+        return a
+
+    def fixed(self, name):
+        a = np.empty(self.shape(name), dtype=np.uint8)
+        self._lib.fsref_fixed(self.h, {"u": 0, "v": 1, "w": 2}[name], _ptr(a, ctypes.c_ubyte))
+        return a.astype(bool)
+
+    def pipe_levelset_advection(self, dt):
+        self._quiet(self._lib.fsref_pipe_levelset_advection, self.h, dt)
+
+    def pipe_velocity_advection(self, dt):
+        self._quiet(self._lib.fsref_pipe_velocity_advection, self.h, dt)
+
+    def pipe_reinitialization(self, dt):
+        self._quiet(self._lib.fsref_pipe_reinitialization, self.h, dt)
+
+    def pipe_gravity(self, dt):
+        self._quiet(self._lib.fsref_pipe_gravity, self.h, dt)
+
+    def boundary_faces(self, name):
+        """The pipe's boundary level set on the faces of a component, as the
+        last velocity set-up computed it."""
+        a = np.empty(self.shape(name))
+        self._lib.fsref_boundary_faces(self.h, {"u": 0, "v": 1, "w": 2}[name], _ptr(a))
+        return a

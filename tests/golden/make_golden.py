@@ -34,6 +34,13 @@ on the air/water unit-cube box with Neumann pressure walls:
                    random velocities, both phase conventions (10^3); the level
                    set's first ghost layer is the oracle's linear
                    extrapolation and the velocity ghosts are zero
+  pipe_levelset    oil/water vertical pipe: ADVECTION_3D::Solve_Levelset (the
+                   cylinder's velocity set-up, periodic ghosts, WENO5 skipping
+                   cells outside the pipe)
+  pipe_reinit      the pipe's Reinitialization (sign function + 10 Sussman
+                   pseudo-steps on periodic ghosts)
+  pipe_forcing     the pipe's dimensionless body force (ApplyGravity), with
+                   the centre-line faces that Solve_Velocity marks fixed
 
     python tests/golden/make_golden.py [name ...]   writes only the named fixtures
 """
@@ -239,6 +246,50 @@ def main():
                               mu_pos=1.8e-5 if water_drop else 1e-3, phi=phi, **vel, out_u=c.get("u"),
                               out_v=c.get("v"), out_w=c.get("w"))
         c.close()
+
+    # oil/water vertical pipe (the reference's production mode): a 21 x 16 x
+    # 21 cell grid of spacing 0.25 around a pipe of radius a = 1.61, the
+    # constants of its 3D_script_1.sim; level set = the reference's own
+    # core-annular seed plus noise, face velocities random around the
+    # dimensionless core flow
+    h, pn = 0.25, (21, 16, 21)
+    lo = (-(pn[0] - 1) / 2 * h, 0.0, -(pn[2] - 1) / 2 * h)
+    hi = ((pn[0] - 1) / 2 * h, (pn[1] - 1) * h, (pn[2] - 1) / 2 * h)
+    pipe_sim = refsim.write_pipe_sim(os.path.join(WORK, "pipe.sim"), pn, lo, hi)
+    rng = np.random.default_rng(11)
+    c = refsim.RefCase(pipe_sim)
+    const = c.pipe_params()
+    phi = c.get("phi") + rng.normal(0.0, 0.02, c.shape("phi"))
+    vel = dict(u=rng.normal(0.0, 0.3, c.shape("u")), v=1.0 + rng.normal(0.0, 0.3, c.shape("v")),
+               w=rng.normal(0.0, 0.3, c.shape("w")))
+    base = dict(n=pn, lo=lo, hi=hi, boundary=c.boundary_levelset(),
+                **{k: const[k] for k in ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We")},
+                oil_density=const["oil_density"], gravity_y=-980.0, reinit_iterations=10, reinit_scaling=2,
+                epsilon=1e-6, phi=phi, **vel)
+    c.close()
+    c = refsim.RefCase(pipe_sim)
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    c.pipe_levelset_advection(0.01)
+    fixtures["pipe_levelset"] = dict(base, dt=0.01, out_phi=c.get("phi"), out_u=c.get("u"), out_v=c.get("v"),
+                                     out_w=c.get("w"))
+    c.close()
+    c = refsim.RefCase(pipe_sim)
+    c.set("phi", phi)
+    c.pipe_reinitialization(0.01)
+    fixtures["pipe_reinit"] = dict(base, out_phi=c.get("phi"))
+    c.close()
+    c = refsim.RefCase(pipe_sim)
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    c.pipe_velocity_advection(0.0)  # marks the centre-line faces fixed (ADVECTION_3D.h:246-275)
+    fixed_v = c.fixed("v")
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    c.pipe_gravity(0.01)
+    fixtures["pipe_forcing"] = dict(base, dt=0.01, fixed_v=fixed_v, out_u=c.get("u"), out_v=c.get("v"),
+                                    out_w=c.get("w"))
+    c.close()
 
     only = set(sys.argv[1:])
     for name, d in fixtures.items():

@@ -1,0 +1,72 @@
+"""Oil/water vertical pipe mode: the oracle against the reference's own
+outputs (fixtures pipe_* made by tests/golden/make_golden.py from the
+headless reference build, one reference thread).
+
+The pipe is the reference's production scenario (all four of its .sim files
+select it): a periodic vertical pipe of radius a in a box, the core-annular
+level set, dimensionless constants derived from the script.  Each operator
+here must agree bit for bit."""
+import os
+
+import numpy as np
+
+from oracle import fs_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+def grids(g):
+    return O.pipe_grids(tuple(int(x) for x in g["n"]), tuple(g["lo"]), tuple(g["hi"]))
+
+
+def test_pipe_constants_and_boundary_match_reference():
+    g = load("pipe_levelset")
+    C = O.pipe_constants(float(g["a"]), 0.47625, float(g["m"]), float(g["eta"]), float(g["K"]), float(g["g"]),
+                         0.995, float(g["oil_density"]), 0.01, 6.01, 8.54)
+    for k in ("R1", "f", "A", "V0", "J", "Re", "We"):
+        assert C[k] == float(g[k]), k
+    b = O.pipe_boundary(grids(g)[0], g["phi"].shape, float(g["a"]))
+    np.testing.assert_array_equal(b, g["boundary"])
+    # the pipe keeps at least three cells of the box around it (its WENO5
+    # cells never read the box's ghost layers)
+    inside = np.argwhere(b <= 0)
+    n = g["phi"].shape
+    assert inside[:, 0].min() >= 3 and inside[:, 0].max() <= n[0] - 4
+    assert inside[:, 2].min() >= 3 and inside[:, 2].max() <= n[2] - 4
+
+
+def test_pipe_levelset_advection_matches_reference():
+    g = load("pipe_levelset")
+    phi, u, v, w = O.pipe_weno5_levelset(g["phi"], g["u"], g["v"], g["w"], grids(g), float(g["a"]), float(g["dt"]),
+                                         float(g["epsilon"]))
+    np.testing.assert_array_equal(phi, g["out_phi"])
+    for k, a in zip("uvw", (u, v, w)):
+        np.testing.assert_array_equal(a, g["out_" + k])
+    # cells outside the pipe keep their value; u and w are zero outside it
+    b = g["boundary"]
+    np.testing.assert_array_equal(phi[b > 0], g["phi"][b > 0])
+    assert (np.abs(phi - g["phi"])[b <= 0] > 0).any()
+
+
+def test_pipe_reinitialization_matches_reference():
+    g = load("pipe_reinit")
+    out = O.pipe_reinitialization(g["phi"], grids(g), int(g["reinit_iterations"]), int(g["reinit_scaling"]),
+                                  float(g["epsilon"]), typo=True)
+    np.testing.assert_array_equal(out, g["out_phi"])
+
+
+def test_pipe_forcing_matches_reference():
+    g = load("pipe_forcing")
+    C = {k: float(g[k]) for k in ("a", "R1", "eta", "f", "V0")}
+    out = O.pipe_forcing(g["phi"], g["v"], grids(g), C, float(g["gravity_y"]), float(g["oil_density"]),
+                         float(g["dt"]), fixed_v=g["fixed_v"])
+    np.testing.assert_array_equal(out, g["out_v"])
+    np.testing.assert_array_equal(g["out_u"], g["u"])
+    np.testing.assert_array_equal(g["out_w"], g["w"])
+    # the centre-line faces are fixed and keep their value
+    assert g["fixed_v"].sum() > 0
+    np.testing.assert_array_equal(out[g["fixed_v"]], g["v"][g["fixed_v"]])
