@@ -38,7 +38,7 @@ FS_PRECOND_RED_BLACK_JACOBI = 4
 
 EXPORTED = ("fs_params_default", "fs_status_str", "fs_last_error", "fs_create", "fs_destroy", "fs_set_params",
             "fs_memory_bytes", "fs_upload", "fs_download", "fs_upload_device", "fs_download_device", "fs_step",
-            "fs_cfl_dt", "fs_project", "fs_advect_levelset", "fs_advect_velocity", "fs_reinitialize",
+            "fs_cfl_dt", "fs_project", "fs_advect_levelset", "fs_advect_velocity", "fs_reinitialize", "fs_apply_gravity",
             "fs_viscosity", "fs_pcg_csr", "fs_pcg_csr_noalloc", "fs_adjoint_reset", "fs_adjoint_density_bars",
             "fs_step_adjoint", "fs_advect_levelset_adjoint", "fs_advect_velocity_adjoint", "fs_reinitialize_adjoint",
             "fs_viscosity_adjoint", "fs_project_adjoint", "fs_curvature", "fs_write_levelset", "fs_read_levelset",
@@ -68,13 +68,17 @@ class Params(ctypes.Structure):
                 ("velocity_epsilon", ctypes.c_double), ("fast_sweeping", ctypes.c_int),
                 ("pressure_preconditioner", ctypes.c_int), ("reliable_delta", ctypes.c_double),
                 ("flux_arithmetic", ctypes.c_int), ("verbose", ctypes.c_int),
-                ("host_loop", ctypes.c_int)]
+                ("host_loop", ctypes.c_int),
+                # oil/water vertical pipe mode (0: the box)
+                ("pipe", ctypes.c_int), ("pipe_radius", ctypes.c_double), ("grid_min", ctypes.c_double * 3),
+                ("grid_max", ctypes.c_double * 3), ("pipe_R1", ctypes.c_double), ("pipe_V0", ctypes.c_double),
+                ("pipe_f", ctypes.c_double), ("pipe_eta", ctypes.c_double), ("pipe_oil_density", ctypes.c_double)]
 
     def as_dict(self):
         d = {}
         for name, _ in self._fields_:
             v = getattr(self, name)
-            d[name] = list(v) if name == "gravity" else v
+            d[name] = list(v) if name in ("gravity", "grid_min", "grid_max") else v
         return d
 
 
@@ -130,6 +134,7 @@ def lib():
         L.fs_advect_levelset.argtypes = [vp, ctypes.c_double]
         L.fs_advect_velocity.argtypes = [vp, ctypes.c_double]
         L.fs_reinitialize.argtypes = [vp]
+        L.fs_apply_gravity.argtypes = [vp, ctypes.c_double]
         L.fs_fast_sweeping.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.fs_surface.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
         L.fs_surface_download.argtypes = [vp, vp, vp, vp]
@@ -177,9 +182,9 @@ def default_params(**overrides):
     p = Params()
     lib().fs_params_default(ctypes.byref(p))
     for k, v in overrides.items():
-        if k == "gravity":
+        if k in ("gravity", "grid_min", "grid_max"):
             for a in range(3):
-                p.gravity[a] = float(v[a])
+                getattr(p, k)[a] = float(v[a])
         else:
             setattr(p, k, v)
     return p
@@ -298,6 +303,11 @@ class Solver:
 
     def advect_velocity(self, dt):
         _check(lib().fs_advect_velocity(self._h, float(dt)), "fs_advect_velocity")
+
+    def apply_gravity(self, dt):
+        """EULERIAN_FLUID_SOLVER_3D::ApplyGravity: gravity in the box, the
+        dimensionless body force in pipe mode."""
+        _check(lib().fs_apply_gravity(self._h, float(dt)), "fs_apply_gravity")
 
     def reinitialize(self):
         _check(lib().fs_reinitialize(self._h), "fs_reinitialize")

@@ -92,6 +92,7 @@ struct fs_ctx {
   double* rb_x = nullptr;          // black FP64 iterate
   float *rb_r = nullptr, *rb_p = nullptr, *rb_q = nullptr, *rb_tau = nullptr;
   unsigned short* rb_dinv = nullptr;  // black bf16 1/diag
+  PipeGeom pipe{};  // the oil/water pipe's geometry (pipe.on = 0: the box)
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
   // viscosity systems, one per component (storage type S)
   void* vs[3][9] = {};  // ax, ay, az, diag, rhs, x, r, p, q
@@ -278,6 +279,67 @@ void apply_params(fs_ctx* c) {
 // residual, e0 p0 = -sum(r).
 int deflate(const fs_ctx* c) { return (c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) ? 1 : 0; }
 
+// The oil/water vertical pipe: its grids as the reference computes them (cell
+// spacing (max - min)/(n - 1); each face grid reaches half a cell further on
+// its own axis, GRID_STRUCTURE_3D.h:91-137, EULERIAN_FLUID_SOLVER_3D.h:
+// 405-427) and the checks the mode needs.
+fs_status setup_pipe(fs_ctx* c) {
+  const fs_params& p = c->prm;
+  c->pipe = PipeGeom{};
+  if (p.pipe == 0) return FS_OK;
+  if (p.pipe != 1) { set_error("pipe must be 0 (the box) or 1 (a vertical pipe)"); return FS_INVALID_ARG; }
+  const int n[3] = {c->grid.nx, c->grid.ny, c->grid.nz};
+  double d[3];
+  for (int a = 0; a < 3; ++a) {
+    d[a] = (p.grid_max[a] - p.grid_min[a]) / (n[a] - 1);
+    if (!(d[a] > 0) || !std::isfinite(d[a]) || std::fabs(d[a] - c->grid.dx) > 1e-9 * c->grid.dx) {
+      set_error("pipe mode: (grid_max - grid_min)/(n - 1) must equal the grid's dx on every axis");
+      return FS_INVALID_ARG;
+    }
+  }
+  if (!(p.pipe_radius > 0) || !(p.pipe_R1 > 0) || !(p.pipe_V0 != 0) || !std::isfinite(p.pipe_V0) ||
+      !std::isfinite(p.pipe_f) || !(p.pipe_eta > 0) || !(p.pipe_oil_density > 0)) {
+    set_error("pipe mode: pipe_radius, pipe_R1, pipe_eta, pipe_oil_density must be positive, pipe_V0 non-zero");
+    return FS_INVALID_ARG;
+  }
+  if (n[1] < 5) { set_error("pipe mode: the pipe needs at least 5 cells along y"); return FS_INVALID_ARG; }
+  PipeGeom& G = c->pipe;
+  G.on = 1;
+  G.a = p.pipe_radius;
+  for (int g = 0; g < 4; ++g) {
+    G.ox[g] = p.grid_min[0];
+    G.hx[g] = d[0];
+    G.oz[g] = p.grid_min[2];
+    G.hz[g] = d[2];
+  }
+  G.ox[1] = p.grid_min[0] - 0.5 * d[0];
+  G.hx[1] = ((p.grid_max[0] + 0.5 * d[0]) - (p.grid_min[0] - 0.5 * d[0])) / n[0];
+  G.oz[3] = p.grid_min[2] - 0.5 * d[2];
+  G.hz[3] = ((p.grid_max[2] + 0.5 * d[2]) - (p.grid_min[2] - 0.5 * d[2])) / n[2];
+  // the WENO5 stencils of the cells inside the pipe must stay off the box's
+  // ghost layers: three cells of the box around the pipe
+  for (int k = 0; k < n[2]; ++k)
+    for (int i = 0; i < n[0]; ++i) {
+      const double X = G.ox[0] + i * G.hx[0], Z = G.oz[0] + k * G.hz[0];
+      if (std::sqrt(X * X + Z * Z) - G.a <= 0.0 && (i < 3 || i > n[0] - 4 || k < 3 || k > n[2] - 4)) {
+        set_error("pipe mode: the pipe must keep three cells of the box around it in x and z");
+        c->pipe = PipeGeom{};
+        return FS_INVALID_ARG;
+      }
+    }
+  return FS_OK;
+}
+
+// Operators of the box only: the pipe mode builds its level-set path and
+// its body force, not yet its ENO3 velocity advection, viscosity and
+// projection.
+fs_status box_only(const fs_ctx* c, const char* what) {
+  if (!c->pipe.on) return FS_OK;
+  set_error("%s is not built for the oil/water pipe mode (its velocity advection, viscosity and projection are not "
+            "built)", what);
+  return FS_NOT_SUPPORTED;
+}
+
 // ---------------------------------------------------------------------------
 // Krylov driver
 // ---------------------------------------------------------------------------
@@ -421,13 +483,25 @@ fs_status advect_levelset_t(fs_ctx* c, double dt, Tape* tp = nullptr) {
   S *phi = F<S>(c->phi), *t1 = F<S>(c->s1), *t2 = F<S>(c->s2);
   S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w);
   cudaStream_t s = c->stream;
+  const PipeGeom* pg = c->pipe.on ? &c->pipe : nullptr;
+  if (pg) {
+    // the pipe's velocity set-up (ADVECTION_3D.h:380-490): u and w zeroed
+    // outside the pipe, the ghost copies the update reads in the RK base
+    // arrays, which the velocity stages fill only after the level set
+    pipe_levelset_velocities<S>(u, v, w, F<S>(c->u0), F<S>(c->v0), F<S>(c->w0), c->Lu, c->Lv, c->Lw, *pg, s);
+    u = F<S>(c->u0);
+    v = F<S>(c->v0);
+    w = F<S>(c->w0);
+    c->launches += 3;
+  }
   int stage = 0;
   auto fe = [&](S* src, const S* base, S* out, double c0, double c1) {
     if (tp && stage < 3)
       cudaMemcpyAsync(tp->ls[stage], src, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s);
     ++stage;
-    fill_extrap<S>(src, c->Lc, s);
-    weno5_levelset<S>(src, base, out, u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, eps, dt, c0, c1, s);
+    if (pg) fill_periodic_y<S>(src, c->Lc, s);
+    else fill_extrap<S>(src, c->Lc, s);
+    weno5_levelset<S>(src, base, out, u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, eps, dt, c0, c1, s, pg);
     c->launches += 2;
   };
   if (P.order == 3 && !(P.flags & FS_FLAG_LEVELSET_FORWARD_EULER)) {
@@ -524,7 +598,8 @@ fs_status reinit_block_t(fs_ctx* c, void* in, void* out, void* base, double c0, 
     const bool last = it == n - 1;
     void* dst = last ? out : (cur == scrA ? scrB : scrA);
     if (tape) CK(cudaMemcpyAsync((*tape)[it], cur, c->Lc.total * c->S(), cudaMemcpyDeviceToDevice, s));
-    fill_extrap<S>(F<S>(cur), c->Lc, s);
+    if (c->pipe.on) fill_periodic_y<S>(F<S>(cur), c->Lc, s);  // ADVECTION_3D.h:360-378
+    else fill_extrap<S>(F<S>(cur), c->Lc, s);
     sussman_step<S>(F<S>(cur), F<S>(c->sgn), F<S>(base), F<S>(dst), c->Lc, dx, P.weno_epsilon, dtau,
                     last ? c0 : 0.0, last ? c1 : 1.0, (P.flags & FS_FLAG_REINIT_TYPO) ? 1 : 0, s);
     cur = dst;
@@ -836,6 +911,17 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
 template <class S>
 fs_status gravity_t(fs_ctx* c, double dt) {
   const double* g = c->prm.gravity;
+  if (c->pipe.on) {
+    // the vertical pipe's dimensionless body force (EULERIAN_FLUID_SOLVER_3D.h:2304-2326)
+    const fs_params& P = c->prm;
+    const double dy = (P.grid_max[1] - P.grid_min[1]) / (c->grid.ny - 1);
+    fill_periodic_y<S>(F<S>(c->phi), c->Lc, c->stream);
+    pipe_forcing<S>(F<S>(c->v), F<S>(c->phi), c->Lv, c->Lc, c->pipe, P.pipe_R1 / (P.pipe_V0 * P.pipe_V0),
+                    dt * g[1], dt * P.pipe_f, P.pipe_oil_density, P.pipe_eta, 1.5 * dy, c->stream);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    return FS_OK;
+  }
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
   void* comps[3] = {c->u, c->v, c->w};
   for (int a = 0; a < 3; ++a)
@@ -1415,6 +1501,10 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
   c->prm = prm;
   c->fp32 = prm.precision == FS_PRECISION_FP32_REFINE;
   apply_params(c);
+  if (fs_status ps = setup_pipe(c); ps != FS_OK) {
+    delete c;
+    return ps;
+  }
   c->Lc = make_lay(grid->nx, grid->ny, grid->nz);
   c->Lu = make_lay(grid->nx + 1, grid->ny, grid->nz);
   c->Lv = make_lay(grid->nx, grid->ny + 1, grid->nz);
@@ -1506,7 +1596,13 @@ fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
     set_error("semi-implicit viscosity buffers were not allocated at creation");
     return FS_INVALID_ARG;
   }
+  const fs_params old = c->prm;
   c->prm = *p;
+  if (fs_status ps = setup_pipe(c); ps != FS_OK) {
+    c->prm = old;
+    setup_pipe(c);
+    return ps;
+  }
   apply_params(c);
   // captured solver graphs hold the operator's arithmetic and preconditioner
   // as kernel arguments: capture them again under the new settings
@@ -1664,6 +1760,7 @@ static fs_status timed_end(fs_ctx* c, float* ms) {
 
 fs_status fs_step(fs_ctx* c, double dt, fs_step_report* rep) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_step"));
   if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
   fs_step_report local{};
   fs_step_report* r = rep ? rep : &local;
@@ -1683,6 +1780,7 @@ fs_status fs_step(fs_ctx* c, double dt, fs_step_report* rep) {
 
 fs_status fs_curvature(fs_ctx* c, double* kappa_max) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_curvature"));
   CKS(DISPATCH(c, curvature_t, c));
   CK(cudaMemcpyAsync(c->sc_host + 13, c->scalars + 13, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1692,11 +1790,13 @@ fs_status fs_curvature(fs_ctx* c, double* kappa_max) {
 
 fs_status fs_cfl_dt(fs_ctx* c, double* dt) {
   if (!c || !dt) { set_error("NULL argument"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_cfl_dt"));
   return DISPATCH(c, cfl_t, c, dt);
 }
 
 fs_status fs_project(fs_ctx* c, double dt, fs_solve_report* rep) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_project"));
   if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
   fs_solve_report local{};
   fs_solve_report* r = rep ? rep : &local;
@@ -1721,8 +1821,17 @@ fs_status fs_advect_levelset(fs_ctx* c, double dt) {
   return FS_OK;
 }
 
+fs_status fs_apply_gravity(fs_ctx* c, double dt) {
+  if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
+  CKS(DISPATCH(c, gravity_t, c, dt));
+  CK(cudaStreamSynchronize(c->stream));
+  return FS_OK;
+}
+
 fs_status fs_advect_velocity(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_advect_velocity"));
   CKS(DISPATCH(c, advect_velocity_t, c, dt));
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;
@@ -1741,6 +1850,7 @@ fs_status fs_reinitialize(fs_ctx* c) {
 
 fs_status fs_fast_sweeping(fs_ctx* c, int direction, int pairs) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_fast_sweeping"));
   if (direction < -1 || direction > 3 || pairs < 1 || pairs > 4) {
     set_error("direction must be -1..3 and pairs 1..4");
     return FS_INVALID_ARG;
@@ -1805,6 +1915,7 @@ fs_status fs_write_obj(fs_ctx* c, const char* path) {
 
 fs_status fs_viscosity(fs_ctx* c, double dt, int* iterations) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_viscosity"));
   if (!(dt > 0)) { set_error("dt must be positive"); return FS_INVALID_ARG; }
   CKS(DISPATCH(c, viscosity_t, c, dt, iterations));
   CK(cudaStreamSynchronize(c->stream));
@@ -1972,6 +2083,7 @@ static void adj_begin(fs_ctx* c) {
 
 fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_step_adjoint"));
   if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
   CKS(adj_check(c));
   fs_step_report local{};
@@ -1993,6 +2105,7 @@ fs_status fs_step_adjoint(fs_ctx* c, double dt, fs_step_report* rep) {
 
 fs_status fs_advect_levelset_adjoint(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_advect_levelset_adjoint"));
   CKS(adj_check(c));
   void* vel[3] = {c->u, c->v, c->w};
   CKS(c->fp32 ? adj_levelset_fe<float>(c, c->phi, vel, c->abar[0], 1.0, c->awork_c[0], &c->abar[1], dt)
@@ -2004,6 +2117,7 @@ fs_status fs_advect_levelset_adjoint(fs_ctx* c, double dt) {
 
 fs_status fs_advect_velocity_adjoint(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_advect_velocity_adjoint"));
   CKS(adj_check(c));
   void* vel[3] = {c->u, c->v, c->w};
   CKS(c->fp32 ? adj_velocity_advect<float>(c, vel, &c->abar[1], c->awork_f[0], dt)
@@ -2015,6 +2129,7 @@ fs_status fs_advect_velocity_adjoint(fs_ctx* c, double dt) {
 
 fs_status fs_reinitialize_adjoint(fs_ctx* c) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_reinitialize_adjoint"));
   CKS(adj_check(c));
   Tape tp;
   CKS(tape_bind(c, &tp));
@@ -2032,6 +2147,7 @@ fs_status fs_reinitialize_adjoint(fs_ctx* c) {
 
 fs_status fs_viscosity_adjoint(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_viscosity_adjoint"));
   if (!(dt > 0)) { set_error("dt must be positive"); return FS_INVALID_ARG; }
   CKS(adj_check(c));
   if (c->prm.viscosity != 1) { set_error("the semi-implicit viscosity is off"); return FS_INVALID_ARG; }
@@ -2053,6 +2169,7 @@ fs_status fs_viscosity_adjoint(fs_ctx* c, double dt) {
 
 fs_status fs_project_adjoint(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
+  CKS(box_only(c, "fs_project_adjoint"));
   if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
   CKS(adj_check(c));
   Tape tp;

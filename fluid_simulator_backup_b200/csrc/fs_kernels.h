@@ -8,10 +8,38 @@ namespace fsb {
 
 // ---- stencil family (fs_stencil.cu)
 template <class T> void fill_extrap(T* f, const Lay& L, cudaStream_t s);
+
+// Geometry of the oil/water vertical pipe (fs_pipe.cu): the wall radius and,
+// for the cell grid (0) and the x, y, z face grids (1..3), the x and z
+// position of index 0 and the spacing, computed as the reference computes
+// its grids (GRID_STRUCTURE_3D.h:91-137).
+struct PipeGeom {
+  int on;  // 0: the box
+  double a;
+  double ox[4], oz[4], hx[4], hz[4];
+};
+// sqrt(x^2 + z^2) - a at point (i, k) of grid g, in the reference's rounding
+__device__ __forceinline__ double pipe_wall_distance(const PipeGeom& G, int g, int i, int k) {
+  const double X = __dadd_rn(G.ox[g], __dmul_rn((double)i, G.hx[g]));
+  const double Z = __dadd_rn(G.oz[g], __dmul_rn((double)k, G.hz[g]));
+  return __dsub_rn(sqrt(__dadd_rn(__dmul_rn(X, X), __dmul_rn(Z, Z))), G.a);
+}
+// periodic ghosts along y of a cell field (cell 0 and cell ny-1 are one
+// point); the x and z ghost layers become 0
+template <class T> void fill_periodic_y(T* f, const Lay& L, cudaStream_t s);
+// the velocities the pipe's level-set advection reads (ghost copies g*) and
+// the zeroing of u and w outside the pipe
+template <class T>
+void pipe_levelset_velocities(T* u, T* v, T* w, T* ug, T* vg, T* wg, const Lay& Lu, const Lay& Lv, const Lay& Lw,
+                              const PipeGeom& G, cudaStream_t s);
+// the pipe's dimensionless body force on v (phi with periodic y ghosts)
+template <class T>
+void pipe_forcing(T* v, const T* phi, const Lay& Lv, const Lay& Lc, const PipeGeom& G, double coef, double gdt,
+                  double fdt, double oil_density, double eta, double eps, cudaStream_t s);
 template <class T>
 void weno5_levelset(const T* src, const T* base, T* out, const T* u, const T* v, const T* w, const Lay& L,
                     const Lay& Lu, const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c0, double c1,
-                    cudaStream_t s);
+                    cudaStream_t s, const PipeGeom* pipe = nullptr);
 template <class T>
 void weno5_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
                const Lay& Lw, int axis, double dx, double eps, double dt, cudaStream_t s);

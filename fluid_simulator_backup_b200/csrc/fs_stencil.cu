@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kTX * kTY) k_weno5_levelset(const T* __restric
                                                            T* __restrict__ out, const T* __restrict__ u,
                                                            const T* __restrict__ v, const T* __restrict__ w, Lay L,
                                                            Lay Lu, Lay Lv, Lay Lw, T inv_h, T eps, T dt, T c0, T c1,
-                                                           int kchunk) {
+                                                           int kchunk, PipeGeom pipe) {
   __shared__ T ring[kRing * kRW * kRH];
   const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
@@ -246,8 +246,11 @@ __global__ void __launch_bounds__(kTX * kTY) k_weno5_levelset(const T* __restric
       const T uc = (u[Lu.at(i + 1, j, k)] + u[Lu.at(i, j, k)]) * T(0.5);
       const T vc = (v[Lv.at(i, j + 1, k)] + v[Lv.at(i, j, k)]) * T(0.5);
       const T wc = (w[Lw.at(i, j, k + 1)] + w[Lw.at(i, j, k)]) * T(0.5);
-      const T fe =
+      T fe =
           vx[3] - dt * ((uc * (uc > T(0) ? dxm : dxp) + vc * (vc > T(0) ? dym : dyp)) + wc * (wc > T(0) ? dzm : dzp));
+      // pipe mode: cells outside the pipe keep their value
+      // (ADVECTION_METHOD_3D.h:293-296)
+      if (pipe.on && pipe_wall_distance(pipe, 0, i, k) > 0.0) fe = vx[3];
       out[c] = c0 == T(0) ? fe : c0 * base[c] + c1 * fe;
     }
     __syncthreads();
@@ -482,10 +485,12 @@ __global__ void k_zero_walls(T* __restrict__ f, Lay L, int axis) {
 template <class T>
 void weno5_levelset(const T* src, const T* base, T* out, const T* u, const T* v, const T* w, const Lay& L,
                     const Lay& Lu, const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c0, double c1,
-                    cudaStream_t s) {
+                    cudaStream_t s, const PipeGeom* pipe) {
   const StagedGrid g = staged_grid(L);
+  PipeGeom none{};
   k_weno5_levelset<T><<<g.grid, dim3(kTX, kTY, 1), 0, s>>>(src, base, out, u, v, w, L, Lu, Lv, Lw, T(1.0 / dx),
-                                                           T(eps), T(dt), T(c0), T(c1), g.kchunk);
+                                                           T(eps), T(dt), T(c0), T(c1), g.kchunk,
+                                                           pipe ? *pipe : none);
 }
 
 template <class T>
@@ -539,7 +544,8 @@ void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s) {
 #define FS_INST(T)                                                                                                    \
   template void fill_extrap<T>(T*, const Lay&, cudaStream_t);                                                         \
   template void weno5_levelset<T>(const T*, const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&,       \
-                                  const Lay&, const Lay&, double, double, double, double, double, cudaStream_t);      \
+                                  const Lay&, const Lay&, double, double, double, double, double, cudaStream_t,       \
+                                  const PipeGeom*);                                                                   \
   template void weno5_mac<T>(const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,          \
                              const Lay&, int, double, double, double, cudaStream_t);                                  \
   template void eno3_mac<T>(const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,           \

@@ -135,6 +135,22 @@ typedef struct {
                                        node repeating 16-iteration batches); 1: the same kernels launched from the
                                        host, 16 iterations between polls of the solver state (for profilers that do
                                        not descend into conditional graph nodes) */
+  /* Oil/water pipe mode, the reference's oil_water_simulation with a vertical
+     pipe (PIPE_OPTIONS.is_vertical): 0 (default) the air/water box with walls;
+     1 a pipe along y, periodic in y with the reference's node convention (cell
+     0 and cell ny-1 are one point), its wall at sqrt(x^2 + z^2) = pipe_radius.
+     Built for the level-set advection, the reinitialisation and the body force
+     (fs_advect_levelset, fs_reinitialize, fs_apply_gravity); the other
+     operators and fs_step return FS_NOT_SUPPORTED in this mode. */
+  int pipe;
+  double pipe_radius;               /* a: the wall radius in units of the core radius R1 */
+  double grid_min[3], grid_max[3];  /* the script's base_grid_min and base_grid_max: cell (i,j,k) sits at
+                                       grid_min + (i,j,k) (grid_max - grid_min)/(n - 1), as in the reference */
+  double pipe_R1;                   /* R1 = R2/a */
+  double pipe_V0;                   /* V0, the velocity scale of the dimensionless form */
+  double pipe_f;                    /* f, the driving pressure gradient */
+  double pipe_eta;                  /* eta, the density ratio of the dimensionless form */
+  double pipe_oil_density;          /* oil_density */
 } fs_params;
 
 typedef struct {
@@ -202,6 +218,12 @@ fs_status fs_advect_levelset(fs_ctx* ctx, double dt);
 fs_status fs_advect_velocity(fs_ctx* ctx, double dt);
 /* One reinitialisation block (EULERIAN_FLUID_SOLVER_3D::Reinitialization, :2198). */
 fs_status fs_reinitialize(fs_ctx* ctx);
+/* EULERIAN_FLUID_SOLVER_3D::ApplyGravity (EULERIAN_FLUID_SOLVER_3D.h:2237-2432):
+   u += dt g on interior faces in the box; in pipe mode the dimensionless body
+   force on the y faces inside the pipe, R1/V0^2 (dt g_y + dt f/(oil_density
+   rho_f)), rho_f = 1 + (eta - 1) H(phi_f), except the centre-line faces the
+   reference holds fixed (i = (nx-1)/2, k = (nz-1)/2). */
+fs_status fs_apply_gravity(fs_ctx* ctx, double dt);
 /* LEVELSET_3D::ReinitializeByFastSweeping (LEVELSET_3D.h:601-610) on phi,
  * without the closing normals and curvature: the set-up (cells beyond
  * 20 dx and cells next to the interface fixed, the others reset to
