@@ -1626,3 +1626,128 @@ def pipe_forcing(phi, v, grids, C, gravity_y, oil_density, dt, fixed_v=None):
     if fixed_v is not None:
         mask &= ~fixed_v
     return np.where(mask, v + add, v)
+
+
+def _pipe_periodic_copy(c, b, y_component):
+    """The masked periodic ghost copy of one face component of a vertical pipe
+    (FIELD_STRUCTURE_3D.h:1432-1540): interior = c where b < 1e-8, else 0;
+    the y ghost rows of interior columns hold the periodic images of c (the
+    reference tests b there on its unfilled ghost rows, which hold 0); for the
+    y component the first and last face rows are rewritten with their images
+    where b < 1e-8 too (face 0 is face ny-1, face ny is face 1).  Faces outside
+    the pipe in a row or column that crosses it take the linear extrapolation
+    below; the rest of the x and z ghost layers hold 0."""
+    g = G
+    nz, Ny, nx = c.shape
+    out = np.zeros((nz + 2 * g, Ny + 2 * g, nx + 2 * g))
+    inner = np.where(b < 1e-8, c, 0.0)
+    if y_component:
+        inner[:, 0, :] = np.where(b[:, 0, :] < 1e-8, c[:, Ny - 2, :], inner[:, 0, :])
+        inner[:, Ny - 1, :] = np.where(b[:, Ny - 1, :] < 1e-8, c[:, 1, :], inner[:, Ny - 1, :])
+        lo = lambda m: c[:, Ny - 2 - m, :]
+        hi = lambda m: c[:, 1 + m, :]
+    else:
+        lo = lambda m: c[:, Ny - 1 - m, :]
+        hi = lambda m: c[:, m, :]
+    out[g:g + nz, g:g + Ny, g:g + nx] = inner
+    for m in range(1, g + 1):
+        out[g:g + nz, g - m, g:g + nx] = lo(m)
+        out[g:g + nz, g + Ny - 1 + m, g:g + nx] = hi(m)
+    # then, along each row and column of the pipe's cross-section, every face
+    # from the first one outside the pipe to the end of the row (ghost layers
+    # included) takes the linear extrapolation of the velocity itself,
+    # 2 c(t-1) - c(t-2) outward (FIELD_STRUCTURE_3D.h:1563-1610): x rows
+    # first, right then left side, then z columns, which overwrite
+    cp = np.pad(c, g)  # the velocity's own ghost layers hold 0
+    bp = np.pad(b, 1)  # the boundary array's unfilled ghost layer holds 0
+    for (k, j, i) in np.argwhere((bp[1:-1, 1:-1, :-2] < 0) & (b > 0)):  # x: inside at i-1
+        for t in range(i, nx + g):
+            out[k + g, j + g, t + g] = 2.0 * cp[k + g, j + g, t - 1 + g] - cp[k + g, j + g, t - 2 + g]
+    for (k, j, i) in np.argwhere((bp[1:-1, 1:-1, 2:] < 0) & (b > 0)):  # x: inside at i+1
+        for t in range(i, -g - 1, -1):
+            out[k + g, j + g, t + g] = 2.0 * cp[k + g, j + g, t + 1 + g] - cp[k + g, j + g, t + 2 + g]
+    for (k, j, i) in np.argwhere((bp[:-2, 1:-1, 1:-1] < 0) & (b > 0)):  # z: inside at k-1
+        for t in range(k, nz + g):
+            out[t + g, j + g, i + g] = 2.0 * cp[t - 1 + g, j + g, i + g] - cp[t - 2 + g, j + g, i + g]
+    for (k, j, i) in np.argwhere((bp[2:, 1:-1, 1:-1] < 0) & (b > 0)):  # z: inside at k+1
+        for t in range(k, -g - 1, -1):
+            out[t + g, j + g, i + g] = 2.0 * cp[t + 1 + g, j + g, i + g] - cp[t + 2 + g, j + g, i + g]
+    return out
+
+
+def _pipe_eno_guard(gc, b, axis):
+    """The copy of a component that the pipe's ENO3 reads along x (axis 0) or
+    z (axis 2) (ADVECTION_3D.h:560-700): next to each inside face whose
+    neighbour along the axis is outside, the neighbour gets the value
+    extrapolated across the wall, (theta-1)/theta times the inside face's,
+    theta = |b_in|/(|b_in| + |b_out|), and the next three faces the large
+    values (10t)^t, t = 2, 3, 4, so that the ENO stencil choice stays inside
+    the pipe."""
+    g = G
+    out = gc.copy()
+    ax = 2 - axis
+    nz, Ny, nx = b.shape
+    for s in (1, -1):
+        bn = np.zeros_like(b)
+        src = [slice(None)] * 3
+        dst = [slice(None)] * 3
+        if s == 1:
+            src[ax], dst[ax] = slice(1, None), slice(0, -1)
+        else:
+            src[ax], dst[ax] = slice(0, -1), slice(1, None)
+        bn[tuple(dst)] = b[tuple(src)]
+        idx = np.argwhere((b < 0) & (bn > 0))
+        for (k, j, i) in idx:
+            pos = [k + g, j + g, i + g]
+            theta = abs(b[k, j, i]) / (abs(bn[k, j, i]) + abs(b[k, j, i]))
+            p1 = list(pos)
+            p1[ax] += s
+            out[tuple(p1)] = (theta - 1) / theta * gc[tuple(pos)]
+            for t in range(2, 5):
+                pt = list(pos)
+                pt[ax] += s * t
+                out[tuple(pt)] = float((10 * t) ** t)
+    return out
+
+
+def pipe_fixed_faces(n):
+    """The centre-line faces Solve_Velocity holds fixed in a vertical pipe
+    (ADVECTION_3D.h:246-275): x faces i = nx/2, nx/2 + 1 and z faces k =
+    nz/2, nz/2 + 1 at the centre of the other axis, the y faces of the centre
+    column (integer halves of the face grids' last indices)."""
+    nx, ny, nz = n
+    fu = np.zeros((nz, ny, nx + 1), bool)
+    fv = np.zeros((nz, ny + 1, nx), bool)
+    fw = np.zeros((nz + 1, ny, nx), bool)
+    fu[(nz - 1) // 2, :, nx // 2] = True
+    fu[(nz - 1) // 2, :, nx // 2 + 1] = True
+    fv[(nz - 1) // 2, :, (nx - 1) // 2] = True
+    fw[nz // 2, :, (nx - 1) // 2] = True
+    fw[nz // 2 + 1, :, (nx - 1) // 2] = True
+    return fu, fv, fw
+
+
+def pipe_eno3_velocity(u, v, w, grids, a, dt):
+    """ADVECTION_3D::Solve_Velocity of a vertical pipe with ENO3
+    (ADVECTION_3D.h:244-358, ADVECTION_METHOD_3D.h:1935-2240): each face
+    inside the pipe and not fixed takes the ENO3 upwind update, its x and z
+    derivatives from the guarded copies, its y derivative and the advecting
+    velocities from the masked periodic copies; the other faces keep their
+    value.  Returns (u, v, w)."""
+    comps = (u, v, w)
+    bs = [pipe_boundary(grids[1 + ax], comps[ax].shape, a) for ax in range(3)]
+    gen = [_pipe_periodic_copy(comps[ax], bs[ax], ax == 1) for ax in range(3)]
+    nz, ny, nx = u.shape[0], u.shape[1], u.shape[2] - 1
+    fixed = pipe_fixed_faces((nx, ny, nz))
+    out = []
+    for ax in range(3):
+        gx = _pipe_eno_guard(gen[ax], bs[ax], 0)
+        gz = _pipe_eno_guard(gen[ax], bs[ax], 2)
+        gr = grids[1 + ax]
+        uvel, vvel, wvel = _face_velocities(ax, gen[0], gen[1], gen[2])
+        dxm, dxp = eno3_derivatives(gx, 0, gr[3])
+        dym, dyp = eno3_derivatives(gen[ax], 1, gr[4])
+        dzm, dzp = eno3_derivatives(gz, 2, gr[5])
+        new = _upwind_update(comps[ax], dt, uvel, vvel, wvel, dxm, dxp, dym, dyp, dzm, dzp)
+        out.append(np.where((bs[ax] < 0) & ~fixed[ax], new, comps[ax]))
+    return tuple(out)

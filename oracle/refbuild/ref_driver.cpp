@@ -473,6 +473,23 @@ void fsref_boundary_faces(void* h, int comp, double* dst) {
   for_interior(*f[comp], [&](T& v, long n) { dst[n] = v; });
 }
 
+// One of the advection's per-axis velocity ghost copies (ADVECTION_3D.h:
+// 40-48; id = 3 * component + axis), with its three ghost layers, x fastest.
+void fsref_adv_ghost(void* h, int id, double* dst) {
+  ADVECTION_3D& adv = *static_cast<RefCase*>(h)->world.eulerian_solver.advecting_field_variables;
+  FIELD_STRUCTURE_3D<T>* f[] = {&adv.velocity_field_mac_ghost_x_x, &adv.velocity_field_mac_ghost_x_y,
+                                &adv.velocity_field_mac_ghost_x_z, &adv.velocity_field_mac_ghost_y_x,
+                                &adv.velocity_field_mac_ghost_y_y, &adv.velocity_field_mac_ghost_y_z,
+                                &adv.velocity_field_mac_ghost_z_x, &adv.velocity_field_mac_ghost_z_y,
+                                &adv.velocity_field_mac_ghost_z_z};
+  FIELD_STRUCTURE_3D<T>& a = *f[id];
+  const GRID_STRUCTURE_3D& g = a.grid;
+  long idx = 0;
+  for (int k = g.k_start - 3; k <= g.k_end + 3; ++k)
+    for (int j = g.j_start - 3; j <= g.j_end + 3; ++j)
+      for (int i = g.i_start - 3; i <= g.i_end + 3; ++i) dst[idx++] = a.array_for_this(i, j, k);
+}
+
 // The fixed flags of a velocity component (1: the face keeps its value).
 void fsref_fixed(void* h, int comp, unsigned char* dst) {
   EULERIAN_FLUID_SOLVER_3D& s = static_cast<RefCase*>(h)->world.eulerian_solver;

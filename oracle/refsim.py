@@ -78,6 +78,7 @@ def _lib():
         lib.fsref_boundary_levelset.argtypes = [ctypes.c_void_p, _dp]
         lib.fsref_ghost_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         lib.fsref_boundary_faces.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        lib.fsref_adv_ghost.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         lib.fsref_fixed.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_ubyte)]
         for fn in ("fsref_pipe_levelset_advection", "fsref_pipe_velocity_advection", "fsref_pipe_reinitialization",
                    "fsref_pipe_gravity"):
@@ -561,4 +562,12 @@ class RefCase:
         last velocity set-up computed it."""
         a = np.empty(self.shape(name))
         self._lib.fsref_boundary_faces(self.h, {"u": 0, "v": 1, "w": 2}[name], _ptr(a))
+        return a
+
+    def advection_ghost(self, comp, axis):
+        """The advection's per-axis ghost copy of component comp ("u", "v",
+        "w") read along axis ("x", "y", "z"), with its three ghost layers."""
+        sh = tuple(d + 6 for d in self.shape(comp))
+        a = np.empty(sh)
+        self._lib.fsref_adv_ghost(self.h, 3 * "uvw".index(comp) + "xyz".index(axis), _ptr(a))
         return a

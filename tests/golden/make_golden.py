@@ -37,6 +37,9 @@ on the air/water unit-cube box with Neumann pressure walls:
   pipe_levelset    oil/water vertical pipe: ADVECTION_3D::Solve_Levelset (the
                    cylinder's velocity set-up, periodic ghosts, WENO5 skipping
                    cells outside the pipe)
+  pipe_velocity    the pipe's ADVECTION_3D::Solve_Velocity with ENO3: masked
+                   periodic ghost copies with the wall extrapolation, the
+                   guarded copies of the ENO stencils, fixed centre-line faces
   pipe_reinit      the pipe's Reinitialization (sign function + 10 Sussman
                    pseudo-steps on periodic ghosts)
   pipe_forcing     the pipe's dimensionless body force (ApplyGravity), with
@@ -273,6 +276,13 @@ def main():
     c.pipe_levelset_advection(0.01)
     fixtures["pipe_levelset"] = dict(base, dt=0.01, out_phi=c.get("phi"), out_u=c.get("u"), out_v=c.get("v"),
                                      out_w=c.get("w"))
+    c.close()
+    c = refsim.RefCase(pipe_sim)
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    c.pipe_velocity_advection(0.01)
+    fixtures["pipe_velocity"] = dict(base, dt=0.01, out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"),
+                                     fixed_u=c.fixed("u"), fixed_v=c.fixed("v"), fixed_w=c.fixed("w"))
     c.close()
     c = refsim.RefCase(pipe_sim)
     c.set("phi", phi)

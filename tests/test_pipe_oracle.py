@@ -70,3 +70,15 @@ def test_pipe_forcing_matches_reference():
     # the centre-line faces are fixed and keep their value
     assert g["fixed_v"].sum() > 0
     np.testing.assert_array_equal(out[g["fixed_v"]], g["v"][g["fixed_v"]])
+
+
+def test_pipe_velocity_advection_matches_reference():
+    g = load("pipe_velocity")
+    out = O.pipe_eno3_velocity(g["u"], g["v"], g["w"], grids(g), float(g["a"]), float(g["dt"]))
+    for k, a in zip("uvw", out):
+        np.testing.assert_array_equal(a, g["out_" + k])
+    fixed = O.pipe_fixed_faces(tuple(int(x) for x in g["n"]))
+    for k, f in zip("uvw", fixed):
+        np.testing.assert_array_equal(f, g["fixed_" + k])
+        # fixed faces and faces outside the pipe keep their value
+        np.testing.assert_array_equal(g["out_" + k][f], g[k][f])
