@@ -93,6 +93,9 @@ struct fs_ctx {
   float *rb_r = nullptr, *rb_p = nullptr, *rb_q = nullptr, *rb_tau = nullptr;
   unsigned short* rb_dinv = nullptr;  // black bf16 1/diag
   PipeGeom pipe{};  // the oil/water pipe's geometry (pipe.on = 0: the box)
+  void* pgen[3] = {nullptr, nullptr, nullptr};  // pipe: masked periodic velocity copies
+  void* pgx[3] = {nullptr, nullptr, nullptr};   // pipe: their ENO3-guarded copies along x
+  void* pgz[3] = {nullptr, nullptr, nullptr};   // and along z
   void *px = nullptr, *pr = nullptr, *pp = nullptr, *pq = nullptr, *prhs = nullptr;
   // viscosity systems, one per component (storage type S)
   void* vs[3][9] = {};  // ax, ay, az, diag, rhs, x, r, p, q
@@ -330,13 +333,12 @@ fs_status setup_pipe(fs_ctx* c) {
   return FS_OK;
 }
 
-// Operators of the box only: the pipe mode builds its level-set path and
-// its body force, not yet its ENO3 velocity advection, viscosity and
+// Operators of the box only: the pipe mode builds its level-set path, its
+// ENO3 velocity advection and its body force, not yet its viscosity and
 // projection.
 fs_status box_only(const fs_ctx* c, const char* what) {
   if (!c->pipe.on) return FS_OK;
-  set_error("%s is not built for the oil/water pipe mode (its velocity advection, viscosity and projection are not "
-            "built)", what);
+  set_error("%s is not built for the oil/water pipe mode (its viscosity and projection are not built)", what);
   return FS_NOT_SUPPORTED;
 }
 
@@ -531,6 +533,26 @@ template <class S>
 fs_status advect_velocity_t(fs_ctx* c, double dt) {
   const double eps = velocity_epsilon(c), dx = c->grid.dx;
   S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w);
+  if (c->pipe.on) {
+    // the vertical pipe (ADVECTION_3D.h:244-358, the oil/water ENO3 path):
+    // the ghost copies, then each component in place
+    if (c->prm.velocity_scheme != FS_VELOCITY_ENO3) {
+      set_error("the pipe mode advects the velocity with ENO3 (use_3rd_eno_v) only");
+      return FS_NOT_SUPPORTED;
+    }
+    S* comps[3] = {u, v, w};
+    const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
+    S* gen[3] = {F<S>(c->pgen[0]), F<S>(c->pgen[1]), F<S>(c->pgen[2])};
+    S* gx[3] = {F<S>(c->pgx[0]), F<S>(c->pgx[1]), F<S>(c->pgx[2])};
+    S* gz[3] = {F<S>(c->pgz[0]), F<S>(c->pgz[1]), F<S>(c->pgz[2])};
+    c->launches += pipe_velocity_copies<S>(comps, gen, gx, gz, lays, c->pipe, c->stream);
+    for (int a = 0; a < 3; ++a)
+      eno3_pipe<S>(comps[a], gen[a], gx[a], gz[a], gen[0], gen[1], gen[2], c->Lc, c->Lu, c->Lv, c->Lw, a, c->pipe,
+                   dx, dt, c->stream);
+    c->launches += 3;
+    CK(cudaGetLastError());
+    return FS_OK;
+  }
   if (c->prm.velocity_scheme == FS_VELOCITY_ENO3) {
     eno3_mac<S>(u, F<S>(c->ua), u, v, w, c->Lu, c->Lu, c->Lv, c->Lw, 0, dx, dt, c->stream);
     eno3_mac<S>(v, F<S>(c->va), u, v, w, c->Lv, c->Lu, c->Lv, c->Lw, 1, dx, dt, c->stream);
@@ -1548,6 +1570,12 @@ fs_status fs_create(const fs_grid_desc* grid, const fs_params* params, fs_ctx** 
     for (float** p : hv) if ((s = dalloc(c, (void**)p, hb * sizeof(float))) != FS_OK) return fail(s);
     if ((s = dalloc(c, (void**)&c->rb_dinv, hb * sizeof(unsigned short))) != FS_OK) return fail(s);
   }
+  if (prm.pipe) {
+    const size_t fb[3] = {ub, vb, wb};
+    for (int a = 0; a < 3; ++a)
+      for (void** p : {&c->pgen[a], &c->pgx[a], &c->pgz[a]})
+        if ((s = dalloc(c, p, fb[a])) != FS_OK) return fail(s);
+  }
   if (prm.viscosity == 1) {
     const size_t fb[3] = {ub, vb, wb};
     for (int a = 0; a < 3; ++a)
@@ -1592,6 +1620,7 @@ fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
   if (!c || !p) { set_error("NULL argument"); return FS_INVALID_ARG; }
   CKS(check_params(p));
   if (p->precision != c->prm.precision) { set_error("precision is fixed at creation"); return FS_INVALID_ARG; }
+  if ((p->pipe != 0) != (c->prm.pipe != 0)) { set_error("the pipe mode is fixed at creation"); return FS_INVALID_ARG; }
   if (p->viscosity == 1 && !c->vs[0][0]) {
     set_error("semi-implicit viscosity buffers were not allocated at creation");
     return FS_INVALID_ARG;
@@ -1831,7 +1860,6 @@ fs_status fs_apply_gravity(fs_ctx* c, double dt) {
 
 fs_status fs_advect_velocity(fs_ctx* c, double dt) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
-  CKS(box_only(c, "fs_advect_velocity"));
   CKS(DISPATCH(c, advect_velocity_t, c, dt));
   CK(cudaStreamSynchronize(c->stream));
   return FS_OK;

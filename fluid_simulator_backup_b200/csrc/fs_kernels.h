@@ -32,6 +32,17 @@ template <class T> void fill_periodic_y(T* f, const Lay& L, cudaStream_t s);
 template <class T>
 void pipe_levelset_velocities(T* u, T* v, T* w, T* ug, T* vg, T* wg, const Lay& Lu, const Lay& Lv, const Lay& Lw,
                               const PipeGeom& G, cudaStream_t s);
+// the ghost copies of the pipe's velocity advection: per component the masked
+// periodic copy with its wall extrapolation (gen) and the copies guarded for
+// the ENO3 stencils along x (gx) and z (gz); returns the kernels launched
+template <class T>
+int pipe_velocity_copies(const T* const comp[3], T* const gen[3], T* const gx[3], T* const gz[3], const Lay* const L[3],
+                         const PipeGeom& G, cudaStream_t s);
+// the pipe's ENO3 self-advection of one component, in place
+template <class T>
+void eno3_pipe(T* comp, const T* gen, const T* gx, const T* gz, const T* ug, const T* vg, const T* wg, const Lay& Lc,
+               const Lay& Lu, const Lay& Lv, const Lay& Lw, int axis, const PipeGeom& G, double dx, double dt,
+               cudaStream_t s);
 // the pipe's dimensionless body force on v (phi with periodic y ghosts)
 template <class T>
 void pipe_forcing(T* v, const T* phi, const Lay& Lv, const Lay& Lc, const PipeGeom& G, double coef, double gdt,

@@ -374,6 +374,43 @@ __global__ void __launch_bounds__(kTX * kTY) k_eno3_mac(const T* __restrict__ co
   }
 }
 
+// The vertical pipe's ENO3 self-advection of component `axis`
+// (ADVECTION_METHOD_3D.h:1935-2240): faces inside the pipe and off the
+// fixed centre line take the ENO3 upwind update in place, the x and z
+// derivatives from the guarded copies gx, gz, the y derivative from the
+// masked periodic copy gen, the advecting velocities from the masked
+// periodic copies ug, vg, wg; the other faces keep their value.  One thread
+// per face: the pipe grids are small and the three stencil sources differ.
+template <class T>
+__global__ void k_eno3_pipe(T* comp, const T* __restrict__ gen, const T* __restrict__ gx, const T* __restrict__ gz,
+                            const T* __restrict__ ug, const T* __restrict__ vg, const T* __restrict__ wg, Lay Lf,
+                            Lay Lu, Lay Lv, Lay Lw, int axis, PipeGeom G, T h, T dt, int fi0, int fi1, int fk0,
+                            int fk1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= Lf.nx || j >= Lf.ny || k >= Lf.nz) return;
+  if ((i == fi0 || i == fi1) && (k == fk0 || k == fk1)) return;  // the fixed centre line
+  if (!(pipe_wall_distance(G, 1 + axis, i, k) < 0.0)) return;
+  const T inv = T(1) / h, o2 = T(0.5) / h, o3 = inv * T(1) / T(3);
+  T vx[7], vy[7], vz[7];
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    vx[q] = gx[Lf.at(i + q - 3, j, k)];
+    vy[q] = gen[Lf.at(i, j + q - 3, k)];
+    vz[q] = gz[Lf.at(i, j, k + q - 3)];
+  }
+  T uvel, vvel, wvel;
+  mac_velocity(ug, vg, wg, Lu, Lv, Lw, axis, i, j, k, uvel, vvel, wvel);
+  T dxm, dxp, dym, dyp, dzm, dzp;
+  eno3_pair7(vx, h, inv, o2, o3, dxm, dxp);
+  eno3_pair7(vy, h, inv, o2, o3, dym, dyp);
+  eno3_pair7(vz, h, inv, o2, o3, dzm, dzp);
+  const int64_t f = Lf.at(i, j, k);
+  comp[f] = comp[f] - dt * ((uvel * (uvel > T(0) ? dxm : dxp) + vvel * (vvel > T(0) ? dym : dyp)) +
+                            wvel * (wvel > T(0) ? dzm : dzp));
+}
+
 // ---------------------------------------------------------------------------
 // Sussman reinitialisation
 // ---------------------------------------------------------------------------
@@ -510,6 +547,22 @@ void eno3_mac(const T* comp, T* out, const T* u, const T* v, const T* w, const L
 }
 
 template <class T>
+void eno3_pipe(T* comp, const T* gen, const T* gx, const T* gz, const T* ug, const T* vg, const T* wg, const Lay& Lc,
+               const Lay& Lu, const Lay& Lv, const Lay& Lw, int axis, const PipeGeom& G, double dx, double dt,
+               cudaStream_t s) {
+  const Lay& Lf = axis == 0 ? Lu : axis == 1 ? Lv : Lw;
+  // the faces Solve_Velocity holds fixed (ADVECTION_3D.h:246-275): the
+  // integer halves of the face grid's last indices
+  int fi0, fi1, fk0, fk1;
+  if (axis == 0) { fi0 = (Lf.nx - 1) / 2; fi1 = fi0 + 1; fk0 = fk1 = (Lc.nz - 1) / 2; }
+  else if (axis == 1) { fi0 = fi1 = (Lc.nx - 1) / 2; fk0 = fk1 = (Lc.nz - 1) / 2; }
+  else { fi0 = fi1 = (Lc.nx - 1) / 2; fk0 = (Lf.nz - 1) / 2; fk1 = fk0 + 1; }
+  Launch3 g = launch3(Lf.nx, Lf.ny, Lf.nz);
+  k_eno3_pipe<T><<<g.grid, g.block, 0, s>>>(comp, gen, gx, gz, ug, vg, wg, Lf, Lu, Lv, Lw, axis, G, T(dx), T(dt), fi0,
+                                            fi1, fk0, fk1);
+}
+
+template <class T>
 void sign_function(const T* phi, T* sgn, const Lay& L, double dx, cudaStream_t s) {
   Launch3 g = launch3(L.nx, L.ny, L.nz);
   k_sign<T><<<g.grid, g.block, 0, s>>>(phi, sgn, L, T(dx));
@@ -548,6 +601,8 @@ void zero_walls(T* f, const Lay& L, int axis, cudaStream_t s) {
                                   const PipeGeom*);                                                                   \
   template void weno5_mac<T>(const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,          \
                              const Lay&, int, double, double, double, cudaStream_t);                                  \
+  template void eno3_pipe<T>(T*, const T*, const T*, const T*, const T*, const T*, const T*, const Lay&, const Lay&,  \
+                             const Lay&, const Lay&, int, const PipeGeom&, double, double, cudaStream_t);             \
   template void eno3_mac<T>(const T*, T*, const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,           \
                             const Lay&, int, double, double, cudaStream_t);                                          \
   template void sign_function<T>(const T*, T*, const Lay&, double, cudaStream_t);                                    \

@@ -139,9 +139,12 @@ typedef struct {
      pipe (PIPE_OPTIONS.is_vertical): 0 (default) the air/water box with walls;
      1 a pipe along y, periodic in y with the reference's node convention (cell
      0 and cell ny-1 are one point), its wall at sqrt(x^2 + z^2) = pipe_radius.
-     Built for the level-set advection, the reinitialisation and the body force
-     (fs_advect_levelset, fs_reinitialize, fs_apply_gravity); the other
-     operators and fs_step return FS_NOT_SUPPORTED in this mode. */
+     Built for the level-set advection, the reinitialisation, the ENO3 velocity
+     advection and the body force (fs_advect_levelset, fs_reinitialize,
+     fs_advect_velocity with velocity_scheme FS_VELOCITY_ENO3,
+     fs_apply_gravity); the viscosity, the projection, the CFL time step,
+     fs_step and the adjoints return FS_NOT_SUPPORTED in this mode.  Fixed at
+     creation. */
   int pipe;
   double pipe_radius;               /* a: the wall radius in units of the core radius R1 */
   double grid_min[3], grid_max[3];  /* the script's base_grid_min and base_grid_max: cell (i,j,k) sits at

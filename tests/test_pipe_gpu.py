@@ -2,10 +2,10 @@
 own outputs (fixtures pipe_*, made by tests/golden/make_golden.py from the
 headless reference build) and against the oracle.
 
-The pipe mode's level-set advection, reinitialisation and dimensionless body
-force run on the GPU; its velocity advection, viscosity and projection are
-not built, and those entry points (and fs_step) return FS_NOT_SUPPORTED in
-this mode."""
+The pipe mode's level-set advection, reinitialisation, ENO3 velocity
+advection and dimensionless body force run on the GPU; its viscosity and
+projection are not built, and those entry points (and fs_step) return
+FS_NOT_SUPPORTED in this mode."""
 import os
 
 import numpy as np
@@ -31,7 +31,7 @@ def solver(g, precision=fs.FS_PRECISION_FP64, flags=fs.FS_FLAG_REINIT_TYPO):
                      pipe_eta=float(g["eta"]), pipe_oil_density=float(g["oil_density"]),
                      gravity=(0.0, float(g["gravity_y"]), 0.0), weno_epsilon=float(g["epsilon"]),
                      reinit_iterations=int(g["reinit_iterations"]), reinit_scaling=int(g["reinit_scaling"]),
-                     flags=flags, viscosity=0)
+                     flags=flags, viscosity=0, velocity_scheme=fs.FS_VELOCITY_ENO3)
 
 
 def upload(s, g, keys=("phi", "u", "v", "w")):
@@ -91,12 +91,30 @@ def test_pipe_forcing_matches_reference(precision, tol):
         assert np.abs(v[fixed] - g["v"][fixed]).max() <= (0.0 if precision == fs.FS_PRECISION_FP64 else 1e-6)
 
 
+@pytest.mark.parametrize("precision,tol", [(fs.FS_PRECISION_FP64, 1e-12), (fs.FS_PRECISION_FP32_REFINE, 2e-5)])
+def test_pipe_velocity_advection_matches_reference(precision, tol):
+    g = load("pipe_velocity")
+    with solver(g, precision) as s:
+        upload(s, g)
+        s.advect_velocity(float(g["dt"]))
+        for k in "uvw":
+            out = s.download(k)
+            ref, inp = g["out_" + k], g[k]
+            scale = max(np.abs(inp).max(), 1.0)
+            assert np.abs(out - ref).max() <= tol * scale, (k, np.abs(out - ref).max())
+            # the fixed centre line and the faces outside the pipe keep their value
+            keep = g["fixed_" + k] | (ref == inp)
+            assert np.abs(out[keep] - inp[keep]).max() <= (0.0 if precision == fs.FS_PRECISION_FP64 else 1e-6)
+        # the level set is not touched
+        assert np.abs(s.download("phi") - g["phi"]).max() <= (0.0 if precision == fs.FS_PRECISION_FP64 else 1e-6)
+
+
 def test_pipe_mode_refuses_the_operators_it_does_not_build():
     g = load("pipe_levelset")
     with solver(g) as s:
         upload(s, g)
-        for call in (lambda: s.step(1e-3), lambda: s.project(1e-3), lambda: s.advect_velocity(1e-3),
-                     lambda: s.viscosity(1e-3), lambda: s.cfl_dt()):
+        for call in (lambda: s.step(1e-3), lambda: s.project(1e-3), lambda: s.viscosity(1e-3),
+                     lambda: s.cfl_dt()):
             with pytest.raises(fs.FsError) as e:
                 call()
             assert e.value.status == fs.FS_NOT_SUPPORTED
