@@ -681,11 +681,14 @@ def jump_rhs(phi, jc, dx, rho_neg, rho_pos, walls=True):
     with jc_on_derivative = 0: an arm whose two cells lie in different phases
     carries F = +-inv_dx2 * a * beta, a = (jc_c |phi_n| + jc_n |phi_c|) /
     (|phi_c| + |phi_n|), + when the cell is in the phi <= 0 phase.  With
-    walls (the reference), arms to the wall ghosts use the extrapolated ghost
-    phi, jc = 0 and the clamped 1/rho; without (corrected), only arms between
-    two cells of the box carry a jump, as only they have a face the velocity
-    update corrects.  Returns (F_X, F_Y, F_Z)."""
-    pg = extrapolate_ghosts(phi, 1)
+    walls (the reference), arms to the wall ghosts are evaluated too, with the
+    ghost phi the reference holds when it builds the system: ComputeNormals
+    (LEVELSET_3D.h:931), called just before, fills the ghosts by copying the
+    nearest cell, so a wall arm never crosses the interface.  Without
+    (corrected), only arms between two cells of the box are evaluated, as
+    only they have a face the velocity update corrects.  Both give the same
+    terms.  Returns (F_X, F_Y, F_Z)."""
+    pg = np.pad(phi, 1, mode="edge")
     var = 1.0 / np.where(phi <= 0, rho_neg, rho_pos)
     vg = np.pad(var, 1, mode="edge")
     jg = np.pad(jc, 1)
@@ -1751,3 +1754,218 @@ def pipe_eno3_velocity(u, v, w, grids, a, dt):
         new = _upwind_update(comps[ax], dt, uvel, vvel, wvel, dxm, dxp, dym, dyp, dzm, dzp)
         out.append(np.where((bs[ax] < 0) & ~fixed[ax], new, comps[ax]))
     return tuple(out)
+
+
+# ----------------------------------------------------------------------------
+# Oil/water pipe mode, vertical pipe: the projection (PROJECTION_3D.h:416-441,
+# 596-834, 849-1097, 1099-1449, 1475-1610; POISSON_SOLVER_3D.h:165-252,
+# 527-552, 1360-1819)
+# ----------------------------------------------------------------------------
+
+def pipe_fluid_cells(grids, shape, a):
+    """The cells that are unknowns of the pipe's pressure system: wall distance
+    <= 0 (SetupBoundaryConditions, Neumann + cylindrical_boundary + is_vertical,
+    PROJECTION_3D.h:1017-1040, marks the others BC_NEUM)."""
+    return pipe_boundary(grids[0], shape, a) <= 0
+
+
+def pipe_density(phi, water_density, oil_density):
+    """DetermineProjectionDensity in the dimensionless form (PROJECTION_3D.h:
+    642-669): 1 in the oil (phi <= 0), water_density/oil_density in the water."""
+    return np.where(phi <= 0, 1.0, water_density / oil_density)
+
+
+def pipe_divergence(u, v, w, grids, a, dt):
+    """DetermineDivergence of the pipe (PROJECTION_3D.h:697-719, 1519-1610):
+    the MAC divergence of the masked periodic velocity copies with the linear
+    wall extrapolation on x and z faces just outside the pipe (the copies the
+    level-set advection reads; the projection's if/else chain prefers the -
+    side where the advection's prefers the +, which differ only on faces
+    outside the pipe with an inside neighbour on both sides, impossible for a
+    convex wall), zero in cells outside the pipe, then scaled by 1/dt."""
+    _, _, _, ug, vg, wg = pipe_levelset_velocities(u, v, w, grids, a)
+    cg = grids[0]
+    d = (1.0 / cg[3]) * (ug[:, :, 1:] - ug[:, :, :-1])
+    d = d + (1.0 / cg[4]) * (vg[:, 1:, :] - vg[:, :-1, :])
+    d = d + (1.0 / cg[5]) * (wg[1:, :, :] - wg[:-1, :, :])
+    d = np.where(pipe_boundary(cg, d.shape, a) > 0, 0.0, d)
+    return d * (1.0 / dt)
+
+
+def _periodic_y_pad1(f):
+    """One ghost layer around a cell field: the y ghosts of interior columns
+    are the periodic images (node convention: ghost -1 is cell ny-2, ghost ny
+    is cell 1; FIELD_STRUCTURE_3D.h:1328-1431), the x and z ghost layers 0."""
+    nz, ny, nx = f.shape
+    out = np.zeros((nz + 2, ny + 2, nx + 2))
+    out[1:-1, 1:-1, 1:-1] = f
+    out[1:-1, 0, 1:-1] = f[:, ny - 2, :]
+    out[1:-1, ny + 1, 1:-1] = f[:, 1, :]
+    return out
+
+
+def pipe_poisson(phi, fluid, var, dx, deflate=True):
+    """The pipe's pressure matrix (oil/water branch of
+    BuildLinearSystemNodeJumpConditionVaribleCoefficient, POISSON_SOLVER_3D.h:
+    1360-1499) in the matrix-free form of poisson_operator: couplings
+    beta/dx^2 only between two unknowns (cells of the pipe), the diagonal the
+    sum of those betas in the order l, r, b, t, d, u; the first unknown in
+    the reference's row order (k, j, i) adds the beta of its down neighbour,
+    a Neumann cell below the pipe's lowest row, computed from that cell's
+    level set and 1/rho (the deflation; its other Neumann arms add 0); a
+    zero sum becomes 1.  Cells outside the pipe get diagonal 1 and no
+    coupling (they are not unknowns)."""
+    nz, ny, nx = phi.shape
+    ab = np.abs(phi)
+
+    def beta(vc, vn, ac, an):
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return vc * vn * (an + ac) / (vn * ac + vc * an)
+
+    bx = np.zeros((nz, ny, nx + 1)); by = np.zeros((nz, ny + 1, nx)); bz = np.zeros((nz + 1, ny, nx))
+    bx[:, :, 1:-1] = np.where(fluid[:, :, :-1] & fluid[:, :, 1:],
+                              beta(var[:, :, :-1], var[:, :, 1:], ab[:, :, :-1], ab[:, :, 1:]), 0.0)
+    by[:, 1:-1, :] = np.where(fluid[:, :-1, :] & fluid[:, 1:, :],
+                              beta(var[:, :-1, :], var[:, 1:, :], ab[:, :-1, :], ab[:, 1:, :]), 0.0)
+    bz[1:-1, :, :] = np.where(fluid[:-1, :, :] & fluid[1:, :, :],
+                              beta(var[:-1, :, :], var[1:, :, :], ab[:-1, :, :], ab[1:, :, :]), 0.0)
+    inv2 = 1.0 / (dx * dx)
+    coef = ((((bx[:, :, :-1] + bx[:, :, 1:]) + by[:, :-1, :]) + by[:, 1:, :]) + bz[:-1, :, :]) + bz[1:, :, :]
+    first = tuple(int(q) for q in np.argwhere(fluid)[0])  # (k, j, i) of row 0
+    if deflate:
+        k, j, i = first
+        vc, vd, ac, ad = var[k, j, i], var[k - 1, j, i], ab[k, j, i], ab[k - 1, j, i]
+        coef[k, j, i] = coef[k, j, i] + vc * vd * (ad + ac) / (vc * ad + vd * ac)
+    coef = np.where(fluid & (coef == 0), 1.0, coef)
+    coef = np.where(fluid, coef, 1.0 / inv2)
+    return bx * inv2, by * inv2, bz * inv2, inv2 * coef, first
+
+
+def pipe_jump_terms(phi, jc, var, dx):
+    """The jump terms F_X, F_Y, F_Z of the pipe's right-hand side
+    (POISSON_SOLVER_3D.h:1690-1788, jc_on_derivative = 0), every arm of an
+    unknown included: arms into Neumann cells too.  The y arms of the first
+    and last rows read the level set's clamped ghost (ComputeNormals,
+    LEVELSET_3D.h:931, fills the ghosts by copying the nearest cell just
+    before the system is built), so they never cross the interface; jc and
+    1/rho carry their periodic images there (PROJECTION_3D.h:778-827)."""
+    pg = np.pad(phi, 1, mode="edge")
+    vg = _periodic_y_pad1(var)
+    jg = _periodic_y_pad1(jc)
+    nz, ny, nx = phi.shape
+    inv2 = 1.0 / (dx * dx)
+
+    def nb(arr, di, dj, dk):
+        return arr[1 + dk:1 + dk + nz, 1 + dj:1 + dj + ny, 1 + di:1 + di + nx]
+
+    pc, vc, jcc = phi, var, jc
+    ac = np.abs(pc)
+    out = []
+    for (lo, hi) in (((-1, 0, 0), (1, 0, 0)), ((0, -1, 0), (0, 1, 0)), ((0, 0, -1), (0, 0, 1))):
+        F = []
+        for d, low in ((lo, True), (hi, False)):
+            pn, vn, jn = nb(pg, *d), nb(vg, *d), nb(jg, *d)
+            an = np.abs(pn)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                a = (jcc * an + jn * ac) / (ac + an)
+                if low:
+                    beta = vc * vn * (an + ac) / (vc * an + vn * ac)
+                else:
+                    beta = vc * vn * (an + ac) / (vn * ac + vc * an)
+            f = np.where((pc <= 0) & (pn > 0), inv2 * a * beta,
+                         np.where((pc > 0) & (pn <= 0), -inv2 * a * beta, 0.0))
+            F.append(f)
+        out.append(F[0] + F[1])
+    return tuple(out)
+
+
+def pipe_velocity_update(u, v, w, p, phi, jc, fluid, first, grids, dt, water_density, oil_density, fixed=None):
+    """UpdateVelocityByPressureGradientVariableDensity of a vertical pipe
+    (PROJECTION_3D.h:1099-1449).  A face whose + side cell is an unknown is
+    updated when its - side cell is one too, or when the + side cell is the
+    first unknown (row index 0 makes bc*bc_nb >= 0 hold against a Neumann
+    cell, whose pressure stays 0); y faces only for 0 < j < ny.  Same-phase
+    faces: -= dt (p_c - p_n)/rho_c/dx with the sharp density of the + side
+    cell; faces crossing the interface: -= dt (p_c - p_n +- gamma)/rho_f/dx,
+    gamma = (jc_c|phi_n| + jc_n|phi_c|)/(|phi_n| + |phi_c|), rho_f = 1 +
+    (water/oil - 1) H(phi_f) with phi_f the face average from the periodic
+    ghost copy and H of epsilon 1.5 dx.  Fixed faces keep their value.  Then
+    the periodic copies: u and w row ny-1 = row 0; v row ny = row 1 and row
+    0 = row ny-1."""
+    cg = grids[0]
+    h = (cg[3], cg[4], cg[5])
+    nz, ny, nx = phi.shape
+    rho_c = pipe_density(phi, water_density, oil_density)
+    pgy = periodic_ghosts_y(phi)[G:G + nz, :, G:G + nx]  # periodic y ghosts, interior columns
+    ratio = water_density / oil_density
+    row0 = np.zeros_like(fluid)
+    row0[first] = True
+    out = [u.copy(), v.copy(), w.copy()]
+    fixed = fixed if fixed is not None else (None, None, None)
+    for axis in range(3):
+        ax = 2 - axis
+        sl_c = [slice(None)] * 3; sl_n = [slice(None)] * 3
+        sl_c[ax] = slice(1, None); sl_n[ax] = slice(0, -1)
+        sl_c, sl_n = tuple(sl_c), tuple(sl_n)
+        ph_c, ph_n = phi[sl_c], phi[sl_n]
+        if axis == 1:
+            face_phi = 0.5 * (pgy[:, G + 1:G + ny, :] + pgy[:, G:G + ny - 1, :])
+        else:
+            face_phi = 0.5 * (ph_c + ph_n)
+        rho_f = 1.0 + (ratio - 1.0) * heaviside_projection(face_phi, 1.5 * h[axis])
+        with np.errstate(invalid="ignore", divide="ignore"):
+            gamma = (jc[sl_c] * np.abs(ph_n) + jc[sl_n] * np.abs(ph_c)) / (np.abs(ph_n) + np.abs(ph_c))
+        dp = p[sl_c] - p[sl_n]
+        same = ph_c * ph_n > 0
+        inv_h = 1.0 / h[axis]
+        upd = np.where(same, dt * dp * (1.0 / rho_c[sl_c]) * inv_h,
+                       np.where(ph_c <= 0, dt * (dp + gamma) * (1.0 / rho_f) * inv_h,
+                                dt * (dp - gamma) * (1.0 / rho_f) * inv_h))
+        ok = fluid[sl_c] & (fluid[sl_n] | row0[sl_c])
+        fs = [slice(None)] * 3
+        fs[ax] = slice(1, -1)
+        fs = tuple(fs)
+        if fixed[axis] is not None:
+            ok = ok & ~fixed[axis][fs]
+        f = out[axis]
+        f[fs] = np.where(ok, f[fs] - upd, f[fs])
+    out[0][:, ny - 1, :] = out[0][:, 0, :]
+    out[1][:, ny, :] = out[1][:, 1, :]
+    out[1][:, 0, :] = out[1][:, ny - 1, :]
+    out[2][:, ny - 1, :] = out[2][:, 0, :]
+    return tuple(out)
+
+
+def pipe_projection(phi, u, v, w, grids, C, dt, tol, max_iter, water_density, oil_density, fixed=None, p0=None,
+                    mode="faithful", criterion="abs"):
+    """PROJECTION_3D::Solve of a vertical pipe with Neumann walls
+    (cylindrical_boundary, dimensionless_form): divergence of the pipe's
+    velocity copies, jump condition jc = kappa/We (PROJECTION_3D.h:758-768),
+    the pipe's matrix (faithful: with the reference's deflation; corrected:
+    the singular consistent system), right-hand side -div - F minus its mean
+    over the unknowns (POISSON_SOLVER_3D.h:225-246), Jacobi-PCG from the
+    previous pressure on the unknowns, and the pipe's velocity update.  The
+    pressure of cells outside the pipe is not touched.  Returns
+    (u, v, w, p, info)."""
+    cg = grids[0]
+    dx = cg[3]
+    fluid = pipe_fluid_cells(grids, phi.shape, C["a"])
+    rho = pipe_density(phi, water_density, oil_density)
+    var = 1.0 / rho
+    div = pipe_divergence(u, v, w, grids, C["a"], dt)
+    kappa, _ = curvature(phi, dx, typo=True)
+    jc = (1.0 / C["We"]) * kappa
+    ax_, ay_, az_, diag, first = pipe_poisson(phi, fluid, var, dx, deflate=(mode == "faithful"))
+    op = (ax_, ay_, az_, diag)
+    FX, FY, FZ = pipe_jump_terms(phi, jc, var, dx)
+    b = np.where(fluid, ((-div - FX) - FY) - FZ, 0.0)
+    nrow = int(fluid.sum())
+    b = np.where(fluid, b - (1.0 / nrow) * _seqsum(b[fluid]), 0.0)
+    p_prev = np.zeros_like(phi) if p0 is None else p0
+    x0 = np.where(fluid, p_prev, 0.0)
+    x, it, rz, rel = pcg(lambda q: apply_poisson(op, q), diag, b, x0, tol, max_iter, criterion)
+    p = np.where(fluid, x, p_prev)
+    u2, v2, w2 = pipe_velocity_update(u, v, w, p, phi, jc, fluid, first, grids, dt, water_density, oil_density,
+                                      fixed)
+    return u2, v2, w2, p, {"iterations": it, "rz": rz, "rel_residual": rel, "b": b, "div": div, "jc": jc,
+                           "fluid": fluid, "op": op}

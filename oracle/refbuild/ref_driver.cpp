@@ -534,4 +534,21 @@ void fsref_pipe_gravity(void* h, double dt) {
   run_threads(c, [&](int t) { s.ApplyGravity(t, dt); });
 }
 
+// EULERIAN_FLUID_SOLVER_3D::Projection of the pipe (EULERIAN_FLUID_SOLVER_3D.h:
+// 2226-2235 -> PROJECTION_3D::Solve, PROJECTION_3D.h:416-441): the cylinder's
+// Neumann cells, the pipe divergence, the jump 1/We kappa, the PCG and the
+// pipe velocity update.  Returns the PCG iteration count.
+int fsref_pipe_projection(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  run_threads(c, [&](int t) { s.Projection(t, dt); });
+  return s.water_projection->poisson_solver.linear_solver->num_iteration;
+}
+
+// The jump condition and the divergence of the last projection (cells).
+void fsref_projection_jc(void* h, double* dst) {
+  PROJECTION_3D& p = *static_cast<RefCase*>(h)->world.eulerian_solver.water_projection;
+  for_interior(p.jc_on_solution, [&](T& v, long n) { dst[n] = v; });
+}
+
 }  // extern "C"

@@ -83,6 +83,10 @@ def _lib():
         for fn in ("fsref_pipe_levelset_advection", "fsref_pipe_velocity_advection", "fsref_pipe_reinitialization",
                    "fsref_pipe_gravity"):
             getattr(lib, fn).argtypes = [ctypes.c_void_p, ctypes.c_double]
+    if hasattr(lib, "fsref_pipe_projection"):
+        lib.fsref_pipe_projection.restype = ctypes.c_int
+        lib.fsref_pipe_projection.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.fsref_projection_jc.argtypes = [ctypes.c_void_p, _dp]
     return lib
 
 
@@ -556,6 +560,16 @@ class RefCase:
 
     def pipe_gravity(self, dt):
         self._quiet(self._lib.fsref_pipe_gravity, self.h, dt)
+
+    def pipe_projection(self, dt):
+        """EULERIAN_FLUID_SOLVER_3D::Projection of the pipe; returns the PCG
+        iteration count."""
+        return self._quiet(self._lib.fsref_pipe_projection, self.h, dt)
+
+    def projection_jc(self):
+        a = np.empty(self.shape("phi"))
+        self._lib.fsref_projection_jc(self.h, _ptr(a))
+        return a
 
     def boundary_faces(self, name):
         """The pipe's boundary level set on the faces of a component, as the

@@ -44,6 +44,10 @@ on the air/water unit-cube box with Neumann pressure walls:
                    pseudo-steps on periodic ghosts)
   pipe_forcing     the pipe's dimensionless body force (ApplyGravity), with
                    the centre-line faces that Solve_Velocity marks fixed
+  pipe_projection  the pipe's Projection: Neumann cells outside the
+                   cylinder, the pipe divergence, jump 1/We kappa, the
+                   deflated system (right-hand side and solution in row
+                   order), PCG and the pipe velocity update
 
     python tests/golden/make_golden.py [name ...]   writes only the named fixtures
 """
@@ -299,6 +303,25 @@ def main():
     c.pipe_gravity(0.01)
     fixtures["pipe_forcing"] = dict(base, dt=0.01, fixed_v=fixed_v, out_u=c.get("u"), out_v=c.get("v"),
                                     out_w=c.get("w"))
+    c.close()
+    # the pipe's projection (EULERIAN_FLUID_SOLVER_3D::Projection): the
+    # centre-line faces marked fixed first, as in a run; the previous
+    # pressure of a fresh case is 0; the system's right-hand side and
+    # solution in the reference's row order pin the matrix assembly
+    c = refsim.RefCase(pipe_sim)
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    c.pipe_velocity_advection(0.0)
+    fixed = {f"fixed_{k}": c.fixed(k) for k in "uvw"}
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    it = c.pipe_projection(0.01)
+    vals, cols, rowptr, b_rows, x_rows = c.poisson_csr()
+    fixtures["pipe_projection"] = dict(base, dt=0.01, tolerance=1e-6, max_iteration=10000, **fixed,
+                                       water_density=const["water_density"], iterations=it,
+                                       div=c.divergence(), jc=c.projection_jc(), csr_vals=vals, csr_cols=cols,
+                                       csr_rowptr=rowptr, b_rows=b_rows, x_rows=x_rows, out_p=c.get("p"),
+                                       out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"))
     c.close()
 
     only = set(sys.argv[1:])

@@ -82,3 +82,29 @@ def test_pipe_velocity_advection_matches_reference():
         np.testing.assert_array_equal(f, g["fixed_" + k])
         # fixed faces and faces outside the pipe keep their value
         np.testing.assert_array_equal(g["out_" + k][f], g[k][f])
+
+
+def test_pipe_projection_matches_reference():
+    """EULERIAN_FLUID_SOLVER_3D::Projection of the pipe, bit for bit: the
+    divergence of the pipe's velocity copies, the deflated system's diagonal,
+    right-hand side (jump terms kappa/We, mean removed over the unknowns) and
+    solution in the reference's row order, the PCG iteration count, the
+    pressure and the updated velocities."""
+    g = load("pipe_projection")
+    C = {k: float(g[k]) for k in ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We")}
+    fixed = (g["fixed_u"], g["fixed_v"], g["fixed_w"])
+    u, v, w, p, info = O.pipe_projection(g["phi"], g["u"], g["v"], g["w"], grids(g), C, float(g["dt"]),
+                                         float(g["tolerance"]), int(g["max_iteration"]), float(g["water_density"]),
+                                         float(g["oil_density"]), fixed=fixed)
+    fl = info["fluid"]
+    assert fl.sum() == len(g["b_rows"])
+    np.testing.assert_array_equal(info["div"], g["div"])
+    np.testing.assert_array_equal(info["jc"][fl], g["jc"][fl])
+    vals, rp = g["csr_vals"], g["csr_rowptr"]
+    np.testing.assert_array_equal(info["op"][3][fl], vals[rp[1:] - 1])  # the diagonal is each row's last entry
+    np.testing.assert_array_equal(info["b"][fl], g["b_rows"])
+    assert info["iterations"] == int(g["iterations"])
+    np.testing.assert_array_equal(p[fl], g["x_rows"])
+    np.testing.assert_array_equal(p, g["out_p"])
+    for k, a in zip("uvw", (u, v, w)):
+        np.testing.assert_array_equal(a, g["out_" + k])
