@@ -72,7 +72,8 @@ class Params(ctypes.Structure):
                 # oil/water vertical pipe mode (0: the box)
                 ("pipe", ctypes.c_int), ("pipe_radius", ctypes.c_double), ("grid_min", ctypes.c_double * 3),
                 ("grid_max", ctypes.c_double * 3), ("pipe_R1", ctypes.c_double), ("pipe_V0", ctypes.c_double),
-                ("pipe_f", ctypes.c_double), ("pipe_eta", ctypes.c_double), ("pipe_oil_density", ctypes.c_double)]
+                ("pipe_f", ctypes.c_double), ("pipe_eta", ctypes.c_double), ("pipe_oil_density", ctypes.c_double),
+                ("pipe_We", ctypes.c_double)]
 
     def as_dict(self):
         d = {}

@@ -240,6 +240,11 @@ fs_status check_params(const fs_params* p) {
     set_error("unknown pressure preconditioner %d for this precision", p->pressure_preconditioner);
     return FS_INVALID_ARG;
   }
+  if (p->pipe && (p->pressure_preconditioner == FS_PRECOND_RED_BLACK ||
+                  p->pressure_preconditioner == FS_PRECOND_RED_BLACK_JACOBI)) {
+    set_error("the pipe mode's pressure solve takes the Jacobi preconditioners only");
+    return FS_INVALID_ARG;
+  }
   if (!(p->reliable_delta >= 0.0 && p->reliable_delta < 1.0)) {
     set_error("reliable_delta must be in [0, 1)");
     return FS_INVALID_ARG;
@@ -267,8 +272,10 @@ void apply_params(fs_ctx* c) {
   c->flux32 = p.flux_arithmetic;
   c->lean = p.pressure_preconditioner != FS_PRECOND_JACOBI;
   // FP32_REFINE: the default is red-black IC(0), which halves the
-  // iterations of the Jacobi-PCG (FP64 keeps the reference's Jacobi)
-  c->red_black = c->fp32 && (p.pressure_preconditioner == FS_PRECOND_DEFAULT ||
+  // iterations of the Jacobi-PCG (FP64 keeps the reference's Jacobi); the
+  // pipe mode's default is the bf16 Jacobi (its red cells would need the
+  // pipe's Neumann cells in the FP64 elimination)
+  c->red_black = c->fp32 && !p.pipe && (p.pressure_preconditioner == FS_PRECOND_DEFAULT ||
                               p.pressure_preconditioner == FS_PRECOND_RED_BLACK ||
                               p.pressure_preconditioner == FS_PRECOND_RED_BLACK_JACOBI);
   c->rb_ic0 = p.pressure_preconditioner != FS_PRECOND_RED_BLACK_JACOBI;
@@ -281,6 +288,10 @@ void apply_params(fs_ctx* c) {
 // with the deflation the first cell's divergence would carry the sum of the
 // residual, e0 p0 = -sum(r).
 int deflate(const fs_ctx* c) { return (c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) ? 1 : 0; }
+// The pipe's geometry for the projection kernels (nullptr in the box) and the
+// cell that carries the deflation (-1: cell (0,0,0) of the box).
+const PipeGeom* pipe_of(const fs_ctx* c) { return c->pipe.on ? &c->pipe : nullptr; }
+int64_t deflated_cell(const fs_ctx* c) { return c->pipe.on ? c->Lc.at(c->pipe.fi, c->pipe.fj, c->pipe.fk) : -1; }
 
 // The oil/water vertical pipe: its grids as the reference computes them (cell
 // spacing (max - min)/(n - 1); each face grid reaches half a cell further on
@@ -301,8 +312,10 @@ fs_status setup_pipe(fs_ctx* c) {
     }
   }
   if (!(p.pipe_radius > 0) || !(p.pipe_R1 > 0) || !(p.pipe_V0 != 0) || !std::isfinite(p.pipe_V0) ||
-      !std::isfinite(p.pipe_f) || !(p.pipe_eta > 0) || !(p.pipe_oil_density > 0)) {
-    set_error("pipe mode: pipe_radius, pipe_R1, pipe_eta, pipe_oil_density must be positive, pipe_V0 non-zero");
+      !std::isfinite(p.pipe_f) || !(p.pipe_eta > 0) || !(p.pipe_oil_density > 0) || !(p.pipe_We > 0) ||
+      !std::isfinite(p.pipe_We)) {
+    set_error("pipe mode: pipe_radius, pipe_R1, pipe_eta, pipe_oil_density, pipe_We must be positive, pipe_V0 "
+              "non-zero");
     return FS_INVALID_ARG;
   }
   if (n[1] < 5) { set_error("pipe mode: the pipe needs at least 5 cells along y"); return FS_INVALID_ARG; }
@@ -330,15 +343,34 @@ fs_status setup_pipe(fs_ctx* c) {
         return FS_INVALID_ARG;
       }
     }
+  // the unknowns of the pressure system: every cell of a column inside the
+  // pipe (wall distance <= 0, pipe_solid's test in the same rounding); the
+  // first in the reference's row order (k, j, i) carries the deflation
+  G.fi = G.fj = G.fk = -1;
+  int64_t columns = 0;
+  for (int k = 0; k < n[2]; ++k)
+    for (int i = 0; i < n[0]; ++i) {
+      const double X = G.ox[0] + i * G.hx[0], Z = G.oz[0] + k * G.hz[0];
+      if (!(std::sqrt(X * X + Z * Z) - G.a > 0.0)) {
+        if (G.fk < 0) { G.fi = i; G.fj = 0; G.fk = k; }
+        ++columns;
+      }
+    }
+  if (columns == 0) {
+    set_error("pipe mode: no cell of the grid lies inside the pipe");
+    c->pipe = PipeGeom{};
+    return FS_INVALID_ARG;
+  }
+  G.cells = columns * n[1];
   return FS_OK;
 }
 
 // Operators of the box only: the pipe mode builds its level-set path, its
-// ENO3 velocity advection and its body force, not yet its viscosity and
-// projection.
+// ENO3 velocity advection, its body force and its projection, not yet its
+// viscosity (and so neither its whole step).
 fs_status box_only(const fs_ctx* c, const char* what) {
   if (!c->pipe.on) return FS_OK;
-  set_error("%s is not built for the oil/water pipe mode (its viscosity and projection are not built)", what);
+  set_error("%s is not built for the oil/water pipe mode (its viscosity is not built)", what);
   return FS_NOT_SUPPORTED;
 }
 
@@ -711,8 +743,9 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
   const bool rb = c->red_black;
   build_pressure_operator<S, float>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (float*)c->pax, (float*)c->pay,
                                     (float*)c->paz, (float*)c->pdiag, c->scalars + 12, deflate(c), s,
-                                    (c->lean || rb) ? c->pdinv : nullptr);
+                                    (c->lean || rb) ? c->pdinv : nullptr, pipe_of(c));
   Op7<float> A{(float*)c->pax, (float*)c->pay, (float*)c->paz, (float*)c->pdiag, c->Lc, 1, c->scalars + 12};
+  A.c_extra = deflated_cell(c);
   A.flux32 = c->flux32;
   if (c->lean) A.dinv16 = c->pdinv;
   // red-black: the black Schur complement on the packed half layout, its
@@ -746,7 +779,7 @@ fs_status mixed_solve(fs_ctx* c, S* phi, double* b, double* x, int* iters_out, i
   // residual), the Krylov residual of the mixed solve
   auto defect = [&](const float* x32, double* rel_out) -> fs_status {
     defect_residual<S>(phi, x, x32, b, nullptr, r32, c->Lc, dx, P.rho_neg, P.rho_pos, c->partials,
-                       c->tickets + 2, c->scalars + 2, deflate(c), s);
+                       c->tickets + 2, c->scalars + 2, deflate(c), s, pipe_of(c));
     c->launches += 1;
     if (rb) {
       rb_gather<float, float>(r32, c->rb_r, c->Lc, c->Lh, s);
@@ -872,44 +905,62 @@ fs_status project_t(fs_ctx* c, double dt, double c0, double c1, fs_solve_report*
   const double dx = c->grid.dx;
   cudaStream_t s = c->stream;
   const bool faithful = (P.flags & FS_FLAG_FAITHFUL_PROJECTION) != 0;
+  const bool pipe = c->pipe.on != 0;
   S *u = F<S>(c->u), *v = F<S>(c->v), *w = F<S>(c->w), *phi = F<S>(c->phi);
-  divergence_rhs<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, dt, c->b64, c->div64, c->partials, c->tickets + 0,
-                    c->scalars + 0, s);
+  if (pipe) {
+    // the vertical pipe (PROJECTION_3D.h:416-441 with oil_water_simulation):
+    // the divergence of the pipe's velocity copies on the cells inside it
+    pipe_divergence_rhs<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, c->pipe, dx, dt, c->b64, c->div64, c->partials,
+                           c->tickets + 0, c->scalars + 0, s);
+  } else {
+    divergence_rhs<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, dt, c->b64, c->div64, c->partials, c->tickets + 0,
+                      c->scalars + 0, s);
+  }
   // surface tension: curvature, jc = sigma kappa, and the jump terms of the
-  // right-hand side (DetermineJumpConditionField, PROJECTION_3D.h:746-792)
-  const double sigma = P.surface_tension;
+  // right-hand side (DetermineJumpConditionField, PROJECTION_3D.h:746-792);
+  // the pipe's dimensionless form always carries jc = kappa/We (:758-762)
+  const double sigma = pipe ? 1.0 / P.pipe_We : P.surface_tension;
   const double* kap = nullptr;
   if (sigma != 0.0) {
-    fill_extrap<S>(phi, c->Lc, s);
+    fill_extrap<S>(phi, c->Lc, s);  // the curvature's ghost fill (LEVELSET_3D.h:999), the pipe's too
     curvature<S>(phi, c->kappa, c->Lc, dx, (P.flags & FS_FLAG_CURVATURE_TYPO) ? 1 : 0, c->scalars + 13, s);
     jump_rhs<S>(phi, c->kappa, sigma, c->b64, c->Lc, dx, P.rho_neg, P.rho_pos, faithful ? 1 : 0, c->partials,
-                c->tickets + 5,
-                c->scalars + 0, s);
+                c->tickets + 5, c->scalars + 0, s, pipe_of(c));
     kap = c->kappa;
     c->launches += 3;
   }
-  subtract_mean(c->b64, c->Lc, c->scalars + 0, c->partials, c->tickets + 1, c->scalars + 1, s);
+  subtract_mean(c->b64, c->Lc, c->scalars + 0, c->partials, c->tickets + 1, c->scalars + 1, s, pipe_of(c));
   c->launches += 4;  // divergence, mean, pressure faces, pressure diagonal
   CK(cudaGetLastError());
   int iters = 0, outer = 0, st = 0;
   double rel = 0.0;
   if (!c->fp32) {
     build_pressure_operator<S, double>(phi, c->Lc, dx, P.rho_neg, P.rho_pos, (double*)c->pax, (double*)c->pay,
-                                       (double*)c->paz, (double*)c->pdiag, c->scalars + 12, deflate(c), s);
+                                       (double*)c->paz, (double*)c->pdiag, c->scalars + 12, deflate(c), s, nullptr,
+                                       pipe_of(c));
     Op7<double> A{(double*)c->pax, (double*)c->pay, (double*)c->paz, (double*)c->pdiag, c->Lc, 1, c->scalars + 12};
+    A.c_extra = deflated_cell(c);
     CKS(run_pcg<double>(c, 1, A, c->b64, c->p64, (double*)c->pr, (double*)c->pp, (double*)c->pq, P.tolerance,
                         P.max_iteration, P.stop, &iters, &rel, &st));
     outer = 1;
   } else {
     CKS(mixed_solve<S>(c, phi, c->b64, c->p64, &iters, &outer, &rel, &st));
   }
-  velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
-                      kap, sigma, s);
-  velocity_correct<S>(v, F<S>(c->v0), c->p64, phi, c->Lv, c->Lc, 1, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
-                      kap, sigma, s);
-  velocity_correct<S>(w, F<S>(c->w0), c->p64, phi, c->Lw, c->Lc, 2, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
-                      kap, sigma, s);
-  c->launches += 3;
+  if (pipe) {
+    // the pipe's velocity update and periodic rows (PROJECTION_3D.h:1099-1449);
+    // the RK combination, if any, is the caller's
+    pipe_velocity_correct<S>(u, v, w, c->p64, phi, c->kappa, c->Lc, c->Lu, c->Lv, c->Lw, c->pipe, dx, dt, P.rho_neg,
+                             P.rho_pos, sigma, s);
+    c->launches += 4;
+  } else {
+    velocity_correct<S>(u, F<S>(c->u0), c->p64, phi, c->Lu, c->Lc, 0, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
+                        kap, sigma, s);
+    velocity_correct<S>(v, F<S>(c->v0), c->p64, phi, c->Lv, c->Lc, 1, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
+                        kap, sigma, s);
+    velocity_correct<S>(w, F<S>(c->w0), c->p64, phi, c->Lw, c->Lc, 2, dx, dt, P.rho_neg, P.rho_pos, faithful, c0, c1,
+                        kap, sigma, s);
+    c->launches += 3;
+  }
   CK(cudaGetLastError());
   if (rep) {
     divergence_norms<S>(u, v, w, c->Lc, c->Lu, c->Lv, c->Lw, dx, c->partials, c->tickets + 3, c->scalars + 4, s);
@@ -1825,7 +1876,6 @@ fs_status fs_cfl_dt(fs_ctx* c, double* dt) {
 
 fs_status fs_project(fs_ctx* c, double dt, fs_solve_report* rep) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
-  CKS(box_only(c, "fs_project"));
   if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
   fs_solve_report local{};
   fs_solve_report* r = rep ? rep : &local;

@@ -17,12 +17,22 @@ struct PipeGeom {
   int on;  // 0: the box
   double a;
   double ox[4], oz[4], hx[4], hz[4];
+  // the first unknown of the pressure system in the reference's row order
+  // (k, j, i): the cell that carries the faithful projection's deflation
+  int fi, fj, fk;
+  int64_t cells;  // unknowns of the pressure system (cells inside the pipe)
 };
 // sqrt(x^2 + z^2) - a at point (i, k) of grid g, in the reference's rounding
 __device__ __forceinline__ double pipe_wall_distance(const PipeGeom& G, int g, int i, int k) {
   const double X = __dadd_rn(G.ox[g], __dmul_rn((double)i, G.hx[g]));
   const double Z = __dadd_rn(G.oz[g], __dmul_rn((double)k, G.hz[g]));
   return __dsub_rn(sqrt(__dadd_rn(__dmul_rn(X, X), __dmul_rn(Z, Z))), G.a);
+}
+// A cell of the box that is no unknown of the pipe's pressure system: wall
+// distance > 0, the reference's Neumann cells (PROJECTION_3D.h:1017-1040).
+// Always false in the box.
+__device__ __forceinline__ bool pipe_solid(const PipeGeom& G, int i, int k) {
+  return G.on && pipe_wall_distance(G, 0, i, k) > 0.0;
 }
 // periodic ghosts along y of a cell field (cell 0 and cell ny-1 are one
 // point); the x and z ghost layers become 0
@@ -47,6 +57,18 @@ void eno3_pipe(T* comp, const T* gen, const T* gx, const T* gz, const T* ug, con
 template <class T>
 void pipe_forcing(T* v, const T* phi, const Lay& Lv, const Lay& Lc, const PipeGeom& G, double coef, double gdt,
                   double fdt, double oil_density, double eta, double eps, cudaStream_t s);
+// the pipe's projection: b = -(div u)/dt on the unknowns from the pipe's
+// velocity copies (0 elsewhere) with sum(b) in scalars[0]; the pipe's
+// velocity update and its periodic rows (pressure p in FP64, kappa the
+// curvature, jc = sigma kappa)
+template <class T>
+void pipe_divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+                         const Lay& Lw, const PipeGeom& G, double dx, double dt, double* b, double* div_out,
+                         double* partials, unsigned int* ticket, double* scalars, cudaStream_t s);
+template <class T>
+void pipe_velocity_correct(T* u, T* v, T* w, const double* p, const T* phi, const double* kappa, const Lay& Lc,
+                           const Lay& Lu, const Lay& Lv, const Lay& Lw, const PipeGeom& G, double dx, double dt,
+                           double rho_neg, double rho_pos, double sigma, cudaStream_t s);
 template <class T>
 void weno5_levelset(const T* src, const T* base, T* out, const T* u, const T* v, const T* w, const Lay& L,
                     const Lay& Lu, const Lay& Lv, const Lay& Lw, double dx, double eps, double dt, double c0, double c1,
@@ -124,7 +146,8 @@ template <class V> struct Op7 {
   const V* diag;
   Lay L;
   int flux_form = 0;
-  const double* extra0 = nullptr;  // device scalar: diag - sum of couplings at cell (0,0,0)
+  const double* extra0 = nullptr;  // device scalar: diag - sum of couplings at the deflated cell
+  int64_t c_extra = -1;            // the deflated cell (-1: cell (0,0,0) of the box)
   // flux form with FP32 vectors: 0 sums FP64 fluxes formed from exact FP64
   // differences and products; 1 forms each flux in FP32 (difference and
   // product correctly rounded) and sums them in FP64; 2 does all in FP32.
@@ -204,19 +227,25 @@ template <class T>
 void divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
                     double dx, double dt, double* b, double* div_out, double* partials, unsigned int* ticket,
                     double* scalars, cudaStream_t s);
+// pipe: only the unknowns (cells inside the pipe) count and change
 void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* partials, unsigned int* ticket,
-                   double* scalars_out, cudaStream_t s);
+                   double* scalars_out, cudaStream_t s, const PipeGeom* pipe = nullptr);
 template <class T, class V>
 // deflate: the reference's fix of the first cell (the betas of its bottom and
 // down Neumann ghosts added to its diagonal, POISSON_SOLVER_3D.h:1145-1179),
 // which makes the Neumann system nonsingular; without it the system is
 // singular and consistent (b has zero mean) and CG solves it as such.
+// pipe: couplings only between two cells inside the pipe (the others are
+// Neumann cells, no unknowns: zero couplings, diagonal 1); the deflation of
+// the faithful system sits on the pipe's first unknown and adds the beta of
+// its down neighbour (POISSON_SOLVER_3D.h:1451-1486).
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
-                             V* diag, double* extra0, int deflate, cudaStream_t s, unsigned short* dinv16 = nullptr);
+                             V* diag, double* extra0, int deflate, cudaStream_t s, unsigned short* dinv16 = nullptr,
+                             const PipeGeom* pipe = nullptr);
 template <class T>
 void defect_residual(const T* phi, const double* p64, const float* x32, const double* b, double* r64, float* r32,
                      const Lay& Lc, double dx, double rho_neg, double rho_pos, double* partials, unsigned int* ticket,
-                     double* rr_out, int deflate, cudaStream_t s);
+                     double* rr_out, int deflate, cudaStream_t s, const PipeGeom* pipe = nullptr);
 void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s);
 template <class T>
 void velocity_correct(T* f, const T* base, const double* p, const T* phi, const Lay& Lf, const Lay& Lc, int axis,
@@ -225,12 +254,14 @@ void velocity_correct(T* f, const T* base, const double* p, const T* phi, const 
 // mean curvature of phi (ghosts must be filled) and max |kappa| near the interface
 template <class T>
 void curvature(const T* phi, double* kappa, const Lay& L, double dx, int typo, double* kmax, cudaStream_t s);
-// ghost-fluid jump terms of the pressure right-hand side (ghosts of phi filled);
-// walls: arms to the wall ghosts carry jumps too (the reference's system);
-// sum(b) of the result lands in sum_out
+// ghost-fluid jump terms of the pressure right-hand side (arms to interior
+// cells; the reference's wall arms never cross the interface, and `walls` is
+// kept for the call sites only); sum(b) of the result lands in sum_out;
+// pipe: only the unknowns (cells inside the pipe) get terms and count
 template <class T>
 void jump_rhs(const T* phi, const double* kappa, double sigma, double* b, const Lay& Lc, double dx, double rho_neg,
-              double rho_pos, int walls, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s);
+              double rho_pos, int walls, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s,
+              const PipeGeom* pipe = nullptr);
 template <class T>
 void divergence_norms(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv, const Lay& Lw,
                       double dx, double* partials, unsigned int* ticket, double* out2, cudaStream_t s);

@@ -75,7 +75,7 @@ __device__ __forceinline__ X apply7(const Op7<V>& A, const X* __restrict__ x, in
     double acc = (double)A.ax[c] * (d - (double)x[c - 1]) + (double)A.ax[c + 1] * (d - (double)x[c + 1]);
     acc += (double)A.ay[c] * (d - (double)x[c - sy]) + (double)A.ay[c + sy] * (d - (double)x[c + sy]);
     acc += (double)A.az[c] * (d - (double)x[c - sz]) + (double)A.az[c + sz] * (d - (double)x[c + sz]);
-    if (c == A.L.at(0, 0, 0)) acc += (*A.extra0) * d;
+    if (c == (A.c_extra >= 0 ? A.c_extra : A.L.at(0, 0, 0))) acc += (*A.extra0) * d;
     return (X)acc;
   }
   X acc = (X)A.diag[c] * xc;
@@ -344,7 +344,7 @@ __device__ __forceinline__ void spmv_row4(const Op7<V>& A, const V* __restrict__
     pr = p[c + 4];
     axr = A.ax[c + 4];
   }
-  const int64_t c00 = A.L.at(0, 0, 0);
+  const int64_t c00 = A.c_extra >= 0 ? A.c_extra : A.L.at(0, 0, 0);
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
     const V xc = lane(pc, m);

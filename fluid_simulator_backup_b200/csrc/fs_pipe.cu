@@ -276,12 +276,181 @@ void pipe_forcing(T* v, const T* phi, const Lay& Lv, const Lay& Lc, const PipeGe
                                                 1.0 / kPi, (Lc.nx - 1) / 2, (Lc.nz - 1) / 2);
 }
 
+// ---- the pipe's projection (PROJECTION_3D.h:681-744, 1099-1449, 1519-1610)
+
+// The velocity of face (i, j, k) as the pipe's divergence reads it
+// (SetupBoundaryConditionsForVelocityDivergence, PROJECTION_3D.h:1519-1610):
+// x and z faces outside the pipe (b > 0) take 0 when all four transverse
+// neighbours are outside, else the linear extrapolation across the wall,
+// (theta - 1)/theta times the inside neighbour along the axis, the - side
+// first, theta = |b_in|/(|b_in| + |b|) (neighbours beyond the face grid have
+// b = 0, the boundary array's unfilled ghost layer); the other faces the
+// masked periodic copy: the face's own velocity where b < 1e-8 (for the y
+// component face 0 reads face ny-1 and face ny face 1), else 0.
+template <class T, int AXIS>
+__device__ __forceinline__ double pipe_div_face(const T* __restrict__ vel, const Lay& Lf, const PipeGeom& G, int i,
+                                                int j, int k) {
+  const int g = 1 + AXIS;
+  const double b = pipe_wall_distance(G, g, i, k);
+  if (AXIS != 1 && b > 0.0) {
+    auto bd = [&](int ii, int kk) -> double {
+      return (ii < 0 || ii >= Lf.nx || kk < 0 || kk >= Lf.nz) ? 0.0 : pipe_wall_distance(G, g, ii, kk);
+    };
+    if (bd(i - 1, k) > 0.0 && bd(i + 1, k) > 0.0 && bd(i, k - 1) > 0.0 && bd(i, k + 1) > 0.0) return 0.0;
+    for (int s = -1; s <= 1; s += 2) {
+      const int ii = AXIS == 0 ? i + s : i, kk = AXIS == 0 ? k : k + s;
+      const double bn = bd(ii, kk);
+      if (bn < 0.0) {
+        const double theta = fabs(bn) / (fabs(bn) + fabs(b));
+        return (theta - 1.0) / theta * (double)vel[Lf.at(ii, j, kk)];
+      }
+    }
+    return 0.0;
+  }
+  if (b < 1e-8) {
+    if (AXIS == 1 && j == 0) return (double)vel[Lf.at(i, Lf.ny - 2, k)];
+    if (AXIS == 1 && j == Lf.ny - 1) return (double)vel[Lf.at(i, 1, k)];
+    return (double)vel[Lf.at(i, j, k)];
+  }
+  return 0.0;
+}
+
+// b = -(div u)/dt on the cells inside the pipe, 0 on the others (no
+// unknowns), and sum(b) for the mean removal (DetermineDivergence,
+// PROJECTION_3D.h:697-722: one_over_dx (u_r - u_l) + one_over_dy (v_t - v_b)
+// + one_over_dz (w_u - w_d) in that order, then times 1/dt).
+template <class T>
+__global__ void k_pipe_divergence_rhs(const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w,
+                                      Lay Lc, Lay Lu, Lay Lv, Lay Lw, PipeGeom G, double inv_h, double inv_dt,
+                                      double* __restrict__ b, double* __restrict__ div_out, double* partials,
+                                      unsigned int* ticket, double* scalars) {
+  double bv = 0.0;
+  Cursor cur;
+  for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
+    const int i = cur.i, j = cur.j, k = cur.k;
+    const int64_t c = Lc.at(i, j, k);
+    if (pipe_solid(G, i, k)) {
+      div_out[c] = 0.0;
+      b[c] = 0.0;
+      continue;
+    }
+    double d = inv_h * (pipe_div_face<T, 0>(u, Lu, G, i + 1, j, k) - pipe_div_face<T, 0>(u, Lu, G, i, j, k));
+    d += inv_h * (pipe_div_face<T, 1>(v, Lv, G, i, j + 1, k) - pipe_div_face<T, 1>(v, Lv, G, i, j, k));
+    d += inv_h * (pipe_div_face<T, 2>(w, Lw, G, i, j, k + 1) - pipe_div_face<T, 2>(w, Lw, G, i, j, k));
+    const double dv = d * inv_dt;
+    div_out[c] = dv;
+    b[c] = -dv;
+    bv += -dv;
+  }
+  bv = block_sum(bv);
+  double tot;
+  if (grid_reduce_sum(bv, partials, ticket, &tot)) scalars[0] = tot;
+}
+
+// UpdateVelocityByPressureGradientVariableDensity of a vertical pipe
+// (PROJECTION_3D.h:1151-1449), one component.  Face (i, j, k) lies between
+// cell c = (i, j, k) and cell n one step back along the axis.  It is updated
+// when it is not one of the centre-line faces Solve_Velocity holds fixed,
+// c is an unknown (inside the pipe) and n is one too or c is the first
+// unknown (its row index 0 makes the reference's bc*bc_n >= 0 hold against
+// a Neumann cell, whose pressure the solve never writes); y faces only for
+// 0 < j < ny.  Same-phase faces: -= dt (p_c - p_n)/rho_c/h with the sharp
+// density of c; faces with phi_c phi_n <= 0: -= dt (p_c - p_n +- gamma)/
+// rho_f/h, gamma = (jc_c|phi_n| + jc_n|phi_c|)/(|phi_n| + |phi_c|), jc =
+// sigma kappa, + when phi_c <= 0, rho_f = rn + (rp - rn) H(phi_f) with phi_f
+// the face average and H the projection's smeared Heaviside of epsilon eps.
+template <class T, int AXIS>
+__global__ void k_pipe_velocity_correct(T* __restrict__ f, const double* __restrict__ p, const T* __restrict__ phi,
+                                        const double* __restrict__ kappa, Lay Lf, Lay Lc, PipeGeom G, double inv_h,
+                                        double dt, double rn, double rp, double sigma, double eps, int fi0, int fi1,
+                                        int fk0, int fk1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= Lf.nx || j >= Lf.ny || k >= Lf.nz) return;
+  if ((i == fi0 || i == fi1) && (k == fk0 || k == fk1)) return;  // the fixed centre line
+  if (AXIS == 1 && (j == 0 || j >= Lc.ny)) return;
+  if (AXIS == 0 && i >= Lc.nx) return;  // the last face's + cell is the Neumann ghost layer
+  if (AXIS == 2 && k >= Lc.nz) return;
+  if (pipe_solid(G, i, k)) return;
+  const int in = AXIS == 0 ? i - 1 : i, jn = AXIS == 1 ? j - 1 : j, kn = AXIS == 2 ? k - 1 : k;
+  const bool first = i == G.fi && j == G.fj && k == G.fk;
+  if (in < 0 || kn < 0 || (pipe_solid(G, in, kn) && !first)) return;
+  const int64_t c = Lc.at(i, j, k), n = Lc.at(in, jn, kn);
+  const double pc = (double)phi[c], pn = (double)phi[n];
+  const double dp = p[c] - p[n];
+  const int64_t fo = Lf.at(i, j, k);
+  double val = (double)f[fo];
+  if (pc * pn > 0.0) {
+    val -= dt * dp * (1.0 / (pc <= 0.0 ? rn : rp)) * inv_h;
+  } else {
+    const double jc = sigma * kappa[c], jn = sigma * kappa[n];
+    const double ac = fabs(pc), an = fabs(pn);
+    const double gamma = (jc * an + jn * ac) / (an + ac);
+    const double pf = 0.5 * (pc + pn);
+    double h;
+    if (pf < -eps) h = 0.0;
+    else if (pf > eps) h = 1.0;
+    else h = (0.5 + pf * (1.0 / eps) * 0.5) + 0.5 * (1.0 / kPi) * sin(kPi * pf * (1.0 / eps));
+    const double inv_rf = 1.0 / (rn + (rp - rn) * h);
+    val -= dt * (pc <= 0.0 ? dp + gamma : dp - gamma) * inv_rf * inv_h;
+  }
+  f[fo] = (T)val;
+}
+
+// The periodic rows the pipe's velocity update ends with: u and w row ny-1
+// takes row 0; v row ny takes row 1 and row 0 takes row ny-1.
+template <class T>
+__global__ void k_pipe_periodic_rows(T* u, T* v, T* w, Lay Lu, Lay Lv, Lay Lw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < Lu.nx && k < Lu.nz) u[Lu.at(i, Lu.ny - 1, k)] = u[Lu.at(i, 0, k)];
+  if (i < Lv.nx && k < Lv.nz) {
+    v[Lv.at(i, Lv.ny - 1, k)] = v[Lv.at(i, 1, k)];
+    v[Lv.at(i, 0, k)] = v[Lv.at(i, Lv.ny - 2, k)];
+  }
+  if (i < Lw.nx && k < Lw.nz) w[Lw.at(i, Lw.ny - 1, k)] = w[Lw.at(i, 0, k)];
+}
+
+template <class T>
+void pipe_divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay& Lu, const Lay& Lv,
+                         const Lay& Lw, const PipeGeom& G, double dx, double dt, double* b, double* div_out,
+                         double* partials, unsigned int* ticket, double* scalars, cudaStream_t s) {
+  k_pipe_divergence_rhs<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(u, v, w, Lc, Lu, Lv, Lw, G, 1.0 / dx, 1.0 / dt, b,
+                                                                  div_out, partials, ticket, scalars);
+}
+
+template <class T>
+void pipe_velocity_correct(T* u, T* v, T* w, const double* p, const T* phi, const double* kappa, const Lay& Lc,
+                           const Lay& Lu, const Lay& Lv, const Lay& Lw, const PipeGeom& G, double dx, double dt,
+                           double rho_neg, double rho_pos, double sigma, cudaStream_t s) {
+  const double eps = 1.5 * dx, inv_h = 1.0 / dx;
+  // the faces Solve_Velocity holds fixed (ADVECTION_3D.h:246-275), as eno3_pipe
+  const int ci = (Lc.nx - 1) / 2, ck = (Lc.nz - 1) / 2;
+  Launch3 a = launch3(Lu.nx, Lu.ny, Lu.nz), b = launch3(Lv.nx, Lv.ny, Lv.nz), c = launch3(Lw.nx, Lw.ny, Lw.nz);
+  k_pipe_velocity_correct<T, 0><<<a.grid, a.block, 0, s>>>(u, p, phi, kappa, Lu, Lc, G, inv_h, dt, rho_neg, rho_pos,
+                                                           sigma, eps, (Lu.nx - 1) / 2, (Lu.nx - 1) / 2 + 1, ck, ck);
+  k_pipe_velocity_correct<T, 1><<<b.grid, b.block, 0, s>>>(v, p, phi, kappa, Lv, Lc, G, inv_h, dt, rho_neg, rho_pos,
+                                                           sigma, eps, ci, ci, ck, ck);
+  k_pipe_velocity_correct<T, 2><<<c.grid, c.block, 0, s>>>(w, p, phi, kappa, Lw, Lc, G, inv_h, dt, rho_neg, rho_pos,
+                                                           sigma, eps, ci, ci, (Lw.nz - 1) / 2, (Lw.nz - 1) / 2 + 1);
+  const dim3 rb(32, 4);
+  const dim3 rg((Lu.nx + 31) / 32, (Lw.nz + 3) / 4);
+  k_pipe_periodic_rows<T><<<rg, rb, 0, s>>>(u, v, w, Lu, Lv, Lw);
+}
+
 #define FS_PIPE_INST(T)                                                                                          \
   template void fill_periodic_y<T>(T*, const Lay&, cudaStream_t);                                              \
   template void pipe_levelset_velocities<T>(T*, T*, T*, T*, T*, T*, const Lay&, const Lay&, const Lay&,          \
                                             const PipeGeom&, cudaStream_t);                                     \
   template void pipe_forcing<T>(T*, const T*, const Lay&, const Lay&, const PipeGeom&, double, double, double,  \
-                                double, double, double, cudaStream_t);
+                                double, double, double, cudaStream_t);                                          \
+  template void pipe_divergence_rhs<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&,         \
+                                       const Lay&, const PipeGeom&, double, double, double*, double*, double*,   \
+                                       unsigned int*, double*, cudaStream_t);                                    \
+  template void pipe_velocity_correct<T>(T*, T*, T*, const double*, const T*, const double*, const Lay&,         \
+                                         const Lay&, const Lay&, const Lay&, const PipeGeom&, double, double,    \
+                                         double, double, double, cudaStream_t);
 #define FS_PIPE_INST2(T)                                                                                         \
   template int pipe_velocity_copies<T>(const T* const[3], T* const[3], T* const[3], T* const[3],                 \
                                        const Lay* const[3], const PipeGeom&, cudaStream_t);

@@ -50,11 +50,12 @@ __global__ void k_divergence_rhs(const T* __restrict__ u, const T* __restrict__ 
 }
 
 __global__ void k_subtract_mean(double* __restrict__ b, Lay Lc, const double* mean_src, double inv_n,
-                                double* partials, unsigned int* ticket, double* out) {
+                                double* partials, unsigned int* ticket, double* out, PipeGeom pg) {
   const double m = inv_n * mean_src[0];
   double bb = 0.0;
   Cursor cur;
   for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
+    if (pipe_solid(pg, cur.i, cur.k)) continue;  // no unknown: b stays 0
     const int64_t c = Lc.at(cur.i, cur.j, cur.k);
     const double v = b[c] - m;
     b[c] = v;
@@ -73,22 +74,25 @@ __global__ void k_subtract_mean(double* __restrict__ b, Lay Lc, const double* me
 // zero sum becomes one.
 template <class T, class V>
 __global__ void k_pressure_faces(const T* __restrict__ phi, Lay Lc, double rn, double rp, double inv2,
-                                 V* __restrict__ ax, V* __restrict__ ay, V* __restrict__ az) {
+                                 V* __restrict__ ax, V* __restrict__ ay, V* __restrict__ az, PipeGeom pg) {
   // one thread per cell, writing the couplings on its low faces; the
   // (i = nx, j = ny, k = nz) ghost faces stay zero from allocation
   FS_IJK(Lc);
   const int64_t c = Lc.at(i, j, k);
   const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
   double bx = 0.0, by = 0.0, bz = 0.0;
-  if (i > 0) {
+  // pipe: a coupling only between two unknowns (a y neighbour shares the
+  // cell's wall distance)
+  const bool solid = pipe_solid(pg, i, k);
+  if (i > 0 && !solid && !pipe_solid(pg, i - 1, k)) {
     const double pn = (double)phi[c - 1];
     bx = face_beta(inv_rho(phi[c - 1], rn, rp), vc, fabs(pn), acv);
   }
-  if (j > 0) {
+  if (j > 0 && !solid) {
     const double pn = (double)phi[c - Lc.px];
     by = face_beta(inv_rho(phi[c - Lc.px], rn, rp), vc, fabs(pn), acv);
   }
-  if (k > 0) {
+  if (k > 0 && !solid && !pipe_solid(pg, i, k - 1)) {
     const double pn = (double)phi[c - Lc.slab];
     bz = face_beta(inv_rho(phi[c - Lc.slab], rn, rp), vc, fabs(pn), acv);
   }
@@ -100,18 +104,39 @@ __global__ void k_pressure_faces(const T* __restrict__ phi, Lay Lc, double rn, d
 template <class T, class V>
 __global__ void k_pressure_diag(const T* __restrict__ phi, Lay Lc, double rn, double rp, double inv2,
                                 V* __restrict__ diag, double* __restrict__ extra0, unsigned short* __restrict__ dinv16,
-                                int deflate) {
+                                int deflate, PipeGeom pg) {
   FS_IJK(Lc);
   const int64_t c = Lc.at(i, j, k);
+  if (pipe_solid(pg, i, k)) {
+    // a Neumann cell of the pipe, no unknown: no couplings, diagonal 1
+    diag[c] = (V)1.0;
+    if (dinv16) dinv16[c] = __bfloat16_as_ushort(__float2bfloat16_rn(1.0f));
+    return;
+  }
   const double pc = (double)phi[c], vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
   double s = 0.0;
-  if (i > 0) s += face_beta(vc, inv_rho(phi[c - 1], rn, rp), acv, fabs((double)phi[c - 1]));
-  if (i < Lc.nx - 1) s += face_beta(vc, inv_rho(phi[c + 1], rn, rp), acv, fabs((double)phi[c + 1]));
+  if (i > 0 && !pipe_solid(pg, i - 1, k)) s += face_beta(vc, inv_rho(phi[c - 1], rn, rp), acv, fabs((double)phi[c - 1]));
+  if (i < Lc.nx - 1 && !pipe_solid(pg, i + 1, k))
+    s += face_beta(vc, inv_rho(phi[c + 1], rn, rp), acv, fabs((double)phi[c + 1]));
   if (j > 0) s += face_beta(vc, inv_rho(phi[c - Lc.px], rn, rp), acv, fabs((double)phi[c - Lc.px]));
   if (j < Lc.ny - 1) s += face_beta(vc, inv_rho(phi[c + Lc.px], rn, rp), acv, fabs((double)phi[c + Lc.px]));
-  if (k > 0) s += face_beta(vc, inv_rho(phi[c - Lc.slab], rn, rp), acv, fabs((double)phi[c - Lc.slab]));
-  if (k < Lc.nz - 1) s += face_beta(vc, inv_rho(phi[c + Lc.slab], rn, rp), acv, fabs((double)phi[c + Lc.slab]));
-  if (i == 0 && j == 0 && k == 0 && !deflate) {
+  if (k > 0 && !pipe_solid(pg, i, k - 1))
+    s += face_beta(vc, inv_rho(phi[c - Lc.slab], rn, rp), acv, fabs((double)phi[c - Lc.slab]));
+  if (k < Lc.nz - 1 && !pipe_solid(pg, i, k + 1))
+    s += face_beta(vc, inv_rho(phi[c + Lc.slab], rn, rp), acv, fabs((double)phi[c + Lc.slab]));
+  if (pg.on) {
+    // the pipe's first unknown (row 0): the faithful system adds the beta of
+    // its down neighbour, a Neumann cell (its other Neumann arms add 0)
+    if (i == pg.fi && j == pg.fj && k == pg.fk) {
+      double e = 0.0;
+      if (deflate) {
+        const double pd = (double)phi[c - Lc.slab];
+        e = face_beta(vc, inv_rho(phi[c - Lc.slab], rn, rp), acv, fabs(pd));
+        s = s + e;
+      }
+      if (extra0) *extra0 = inv2 * e;
+    }
+  } else if (i == 0 && j == 0 && k == 0 && !deflate) {
     if (extra0) *extra0 = 0.0;
   } else if (i == 0 && j == 0 && k == 0) {
     // deflation: the ghost 1/rho is the clamped copy of vc and the ghost phi
@@ -135,16 +160,22 @@ template <class T>
 __global__ void k_defect_residual(const T* __restrict__ phi, const double* __restrict__ p, const float* __restrict__ x32,
                                   const double* __restrict__ b, double* __restrict__ r64, float* __restrict__ r32,
                                   Lay Lc, double rn, double rp, double inv2, double* partials, unsigned int* ticket,
-                                  double* rr_out, int deflate) {
+                                  double* rr_out, int deflate, PipeGeom pg) {
   double rr = 0.0;
   Cursor cur;
   for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
     const int i = cur.i, j = cur.j, k = cur.k;
     const int64_t c = Lc.at(i, j, k);
+    if (pipe_solid(pg, i, k)) {  // no unknown: residual 0
+      if (r64) r64[c] = 0.0;
+      if (r32) r32[c] = 0.0f;
+      continue;
+    }
     const double pc = (double)phi[c];
     const double xc = x32 ? p[c] + (double)x32[c] : p[c];
     const int64_t nb[6] = {c - 1, c + 1, c - Lc.px, c + Lc.px, c - Lc.slab, c + Lc.slab};
-    const bool ok[6] = {i > 0, i < Lc.nx - 1, j > 0, j < Lc.ny - 1, k > 0, k < Lc.nz - 1};
+    const bool ok[6] = {i > 0 && !pipe_solid(pg, i - 1, k), i < Lc.nx - 1 && !pipe_solid(pg, i + 1, k), j > 0,
+                        j < Lc.ny - 1, k > 0 && !pipe_solid(pg, i, k - 1), k < Lc.nz - 1 && !pipe_solid(pg, i, k + 1)};
     // flux form with the same face coefficients as the on-the-fly SpMV
     double flux = 0.0;
 #pragma unroll
@@ -153,7 +184,10 @@ __global__ void k_defect_residual(const T* __restrict__ phi, const double* __res
       const double xn = x32 ? p[nb[q]] + (double)x32[nb[q]] : p[nb[q]];
       flux += face_coef(pc, (double)phi[nb[q]], 1.0 / rn, 1.0 / rp) * (xc - xn);
     }
-    if (deflate && i == 0 && j == 0 && k == 0) {
+    if (deflate && pg.on && i == pg.fi && j == pg.fj && k == pg.fk) {
+      const double pd = (double)phi[c - Lc.slab];
+      flux += face_beta(inv_rho(phi[c], rn, rp), inv_rho(phi[c - Lc.slab], rn, rp), fabs(pc), fabs(pd)) * xc;
+    } else if (deflate && !pg.on && i == 0 && j == 0 && k == 0) {
       const double vc = inv_rho(phi[c], rn, rp), acv = fabs(pc);
       const double gb = fabs(2.0 * pc - (double)phi[c + Lc.px]);
       const double gd = fabs(2.0 * pc - (double)phi[c + Lc.slab]);
@@ -319,21 +353,22 @@ __global__ void k_curvature(const T* __restrict__ phi, double* __restrict__ kapp
 // b_c = ((b_c - F_X) - F_Y) - F_Z with the ghost-fluid jump terms of the six
 // arms (jc_on_derivative = 0): an arm across the interface carries
 // +-inv_dx2 * a * beta, a = (jc_c |phi_n| + jc_n |phi_c|)/(|phi_c| + |phi_n|),
-// jc = sigma * kappa, + when the cell is in the phi <= 0 phase.  With walls
-// (the reference's system, POISSON_SOLVER_3D.h:1216-1328) arms to the wall
-// ghosts count too, with the extrapolated ghost phi (the ghosts of phi must
-// be filled), jc = 0 and the cell's own 1/rho; without (the corrected
-// projection) only arms to interior cells carry a jump, as only they have a
-// face whose velocity the update corrects.  The last block stores sum(b) in
-// sum_out for the mean removal.
+// jc = sigma * kappa, + when the cell is in the phi <= 0 phase.  Only arms
+// to interior cells can carry a jump: the reference's system
+// (POISSON_SOLVER_3D.h:1216-1328) evaluates the wall arms too, but with the
+// ghost phi that ComputeNormals (LEVELSET_3D.h:931) has just filled by
+// copying the nearest cell, so a wall arm never crosses the interface; the
+// corrected projection has no face to correct there either.  The last block
+// stores sum(b) in sum_out for the mean removal.
 template <class T>
 __global__ void k_jump_rhs(const T* __restrict__ phi, const double* __restrict__ kappa, double sigma,
                            double* __restrict__ b, Lay Lc, double rn, double rp, double inv2, int walls,
-                           double* partials, unsigned int* ticket, double* sum_out) {
+                           double* partials, unsigned int* ticket, double* sum_out, PipeGeom pg) {
   double bs = 0.0;
   Cursor cur;
   for (cur.init(Lc); cur.valid(Lc); cur.next(Lc)) {
     const int i = cur.i, j = cur.j, k = cur.k;
+    if (pipe_solid(pg, i, k)) continue;  // no unknown: b stays 0
     const int64_t c = Lc.at(i, j, k);
     const double pc = (double)phi[c], ac = fabs(pc);
     const double vc = 1.0 / (pc <= 0.0 ? rn : rp);
@@ -347,10 +382,10 @@ __global__ void k_jump_rhs(const T* __restrict__ phi, const double* __restrict__
       for (int side = 0; side < 2; ++side) {
         const int64_t nb = side == 0 ? c - step[a] : c + step[a];
         const bool ghost = side == 0 ? e[a] == 0 : e[a] == n[a] - 1;
-        if (ghost && !walls) continue;
+        if (ghost) continue;
         const double pn = (double)phi[nb], an = fabs(pn);
-        const double vn = ghost ? vc : 1.0 / (pn <= 0.0 ? rn : rp);
-        const double jn = ghost ? 0.0 : sigma * kappa[nb];
+        const double vn = 1.0 / (pn <= 0.0 ? rn : rp);
+        const double jn = sigma * kappa[nb];
         double f = 0.0;
         if ((pc <= 0.0) != (pn <= 0.0)) {
           const double av = (jcc * an + jn * ac) / (ac + an);
@@ -432,26 +467,31 @@ void divergence_rhs(const T* u, const T* v, const T* w, const Lay& Lc, const Lay
 }
 
 void subtract_mean(double* b, const Lay& Lc, const double* scalars, double* partials, unsigned int* ticket,
-                   double* scalars_out, cudaStream_t s) {
-  const double inv_n = 1.0 / ((double)Lc.nx * Lc.ny * Lc.nz);
-  k_subtract_mean<<<pcg_blocks(Lc), kRedThreads, 0, s>>>(b, Lc, scalars, inv_n, partials, ticket, scalars_out);
+                   double* scalars_out, cudaStream_t s, const PipeGeom* pipe) {
+  const PipeGeom pg = pipe ? *pipe : PipeGeom{};
+  const double inv_n = 1.0 / (pg.on ? (double)pg.cells : (double)Lc.nx * Lc.ny * Lc.nz);
+  k_subtract_mean<<<pcg_blocks(Lc), kRedThreads, 0, s>>>(b, Lc, scalars, inv_n, partials, ticket, scalars_out, pg);
 }
 
 template <class T, class V>
 void build_pressure_operator(const T* phi, const Lay& Lc, double dx, double rho_neg, double rho_pos, V* ax, V* ay, V* az,
-                             V* diag, double* extra0, int deflate, cudaStream_t s, unsigned short* dinv16) {
+                             V* diag, double* extra0, int deflate, cudaStream_t s, unsigned short* dinv16,
+                             const PipeGeom* pipe) {
   Launch3 g = launch3(Lc.nx, Lc.ny, Lc.nz);
   const double inv2 = 1.0 / (dx * dx);
-  k_pressure_faces<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, ax, ay, az);
-  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag, extra0, dinv16, deflate);
+  const PipeGeom pg = pipe ? *pipe : PipeGeom{};
+  k_pressure_faces<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, ax, ay, az, pg);
+  k_pressure_diag<T, V><<<g.grid, g.block, 0, s>>>(phi, Lc, rho_neg, rho_pos, inv2, diag, extra0, dinv16, deflate,
+                                                    pg);
 }
 
 template <class T>
 void defect_residual(const T* phi, const double* p64, const float* x32, const double* b, double* r64, float* r32,
                      const Lay& Lc, double dx, double rho_neg, double rho_pos, double* partials, unsigned int* ticket,
-                     double* rr_out, int deflate, cudaStream_t s) {
+                     double* rr_out, int deflate, cudaStream_t s, const PipeGeom* pipe) {
+  const PipeGeom pg = pipe ? *pipe : PipeGeom{};
   k_defect_residual<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, p64, x32, b, r64, r32, Lc, rho_neg, rho_pos,
-                                                              1.0 / (dx * dx), partials, ticket, rr_out, deflate);
+                                                              1.0 / (dx * dx), partials, ticket, rr_out, deflate, pg);
 }
 
 void add_correction(double* p64, const float* e, const Lay& Lc, cudaStream_t s) {
@@ -477,9 +517,11 @@ void curvature(const T* phi, double* kappa, const Lay& L, double dx, int typo, d
 
 template <class T>
 void jump_rhs(const T* phi, const double* kappa, double sigma, double* b, const Lay& Lc, double dx, double rho_neg,
-              double rho_pos, int walls, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s) {
+              double rho_pos, int walls, double* partials, unsigned int* ticket, double* sum_out, cudaStream_t s,
+              const PipeGeom* pipe) {
+  const PipeGeom pg = pipe ? *pipe : PipeGeom{};
   k_jump_rhs<T><<<pcg_blocks(Lc), kRedThreads, 0, s>>>(phi, kappa, sigma, b, Lc, rho_neg, rho_pos, 1.0 / (dx * dx),
-                                                       walls, partials, ticket, sum_out);
+                                                       walls, partials, ticket, sum_out, pg);
 }
 
 template <class T>
@@ -521,13 +563,13 @@ void unpack_from_double(T* dst, const double* src, const Lay& L, cudaStream_t s)
                                   double, double, double*, double*, double*, unsigned int*, double*, cudaStream_t); \
   template void defect_residual<T>(const T*, const double*, const float*, const double*, double*, float*,         \
                                    const Lay&, double, double, double, double*, unsigned int*, double*, int,        \
-                                   cudaStream_t);                                                                   \
+                                   cudaStream_t, const PipeGeom*);                                                  \
   template void velocity_correct<T>(T*, const T*, const double*, const T*, const Lay&, const Lay&, int, double,     \
                                     double, double, double, int, double, double, const double*, double,            \
                                     cudaStream_t);                                                                  \
   template void curvature<T>(const T*, double*, const Lay&, double, int, double*, cudaStream_t);                   \
   template void jump_rhs<T>(const T*, const double*, double, double*, const Lay&, double, double, double, int,    \
-                            double*, unsigned int*, double*, cudaStream_t);                                                  \
+                            double*, unsigned int*, double*, cudaStream_t, const PipeGeom*);                 \
   template void divergence_norms<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, const Lay&,   \
                                     double, double*, unsigned int*, double*, cudaStream_t);                         \
   template void absmax3<T>(const T*, const T*, const T*, const Lay&, const Lay&, const Lay&, double*, cudaStream_t); \
@@ -539,7 +581,7 @@ FS_PINST(double)
 
 #define FS_BINST(T, V)                                                                                        \
   template void build_pressure_operator<T, V>(const T*, const Lay&, double, double, double, V*, V*, V*, V*, double*, \
-                                              int, cudaStream_t, unsigned short*);
+                                              int, cudaStream_t, unsigned short*, const PipeGeom*);
 FS_BINST(float, float)
 FS_BINST(double, double)
 FS_BINST(double, float)

@@ -140,11 +140,14 @@ typedef struct {
      1 a pipe along y, periodic in y with the reference's node convention (cell
      0 and cell ny-1 are one point), its wall at sqrt(x^2 + z^2) = pipe_radius.
      Built for the level-set advection, the reinitialisation, the ENO3 velocity
-     advection and the body force (fs_advect_levelset, fs_reinitialize,
-     fs_advect_velocity with velocity_scheme FS_VELOCITY_ENO3,
-     fs_apply_gravity); the viscosity, the projection, the CFL time step,
-     fs_step and the adjoints return FS_NOT_SUPPORTED in this mode.  Fixed at
-     creation. */
+     advection, the body force and the projection (fs_advect_levelset,
+     fs_reinitialize, fs_advect_velocity with velocity_scheme
+     FS_VELOCITY_ENO3, fs_apply_gravity, fs_project: the cylinder's cells are
+     the unknowns, the cells outside it Neumann cells, rho_neg and rho_pos
+     the dimensionless densities 1 and water_density/oil_density, the
+     pressure solve with the Jacobi preconditioners only); the viscosity,
+     the CFL time step, fs_step and the adjoints return FS_NOT_SUPPORTED in
+     this mode.  Fixed at creation. */
   int pipe;
   double pipe_radius;               /* a: the wall radius in units of the core radius R1 */
   double grid_min[3], grid_max[3];  /* the script's base_grid_min and base_grid_max: cell (i,j,k) sits at
@@ -154,6 +157,8 @@ typedef struct {
   double pipe_f;                    /* f, the driving pressure gradient */
   double pipe_eta;                  /* eta, the density ratio of the dimensionless form */
   double pipe_oil_density;          /* oil_density */
+  double pipe_We;                   /* We, the Weber number of the dimensionless form: the pipe's projection
+                                       carries the jump condition kappa/We (PROJECTION_3D.h:758-762) */
 } fs_params;
 
 typedef struct {

@@ -3,9 +3,9 @@ own outputs (fixtures pipe_*, made by tests/golden/make_golden.py from the
 headless reference build) and against the oracle.
 
 The pipe mode's level-set advection, reinitialisation, ENO3 velocity
-advection and dimensionless body force run on the GPU; its viscosity and
-projection are not built, and those entry points (and fs_step) return
-FS_NOT_SUPPORTED in this mode."""
+advection, dimensionless body force and projection run on the GPU; its
+viscosity is not built, and that entry point (with fs_step and the CFL time
+step) returns FS_NOT_SUPPORTED in this mode."""
 import os
 
 import numpy as np
@@ -23,15 +23,19 @@ def load(name):
     return dict(np.load(os.path.join(GOLD, name + ".npz")))
 
 
-def solver(g, precision=fs.FS_PRECISION_FP64, flags=fs.FS_FLAG_REINIT_TYPO):
+def solver(g, precision=fs.FS_PRECISION_FP64, flags=fs.FS_FLAG_REINIT_TYPO, **kw):
     n = tuple(int(x) for x in g["n"])
     dx = (float(g["hi"][0]) - float(g["lo"][0])) / (n[0] - 1)
+    # the projection's dimensionless densities: 1 in the oil (phi <= 0),
+    # water_density/oil_density in the water (PROJECTION_3D.h:642-669)
+    water = float(g["water_density"]) if "water_density" in g else 0.995
     return fs.Solver(n, dx, precision=precision, pipe=1, pipe_radius=float(g["a"]), grid_min=tuple(g["lo"]),
                      grid_max=tuple(g["hi"]), pipe_R1=float(g["R1"]), pipe_V0=float(g["V0"]), pipe_f=float(g["f"]),
-                     pipe_eta=float(g["eta"]), pipe_oil_density=float(g["oil_density"]),
+                     pipe_eta=float(g["eta"]), pipe_oil_density=float(g["oil_density"]), pipe_We=float(g["We"]),
+                     rho_neg=1.0, rho_pos=water / float(g["oil_density"]),
                      gravity=(0.0, float(g["gravity_y"]), 0.0), weno_epsilon=float(g["epsilon"]),
                      reinit_iterations=int(g["reinit_iterations"]), reinit_scaling=int(g["reinit_scaling"]),
-                     flags=flags, viscosity=0, velocity_scheme=fs.FS_VELOCITY_ENO3)
+                     flags=flags, viscosity=0, velocity_scheme=fs.FS_VELOCITY_ENO3, **kw)
 
 
 def upload(s, g, keys=("phi", "u", "v", "w")):
@@ -113,8 +117,7 @@ def test_pipe_mode_refuses_the_operators_it_does_not_build():
     g = load("pipe_levelset")
     with solver(g) as s:
         upload(s, g)
-        for call in (lambda: s.step(1e-3), lambda: s.project(1e-3), lambda: s.viscosity(1e-3),
-                     lambda: s.cfl_dt()):
+        for call in (lambda: s.step(1e-3), lambda: s.viscosity(1e-3), lambda: s.cfl_dt()):
             with pytest.raises(fs.FsError) as e:
                 call()
             assert e.value.status == fs.FS_NOT_SUPPORTED
@@ -129,9 +132,69 @@ def test_pipe_geometry_is_checked():
     # a pipe that reaches the box's ghost layers
     with pytest.raises(fs.FsError) as e:
         fs.Solver(n, 0.25, pipe=1, pipe_radius=2.45, grid_min=tuple(g["lo"]), grid_max=tuple(g["hi"]), pipe_R1=1.0,
-                  pipe_V0=1.0, pipe_f=1.0, pipe_eta=1.1, pipe_oil_density=0.9)
+                  pipe_V0=1.0, pipe_f=1.0, pipe_eta=1.1, pipe_oil_density=0.9, pipe_We=1.0)
     assert e.value.status == fs.FS_INVALID_ARG
     # grid_min/grid_max that do not give the grid's dx
     with pytest.raises(fs.FsError):
         fs.Solver(n, 0.2, pipe=1, pipe_radius=1.61, grid_min=tuple(g["lo"]), grid_max=tuple(g["hi"]), pipe_R1=1.0,
-                  pipe_V0=1.0, pipe_f=1.0, pipe_eta=1.1, pipe_oil_density=0.9)
+                  pipe_V0=1.0, pipe_f=1.0, pipe_eta=1.1, pipe_oil_density=0.9, pipe_We=1.0)
+
+
+@pytest.mark.parametrize("precision", [fs.FS_PRECISION_FP64, fs.FS_PRECISION_FP32_REFINE])
+def test_pipe_projection_matches_reference(precision):
+    """EULERIAN_FLUID_SOLVER_3D::Projection of the pipe (fixture
+    pipe_projection): Neumann cells outside the cylinder, the divergence of
+    the pipe's velocity copies, the jump kappa/We, the deflated system solved
+    to the reference's absolute r.z < tol^2, the pipe's velocity update with
+    its fixed centre line and periodic rows.  FP64: the divergence to
+    rounding, the PCG iterations within 2, pressure and velocities to 1e-9 of
+    their scale; FP32 + refinement (the same system solved to the
+    equivalent relative residual): pressure and velocities to 1e-5."""
+    g = load("pipe_projection")
+    fp64 = precision == fs.FS_PRECISION_FP64
+    flags = fs.FS_FLAG_REINIT_TYPO | fs.FS_FLAG_FAITHFUL_PROJECTION | fs.FS_FLAG_CURVATURE_TYPO
+    kw = dict(stop=fs.FS_STOP_ABSOLUTE, tolerance=float(g["tolerance"])) if fp64 else dict(tolerance=1e-9)
+    with solver(g, precision, flags=flags, max_iteration=int(g["max_iteration"]), **kw) as s:
+        upload(s, g)
+        rep = s.project(float(g["dt"]))
+        p = s.download("pressure")
+        div = s.download("divergence")
+        vel = {k: s.download(k) for k in "uvw"}
+    fl = g["boundary"] <= 0
+    assert fl.sum() == len(g["b_rows"])
+    dscale = np.abs(g["div"]).max()
+    assert np.abs(div - g["div"]).max() <= (1e-12 if fp64 else 1e-5) * dscale
+    if fp64:
+        assert abs(rep["iterations"] - int(g["iterations"])) <= 2
+    pscale = np.abs(g["out_p"]).max()
+    ptol = 1e-9 if fp64 else 1e-5
+    assert np.abs(p[fl] - g["x_rows"]).max() <= ptol * pscale
+    # the cells outside the pipe are no unknowns: their pressure stays 0
+    assert np.abs(p[~fl]).max() == 0.0
+    for k in "uvw":
+        ref, inp = g["out_" + k], g[k]
+        scale = max(np.abs(ref - inp).max(), 1.0)
+        assert np.abs(vel[k] - ref).max() <= ptol * scale, (k, np.abs(vel[k] - ref).max())
+
+
+def test_pipe_projection_matches_oracle_corrected_system():
+    """The corrected pipe projection (the singular consistent system, no
+    deflation) against the oracle's, FP64, solved to 1e-10 relative."""
+    g = load("pipe_projection")
+    grids = O.pipe_grids(tuple(int(x) for x in g["n"]), tuple(g["lo"]), tuple(g["hi"]))
+    C = {k: float(g[k]) for k in ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We")}
+    fixed = (g["fixed_u"], g["fixed_v"], g["fixed_w"])
+    u, v, w, p, info = O.pipe_projection(g["phi"], g["u"], g["v"], g["w"], grids, C, float(g["dt"]), 1e-12, 20000,
+                                         float(g["water_density"]), float(g["oil_density"]), fixed=fixed,
+                                         mode="corrected", criterion="rel")
+    flags = fs.FS_FLAG_REINIT_TYPO | fs.FS_FLAG_CURVATURE_TYPO
+    with solver(g, flags=flags, tolerance=1e-12, max_iteration=20000) as s:
+        upload(s, g)
+        s.project(float(g["dt"]))
+        got = {k: s.download(k) for k in ("u", "v", "w", "pressure")}
+    fl = info["fluid"]
+    # the singular system's pressure is fixed up to a constant
+    dp = (got["pressure"] - p)[fl]
+    assert np.abs(dp - dp.mean()).max() <= 1e-8 * np.abs(p[fl]).max()
+    for k, ref in zip("uvw", (u, v, w)):
+        assert np.abs(got[k] - ref).max() <= 1e-8 * max(np.abs(ref - g[k]).max(), 1.0), k
