@@ -178,6 +178,10 @@ void cg_iteration(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double*
 // alpha in the state.
 template <class V, class X>
 void cg_vector_updates(const Op7<V>& A, X* x, V* r, V* p, V* q, PcgState* st, double* partials, cudaStream_t s);
+// p.q and the step length (alpha, or a stagnation stop) for a SpMV that
+// wrote q without reducing p.q (the red-black black pass)
+template <class V>
+void pq_alpha(const Op7<V>& A, const V* p, const V* q, PcgState* st, double* partials, cudaStream_t s);
 // Occupancy queries that size cg_iteration's grids: call once per (V, X)
 // before the first iteration (outside stream capture).
 template <class V, class X> void cg_prepare();

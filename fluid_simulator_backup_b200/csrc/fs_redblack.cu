@@ -38,11 +38,12 @@
 //
 // Kernels of one iteration (each array element once per kernel):
 //   k_rb_red    tau of every red cell          reads ax, ay, az, p     writes tau
-//   k_rb_black  q = S p, p.q and alpha         reads ax, ay, az, p, tau writes q
+//   k_rb_black  q = S p                        reads ax, ay, az, p, tau writes q
+//   k_pq_alpha  p.q and alpha                  reads p, q
 //   k_cg_update / k_cg_pupdate (fs_krylov.cu) on the packed black vectors
-// = 16 + 18 + 7 + 15 = 56 bytes per cell and iteration (FP32 couplings and
-// vectors, FP64 black iterate, bf16 black pivots), at half the iterations of
-// the full Jacobi-PCG's 64.
+// = 16 + 18 + 4 + 7 + 15 = 60 bytes per cell and iteration (FP32 couplings
+// and vectors, FP64 black iterate, bf16 black pivots), at half the
+// iterations of the full Jacobi-PCG's 64.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -55,19 +56,16 @@ Lay make_half_lay(const Lay& L) { return make_lay((L.nx + 1) / 2, L.ny, L.nz); }
 
 namespace {
 
-// q = S p in two passes.  The red pass writes tau of every red cell (one
-// thread per packed slot and plane of a 4-plane chunk, a (32, 8) tile of
-// slots per block); the
-// black pass reads the couplings, p and the six tau of each black cell,
-// writes q and reduces p.q.  Each block of the black pass walks a chunk of
-// 8 z planes so that the p.q reduction has thousands of partial sums
-// instead of one per plane and tile (measured at 256^3: 95 us for the pass
-// against 102 us with one block per plane and tile, and 64 us for the same
-// pass without the reduction).  Both passes are plain streaming kernels with
-// few instructions per cell: measured at 256^3 they run faster than fused
-// forms that keep tau on chip (a z-marching shared-memory ring, and a
-// cp.async-staged pipeline), whose per-plane barriers and index arithmetic
-// made them issue- and latency-bound.
+// q = S p in two passes.  The red pass writes tau of every red cell, the
+// black pass reads the couplings, p and the six tau of each black cell and
+// writes q; each is one thread per packed slot and plane of a 4-plane z
+// chunk, a (32, 8) tile of slots per block.  p.q and the step length follow
+// in a separate streaming pass over p and q (pq_alpha, fs_krylov.cu).
+// Both passes are plain streaming kernels with few instructions per cell:
+// measured at 256^3 they run faster than fused forms that keep tau on chip
+// (a z-marching shared-memory ring, and a cp.async-staged pipeline), whose
+// per-plane barriers and index arithmetic made them issue- and
+// latency-bound.
 constexpr int kRbBY = 8;
 
 // tau of the red cell in slot (h, j, k) (in range)
@@ -110,12 +108,11 @@ __global__ void __launch_bounds__(32 * kRbBY) k_rb_red(RbOp A, const float* __re
 
 __global__ void __launch_bounds__(32 * kRbBY) k_rb_black(RbOp A, const float* __restrict__ p,
                                                         const float* __restrict__ tau, float* __restrict__ q,
-                                                        PcgState* st, double* partials, int kchunk) {
-  if (((volatile PcgState*)st)->done) return;
+                                                        const PcgState* st, int kchunk) {
+  if (((volatile const PcgState*)st)->done) return;
   const Lay& L = A.L;
   const Lay& H = A.Lh;
   const int h = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * kRbBY + threadIdx.y;
-  double pq = 0.0;
   if (h < H.nx && j < H.ny) {
     const int k0 = blockIdx.z * kchunk, k1 = min(H.nz, k0 + kchunk);
     for (int k = k0; k < k1; ++k) {
@@ -146,23 +143,8 @@ __global__ void __launch_bounds__(32 * kRbBY) k_rb_black(RbOp A, const float* __
         acc += aym * (dym - tym) + ayp * (dyp - typ);
         acc += azm * (dzm - tzm) + azp * (dzp - tzp);
         qv = acc;
-        pq += (double)pc * (double)qv;
       }
       q[s] = qv;
-    }
-  }
-  pq = block_sum(pq);
-  double tot;
-  if (grid_reduce_sum(pq, partials, &st->ticket, &tot)) {
-    st->pq = tot;
-    const double alpha = st->rz / tot;
-    if (!(tot > 0.0) || !isfinite(alpha)) {
-      st->status = PCG_STAGNATED;
-      st->done = 1;
-      st->x_pending = 0;
-    } else {
-      st->alpha = alpha;
-      st->x_pending = 1;
     }
   }
 }
@@ -275,9 +257,9 @@ const dim3 kRbBlock(32, 4, 2);
 // one kernel at a time): the red pass takes 94 us with one block per tile
 // and plane, 59 us with 2 planes per block and 54 us with 4 (a thread per
 // cell is bound by block scheduling: each block lives about as long as one
-// round trip to memory); the black pass is flat at 95-97 us from 8 to 32
-// planes per block.
-constexpr int kRbChunk = 8;
+// round trip to memory); the black pass 98 us with one plane per block and
+// 66-74 us with 4 to 32.  The black pass reducing p.q itself took 95-97 us.
+constexpr int kRbChunk = 4;
 constexpr int kRbRedChunk = 4;
 
 dim3 rb_red_grid(const Lay& H) {
@@ -295,7 +277,8 @@ int rb_blocks(const Lay& H) {
 void rb_iteration(const RbOp& A, const Op7<float>& Ah, double* xh, float* rh, float* ph, float* qh, float* tau,
                   PcgState* st, double* partials, cudaStream_t s) {
   k_rb_red<<<rb_red_grid(A.Lh), dim3(32, kRbBY, 1), 0, s>>>(A, ph, tau, st, kRbRedChunk);
-  k_rb_black<<<rb_black_grid(A.Lh), dim3(32, kRbBY, 1), 0, s>>>(A, ph, tau, qh, st, partials, kRbChunk);
+  k_rb_black<<<rb_black_grid(A.Lh), dim3(32, kRbBY, 1), 0, s>>>(A, ph, tau, qh, st, kRbChunk);
+  pq_alpha<float>(Ah, ph, qh, st, partials, s);
   cg_vector_updates<float, double>(Ah, xh, rh, ph, qh, st, partials, s);
 }
 
