@@ -1969,3 +1969,23 @@ def pipe_projection(phi, u, v, w, grids, C, dt, tol, max_iter, water_density, oi
                                       fixed)
     return u2, v2, w2, p, {"iterations": it, "rz": rz, "rel_residual": rel, "b": b, "div": div, "jc": jc,
                            "fluid": fluid, "op": op}
+
+
+def pipe_cfl_dt(u, v, w, grids, C, gravity_y, water_density, oil_density, kappa_max):
+    """EULERIAN_FLUID_SOLVER_3D::CFLOneTimeStep in the pipe's dimensionless
+    form with the semi-implicit viscosity (EULERIAN_FLUID_SOLVER_3D.h:
+    2673-2785): 1/cfl, cfl = 0.5 (c + sqrt(c^2 + 4 g^2 + 4 s^2)) with
+      c = max|u|/dx_u + max|v|/dy_v + max|w|/dz_w    (the face grids' spacings)
+      g = sqrt(R1/V0^2 (|g_y| + |f/min(oil, water)|)/dy_v)
+      s = sqrt((kappa_max/We)/(min(water/oil, 1) min(dx_u, dy_v, dz_w)^2))
+    and no viscous term; kappa_max is max |kappa| over cells with
+    |phi| < 0.1 of the last curvature the projection computed."""
+    inv_x, inv_y, inv_z = 1.0 / grids[1][3], 1.0 / grids[2][4], 1.0 / grids[3][5]
+    c_f = (float(np.max(np.abs(u))) * inv_x + float(np.max(np.abs(v))) * inv_y) + float(np.max(np.abs(w))) * inv_z
+    g_f = math.sqrt(C["R1"] / (C["V0"] * C["V0"]) * (abs(gravity_y) + abs(1.0 / min(oil_density, water_density) * C["f"]))
+                    * inv_y)
+    h = min(grids[1][3], grids[2][4], grids[3][5])
+    s_f = math.sqrt(((1.0 / C["We"]) * kappa_max) / (min(water_density / oil_density, 1.0) * (h * h)))
+    cv = c_f + 0.0
+    cfl = 0.5 * (cv + math.sqrt((cv * cv + 4.0 * (g_f * g_f)) + 4.0 * (s_f * s_f)))
+    return 1.0 / cfl

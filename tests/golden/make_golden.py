@@ -47,7 +47,8 @@ on the air/water unit-cube box with Neumann pressure walls:
   pipe_projection  the pipe's Projection: Neumann cells outside the
                    cylinder, the pipe divergence, jump 1/We kappa, the
                    deflated system (right-hand side and solution in row
-                   order), PCG and the pipe velocity update
+                   order), PCG and the pipe velocity update; then the
+                   pipe's CFLOneTimeStep
 
     python tests/golden/make_golden.py [name ...]   writes only the named fixtures
 """
@@ -316,9 +317,10 @@ def main():
     for k, a_ in dict(phi=phi, **vel).items():
         c.set(k, a_)
     it = c.pipe_projection(0.01)
+    cfl = c.cfl()  # CFLOneTimeStep on the projected velocities and the projection's curvature
     vals, cols, rowptr, b_rows, x_rows = c.poisson_csr()
     fixtures["pipe_projection"] = dict(base, dt=0.01, tolerance=1e-6, max_iteration=10000, **fixed,
-                                       water_density=const["water_density"], iterations=it,
+                                       water_density=const["water_density"], iterations=it, cfl=cfl,
                                        div=c.divergence(), jc=c.projection_jc(), csr_vals=vals, csr_cols=cols,
                                        csr_rowptr=rowptr, b_rows=b_rows, x_rows=x_rows, out_p=c.get("p"),
                                        out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"))

@@ -108,3 +108,16 @@ def test_pipe_projection_matches_reference():
     np.testing.assert_array_equal(p, g["out_p"])
     for k, a in zip("uvw", (u, v, w)):
         np.testing.assert_array_equal(a, g["out_" + k])
+
+
+def test_pipe_cfl_matches_reference():
+    """CFLOneTimeStep of the pipe (dimensionless form, semi-implicit
+    viscosity) on the projected velocities, with the projection's curvature
+    maximum."""
+    g = load("pipe_projection")
+    C = {k: float(g[k]) for k in ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We")}
+    gr = grids(g)
+    _, kmax = O.curvature(g["phi"], gr[0][3], typo=True)
+    dt = O.pipe_cfl_dt(g["out_u"], g["out_v"], g["out_w"], gr, C, float(g["gravity_y"]), float(g["water_density"]),
+                       float(g["oil_density"]), kmax)
+    assert dt == float(g["cfl"])
