@@ -1989,3 +1989,33 @@ def pipe_cfl_dt(u, v, w, grids, C, gravity_y, water_density, oil_density, kappa_
     cv = c_f + 0.0
     cfl = 0.5 * (cv + math.sqrt((cv * cv + 4.0 * (g_f * g_f)) + 4.0 * (s_f * s_f)))
     return 1.0 / cfl
+
+
+def pipe_step(phi, u, v, w, grids, C, dt, P):
+    """EULERIAN_FLUID_SOLVER_3D::AdvanceOneTimeStepThread of a vertical pipe
+    with order_for_time_advancing = 2 and the sourcing step off
+    (EULERIAN_FLUID_SOLVER_3D.h:886-979, SolveForRK :1453-1476): the level
+    set by Heun over two WENO5 advections (each zeroing u and w outside the
+    pipe), the velocity by Heun over two stages of ENO3 advection, body force
+    and projection (the pressure of the first stage is the second's initial
+    guess), the reinitialisation by Heun over two blocks.  P: tolerance,
+    max_iteration, water_density, oil_density, gravity_y, epsilon,
+    reinit_iterations, reinit_scaling, p0 (optional).  Returns
+    (phi, u, v, w, p)."""
+    a = C["a"]
+    fixed = pipe_fixed_faces((phi.shape[2], phi.shape[1], phi.shape[0]))
+    ph1, u, v, w = pipe_weno5_levelset(phi, u, v, w, grids, a, dt, P["epsilon"])
+    ph2, u, v, w = pipe_weno5_levelset(ph1, u, v, w, grids, a, dt, P["epsilon"])
+    phi = 0.5 * (phi + ph2)
+    rk = (u, v, w)
+    p = P.get("p0")
+    for _ in range(2):
+        u, v, w = pipe_eno3_velocity(u, v, w, grids, a, dt)
+        v = pipe_forcing(phi, v, grids, C, P["gravity_y"], P["oil_density"], dt, fixed_v=fixed[1])
+        u, v, w, p, _info = pipe_projection(phi, u, v, w, grids, C, dt, P["tolerance"], P["max_iteration"],
+                                            P["water_density"], P["oil_density"], fixed=fixed, p0=p)
+    u, v, w = (0.5 * rk[0] + 0.5 * u, 0.5 * rk[1] + 0.5 * v, 0.5 * rk[2] + 0.5 * w)
+    r1 = pipe_reinitialization(phi, grids, P["reinit_iterations"], P["reinit_scaling"], P["epsilon"])
+    r2 = pipe_reinitialization(r1, grids, P["reinit_iterations"], P["reinit_scaling"], P["epsilon"])
+    phi = 0.5 * (phi + r2)
+    return phi, u, v, w, p

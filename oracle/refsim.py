@@ -214,7 +214,7 @@ def write_pipe_sim(path, res, grid_min, grid_max, *, vertical=True, threads=1, a
                    alpha=2.4, m=0.00166, eta=1.1, K=-2.03030303, g=-980.0, water_density=0.995, oil_density=0.905,
                    water_viscosity=0.01, oil_viscosity=6.01, surface_tension=8.54, gravity=(0.0, -980.0, 0.0),
                    order=2, tolerance=1e-6, max_iteration=10000, reinit_iterations=10, reinit_scaling=2,
-                   epsilon=1e-6, periodic_num=5, cfl=0.8):
+                   epsilon=1e-6, periodic_num=5, cfl=0.8, sourcing=True):
     """Write an oil/water pipe scenario in the reference's .sim syntax, with
     the keys of the reference's own pipe scripts (3D_script_1.sim):
     SIMULATION_WORLD (a, R2, A_0, alpha; SIMULATION_WORLD.h:120-129),
@@ -283,7 +283,7 @@ FLUID_SOLVER_UNIFORM_OIL_WATER
 	is_Levelset_advection_active = true
 	is_Velocity_advection_active = true
 	is_external_force_active = true
-	is_sourcing_active = true
+	is_sourcing_active = {b(sourcing)}
 	is_projection_active = true
 	fastsweeping_reinitialization = false
 	sussmanstyle_reinitialization = true

@@ -49,6 +49,9 @@ on the air/water unit-cube box with Neumann pressure walls:
                    deflated system (right-hand side and solution in row
                    order), PCG and the pipe velocity update; then the
                    pipe's CFLOneTimeStep
+  pipe_frame       one SIMULATION_WORLD::AdvanceOneFrame of the pipe with
+                   is_sourcing_active = false (no viscosity): CFL dt and the
+                   order-2 step
 
     python tests/golden/make_golden.py [name ...]   writes only the named fixtures
 """
@@ -324,6 +327,23 @@ def main():
                                        div=c.divergence(), jc=c.projection_jc(), csr_vals=vals, csr_cols=cols,
                                        csr_rowptr=rowptr, b_rows=b_rows, x_rows=x_rows, out_p=c.get("p"),
                                        out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"))
+    c.close()
+
+    # one whole frame of the pipe with the reference's sourcing step off
+    # (is_sourcing_active = false: no viscosity), SIMULATION_WORLD::
+    # AdvanceOneFrame: curvature, CFL dt, order-2 step (level-set Heun,
+    # velocity Heun over ENO3 advection + body force + projection,
+    # reinitialisation Heun); the level set and velocities of the other pipe
+    # fixtures
+    frame_sim = refsim.write_pipe_sim(os.path.join(WORK, "pipe_frame.sim"), pn, lo, hi, sourcing=False)
+    c = refsim.RefCase(frame_sim)
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    dt, it = c.advance_frame()
+    fixtures["pipe_frame"] = dict(base, cfl_number=0.8, tolerance=1e-6, max_iteration=10000,
+                                  water_density=const["water_density"], dt=dt, iterations=it,
+                                  out_phi=c.get("phi"), out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"),
+                                  out_p=c.get("p"))
     c.close()
 
     only = set(sys.argv[1:])

@@ -121,3 +121,25 @@ def test_pipe_cfl_matches_reference():
     dt = O.pipe_cfl_dt(g["out_u"], g["out_v"], g["out_w"], gr, C, float(g["gravity_y"]), float(g["water_density"]),
                        float(g["oil_density"]), kmax)
     assert dt == float(g["cfl"])
+
+
+def test_pipe_frame_matches_reference():
+    """One whole SIMULATION_WORLD::AdvanceOneFrame of the pipe with the
+    reference's sourcing step off (no viscosity), bit for bit: the CFL dt
+    from the level set's curvature, then the order-2 step (level-set Heun,
+    velocity Heun over ENO3 advection + body force + projection,
+    reinitialisation Heun)."""
+    g = load("pipe_frame")
+    gr = grids(g)
+    C = {k: float(g[k]) for k in ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We")}
+    _, kmax = O.curvature(g["phi"], gr[0][3], typo=True)
+    dt = O.pipe_cfl_dt(g["u"], g["v"], g["w"], gr, C, float(g["gravity_y"]), float(g["water_density"]),
+                       float(g["oil_density"]), kmax) * float(g["cfl_number"])
+    assert dt == float(g["dt"])
+    P = dict(tolerance=float(g["tolerance"]), max_iteration=int(g["max_iteration"]),
+             water_density=float(g["water_density"]), oil_density=float(g["oil_density"]),
+             gravity_y=float(g["gravity_y"]), epsilon=float(g["epsilon"]),
+             reinit_iterations=int(g["reinit_iterations"]), reinit_scaling=int(g["reinit_scaling"]))
+    out = O.pipe_step(g["phi"], g["u"], g["v"], g["w"], gr, C, dt, P)
+    for name, a in zip(("phi", "u", "v", "w", "p"), out):
+        np.testing.assert_array_equal(a, g["out_" + name])
