@@ -1021,7 +1021,7 @@ fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* re
   if (tp) CKS(tape_velocity(c, tp->vel[stage][0]));
   CKS(advect_velocity_t<S>(c, dt));
   const Lay* lays[3] = {&c->Lu, &c->Lv, &c->Lw};
-  if (!(c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION)) {
+  if (!(c->prm.flags & FS_FLAG_FAITHFUL_PROJECTION) && !c->pipe.on) {
     // no penetration: advection also updates the wall faces, which hold zero
     zero_walls<S>(F<S>(c->u), *lays[0], 0, c->stream);
     zero_walls<S>(F<S>(c->v), *lays[1], 1, c->stream);
@@ -1036,6 +1036,15 @@ fs_status stage_t(fs_ctx* c, double dt, double c0, double c1, fs_step_report* re
   fs_solve_report pr{};
   fs_status st = project_t<S>(c, dt, c0, c1, &pr);
   if (st != FS_OK && st != FS_NOT_CONVERGED) return st;
+  if (c->pipe.on && c0 != 0.0) {
+    // the pipe's projection leaves the RK combination to its caller
+    // (EULERIAN_FLUID_SOLVER_3D.h:938-955: c0 u_rk + c1 u on every face)
+    void* comps[3] = {c->u, c->v, c->w};
+    void* base[3] = {c->u0, c->v0, c->w0};
+    for (int a = 0; a < 3; ++a) axpby<S>(F<S>(comps[a]), F<S>(base[a]), F<S>(comps[a]), c0, c1, *lays[a], c->stream);
+    c->launches += 3;
+    CK(cudaGetLastError());
+  }
   if (tp) CK(cudaMemcpyAsync(tp->p[stage], c->p64, c->Lc.total * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   if (rep) {
     rep->pcg_iterations += pr.iterations;
@@ -1095,11 +1104,34 @@ template <class S>
 fs_status cfl_t(fs_ctx* c, double* dt) {
   absmax3<S>(F<S>(c->u), F<S>(c->v), F<S>(c->w), c->Lu, c->Lv, c->Lw, c->scalars + 8, c->stream);
   c->launches += 3;
-  if (c->prm.surface_tension != 0.0) CKS(curvature_t<S>(c));
+  if (c->prm.surface_tension != 0.0 || c->pipe.on) CKS(curvature_t<S>(c));
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->sc_host + 8, c->scalars + 8, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   const fs_params& P = c->prm;
+  if (c->pipe.on) {
+    // the pipe's dimensionless form with the semi-implicit viscosity
+    // (EULERIAN_FLUID_SOLVER_3D.h:2673-2785): each velocity's maximum over
+    // the spacing of its own face grid, the body force's term with R1/V0^2
+    // and f, the surface term with 1/We and min(water/oil, 1), no viscous
+    // term.  The curvature maximum is that of the current level set (the
+    // reference reads the one its last projection computed).
+    const PipeGeom& G = c->pipe;
+    const int ny = c->grid.ny;
+    const double d1 = (P.grid_max[1] - P.grid_min[1]) / (ny - 1);
+    const double hv = ((P.grid_max[1] + 0.5 * d1) - (P.grid_min[1] - 0.5 * d1)) / ny;  // dy of the v faces
+    const double hu = G.hx[1], hw = G.hz[3];
+    const double c_f = (c->sc_host[8] * (1.0 / hu) + c->sc_host[9] * (1.0 / hv)) + c->sc_host[10] * (1.0 / hw);
+    const double rho_min = std::min(P.pipe_oil_density, P.pipe_oil_density * P.rho_pos);  // min(oil, water)
+    const double g_f = std::sqrt(P.pipe_R1 / (P.pipe_V0 * P.pipe_V0) *
+                                 (std::fabs(P.gravity[1]) + std::fabs(1.0 / rho_min * P.pipe_f)) * (1.0 / hv));
+    const double h = std::min(std::min(hu, hv), hw);
+    const double s_f = std::sqrt(((1.0 / P.pipe_We) * c->sc_host[13]) / (std::min(P.rho_pos, 1.0) * (h * h)));
+    const double cv = c_f + 0.0;
+    const double cfl = 0.5 * (cv + std::sqrt((cv * cv + 4.0 * (g_f * g_f)) + 4.0 * (s_f * s_f)));
+    *dt = P.cfl / cfl;
+    return FS_OK;
+  }
   const double inv = 1.0 / c->grid.dx, inv2 = 1.0 / (c->grid.dx * c->grid.dx);
   const double c_f = (c->sc_host[8] * inv + c->sc_host[9] * inv) + c->sc_host[10] * inv;
   const double g_f = std::sqrt(std::fabs(P.gravity[1]) * inv);
@@ -1840,7 +1872,12 @@ static fs_status timed_end(fs_ctx* c, float* ms) {
 
 fs_status fs_step(fs_ctx* c, double dt, fs_step_report* rep) {
   if (!c) { set_error("NULL context"); return FS_INVALID_ARG; }
-  CKS(box_only(c, "fs_step"));
+  if (c->pipe.on && c->prm.viscosity != 0) {
+    // the pipe's semi-implicit viscosity is not built: the step runs as the
+    // reference's with is_sourcing_active = false
+    set_error("fs_step in the pipe mode needs viscosity = 0 (the pipe's viscosity is not built)");
+    return FS_NOT_SUPPORTED;
+  }
   if (!(dt > 0) || !std::isfinite(dt)) { set_error("dt must be positive and finite"); return FS_INVALID_ARG; }
   fs_step_report local{};
   fs_step_report* r = rep ? rep : &local;
@@ -1870,7 +1907,6 @@ fs_status fs_curvature(fs_ctx* c, double* kappa_max) {
 
 fs_status fs_cfl_dt(fs_ctx* c, double* dt) {
   if (!c || !dt) { set_error("NULL argument"); return FS_INVALID_ARG; }
-  CKS(box_only(c, "fs_cfl_dt"));
   return DISPATCH(c, cfl_t, c, dt);
 }
 

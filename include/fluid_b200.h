@@ -145,9 +145,12 @@ typedef struct {
      FS_VELOCITY_ENO3, fs_apply_gravity, fs_project: the cylinder's cells are
      the unknowns, the cells outside it Neumann cells, rho_neg and rho_pos
      the dimensionless densities 1 and water_density/oil_density, the
-     pressure solve with the Jacobi preconditioners only); the viscosity,
-     the CFL time step, fs_step and the adjoints return FS_NOT_SUPPORTED in
-     this mode.  Fixed at creation. */
+     pressure solve with the Jacobi preconditioners only), the CFL time
+     step (fs_cfl_dt: the dimensionless form's terms, no viscous term) and
+     the whole step with viscosity = 0 (fs_step: the reference's step with
+     is_sourcing_active = false); the viscosity (fs_viscosity, fs_step with
+     viscosity != 0) and the adjoints return FS_NOT_SUPPORTED in this mode.
+     Fixed at creation. */
   int pipe;
   double pipe_radius;               /* a: the wall radius in units of the core radius R1 */
   double grid_min[3], grid_max[3];  /* the script's base_grid_min and base_grid_max: cell (i,j,k) sits at

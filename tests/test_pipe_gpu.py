@@ -3,9 +3,11 @@ own outputs (fixtures pipe_*, made by tests/golden/make_golden.py from the
 headless reference build) and against the oracle.
 
 The pipe mode's level-set advection, reinitialisation, ENO3 velocity
-advection, dimensionless body force and projection run on the GPU; its
-viscosity is not built, and that entry point (with fs_step and the CFL time
-step) returns FS_NOT_SUPPORTED in this mode."""
+advection, dimensionless body force, projection and CFL time step run on the
+GPU, and so does the whole step without viscosity (the reference's step with
+is_sourcing_active = false); the pipe's viscosity is not built, and that
+entry point (with fs_step when viscosity != 0) returns FS_NOT_SUPPORTED in
+this mode."""
 import os
 
 import numpy as np
@@ -29,13 +31,15 @@ def solver(g, precision=fs.FS_PRECISION_FP64, flags=fs.FS_FLAG_REINIT_TYPO, **kw
     # the projection's dimensionless densities: 1 in the oil (phi <= 0),
     # water_density/oil_density in the water (PROJECTION_3D.h:642-669)
     water = float(g["water_density"]) if "water_density" in g else 0.995
-    return fs.Solver(n, dx, precision=precision, pipe=1, pipe_radius=float(g["a"]), grid_min=tuple(g["lo"]),
-                     grid_max=tuple(g["hi"]), pipe_R1=float(g["R1"]), pipe_V0=float(g["V0"]), pipe_f=float(g["f"]),
-                     pipe_eta=float(g["eta"]), pipe_oil_density=float(g["oil_density"]), pipe_We=float(g["We"]),
-                     rho_neg=1.0, rho_pos=water / float(g["oil_density"]),
-                     gravity=(0.0, float(g["gravity_y"]), 0.0), weno_epsilon=float(g["epsilon"]),
-                     reinit_iterations=int(g["reinit_iterations"]), reinit_scaling=int(g["reinit_scaling"]),
-                     flags=flags, viscosity=0, velocity_scheme=fs.FS_VELOCITY_ENO3, **kw)
+    args = dict(precision=precision, pipe=1, pipe_radius=float(g["a"]), grid_min=tuple(g["lo"]),
+                grid_max=tuple(g["hi"]), pipe_R1=float(g["R1"]), pipe_V0=float(g["V0"]), pipe_f=float(g["f"]),
+                pipe_eta=float(g["eta"]), pipe_oil_density=float(g["oil_density"]), pipe_We=float(g["We"]),
+                rho_neg=1.0, rho_pos=water / float(g["oil_density"]),
+                gravity=(0.0, float(g["gravity_y"]), 0.0), weno_epsilon=float(g["epsilon"]),
+                reinit_iterations=int(g["reinit_iterations"]), reinit_scaling=int(g["reinit_scaling"]),
+                flags=flags, viscosity=0, velocity_scheme=fs.FS_VELOCITY_ENO3)
+    args.update(kw)
+    return fs.Solver(n, dx, **args)
 
 
 def upload(s, g, keys=("phi", "u", "v", "w")):
@@ -117,7 +121,7 @@ def test_pipe_mode_refuses_the_operators_it_does_not_build():
     g = load("pipe_levelset")
     with solver(g) as s:
         upload(s, g)
-        for call in (lambda: s.step(1e-3), lambda: s.viscosity(1e-3), lambda: s.cfl_dt()):
+        for call in (lambda: s.viscosity(1e-3),):
             with pytest.raises(fs.FsError) as e:
                 call()
             assert e.value.status == fs.FS_NOT_SUPPORTED
@@ -198,3 +202,54 @@ def test_pipe_projection_matches_oracle_corrected_system():
     assert np.abs(dp - dp.mean()).max() <= 1e-8 * np.abs(p[fl]).max()
     for k, ref in zip("uvw", (u, v, w)):
         assert np.abs(got[k] - ref).max() <= 1e-8 * max(np.abs(ref - g[k]).max(), 1.0), k
+
+
+@pytest.mark.parametrize("precision,tol", [(fs.FS_PRECISION_FP64, 1e-14), (fs.FS_PRECISION_FP32_REFINE, 1e-6)])
+def test_pipe_cfl_matches_reference(precision, tol):
+    """CFLOneTimeStep of the pipe on the projected velocities of fixture
+    pipe_projection, with the curvature maximum of its level set (the
+    reference's comes from the projection just run on the same level set)."""
+    g = load("pipe_projection")
+    with solver(g, precision, flags=fs.FS_FLAG_REINIT_TYPO | fs.FS_FLAG_CURVATURE_TYPO, cfl=1.0) as s:
+        s.upload("phi", g["phi"])
+        for k in "uvw":
+            s.upload(k, g["out_" + k])
+        dt = s.cfl_dt()
+    assert abs(dt - float(g["cfl"])) <= tol * float(g["cfl"])
+
+
+@pytest.mark.parametrize("precision,tol", [(fs.FS_PRECISION_FP64, 1e-9), (fs.FS_PRECISION_FP32_REFINE, 5e-4)])
+def test_pipe_frame_matches_reference(precision, tol):
+    """One whole SIMULATION_WORLD::AdvanceOneFrame of the pipe with the
+    sourcing step off (fixture pipe_frame): fs_cfl_dt times the script's CFL
+    gives the reference's dt, then fs_step (order 2: level-set Heun, velocity
+    Heun over ENO3 advection + body force + projection, reinitialisation
+    Heun).  Fields to `tol` of their maximum: 1e-9 in FP64 (the PCG stops at
+    the reference's absolute r.z < tol^2 within an iteration or two of it),
+    5e-4 with FP32 storage; the pressure on the unknowns likewise."""
+    g = load("pipe_frame")
+    fp64 = precision == fs.FS_PRECISION_FP64
+    flags = fs.FS_FLAG_REINIT_TYPO | fs.FS_FLAG_FAITHFUL_PROJECTION | fs.FS_FLAG_CURVATURE_TYPO
+    kw = dict(stop=fs.FS_STOP_ABSOLUTE, tolerance=float(g["tolerance"])) if fp64 else dict(tolerance=1e-9)
+    with solver(g, precision, flags=flags, order=2, cfl=float(g["cfl_number"]),
+                max_iteration=int(g["max_iteration"]), **kw) as s:
+        upload(s, g)
+        dt = s.cfl_dt()
+        assert abs(dt - float(g["dt"])) <= (1e-14 if fp64 else 1e-6) * float(g["dt"])
+        s.step(float(g["dt"]))
+        got = {k: s.download(k) for k in ("phi", "u", "v", "w", "pressure")}
+    for k in ("phi", "u", "v", "w"):
+        ref = g["out_" + k]
+        assert np.abs(got[k] - ref).max() <= tol * np.abs(ref).max(), (k, np.abs(got[k] - ref).max())
+    fl = g["boundary"] <= 0
+    ref = g["out_p"]
+    assert np.abs(got["pressure"][fl] - ref[fl]).max() <= tol * np.abs(ref).max()
+
+
+def test_pipe_step_refuses_viscosity():
+    g = load("pipe_frame")
+    with solver(g, viscosity=1) as s:
+        upload(s, g)
+        with pytest.raises(fs.FsError) as e:
+            s.step(1e-3)
+        assert e.value.status == fs.FS_NOT_SUPPORTED
