@@ -9,8 +9,9 @@ thread ids return without doing anything.
 """
 import numpy as np
 
-from . import (FS_FLAG_FAITHFUL_PROJECTION, FS_PRECISION_FP32_REFINE, FS_PRECISION_FP64, FS_STOP_ABSOLUTE,
-               FS_STOP_RELATIVE, FS_VELOCITY_ENO3, FS_VELOCITY_WENO5, FsError, Solver, default_params, pcg_csr)
+from . import (FS_FLAG_CURVATURE_TYPO, FS_FLAG_FAITHFUL_PROJECTION, FS_FLAG_REINIT_TYPO, FS_PRECISION_FP32_REFINE,
+               FS_PRECISION_FP64, FS_STOP_ABSOLUTE, FS_STOP_RELATIVE, FS_VELOCITY_ENO3, FS_VELOCITY_WENO5, FsError,
+               Solver, default_params, pcg_csr)
 from .script import SCRIPT_BLOCK, SCRIPT_READER
 
 
@@ -153,6 +154,59 @@ def params_from_block(block, base_grid):
     return p
 
 
+def pipe_params_from_script(world, fluid_block, grid):
+    """fs_params for the reference's oil/water vertical pipe (pipe = 1) from
+    its SIMULATION_WORLD block (a, R2, CFL; SIMULATION_WORLD.h:119-125) and
+    FLUID_SOLVER_UNIFORM_OIL_WATER block, with the dimensionless constants
+    the reference derives from them (EULERIAN_FLUID_SOLVER_3D.h:496-514):
+      R1 = R2/a,  f = g (oil - K water)/(K - 1),
+      A = (a^2 - 1) + (m K + 2 (K - 1) ln a),
+      V0 = (f + water g) R1^2/(4 water_viscosity) A,
+      J = sigma R1 oil/oil_viscosity^2,  Re = oil R1 |V0|/oil_viscosity,
+      We = Re^2/J.
+    The projection's densities are 1 (oil, phi <= 0) and water/oil; the
+    operators run as the reference's do (its Sussman and curvature slips,
+    the deflated pressure system, PCG to r.z < tol^2).  The pipe's
+    viscosity is not built, so the script must switch the sourcing step off
+    (is_sourcing_active = false)."""
+    if fluid_block.GetBoolean("is_sourcing_active", True):
+        raise ValueError("the pipe mode's viscosity is not built: set is_sourcing_active = false in "
+                         "FLUID_SOLVER_UNIFORM_OIL_WATER")
+    if not fluid_block.GetBoolean("dimensionless_form", False):
+        raise ValueError("the pipe mode is built for dimensionless_form = true")
+    if fluid_block.FindBlock("VELOCITY_ADVECTION").GetBoolean("use_5th_weno_v", False):
+        raise ValueError("the pipe mode advects the velocity with ENO3 (use_3rd_eno_v) only")
+    a, R2 = world.GetFloat("a", 1.0), world.GetFloat("R2", 1.0)
+    m, eta = fluid_block.GetFloat("m", 1.0), fluid_block.GetFloat("eta", 1.0)
+    K, g = fluid_block.GetFloat("K", 1.0), fluid_block.GetFloat("g", 1.0)
+    wd, od = fluid_block.GetFloat("water_density", 1.0), fluid_block.GetFloat("oil_density", 1.0)
+    wv, ov = fluid_block.GetFloat("water_viscosity", 1.0), fluid_block.GetFloat("oil_viscosity", 0.0)
+    sigma = fluid_block.GetFloat("surface_tension", 0.0)
+    R1 = R2 / a
+    f = 1.0 / (K - 1.0) * g * (od - K * wd)
+    A = (a * a - 1.0) + (m * K + 2.0 * (K - 1) * np.log(a))
+    V0 = (f + wd * g) * (R1 * R1) / (4.0 * wv) * A
+    J = sigma * R1 * od / (ov * ov)
+    Re = (od * R1 * abs(V0)) / ov
+    We = (1.0 / J) * (Re * Re)
+    proj = fluid_block.FindBlock("PROJECTION_WATER")
+    adv = fluid_block.FindBlock("LEVELSET_ADVECTION")
+    return default_params(
+        pipe=1, pipe_radius=a, grid_min=(grid.x_min, grid.y_min, grid.z_min),
+        grid_max=(grid.x_max, grid.y_max, grid.z_max), pipe_R1=R1, pipe_V0=float(V0), pipe_f=f, pipe_eta=eta,
+        pipe_oil_density=od, pipe_We=float(We), rho_neg=1.0, rho_pos=wd / od,
+        gravity=fluid_block.GetVector3("gravity", (0.0, -9.8, 0.0)),
+        weno_epsilon=adv.GetFloat("epsilon", 10e-6),
+        reinit_iterations=(fluid_block.GetInteger("iteration_number_for_reinitialization", 10)
+                           if fluid_block.GetBoolean("sussmanstyle_reinitialization", False) else 0),
+        reinit_scaling=fluid_block.GetInteger("scaling_number_for_reinitialization", 5),
+        order=fluid_block.GetInteger("order_for_time_advancing", 1),
+        stop=FS_STOP_ABSOLUTE, tolerance=proj.GetFloat("tolerance", 1e-4),
+        max_iteration=proj.GetInteger("max_iteration", 30), viscosity=0,
+        flags=FS_FLAG_FAITHFUL_PROJECTION | FS_FLAG_REINIT_TYPO | FS_FLAG_CURVATURE_TYPO,
+        velocity_scheme=FS_VELOCITY_ENO3, cfl=world.GetFloat("CFL", 0.5))
+
+
 class PROJECTION_3D:
     """Pressure projection bound to a solver's fields (PROJECTION_3D.h:416)."""
 
@@ -194,14 +248,27 @@ class EULERIAN_FLUID_SOLVER_3D:
 
     @classmethod
     def FromScript(cls, path, cfl=None):
-        """Build from a reference .sim file (air/water box mode).  A script
-        in the reference's oil/water pipe mode (SIMULATION_WORLD.h:119-122,
-        the mode its own four scripts select) is refused: this solver has no
-        pipe geometry, so running it as a box would be silently wrong."""
+        """Build from a reference .sim file: the air/water box mode, or the
+        oil/water vertical pipe (SIMULATION_WORLD.h:119-122, the mode the
+        reference's own four scripts select) with its sourcing step off
+        (pipe_params_from_script).  Pipe scripts that need the pipe's
+        viscosity, and horizontal pipes, are refused rather than run wrong."""
         r = SCRIPT_READER(path)
         world = r.FindBlock("SIMULATION_WORLD")
         if world.GetBoolean("oil_water_simulation", False):
-            raise ValueError("oil_water_simulation (the pipe mode) is not supported; use air_water_simulation")
+            disc = world.FindBlock("WORLD_DISCRETIZATION_OIL_WATER")
+            if not disc.FindBlock("PIPE_OPTIONS").GetBoolean("is_vertical", False):
+                raise ValueError("the pipe mode is built for the vertical pipe (PIPE_OPTIONS.is_vertical) only")
+            grid = GRID_STRUCTURE_3D().InitializeFromBlock(disc.FindBlock("GRID_STRUCTURE_3D_VERTICAL"))
+            p = pipe_params_from_script(world, r.FindBlock("FLUID_SOLVER_UNIFORM_OIL_WATER"), grid)
+            if cfl is not None:
+                p.cfl = cfl
+            s = cls()
+            s.base_grid = grid
+            s.order_for_time_advancing = p.order
+            s.solver = Solver((grid.i_res, grid.j_res, grid.k_res), grid.dx, p)
+            s.water_projection = PROJECTION_3D(s.solver)
+            return s
         grid = GRID_STRUCTURE_3D().InitializeFromBlock(
             world.FindBlock("WORLD_DISCRETIZATION_AIR_WATER").FindBlock("GRID_STRUCTURE_3D_LARGE"))
         s = cls().InitializeFromScriptBlock(None, grid, r.FindBlock("FLUID_SOLVER_UNIFORM_AIR_WATER"))

@@ -376,6 +376,69 @@ inline fs_params params_from_block(const SCRIPT_BLOCK& block, const GRID_STRUCTU
   return p;
 }
 
+// fs_params for the reference's oil/water vertical pipe from its
+// SIMULATION_WORLD block (a, R2, CFL; SIMULATION_WORLD.h:119-125) and
+// FLUID_SOLVER_UNIFORM_OIL_WATER block, with the dimensionless constants the
+// reference derives (EULERIAN_FLUID_SOLVER_3D.h:496-514): R1 = R2/a,
+// f = g (oil - K water)/(K - 1), A = (a^2 - 1) + (m K + 2 (K - 1) ln a),
+// V0 = (f + water g) R1^2/(4 water_viscosity) A, J = sigma R1 oil/
+// oil_viscosity^2, Re = oil R1 |V0|/oil_viscosity, We = Re^2/J.  The
+// operators run as the reference's do; the pipe's viscosity is not built, so
+// the script must switch the sourcing step off (is_sourcing_active = false).
+inline fs_params pipe_params_from_script(const SCRIPT_BLOCK& world, const SCRIPT_BLOCK& block,
+                                         const GRID_STRUCTURE_3D& grid) {
+  if (block.GetBoolean("is_sourcing_active", true))
+    throw std::invalid_argument("the pipe mode's viscosity is not built: set is_sourcing_active = false");
+  if (!block.GetBoolean("dimensionless_form", false))
+    throw std::invalid_argument("the pipe mode is built for dimensionless_form = true");
+  if (block.FindBlock("VELOCITY_ADVECTION").GetBoolean("use_5th_weno_v", false))
+    throw std::invalid_argument("the pipe mode advects the velocity with ENO3 (use_3rd_eno_v) only");
+  const double a = world.GetFloat("a", 1.0), R2 = world.GetFloat("R2", 1.0);
+  const double m = block.GetFloat("m", 1.0), eta = block.GetFloat("eta", 1.0);
+  const double K = block.GetFloat("K", 1.0), g = block.GetFloat("g", 1.0);
+  const double wd = block.GetFloat("water_density", 1.0), od = block.GetFloat("oil_density", 1.0);
+  const double wv = block.GetFloat("water_viscosity", 1.0), ov = block.GetFloat("oil_viscosity", 0.0);
+  const double sigma = block.GetFloat("surface_tension", 0.0);
+  const double R1 = R2 / a;
+  const double f = 1.0 / (K - 1.0) * g * (od - K * wd);
+  const double A = (a * a - 1.0) + (m * K + 2.0 * (K - 1) * std::log(a));
+  const double V0 = (f + wd * g) * (R1 * R1) / (4.0 * wv) * A;
+  const double J = sigma * R1 * od / (ov * ov);
+  const double Re = (od * R1 * std::abs(V0)) / ov;
+  const double We = (1.0 / J) * (Re * Re);
+  const SCRIPT_BLOCK& proj = block.FindBlock("PROJECTION_WATER");
+  fs_params p;
+  fs_params_default(&p);
+  p.pipe = 1;
+  p.pipe_radius = a;
+  p.grid_min[0] = grid.x_min; p.grid_min[1] = grid.y_min; p.grid_min[2] = grid.z_min;
+  p.grid_max[0] = grid.x_max; p.grid_max[1] = grid.y_max; p.grid_max[2] = grid.z_max;
+  p.pipe_R1 = R1;
+  p.pipe_V0 = V0;
+  p.pipe_f = f;
+  p.pipe_eta = eta;
+  p.pipe_oil_density = od;
+  p.pipe_We = We;
+  p.rho_neg = 1.0;
+  p.rho_pos = wd / od;
+  const double g_def[3] = {0.0, -9.8, 0.0};
+  block.GetVector3("gravity", p.gravity, g_def);
+  p.weno_epsilon = block.FindBlock("LEVELSET_ADVECTION").GetFloat("epsilon", 10e-6);
+  p.reinit_iterations = block.GetBoolean("sussmanstyle_reinitialization", false)
+                            ? block.GetInteger("iteration_number_for_reinitialization", 10)
+                            : 0;
+  p.reinit_scaling = block.GetInteger("scaling_number_for_reinitialization", 5);
+  p.order = block.GetInteger("order_for_time_advancing", 1);
+  p.stop = FS_STOP_ABSOLUTE;
+  p.tolerance = proj.GetFloat("tolerance", 1e-4);
+  p.max_iteration = proj.GetInteger("max_iteration", 30);
+  p.viscosity = 0;
+  p.flags = FS_FLAG_FAITHFUL_PROJECTION | FS_FLAG_REINIT_TYPO | FS_FLAG_CURVATURE_TYPO;
+  p.velocity_scheme = FS_VELOCITY_ENO3;
+  p.cfl = world.GetFloat("CFL", 0.5);
+  return p;
+}
+
 // ---------------------------------------------------------------------------
 // solver classes
 // ---------------------------------------------------------------------------
@@ -432,14 +495,25 @@ class EULERIAN_FLUID_SOLVER_3D {  // EULERIAN_FLUID_SOLVER_3D.h
     water_projection->nz_ = g.nz;
     params_ = p;
   }
-  // an air/water box .sim script (SIMULATION_WORLD.h:InitializeFromScript)
+  // a .sim script (SIMULATION_WORLD.h:InitializeFromScript): the air/water
+  // box, or the oil/water vertical pipe with its sourcing step off
+  // (pipe_params_from_script); pipe scripts that need the pipe's viscosity,
+  // and horizontal pipes, are refused rather than run wrong
   void InitializeFromScript(const std::string& path) {
     SCRIPT_READER r(path);
     const SCRIPT_BLOCK& world = r.FindBlock("SIMULATION_WORLD");
-    // the reference's oil/water pipe mode (SIMULATION_WORLD.h:119-122) has no
-    // counterpart here: refuse it rather than run the script as a box
-    if (world.GetBoolean("oil_water_simulation", false))
-      throw std::invalid_argument("oil_water_simulation (the pipe mode) is not supported; use air_water_simulation");
+    if (world.GetBoolean("oil_water_simulation", false)) {
+      const SCRIPT_BLOCK& disc = world.FindBlock("WORLD_DISCRETIZATION_OIL_WATER");
+      if (!disc.FindBlock("PIPE_OPTIONS").GetBoolean("is_vertical", false))
+        throw std::invalid_argument("the pipe mode is built for the vertical pipe (PIPE_OPTIONS.is_vertical) only");
+      GRID_STRUCTURE_3D g;
+      g.InitializeFromBlock(disc.FindBlock("GRID_STRUCTURE_3D_VERTICAL"));
+      base_grid = g;
+      const fs_params p = pipe_params_from_script(world, r.FindBlock("FLUID_SOLVER_UNIFORM_OIL_WATER"), g);
+      order_for_time_advancing = p.order;
+      Create(p);
+      return;
+    }
     GRID_STRUCTURE_3D g;
     g.InitializeFromBlock(world.FindBlock("WORLD_DISCRETIZATION_AIR_WATER").FindBlock("GRID_STRUCTURE_3D_LARGE"));
     InitializeFromScriptBlock(g, r.FindBlock("FLUID_SOLVER_UNIFORM_AIR_WATER"));

@@ -138,8 +138,9 @@ def test_cpp_levelset_mirror_sweeps_and_writes_obj_like_python(mirror, tmp_path)
 
 
 def test_pipe_mode_scripts_are_refused(mirror, tmp_path):
-    """A script in the reference's oil/water pipe mode is refused by both
-    script readers instead of being run as a box."""
+    """A box script switched to the reference's oil/water pipe mode (no pipe
+    blocks, so no vertical pipe) is refused by both script readers instead of
+    being run as a box."""
     path = write_script(str(tmp_path / "pipe.sim"), 16)
     text = open(path).read()
     assert "oil_water_simulation = false" in text

@@ -253,3 +253,26 @@ def test_pipe_step_refuses_viscosity():
         with pytest.raises(fs.FsError) as e:
             s.step(1e-3)
         assert e.value.status == fs.FS_NOT_SUPPORTED
+
+
+def test_pipe_script_frame_matches_reference(tmp_path):
+    """The drop-in path: the reference's pipe script (sourcing off) read by
+    EULERIAN_FLUID_SOLVER_3D.FromScript, the fixture's fields set, the CFL dt
+    and one AdvanceOneTimeStepThread against the reference's frame."""
+    from fluid_simulator_backup_b200 import reference_api as R
+    from oracle import refsim
+    g = load("pipe_frame")
+    n = tuple(int(x) for x in g["n"])
+    path = refsim.write_pipe_sim(str(tmp_path / "pipe.sim"), n, tuple(g["lo"]), tuple(g["hi"]), sourcing=False)
+    s = R.EULERIAN_FLUID_SOLVER_3D.FromScript(path)
+    try:
+        s.water_levelset = g["phi"]
+        s.set_velocity(g["u"], g["v"], g["w"])
+        dt = s.CFLOneTimeStep() * s.solver.params.cfl
+        assert abs(dt - float(g["dt"])) <= 1e-14 * float(g["dt"])
+        s.AdvanceOneTimeStepThread(0, float(g["dt"]))
+        assert np.abs(s.water_levelset - g["out_phi"]).max() <= 1e-9 * np.abs(g["out_phi"]).max()
+        for k, a in zip("uvw", s.velocity()):
+            assert np.abs(a - g["out_" + k]).max() <= 1e-9 * np.abs(g["out_" + k]).max(), k
+    finally:
+        s.solver.close()
