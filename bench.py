@@ -597,7 +597,8 @@ def main():
         traffic = None
     elif rb:
         bpu = BYTES_PER_CELL_PCG_RB
-        kernel = "red-black IC(0) PCG iteration (pipelined Schur-complement spmv + update + direction, 3 kernels)"
+        kernel = ("red-black IC(0) PCG iteration (Schur-complement red and black passes, p.q, residual update, "
+                  "direction update: 5 kernels)")
         traffic = TRAFFIC_PER_ITERATION_256_RB * N / 256 ** 3 if TRAFFIC_PER_ITERATION_256_RB else None
     else:
         bpu, kernel = BYTES_PER_UNKNOWN_PCG_FP32, "FP32 Jacobi PCG iteration (spmv + update + direction, 3 kernels)"
