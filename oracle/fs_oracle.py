@@ -2019,3 +2019,236 @@ def pipe_step(phi, u, v, w, grids, C, dt, P):
     r2 = pipe_reinitialization(r1, grids, P["reinit_iterations"], P["reinit_scaling"], P["epsilon"])
     phi = 0.5 * (phi + r2)
     return phi, u, v, w, p
+
+
+# ----------------------------------------------------------------------------
+# Oil/water pipe mode, vertical pipe: the semi-implicit viscosity
+# (VISCOSITY_3D.h:565-990, 1234-1547, 2048-2300; POISSON_SOLVER_3D.h:342-378,
+# 3641-3828)
+# ----------------------------------------------------------------------------
+
+def _pipe_visc_copies(comp, b, axis):
+    """The velocity copies SetupBoundaryConditionsForVelocity makes for the
+    pipe's viscosity (VISCOSITY_3D.h:2048-2300), one component: the masked
+    periodic copy `gen` and the copies guarded along x (`cx`) and z (`cz`).
+    On faces outside the pipe the guarded copies follow one if/else chain:
+    all four transverse neighbours outside -> both 0; else an inside x-1
+    (x+1) neighbour gives cx the extrapolation (theta-1)/theta of that
+    neighbour; else an inside z-1 (z+1) neighbour gives cz the same; else
+    both 0.  The neighbour's value is the masked copy's (the y component
+    reads its raw velocity instead, :2166-2200).  Ghosted arrays (G)."""
+    g = G
+    gen = _pipe_periodic_copy(comp, b, axis == 1)
+    src = np.pad(comp, g) if axis == 1 else gen
+    cx, cz = gen.copy(), gen.copy()
+    nz, ny, nx = b.shape
+    bp = np.pad(b, 1)
+    c = (slice(1, -1),) * 3
+
+    def bn(ax, s):
+        sl = list(c)
+        sl[ax] = slice(1 + s, bp.shape[ax] - 1 + s)
+        return bp[tuple(sl)]
+
+    def vn(ax, s):
+        sl = [slice(g, g + nz), slice(g, g + ny), slice(g, g + nx)]
+        sl[ax] = slice(g + s, g + s + b.shape[ax])
+        return src[tuple(sl)]
+
+    def ext(bnb, val):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            theta = np.abs(bnb) / (np.abs(bnb) + np.abs(b))
+            return (theta - 1.0) / theta * val
+
+    out = b > 0
+    all4 = (bn(2, -1) > 0) & (bn(2, 1) > 0) & (bn(0, -1) > 0) & (bn(0, 1) > 0)
+    xm, xp, zm, zp = bn(2, -1) < 0, bn(2, 1) < 0, bn(0, -1) < 0, bn(0, 1) < 0
+    ix = (slice(g, g + nz), slice(g, g + ny), slice(g, g + nx))
+    cxi, czi = cx[ix], cz[ix]
+    new_x = np.where(out & all4, 0.0, cxi)
+    new_z = np.where(out & all4, 0.0, czi)
+    r1 = out & ~all4 & xm
+    r2 = out & ~all4 & ~xm & xp
+    r3 = out & ~all4 & ~xm & ~xp & zm
+    r4 = out & ~all4 & ~xm & ~xp & ~zm & zp
+    r5 = out & ~all4 & ~xm & ~xp & ~zm & ~zp
+    new_x = np.where(r1, ext(bn(2, -1), vn(2, -1)), new_x)
+    new_x = np.where(r2, ext(bn(2, 1), vn(2, 1)), new_x)
+    new_z = np.where(r3, ext(bn(0, -1), vn(0, -1)), new_z)
+    new_z = np.where(r4, ext(bn(0, 1), vn(0, 1)), new_z)
+    new_x = np.where(r5, 0.0, new_x)
+    new_z = np.where(r5, 0.0, new_z)
+    cx[ix] = new_x
+    cz[ix] = new_z
+    return gen, cx, cz
+
+
+def _shifted(a, ax, s, fill=0.0):
+    """a shifted so that out[idx] = a[idx + s e_ax], `fill` beyond the array."""
+    out = np.full_like(a, fill)
+    src = [slice(None)] * 3
+    dst = [slice(None)] * 3
+    if s > 0:
+        src[ax], dst[ax] = slice(s, None), slice(0, -s)
+    else:
+        src[ax], dst[ax] = slice(0, s), slice(-s, None)
+    out[tuple(dst)] = a[tuple(src)]
+    return out
+
+
+def pipe_viscosity_system(comp, b, axis, coefs, explicit, gen, dx_copy, dz_copy, dx, tol, max_iter):
+    """One component of the pipe's semi-implicit solve (SolveForViscosity,
+    POISSON_SOLVER_3D.h:342-378, with BuildLinearSystemNodeForSemiImplicit-
+    Viscosity :3641-3828 and the boundary tags of SetupBoundaryConditions-
+    ForVelocity, VISCOSITY_3D.h:1350-1547).  Unknowns: faces inside the pipe
+    (wall distance <= 0) with 0 <= j < ny; faces outside are Dirichlet, the
+    rows beyond the ends periodic (row -1 is row ny-2, row ny is row 1, for
+    every component).  Row: (1 + sum(coef)/dx^2) x_c - sum coef_n/dx^2 x_n,
+    the sum in the reference's order (unknown neighbours l, r, b, t, d, u,
+    then periodic b, t, then Dirichlet l, r, d, u; a zero sum becomes 1);
+    right-hand side the explicit term plus the Dirichlet neighbours'
+    coef/dx^2 times their guarded copies (dx_copy along x, dz_copy along z);
+    initial guess the masked copy; the reference's PCG (asymmetric matrix,
+    absolute r.z < tol^2).  Returns (new component, iterations)."""
+    g = G
+    c1, c2, c3, c4, c5, c6 = coefs
+    nz, ny, nx = b.shape
+    jrows = np.arange(ny)[None, :, None]
+    rows = (b <= 0) & (jrows < (ny - 1 if axis == 1 else ny))
+    inv2 = 1.0 / (dx * dx)
+    zero = np.zeros_like(b)
+    l_full, r_full = _shifted(rows, 2, -1, False) & rows, _shifted(rows, 2, 1, False) & rows
+    d_full, u_full = _shifted(rows, 0, -1, False) & rows, _shifted(rows, 0, 1, False) & rows
+    b_full = rows & (jrows > 0)
+    t_full = rows & (jrows < ny - (2 if axis == 1 else 1))
+    b_per = rows & (jrows == 0)
+    t_per = rows & (jrows == ny - (2 if axis == 1 else 1))
+    l_dir, r_dir = rows & (_shifted(b, 2, -1) > 0), rows & (_shifted(b, 2, 1) > 0)
+    d_dir, u_dir = rows & (_shifted(b, 0, -1) > 0), rows & (_shifted(b, 0, 1) > 0)
+    coef = zero
+    for m, cv in ((l_full, c2), (r_full, c1), (b_full, c4), (t_full, c3), (d_full, c6), (u_full, c5),
+                  (b_per, c4), (t_per, c3), (l_dir, c2), (r_dir, c1), (d_dir, c6), (u_dir, c5)):
+        coef = coef + np.where(m, cv, 0.0)
+    coef = np.where(rows & (coef == 0), 1.0, coef)
+    diag = np.where(rows, 1.0 + inv2 * coef, 1.0)
+    ix = (slice(g, g + nz), slice(g, g + ny), slice(g, g + nx))
+    vx, vz = dx_copy, dz_copy
+
+    def nbv(a, ax, s):
+        sl = list(ix)
+        sl[ax] = slice(ix[ax].start + s, ix[ax].stop + s)
+        return a[tuple(sl)]
+
+    rhs = np.where(rows, explicit, 0.0)
+    for m, cv, val in ((l_dir, c2, nbv(vx, 2, -1)), (r_dir, c1, nbv(vx, 2, 1)), (d_dir, c6, nbv(vz, 0, -1)),
+                       (u_dir, c5, nbv(vz, 0, 1))):
+        rhs = np.where(m, rhs + cv * inv2 * val, rhs)
+    x0 = np.where(rows, gen[ix], 0.0)
+    off = [(l_full, -c2 * inv2, (2, -1)), (r_full, -c1 * inv2, (2, 1)), (b_full, -c4 * inv2, (1, -1)),
+           (t_full, -c3 * inv2, (1, 1)), (d_full, -c6 * inv2, (0, -1)), (u_full, -c5 * inv2, (0, 1))]
+    jb = ny - 2 if axis != 1 else ny - 3  # the periodic images of rows -1 and ny-1+1
+
+    def apply(x):
+        q = np.zeros_like(x)
+        for m, val, (ax, s) in off:
+            q = q + np.where(m, val * _shifted(x, ax, s), 0.0)
+        q = q + np.where(b_per, (-c4 * inv2) * np.broadcast_to(x[:, jb:jb + 1, :], x.shape), 0.0)
+        q = q + np.where(t_per, (-c3 * inv2) * np.broadcast_to(x[:, 1:2, :], x.shape), 0.0)
+        return q + diag * x
+
+    x, it, _rz, _rel = pcg(apply, diag, rhs, x0, tol, max_iter, "abs")
+    out = np.where(rows, x, comp)
+    if axis == 1:
+        out[:, ny - 1, :] = out[:, 1, :]
+    return out, it
+
+
+def pipe_viscosity(phi, u, v, w, grids, C, dt, tol, max_iter):
+    """VISCOSITY_3D::ApplyViscosity of a vertical pipe, the oil/water
+    semi-implicit branch in the dimensionless form (VISCOSITY_3D.h:565-990),
+    epsilon 1.5 dx (EULERIAN_FLUID_SOLVER_3D.h:394).  Per component, from
+    the velocity copies made before any component is solved: smeared
+    density rho = 1 + (eta - 1) H and viscosity mu = 1 + (m - 1) H (H the
+    viscosity's Heaviside, :1234-1350) of face and edge averages of the
+    periodic level set; coef_q = dt/(Re rho) mu (2 dt/(Re rho) mu along the
+    component's own axis); the explicit cross terms; then the implicit solve
+    (pipe_viscosity_system).  Returns (u, v, w, info)."""
+    g = G
+    dx = grids[0][3]
+    idx = idy = idz = 1.0 / dx
+    eps = 1.5 * dx
+    Re, m, eta = C["Re"], C["m"], C["eta"]
+    comps = (u, v, w)
+    bs = [pipe_boundary(grids[1 + a], comps[a].shape, C["a"]) for a in range(3)]
+    cp = [_pipe_visc_copies(comps[a], bs[a], a) for a in range(3)]  # (gen, cx, cz)
+    wa = periodic_ghosts_y(phi)
+    H = lambda x: heaviside_viscosity(x, eps)
+    rho_of = lambda x: 1.0 + (eta - 1.0) * H(x)
+    mu_of = lambda x: 1.0 + (m - 1.0) * H(x)
+    nzc, nyc, nxc = phi.shape
+    out, info = [], {}
+    for a in range(3):
+        sh = comps[a].shape
+
+        def W(di, dj, dk):
+            return wa[g + dk:g + dk + sh[0], g + dj:g + dj + sh[1], g + di:g + di + sh[2]]
+
+        def F(arr, di, dj, dk, shape):  # a ghosted face copy at the offset, on this component's face grid
+            return arr[g + dk:g + dk + sh[0], g + dj:g + dj + sh[1], g + di:g + di + sh[2]]
+
+        if a == 0:
+            lo, hi = W(-1, 0, 0), W(0, 0, 0)
+            half = 0.5 * (lo + hi)
+            e1 = 0.25 * (((lo + hi) + W(-1, 1, 0)) + W(0, 1, 0))   # cu
+            e2 = 0.25 * (((lo + hi) + W(-1, -1, 0)) + W(0, -1, 0))  # cd
+            e3 = 0.25 * (((lo + hi) + W(-1, 0, 1)) + W(0, 0, 1))   # ct
+            e4 = 0.25 * (((lo + hi) + W(-1, 0, -1)) + W(0, 0, -1))  # cb
+            rho = rho_of(half)
+            mu_r, mu_c, mu_cu, mu_cd, mu_ct, mu_cb = (mu_of(x) for x in (hi, lo, e1, e2, e3, e4))
+            A, A2 = dt / (Re * rho), (2.0 * dt) / (Re * rho)
+            coefs = (A2 * mu_r, A2 * mu_c, A * mu_cu, A * mu_cd, A * mu_ct, A * mu_cb)
+            yx, zx = cp[1][1], cp[2][1]
+            ex = F(cp[0][0], 0, 0, 0, sh) + A * (idy * (mu_cu * idx * (F(yx, 0, 1, 0, sh) - F(yx, -1, 1, 0, sh))
+                                                      - mu_cd * idx * (F(yx, 0, 0, 0, sh) - F(yx, -1, 0, 0, sh))))
+            ex = ex + A * (idz * (mu_ct * idx * (F(zx, 0, 0, 1, sh) - F(zx, -1, 0, 1, sh))
+                                  - mu_cb * idx * (F(zx, 0, 0, 0, sh) - F(zx, -1, 0, 0, sh))))
+        elif a == 1:
+            lo, hi = W(0, -1, 0), W(0, 0, 0)
+            half = 0.5 * (lo + hi)
+            e1 = 0.25 * (((lo + W(1, -1, 0)) + hi) + W(1, 0, 0))             # cu
+            e2 = 0.25 * (((W(-1, -1, 0) + lo) + W(-1, 0, 0)) + hi)           # cl
+            e3 = 0.25 * (((W(0, -1, 1) + lo) + W(0, 0, 1)) + hi)             # ct
+            e4 = 0.25 * (((W(0, -1, -1) + lo) + W(0, 0, -1)) + hi)           # cb
+            rho = rho_of(half)
+            mu_cu, mu_cl, mu_u, mu_c, mu_ct, mu_cb = (mu_of(x) for x in (e1, e2, hi, lo, e3, e4))
+            A, A2 = dt / (Re * rho), (2.0 * dt) / (Re * rho)
+            coefs = (A * mu_cu, A * mu_cl, A2 * mu_u, A2 * mu_c, A * mu_ct, A * mu_cb)
+            xx, zz = cp[0][1], cp[2][2]
+            ex = F(cp[1][0], 0, 0, 0, sh) + A * (idx * (mu_cu * idy * (F(xx, 1, 0, 0, sh) - F(xx, 1, -1, 0, sh))
+                                                      - mu_cl * idy * (F(xx, 0, 0, 0, sh) - F(xx, 0, -1, 0, sh))))
+            ex = ex + A * (idz * (mu_ct * idy * (F(zz, 0, 0, 1, sh) - F(zz, 0, -1, 1, sh))
+                                  - mu_cb * idx * (F(zz, 0, 0, 0, sh) - F(zz, 0, -1, 0, sh))))
+        else:
+            lo, hi = W(0, 0, -1), W(0, 0, 0)
+            half = 0.5 * (lo + hi)
+            e1 = 0.25 * (((lo + W(1, 0, -1)) + hi) + W(1, 0, 0))    # ct
+            e2 = 0.25 * (((lo + W(-1, 0, -1)) + hi) + W(-1, 0, 0))  # cb
+            e3 = 0.25 * (((lo + W(0, 1, -1)) + hi) + W(0, 1, 0))    # cu
+            e4 = 0.25 * (((lo + W(0, -1, -1)) + hi) + W(0, -1, 0))  # cd
+            rho = rho_of(half)
+            mu_ct, mu_cb, mu_cu, mu_cd, mu_t, mu_c = (mu_of(x) for x in (e1, e2, e3, e4, hi, lo))
+            A, A2 = dt / (Re * rho), (2.0 * dt) / (Re * rho)
+            coefs = (A * mu_ct, A * mu_cb, A * mu_cu, A * mu_cd, A2 * mu_t, A2 * mu_c)
+            xz, yz = cp[0][2], cp[1][2]
+            ex = F(cp[2][0], 0, 0, 0, sh) + A * (idx * (idz * (mu_ct * (F(xz, 1, 0, 0, sh) - F(xz, 1, 0, -1, sh)))
+                                                      - idz * (mu_cb * (F(xz, 0, 0, 0, sh) - F(xz, 0, 0, -1, sh)))))
+            ex = ex + A * (idy * (idz * (mu_cu * (F(yz, 0, 1, 0, sh) - F(yz, 0, 1, -1, sh)))
+                                  - idz * (mu_cd * (F(yz, 0, 0, 0, sh) - F(yz, 0, 0, -1, sh)))))
+        gen, cx, cz = cp[a]
+        new, it = pipe_viscosity_system(comps[a], bs[a], a, coefs, ex, gen, cx if a != 1 else cx, cz, dx, tol,
+                                        max_iter)
+        out.append(new)
+        info[f"coef_{'uvw'[a]}"] = coefs
+        info[f"explicit_{'uvw'[a]}"] = ex
+        info[f"iterations_{'uvw'[a]}"] = it
+    return out[0], out[1], out[2], info

@@ -545,6 +545,27 @@ int fsref_pipe_projection(void* h, double dt) {
   return s.water_projection->poisson_solver.linear_solver->num_iteration;
 }
 
+// VISCOSITY_3D::ApplyViscosity of the pipe (the oil/water semi-implicit
+// branch, VISCOSITY_3D.h:565-990) with the reference's epsilon 1.5 dx
+// (EULERIAN_FLUID_SOLVER_3D.h:394), as Sourcing calls it (:2082).
+void fsref_pipe_viscosity(void* h, double dt) {
+  RefCase* c = static_cast<RefCase*>(h);
+  EULERIAN_FLUID_SOLVER_3D& s = c->world.eulerian_solver;
+  run_threads(c, [&](int t) { s.viscosity_solver->ApplyViscosity(t, s.epsilon_for_mollification, dt); });
+}
+
+// A coefficient field of the last semi-implicit viscosity solve: id = 7 *
+// component + q, q = 0 the explicit term, 1..6 coef_1..coef_6 (interior
+// faces of that component).
+void fsref_visc_field(void* h, int id, double* dst) {
+  VISCOSITY_3D& v = *static_cast<RefCase*>(h)->world.eulerian_solver.viscosity_solver;
+  FIELD_STRUCTURE_3D<T>* f[] = {&v.explicit_term_x, &v.coef_1_x, &v.coef_2_x, &v.coef_3_x, &v.coef_4_x, &v.coef_5_x,
+                                &v.coef_6_x, &v.explicit_term_y, &v.coef_1_y, &v.coef_2_y, &v.coef_3_y, &v.coef_4_y,
+                                &v.coef_5_y, &v.coef_6_y, &v.explicit_term_z, &v.coef_1_z, &v.coef_2_z, &v.coef_3_z,
+                                &v.coef_4_z, &v.coef_5_z, &v.coef_6_z};
+  for_interior(*f[id], [&](T& x, long n) { dst[n] = x; });
+}
+
 // The jump condition and the divergence of the last projection (cells).
 void fsref_projection_jc(void* h, double* dst) {
   PROJECTION_3D& p = *static_cast<RefCase*>(h)->world.eulerian_solver.water_projection;

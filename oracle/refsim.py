@@ -83,6 +83,9 @@ def _lib():
         for fn in ("fsref_pipe_levelset_advection", "fsref_pipe_velocity_advection", "fsref_pipe_reinitialization",
                    "fsref_pipe_gravity"):
             getattr(lib, fn).argtypes = [ctypes.c_void_p, ctypes.c_double]
+    if hasattr(lib, "fsref_pipe_viscosity"):
+        lib.fsref_pipe_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.fsref_visc_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
     if hasattr(lib, "fsref_pipe_projection"):
         lib.fsref_pipe_projection.restype = ctypes.c_int
         lib.fsref_pipe_projection.argtypes = [ctypes.c_void_p, ctypes.c_double]
@@ -560,6 +563,17 @@ class RefCase:
 
     def pipe_gravity(self, dt):
         self._quiet(self._lib.fsref_pipe_gravity, self.h, dt)
+
+    def pipe_viscosity(self, dt):
+        """VISCOSITY_3D::ApplyViscosity of the pipe (semi-implicit, in place)."""
+        self._quiet(self._lib.fsref_pipe_viscosity, self.h, dt)
+
+    def visc_field(self, comp, q):
+        """The explicit term (q = 0) or coef_q (1..6) of component comp
+        ("u", "v", "w") of the last semi-implicit viscosity."""
+        a = np.empty(self.shape(comp))
+        self._lib.fsref_visc_field(self.h, 7 * "uvw".index(comp) + q, _ptr(a))
+        return a
 
     def pipe_projection(self, dt):
         """EULERIAN_FLUID_SOLVER_3D::Projection of the pipe; returns the PCG

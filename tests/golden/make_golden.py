@@ -49,6 +49,9 @@ on the air/water unit-cube box with Neumann pressure walls:
                    deflated system (right-hand side and solution in row
                    order), PCG and the pipe velocity update; then the
                    pipe's CFLOneTimeStep
+  pipe_viscosity   the pipe's VISCOSITY_3D::ApplyViscosity (oil/water
+                   semi-implicit branch): per component the explicit term,
+                   coef_1..coef_6 and the solved velocity
   pipe_frame       one SIMULATION_WORLD::AdvanceOneFrame of the pipe with
                    is_sourcing_active = false (no viscosity): CFL dt and the
                    order-2 step
@@ -327,6 +330,18 @@ def main():
                                        div=c.divergence(), jc=c.projection_jc(), csr_vals=vals, csr_cols=cols,
                                        csr_rowptr=rowptr, b_rows=b_rows, x_rows=x_rows, out_p=c.get("p"),
                                        out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"))
+    c.close()
+
+    # the pipe's semi-implicit viscosity (VISCOSITY_3D::ApplyViscosity, the
+    # oil/water branch): every component's coefficients and explicit term
+    # and the solved velocities
+    c = refsim.RefCase(pipe_sim)
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    c.pipe_viscosity(0.01)
+    vf = {f"{comp}_q{q}": c.visc_field(comp, q) for comp in "uvw" for q in range(7)}
+    fixtures["pipe_viscosity"] = dict(base, dt=0.01, tolerance=1e-6, max_iteration=10000, **vf,
+                                      out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"))
     c.close()
 
     # one whole frame of the pipe with the reference's sourcing step off

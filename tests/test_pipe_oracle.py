@@ -143,3 +143,24 @@ def test_pipe_frame_matches_reference():
     out = O.pipe_step(g["phi"], g["u"], g["v"], g["w"], gr, C, dt, P)
     for name, a in zip(("phi", "u", "v", "w", "p"), out):
         np.testing.assert_array_equal(a, g["out_" + name])
+
+
+def test_pipe_viscosity_matches_reference():
+    """VISCOSITY_3D::ApplyViscosity of the pipe (the reference's oil/water
+    semi-implicit branch), bit for bit: per component the six coefficients
+    and the explicit term on the unknowns (faces inside the pipe), and the
+    solved velocities everywhere."""
+    g = load("pipe_viscosity")
+    gr = grids(g)
+    C = {k: float(g[k]) for k in ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We")}
+    u, v, w, info = O.pipe_viscosity(g["phi"], g["u"], g["v"], g["w"], gr, C, float(g["dt"]), float(g["tolerance"]),
+                                     int(g["max_iteration"]))
+    for a, k in enumerate("uvw"):
+        b = O.pipe_boundary(gr[1 + a], g[k].shape, C["a"])
+        ny = b.shape[1]
+        rows = (b <= 0) & (np.arange(ny)[None, :, None] < (ny - 1 if a == 1 else ny))
+        np.testing.assert_array_equal(info["explicit_" + k][rows], g[f"{k}_q0"][rows])
+        for q in range(6):
+            np.testing.assert_array_equal(info["coef_" + k][q][rows], g[f"{k}_q{q + 1}"][rows])
+    for k, a in zip("uvw", (u, v, w)):
+        np.testing.assert_array_equal(a, g["out_" + k])
