@@ -2000,8 +2000,11 @@ def pipe_step(phi, u, v, w, grids, C, dt, P):
     and projection (the pressure of the first stage is the second's initial
     guess), the reinitialisation by Heun over two blocks.  P: tolerance,
     max_iteration, water_density, oil_density, gravity_y, epsilon,
-    reinit_iterations, reinit_scaling, p0 (optional).  Returns
-    (phi, u, v, w, p)."""
+    reinit_iterations, reinit_scaling, p0 (optional), sourcing (optional:
+    True runs the reference's Sourcing step, the pipe's semi-implicit
+    viscosity, between the body force and the projection, :1466-1469, 2076-
+    2100; the object list's sourcing leaves the fields alone for a pipe
+    whose only object is the water).  Returns (phi, u, v, w, p)."""
     a = C["a"]
     fixed = pipe_fixed_faces((phi.shape[2], phi.shape[1], phi.shape[0]))
     ph1, u, v, w = pipe_weno5_levelset(phi, u, v, w, grids, a, dt, P["epsilon"])
@@ -2012,6 +2015,8 @@ def pipe_step(phi, u, v, w, grids, C, dt, P):
     for _ in range(2):
         u, v, w = pipe_eno3_velocity(u, v, w, grids, a, dt)
         v = pipe_forcing(phi, v, grids, C, P["gravity_y"], P["oil_density"], dt, fixed_v=fixed[1])
+        if P.get("sourcing"):
+            u, v, w, _vinfo = pipe_viscosity(phi, u, v, w, grids, C, dt, P["tolerance"], P["max_iteration"], fixed)
         u, v, w, p, _info = pipe_projection(phi, u, v, w, grids, C, dt, P["tolerance"], P["max_iteration"],
                                             P["water_density"], P["oil_density"], fixed=fixed, p0=p)
     u, v, w = (0.5 * rk[0] + 0.5 * u, 0.5 * rk[1] + 0.5 * v, 0.5 * rk[2] + 0.5 * w)
@@ -2096,7 +2101,7 @@ def _shifted(a, ax, s, fill=0.0):
     return out
 
 
-def pipe_viscosity_system(comp, b, axis, coefs, explicit, gen, dx_copy, dz_copy, dx, tol, max_iter):
+def pipe_viscosity_system(comp, b, axis, coefs, explicit, gen, dx_copy, dz_copy, dx, tol, max_iter, fixed=None):
     """One component of the pipe's semi-implicit solve (SolveForViscosity,
     POISSON_SOLVER_3D.h:342-378, with BuildLinearSystemNodeForSemiImplicit-
     Viscosity :3641-3828 and the boundary tags of SetupBoundaryConditions-
@@ -2109,7 +2114,10 @@ def pipe_viscosity_system(comp, b, axis, coefs, explicit, gen, dx_copy, dz_copy,
     right-hand side the explicit term plus the Dirichlet neighbours'
     coef/dx^2 times their guarded copies (dx_copy along x, dz_copy along z);
     initial guess the masked copy; the reference's PCG (asymmetric matrix,
-    absolute r.z < tol^2).  Returns (new component, iterations)."""
+    absolute r.z < tol^2).  The solution is written back to every unknown
+    but the fixed faces (VectorToGrid, POISSON_SOLVER_3D.h:4060-4077, skips
+    faces Solve_Velocity marked fixed).  Returns (new component,
+    iterations)."""
     g = G
     c1, c2, c3, c4, c5, c6 = coefs
     nz, ny, nx = b.shape
@@ -2157,13 +2165,14 @@ def pipe_viscosity_system(comp, b, axis, coefs, explicit, gen, dx_copy, dz_copy,
         return q + diag * x
 
     x, it, _rz, _rel = pcg(apply, diag, rhs, x0, tol, max_iter, "abs")
-    out = np.where(rows, x, comp)
+    keep = ~rows if fixed is None else (~rows | fixed)
+    out = np.where(keep, comp, x)
     if axis == 1:
         out[:, ny - 1, :] = out[:, 1, :]
     return out, it
 
 
-def pipe_viscosity(phi, u, v, w, grids, C, dt, tol, max_iter):
+def pipe_viscosity(phi, u, v, w, grids, C, dt, tol, max_iter, fixed=None):
     """VISCOSITY_3D::ApplyViscosity of a vertical pipe, the oil/water
     semi-implicit branch in the dimensionless form (VISCOSITY_3D.h:565-990),
     epsilon 1.5 dx (EULERIAN_FLUID_SOLVER_3D.h:394).  Per component, from
@@ -2172,7 +2181,9 @@ def pipe_viscosity(phi, u, v, w, grids, C, dt, tol, max_iter):
     viscosity's Heaviside, :1234-1350) of face and edge averages of the
     periodic level set; coef_q = dt/(Re rho) mu (2 dt/(Re rho) mu along the
     component's own axis); the explicit cross terms; then the implicit solve
-    (pipe_viscosity_system).  Returns (u, v, w, info)."""
+    (pipe_viscosity_system); `fixed` (per component, optional) are the
+    faces Solve_Velocity marked fixed, which keep their value.  Returns
+    (u, v, w, info)."""
     g = G
     dx = grids[0][3]
     idx = idy = idz = 1.0 / dx
@@ -2245,8 +2256,8 @@ def pipe_viscosity(phi, u, v, w, grids, C, dt, tol, max_iter):
             ex = ex + A * (idy * (idz * (mu_cu * (F(yz, 0, 1, 0, sh) - F(yz, 0, 1, -1, sh)))
                                   - idz * (mu_cd * (F(yz, 0, 0, 0, sh) - F(yz, 0, 0, -1, sh)))))
         gen, cx, cz = cp[a]
-        new, it = pipe_viscosity_system(comps[a], bs[a], a, coefs, ex, gen, cx if a != 1 else cx, cz, dx, tol,
-                                        max_iter)
+        new, it = pipe_viscosity_system(comps[a], bs[a], a, coefs, ex, gen, cx, cz, dx, tol, max_iter,
+                                        None if fixed is None else fixed[a])
         out.append(new)
         info[f"coef_{'uvw'[a]}"] = coefs
         info[f"explicit_{'uvw'[a]}"] = ex

@@ -55,6 +55,8 @@ on the air/water unit-cube box with Neumann pressure walls:
   pipe_frame       one SIMULATION_WORLD::AdvanceOneFrame of the pipe with
                    is_sourcing_active = false (no viscosity): CFL dt and the
                    order-2 step
+  pipe_frame_viscous  the same frame with sourcing on, as the reference's own
+                   pipe scripts run it (semi-implicit viscosity in each stage)
 
     python tests/golden/make_golden.py [name ...]   writes only the named fixtures
 """
@@ -359,6 +361,18 @@ def main():
                                   water_density=const["water_density"], dt=dt, iterations=it,
                                   out_phi=c.get("phi"), out_u=c.get("u"), out_v=c.get("v"), out_w=c.get("w"),
                                   out_p=c.get("p"))
+    c.close()
+
+    # the same frame as the reference's own pipe scripts run it, sourcing on
+    # (the semi-implicit viscosity in every velocity stage)
+    c = refsim.RefCase(pipe_sim)
+    for k, a_ in dict(phi=phi, **vel).items():
+        c.set(k, a_)
+    dt, it = c.advance_frame()
+    fixtures["pipe_frame_viscous"] = dict(base, cfl_number=0.8, tolerance=1e-6, max_iteration=10000,
+                                          water_density=const["water_density"], dt=dt, iterations=it,
+                                          out_phi=c.get("phi"), out_u=c.get("u"), out_v=c.get("v"),
+                                          out_w=c.get("w"), out_p=c.get("p"))
     c.close()
 
     only = set(sys.argv[1:])

@@ -164,3 +164,24 @@ def test_pipe_viscosity_matches_reference():
             np.testing.assert_array_equal(info["coef_" + k][q][rows], g[f"{k}_q{q + 1}"][rows])
     for k, a in zip("uvw", (u, v, w)):
         np.testing.assert_array_equal(a, g["out_" + k])
+
+
+def test_pipe_frame_with_viscosity_matches_reference():
+    """One whole AdvanceOneFrame of the pipe as the reference's own pipe
+    scripts run it (sourcing on: the semi-implicit viscosity between the
+    body force and the projection in each velocity stage, the fixed
+    centre-line faces kept), bit for bit, dt included."""
+    g = load("pipe_frame_viscous")
+    gr = grids(g)
+    C = {k: float(g[k]) for k in ("a", "R1", "m", "eta", "K", "g", "f", "A", "V0", "J", "Re", "We")}
+    _, kmax = O.curvature(g["phi"], gr[0][3], typo=True)
+    dt = O.pipe_cfl_dt(g["u"], g["v"], g["w"], gr, C, float(g["gravity_y"]), float(g["water_density"]),
+                       float(g["oil_density"]), kmax) * float(g["cfl_number"])
+    assert dt == float(g["dt"])
+    P = dict(tolerance=float(g["tolerance"]), max_iteration=int(g["max_iteration"]),
+             water_density=float(g["water_density"]), oil_density=float(g["oil_density"]),
+             gravity_y=float(g["gravity_y"]), epsilon=float(g["epsilon"]),
+             reinit_iterations=int(g["reinit_iterations"]), reinit_scaling=int(g["reinit_scaling"]), sourcing=True)
+    out = O.pipe_step(g["phi"], g["u"], g["v"], g["w"], gr, C, dt, P)
+    for name, a in zip(("phi", "u", "v", "w", "p"), out):
+        np.testing.assert_array_equal(a, g["out_" + name])
