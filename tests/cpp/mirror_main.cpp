@@ -44,6 +44,20 @@ int main(int argc, char** argv) {
       std::printf("fast_sweeping %d reinit_iterations %d\n", p.fast_sweeping, p.reinit_iterations);
       return 0;
     }
+    if (mode == "pipe_script") {
+      // the pipe reader's parameters (no GPU needed)
+      SCRIPT_READER r(argv[2]);
+      const SCRIPT_BLOCK& world = r.FindBlock("SIMULATION_WORLD");
+      const SCRIPT_BLOCK& disc = world.FindBlock("WORLD_DISCRETIZATION_OIL_WATER");
+      GRID_STRUCTURE_3D g;
+      g.InitializeFromBlock(disc.FindBlock("GRID_STRUCTURE_3D_VERTICAL"));
+      const fs_params p = pipe_params_from_script(world, r.FindBlock("FLUID_SOLVER_UNIFORM_OIL_WATER"), g);
+      std::printf("pipe %d radius %.17g R1 %.17g V0 %.17g f %.17g eta %.17g We %.17g oil %.17g rho_pos %.17g "
+                  "order %d viscosity %d cfl %.17g\n",
+                  p.pipe, p.pipe_radius, p.pipe_R1, p.pipe_V0, p.pipe_f, p.pipe_eta, p.pipe_We, p.pipe_oil_density,
+                  p.rho_pos, p.order, p.viscosity, p.cfl);
+      return 0;
+    }
     if (mode == "csr" && argc >= 4) {
       std::ifstream f(argv[2], std::ios::binary);
       int hdr[2];

@@ -152,3 +152,23 @@ def test_pipe_mode_scripts_are_refused(mirror, tmp_path):
     res = subprocess.run([mirror, "step", path, "/dev/null", str(tmp_path / "out.bin")], capture_output=True,
                          text=True)
     assert res.returncode != 0 and "pipe mode" in res.stderr
+
+
+def test_cpp_pipe_reader_gives_the_reference_constants(mirror, tmp_path):
+    """The C++ mirror's pipe reader (pipe_params_from_script) derives the
+    reference's dimensionless constants bit for bit (fixture pipe_frame, made
+    by the reference) and refuses a script with the sourcing step on."""
+    from oracle.refsim import write_pipe_sim
+    g = dict(np.load(os.path.join(ROOT, "tests", "golden", "pipe_frame.npz")))
+    n = tuple(int(x) for x in g["n"])
+    path = write_pipe_sim(str(tmp_path / "pipe.sim"), n, tuple(g["lo"]), tuple(g["hi"]), sourcing=False)
+    out = subprocess.run([mirror, "pipe_script", path], check=True, capture_output=True, text=True).stdout.split()
+    val = {out[q]: out[q + 1] for q in range(0, len(out), 2)}
+    assert int(val["pipe"]) == 1 and int(val["viscosity"]) == 0 and int(val["order"]) == 2
+    for key, ref in (("radius", "a"), ("R1", "R1"), ("V0", "V0"), ("f", "f"), ("eta", "eta"), ("We", "We"),
+                     ("oil", "oil_density")):
+        assert float(val[key]) == float(g[ref]), key
+    assert float(val["rho_pos"]) == float(g["water_density"]) / float(g["oil_density"])
+    path = write_pipe_sim(str(tmp_path / "pipe_on.sim"), n, tuple(g["lo"]), tuple(g["hi"]), sourcing=True)
+    res = subprocess.run([mirror, "pipe_script", path], capture_output=True, text=True)
+    assert res.returncode != 0 and "is_sourcing_active" in res.stderr
